@@ -1,0 +1,184 @@
+/*
+ * rsgpu.h -- C ABI of the B200 finite-difference wave-propagation library.
+ *
+ * This is the drop-in boundary beneath RockSeis's C++ drivers.  Each entry
+ * point replaces the body of one reference method; the comment beside it cites
+ * the reference interface (paths relative to the RockSeis source tree).  The
+ * reference-side bindings a maintainer adds are shown in INTEGRATION.md.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Array layouts are the reference's:
+ *      2D grids   a[iz*nx + ix]                (I2D, lib/waves.cpp:4)
+ *      3D grids   a[iz*nx*ny + iy*nx + ix]     (I3D, lib/waves.cpp:8)
+ *      traces     d[it + itr*nt]               (Idat, lib/waves.cpp:13)
+ *      maps       Point2D<int> {x,z} / Point3D<int> {x,y,z} pairs, -1 = off grid
+ *  - Element type of every real array is float for RSGPU_F32_* precisions
+ *    and double for RSGPU_F64.
+ *  - Output trace and image arrays are ACCUMULATED into (+=), exactly like the
+ *    reference's recordData / crossCorr; callers pass zero-initialised arrays
+ *    for a fresh result (the reference's Data2D/Image2D calloc).
+ *  - Every call returns an rsgpu_status; nothing exits or throws.  The text of
+ *    the last error on the calling thread is rsgpu_last_error().
+ *  - No CPU fallback: without a usable CUDA device every compute entry point
+ *    returns RSGPU_ERR_NODEVICE.
+ */
+#ifndef RSGPU_H
+#define RSGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSGPU_ABI_VERSION 1
+
+typedef enum {
+    RSGPU_OK = 0,
+    RSGPU_ERR_ARG = 1,          /* invalid argument (sizes, order, null pointers, ...) */
+    RSGPU_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    RSGPU_ERR_NOMEM = 3,        /* device or pinned-host allocation failed */
+    RSGPU_ERR_STATE = 4,        /* call not valid in the plan's current state */
+    RSGPU_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+    RSGPU_ERR_UNSUPPORTED = 6,  /* option not implemented for this physics */
+    RSGPU_ERR_NODEVICE = 7,     /* no CUDA device / kernels not loadable */
+    RSGPU_ERR_REVOLVE = 8       /* checkpoint schedule reported an error */
+} rsgpu_status;
+
+/* physics */
+enum { RSGPU_ACOUSTIC2D = 0, RSGPU_ELASTIC2D = 1, RSGPU_ACOUSTIC3D = 2, RSGPU_ELASTIC3D = 3 };
+/* arithmetic of the propagator:
+ *   F32_EXACT: float, every operation rounded in the reference's order (no FMA);
+ *              reproduces a stock float build of the reference bit for bit.
+ *   F32_FAST : float, FMA and pre-scaled coefficients.
+ *   F64      : double precision, exact reference order (the FP64 GPU oracle). */
+enum { RSGPU_F32_EXACT = 0, RSGPU_F32_FAST = 1, RSGPU_F64 = 2 };
+/* field codes: identical to the reference's rs_field (include/utils.h:22) */
+enum { RSGPU_PRESSURE = 0, RSGPU_VX = 1, RSGPU_VY = 2, RSGPU_VZ = 3 };
+/* misfit codes: identical to rs_fwimisfit (include/utils.h:26) */
+enum { RSGPU_MISFIT_DIFFERENCE = 0, RSGPU_MISFIT_CORRELATION = 1 };
+/* checkpoint storage precision of the FWI/RTM gradient drivers */
+enum { RSGPU_CKPT_NATIVE = 0, RSGPU_CKPT_F16 = 1, RSGPU_CKPT_BF16 = 2 };
+/* revolve actions: identical to revolve_action (include/revolve.h:25) */
+enum { RSGPU_ADVANCE = 0, RSGPU_TAKESHOT = 1, RSGPU_RESTORE = 2, RSGPU_FIRSTURN = 3,
+       RSGPU_YOUTURN = 4, RSGPU_TERMINATE = 5, RSGPU_ERROR = 6 };
+
+/* Run-wide settings shared by every shot of a batch (the reference's Modelling /
+ * Fwi / Rtm object settings plus Der and Pml construction arguments). */
+typedef struct {
+    int physics;        /* RSGPU_ACOUSTIC2D ... */
+    int precision;      /* RSGPU_F32_EXACT ... */
+    int lpml;           /* Model::getLpml */
+    int order;          /* Der order, clamped to 1..8 like Der::Der (lib/der.cpp:98-99) */
+    int fs;             /* free surface (Model::getFs) */
+    int nt;             /* time samples (Data::getNt) */
+    double dx, dy, dz;  /* grid spacing (dy ignored in 2D) */
+    double dt;          /* time step (Data::getDt) */
+    const void *pml;    /* 12*lpml C-PML tables in the order A,B,C ltf; A,B,C ltf_stag;
+                           A,B,C rbb; A,B,C rbb_stag (include/pml.h:31-81).  NULL: computed
+                           by rsgpu_pml_tables with Smax = 1200. */
+    int tile;           /* kernel tile shape, -1 = autotuned/default */
+    int reserved[7];
+} rsgpu_config;
+
+/* One shot (work item) of a batch.  nx/ny/nz are the UNPADDED window the
+ * reference's local model holds; device arrays are (n + 2*lpml) per axis. */
+typedef struct {
+    int nx, ny, nz;
+    /* Padded, staggered parameters in the order of the reference's Model getters:
+     *  acoustic 2D: Rx, Rz, L              (ModelAcoustic2D::staggerModels, lib/model.cpp:1350)
+     *  elastic 2D : Rx, Rz, L, L2M, M      (ModelElastic2D::staggerModels, lib/model.cpp:2720)
+     *  acoustic 3D: Rx, Ry, Rz, L          (lib/model.cpp:1965)
+     *  elastic 3D : Rx, Ry, Rz, L, L2M, M_yz, M_xz, M_xy   (lib/model.cpp:3371) */
+    const void *model[8];
+    /* source traces (Data2D/3D with SMAP maps, Geometry2D::makeMap lib/geometry.cpp:137) */
+    int nsrc;
+    const int *smap;            /* nsrc * dim ints */
+    const void *sshift;         /* nsrc * dim reals */
+    const void *wavelet;        /* nsrc * nt reals, trace-major */
+    int src_field;              /* RSGPU_PRESSURE / RSGPU_VX / RSGPU_VY / RSGPU_VZ */
+    /* receiver traces (GMAP) */
+    int nrec;
+    const int *gmap;
+    const void *gshift;
+    int rec_field;
+    const void *rec_factor;     /* elastic pressure reciprocity divisor per trace, NULL = 1 */
+    void *rec_out;              /* nrec * nt reals, accumulated (+=) */
+} rsgpu_shot;
+
+typedef struct rsgpu_plan rsgpu_plan;
+
+/* ---------------------------------------------------------------------------
+ * Library
+ * ------------------------------------------------------------------------- */
+int rsgpu_abi_version(void);
+const char *rsgpu_last_error(void);
+/* Number of CUDA devices visible, or 0. */
+int rsgpu_device_count(void);
+
+/* ---------------------------------------------------------------------------
+ * Forward modelling
+ * ------------------------------------------------------------------------- */
+
+/* Replaces ModellingAcoustic2D::run (lib/modelling.cpp:197-291),
+ * ModellingElastic2D::run (lib/modelling.cpp:545-645), ModellingAcoustic3D::run
+ * (lib/modelling.cpp:363-474) and ModellingElastic3D::run (lib/modelling.cpp:727-850):
+ * nt time steps of forwardstepVelocity, forwardstepStress, insertSource and
+ * recordData for every shot of the batch, all shots advancing together.
+ * Host arrays in, host traces accumulated into shots[i].rec_out. */
+rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_shot *shots);
+
+/* The same work split into steps, for callers that keep the batch resident:
+ * create uploads models/maps/wavelets once; run advances steps on the device;
+ * read copies one shot's traces to the host (accumulating). */
+rsgpu_status rsgpu_plan_create(const rsgpu_config *cfg, int nshots, const rsgpu_shot *shots, rsgpu_plan **plan);
+rsgpu_status rsgpu_plan_reset(rsgpu_plan *plan);                 /* zero wavefields, C-PML memory, traces */
+rsgpu_status rsgpu_plan_run(rsgpu_plan *plan, int it0, int nsteps);
+rsgpu_status rsgpu_plan_read_traces(rsgpu_plan *plan, int shot, void *host_out);
+rsgpu_status rsgpu_plan_sync(rsgpu_plan *plan);
+/* cudaStream_t of the plan (as void*), for callers that time it with events */
+void *rsgpu_plan_stream(rsgpu_plan *plan);
+/* Device launches of the propagator kernels issued since the plan was created. */
+long long rsgpu_plan_launch_count(rsgpu_plan *plan);
+/* Copy one wavefield (reference field code, SXX=4.. for elastic) of one shot to the host
+ * in the reference's padded layout (for step-level parity tests). */
+rsgpu_status rsgpu_plan_read_field(rsgpu_plan *plan, int shot, int field, void *host_out);
+void rsgpu_plan_destroy(rsgpu_plan *plan);
+
+/* ---------------------------------------------------------------------------
+ * Host preprocessing (restatements of the reference's host-side code; callers
+ * that hold reference objects pass the reference's own arrays instead)
+ * ------------------------------------------------------------------------- */
+
+/* Pml::computeABC with Amax=0, Kmax=2, Smax=1200 (lib/pml.cpp:79-126). */
+rsgpu_status rsgpu_pml_tables(int lpml, double dt, int precision, void *out12);
+
+/* Model*::staggerModels (lib/model.cpp:93-240, 1350-1411, 1965, 2720-2802, 3371-3475):
+ * pad by lpml with edge replication, form moduli, stagger, invert density,
+ * free-surface adjustments.  vs is ignored for acoustic physics.  out[] receives
+ * the parameters in the rsgpu_shot.model order, each (nx+2l)(ny+2l)(nz+2l). */
+rsgpu_status rsgpu_stagger_model(int physics, int nx, int ny, int nz, int lpml, int fs, int precision,
+                                 const void *vp, const void *vs, const void *rho, void *const *out);
+
+/* Data2D/3D::makeMap -> Geometry2D/3D::makeMap (lib/data.cpp:440-460, 1116-1141;
+ * lib/geometry.cpp:137-230, 303-420) with zero padding arguments.  coords: ntr*dim
+ * doubles (x,z) or (x,y,z) holding the T-typed coordinates; n/o/d: model size,
+ * origin and spacing per axis as in Model::getGeom; gshift: per-axis staggering
+ * shift in cells (the reference uses -0.5 along the component of a VX/VY/VZ
+ * trace set, 0 otherwise; NULL = all 0).  map gets -1 where off the grid. */
+rsgpu_status rsgpu_make_map(int dim, int precision, int ntr, const double *coords, const int *n, const double *o,
+                            const double *d, const double *gshift, int *map, void *shift);
+
+/* ---------------------------------------------------------------------------
+ * Checkpoint schedule
+ * ------------------------------------------------------------------------- */
+/* Revolve<T>::revolve action trace for (nt, ncheck) (lib/revolve.cpp:150-305).
+ * Writes up to max (action, capo, check) triples; returns the count through *n. */
+rsgpu_status rsgpu_revolve_trace(int nt, int ncheck, int max, int *actions, int *capos, int *checks, int *n);
+/* Revolve<T>::numforw (lib/revolve.cpp:31-62) */
+int rsgpu_revolve_numforw(int nt, int ncheck);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RSGPU_H */

@@ -1,0 +1,245 @@
+"""ctypes wrappers of the two CPU checkers (test infrastructure only).
+
+  ORACLE : oracle/librsoracle.so, this repository's C restatement (rs_oracle.c)
+  REF    : oracle/_ref/librsref.so, the unmodified reference library plus the
+           in-process harness (ref_harness*.cpp); present only where it was built.
+
+Only the test-suite, __graft_entry__.smoke() and bench.py's CPU-baseline arm
+import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "librsoracle.so")
+REF_SO = os.path.join(HERE, "_ref", "librsref.so")
+REFSRC = "/root/reference"
+
+
+def build(ref: bool = True) -> None:
+    """Build the checkers (the reference part only where its sources exist)."""
+    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(REFSRC) else [])
+    subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}"] + targets, check=True)
+
+
+class OrcGrid(C.Structure):
+    _fields_ = [("nxp", C.c_int), ("nzp", C.c_int), ("lpml", C.c_int), ("order", C.c_int), ("fs", C.c_int),
+                ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int)]
+
+
+class RefGrid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("lpml", C.c_int), ("order", C.c_int),
+                ("fs", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("ox", C.c_double),
+                ("oy", C.c_double), ("oz", C.c_double), ("dt", C.c_double), ("nt", C.c_int)]
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+_oracle = None
+_ref = None
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        _oracle = C.CDLL(ORACLE_SO)
+        V, I = C.c_void_p, C.c_int
+        _oracle.orc_mod_a2d.argtypes = [C.POINTER(OrcGrid)] + [V] * 4 + [I, V, V, V, I, I, V, V, I, V, I, V]
+        _oracle.orc_mod_e2d.argtypes = [C.POINTER(OrcGrid)] + [V] * 6 + [I, V, V, V, I, I, V, V, I, V, V, I, V]
+        _oracle.orc_e2d_adjoint_steps.argtypes = [C.POINTER(OrcGrid)] + [V] * 6 + [I, V]
+        _oracle.orc_fwi_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 6 + [I, V, V, V, I, V, V, V, V, V, V,
+                                                                                  V, V, V]
+        _oracle.orc_rtm_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 4 + [I, V, V, V, I, V, V, V, I, I, V]
+        _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
+    return _oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError("reference oracle not built (oracle/_ref/librsref.so)")
+        _ref = C.CDLL(REF_SO)
+        V, I, D = C.c_void_p, C.c_int, C.c_double
+        G = C.POINTER(RefGrid)
+        for t in ("f", "d"):
+            getattr(_ref, f"ref_der_{t}").argtypes = [I, I, I, D, D, D, I, I, V, V]
+            getattr(_ref, f"ref_pml_tables_{t}").argtypes = [I, D, V]
+            getattr(_ref, f"ref_mod_a2d_{t}").argtypes = [G, V, V, I, V, V, I, I, V, I, V]
+            getattr(_ref, f"ref_mod_e2d_{t}").argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
+            getattr(_ref, f"ref_fwi_a2d_{t}").argtypes = [G, V, V, I, V, V, I, V, V, I, I, V, V, V, V, V, V]
+        _ref.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
+        _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
+        _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
+        _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
+        _ref.ref_stagger_e2d_f.argtypes = [G, V, V, V, V, V, V, V, V]
+        _ref.ref_stagger_a3d_f.argtypes = [G, V, V, V, V, V, V]
+        _ref.ref_stagger_e3d_f.argtypes = [G, V, V, V] + [V] * 8
+        _ref.ref_makemap2d_f.argtypes = [G, I, V, I, V, V]
+        _ref.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
+        _ref.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
+        _ref.ref_revolve_numforw.argtypes = [I, I]
+        _ref.ref_revolve_adjust.argtypes = [I]
+        _ref.ref_steps_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
+        _ref.ref_steps_a2d_f.argtypes = [G, V, V, I, V, V, I, I, V]
+    return _ref
+
+
+# ---------------------------------------------------------------- problem description
+class Problem2D:
+    """One 2D shot in the form both checkers and the GPU library consume."""
+
+    def __init__(self, nx, nz, dx, dz, lpml, order, fs, dt, nt, vp, rho, vs=None, ox=0.0, oz=0.0):
+        self.nx, self.nz, self.dx, self.dz, self.lpml, self.order, self.fs = nx, nz, dx, dz, lpml, order, fs
+        self.dt, self.nt, self.ox, self.oz = dt, nt, ox, oz
+        self.vp, self.rho, self.vs = vp, rho, vs
+        self.src = self.rec = None
+
+    def ref_grid(self) -> RefGrid:
+        return RefGrid(self.nx, 1, self.nz, self.lpml, self.order, int(self.fs), self.dx, 1.0, self.dz, self.ox,
+                       0.0, self.oz, self.dt, self.nt)
+
+    def orc_grid(self) -> OrcGrid:
+        return OrcGrid(self.nx + 2 * self.lpml, self.nz + 2 * self.lpml, self.lpml, min(max(self.order, 1), 8),
+                       int(self.fs), self.dx, self.dz, self.dt, self.nt)
+
+
+def ref_modelling_a2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32):
+    t = "f" if dtype == np.float32 else "d"
+    out = np.zeros((len(gcoords), pb.nt), dtype)
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    vp, rho, w = (np.ascontiguousarray(a, dtype) for a in (pb.vp, pb.rho, wav))
+    r = getattr(ref(), f"ref_mod_a2d_{t}")(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), sfield, len(gc),
+                                           _p(gc), rfield, _p(out))
+    assert r == 1
+    return out
+
+
+def ref_modelling_e2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32):
+    t = "f" if dtype == np.float32 else "d"
+    out = np.zeros((len(gcoords), pb.nt), dtype)
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    vp, vs, rho = (np.ascontiguousarray(a, dtype) for a in (pb.vp, pb.vs, pb.rho))
+    w = np.ascontiguousarray(wav, dtype)
+    r = getattr(ref(), f"ref_mod_e2d_{t}")(C.byref(g), _p(vp), _p(vs), _p(rho), len(sc), _p(sc), _p(w), sfield,
+                                           len(gc), _p(gc), rfield, _p(out))
+    assert r == 1
+    return out
+
+
+def _keep(*arrs, dtype=None):
+    """Contiguous copies bound to the caller so the buffers outlive the C call."""
+    return [None if a is None else np.ascontiguousarray(a, dtype if dtype is not None else a.dtype) for a in arrs]
+
+
+def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32):
+    t = "f" if dtype == np.float32 else "d"
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    ns, nr = len(sc), len(gc)
+    vpg = np.zeros((pb.nz, pb.nx), dtype)
+    rhog = np.zeros((pb.nz, pb.nx), dtype)
+    wg = np.zeros((ns, pb.nt), dtype)
+    dm = np.zeros((nr, pb.nt), dtype)
+    dr = np.zeros((nr, pb.nt), dtype)
+    mis = C.c_double()
+    vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=dtype)
+    r = getattr(ref(), f"ref_fwi_a2d_{t}")(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
+                                           ncheck, 0, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
+    assert r == 1
+    return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
+
+
+def ref_rtm_a2d(pb, scoords, wav, gcoords, data, ncheck, nhx=1, nhz=1):
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    img = np.zeros((nhz, nhx, pb.nz, pb.nx), np.float32)
+    vp, rho, w, d = _keep(pb.vp, pb.rho, wav, data, dtype=np.float32)
+    r = ref().ref_rtm_a2d_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d), ncheck,
+                            nhx, nhz, _p(img))
+    assert r == 1
+    return img
+
+
+def ref_revolve_trace(nt, ncheck, maxn=200000):
+    a = np.zeros(maxn, np.int32)
+    c = np.zeros(maxn, np.int32)
+    k = np.zeros(maxn, np.int32)
+    n = ref().ref_revolve_trace(nt, ncheck, _p(a), _p(c), _p(k), maxn)
+    assert n > 0
+    return a[:n], c[:n], k[:n]
+
+
+# ---------------------------------------------------------------- restated oracle drivers
+def orc_modelling_a2d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, rfield, nsteps=None,
+                      want_state=False):
+    g = pb.orc_grid()
+    nr = len(gmap)
+    out = np.zeros((nr, pb.nt), np.float32)
+    nxp, nzp = pb.nx + 2 * pb.lpml, pb.nz + 2 * pb.lpml
+    st = np.zeros((3, nzp, nxp), np.float32) if want_state else None
+    Rx, Rz, L, tb, ss, w, gs = _keep(*padded, tab, sshift, wav, gshift, dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    oracle().orc_mod_a2d(C.byref(g), _p(Rx), _p(Rz), _p(L), _p(tb), len(sm), _p(sm), _p(ss), _p(w), sfield, nr,
+                         _p(gm), _p(gs), rfield, _p(out), pb.nt if nsteps is None else nsteps, _p(st))
+    return (out, st) if want_state else out
+
+
+def orc_modelling_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, rfield, factor=None, nsteps=None,
+                      want_state=False):
+    g = pb.orc_grid()
+    nr = len(gmap)
+    out = np.zeros((nr, pb.nt), np.float32)
+    nxp, nzp = pb.nx + 2 * pb.lpml, pb.nz + 2 * pb.lpml
+    st = np.zeros((5, nzp, nxp), np.float32) if want_state else None
+    Rx, Rz, L, L2M, M, tb, ss, w, gs, fac = _keep(*padded, tab, sshift, wav, gshift, factor, dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    oracle().orc_mod_e2d(C.byref(g), _p(Rx), _p(Rz), _p(L), _p(L2M), _p(M), _p(tb), len(sm), _p(sm), _p(ss), _p(w),
+                         sfield, nr, _p(gm), _p(gs), rfield, _p(fac), _p(out), pb.nt if nsteps is None else nsteps,
+                         _p(st))
+    return (out, st) if want_state else out
+
+
+def orc_fwi_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
+    g = pb.orc_grid()
+    ns, nr = len(smap), len(gmap)
+    vpg = np.zeros((pb.nz, pb.nx), np.float32)
+    rhog = np.zeros((pb.nz, pb.nx), np.float32)
+    wg = np.zeros((ns, pb.nt), np.float32)
+    dm = np.zeros((nr, pb.nt), np.float32)
+    dr = np.zeros((nr, pb.nt), np.float32)
+    mis = C.c_double()
+    Rx, Rz, L, tb, ss, w, gs, ob, vp, rho = _keep(*padded, tab, sshift, wav, gshift, obs, pb.vp, pb.rho,
+                                                  dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    r = oracle().orc_fwi_a2d(C.byref(g), pb.nx, pb.nz, _p(vp), _p(rho), _p(Rx), _p(Rz), _p(L), _p(tb), ns, _p(sm),
+                             _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr),
+                             C.byref(mis))
+    assert r == 0
+    return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
+
+
+def orc_rtm_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, data, nhx=1, nhz=1):
+    g = pb.orc_grid()
+    img = np.zeros((nhz, nhx, pb.nz, pb.nx), np.float32)
+    Rx, Rz, L, tb, ss, w, gs, d = _keep(*padded, tab, sshift, wav, gshift, data, dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    r = oracle().orc_rtm_a2d(C.byref(g), pb.nx, pb.nz, _p(Rx), _p(Rz), _p(L), _p(tb), len(sm), _p(sm), _p(ss), _p(w),
+                             len(gm), _p(gm), _p(gs), _p(d), nhx, nhz, _p(img))
+    assert r == 0
+    return img

@@ -1,0 +1,39 @@
+/*
+ * ref_harness_rtm.cpp -- extern "C" driver of the unmodified reference RTM
+ * classes.  A separate translation unit because the reference's fwi.h and
+ * rtm.h both declare rs_snapmethod.  Test infrastructure only.
+ */
+#include "ref_harness_common.h"
+#include "rtm.h"
+
+using namespace rockseis;
+using namespace refh;
+
+namespace {
+/* ---------------------------------------------------------------- RTM image */
+template <typename T>
+int rtm_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav,
+            int nr, const double *gc, const T *data, int ncheck, int nhx, int nhz, T *image)
+{
+    auto model = make_a2d<T>(g, vp, rho);
+    auto src = make_data2d<T>(ns, g, sc, PRESSURE, SMAP, model->getGeom(), wav);
+    auto drec = make_data2d<T>(nr, g, gc, PRESSURE, GMAP, model->getGeom(), data);
+    auto img = std::make_shared<Image2D<T>>(g->nx, g->nz, nhx, nhz, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
+    RtmAcoustic2D<T> rtm(model, img, src, drec, g->order, 1);
+    rtm.setNcheck(ncheck);
+    rtm.setIncore(true);
+    rtm.setSnapfile(tmpname("rtma2d"));
+    int r = rtm.run_optimal();
+    std::memcpy(image, img->getImagedata(), sizeof(T) * (size_t)g->nx * g->nz * nhx * nhz);
+    return r;
+}
+
+} // namespace
+
+extern "C" {
+int ref_rtm_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                  const float *wav, int nr, const double *gc, const float *data, int ncheck, int nhx,
+                  int nhz, float *image)
+{ return rtm_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, data, ncheck, nhx, nhz, image); }
+
+} // extern "C"

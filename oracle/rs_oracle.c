@@ -1,0 +1,520 @@
+/*
+ * rs_oracle.c -- CPU restatement of the RockSeis finite-difference hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The test-suite uses this file as the checker for
+ * the CUDA library (rockseis_b200/librsgpu.so); the product never links or
+ * calls it.  It is pinned against the unmodified reference (oracle/_ref,
+ * built from the reference's own sources) by tests/test_oracle_pin.py and
+ * against the committed fixtures in tests/golden/.
+ *
+ * Scope: one shot, float arithmetic in the reference's operation order (build
+ * with -ffp-contract=off), inputs already preprocessed the way the reference's
+ * Model/Pml/Geometry classes hold them:
+ *   - padded staggered parameters (Rx, Rz, L [, L2M, M]) in a[iz*nxp + ix];
+ *   - C-PML tables, 12 arrays of lpml: A,B,C ltf; A,B,C ltf_stag; A,B,C rbb; A,B,C rbb_stag;
+ *   - trace maps (x,z) and shifts as produced by Geometry2D::makeMap;
+ *   - traces d[it + itr*nt].
+ * Reference functions restated (paths relative to the RockSeis tree):
+ *   Der::ddx_fw/ddz_fw/ddx_bw/ddz_bw       lib/der.cpp:155-540
+ *   WavesAcoustic2D::forwardstep*           lib/waves.cpp:217-404
+ *   WavesAcoustic2D::insertSource/record    lib/waves.cpp:407-595
+ *   WavesElastic2D::forwardstep*            lib/waves.cpp:1416-1735
+ *   WavesElastic2D::backwardstep*           lib/waves.cpp:1738-2080
+ *   WavesElastic2D::insertSource/record     lib/waves.cpp:2085-2288
+ *   FwiAcoustic2D::crossCorr                lib/fwi.cpp:511-571
+ *   FwiAcoustic2D::computeMisfit/Residuals  lib/fwi.cpp:574-1027 (DIFFERENCE)
+ *   FwiAcoustic2D::run_optimal              lib/fwi.cpp:1159-1332 (all states kept in memory)
+ *   RtmAcoustic2D::crossCorr/run_optimal    lib/rtm.cpp:191-219, 423-545
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* optimised staggered coefficients per half-length K (lib/der.cpp:3-53) */
+static const double COEF[9][8] = {
+    {0, 0, 0, 0, 0, 0, 0, 0},
+    {(double)1.0029f, 0, 0, 0, 0, 0, 0, 0},
+    {1.188401e+0, -7.046382e-2, 0, 0, 0, 0, 0, 0},
+    {1.216624e+0, -9.197724e-2, 1.300041e-2, 0, 0, 0, 0, 0},
+    {1.230862e+0, -1.034123e-1, 2.011671e-2, -3.245760e-3, 0, 0, 0, 0},
+    {1.239407e+0, -1.105315e-1, 2.496329e-2, -5.804879e-3, 9.358680e-4, 0, 0, 0},
+    {1.245095e+0, -1.153979e-1, 2.848442e-2, -7.899473e-3, 1.898222e-3, -2.935304e-4, 0, 0},
+    {1.249150e+0, -1.189375e-1, 3.116091e-2, -9.623004e-3, 2.812069e-3, -6.655106e-4, 9.728191e-5, 0},
+    {1.252186e+0, -1.216289e-1, 3.326513e-2, -1.105777e-2, 3.647865e-3, -1.066144e-3, 2.437491e-4, -3.351959e-5},
+};
+
+typedef struct {
+    int nxp, nzp;      /* padded grid */
+    int lpml, order, fs;
+    float dx, dz, dt;
+    int nt;
+} orc_grid;
+
+/* Coefficient pairs used at index i of an axis of length n: the reference's three
+ * loops overwrite each other near the ends, the last writer defines the rule. */
+static int k_fw(int i, int n, int order)
+{
+    if (i >= n - 1) return 0;
+    if (i >= n - order - 1) return n - 1 - i;
+    if (i >= order - 1) return order;
+    return i + 1;
+}
+static int k_bw(int i, int n, int order)
+{
+    if (i >= n - order) return n - i;
+    if (i >= order) return order;
+    return i;
+}
+
+/* forward staggered derivative at linear index p along stride s; pos/n for the order rule */
+static float d_fw(const float *f, long p, long s, int pos, int n, int order, float d)
+{
+    int K = k_fw(pos, n, order);
+    if (K == 0) return 0.0f;
+    float c[8];
+    for (int k = 0; k < K; k++) c[k] = (float)COEF[K][k];
+    float acc = (f[p + s] - f[p]) * c[0];
+    for (int k = 1; k < K; k++) acc += (f[p + (k + 1) * s] - f[p - k * s]) * c[k];
+    return acc / d;
+}
+static float d_bw(const float *f, long p, long s, int pos, int n, int order, float d)
+{
+    int K = k_bw(pos, n, order);
+    if (K == 0) return 0.0f;
+    float c[8];
+    for (int k = 0; k < K; k++) c[k] = (float)COEF[K][k];
+    float acc = (f[p] - f[p - s]) * c[0];
+    for (int k = 1; k < K; k++) acc += (f[p + k * s] - f[p - (k + 1) * s]) * c[k];
+    return acc / d;
+}
+
+/* whole-array derivatives (which: 0 x_fw, 2 z_fw, 3 x_bw, 5 z_bw), for Der parity tests */
+void orc_der2d(int nxp, int nzp, int order, float dx, float dz, int which, const float *f, float *df)
+{
+    for (int iz = 0; iz < nzp; iz++)
+        for (int ix = 0; ix < nxp; ix++) {
+            long p = (long)iz * nxp + ix;
+            switch (which) {
+            case 0: df[p] = d_fw(f, p, 1, ix, nxp, order, dx); break;
+            case 2: df[p] = d_fw(f, p, nxp, iz, nzp, order, dz); break;
+            case 3: df[p] = d_bw(f, p, 1, ix, nxp, order, dx); break;
+            default: df[p] = d_bw(f, p, nxp, iz, nzp, order, dz); break;
+            }
+        }
+}
+
+/* C-PML strip of a coordinate: returns table index (or -1) and sets table base (0 ltf, 6 rbb) */
+static int strip(int i, int n, int L, int *base, int *slot)
+{
+    if (i < L) { *base = 0; *slot = i; return i; }
+    if (i >= n - L) { *base = 6; *slot = L + (i - (n - L)); return i - (n - L); }
+    return -1;
+}
+
+/* psi = B*psi + A*df ;  F -= a*(psi + C*df)   (lib/waves.cpp:252-253) */
+static float cpml(float F, float a, float df, float *psi, const float *tab, int L, int base, int idx)
+{
+    *psi = tab[(base + 1) * L + idx] * (*psi) + tab[(base + 0) * L + idx] * df;
+    return F - a * (*psi + tab[(base + 2) * L + idx] * df);
+}
+
+/* ------------------------------------------------------------------ wave state */
+typedef struct {
+    orc_grid g;
+    int elastic;
+    float *f[5];          /* A: P,Vx,Vz   E: Vx,Vz,Sxx,Szz,Sxz */
+    float *psix[4];       /* [nzp][2L] */
+    float *psiz[4];       /* [2L][nxp] */
+} orc_state;
+
+static void st_alloc(orc_state *s, const orc_grid *g, int elastic)
+{
+    s->g = *g;
+    s->elastic = elastic;
+    long n = (long)g->nxp * g->nzp;
+    int nf = elastic ? 5 : 3, np = elastic ? 4 : 2;
+    for (int k = 0; k < 5; k++) s->f[k] = k < nf ? calloc(n, sizeof(float)) : NULL;
+    for (int k = 0; k < 4; k++) {
+        s->psix[k] = k < np ? calloc((long)g->nzp * 2 * g->lpml, sizeof(float)) : NULL;
+        s->psiz[k] = k < np ? calloc((long)g->nxp * 2 * g->lpml, sizeof(float)) : NULL;
+    }
+}
+static void st_free(orc_state *s)
+{
+    for (int k = 0; k < 5; k++) free(s->f[k]);
+    for (int k = 0; k < 4; k++) { free(s->psix[k]); free(s->psiz[k]); }
+}
+static long st_bytes_fields(const orc_state *s) { return (long)s->g.nxp * s->g.nzp * (s->elastic ? 5 : 3); }
+static void st_copy_fields(float *dst, const orc_state *s)
+{
+    long n = (long)s->g.nxp * s->g.nzp;
+    for (int k = 0; k < (s->elastic ? 5 : 3); k++) memcpy(dst + k * n, s->f[k], n * sizeof(float));
+}
+
+/* ------------------------------------------------------------------ acoustic 2D step */
+static void a2d_step(orc_state *s, const float *Rx, const float *Rz, const float *Lm, const float *tab)
+{
+    const orc_grid *g = &s->g;
+    const int nx = g->nxp, nz = g->nzp, L = g->lpml;
+    float *P = s->f[0], *Vx = s->f[1], *Vz = s->f[2];
+    int b, sl, t;
+    for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+            long p = (long)iz * nx + ix;
+            float dfx = d_fw(P, p, 1, ix, nx, g->order, g->dx);
+            float ax = g->dt * Rx[p];
+            Vx[p] += ax * dfx;
+            if ((t = strip(ix, nx, L, &b, &sl)) >= 0) Vx[p] = cpml(Vx[p], ax, dfx, &s->psix[0][(long)iz * 2 * L + sl], tab, L, b + 3, t);
+            float dfz = d_fw(P, p, nx, iz, nz, g->order, g->dz);
+            float az = g->dt * Rz[p];
+            Vz[p] += az * dfz;
+            if ((t = strip(iz, nz, L, &b, &sl)) >= 0) Vz[p] = cpml(Vz[p], az, dfz, &s->psiz[0][(long)sl * nx + ix], tab, L, b + 3, t);
+        }
+    for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+            long p = (long)iz * nx + ix;
+            float al = g->dt * Lm[p];
+            float dfx = d_bw(Vx, p, 1, ix, nx, g->order, g->dx);
+            P[p] += al * dfx;
+            if ((t = strip(ix, nx, L, &b, &sl)) >= 0) P[p] = cpml(P[p], al, dfx, &s->psix[1][(long)iz * 2 * L + sl], tab, L, b, t);
+            float dfz = d_bw(Vz, p, nx, iz, nz, g->order, g->dz);
+            P[p] += al * dfz;
+            if ((t = strip(iz, nz, L, &b, &sl)) >= 0) P[p] = cpml(P[p], al, dfz, &s->psiz[1][(long)sl * nx + ix], tab, L, b, t);
+        }
+}
+
+/* ------------------------------------------------------------------ elastic 2D steps */
+static void e2d_vel(orc_state *s, const float *Rx, const float *Rz, const float *Lm, const float *L2M,
+                    const float *M, const float *tab, int adj)
+{
+    const orc_grid *g = &s->g;
+    const int nx = g->nxp, nz = g->nzp, L = g->lpml;
+    float *Vx = s->f[0], *Vz = s->f[1], *Sxx = s->f[2], *Szz = s->f[3], *Sxz = s->f[4];
+    long n = (long)nx * nz;
+    const float *w1 = Sxx, *w2 = Sxz, *w3 = Szz;
+    float *b1 = NULL, *b2 = NULL, *b3 = NULL;
+    if (adj) {
+        /* adjoint work arrays (lib/waves.cpp:1774, 1812, 1885) */
+        b1 = malloc(n * sizeof(float)); b2 = malloc(n * sizeof(float)); b3 = malloc(n * sizeof(float));
+        for (long p = 0; p < n; p++) {
+            b1[p] = L2M[p] * Sxx[p] + Lm[p] * Szz[p];
+            b2[p] = M[p] * Sxz[p];
+            b3[p] = Lm[p] * Sxx[p] + L2M[p] * Szz[p];
+        }
+        w1 = b1; w2 = b2; w3 = b3;
+    }
+    int b, sl, t;
+    for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+            long p = (long)iz * nx + ix;
+            float a = g->dt * Rx[p];
+            float d1 = d_fw(w1, p, 1, ix, nx, g->order, g->dx);
+            Vx[p] += a * d1;
+            if ((t = strip(ix, nx, L, &b, &sl)) >= 0) Vx[p] = cpml(Vx[p], a, d1, &s->psix[0][(long)iz * 2 * L + sl], tab, L, b + 3, t);
+            float d2 = d_bw(w2, p, nx, iz, nz, g->order, g->dz);
+            Vx[p] += a * d2;
+            if ((t = strip(iz, nz, L, &b, &sl)) >= 0) Vx[p] = cpml(Vx[p], a, d2, &s->psiz[0][(long)sl * nx + ix], tab, L, b, t);
+            a = g->dt * Rz[p];
+            d1 = d_bw(w2, p, 1, ix, nx, g->order, g->dx);
+            Vz[p] += a * d1;
+            if ((t = strip(ix, nx, L, &b, &sl)) >= 0) Vz[p] = cpml(Vz[p], a, d1, &s->psix[1][(long)iz * 2 * L + sl], tab, L, b, t);
+            d2 = d_fw(w3, p, nx, iz, nz, g->order, g->dz);
+            Vz[p] += a * d2;
+            if ((t = strip(iz, nz, L, &b, &sl)) >= 0) Vz[p] = cpml(Vz[p], a, d2, &s->psiz[1][(long)sl * nx + ix], tab, L, b + 3, t);
+        }
+    free(b1); free(b2); free(b3);
+}
+
+static void e2d_str(orc_state *s, const float *Lm, const float *L2M, const float *M, const float *tab, int adj)
+{
+    const orc_grid *g = &s->g;
+    const int nx = g->nxp, nz = g->nzp, L = g->lpml;
+    float *Vx = s->f[0], *Vz = s->f[1], *Sxx = s->f[2], *Szz = s->f[3], *Sxz = s->f[4];
+    int b, sl, t;
+    for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+            long p = (long)iz * nx + ix;
+            float d1 = d_bw(Vx, p, 1, ix, nx, g->order, g->dx);
+            float d2 = d_bw(Vz, p, nx, iz, nz, g->order, g->dz);
+            if (!adj) {
+                float a2 = g->dt * L2M[p], a1 = g->dt * Lm[p];
+                Sxx[p] += a2 * d1;
+                Szz[p] += a1 * d1;
+                if ((t = strip(ix, nx, L, &b, &sl)) >= 0) {
+                    float *ps = &s->psix[2][(long)iz * 2 * L + sl];
+                    *ps = tab[(b + 1) * L + t] * (*ps) + tab[b * L + t] * d1;
+                    Sxx[p] -= a2 * (*ps + tab[(b + 2) * L + t] * d1);
+                    Szz[p] -= a1 * (*ps + tab[(b + 2) * L + t] * d1);
+                }
+                Sxx[p] += a1 * d2;
+                Szz[p] += a2 * d2;
+                if ((t = strip(iz, nz, L, &b, &sl)) >= 0) {
+                    float *ps = &s->psiz[2][(long)sl * nx + ix];
+                    *ps = tab[(b + 1) * L + t] * (*ps) + tab[b * L + t] * d2;
+                    Sxx[p] -= a1 * (*ps + tab[(b + 2) * L + t] * d2);
+                    Szz[p] -= a2 * (*ps + tab[(b + 2) * L + t] * d2);
+                }
+            } else {
+                Sxx[p] += g->dt * d1;
+                if ((t = strip(ix, nx, L, &b, &sl)) >= 0) Sxx[p] = cpml(Sxx[p], g->dt, d1, &s->psix[2][(long)iz * 2 * L + sl], tab, L, b, t);
+                Szz[p] += g->dt * d2;
+                if ((t = strip(iz, nz, L, &b, &sl)) >= 0) Szz[p] = cpml(Szz[p], g->dt, d2, &s->psiz[2][(long)sl * nx + ix], tab, L, b, t);
+            }
+            if (g->fs && iz == L) Szz[p] = 0.0f;
+            float a = adj ? g->dt : g->dt * M[p];
+            d1 = d_fw(Vz, p, 1, ix, nx, g->order, g->dx);
+            Sxz[p] += a * d1;
+            if ((t = strip(ix, nx, L, &b, &sl)) >= 0) Sxz[p] = cpml(Sxz[p], a, d1, &s->psix[3][(long)iz * 2 * L + sl], tab, L, b + 3, t);
+            d2 = d_fw(Vx, p, nx, iz, nz, g->order, g->dz);
+            Sxz[p] += a * d2;
+            if ((t = strip(iz, nz, L, &b, &sl)) >= 0) Sxz[p] = cpml(Sxz[p], a, d2, &s->psiz[3][(long)sl * nx + ix], tab, L, b + 3, t);
+        }
+}
+
+/* ------------------------------------------------------------------ sources / receivers */
+/* field codes (include/utils.h:22): 0 PRESSURE, 1 VX, 3 VZ */
+static void inject(orc_state *s, const float *Mod, int field, int ntr, const int *map, const float *shift,
+                   const float *wav, int it)
+{
+    const orc_grid *g = &s->g;
+    const int nx = g->nxp, L = g->lpml;
+    for (int i = 0; i < ntr; i++) {
+        if (map[2 * i] < 0 || map[2 * i + 1] < 0) continue;
+        float xt[2] = {1 - shift[2 * i], shift[2 * i]}, zt[2] = {1 - shift[2 * i + 1], shift[2 * i + 1]};
+        for (int i1 = 0; i1 < 2; i1++)
+            for (int i2 = 0; i2 < 2; i2++) {
+                long p = (long)(L + map[2 * i + 1] + i1) * nx + (L + map[2 * i] + i2);
+                float w = wav[it + (long)i * g->nt];
+                if (!s->elastic) {
+                    float *F = field == 0 ? s->f[0] : field == 1 ? s->f[1] : s->f[2];
+                    F[p] += g->dt * Mod[p] * w * xt[i2] * zt[i1];
+                } else if (field == 0) {
+                    s->f[2][p] -= g->dt * w * xt[i2] * zt[i1];
+                    s->f[3][p] -= g->dt * w * xt[i2] * zt[i1];
+                } else {
+                    float *F = field == 1 ? s->f[0] : s->f[1];
+                    F[p] += g->dt * Mod[p] * w * xt[i2] * zt[i1];
+                }
+            }
+    }
+}
+
+static void record(const orc_state *s, int field, int ntr, const int *map, const float *shift, const float *factor,
+                   float *out, int it)
+{
+    const orc_grid *g = &s->g;
+    const int nx = g->nxp, L = g->lpml;
+    for (int i = 0; i < ntr; i++) {
+        if (map[2 * i] < 0 || map[2 * i + 1] < 0) continue;
+        float xt[2] = {1 - shift[2 * i], shift[2 * i]}, zt[2] = {1 - shift[2 * i + 1], shift[2 * i + 1]};
+        float *o = &out[it + (long)i * g->nt];
+        for (int i1 = 0; i1 < 2; i1++)
+            for (int i2 = 0; i2 < 2; i2++) {
+                long p = (long)(L + map[2 * i + 1] + i1) * nx + (L + map[2 * i] + i2);
+                if (!s->elastic) {
+                    const float *F = field == 0 ? s->f[0] : field == 1 ? s->f[1] : s->f[2];
+                    *o += xt[i2] * zt[i1] * F[p];
+                } else if (field == 0) {
+                    float fac = factor ? factor[i] : 1.0f;
+                    *o += (1. / 2.) * xt[i2] * zt[i1] * s->f[2][p] / fac;
+                    *o += (1. / 2.) * xt[i2] * zt[i1] * s->f[3][p] / fac;
+                } else {
+                    const float *F = field == 1 ? s->f[0] : s->f[1];
+                    *o += xt[i2] * zt[i1] * F[p];
+                }
+            }
+    }
+}
+
+static const float *src_mod_a2d(int field, const float *Rx, const float *Rz, const float *Lm)
+{
+    return field == 0 ? Lm : field == 1 ? Rx : Rz;
+}
+
+/* ------------------------------------------------------------------ drivers */
+/* ModellingAcoustic2D::run for one shot.  models: Rx, Rz, L.  nsteps <= nt steps
+ * are run (nsteps < nt gives a bounded sample for CPU timing).  state_out, if
+ * given, receives P,Vx,Vz after the last step. */
+int orc_mod_a2d(const orc_grid *g, const float *Rx, const float *Rz, const float *Lm, const float *tab,
+                int ns, const int *smap, const float *sshift, const float *wav, int sfield,
+                int nr, const int *gmap, const float *gshift, int rfield, float *out, int nsteps, float *state_out)
+{
+    orc_state s;
+    st_alloc(&s, g, 0);
+    for (int it = 0; it < nsteps; it++) {
+        a2d_step(&s, Rx, Rz, Lm, tab);
+        inject(&s, src_mod_a2d(sfield, Rx, Rz, Lm), sfield, ns, smap, sshift, wav, it);
+        record(&s, rfield, nr, gmap, gshift, NULL, out, it);
+    }
+    if (state_out) st_copy_fields(state_out, &s);
+    st_free(&s);
+    return 0;
+}
+
+/* ModellingElastic2D::run for one shot.  models: Rx, Rz, L, L2M, M. */
+int orc_mod_e2d(const orc_grid *g, const float *Rx, const float *Rz, const float *Lm, const float *L2M,
+                const float *M, const float *tab, int ns, const int *smap, const float *sshift, const float *wav,
+                int sfield, int nr, const int *gmap, const float *gshift, int rfield, const float *factor, float *out,
+                int nsteps, float *state_out)
+{
+    orc_state s;
+    st_alloc(&s, g, 1);
+    const float *smod = sfield == 1 ? Rx : Rz;
+    for (int it = 0; it < nsteps; it++) {
+        e2d_vel(&s, Rx, Rz, Lm, L2M, M, tab, 0);
+        e2d_str(&s, Lm, L2M, M, tab, 0);
+        inject(&s, smod, sfield, ns, smap, sshift, wav, it);
+        record(&s, rfield, nr, gmap, gshift, factor, out, it);
+    }
+    if (state_out) st_copy_fields(state_out, &s);
+    st_free(&s);
+    return 0;
+}
+
+/* One adjoint (backward) elastic step from a given state, for step-level tests.
+ * state: Vx,Vz,Sxx,Szz,Sxz in/out; C-PML memory starts at zero. */
+int orc_e2d_adjoint_steps(const orc_grid *g, const float *Rx, const float *Rz, const float *Lm, const float *L2M,
+                          const float *M, const float *tab, int nsteps, float *state)
+{
+    orc_state s;
+    st_alloc(&s, g, 1);
+    long n = (long)g->nxp * g->nzp;
+    for (int k = 0; k < 5; k++) memcpy(s.f[k], state + k * n, n * sizeof(float));
+    for (int it = 0; it < nsteps; it++) {
+        e2d_vel(&s, Rx, Rz, Lm, L2M, M, tab, 1);
+        e2d_str(&s, Lm, L2M, M, tab, 1);
+    }
+    st_copy_fields(state, &s);
+    st_free(&s);
+    return 0;
+}
+
+/* Forward pressure paired with the adjoint field at time index `it` by the
+ * reference's Revolve-driven loops: at FIRSTURN (it = nt-1) the forward field has
+ * just been stepped to it; at every YOUTURN the forward field was advanced only to
+ * the state before step it (lib/fwi.cpp:1213-1217, 1281-1289; lib/rtm.cpp:459-524),
+ * i.e. the state after step it-1, and the zero initial state for it = 0. */
+static const float *fw_state_at(const float *Ps, const float *zero, long n, int nt, int it)
+{
+    if (it == nt - 1) return Ps + (size_t)it * n;
+    if (it == 0) return zero;
+    return Ps + (size_t)(it - 1) * n;
+}
+
+/* FwiAcoustic2D::crossCorr (lib/fwi.cpp:511-571), unpadded interior 1..n-2 */
+static void a2d_corr(const orc_grid *g, int nx, int nz, const float *Vp, const float *Rho, const float *Rx,
+                     const float *Rz, const float *wsp, const float *wrx, const float *wrz, float *vpgrad,
+                     float *rhograd)
+{
+    const int L = g->lpml, nxp = g->nxp;
+    const float dx = g->dx, dz = g->dz;
+    for (int ix = 1; ix < nx - 1; ix++)
+        for (int iz = 1; iz < nz - 1; iz++) {
+            long q = (long)(iz + L) * nxp + (ix + L);
+            float vpscale = -2.0 / (Vp[(long)iz * nx + ix]);
+            float rhoscale1 = -1.0 / (Rho[(long)iz * nx + ix]);
+            float mrxx = (wrx[q] - wrx[q - 1]) / dx;
+            float mrzz = (wrz[q] - wrz[q - nxp]) / dz;
+            vpgrad[(long)iz * nx + ix] -= vpscale * wsp[q] * (mrxx + mrzz);
+            rhograd[(long)iz * nx + ix] -= rhoscale1 * wsp[q] * (mrxx + mrzz);
+            float uderx = 0.5 * wrx[q] * Rx[q] * (wsp[q + 1] - wsp[q]) / dx;
+            uderx += 0.5 * wrx[q - 1] * Rx[q - 1] * (wsp[q] - wsp[q - 1]) / dx;
+            float uderz = 0.5 * wrz[q] * Rz[q] * (wsp[q + nxp] - wsp[q]) / dz;
+            uderz += 0.5 * wrz[q - nxp] * Rz[q - nxp] * (wsp[q] - wsp[q - nxp]) / dz;
+            rhograd[(long)iz * nx + ix] += (uderx + uderz);
+        }
+}
+
+/* FwiAcoustic2D::run_optimal with the DIFFERENCE misfit and pressure data, one shot.
+ * The forward states are kept for every step instead of being recomputed from
+ * checkpoints; recomputation is deterministic, so the gradient is the same.
+ * The pairing of forward and adjoint time levels follows fw_state_at().
+ * vp, rho: unpadded models [nz][nx]; outputs accumulate (+=) like the reference. */
+int orc_fwi_a2d(const orc_grid *g, int nx, int nz, const float *vp, const float *rho, const float *Rx,
+                const float *Rz, const float *Lm, const float *tab, int ns, const int *smap, const float *sshift,
+                const float *wav, int nr, const int *gmap, const float *gshift, const float *obs, float *vpgrad,
+                float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
+{
+    const int nt = g->nt;
+    const long n = (long)g->nxp * g->nzp;
+    float *Ps = malloc((size_t)nt * n * sizeof(float));
+    if (!Ps) return -1;
+    orc_state fw, bw;
+    st_alloc(&fw, g, 0);
+    st_alloc(&bw, g, 0);
+    for (int it = 0; it < nt; it++) {
+        a2d_step(&fw, Rx, Rz, Lm, tab);
+        inject(&fw, Lm, 0, ns, smap, sshift, wav, it);
+        record(&fw, 0, nr, gmap, gshift, NULL, datamod, it);
+        memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
+    }
+    /* computeMisfit / computeResiduals, DIFFERENCE (lib/fwi.cpp:597-611, 798-806) */
+    float mis = 0.0f;
+    for (int tr = 0; tr < nr; tr++) {
+        if (gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0)
+            for (int it = 0; it < nt; it++) {
+                float r = datamod[it + (long)tr * nt] - obs[it + (long)tr * nt];
+                mis += 0.5 * r * r;
+            }
+        for (int it = 0; it < nt; it++) datares[it + (long)tr * nt] = 1 * (datamod[it + (long)tr * nt] - obs[it + (long)tr * nt]);
+    }
+    *misfit = mis;
+    float *zero = calloc(n, sizeof(float));
+    for (int it = nt - 1; it >= 0; it--) {
+        if (it < nt - 1) a2d_step(&bw, Rx, Rz, Lm, tab);
+        inject(&bw, Lm, 0, nr, gmap, gshift, datares, it);
+        a2d_corr(g, nx, nz, vp, rho, Rx, Rz, fw_state_at(Ps, zero, n, nt, it), bw.f[1], bw.f[2], vpgrad, rhograd);
+        record(&bw, 0, ns, smap, sshift, NULL, wavgrad, it);
+    }
+    free(zero);
+    st_free(&fw);
+    st_free(&bw);
+    free(Ps);
+    return 0;
+}
+
+/* RtmAcoustic2D::run_optimal, zero or extended lags (lib/rtm.cpp:191-219, 423-545). */
+int orc_rtm_a2d(const orc_grid *g, int nx, int nz, const float *Rx, const float *Rz, const float *Lm,
+                const float *tab, int ns, const int *smap, const float *sshift, const float *wav, int nr,
+                const int *gmap, const float *gshift, const float *data, int nhx, int nhz, float *image)
+{
+    const int nt = g->nt, L = g->lpml, nxp = g->nxp;
+    const long n = (long)g->nxp * g->nzp;
+    float *Ps = malloc((size_t)nt * n * sizeof(float));
+    if (!Ps) return -1;
+    orc_state fw, bw;
+    st_alloc(&fw, g, 0);
+    st_alloc(&bw, g, 0);
+    for (int it = 0; it < nt; it++) {
+        a2d_step(&fw, Rx, Rz, Lm, tab);
+        inject(&fw, Lm, 0, ns, smap, sshift, wav, it);
+        memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
+    }
+    float *zero = calloc(n, sizeof(float));
+    for (int it = nt - 1; it >= 0; it--) {
+        if (it < nt - 1) a2d_step(&bw, Rx, Rz, Lm, tab);
+        inject(&bw, Lm, 0, nr, gmap, gshift, data, it);
+        const float *ws = fw_state_at(Ps, zero, n, nt, it), *wr = bw.f[0];
+        for (int ihx = 0; ihx < nhx; ihx++) {
+            int hx = -(nhx - 1) / 2 + ihx;
+            for (int ihz = 0; ihz < nhz; ihz++) {
+                int hz = -(nhz - 1) / 2 + ihz;
+                for (int ix = 0; ix < nx; ix++) {
+                    if (ix - hx < 0 || ix - hx >= nx || ix + hx < 0 || ix + hx >= nx) continue;
+                    for (int iz = 0; iz < nz; iz++) {
+                        if (iz - hz < 0 || iz - hz >= nz || iz + hz < 0 || iz + hz >= nz) continue;
+                        image[(((long)ihz * nhx + ihx) * nz + iz) * nx + ix] +=
+                            ws[(long)(iz - hz + L) * nxp + (ix - hx + L)] * wr[(long)(iz + hz + L) * nxp + (ix + hx + L)];
+                    }
+                }
+            }
+        }
+    }
+    free(zero);
+    st_free(&fw);
+    st_free(&bw);
+    free(Ps);
+    return 0;
+}
+
+long orc_state_size(int nxp, int nzp, int elastic) { return (long)nxp * nzp * (elastic ? 5 : 3); }

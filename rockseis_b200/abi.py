@@ -1,0 +1,96 @@
+"""ctypes binding of the C ABI declared in include/rsgpu.h.
+
+The library is loaded from this package directory (built in-tree by
+``python -m rockseis_b200.build``).  There is no fallback: if librsgpu.so is
+missing or cannot be loaded, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librsgpu.so")
+
+# status codes
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_NODEVICE, ERR_REVOLVE = range(9)
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_STATE", 5: "ERR_TIMEOUT",
+                6: "ERR_UNSUPPORTED", 7: "ERR_NODEVICE", 8: "ERR_REVOLVE"}
+# physics / precision / fields (rs_field values of the reference, include/utils.h:22)
+ACOUSTIC2D, ELASTIC2D, ACOUSTIC3D, ELASTIC3D = 0, 1, 2, 3
+F32_EXACT, F32_FAST, F64 = 0, 1, 2
+PRESSURE, VX, VY, VZ, SXX, SYY, SZZ, SYZ, SXZ, SXY = range(10)
+CKPT_NATIVE, CKPT_F16, CKPT_BF16 = 0, 1, 2
+ADVANCE, TAKESHOT, RESTORE, FIRSTURN, YOUTURN, TERMINATE, ERROR = range(7)
+
+
+class RsgpuError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"rsgpu {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [("physics", C.c_int), ("precision", C.c_int), ("lpml", C.c_int), ("order", C.c_int),
+                ("fs", C.c_int), ("nt", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("dt", C.c_double), ("pml", C.c_void_p), ("tile", C.c_int), ("reserved", C.c_int * 7)]
+
+
+class Shot(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("model", C.c_void_p * 8),
+                ("nsrc", C.c_int), ("smap", C.c_void_p), ("sshift", C.c_void_p), ("wavelet", C.c_void_p),
+                ("src_field", C.c_int), ("nrec", C.c_int), ("gmap", C.c_void_p), ("gshift", C.c_void_p),
+                ("rec_field", C.c_int), ("rec_factor", C.c_void_p), ("rec_out", C.c_void_p)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m rockseis_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    P, I, D, V = C.POINTER, C.c_int, C.c_double, C.c_void_p
+    sig = {
+        "rsgpu_abi_version": (I, []),
+        "rsgpu_last_error": (C.c_char_p, []),
+        "rsgpu_device_count": (I, []),
+        "rsgpu_modelling": (I, [P(Config), I, P(Shot)]),
+        "rsgpu_plan_create": (I, [P(Config), I, P(Shot), P(V)]),
+        "rsgpu_plan_reset": (I, [V]),
+        "rsgpu_plan_run": (I, [V, I, I]),
+        "rsgpu_plan_read_traces": (I, [V, I, V]),
+        "rsgpu_plan_read_field": (I, [V, I, I, V]),
+        "rsgpu_plan_sync": (I, [V]),
+        "rsgpu_plan_stream": (V, [V]),
+        "rsgpu_plan_launch_count": (C.c_longlong, [V]),
+        "rsgpu_plan_destroy": (None, [V]),
+        "rsgpu_pml_tables": (I, [I, D, I, V]),
+        "rsgpu_stagger_model": (I, [I, I, I, I, I, I, I, V, V, V, P(V)]),
+        "rsgpu_make_map": (I, [I, I, I, P(D), P(I), P(D), P(D), P(D), P(I), V]),
+        "rsgpu_revolve_trace": (I, [I, I, I, P(I), P(I), P(I), P(I)]),
+        "rsgpu_revolve_numforw": (I, [I, I]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != OK:
+        raise RsgpuError(status, lib.rsgpu_last_error().decode())
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays crossing the C ABI must be C-contiguous"
+    return a.ctypes.data
+
+
+def real_dtype(precision: int):
+    return np.float64 if precision == F64 else np.float32

@@ -1,0 +1,627 @@
+// Host runtime of librsgpu: the C ABI of include/rsgpu.h.
+//
+// A plan owns one device arena holding, for every shot of a batch, the pitched
+// wavefields, parameters, C-PML memory variables and trace buffers, plus the
+// tile table that lets one kernel launch cover all shots.  The time loop is
+// replayed from a captured CUDA graph (velocity, stress, inject/record per step).
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "rsgpu.h"
+#include "rsgpu_host.h"
+#include "rsgpu_internal.h"
+#include "rsgpu_plan.h"
+
+namespace rsgpu {
+
+static thread_local std::string g_err;
+
+void set_error(const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return RSGPU_ERR_CUDA;                                                        \
+        }                                                                                 \
+    } while (0)
+
+static inline size_t rup(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+// Coefficient rows for each stencil half-length K (lib/der.cpp:3-53).  The values
+// are the reference's optimised staggered-grid coefficients; row K holds the K
+// pairs used where the reference reduces the order near an array end.  The K=1
+// value is a float literal in the reference, hence its float-rounded double.
+static const double kCoef[9][8] = {
+    {0, 0, 0, 0, 0, 0, 0, 0},
+    {(double)1.0029f, 0, 0, 0, 0, 0, 0, 0},
+    {1.188401e+0, -7.046382e-2, 0, 0, 0, 0, 0, 0},
+    {1.216624e+0, -9.197724e-2, 1.300041e-2, 0, 0, 0, 0, 0},
+    {1.230862e+0, -1.034123e-1, 2.011671e-2, -3.245760e-3, 0, 0, 0, 0},
+    {1.239407e+0, -1.105315e-1, 2.496329e-2, -5.804879e-3, 9.358680e-4, 0, 0, 0},
+    {1.245095e+0, -1.153979e-1, 2.848442e-2, -7.899473e-3, 1.898222e-3, -2.935304e-4, 0, 0},
+    {1.249150e+0, -1.189375e-1, 3.116091e-2, -9.623004e-3, 2.812069e-3, -6.655106e-4, 9.728191e-5, 0},
+    {1.252186e+0, -1.216289e-1, 3.326513e-2, -1.105777e-2, 3.647865e-3, -1.066144e-3, 2.437491e-4, -3.351959e-5},
+};
+
+template <typename T>
+static void build_coefs(int prec, double dx, double dz, std::vector<unsigned char> &out)
+{
+    const int cr = coef_row_stride();
+    std::vector<T> c(2 * 9 * cr, T(0));
+    for (int K = 0; K <= 8; K++)
+        for (int k = 0; k < 8; k++) {
+            T v = (T)kCoef[K][k];
+            if (prec == PREC_F32_FAST) {
+                c[K * cr + k] = (T)((double)v / (double)(T)dx);
+                c[9 * cr + K * cr + k] = (T)((double)v / (double)(T)dz);
+            } else {
+                c[K * cr + k] = v;
+                c[9 * cr + K * cr + k] = v;
+            }
+        }
+    out.resize(c.size() * sizeof(T));
+    std::memcpy(out.data(), c.data(), out.size());
+}
+
+int esize(int prec) { return prec == PREC_F64 ? 8 : 4; }
+static int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 9; }
+static int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
+static int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
+
+// ---------------------------------------------------------------- plan
+Plan::~Plan()
+{
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (arena) cudaFree(arena);
+    if (d_meta) cudaFree(d_meta);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s)
+{
+    if (!c || !s || ns < 1) { set_error("null config/shots or nshots < 1"); return RSGPU_ERR_ARG; }
+    if (c->physics < 0 || c->physics > 3) { set_error("bad physics %d", c->physics); return RSGPU_ERR_ARG; }
+    if (c->physics >= PHYS_A3D) { set_error("3D physics is not built into this plan type"); return RSGPU_ERR_UNSUPPORTED; }
+    if (c->precision < 0 || c->precision > 2) { set_error("bad precision %d", c->precision); return RSGPU_ERR_ARG; }
+    if (c->lpml < 1 || c->nt < 1 || !(c->dt > 0) || !(c->dx > 0) || !(c->dz > 0)) {
+        set_error("lpml, nt, dt, dx, dz must be positive");
+        return RSGPU_ERR_ARG;
+    }
+    const int order = std::min(std::max(c->order, 1), 8);
+    for (int i = 0; i < ns; i++) {
+        const int nxp = s[i].nx + 2 * c->lpml, nzp = s[i].nz + 2 * c->lpml;
+        if (s[i].nx < 1 || s[i].nz < 1) { set_error("shot %d: empty model window", i); return RSGPU_ERR_ARG; }
+        // the reference's Der writes out of bounds for an axis of <= order cells
+        if (nxp <= order || nzp <= order) { set_error("shot %d: padded grid smaller than stencil", i); return RSGPU_ERR_ARG; }
+        for (int k = 0; k < nparams(c->physics); k++)
+            if (!s[i].model[k]) { set_error("shot %d: model parameter %d is null", i, k); return RSGPU_ERR_ARG; }
+        if (s[i].nsrc < 0 || s[i].nrec < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
+        if (s[i].nsrc > 0 && (!s[i].smap || !s[i].sshift || !s[i].wavelet)) {
+            set_error("shot %d: source arrays missing", i);
+            return RSGPU_ERR_ARG;
+        }
+        if (s[i].nrec > 0 && (!s[i].gmap || !s[i].gshift)) { set_error("shot %d: receiver arrays missing", i); return RSGPU_ERR_ARG; }
+        const int sf = s[i].src_field, rf = s[i].rec_field;
+        if (sf != RSGPU_PRESSURE && sf != RSGPU_VX && sf != RSGPU_VZ) { set_error("shot %d: bad source field", i); return RSGPU_ERR_ARG; }
+        if (s[i].nrec > 0 && rf != RSGPU_PRESSURE && rf != RSGPU_VX && rf != RSGPU_VZ) {
+            set_error("shot %d: bad receiver field", i);
+            return RSGPU_ERR_ARG;
+        }
+    }
+    return RSGPU_OK;
+}
+
+// Build the device arena layout and upload everything.
+rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
+{
+    rsgpu_status st = check_config(c, ns, s);
+    if (st != RSGPU_OK) return st;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        set_error("no CUDA device");
+        return RSGPU_ERR_NODEVICE;
+    }
+    cfg = *c;
+    cfg.order = std::min(std::max(c->order, 1), 8);
+    prec = c->precision;
+    phys = c->physics;
+    nshots = ns;
+    const int es = esize(prec);
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+    tilecfg = (c->tile >= 0 && c->tile < TILECFG_COUNT_2D) ? c->tile : default_tile();
+    const TileShape ts = tile_shape_2d(tilecfg);
+    const int lp = cfg.lpml;
+
+    // ---- per-shot layout (byte offsets into the arena)
+    shots.resize(ns);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = rup(off + bytes, 256); return o; };
+    for (int i = 0; i < ns; i++) {
+        ShotLayout &L = shots[i];
+        L.nx = s[i].nx; L.nz = s[i].nz;
+        L.nxp = s[i].nx + 2 * lp; L.nzp = s[i].nz + 2 * lp;
+        L.pitch = (int)rup(GUARD + rup(L.nxp, 128) + GUARD, 32);
+        L.rows = GUARD + (int)rup(L.nzp, 64) + GUARD;
+        const size_t fbytes = (size_t)L.pitch * L.rows * es;
+        for (int k = 0; k < nfields(phys); k++) L.f[k] = take(fbytes);
+        for (int k = 0; k < nparams(phys); k++) L.m[k] = take(fbytes);
+        for (int k = 0; k < npsi(phys); k++) L.psix[k] = take((size_t)L.nzp * 2 * lp * es);
+        for (int k = 0; k < npsi(phys); k++) L.psiz[k] = take((size_t)2 * lp * L.nxp * es);
+        L.nrec = s[i].nrec;
+        L.nsrc = s[i].nsrc;
+        L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
+        L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
+        L.field_begin = L.f[0];
+    }
+    state_end = off;   // everything above is state or data; plan tables follow
+    // ---- injection / recording plans
+    std::vector<std::vector<int>> inj_pt(ns), inj_start(ns), inj_tr(ns), rec_pt(ns);
+    std::vector<std::vector<double>> inj_wx(ns), inj_wz(ns), rec_w(ns), rec_fac(ns);
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = shots[i];
+        // contributions in reference loop order: trace, z-corner, x-corner
+        std::map<int, std::vector<std::pair<int, std::pair<double, double>>>> per_pt;
+        std::vector<int> order_pts;
+        for (int t = 0; t < s[i].nsrc; t++) {
+            const int mx = s[i].smap[2 * t], mz = s[i].smap[2 * t + 1];
+            if (mx < 0 || mz < 0) continue;
+            double sx, sz;
+            if (prec == PREC_F64) { sx = ((const double *)s[i].sshift)[2 * t]; sz = ((const double *)s[i].sshift)[2 * t + 1]; }
+            else { sx = ((const float *)s[i].sshift)[2 * t]; sz = ((const float *)s[i].sshift)[2 * t + 1]; }
+            double xt[2], zt[2];
+            if (prec == PREC_F64) { xt[0] = 1 - sx; xt[1] = sx; zt[0] = 1 - sz; zt[1] = sz; }
+            else { xt[0] = (float)(1 - (float)sx); xt[1] = (float)sx; zt[0] = (float)(1 - (float)sz); zt[1] = (float)sz; }
+            for (int i1 = 0; i1 < 2; i1++)
+                for (int i2 = 0; i2 < 2; i2++) {
+                    const int ix = lp + mx + i2, iz = lp + mz + i1;
+                    if (ix >= L.nxp || iz >= L.nzp) { set_error("shot %d: source %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
+                    const int p = iz * L.pitch + ix;
+                    if (!per_pt.count(p)) order_pts.push_back(p);
+                    per_pt[p].push_back({t, {xt[i2], zt[i1]}});
+                }
+        }
+        inj_start[i].push_back(0);
+        for (int p : order_pts) {
+            inj_pt[i].push_back(p);
+            for (auto &cw : per_pt[p]) {
+                inj_tr[i].push_back(cw.first);
+                inj_wx[i].push_back(cw.second.first);
+                inj_wz[i].push_back(cw.second.second);
+            }
+            inj_start[i].push_back((int)inj_tr[i].size());
+        }
+        for (int t = 0; t < s[i].nrec; t++) {
+            const int mx = s[i].gmap[2 * t], mz = s[i].gmap[2 * t + 1];
+            if (mx < 0 || mz < 0) { rec_pt[i].push_back(-1); for (int k = 0; k < 4; k++) rec_w[i].push_back(0); }
+            else {
+                if (lp + mx + 1 >= L.nxp || lp + mz + 1 >= L.nzp) { set_error("shot %d: receiver %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
+                rec_pt[i].push_back((lp + mz) * L.pitch + lp + mx);
+                double sx, sz;
+                if (prec == PREC_F64) { sx = ((const double *)s[i].gshift)[2 * t]; sz = ((const double *)s[i].gshift)[2 * t + 1]; }
+                else { sx = ((const float *)s[i].gshift)[2 * t]; sz = ((const float *)s[i].gshift)[2 * t + 1]; }
+                if (prec == PREC_F64) { rec_w[i].push_back(1 - sx); rec_w[i].push_back(sx); rec_w[i].push_back(1 - sz); rec_w[i].push_back(sz); }
+                else {
+                    rec_w[i].push_back((float)(1 - (float)sx)); rec_w[i].push_back((float)sx);
+                    rec_w[i].push_back((float)(1 - (float)sz)); rec_w[i].push_back((float)sz);
+                }
+            }
+            double fac = 1.0;
+            if (s[i].rec_factor) fac = prec == PREC_F64 ? ((const double *)s[i].rec_factor)[t] : ((const float *)s[i].rec_factor)[t];
+            rec_fac[i].push_back(fac);
+        }
+    }
+    // plan tables in the same arena
+    std::vector<size_t> o_inj_pt(ns), o_inj_start(ns), o_inj_tr(ns), o_inj_wx(ns), o_inj_wz(ns), o_rec_pt(ns), o_rec_w(ns),
+        o_rec_fac(ns);
+    for (int i = 0; i < ns; i++) {
+        o_inj_pt[i] = take(std::max<size_t>(1, inj_pt[i].size()) * 4);
+        o_inj_start[i] = take(inj_start[i].size() * 4);
+        o_inj_tr[i] = take(std::max<size_t>(1, inj_tr[i].size()) * 4);
+        o_inj_wx[i] = take(std::max<size_t>(1, inj_wx[i].size()) * es);
+        o_inj_wz[i] = take(std::max<size_t>(1, inj_wz[i].size()) * es);
+        o_rec_pt[i] = take(std::max<size_t>(1, rec_pt[i].size()) * 4);
+        o_rec_w[i] = take(std::max<size_t>(1, rec_w[i].size()) * es);
+        o_rec_fac[i] = take(std::max<size_t>(1, rec_fac[i].size()) * es);
+    }
+    const size_t o_pml = take((size_t)12 * lp * es);
+    arena_bytes = off;
+    if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of %zu bytes failed", arena_bytes);
+        return RSGPU_ERR_NOMEM;
+    }
+    CU(cudaMemsetAsync(arena, 0, arena_bytes, stream));
+    char *A = (char *)arena;
+
+    // ---- uploads
+    std::vector<unsigned char> hb;
+    auto upload_vec_real = [&](size_t o, const std::vector<double> &v) -> rsgpu_status {
+        if (v.empty()) return RSGPU_OK;
+        hb.resize(v.size() * es);
+        for (size_t k = 0; k < v.size(); k++) {
+            if (es == 8) ((double *)hb.data())[k] = v[k];
+            else ((float *)hb.data())[k] = (float)v[k];
+        }
+        CU(cudaMemcpy(A + o, hb.data(), hb.size(), cudaMemcpyHostToDevice));
+        return RSGPU_OK;
+    };
+    auto upload_vec_int = [&](size_t o, const std::vector<int> &v) -> rsgpu_status {
+        if (v.empty()) return RSGPU_OK;
+        CU(cudaMemcpy(A + o, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+        return RSGPU_OK;
+    };
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = shots[i];
+        const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
+        for (int k = 0; k < nparams(phys); k++)
+            CU(cudaMemcpy2DAsync(A + L.m[k] + org, (size_t)L.pitch * es, s[i].model[k], (size_t)L.nxp * es,
+                                 (size_t)L.nxp * es, L.nzp, cudaMemcpyHostToDevice, stream));
+        if (s[i].nsrc > 0)
+            CU(cudaMemcpyAsync(A + L.wav, s[i].wavelet, (size_t)s[i].nsrc * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        if ((st = upload_vec_int(o_inj_pt[i], inj_pt[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_int(o_inj_start[i], inj_start[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_int(o_inj_tr[i], inj_tr[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_real(o_inj_wx[i], inj_wx[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_real(o_inj_wz[i], inj_wz[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_int(o_rec_pt[i], rec_pt[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_real(o_rec_w[i], rec_w[i])) != RSGPU_OK) return st;
+        if ((st = upload_vec_real(o_rec_fac[i], rec_fac[i])) != RSGPU_OK) return st;
+    }
+    {
+        std::vector<unsigned char> tab((size_t)12 * lp * es);
+        if (c->pml) std::memcpy(tab.data(), c->pml, tab.size());
+        else pml_tables_host(lp, cfg.dt, prec, tab.data());
+        CU(cudaMemcpy(A + o_pml, tab.data(), tab.size(), cudaMemcpyHostToDevice));
+    }
+    d_pml = A + o_pml;
+
+    // ---- device metadata: shot descriptors, injection plans, tiles, coefficients, step counter
+    const size_t shot_bytes = prec == PREC_F64 ? sizeof(Shot2D<double>) : sizeof(Shot2D<float>);
+    const size_t ir_bytes = prec == PREC_F64 ? sizeof(InjRec<double>) : sizeof(InjRec<float>);
+    std::vector<Tile2D> tiles;
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = shots[i];
+        for (int z0 = 0; z0 < L.nzp; z0 += ts.tz)
+            for (int x0 = 0; x0 < L.nxp; x0 += ts.tx) {
+                int fl = 0;
+                const int o = cfg.order;
+                if (x0 < o || x0 + ts.tx > L.nxp - o - 1) fl |= TILE_XEDGE;
+                if (z0 < o || z0 + ts.tz > L.nzp - o - 1) fl |= TILE_ZEDGE;
+                if (x0 < lp || x0 + ts.tx > L.nxp - lp) fl |= TILE_XPML;
+                if (z0 < lp || z0 + ts.tz > L.nzp - lp) fl |= TILE_ZPML;
+                tiles.push_back({i, x0, z0, fl});
+            }
+    }
+    ntiles = (int)tiles.size();
+    std::vector<unsigned char> coefs;
+    if (prec == PREC_F64) build_coefs<double>(prec, cfg.dx, cfg.dz, coefs);
+    else build_coefs<float>(prec, cfg.dx, cfg.dz, coefs);
+    const size_t m_shots = 0;
+    const size_t m_ir = rup(m_shots + ns * shot_bytes, 256);
+    const size_t m_tiles = rup(m_ir + ns * ir_bytes, 256);
+    const size_t m_coef = rup(m_tiles + tiles.size() * sizeof(Tile2D), 256);
+    const size_t m_it = rup(m_coef + coefs.size(), 256);
+    const size_t m_end = m_it + 256;
+    CU(cudaMalloc(&d_meta, m_end));
+    std::vector<unsigned char> meta(m_end, 0);
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = shots[i];
+        const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
+        if (prec == PREC_F64) fill_desc<double>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org,
+                                                o_inj_pt[i], o_inj_start[i], o_inj_tr[i], o_inj_wx[i], o_inj_wz[i], o_rec_pt[i],
+                                                o_rec_w[i], o_rec_fac[i], (int)inj_pt[i].size(), s[i]);
+        else fill_desc<float>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org,
+                              o_inj_pt[i], o_inj_start[i], o_inj_tr[i], o_inj_wx[i], o_inj_wz[i], o_rec_pt[i],
+                              o_rec_w[i], o_rec_fac[i], (int)inj_pt[i].size(), s[i]);
+    }
+    std::memcpy(meta.data() + m_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
+    std::memcpy(meta.data() + m_coef, coefs.data(), coefs.size());
+    CU(cudaMemcpy(d_meta, meta.data(), m_end, cudaMemcpyHostToDevice));
+    d_shots = (char *)d_meta + m_shots;
+    d_injrec = (char *)d_meta + m_ir;
+    d_tiles = (char *)d_meta + m_tiles;
+    d_coefs = (char *)d_meta + m_coef;
+    d_it = (int *)((char *)d_meta + m_it);
+    CU(cudaStreamSynchronize(stream));
+    return RSGPU_OK;
+}
+
+template <typename T>
+void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, size_t o_ip, size_t o_is,
+                     size_t o_it, size_t o_wx, size_t o_wz, size_t o_rp, size_t o_rw, size_t o_rf, int ninj,
+                     const rsgpu_shot &s)
+{
+    char *A = (char *)arena;
+    Shot2D<T> d{};
+    d.nxp = L.nxp; d.nzp = L.nzp; d.pitch = L.pitch; d.lpml = cfg.lpml; d.fs = cfg.fs;
+    for (int k = 0; k < nfields(phys); k++) d.f[k] = (T *)(A + L.f[k] + org);
+    for (int k = 0; k < nparams(phys); k++) d.m[k] = (const T *)(A + L.m[k] + org);
+    for (int k = 0; k < npsi(phys); k++) { d.psix[k] = (T *)(A + L.psix[k]); d.psiz[k] = (T *)(A + L.psiz[k]); }
+    std::memcpy(sd, &d, sizeof d);
+    InjRec<T> r{};
+    r.ninj = ninj;
+    r.kind_inj = INJ_NONE;
+    if (ninj > 0) {
+        if (phys == PHYS_A2D) r.kind_inj = s.src_field == RSGPU_PRESSURE ? INJ_A2_P : s.src_field == RSGPU_VX ? INJ_A2_VX : INJ_A2_VZ;
+        else r.kind_inj = s.src_field == RSGPU_PRESSURE ? INJ_E2_P : s.src_field == RSGPU_VX ? INJ_E2_VX : INJ_E2_VZ;
+    }
+    r.inj_pt = (const int *)(A + o_ip);
+    r.inj_start = (const int *)(A + o_is);
+    r.inj_trace = (const int *)(A + o_it);
+    r.inj_wx = (const T *)(A + o_wx);
+    r.inj_wz = (const T *)(A + o_wz);
+    r.wav = (const T *)(A + L.wav);
+    r.nrec = L.nrec;
+    r.kind_rec = REC_NONE;
+    if (L.nrec > 0) {
+        if (phys == PHYS_A2D) r.kind_rec = s.rec_field == RSGPU_PRESSURE ? REC_A2_P : s.rec_field == RSGPU_VX ? REC_A2_VX : REC_A2_VZ;
+        else r.kind_rec = s.rec_field == RSGPU_PRESSURE ? REC_E2_P : s.rec_field == RSGPU_VX ? REC_E2_VX : REC_E2_VZ;
+    }
+    r.rec_pt = (const int *)(A + o_rp);
+    r.rec_w = (const T *)(A + o_rw);
+    r.rec_factor = (const T *)(A + o_rf);
+    r.rec_out = (T *)(A + L.traces);
+    r.nt = cfg.nt;
+    std::memcpy(irp, &r, sizeof r);
+}
+
+int Plan::default_tile() const
+{
+    // Small single-shot grids need more, smaller CTAs to fill 148 SMs.
+    long pts = 0;
+    for (const auto &L : shots) pts += (long)L.nxp * L.nzp;
+    (void)pts;
+    return TILECFG_64x32;
+}
+
+rsgpu_status Plan::reset()
+{
+    for (const auto &L : shots) {
+        const size_t es = esize(prec);
+        CU(cudaMemsetAsync((char *)arena + L.field_begin, 0, L.wav - L.field_begin, stream));
+        (void)es;
+    }
+    return RSGPU_OK;
+}
+
+template <typename T>
+static void make_args(void *out, const Plan &p)
+{
+    Step2DArgs<T> a;
+    a.shots = (const Shot2D<T> *)p.d_shots;
+    a.tiles = (const Tile2D *)p.d_tiles;
+    a.ntiles = p.ntiles;
+    a.order = p.cfg.order;
+    a.dt = (T)p.cfg.dt; a.dx = (T)p.cfg.dx; a.dz = (T)p.cfg.dz;
+    a.pml = (const T *)p.d_pml;
+    a.lpml = p.cfg.lpml;
+    static_assert(sizeof a <= 128, "argument block");
+    std::memcpy(out, &a, sizeof a);
+}
+
+rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj)
+{
+    alignas(16) unsigned char args[128];
+    if (prec == PREC_F64) make_args<double>(args, *this);
+    else make_args<float>(args, *this);
+    const int grid = ntiles;
+    cudaError_t e;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 0, adj, args, d_coefs, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 1, adj, args, d_coefs, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = launch_injrec_2d(prec, d_shots, d_injrec, nshots, cfg.dt, it_base, it_dev, stream)) != cudaSuccess) goto fail;
+    launches += 3;
+    return RSGPU_OK;
+fail:
+    set_error("kernel launch failed: %s", cudaGetErrorString(e));
+    return RSGPU_ERR_CUDA;
+}
+
+rsgpu_status Plan::run(int it0, int nsteps)
+{
+    if (it0 < 0 || nsteps < 0 || it0 + nsteps > cfg.nt) { set_error("step range [%d,%d) outside [0,%d)", it0, it0 + nsteps, cfg.nt); return RSGPU_ERR_ARG; }
+    int done = 0;
+    const int G = graph_steps;
+    if (use_graph && nsteps >= G) {
+        if (!graph_exec) {
+            cudaGraph_t g;
+            CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            rsgpu_status st = RSGPU_OK;
+            for (int s = 0; s < G && st == RSGPU_OK; s++) st = launch_step(s, d_it, false);
+            if (st == RSGPU_OK) {
+                cudaError_t e = launch_advance(d_it, G, stream);
+                if (e != cudaSuccess) { set_error("launch_advance: %s", cudaGetErrorString(e)); st = RSGPU_ERR_CUDA; }
+            }
+            cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            if (st != RSGPU_OK) return st;
+            if (ce != cudaSuccess) { set_error("graph capture failed: %s", cudaGetErrorString(ce)); return RSGPU_ERR_CUDA; }
+            CU(cudaGraphInstantiate(&graph_exec, g, 0));
+            cudaGraphDestroy(g);
+            launches -= 3L * G;   // captured launches are counted at replay
+        }
+        CU(cudaMemcpyAsync(d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, stream));
+        CU(cudaStreamSynchronize(stream));
+        while (nsteps - done >= G) {
+            CU(cudaGraphLaunch(graph_exec, stream));
+            launches += 3L * G;
+            done += G;
+        }
+    }
+    for (; done < nsteps; done++) {
+        rsgpu_status st = launch_step(it0 + done, nullptr, false);
+        if (st != RSGPU_OK) return st;
+    }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::read_traces(int shot, void *host_out)
+{
+    if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
+    const ShotLayout &L = shots[shot];
+    if (L.nrec == 0) return RSGPU_OK;
+    const int es = esize(prec);
+    const size_t n = (size_t)L.nrec * cfg.nt;
+    std::vector<unsigned char> tmp(n * es);
+    CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.traces, n * es, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    if (es == 8) { double *o = (double *)host_out; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
+    else { float *o = (float *)host_out; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::read_field(int shot, int field, void *host_out)
+{
+    if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
+    int slot = -1;
+    if (phys == PHYS_A2D) slot = field == RSGPU_PRESSURE ? A2_P : field == RSGPU_VX ? A2_VX : field == RSGPU_VZ ? A2_VZ : -1;
+    else slot = field == RSGPU_VX ? E2_VX : field == RSGPU_VZ ? E2_VZ : field == 4 ? E2_SXX : field == 6 ? E2_SZZ : field == 8 ? E2_SXZ : -1;
+    if (slot < 0) { set_error("field %d not held by this physics", field); return RSGPU_ERR_ARG; }
+    const ShotLayout &L = shots[shot];
+    const int es = esize(prec);
+    const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
+    CU(cudaMemcpy2DAsync(host_out, (size_t)L.nxp * es, (char *)arena + L.f[slot] + org, (size_t)L.pitch * es,
+                         (size_t)L.nxp * es, L.nzp, cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    return RSGPU_OK;
+}
+
+}  // namespace rsgpu
+
+using namespace rsgpu;
+
+struct rsgpu_plan { std::unique_ptr<Plan> p; };
+
+extern "C" {
+
+int rsgpu_abi_version(void) { return RSGPU_ABI_VERSION; }
+const char *rsgpu_last_error(void) { return g_err.c_str(); }
+int rsgpu_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n;
+}
+
+rsgpu_status rsgpu_plan_create(const rsgpu_config *cfg, int nshots, const rsgpu_shot *shots, rsgpu_plan **plan)
+{
+    if (!plan) { set_error("plan pointer is null"); return RSGPU_ERR_ARG; }
+    *plan = nullptr;
+    auto h = std::unique_ptr<rsgpu_plan>(new rsgpu_plan);
+    h->p.reset(new Plan());
+    rsgpu_status st = h->p->create(cfg, nshots, shots);
+    if (st != RSGPU_OK) return st;
+    *plan = h.release();
+    return RSGPU_OK;
+}
+rsgpu_status rsgpu_plan_reset(rsgpu_plan *p)
+{
+    if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
+    return p->p->reset();
+}
+rsgpu_status rsgpu_plan_run(rsgpu_plan *p, int it0, int nsteps)
+{
+    if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
+    return p->p->run(it0, nsteps);
+}
+rsgpu_status rsgpu_plan_read_traces(rsgpu_plan *p, int shot, void *out)
+{
+    if (!p || !out) { set_error("null plan/output"); return RSGPU_ERR_ARG; }
+    return p->p->read_traces(shot, out);
+}
+rsgpu_status rsgpu_plan_read_field(rsgpu_plan *p, int shot, int field, void *out)
+{
+    if (!p || !out) { set_error("null plan/output"); return RSGPU_ERR_ARG; }
+    return p->p->read_field(shot, field, out);
+}
+rsgpu_status rsgpu_plan_sync(rsgpu_plan *p)
+{
+    if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
+    cudaError_t e = cudaStreamSynchronize(p->p->stream);
+    if (e != cudaSuccess) { set_error("stream sync: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    return RSGPU_OK;
+}
+void *rsgpu_plan_stream(rsgpu_plan *p) { return p ? (void *)p->p->stream : nullptr; }
+long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? p->p->launches : 0; }
+void rsgpu_plan_destroy(rsgpu_plan *p) { delete p; }
+
+rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_shot *shots)
+{
+    rsgpu_plan *p = nullptr;
+    rsgpu_status st = rsgpu_plan_create(cfg, nshots, shots, &p);
+    if (st != RSGPU_OK) return st;
+    st = rsgpu_plan_run(p, 0, cfg->nt);
+    for (int i = 0; st == RSGPU_OK && i < nshots; i++)
+        if (shots[i].nrec > 0) {
+            if (!shots[i].rec_out) { set_error("shot %d: rec_out is null", i); st = RSGPU_ERR_ARG; break; }
+            st = rsgpu_plan_read_traces(p, i, shots[i].rec_out);
+        }
+    rsgpu_plan_destroy(p);
+    return st;
+}
+
+rsgpu_status rsgpu_pml_tables(int lpml, double dt, int precision, void *out12)
+{
+    if (lpml < 1 || !out12 || precision < 0 || precision > 2) { set_error("bad arguments"); return RSGPU_ERR_ARG; }
+    pml_tables_host(lpml, dt, precision, out12);
+    return RSGPU_OK;
+}
+
+rsgpu_status rsgpu_stagger_model(int physics, int nx, int ny, int nz, int lpml, int fs, int precision,
+                                 const void *vp, const void *vs, const void *rho, void *const *out)
+{
+    if (physics < 0 || physics > 3 || nx < 2 || nz < 2 || lpml < 0 || !vp || !rho || !out) { set_error("bad arguments"); return RSGPU_ERR_ARG; }
+    if ((physics == PHYS_E2D || physics == PHYS_E3D) && !vs) { set_error("elastic physics needs vs"); return RSGPU_ERR_ARG; }
+    if ((physics == PHYS_A3D || physics == PHYS_E3D) && ny < 2) { set_error("3D physics needs ny >= 2"); return RSGPU_ERR_ARG; }
+    int r = stagger_host(physics, nx, ny, nz, lpml, fs, precision, vp, vs, rho, out);
+    if (r == -2) { set_error("physics not supported"); return RSGPU_ERR_UNSUPPORTED; }
+    if (r != 0) { set_error("staggerModels: Zero density found."); return RSGPU_ERR_ARG; }
+    return RSGPU_OK;
+}
+
+rsgpu_status rsgpu_make_map(int dim, int precision, int ntr, const double *coords, const int *n, const double *o,
+                            const double *d, const double *gshift, int *map, void *shift)
+{
+    if ((dim != 2 && dim != 3) || ntr < 0 || (ntr > 0 && (!coords || !map || !shift)) || !n || !o || !d) {
+        set_error("bad arguments");
+        return RSGPU_ERR_ARG;
+    }
+    make_map_host(dim, precision, ntr, coords, n, o, d, gshift, map, shift);
+    return RSGPU_OK;
+}
+
+rsgpu_status rsgpu_revolve_trace(int nt, int ncheck, int max, int *actions, int *capos, int *checks, int *n)
+{
+    if (nt < 1 || !actions || !capos || !checks || !n) { set_error("bad arguments"); return RSGPU_ERR_ARG; }
+    RevolveSchedule r(nt, ncheck);
+    int k = 0, a;
+    do {
+        a = r.next();
+        if (k >= max) { set_error("action trace longer than %d", max); return RSGPU_ERR_ARG; }
+        actions[k] = a; capos[k] = r.capo(); checks[k] = r.check();
+        k++;
+    } while (a != RSGPU_TERMINATE && a != RSGPU_ERROR);
+    *n = k;
+    return RSGPU_OK;
+}
+
+int rsgpu_revolve_numforw(int nt, int ncheck) { return RevolveSchedule::numforw(nt, ncheck); }
+
+}  // extern "C"

@@ -1,0 +1,40 @@
+// Host-runtime internals of librsgpu (not part of the C ABI).
+#pragma once
+#include <cstdarg>
+#include <cstddef>
+#include <string>
+#include "rsgpu_kernels.h"
+
+namespace rsgpu {
+
+// thread-local last-error text behind rsgpu_last_error()
+void set_error(const char *fmt, ...);
+
+void pml_tables_host(int lpml, double dt, int prec, void *out);
+int stagger_host(int physics, int nx, int ny, int nz, int l, int fs, int prec, const void *vp, const void *vs,
+                 const void *rho, void *const *out);
+template <typename T>
+int stagger_e3d_host(int nx, int ny, int nz, int l, int fs, const T *vp, const T *vs, const T *rho, T *const *out);
+void make_map_host(int dim, int prec, int ntr, const double *coords, const int *n, const double *o, const double *d,
+                   const double *gshift, int *map, void *shift);
+
+// Griewank binomial checkpoint schedule (reference: lib/revolve.cpp:31-305).
+class RevolveSchedule {
+public:
+    RevolveSchedule(int steps, int snaps);
+    int next();             // returns an RSGPU_ADVANCE.. action code
+    int capo() const { return capo_; }
+    int check() const { return check_; }
+    int snaps() const { return snaps_; }
+    int info() const { return info_; }
+    static int numforw(int steps, int snaps);
+    static int adjust(int steps);
+
+private:
+    static int maxrange(int ss, int tt);
+    int check_, capo_, fine_, steps_, snaps_, info_;
+    int turn_, reps_, range_, oldsnaps_, oldfine_;
+    int ch_[512];
+};
+
+}  // namespace rsgpu

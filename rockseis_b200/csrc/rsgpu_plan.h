@@ -1,0 +1,55 @@
+// Plan object behind the opaque rsgpu_plan handle (host runtime, not ABI).
+#pragma once
+#include <cstddef>
+#include <vector>
+#include <cuda_runtime.h>
+#include "rsgpu.h"
+#include "rsgpu_kernels.h"
+
+namespace rsgpu {
+
+int esize(int prec);
+
+// Byte offsets of one shot's arrays inside the plan arena.
+struct ShotLayout {
+    int nx = 0, nz = 0, nxp = 0, nzp = 0, pitch = 0, rows = 0;
+    int nrec = 0, nsrc = 0;
+    size_t f[9] = {}, m[8] = {}, psix[4] = {}, psiz[4] = {};
+    size_t traces = 0, wav = 0;
+    size_t field_begin = 0;   // first byte of the zero-initialised state block
+};
+
+class Plan {
+public:
+    ~Plan();
+    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    rsgpu_status reset();
+    rsgpu_status run(int it0, int nsteps);
+    rsgpu_status read_traces(int shot, void *host_out);
+    rsgpu_status read_field(int shot, int field, void *host_out);
+    rsgpu_status launch_step(int it_base, const int *it_dev, bool adj);
+
+    rsgpu_config cfg{};
+    int prec = 0, phys = 0, nshots = 0, tilecfg = 0, ntiles = 0;
+    std::vector<ShotLayout> shots;
+    void *arena = nullptr;
+    size_t arena_bytes = 0, state_end = 0;
+    void *d_meta = nullptr;
+    void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
+    int *d_it = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool use_graph = true;
+    int graph_steps = 32;
+    long long launches = 0;
+
+private:
+    rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    int default_tile() const;
+    template <typename T>
+    void fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, size_t o_ip, size_t o_is,
+                   size_t o_it, size_t o_wx, size_t o_wz, size_t o_rp, size_t o_rw, size_t o_rf, int ninj,
+                   const rsgpu_shot &s);
+};
+
+}  // namespace rsgpu

@@ -1,0 +1,352 @@
+"""Python mirror of the RockSeis driver classes on the hot path.
+
+Same class and method names, argument meanings and return codes as the
+reference's C++ API (include/model.h, data.h, modelling.h, fwi.h, rtm.h of the
+RockSeis tree); every compute call goes through the C ABI of librsgpu
+(include/rsgpu.h) to the sm_100a kernels.  Differences in error behaviour: the
+reference's rs_error prints and calls exit(1); here the same conditions raise
+rockseis_b200.abi.RsgpuError carrying the library's status code and message.
+
+Precision: ``precision`` selects the propagator arithmetic (abi.F32_EXACT,
+F32_FAST, F64); arrays are float32 for the F32 modes and float64 for F64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import abi
+from .abi import check, ptr
+
+MOD_OK, MOD_ERR = 1, 0
+FWI_OK, FWI_ERR = 1, 0
+RTM_OK, RTM_ERR = 1, 0
+SMAP, GMAP = 0, 1
+
+
+def _f(dtype, x):
+    """Round a Python float to the model's element type, as a T member would hold it."""
+    return float(np.asarray(x, dtype=dtype))
+
+
+class _Model:
+    dim = 2
+    physics = abi.ACOUSTIC2D
+    names: tuple[str, ...] = ()
+
+    def __init__(self, nx, ny, nz, lpml, dx, dy, dz, ox, oy, oz, fs, precision=abi.F32_EXACT):
+        self.precision = precision
+        self.dtype = abi.real_dtype(precision)
+        self.nx, self.ny, self.nz, self.lpml = int(nx), int(ny), int(nz), int(lpml)
+        t = self.dtype
+        self.dx, self.dy, self.dz = _f(t, dx), _f(t, dy), _f(t, dz)
+        self.ox, self.oy, self.oz = _f(t, ox), _f(t, oy), _f(t, oz)
+        self.fs = bool(fs)
+        self.realized = False
+        self._padded: dict[str, np.ndarray] = {}
+
+    # getters mirroring Model<T>
+    def getNx(self): return self.nx
+    def getNy(self): return self.ny
+    def getNz(self): return self.nz
+    def getLpml(self): return self.lpml
+    def getDx(self): return self.dx
+    def getDz(self): return self.dz
+    def getFs(self): return self.fs
+    def getNx_pml(self): return self.nx + 2 * self.lpml
+    def getNz_pml(self): return self.nz + 2 * self.lpml
+    def getNy_pml(self): return self.ny + 2 * self.lpml if self.dim == 3 else 1
+
+    def _shape(self):
+        return (self.nz, self.ny, self.nx) if self.dim == 3 else (self.nz, self.nx)
+
+    def _pshape(self):
+        if self.dim == 3:
+            return (self.getNz_pml(), self.getNy_pml(), self.getNx_pml())
+        return (self.getNz_pml(), self.getNx_pml())
+
+    def geom(self):
+        """(n, o, d) of the regular grid along the map axes, as Model::getGeom holds them."""
+        if self.dim == 3:
+            return (np.array([self.nx, self.ny, self.nz], np.int32), np.array([self.ox, self.oy, self.oz]),
+                    np.array([self.dx, self.dy, self.dz]))
+        return (np.array([self.nx, self.nz], np.int32), np.array([self.ox, self.oz]), np.array([self.dx, self.dz]))
+
+    def staggerModels(self):
+        """Pad, form moduli, stagger and invert density (Model*::staggerModels)."""
+        if not self.realized:
+            raise abi.RsgpuError(abi.ERR_STATE, f"{type(self).__name__}::staggerModels: Model is not allocated.")
+        outs = [np.zeros(self._pshape(), self.dtype) for _ in self.names]
+        arr = (C.c_void_p * 8)(*([o.ctypes.data for o in outs] + [None] * (8 - len(outs))))
+        vs = getattr(self, "Vs", None)
+        check(abi.lib.rsgpu_stagger_model(self.physics, self.nx, self.ny, self.nz, self.lpml, int(self.fs),
+                                          self.precision, ptr(self.Vp), ptr(vs), ptr(self.R), arr))
+        self._padded = dict(zip(self.names, outs))
+
+    def padded(self):
+        if not self._padded:
+            self.staggerModels()
+        return [self._padded[n] for n in self.names]
+
+    def getVpmax(self):
+        return float(self.Vp.max())
+
+
+class ModelAcoustic2D(_Model):
+    physics = abi.ACOUSTIC2D
+    names = ("Rx", "Rz", "L")
+
+    def __init__(self, nx, nz, lpml, dx, dz, ox, oz, fs, precision=abi.F32_EXACT):
+        super().__init__(nx, 1, nz, lpml, dx, 1.0, dz, ox, 0.0, oz, fs, precision)
+
+    def createModel(self):
+        self.Vp = np.zeros(self._shape(), self.dtype)
+        self.R = np.zeros(self._shape(), self.dtype)
+        self.realized = True
+
+    def getVp(self): return self.Vp
+    def getR(self): return self.R
+    def getRx(self): return self.padded()[0]
+    def getRz(self): return self.padded()[1]
+    def getL(self): return self.padded()[2]
+
+
+class ModelElastic2D(_Model):
+    physics = abi.ELASTIC2D
+    names = ("Rx", "Rz", "L", "L2M", "M")
+
+    def __init__(self, nx, nz, lpml, dx, dz, ox, oz, fs, precision=abi.F32_EXACT):
+        super().__init__(nx, 1, nz, lpml, dx, 1.0, dz, ox, 1.0, oz, fs, precision)
+
+    def createModel(self):
+        self.Vp = np.zeros(self._shape(), self.dtype)
+        self.Vs = np.zeros(self._shape(), self.dtype)
+        self.R = np.zeros(self._shape(), self.dtype)
+        self.realized = True
+
+    def getVp(self): return self.Vp
+    def getVs(self): return self.Vs
+    def getR(self): return self.R
+    def getRx(self): return self.padded()[0]
+    def getRz(self): return self.padded()[1]
+    def getL(self): return self.padded()[2]
+    def getL2M(self): return self.padded()[3]
+    def getM(self): return self.padded()[4]
+
+
+class Data2D:
+    """Trace container (Data2D<T>): data[itr, it] == reference data[it + itr*nt]."""
+    dim = 2
+
+    def __init__(self, ntrace, nt, dt, ot, precision=abi.F32_EXACT):
+        self.precision = precision
+        self.dtype = abi.real_dtype(precision)
+        self.ntrace, self.nt = int(ntrace), int(nt)
+        self.dt, self.ot = _f(self.dtype, dt), _f(self.dtype, ot)
+        self.data = np.zeros((self.ntrace, self.nt), self.dtype)
+        self.scoords = np.zeros((self.ntrace, self.dim), self.dtype)   # (x, z)
+        self.gcoords = np.zeros((self.ntrace, self.dim), self.dtype)
+        self.smap = np.full((self.ntrace, self.dim), -1, np.int32)
+        self.gmap = np.full((self.ntrace, self.dim), -1, np.int32)
+        self.sshift = np.zeros((self.ntrace, self.dim), self.dtype)
+        self.gshift = np.zeros((self.ntrace, self.dim), self.dtype)
+        self.field = abi.PRESSURE
+        self.reciprocity = False
+
+    def getNtrace(self): return self.ntrace
+    def getNt(self): return self.nt
+    def getDt(self): return self.dt
+    def getOt(self): return self.ot
+    def getData(self): return self.data
+    def getField(self): return self.field
+    def setField(self, f): self.field = int(f)
+    def setReciprocity(self, v): self.reciprocity = bool(v)
+
+    def makeMap(self, model: _Model, which=None):
+        """Geometry2D::makeMap: coordinates -> (cell, fractional shift); -1 if off the grid."""
+        whichs = (SMAP, GMAP) if which is None else (which,)
+        n, o, d = model.geom()
+        # staggered trace positions: -0.5 cell along the traced velocity component
+        gs = np.zeros(self.dim)
+        comp = {abi.VX: 0, abi.VY: 1, abi.VZ: self.dim - 1}.get(self.field)
+        if comp is not None and not (self.dim == 2 and self.field == abi.VY):
+            gs[comp] = -0.5
+        for w in whichs:
+            coords = np.ascontiguousarray((self.scoords if w == SMAP else self.gcoords).astype(np.float64))
+            mp = np.full((self.ntrace, self.dim), -1, np.int32)
+            sh = np.zeros((self.ntrace, self.dim), self.dtype)
+            check(abi.lib.rsgpu_make_map(self.dim, self.precision, self.ntrace,
+                                         coords.ctypes.data_as(C.POINTER(C.c_double)),
+                                         n.ctypes.data_as(C.POINTER(C.c_int)),
+                                         o.astype(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                         d.astype(np.float64).ctypes.data_as(C.POINTER(C.c_double)),
+                                         gs.ctypes.data_as(C.POINTER(C.c_double)),
+                                         mp.ctypes.data_as(C.POINTER(C.c_int)), ptr(sh)))
+            if w == SMAP:
+                self.smap, self.sshift = mp, sh
+            else:
+                self.gmap, self.gshift = mp, sh
+
+
+def check_stability(model: _Model, dt: float, cls: str) -> None:
+    """Modelling*::checkStability (lib/modelling.cpp:181-194)."""
+    t = model.dtype
+    vpmax = t(model.getVpmax())
+    dx, dz = t(model.dx), t(model.dz)
+    if model.dim == 3:
+        dy = t(model.dy)
+        dt_stab = t(2.0 / (3.1415 * math.sqrt((1.0 / float(dx * dx)) + (1 / float(dy * dy)) + (1 / float(dz * dz)))
+                           * float(vpmax)))
+    else:
+        dt_stab = t(2.0 / (3.1415 * math.sqrt((1.0 / float(dx * dx)) + (1 / float(dz * dz))) * float(vpmax)))
+    if not t(dt) < dt_stab:
+        raise abi.RsgpuError(abi.ERR_ARG, f"{cls}::run: Wavelet sampling interval (dt) does not match the "
+                             f"stability criteria (limit {float(dt_stab)}).")
+
+
+def make_config(model: _Model, order: int, nt: int, dt: float, precision: int, tile: int = -1) -> abi.Config:
+    cfg = abi.Config()
+    cfg.physics = model.physics
+    cfg.precision = precision
+    cfg.lpml = model.lpml
+    cfg.order = int(order)
+    cfg.fs = int(model.fs)
+    cfg.nt = int(nt)
+    cfg.dx, cfg.dy, cfg.dz = float(model.dx), float(model.dy), float(model.dz)
+    cfg.dt = float(dt)
+    cfg.pml = None
+    cfg.tile = int(tile)
+    return cfg
+
+
+def make_shot(model: _Model, source: Data2D, rec: Data2D | None, keep: list) -> abi.Shot:
+    """Fill one rsgpu_shot from mirror objects; `keep` holds arrays alive for the call."""
+    s = abi.Shot()
+    s.nx, s.ny, s.nz = model.nx, model.ny, model.nz
+    pads = model.padded()
+    keep.extend(pads)
+    for k, a in enumerate(pads):
+        s.model[k] = a.ctypes.data
+    smap, sshift = np.ascontiguousarray(source.smap), np.ascontiguousarray(source.sshift)
+    wav = np.ascontiguousarray(source.data)
+    keep.extend([smap, sshift, wav])
+    s.nsrc, s.smap, s.sshift, s.wavelet, s.src_field = source.ntrace, ptr(smap), ptr(sshift), ptr(wav), source.field
+    if rec is not None:
+        gmap, gshift = np.ascontiguousarray(rec.gmap), np.ascontiguousarray(rec.gshift)
+        keep.extend([gmap, gshift])
+        s.nrec, s.gmap, s.gshift, s.rec_field = rec.ntrace, ptr(gmap), ptr(gshift), rec.field
+        s.rec_out = ptr(rec.data)
+        if rec.reciprocity and model.physics == abi.ELASTIC2D:
+            fac = reciprocity_factor(model, rec)
+            keep.append(fac)
+            s.rec_factor = ptr(fac)
+    return s
+
+
+def reciprocity_factor(model: _Model, rec: Data2D) -> np.ndarray:
+    """R*Vp*Vp - R*Vs*Vs at each receiver cell, in T (lib/waves.cpp:2218-2220)."""
+    t = model.dtype
+    fac = np.ones(rec.ntrace, t)
+    for i, (mx, mz) in enumerate(rec.gmap):
+        if mx >= 0 and mz >= 0:
+            r, vp, vs = model.R[mz, mx], model.Vp[mz, mx], model.Vs[mz, mx]
+            fac[i] = t(t(r * vp) * vp) - t(t(r * vs) * vs)
+    return fac
+
+
+class _Modelling:
+    physics_name = "ModellingAcoustic2D"
+
+    def __init__(self, model=None, source=None, order=4, snapinc=1, precision=None):
+        self.model, self.source = model, source
+        self.order = int(order) if 1 < int(order) < 9 else 4   # Modelling<T>::Modelling (lib/modelling.cpp:17-22)
+        self.snapinc = snapinc if snapinc > 0 else 1
+        self.precision = precision if precision is not None else (model.precision if model else abi.F32_EXACT)
+        self.recP = self.recVx = self.recVz = None
+        self.tile = -1
+
+    def setModel(self, m): self.model = m
+    def setSource(self, s): self.source = s
+    def setRecP(self, d): self.recP = d
+    def setRecVx(self, d): self.recVx = d
+    def setRecVz(self, d): self.recVz = d
+    def getOrder(self): return self.order
+
+    def checkStability(self):
+        check_stability(self.model, self.source.dt, self.physics_name)
+        return True
+
+    def run(self):
+        self.checkStability()
+        recs = [r for r in (self.recP, self.recVx, self.recVz) if r is not None]
+        cfg = make_config(self.model, self.order, self.source.nt, self.source.dt, self.precision, self.tile)
+        keep: list = []
+        # one shot per recorded field; the wavefield computation is shared by
+        # the reference, here each receiver set is a separate batch entry
+        rec_list = recs or [None]
+        shots = (abi.Shot * len(rec_list))(*[make_shot(self.model, self.source, r, keep) for r in rec_list])
+        check(abi.lib.rsgpu_modelling(C.byref(cfg), len(rec_list), shots))
+        return MOD_OK
+
+
+class ModellingAcoustic2D(_Modelling):
+    physics_name = "ModellingAcoustic2D"
+
+
+class ModellingElastic2D(_Modelling):
+    physics_name = "ModellingElastic2D"
+
+
+def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
+    """Many shots, each with its own model window, advanced together in one plan
+    (the batched form of Modelling*::run).  Traces accumulate into receivers[i].data."""
+    cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
+    keep: list = []
+    shots = (abi.Shot * len(models))(*[make_shot(m, s, r, keep) for m, s, r in zip(models, sources, receivers)])
+    check(abi.lib.rsgpu_modelling(C.byref(cfg), len(models), shots))
+    return MOD_OK
+
+
+class Plan:
+    """Device-resident batch (rsgpu_plan): upload once, run steps, read traces."""
+
+    def __init__(self, models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
+        self.cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
+        self._keep: list = []
+        self.n = len(models)
+        self.receivers = receivers
+        self.shots = (abi.Shot * self.n)(*[make_shot(m, s, r, self._keep) for m, s, r in zip(models, sources, receivers)])
+        self.h = C.c_void_p()
+        check(abi.lib.rsgpu_plan_create(C.byref(self.cfg), self.n, self.shots, C.byref(self.h)))
+
+    def reset(self): check(abi.lib.rsgpu_plan_reset(self.h))
+    def run(self, it0=0, nsteps=None):
+        check(abi.lib.rsgpu_plan_run(self.h, it0, self.cfg.nt if nsteps is None else nsteps))
+    def sync(self): check(abi.lib.rsgpu_plan_sync(self.h))
+    def stream(self) -> int: return abi.lib.rsgpu_plan_stream(self.h) or 0
+    def launch_count(self) -> int: return abi.lib.rsgpu_plan_launch_count(self.h)
+
+    def read_traces(self, i, out=None):
+        r = self.receivers[i]
+        if out is None:
+            out = np.zeros((r.ntrace, r.nt), abi.real_dtype(self.cfg.precision))
+        check(abi.lib.rsgpu_plan_read_traces(self.h, i, ptr(out)))
+        return out
+
+    def read_field(self, i, field, shape):
+        out = np.zeros(shape, abi.real_dtype(self.cfg.precision))
+        check(abi.lib.rsgpu_plan_read_field(self.h, i, field, ptr(out)))
+        return out
+
+    def close(self):
+        if self.h:
+            abi.lib.rsgpu_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,67 @@
+"""Seeded synthetic inputs shared by the tests and the benchmark.
+
+There is no public dataset on this path: the reference is driven by models and
+wavelets its users supply.  These generators produce the workloads' shapes
+and value distributions (layered velocities with smooth perturbations, Gardner
+density, Ricker wavelets, surface receiver lines) from numpy seeds.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def ricker(nt: int, dt: float, f0: float, dtype=np.float32) -> np.ndarray:
+    """(1 - 2a) exp(-a), a = (pi f0 (t - t0))^2, t0 = 1.2 / f0."""
+    t = np.arange(nt) * dt - 1.2 / f0
+    a = (np.pi * f0 * t) ** 2
+    return ((1 - 2 * a) * np.exp(-a)).astype(dtype)
+
+
+def gardner(vp: np.ndarray) -> np.ndarray:
+    return (310.0 * vp.astype(np.float64) ** 0.25).astype(vp.dtype)
+
+
+def _smooth_noise(rng, nz, nx, sigma_cells):
+    f = rng.standard_normal((nz, nx))
+    # separable Gaussian smoothing in the Fourier domain
+    kz = np.fft.fftfreq(nz)[:, None]
+    kx = np.fft.fftfreq(nx)[None, :]
+    g = np.exp(-2 * (np.pi * sigma_cells) ** 2 * (kz ** 2 + kx ** 2))
+    s = np.real(np.fft.ifft2(np.fft.fft2(f) * g))
+    return s / (np.abs(s).max() + 1e-30)
+
+
+def layered_vp(nx: int, nz: int, dx: float, vmin=1500.0, vmax=4500.0, nlayers=6, pert=0.05, sigma_m=150.0,
+               seed=1, vclip=None, dtype=np.float32) -> np.ndarray:
+    """Flat layers vmin..vmax plus a smooth seeded Gaussian perturbation (fraction `pert`)."""
+    rng = np.random.default_rng(seed)
+    edges = np.linspace(0, nz, nlayers + 1).astype(int)
+    vp = np.empty((nz, nx))
+    for k in range(nlayers):
+        vp[edges[k]:edges[k + 1], :] = vmin + (vmax - vmin) * k / max(1, nlayers - 1)
+    vp *= 1.0 + pert * _smooth_noise(rng, nz, nx, sigma_m / dx)
+    if vclip is not None:
+        vp = np.minimum(vp, vclip)
+    return vp.astype(dtype)
+
+
+def elastic_model(nx: int, nz: int, dx: float, seed=2, vclip=4450.0, nlenses=6, dtype=np.float32):
+    """Layered vp (<= vclip), vp/vs in [1.7, 2.0], Gardner density, random elliptical lenses."""
+    rng = np.random.default_rng(seed)
+    vp = layered_vp(nx, nz, dx, 1500.0, 4400.0, 6, 0.03, 100.0, seed, None, np.float64)
+    zz, xx = np.mgrid[0:nz, 0:nx]
+    for _ in range(nlenses):
+        cx, cz = rng.uniform(0.1, 0.9) * nx, rng.uniform(0.2, 0.9) * nz
+        ax, az = rng.uniform(0.03, 0.12) * nx, rng.uniform(0.02, 0.08) * nz
+        m = ((xx - cx) / ax) ** 2 + ((zz - cz) / az) ** 2 < 1
+        vp[m] *= rng.uniform(0.9, 1.1)
+    vp = np.minimum(vp, vclip)
+    ratio = 1.7 + 0.3 * (0.5 + 0.5 * _smooth_noise(rng, nz, nx, 20))
+    vs = vp / ratio
+    rho = 310.0 * vp ** 0.25
+    return vp.astype(dtype), vs.astype(dtype), rho.astype(dtype)
+
+
+def surface_line(n: int, x0: float, dxr: float, z: float) -> np.ndarray:
+    """n positions (x, z) starting at x0 with spacing dxr at depth z."""
+    return np.stack([x0 + dxr * np.arange(n), np.full(n, z)], axis=1)
