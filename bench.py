@@ -1,0 +1,391 @@
+"""Benchmark of the finite-difference hot path (one JSON line on stdout).
+
+Workload: 2D elastic forward modelling, 16 shots at uneven spacing batched in
+one plan: 801 x 401 grid, dx = dz = 5 m, 30-cell C-PML (padded 861 x 461),
+order 8 (16-tap staggered stencil), nt = 4000, dt = 0.5 ms, explosive source at
+z = 10 m, 400 Vx receivers every 10 m at the surface.  Seeded synthetic model
+(layered vp <= 4450 m/s, vp/vs 1.7-2.0, Gardner density, random lenses).
+
+A "step" is one complete forward modelling of the batch (all nt time steps of
+all shots).  Metric: Gpts/s = padded grid points x time steps / second, summed
+over shots (and over ranks with --gpus N: every rank models its own 16 shots,
+weak scaling, no data-path collective).
+
+  value   device-resident plan (models uploaded once), CUDA-event timed.
+  e2e     rsgpu_modelling through the C ABI from pinned host buffers: upload of
+          models, maps and wavelets, the run, and the read-back of the traces.
+  roofline  dominant half-step kernel: algorithmic bytes per launch / its
+          CUDA-event duration inside the timed region (events recorded in the
+          captured graph), against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own ModellingElastic2D::run (oracle/_ref,
+          compiled from the reference sources) on all host cores, one shot per
+          process, first 100 time steps of the same shot (bounded sample).
+
+--impl reference times that CPU reference alone (same metric and config).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+NX, NZ, DX, LPML, ORDER, DT, NT, NSHOTS, NREC = 801, 401, 5.0, 30, 8, 5e-4, 4000, 16, 400
+CPU_SAMPLE_STEPS = 100
+
+
+def workload_inputs(seed_model=2, seed_shots=3):
+    from rockseis_b200 import synth
+    vp, vs, rho = synth.elastic_model(NX, NZ, DX, seed=seed_model)
+    sx = np.sort(np.random.default_rng(seed_shots).uniform(200.0, (NX - 1) * DX - 200.0, NSHOTS))
+    wav = synth.ricker(NT, DT, 15.0)
+    gc = synth.surface_line(NREC, 0.0, 10.0, 0.0)
+    return vp, vs, rho, sx, wav, gc
+
+
+def config_dict(ngpus, precision_name):
+    return {"workload": "elastic2d_forward_16shots_801x401_nt4000", "nx": NX, "nz": NZ, "dx": DX, "lpml": LPML,
+            "order": ORDER, "nt": NT, "dt": DT, "shots_per_gpu": NSHOTS, "receivers": NREC,
+            "padded_points_per_shot": (NX + 2 * LPML) * (NZ + 2 * LPML), "arithmetic": precision_name,
+            "l2": "working set 254 MB per GPU > 126 MB L2 (no flush needed)", "parallelism": f"shots x{ngpus}"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.index, self.proc, self.lines = index, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU reference
+def _ref_sample(args):
+    """One process: the reference's ModellingElastic2D::run on one shot, bounded nt."""
+    shot, nsteps = args
+    sys.path.insert(0, ROOT)
+    import ctypes as C
+    from oracle import api
+    vp, vs, rho, sx, wav, gc = workload_inputs()
+    pb = api.Problem2D(NX, NZ, DX, DX, LPML, ORDER, 0, DT, nsteps, vp, rho, vs)
+    t0 = time.perf_counter()
+    api.ref_modelling_e2d(pb, np.array([[sx[shot], 10.0]]), wav[None, :nsteps], 0, gc, 1)
+    dt = time.perf_counter() - t0
+    return dt
+
+
+def cpu_reference(nsteps=CPU_SAMPLE_STEPS, procs=None):
+    """Aggregate Gpts/s of the reference CPU path on all host cores (P concurrent processes)."""
+    import multiprocessing as mp
+    from oracle import api
+    if not api.ref_available():
+        return None
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_ref_sample, [(i % NSHOTS, nsteps) for i in range(procs)])
+    wall = time.perf_counter() - t0
+    pts = (NX + 2 * LPML) * (NZ + 2 * LPML) * nsteps * procs
+    return {"value": pts / max(times) / 1e9, "unit": "Gpts/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x 1 shot x first {nsteps} of {NT} steps, full 861x461 padded grid",
+            "max_process_s": round(max(times), 3), "wall_s": round(wall, 3)}
+
+
+# ---------------------------------------------------------------- GPU arm
+def build_batch(precision, vp, vs, rho, sx, wav, gc, nt=NT, pinned=False):
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import Data2D, ModelElastic2D
+    models, srcs, recs = [], [], []
+    for i in range(NSHOTS):
+        m = ModelElastic2D(NX, NZ, LPML, DX, DX, 0.0, 0.0, 0, precision)
+        m.createModel()
+        m.Vp[:], m.Vs[:], m.R[:] = vp, vs, rho
+        s = Data2D(1, nt, DT, 0.0, precision)
+        s.scoords[:] = [[sx[i], 10.0]]
+        s.data[:] = wav[None, :nt]
+        s.setField(abi.PRESSURE)
+        s.makeMap(m, 0)
+        r = Data2D(NREC, nt, DT, 0.0, precision)
+        r.gcoords[:] = gc
+        r.setField(abi.VX)
+        r.makeMap(m, 1)
+        models.append(m)
+        srcs.append(s)
+        recs.append(r)
+    if pinned:
+        import torch
+        for m in models:
+            for k, a in m._padded.items() if m._padded else []:
+                pass
+            pads = m.padded()
+            pinned_pads = []
+            for a in pads:
+                t = torch.empty(a.shape, dtype=torch.float32).pin_memory()
+                t.numpy()[:] = a
+                pinned_pads.append(t)
+            m._pinned = pinned_pads
+            m._padded = dict(zip(m.names, [t.numpy() for t in pinned_pads]))
+        for r in recs:
+            t = torch.zeros(r.data.shape, dtype=torch.float32).pin_memory()
+            r._pinned = t
+            r.data = t.numpy()
+        for s in srcs:
+            t = torch.empty(s.data.shape, dtype=torch.float32).pin_memory()
+            t.numpy()[:] = s.data
+            s._pinned = t
+            s.data = t.numpy()
+    return models, srcs, recs
+
+
+def algorithmic_bytes(models):
+    """Algorithmic bytes of one velocity / stress launch over the batch (fp32).
+
+    velocity: read Sxx,Szz,Sxz,Vx,Vz,Rx,Rz; write Vx,Vz  -> 36 B per padded point
+    stress:   read Vx,Vz,Sxx,Szz,Sxz,L,L2M,M; write Sxx,Szz,Sxz -> 44 B per point
+    plus the C-PML memory variables: 2 per strip point per launch, read+write (16 B).
+    """
+    pts = strip = 0
+    for m in models:
+        nxp, nzp, L = m.getNx_pml(), m.getNz_pml(), m.lpml
+        pts += nxp * nzp
+        strip += 2 * L * nzp + 2 * L * nxp
+    return 36 * pts + 16 * strip, 44 * pts + 16 * strip, pts
+
+
+def read_traffic(kernel):
+    """ncu DRAM bytes per launch recorded in profiles/ for the workload, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_elastic2d_16shots.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_gpu(args, rank, world, device):
+    import ctypes as C
+    import torch
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import Plan, make_config, make_shot
+    precision = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
+    vp, vs, rho, sx, wav, gc = workload_inputs()
+    models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc)
+    torch.cuda.set_device(device)
+    plan = Plan(models, srcs, recs, ORDER, precision, args.tile)
+    plan.enable_timing()
+    st = torch.cuda.ExternalStream(plan.stream())
+    pts_per_step = sum(m.getNx_pml() * m.getNz_pml() for m in models) * NT
+
+    def one_step():
+        plan.reset()
+        plan.run(0, NT)
+
+    for _ in range(args.warmup):
+        one_step()
+    plan.sync()
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    l0 = plan.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            one_step()
+        e1.record(st)
+        e1.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    plan.sync()
+    launches = plan.launch_count() - l0
+    ms_vel, ms_str = plan.kernel_times()
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    ms_max = dist_max(ms_total, world)
+    ms_step = ms_max / args.steps
+    value = pts_per_step * world / (ms_step / 1e3) / 1e9
+
+    # roofline of the dominant half-step kernel
+    b_vel, b_str, _ = algorithmic_bytes(models)
+    peak, peak_kind = measured_peak()
+    dom, ms_dom, b_dom = ("e2d_stress", ms_str, b_str) if ms_str >= ms_vel else ("e2d_velocity", ms_vel, b_vel)
+    achieved = b_dom / (ms_dom / 1e3) / 1e9
+    traffic = read_traffic(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": b_dom, "ms_per_launch": round(ms_dom, 5),
+                "ms_velocity": round(ms_vel, 5), "ms_stress": round(ms_str, 5),
+                "step_bytes_fraction": round(((b_vel + b_str) * NT / (ms_step / 1e3) / 1e9) / peak, 4)}
+    plan.close()
+
+    # end to end through the C ABI from pinned host buffers
+    models_p, srcs_p, recs_p = build_batch(precision, vp, vs, rho, sx, wav, gc, pinned=True)
+    cfg = make_config(models_p[0], ORDER, NT, DT, precision, args.tile)
+    keep: list = []
+    shots = (abi.Shot * NSHOTS)(*[make_shot(m, s, r, keep) for m, s, r in zip(models_p, srcs_p, recs_p)])
+    h2d = sum(sum(a.nbytes for a in m.padded()) for m in models_p) + sum(s.data.nbytes + s.smap.nbytes +
+                                                                        s.sshift.nbytes for s in srcs_p)
+    h2d += sum(r.gmap.nbytes + r.gshift.nbytes for r in recs_p)
+    d2h = sum(r.data.nbytes for r in recs_p)
+    for _ in range(1):
+        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), NSHOTS, shots))
+    dist_barrier(world)
+    e2e_steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for r in recs_p:
+            r.data[:] = 0
+        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), NSHOTS, shots))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_s = dist_max(e2e_s * 1e3, world) / 1e3
+    e2e = {"value": round(pts_per_step * world / e2e_s / 1e9, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+           "path": "rsgpu_modelling (C ABI): plan create + upload, nt steps, trace read-back, destroy"}
+    return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary())
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--tile", type=int, default=-1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_init(args)
+
+    if args.impl == "reference":
+        if rank == 0:
+            per = []
+            for _ in range(args.steps):
+                r = cpu_reference()
+                if r is None:
+                    print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                    return
+                per.append(r["value"])
+            val = statistics.median(per)
+            line = {"metric": "Gpts/s", "value": round(val, 5), "unit": "Gpts/s", "impl": "reference",
+                    "n_gpus": world, "steps": args.steps, "warmup": 0, "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                    "config": config_dict(world, "reference float (stock build, no FMA)"),
+                    "cpu_baseline": r, "e2e": {"value": round(val, 5), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
+                                               "d2h_bytes_per_step": 0}}
+            print(json.dumps(line))
+        dist_barrier(world)
+        return
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference()   # before the first CUDA call of this process (spawned workers)
+    r = run_gpu(args, rank, world, local)
+    if rank == 0:
+        line = {"metric": "Gpts/s", "value": round(r["value"], 3), "unit": "Gpts/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded layered elastic model with lenses, Ricker source)",
+                "config": config_dict(world, args.precision), "gpu_launches": int(r["launches"]),
+                "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

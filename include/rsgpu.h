@@ -140,6 +140,11 @@ rsgpu_status rsgpu_plan_sync(rsgpu_plan *plan);
 void *rsgpu_plan_stream(rsgpu_plan *plan);
 /* Device launches of the propagator kernels issued since the plan was created. */
 long long rsgpu_plan_launch_count(rsgpu_plan *plan);
+/* Kernel timing: enable_timing makes the captured time loop record CUDA events
+ * around the velocity and stress launches of the first steps of each replayed
+ * chunk; kernel_times returns their mean durations (ms) from the last replay. */
+rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *plan);
+rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *plan, float *ms_velocity, float *ms_stress);
 /* Copy one wavefield (reference field code, SXX=4.. for elastic) of one shot to the host
  * in the reference's padded layout (for step-level parity tests). */
 rsgpu_status rsgpu_plan_read_field(rsgpu_plan *plan, int shot, int field, void *host_out);

@@ -1,12 +1,22 @@
 """B200-native finite-difference wave propagation behind RockSeis's driver API.
 
 The compute path is librsgpu.so (hand-written sm_100a CUDA behind the C ABI of
-include/rsgpu.h).  Importing this package loads it and raises if it is missing:
-there is no CPU fallback.
+include/rsgpu.h).  The first use of any public name loads it and raises if it
+is missing or stale: there is no CPU fallback.  (The build module itself,
+rockseis_b200.build, does not load the library.)
 """
-from . import abi  # noqa: F401  (loads librsgpu.so or raises)
-from .rockseis import (Data2D, ModelAcoustic2D, ModelElastic2D, ModellingAcoustic2D,  # noqa: F401
-                       ModellingElastic2D, Plan, modelling_batch)
+import importlib
 
 __all__ = ["abi", "Data2D", "ModelAcoustic2D", "ModelElastic2D", "ModellingAcoustic2D", "ModellingElastic2D",
            "Plan", "modelling_batch"]
+
+_FROM_ROCKSEIS = {"Data2D", "ModelAcoustic2D", "ModelElastic2D", "ModellingAcoustic2D", "ModellingElastic2D",
+                  "Plan", "modelling_batch"}
+
+
+def __getattr__(name):
+    if name == "abi":
+        return importlib.import_module(".abi", __name__)
+    if name in _FROM_ROCKSEIS:
+        return getattr(importlib.import_module(".rockseis", __name__), name)
+    raise AttributeError(name)

@@ -63,6 +63,8 @@ def _load() -> C.CDLL:
         "rsgpu_plan_sync": (I, [V]),
         "rsgpu_plan_stream": (V, [V]),
         "rsgpu_plan_launch_count": (C.c_longlong, [V]),
+        "rsgpu_plan_enable_timing": (I, [V]),
+        "rsgpu_plan_kernel_times": (I, [V, P(C.c_float), P(C.c_float)]),
         "rsgpu_plan_destroy": (None, [V]),
         "rsgpu_pml_tables": (I, [I, D, I, V]),
         "rsgpu_stagger_model": (I, [I, I, I, I, I, I, I, V, V, V, P(V)]),

@@ -61,9 +61,65 @@ def _compile(src: str, obj: str, verbose: bool) -> None:
         raise RuntimeError(f"compile failed: {os.path.basename(src)}\n{r.stdout}\n{r.stderr}")
 
 
+# Kernel instantiations of the 2D propagators: (name, T, MODE) x tile configs
+# (TX, TZ, RZ, MINB).  The config index is the `tile` field of rsgpu_config.
+# One small translation unit each so nvcc compiles them in parallel.
+VARIANTS_2D = [("f32x", "float", "MODE_IEEE"), ("f32f", "float", "MODE_FAST"), ("f64", "double", "MODE_IEEE")]
+TILES_2D = [(64, 32, 4, 1), (64, 64, 4, 1), (32, 32, 4, 1), (32, 16, 4, 1), (32, 32, 2, 1), (64, 32, 2, 1),
+            (32, 32, 2, 6), (32, 32, 2, 8), (64, 32, 2, 3), (32, 16, 2, 8)]
+TILES_F64 = (0, 3)   # FP64 oracle propagator: two shapes
+
+
+def _generate() -> list[str]:
+    gen = os.path.join(BUILD, "gen")
+    os.makedirs(gen, exist_ok=True)
+    out, table = [], []
+    for name, t, mode in VARIANTS_2D:
+        for idx, (tx, tz, rz, mb) in enumerate(TILES_2D):
+            if t == "double" and idx not in TILES_F64:
+                continue
+            fn = f"launch_2d_{name}_{tx}x{tz}r{rz}m{mb}"
+            src = ("// generated by rockseis_b200/build.py\n#include \"fd2d_kernels.cuh\"\nnamespace rsgpu {\n"
+                   f"cudaError_t {fn}(int physics, int half, bool adj, const void *args, const void *coefs, "
+                   "const void *maps, int *err, int grid, cudaStream_t st)\n{\n"
+                   f"    return launch_2d_cfg<{t}, {mode}, {tx}, {tz}, {rz}, {mb}>(physics, half, adj, "
+                   f"*static_cast<const Step2DArgs<{t}> *>(args), static_cast<const CoefSet<{t}> *>(coefs), "
+                   "static_cast<const CUtensorMap *>(maps), err, grid, st);\n}\n}  // namespace rsgpu\n")
+            path = os.path.join(gen, fn + ".cu")
+            if not os.path.exists(path) or open(path).read() != src:
+                with open(path, "w") as f:
+                    f.write(src)
+            out.append(path)
+            table.append((name, idx, fn))
+    decl = "".join(f"cudaError_t {fn}(int, int, bool, const void *, const void *, const void *, int *, int, "
+                   "cudaStream_t);\n" for _, _, fn in table)
+    cases = ""
+    for name in [v[0] for v in VARIANTS_2D]:
+        cases += f"    if (variant == \"{name}\") {{\n        switch (cfg) {{\n"
+        for n2, idx, fn in table:
+            if n2 == name:
+                cases += f"        case {idx}: return {fn};\n"
+        cases += "        default: return nullptr;\n        }\n    }\n"
+    shapes = "".join(f"    case {i}: return {{{tx}, {tz}, {rz}, {mb}}};\n" for i, (tx, tz, rz, mb) in enumerate(TILES_2D))
+    disp = ("// generated by rockseis_b200/build.py\n#include <string>\n#include \"rsgpu_kernels.h\"\n"
+            "namespace rsgpu {\n" + decl +
+            "Launch2DFn launch_2d_table(const char *v, int cfg)\n{\n    std::string variant(v);\n" + cases +
+            "    return nullptr;\n}\n"
+            "TileShape tile_shape_2d(int cfg)\n{\n    switch (cfg) {\n" + shapes +
+            "    default: return {0, 0, 0, 0};\n    }\n}\n"
+            f"int tile_count_2d() {{ return {len(TILES_2D)}; }}\n"
+            "}  // namespace rsgpu\n")
+    path = os.path.join(gen, "fd2d_table.cpp")
+    if not os.path.exists(path) or open(path).read() != disp:
+        with open(path, "w") as f:
+            f.write(disp)
+    out.append(path)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp"))) + _generate()
     hdr_mtime = max([os.path.getmtime(h) for h in _headers()] + [0.0])
     jobs = []
     objs = []

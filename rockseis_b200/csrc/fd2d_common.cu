@@ -3,30 +3,30 @@
 #include "fd2d_kernels.cuh"
 
 namespace rsgpu {
-cudaError_t launch_step_2d_f32x(int, int, int, bool, const void *, const void *, int, cudaStream_t);
-cudaError_t launch_step_2d_f32f(int, int, int, bool, const void *, const void *, int, cudaStream_t);
-cudaError_t launch_step_2d_f64(int, int, int, bool, const void *, const void *, int, cudaStream_t);
+
+static_assert(NMAP2D == NMAP, "tensor-map slots per shot");
 
 cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, bool adj, const void *args, const void *coefs,
-                           int grid, cudaStream_t st)
+                           const void *maps, int *err, int grid, cudaStream_t st)
 {
-    if (prec == PREC_F32_EXACT) return launch_step_2d_f32x(cfg, physics, half, adj, args, coefs, grid, st);
-    if (prec == PREC_F32_FAST) return launch_step_2d_f32f(cfg, physics, half, adj, args, coefs, grid, st);
-    return launch_step_2d_f64(cfg, physics, half, adj, args, coefs, grid, st);
+    const char *v = prec == PREC_F32_EXACT ? "f32x" : prec == PREC_F32_FAST ? "f32f" : "f64";
+    Launch2DFn fn = launch_2d_table(v, cfg);
+    if (!fn) return cudaErrorInvalidValue;
+    return fn(physics, half, adj, args, coefs, maps, err, grid, st);
 }
 
 cudaError_t launch_injrec_2d(int prec, const void *shots, const void *plans, int nshots, double dt, int it_base,
                              const int *it_dev, cudaStream_t st)
 {
     if (prec == PREC_F64)
-        inject_record_2d<double, true><<<nshots, 256, 0, st>>>((const Shot2D<double> *)shots,
-                                                               (const InjRec<double> *)plans, dt, it_base, it_dev);
+        inject_record_2d<double, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot2D<double> *)shots,
+                                                                    (const InjRec<double> *)plans, dt, it_base, it_dev);
     else if (prec == PREC_F32_EXACT)
-        inject_record_2d<float, true><<<nshots, 256, 0, st>>>((const Shot2D<float> *)shots,
-                                                              (const InjRec<float> *)plans, (float)dt, it_base, it_dev);
+        inject_record_2d<float, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot2D<float> *)shots,
+                                                                   (const InjRec<float> *)plans, (float)dt, it_base, it_dev);
     else
-        inject_record_2d<float, false><<<nshots, 256, 0, st>>>((const Shot2D<float> *)shots,
-                                                               (const InjRec<float> *)plans, (float)dt, it_base, it_dev);
+        inject_record_2d<float, MODE_FAST><<<nshots, 256, 0, st>>>((const Shot2D<float> *)shots,
+                                                                   (const InjRec<float> *)plans, (float)dt, it_base, it_dev);
     return cudaGetLastError();
 }
 

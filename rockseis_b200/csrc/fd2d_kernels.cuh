@@ -3,46 +3,116 @@
 // One kernel per half-step (velocity, stress), each covering every shot of a
 // batch in one launch: the grid walks a table of (shot, tile) work items, so
 // shots with different aperture windows share a launch.  Each CTA stages the
-// input fields of a TX x TZ tile plus an 8-cell halo in shared memory, then every
-// thread produces a 4(x) x RZ(z) block of outputs with the C-PML memory-variable
-// update and correction fused into the same pass.
+// stencil inputs of its TX x TZ tile plus an 8-cell halo in shared memory with
+// TMA (cp.async.bulk.tensor, completion on an mbarrier), while its threads fetch
+// the point-wise inputs (velocities, moduli) straight into registers.  Every
+// thread then produces a 4(x) x RZ(z) block with the C-PML memory-variable
+// update and correction fused into the same pass:
+//   - x-derivatives: one 128-bit shared load per 4 taps, scalar arithmetic;
+//   - z-derivatives: column pairs, 64-bit shared loads, paired f32x2 arithmetic
+//     (FADD2/FMUL2/FFMA2), each lane rounded exactly like a scalar op;
+//   - interior tiles keep the 8 coefficients in registers; tiles within `order`
+//     cells of an array end use per-point coefficient rows (reduced order).
 //
 // Arithmetic follows the reference operation by operation (Der::ddx_fw etc. in
 // lib/der.cpp:155-540, WavesAcoustic2D/WavesElastic2D::forwardstep* in
-// lib/waves.cpp:217-404, 1416-1735, backwardstep* in lib/waves.cpp:1738-2080).
-// With EXACT=true every add/sub/mul/div is an explicitly rounded IEEE op in the
-// reference's order (no FMA contraction), so a float run reproduces the
-// reference's float results bit for bit; EXACT=false allows FMA and folds 1/dx
-// into the coefficients.
+// lib/waves.cpp:217-404, 1416-1735, backwardstep* in lib/waves.cpp:1738-2080):
+//   MODE_IEEE : every add/sub/mul is a separately rounded IEEE op in the
+//               reference's order and the final division is __fdiv_rn;
+//   MODE_RCP  : as MODE_IEEE, but x/d is computed as q=x*r, e=fma(-q,d,x),
+//               q+=e*r (Markstein's correction with r = RN(1/d)); the host only
+//               selects it after checking on the device, for all 2^32 float x,
+//               that it returns exactly what IEEE division returns for this d;
+//   MODE_FAST : FMA contraction, coefficients pre-divided by the spacing.
 #pragma once
+#include <cuda.h>
+#include <cstdint>
+#include "rsgpu.h"
 #include "rsgpu_internal.h"
 #include "rsgpu_kernels.h"
 
 namespace rsgpu {
 
-// ------------------------------------------------------------------ arithmetic
-template <typename T, bool EXACT> struct Ar;
-template <> struct Ar<float, true> {
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
-    // a + b*c with the product rounded first
-    static __device__ __forceinline__ float mad(float a, float b, float c) { return __fadd_rn(a, __fmul_rn(b, c)); }
+enum { MODE_IEEE = 0, MODE_RCP = 1, MODE_FAST = 2 };
+
+// ------------------------------------------------------------------ scalar arithmetic
+template <typename T, int MODE> struct Ar;
+template <int MODE> struct Ar<float, MODE> {
+    static constexpr bool exact = MODE != MODE_FAST;
+    static __device__ __forceinline__ float add(float a, float b) { return exact ? __fadd_rn(a, b) : a + b; }
+    static __device__ __forceinline__ float sub(float a, float b) { return exact ? __fsub_rn(a, b) : a - b; }
+    static __device__ __forceinline__ float mul(float a, float b) { return exact ? __fmul_rn(a, b) : a * b; }
+    // a + b*c (product rounded separately in the exact modes)
+    static __device__ __forceinline__ float mad(float a, float b, float c)
+    {
+        return exact ? __fadd_rn(a, __fmul_rn(b, c)) : fmaf(b, c, a);
+    }
+    // a - b*c
+    static __device__ __forceinline__ float msub(float a, float b, float c)
+    {
+        return exact ? __fsub_rn(a, __fmul_rn(b, c)) : fmaf(-b, c, a);
+    }
+    static __device__ __forceinline__ float div(float a, float d, float r)
+    {
+        if (MODE == MODE_IEEE) return __fdiv_rn(a, d);
+        const float q = __fmul_rn(a, r);
+        const float e = fmaf(-q, d, a);
+        return fmaf(e, r, q);
+    }
 };
-template <> struct Ar<float, false> {
-    static __device__ __forceinline__ float add(float a, float b) { return a + b; }
-    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
-    static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
-    static __device__ __forceinline__ float div(float a, float b) { return a / b; }
-    static __device__ __forceinline__ float mad(float a, float b, float c) { return fmaf(b, c, a); }
-};
-template <> struct Ar<double, true> {
+template <int MODE> struct Ar<double, MODE> {
+    static constexpr bool exact = true;
     static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
     static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
     static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
     static __device__ __forceinline__ double mad(double a, double b, double c) { return __dadd_rn(a, __dmul_rn(b, c)); }
+    static __device__ __forceinline__ double msub(double a, double b, double c) { return __dsub_rn(a, __dmul_rn(b, c)); }
+    static __device__ __forceinline__ double div(double a, double d, double) { return __ddiv_rn(a, d); }
+};
+
+// ------------------------------------------------------------------ paired arithmetic (x-neighbour columns)
+template <typename T> struct Pair;
+template <> struct Pair<float> { using t = float2; };
+template <> struct Pair<double> { using t = double2; };
+
+template <typename T, int MODE> struct Ar2;
+// Fast mode uses the paired FADD2/FMUL2/FFMA2 instructions; the exact modes
+// evaluate the two lanes with separately rounded scalar operations.
+template <int MODE> struct Ar2<float, MODE> {
+    using P = float2;
+    static constexpr bool exact = MODE != MODE_FAST;
+    static __device__ __forceinline__ P mk(float a) { return make_float2(a, a); }
+    static __device__ __forceinline__ P add(P a, P b)
+    {
+        return exact ? make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y)) : __fadd2_rn(a, b);
+    }
+    static __device__ __forceinline__ P sub(P a, P b)
+    {
+        return exact ? make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y)) : __fadd2_rn(a, make_float2(-b.x, -b.y));
+    }
+    static __device__ __forceinline__ P mul(P a, P b)
+    {
+        return exact ? make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)) : __fmul2_rn(a, b);
+    }
+    static __device__ __forceinline__ P acc(P s, P d, P c)
+    {
+        return exact ? make_float2(__fadd_rn(s.x, __fmul_rn(d.x, c.x)), __fadd_rn(s.y, __fmul_rn(d.y, c.y)))
+                     : __ffma2_rn(d, c, s);
+    }
+    static __device__ __forceinline__ P div(P a, P d, P r)
+    {
+        return make_float2(Ar<float, MODE>::div(a.x, d.x, r.x), Ar<float, MODE>::div(a.y, d.y, r.y));
+    }
+};
+template <int MODE> struct Ar2<double, MODE> {
+    using P = double2;
+    static constexpr bool exact = true;
+    static __device__ __forceinline__ P mk(double a) { return make_double2(a, a); }
+    static __device__ __forceinline__ P add(P a, P b) { return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y)); }
+    static __device__ __forceinline__ P sub(P a, P b) { return make_double2(__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y)); }
+    static __device__ __forceinline__ P mul(P a, P b) { return make_double2(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)); }
+    static __device__ __forceinline__ P acc(P s, P d, P c) { return add(s, mul(d, c)); }
+    static __device__ __forceinline__ P div(P a, P d, P) { return make_double2(__ddiv_rn(a.x, d.x), __ddiv_rn(a.y, d.y)); }
 };
 
 template <typename T> struct Vec4;
@@ -55,20 +125,15 @@ __device__ __forceinline__ void ld4(const T *p, T (&v)[4])
     typename Vec4<T>::type q = *reinterpret_cast<const typename Vec4<T>::type *>(p);
     v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
 }
-
-// Reference order of the stencil for one output (lib/der.cpp:183-188):
-//   acc = (f[a0]-f[b0])*c0 ; acc += (f[ak]-f[bk])*ck for k=1..7 ; acc /= d
-// In EXACT mode the table holds the raw coefficients (unused taps zero) and
-// `d` is the grid spacing.  In fast mode the table is pre-divided by d.
-template <typename T, bool EXACT>
-__device__ __forceinline__ T stencil(const T (&dlt)[NCOEF], const T *c, T d)
+__device__ __forceinline__ void ldg4(const float *p, float (&v)[4])
 {
-    using A = Ar<T, EXACT>;
-    T acc = A::mul(dlt[0], c[0]);
-#pragma unroll
-    for (int k = 1; k < NCOEF; k++) acc = EXACT ? A::add(acc, A::mul(dlt[k], c[k])) : A::mad(acc, dlt[k], c[k]);
-    if (EXACT) acc = A::div(acc, d);
-    return acc;
+    const float4 q = __ldg(reinterpret_cast<const float4 *>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ldg4(const double *p, double (&v)[4])
+{
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p)), b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
 // Number of coefficient pairs the reference uses at index i of an axis of
@@ -88,548 +153,662 @@ __device__ __forceinline__ int kbw(int i, int n, int order)
     return i;   // i == 0 gives 0
 }
 
-// Coefficient rows live in shared memory with a row stride of 9 so that a warp
-// reading rows K=0..8 touches nine distinct banks.
+// Coefficient rows in shared memory, row stride 9 so that a warp reading rows
+// K = 0..8 touches nine distinct banks.
 constexpr int CROW = 9;
-
 template <typename T>
 struct CoefSet {
     T cx[9 * CROW];   // x-direction table (pre-divided by dx in fast mode)
     T cz[9 * CROW];
 };
 
-// ------------------------------------------------------------------ tile loader
-// smem tile: (TZ + 2G) rows x (TX + 2G) cols, origin at (x0 - G, z0 - G).
-template <typename T, int TX, int TZ, int NT>
-__device__ __forceinline__ void load_tile(T *s, const T *origin, int pitch, int x0, int z0)
+// ------------------------------------------------------------------ TMA + mbarrier (bounded waits)
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 {
-    constexpr int W = TX + 2 * GUARD, H = TZ + 2 * GUARD, WQ = W / 4;
-    const T *base = origin + (long)(z0 - GUARD) * pitch + (x0 - GUARD);
-    for (int q = threadIdx.x; q < WQ * H; q += NT) {
-        int r = q / WQ, c = (q - r * WQ) * 4;
-        typename Vec4<T>::type v = *reinterpret_cast<const typename Vec4<T>::type *>(base + (long)r * pitch + c);
-        *reinterpret_cast<typename Vec4<T>::type *>(s + r * W + c) = v;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t phase)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(phase)
+                 : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Wait for the barrier phase with a wall-clock limit; on timeout record an
+// error code for the host and report failure (the caller then skips its work).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, int *err)
+{
+    if (mbar_test(bar, phase)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_test(bar, phase)) {
+        if (global_ns() - t0 > 2000000000ull) {   // 2 s
+            if (err) atomicExch(err, RSGPU_ERR_TIMEOUT);
+            return false;
+        }
+        __nanosleep(64);
     }
+    return true;
+}
+// 2D tiled TMA load of a box at element coordinates (x, y) into shared memory.
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
 }
 
-// Elementwise tile of a combination a*F1 + b*F2 (adjoint work arrays, exact order:
-// lib/waves.cpp:1774 wrk = L2M*Sxx + L*Szz).
-template <typename T, bool EXACT, int TX, int TZ, int NT>
-__device__ __forceinline__ void load_tile_comb(T *s, const T *m1, const T *f1, const T *m2, const T *f2,
-                                               int pitch, int x0, int z0)
+// ------------------------------------------------------------------ derivative blocks
+// x-derivative of a quad of 4 outputs on shared row `srow` (pointer at the
+// quad's first halo column).  FW: f[i+k+1]-f[i-k]; BW: f[i+k]-f[i-k-1]
+// (lib/der.cpp:183-188, 378-383).  `cu` = uniform coefficients (interior), or
+// per-point rows `ce[j]` (edge tiles).
+template <typename T, int MODE, bool FW, bool EDGE>
+__device__ __forceinline__ void dx_quad(const T *srow, const T (&cu)[NCOEF], const T *const (&ce)[4], T d, T r,
+                                        T (&out)[4])
 {
-    using A = Ar<T, EXACT>;
-    constexpr int W = TX + 2 * GUARD, H = TZ + 2 * GUARD;
-    long off0 = (long)(z0 - GUARD) * pitch + (x0 - GUARD);
-    for (int q = threadIdx.x; q < W * H; q += NT) {
-        int r = q / W, c = q - r * W;
-        long o = off0 + (long)r * pitch + c;
-        T v = A::mul(m1[o], f1[o]);
-        if (m2) v = A::add(v, A::mul(m2[o], f2[o]));
-        s[r * W + c] = v;
-    }
-}
-
-// x-derivatives of a quad of 4 outputs on smem row `row` (local x of the quad = xq).
-// FW: df[i] uses f[i+k+1]-f[i-k];  BW: f[i+k]-f[i-k-1].
-template <typename T, bool EXACT, bool FW, int W>
-__device__ __forceinline__ void dx_quad(const T *s, int row, int xq, const T *crow[4], T d, T (&out)[4])
-{
+    using A = Ar<T, MODE>;
     T v[20];
 #pragma unroll
-    for (int j = 0; j < 5; j++) {
-        T q[4];
-        ld4(s + row * W + xq + 4 * j, q);
-        v[4 * j] = q[0]; v[4 * j + 1] = q[1]; v[4 * j + 2] = q[2]; v[4 * j + 3] = q[3];
+    for (int q = 0; q < 5; q++) {
+        T t[4];
+        ld4(srow + 4 * q, t);
+        v[4 * q] = t[0]; v[4 * q + 1] = t[1]; v[4 * q + 2] = t[2]; v[4 * q + 3] = t[3];
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-        T dl[NCOEF];
+        T acc = T(0);
 #pragma unroll
-        for (int k = 0; k < NCOEF; k++)
-            dl[k] = FW ? Ar<T, EXACT>::sub(v[j + 9 + k], v[j + 8 - k]) : Ar<T, EXACT>::sub(v[j + 8 + k], v[j + 7 - k]);
-        out[j] = stencil<T, EXACT>(dl, crow[j], d);
-    }
-}
-
-// z-derivatives of the 4 columns of a quad for RZ rows starting at local row zr.
-// One column at a time with a scalar window of RZ+16 values keeps the register
-// footprint small; the results are returned per (row, column).
-template <typename T, bool EXACT, bool FW, int W, int RZ>
-__device__ __forceinline__ void dz_block(const T *s, int zr, int xq, const T *crow[RZ], T d, T (&out)[RZ][4])
-{
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        T w[RZ + 16];
-#pragma unroll
-        for (int r = 0; r < RZ + 16; r++) w[r] = s[(zr + r) * W + xq + GUARD + j];
-#pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            T dl[NCOEF];
-#pragma unroll
-            for (int k = 0; k < NCOEF; k++)
-                dl[k] = FW ? Ar<T, EXACT>::sub(w[r + 9 + k], w[r + 8 - k]) : Ar<T, EXACT>::sub(w[r + 8 + k], w[r + 7 - k]);
-            out[r][j] = stencil<T, EXACT>(dl, crow[r], d);
+        for (int k = 0; k < NCOEF; k++) {
+            const T dl = FW ? A::sub(v[j + 9 + k], v[j + 8 - k]) : A::sub(v[j + 8 + k], v[j + 7 - k]);
+            const T c = EDGE ? ce[j][k] : cu[k];
+            acc = (k == 0) ? A::mul(dl, c) : A::mad(acc, dl, c);
         }
+        out[j] = (MODE == MODE_FAST) ? acc : A::div(acc, d, r);
     }
 }
 
-// ------------------------------------------------------------------ PML helpers
-// Left/right strip of x: returns table index and psi column, or -1.
+// z-derivatives of a column pair (local columns c, c+1 of the tile, as one
+// 64-bit lane pair) for RZ rows starting at tile row zr.  Window of RZ+16 rows.
+template <typename T, int MODE, bool FW, bool EDGE, int W, int RZ>
+__device__ __forceinline__ void dz_pair(const T *s, int zr, int col, const T (&cu)[NCOEF], const T *const (&ce)[RZ],
+                                        T d, T r, typename Pair<T>::t (&out)[RZ])
+{
+    using A2 = Ar2<T, MODE>;
+    using P = typename Pair<T>::t;
+    P w[RZ + 16];
+#pragma unroll
+    for (int q = 0; q < RZ + 16; q++) w[q] = *reinterpret_cast<const P *>(s + (zr + q) * W + col);
+    const P d2 = A2::mk(d), r2 = A2::mk(r);
+#pragma unroll
+    for (int rr = 0; rr < RZ; rr++) {
+        P acc;
+#pragma unroll
+        for (int k = 0; k < NCOEF; k++) {
+            const P dl = FW ? A2::sub(w[rr + 9 + k], w[rr + 8 - k]) : A2::sub(w[rr + 8 + k], w[rr + 7 - k]);
+            const P c = A2::mk(EDGE ? ce[rr][k] : cu[k]);
+            acc = (k == 0) ? A2::mul(dl, c) : A2::acc(acc, dl, c);
+        }
+        out[rr] = (MODE == MODE_FAST) ? acc : A2::div(acc, d2, r2);
+    }
+}
+
+// ------------------------------------------------------------------ C-PML helpers
 __device__ __forceinline__ int xstrip(int ix, int nxp, int lpml, int &tab_base, int &col)
 {
     if (ix < lpml) { tab_base = 0; col = ix; return ix; }
-    int r = ix - (nxp - lpml);
+    const int r = ix - (nxp - lpml);
     if (r >= 0 && ix < nxp) { tab_base = 6; col = lpml + r; return r; }
     return -1;
 }
 __device__ __forceinline__ int zstrip(int iz, int nzp, int lpml, int &tab_base, int &row)
 {
     if (iz < lpml) { tab_base = 0; row = iz; return iz; }
-    int r = iz - (nzp - lpml);
+    const int r = iz - (nzp - lpml);
     if (r >= 0 && iz < nzp) { tab_base = 6; row = lpml + r; return r; }
     return -1;
 }
-
-// One C-PML correction in the reference's order (lib/waves.cpp:252-253):
-//   psi = B*psi + A*df ;  F -= a*(psi + C*df)      where a = dt*modulus
-template <typename T, bool EXACT>
-__device__ __forceinline__ T pml_correct(T F, T a, T df, T *psi, const T *tab, int lp, int base_stag, int idx)
+// psi = B*psi + A*df ;  F -= a*(psi + C*df)   (lib/waves.cpp:252-253)
+template <typename T, int MODE>
+__device__ __forceinline__ T pml_correct(T F, T a, T df, T *psi, const T *tab, int lp, int base, int idx)
 {
-    using A = Ar<T, EXACT>;
-    const T tA = tab[(base_stag + PT_A) * lp + idx];
-    const T tB = tab[(base_stag + PT_B) * lp + idx];
-    const T tC = tab[(base_stag + PT_C) * lp + idx];
+    using A = Ar<T, MODE>;
+    const T tA = __ldg(tab + (base + PT_A) * lp + idx);
+    const T tB = __ldg(tab + (base + PT_B) * lp + idx);
+    const T tC = __ldg(tab + (base + PT_C) * lp + idx);
     T p = *psi;
-    p = A::add(A::mul(tB, p), A::mul(tA, df));
+    p = A::mad(A::mul(tB, p), tA, df);
     *psi = p;
-    return A::sub(F, A::mul(a, A::add(p, A::mul(tC, df))));
+    return A::msub(F, a, A::mad(p, tC, df));
 }
 
-// ------------------------------------------------------------------ kernels
+// ------------------------------------------------------------------ tile bookkeeping
 template <typename T, int TX, int TZ, int RZ>
 struct Geo2D {
     static constexpr int NTX = TX / 4, NTZ = TZ / RZ, NT = NTX * NTZ;
     static constexpr int W = TX + 2 * GUARD, H = TZ + 2 * GUARD;
+    static constexpr int TILE_BYTES = (int)sizeof(T) * W * H;
+    static constexpr int TILE_STRIDE = (TILE_BYTES + 127) / 128 * 128;
 };
 
-// Fill the per-point coefficient row pointers of a quad (x) and block (z).
-template <typename T, int RZ>
-__device__ __forceinline__ void coef_rows(const CoefSet<T> &cs, bool xedge, bool zedge, bool fwx, bool fwz,
-                                          int gx, int gz, int nxp, int nzp, int order,
-                                          const T *cx[4], const T *cz[RZ])
-{
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        int K = xedge ? (fwx ? kfw(gx + j, nxp, order) : kbw(gx + j, nxp, order)) : order;
-        cx[j] = cs.cx + K * CROW;
-    }
-#pragma unroll
-    for (int r = 0; r < RZ; r++) {
-        int K = zedge ? (fwz ? kfw(gz + r, nzp, order) : kbw(gz + r, nzp, order)) : order;
-        cz[r] = cs.cz + K * CROW;
-    }
-}
+// Shared-memory prologue shared by all 2D kernels: nfield halo'd tiles (TMA),
+// the coefficient tables and one mbarrier.
+template <typename T, int TX, int TZ, int RZ>
+struct Smem2D {
+    using G = Geo2D<T, TX, TZ, RZ>;
+    __host__ __device__ static constexpr size_t coef_off(int nfield) { return (size_t)nfield * G::TILE_STRIDE; }
+    __host__ __device__ static constexpr size_t bar_off(int nfield) { return (coef_off(nfield) + sizeof(CoefSet<T>) + 15) / 16 * 16; }
+    __host__ __device__ static constexpr size_t bytes(int nfield) { return bar_off(nfield) + 16; }
+};
 
 template <typename T>
-__device__ __forceinline__ void load_coefs(CoefSet<T> &s, const CoefSet<T> &g)
+__device__ __forceinline__ void load_coefs(CoefSet<T> &s, const CoefSet<T> *g)
 {
-    const T *src = reinterpret_cast<const T *>(&g);
+    const T *src = reinterpret_cast<const T *>(g);
     T *dst = reinterpret_cast<T *>(&s);
     for (int i = threadIdx.x; i < (int)(sizeof(CoefSet<T>) / sizeof(T)); i += blockDim.x) dst[i] = src[i];
 }
 
-// ---------------------------------------------------------------- acoustic 2D
-// Velocity half-step: Vx += dt*Rx*Dx+P (+ x C-PML), Vz += dt*Rz*Dz+P (+ z C-PML).
-template <typename T, bool EXACT, int TX, int TZ, int RZ>
-__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT)
-a2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs)
+// Issue the TMA loads of `nmap` halo'd tiles (maps[m_0..]) into consecutive tiles.
+template <typename T, int TX, int TZ, int RZ>
+__device__ __forceinline__ void tma_stage(unsigned char *sm, uint64_t *bar, const CUtensorMap *maps, const int *which,
+                                          int nmap, int x0, int z0)
 {
     using G = Geo2D<T, TX, TZ, RZ>;
-    using A = Ar<T, EXACT>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T *sP = reinterpret_cast<T *>(smraw);
-    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sP + G::H * G::W);
-    load_coefs(cs, *coefs);
-    const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile2D tl = a.tiles[t];
-        const Shot2D<T> &sh = a.shots[tl.shot];
-        __syncthreads();
-        load_tile<T, TX, TZ, G::NT>(sP, sh.f[A2_P], sh.pitch, tl.x0, tl.z0);
-        __syncthreads();
-        const int xq = 4 * tx, zr = tz * RZ;
-        const int gx = tl.x0 + xq, gz = tl.z0 + zr;
-        const T *cx[4], *cz[RZ];
-        T dfx[RZ][4], dfz[RZ][4];
-        coef_rows<T, RZ>(cs, tl.flags & TILE_XEDGE, false, true, true, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, (uint32_t)(nmap * G::TILE_BYTES));
+        // element (x0 - GUARD, z0 - GUARD) of the field is element (x0, z0) of the allocation
+        for (int m = 0; m < nmap; m++) tma_load_2d(sm + m * G::TILE_STRIDE, maps + which[m], bar, x0, z0);
+    }
+}
+
+// Per-thread coefficient setup for one derivative direction.
+template <typename T, int N>
+__device__ __forceinline__ void coef_uniform(const T *tab, int order, T (&cu)[NCOEF])
+{
 #pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, true, G::W>(sP, zr + r + GUARD, xq, cx, a.dx, dfx[r]);
-        coef_rows<T, RZ>(cs, false, tl.flags & TILE_ZEDGE, true, true, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
-        dz_block<T, EXACT, true, G::W, RZ>(sP, zr, xq, cz, a.dz, dfz);
+    for (int k = 0; k < NCOEF; k++) cu[k] = tab[order * CROW + k];
+}
+
+// ------------------------------------------------------------------ acoustic 2D
+// Field tensor maps per shot: [0] P, [1] Vx, [2] Vz  (acoustic)
+//                             [0] Vx, [1] Vz, [2] Sxx, [3] Szz, [4] Sxz (elastic)
+constexpr int NMAP = 5;
+
+// Reduced-order stencil of K pairs at one point (reference rule near the array
+// ends): taps read from shared memory, K known only at run time.  Used to
+// overwrite the few outputs of an edge tile whose K differs from the order.
+template <typename T, int MODE>
+__device__ __noinline__ T stencil_k(const T *center, int stride, int K, const T *c, bool fw, T d, T r)
+{
+    using A = Ar<T, MODE>;
+    if (K == 0) return T(0);
+    T acc = A::mul(fw ? A::sub(center[stride], center[0]) : A::sub(center[0], center[-stride]), c[0]);
+    for (int k = 1; k < K; k++) {
+        const T dl = fw ? A::sub(center[(k + 1) * stride], center[-k * stride])
+                        : A::sub(center[k * stride], center[-(k + 1) * stride]);
+        acc = A::mad(acc, dl, c[k]);
+    }
+    return (MODE == MODE_FAST) ? acc : A::div(acc, d, r);
+}
+
+template <typename T, int MODE, int TX, int TZ, int RZ>
+__device__ __forceinline__ void row_dx(const T *tile, int row, int xq, const CoefSet<T> &cs, const T (&cu)[NCOEF],
+                                       bool fw, bool xedge, int gx, int nxp, int order, T d, T r, T (&out)[4])
+{
+    using G = Geo2D<T, TX, TZ, RZ>;
+    const T *ce[4] = {nullptr, nullptr, nullptr, nullptr};
+    const T *srow = tile + row * G::W + xq;
+    if (fw) dx_quad<T, MODE, true, false>(srow, cu, ce, d, r, out);
+    else dx_quad<T, MODE, false, false>(srow, cu, ce, d, r, out);
+    if (xedge) {
 #pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T vx[4], vz[4], rx[4], rz[4];
-            ld4(sh.f[A2_VX] + o, vx); ld4(sh.f[A2_VZ] + o, vz);
-            ld4(sh.m[M_RX] + o, rx); ld4(sh.m[M_RZ] + o, rz);
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                const T ax = A::mul(a.dt, rx[j]);
-                vx[j] = A::add(vx[j], A::mul(ax, dfx[r][j]));
-                if (tl.flags & TILE_XPML) {
-                    int xb, xcol; const int xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
-                    if (xi >= 0)
-                        vx[j] = pml_correct<T, EXACT>(vx[j], ax, dfx[r][j], sh.psix[0] + (long)iz * 2 * a.lpml + xcol,
-                                                      a.pml, a.lpml, xb + 3, xi);
-                }
-                const T az = A::mul(a.dt, rz[j]);
-                vz[j] = A::add(vz[j], A::mul(az, dfz[r][j]));
-                if (zi >= 0 && ix < sh.nxp)
-                    vz[j] = pml_correct<T, EXACT>(vz[j], az, dfz[r][j], sh.psiz[0] + (long)zrow * sh.nxp + ix,
-                                                  a.pml, a.lpml, zb + 3, zi);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) { sh.f[A2_VX][o + j] = vx[j]; sh.f[A2_VZ][o + j] = vz[j]; }
+        for (int j = 0; j < 4; j++) {
+            const int K = fw ? kfw(gx + j, nxp, order) : kbw(gx + j, nxp, order);
+            if (K != order) out[j] = stencil_k<T, MODE>(srow + j + GUARD, 1, K, cs.cx + K * CROW, fw, d, r);
         }
     }
 }
 
-// Stress half-step: P += dt*L*Dx-Vx (+x C-PML), then P += dt*L*Dz-Vz (+z C-PML).
-template <typename T, bool EXACT, int TX, int TZ, int RZ>
-__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT)
-a2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs)
+template <typename T, int MODE, int TX, int TZ, int RZ, bool FW>
+__device__ __forceinline__ void block_dz(const T *tile, int zr, int xq, const CoefSet<T> &cs, const T (&cu)[NCOEF],
+                                         bool zedge, int gz, int nzp, int order, T d, T r, T (&out)[RZ][4])
 {
     using G = Geo2D<T, TX, TZ, RZ>;
-    using A = Ar<T, EXACT>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T *sVx = reinterpret_cast<T *>(smraw);
-    T *sVz = sVx + G::H * G::W;
-    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sVz + G::H * G::W);
-    load_coefs(cs, *coefs);
-    const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile2D tl = a.tiles[t];
-        const Shot2D<T> &sh = a.shots[tl.shot];
-        __syncthreads();
-        load_tile<T, TX, TZ, G::NT>(sVx, sh.f[A2_VX], sh.pitch, tl.x0, tl.z0);
-        load_tile<T, TX, TZ, G::NT>(sVz, sh.f[A2_VZ], sh.pitch, tl.x0, tl.z0);
-        __syncthreads();
-        const int xq = 4 * tx, zr = tz * RZ;
-        const int gx = tl.x0 + xq, gz = tl.z0 + zr;
-        const T *cx[4], *cz[RZ];
-        T dfx[RZ][4], dfz[RZ][4];
-        coef_rows<T, RZ>(cs, tl.flags & TILE_XEDGE, false, false, false, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
+    using P = typename Pair<T>::t;
+    const T *ce[RZ];
 #pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, false, G::W>(sVx, zr + r + GUARD, xq, cx, a.dx, dfx[r]);
-        coef_rows<T, RZ>(cs, false, tl.flags & TILE_ZEDGE, false, false, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
-        dz_block<T, EXACT, false, G::W, RZ>(sVz, zr, xq, cz, a.dz, dfz);
+    for (int q = 0; q < RZ; q++) ce[q] = nullptr;
 #pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T p[4], l[4];
-            ld4(sh.f[A2_P] + o, p); ld4(sh.m[M_L] + o, l);
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
+    for (int cp = 0; cp < 2; cp++) {
+        P o[RZ];
+        dz_pair<T, MODE, FW, false, G::W, RZ>(tile, zr, xq + GUARD + 2 * cp, cu, ce, d, r, o);
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                const T al = A::mul(a.dt, l[j]);
-                p[j] = A::add(p[j], A::mul(al, dfx[r][j]));
-                if (tl.flags & TILE_XPML) {
-                    int xb, xcol; const int xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
-                    if (xi >= 0)
-                        p[j] = pml_correct<T, EXACT>(p[j], al, dfx[r][j], sh.psix[1] + (long)iz * 2 * a.lpml + xcol,
-                                                     a.pml, a.lpml, xb, xi);
-                }
-                p[j] = A::add(p[j], A::mul(al, dfz[r][j]));
-                if (zi >= 0 && ix < sh.nxp)
-                    p[j] = pml_correct<T, EXACT>(p[j], al, dfz[r][j], sh.psiz[1] + (long)zrow * sh.nxp + ix,
-                                                 a.pml, a.lpml, zb, zi);
+        for (int q = 0; q < RZ; q++) { out[q][2 * cp] = o[q].x; out[q][2 * cp + 1] = o[q].y; }
+    }
+    if (zedge) {
+#pragma unroll
+        for (int q = 0; q < RZ; q++) {
+            const int K = FW ? kfw(gz + q, nzp, order) : kbw(gz + q, nzp, order);
+            if (K != order) {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    out[q][j] = stencil_k<T, MODE>(tile + (zr + q + GUARD) * G::W + xq + GUARD + j, G::W, K,
+                                                   cs.cz + K * CROW, FW, d, r);
             }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) sh.f[A2_P][o + j] = p[j];
         }
     }
+}
+
+// Point-wise blocks.  Rows and columns beyond the padded grid (up to the tile
+// edge) lie inside the allocation; their parameters are zero, so the update
+// leaves the fields there exactly zero, and loads and stores need no bounds
+// checks.  `o0` is the element offset of the thread's first output.
+template <typename T, int RZ>
+__device__ __forceinline__ void load_block(const T *base, int o0, int pitch, T (&v)[RZ][4])
+{
+#pragma unroll
+    for (int q = 0; q < RZ; q++) ldg4(base + o0 + q * pitch, v[q]);
+}
+template <typename T, int RZ>
+__device__ __forceinline__ void load_block_rw(const T *base, int o0, int pitch, T (&v)[RZ][4])
+{
+#pragma unroll
+    for (int q = 0; q < RZ; q++) ld4(base + o0 + q * pitch, v[q]);
+}
+template <typename T, int RZ>
+__device__ __forceinline__ void store_block(T *base, int o0, int pitch, const T (&v)[RZ][4])
+{
+#pragma unroll
+    for (int q = 0; q < RZ; q++)
+        *reinterpret_cast<typename Vec4<T>::type *>(base + o0 + q * pitch) = {v[q][0], v[q][1], v[q][2], v[q][3]};
+}
+
+// x-part then z-part of one field, a = dt*modulus (lib/waves.cpp:245-307):
+//   F += a*d1 ; [x strip] psi = B*psi + A*d1, F -= a*(psi + C*d1) ;
+//   F += a*d2 ; [z strip] the same with the z memory variable.
+// PML = false for tiles that do not touch a C-PML strip.
+template <typename T, int MODE, int RZ, bool PML>
+__device__ __forceinline__ void update_field(T (&F)[RZ][4], const T (&Mo)[RZ][4], const T (&d1)[RZ][4],
+                                             const T (&d2)[RZ][4], bool has1, bool has2, const Shot2D<T> &sh,
+                                             const Step2DArgs<T> &a, int gx, int gz, T *psix, int xb_add, T *psiz,
+                                             int zb_add, bool const_mod)
+{
+    using A = Ar<T, MODE>;
+#pragma unroll
+    for (int q = 0; q < RZ; q++) {
+        const int iz = gz + q;
+        int zb = 0, zrow = 0, zi = -1;
+        if (PML) zi = zstrip(iz, sh.nzp, a.lpml, zb, zrow);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const T am = const_mod ? a.dt : A::mul(a.dt, Mo[q][j]);
+            if (has1) {
+                F[q][j] = A::mad(F[q][j], am, d1[q][j]);
+                if (PML) {
+                    int xb, xcol;
+                    const int xi = (iz < sh.nzp) ? xstrip(gx + j, sh.nxp, a.lpml, xb, xcol) : -1;
+                    if (xi >= 0)
+                        F[q][j] = pml_correct<T, MODE>(F[q][j], am, d1[q][j], psix + iz * 2 * a.lpml + xcol, a.pml,
+                                                       a.lpml, xb + xb_add, xi);
+                }
+            }
+            if (has2) {
+                F[q][j] = A::mad(F[q][j], am, d2[q][j]);
+                if (PML && zi >= 0 && gx + j < sh.nxp)
+                    F[q][j] = pml_correct<T, MODE>(F[q][j], am, d2[q][j], psiz + zrow * sh.nxp + gx + j, a.pml, a.lpml,
+                                                   zb + zb_add, zi);
+            }
+        }
+    }
+}
+
+template <typename T, int MODE, int RZ>
+__device__ __forceinline__ void update_field_any(bool pml, T (&F)[RZ][4], const T (&Mo)[RZ][4], const T (&d1)[RZ][4],
+                                                 const T (&d2)[RZ][4], bool has1, bool has2, const Shot2D<T> &sh,
+                                                 const Step2DArgs<T> &a, int gx, int gz, T *psix, int xb_add, T *psiz,
+                                                 int zb_add, bool const_mod)
+{
+    if (pml) update_field<T, MODE, RZ, true>(F, Mo, d1, d2, has1, has2, sh, a, gx, gz, psix, xb_add, psiz, zb_add, const_mod);
+    else update_field<T, MODE, RZ, false>(F, Mo, d1, d2, has1, has2, sh, a, gx, gz, psix, xb_add, psiz, zb_add, const_mod);
+}
+
+#define RS_TILE_SETUP()                                                                        \
+    using G = Geo2D<T, TX, TZ, RZ>;                                                            \
+    const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;                            \
+    const int xq = 4 * tx, zr = tz * RZ, gx = tl.x0 + xq, gz = tl.z0 + zr;                     \
+    const int o0 = gz * sh.pitch + gx, pitch = sh.pitch;                                       \
+    const bool xe = tl.flags & TILE_XEDGE, ze = tl.flags & TILE_ZEDGE;                         \
+    const bool pml = tl.flags & (TILE_XPML | TILE_ZPML);                                       \
+    T cux[NCOEF], cuz[NCOEF];                                                                  \
+    coef_uniform<T, 0>(cs.cx, a.order, cux);                                                   \
+    coef_uniform<T, 0>(cs.cz, a.order, cuz);                                                   \
+    (void)xe; (void)ze; (void)pml
+
+// Velocity half-step: Vx += dt*Rx*Dx+P (+ x C-PML), Vz += dt*Rz*Dz+P (+ z C-PML)
+// (lib/waves.cpp:217-310).
+template <typename T, int MODE, int TX, int TZ, int RZ>
+__device__ __forceinline__ void a2d_velocity_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
+                                                  const T *sP, const CoefSet<T> &cs, int *err, uint64_t *bar)
+{
+    RS_TILE_SETUP();
+    T F[RZ][4], M[RZ][4], F2[RZ][4], M2[RZ][4], d[RZ][4];
+    load_block_rw<T, RZ>(sh.f[A2_VX], o0, pitch, F);
+    load_block<T, RZ>(sh.m[M_RX], o0, pitch, M);
+    load_block_rw<T, RZ>(sh.f[A2_VZ], o0, pitch, F2);
+    load_block<T, RZ>(sh.m[M_RZ], o0, pitch, M2);
+    if (!mbar_wait_bounded(bar, 0, err)) return;
+#pragma unroll
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sP, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d[q]);
+    update_field_any<T, MODE, RZ>(pml, F, M, d, d, true, false, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
+    store_block<T, RZ>(sh.f[A2_VX], o0, pitch, F);
+#pragma unroll
+    for (int q = 0; q < RZ; q++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) { F[q][j] = F2[q][j]; M[q][j] = M2[q][j]; }
+    block_dz<T, MODE, TX, TZ, RZ, true>(sP, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d);
+    update_field_any<T, MODE, RZ>(pml, F, M, d, d, false, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
+    store_block<T, RZ>(sh.f[A2_VZ], o0, pitch, F);
+}
+
+// Stress half-step: P += dt*L*Dx-Vx (+x C-PML), then P += dt*L*Dz-Vz (+z C-PML)
+// (lib/waves.cpp:313-404).
+template <typename T, int MODE, int TX, int TZ, int RZ>
+__device__ __forceinline__ void a2d_stress_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
+                                                const T *sVx, const T *sVz, const CoefSet<T> &cs, int *err,
+                                                uint64_t *bar)
+{
+    RS_TILE_SETUP();
+    T F[RZ][4], M[RZ][4], d1[RZ][4], d2[RZ][4];
+    load_block_rw<T, RZ>(sh.f[A2_P], o0, pitch, F);
+    load_block<T, RZ>(sh.m[M_L], o0, pitch, M);
+    if (!mbar_wait_bounded(bar, 0, err)) return;
+#pragma unroll
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sVx, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+    block_dz<T, MODE, TX, TZ, RZ, false>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 0, false);
+    store_block<T, RZ>(sh.f[A2_P], o0, pitch, F);
 }
 
 // ---------------------------------------------------------------- elastic 2D
 // Velocity half-step.  Forward (lib/waves.cpp:1416-1566):
-//   Vx += dt*Rx*Dx+Sxx [x stag PML psi0] ; Vx += dt*Rx*Dz-Sxz [z PML psi0]
-//   Vz += dt*Rz*Dx-Sxz [x PML psi1]      ; Vz += dt*Rz*Dz+Szz [z stag PML psi1]
-// Adjoint (lib/waves.cpp:1738-1913): the same with Sxx -> L2M*Sxx + L*Szz,
-// Sxz -> M*Sxz, Szz -> L*Sxx + L2M*Szz.
-template <typename T, bool EXACT, bool ADJ, int TX, int TZ, int RZ>
-__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT)
-e2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs)
+//   Vx += dt*Rx*Dx+Sxx [x stag psi0] ; Vx += dt*Rx*Dz-Sxz [z psi0]
+//   Vz += dt*Rz*Dx-Sxz [x psi1]      ; Vz += dt*Rz*Dz+Szz [z stag psi1]
+// Adjoint (lib/waves.cpp:1738-1913): Sxx -> L2M*Sxx + L*Szz, Sxz -> M*Sxz,
+// Szz -> L*Sxx + L2M*Szz (formed in shared memory after the TMA loads).
+template <typename T, int MODE, int TX, int TZ, int RZ>
+__device__ __forceinline__ void e2d_velocity_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
+                                                  const T *sXX, const T *sZZ, const T *sXZ, const CoefSet<T> &cs,
+                                                  uint64_t *bar, int *err)
 {
-    using G = Geo2D<T, TX, TZ, RZ>;
-    using A = Ar<T, EXACT>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T *sXX = reinterpret_cast<T *>(smraw);
-    T *sZZ = sXX + G::H * G::W;
-    T *sXZ = sZZ + G::H * G::W;
-    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sXZ + G::H * G::W);
-    load_coefs(cs, *coefs);
-    const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile2D tl = a.tiles[t];
-        const Shot2D<T> &sh = a.shots[tl.shot];
-        __syncthreads();
-        if (!ADJ) {
-            load_tile<T, TX, TZ, G::NT>(sXX, sh.f[E2_SXX], sh.pitch, tl.x0, tl.z0);
-            load_tile<T, TX, TZ, G::NT>(sZZ, sh.f[E2_SZZ], sh.pitch, tl.x0, tl.z0);
-            load_tile<T, TX, TZ, G::NT>(sXZ, sh.f[E2_SXZ], sh.pitch, tl.x0, tl.z0);
-        } else {
-            load_tile_comb<T, EXACT, TX, TZ, G::NT>(sXX, sh.m[M_L2M], sh.f[E2_SXX], sh.m[M_L], sh.f[E2_SZZ], sh.pitch, tl.x0, tl.z0);
-            load_tile_comb<T, EXACT, TX, TZ, G::NT>(sZZ, sh.m[M_L], sh.f[E2_SXX], sh.m[M_L2M], sh.f[E2_SZZ], sh.pitch, tl.x0, tl.z0);
-            load_tile_comb<T, EXACT, TX, TZ, G::NT>(sXZ, sh.m[M_M], sh.f[E2_SXZ], nullptr, nullptr, sh.pitch, tl.x0, tl.z0);
-        }
-        __syncthreads();
-        const int xq = 4 * tx, zr = tz * RZ;
-        const int gx = tl.x0 + xq, gz = tl.z0 + zr;
-        const bool xe = tl.flags & TILE_XEDGE, ze = tl.flags & TILE_ZEDGE;
-        const T *cx[4], *cz[RZ];
-        T d1[RZ][4], d2[RZ][4];
-        // Vx: Dx+ Sxx and Dz- Sxz
-        coef_rows<T, RZ>(cs, xe, ze, true, false, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
+    RS_TILE_SETUP();
+    T F[RZ][4], M[RZ][4], F2[RZ][4], M2[RZ][4], d1[RZ][4], d2[RZ][4];
+    // all point-wise inputs of both passes are requested before the first wait
+    load_block_rw<T, RZ>(sh.f[E2_VX], o0, pitch, F);
+    load_block<T, RZ>(sh.m[M_RX], o0, pitch, M);
+    load_block_rw<T, RZ>(sh.f[E2_VZ], o0, pitch, F2);
+    load_block<T, RZ>(sh.m[M_RZ], o0, pitch, M2);
+    if (bar && !mbar_wait_bounded(bar, 0, err)) return;
 #pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, true, G::W>(sXX, zr + r + GUARD, xq, cx, a.dx, d1[r]);
-        dz_block<T, EXACT, false, G::W, RZ>(sXZ, zr, xq, cz, a.dz, d2);
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sXX, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+    block_dz<T, MODE, TX, TZ, RZ, false>(sXZ, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 0, false);
+    store_block<T, RZ>(sh.f[E2_VX], o0, pitch, F);
 #pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T v[4], m[4];
-            ld4(sh.f[E2_VX] + o, v); ld4(sh.m[M_RX] + o, m);
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
+    for (int q = 0; q < RZ; q++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                const T am = A::mul(a.dt, m[j]);
-                v[j] = A::add(v[j], A::mul(am, d1[r][j]));
-                if (tl.flags & TILE_XPML) {
-                    int xb, xcol; const int xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
-                    if (xi >= 0)
-                        v[j] = pml_correct<T, EXACT>(v[j], am, d1[r][j], sh.psix[0] + (long)iz * 2 * a.lpml + xcol,
-                                                     a.pml, a.lpml, xb + 3, xi);
+        for (int j = 0; j < 4; j++) { F[q][j] = F2[q][j]; M[q][j] = M2[q][j]; }
+#pragma unroll
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sXZ, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+    block_dz<T, MODE, TX, TZ, RZ, true>(sZZ, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 3, false);
+    store_block<T, RZ>(sh.f[E2_VZ], o0, pitch, F);
+}
+
+// Normal stresses of the elastic stress half-step (lib/waves.cpp:1596-1674):
+//   d1 = Dx-Vx: Sxx += dt*L2M*d1, Szz += dt*L*d1, one x memory update for both;
+//   d2 = Dz-Vz: Sxx += dt*L*d2,   Szz += dt*L2M*d2, one z memory update;
+//   free surface: Szz = 0 on row lpml.
+// Adjoint (lib/waves.cpp:1939-2018): Sxx += dt*d1, Szz += dt*d2 with their own memories.
+template <typename T, int MODE, int RZ, bool PML, bool ADJ>
+__device__ __forceinline__ void update_normal(T (&sxx)[RZ][4], T (&szz)[RZ][4], const T (&l)[RZ][4],
+                                              const T (&l2m)[RZ][4], const T (&d1)[RZ][4], const T (&d2)[RZ][4],
+                                              const Shot2D<T> &sh, const Step2DArgs<T> &a, int gx, int gz)
+{
+    using A = Ar<T, MODE>;
+#pragma unroll
+    for (int q = 0; q < RZ; q++) {
+        const int iz = gz + q;
+        int zb = 0, zrow = 0, zi = -1;
+        if (PML) zi = zstrip(iz, sh.nzp, a.lpml, zb, zrow);
+        const bool fsrow = sh.fs && iz == a.lpml;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int ix = gx + j;
+            int xb = 0, xcol = 0, xi = -1;
+            if (PML && iz < sh.nzp) xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
+            if (!ADJ) {
+                const T a2 = A::mul(a.dt, l2m[q][j]), a1 = A::mul(a.dt, l[q][j]);
+                sxx[q][j] = A::mad(sxx[q][j], a2, d1[q][j]);
+                szz[q][j] = A::mad(szz[q][j], a1, d1[q][j]);
+                if (PML && xi >= 0) {
+                    T *ps = sh.psix[2] + iz * 2 * a.lpml + xcol;
+                    const T tA = __ldg(a.pml + (xb + PT_A) * a.lpml + xi), tB = __ldg(a.pml + (xb + PT_B) * a.lpml + xi),
+                            tC = __ldg(a.pml + (xb + PT_C) * a.lpml + xi);
+                    const T p = A::mad(A::mul(tB, *ps), tA, d1[q][j]);
+                    *ps = p;
+                    const T cq = A::mad(p, tC, d1[q][j]);
+                    sxx[q][j] = A::msub(sxx[q][j], a2, cq);
+                    szz[q][j] = A::msub(szz[q][j], a1, cq);
                 }
-                v[j] = A::add(v[j], A::mul(am, d2[r][j]));
-                if (zi >= 0 && ix < sh.nxp)
-                    v[j] = pml_correct<T, EXACT>(v[j], am, d2[r][j], sh.psiz[0] + (long)zrow * sh.nxp + ix,
-                                                 a.pml, a.lpml, zb, zi);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) sh.f[E2_VX][o + j] = v[j];
-        }
-        // Vz: Dx- Sxz and Dz+ Szz
-        coef_rows<T, RZ>(cs, xe, ze, false, true, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, false, G::W>(sXZ, zr + r + GUARD, xq, cx, a.dx, d1[r]);
-        dz_block<T, EXACT, true, G::W, RZ>(sZZ, zr, xq, cz, a.dz, d2);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T v[4], m[4];
-            ld4(sh.f[E2_VZ] + o, v); ld4(sh.m[M_RZ] + o, m);
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                const T am = A::mul(a.dt, m[j]);
-                v[j] = A::add(v[j], A::mul(am, d1[r][j]));
-                if (tl.flags & TILE_XPML) {
-                    int xb, xcol; const int xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
-                    if (xi >= 0)
-                        v[j] = pml_correct<T, EXACT>(v[j], am, d1[r][j], sh.psix[1] + (long)iz * 2 * a.lpml + xcol,
+                sxx[q][j] = A::mad(sxx[q][j], a1, d2[q][j]);
+                szz[q][j] = A::mad(szz[q][j], a2, d2[q][j]);
+                if (PML && zi >= 0 && ix < sh.nxp) {
+                    T *ps = sh.psiz[2] + zrow * sh.nxp + ix;
+                    const T tA = __ldg(a.pml + (zb + PT_A) * a.lpml + zi), tB = __ldg(a.pml + (zb + PT_B) * a.lpml + zi),
+                            tC = __ldg(a.pml + (zb + PT_C) * a.lpml + zi);
+                    const T p = A::mad(A::mul(tB, *ps), tA, d2[q][j]);
+                    *ps = p;
+                    const T cq = A::mad(p, tC, d2[q][j]);
+                    sxx[q][j] = A::msub(sxx[q][j], a1, cq);
+                    szz[q][j] = A::msub(szz[q][j], a2, cq);
+                }
+            } else {
+                sxx[q][j] = A::mad(sxx[q][j], a.dt, d1[q][j]);
+                if (PML && xi >= 0)
+                    sxx[q][j] = pml_correct<T, MODE>(sxx[q][j], a.dt, d1[q][j], sh.psix[2] + iz * 2 * a.lpml + xcol,
                                                      a.pml, a.lpml, xb, xi);
-                }
-                v[j] = A::add(v[j], A::mul(am, d2[r][j]));
-                if (zi >= 0 && ix < sh.nxp)
-                    v[j] = pml_correct<T, EXACT>(v[j], am, d2[r][j], sh.psiz[1] + (long)zrow * sh.nxp + ix,
-                                                 a.pml, a.lpml, zb + 3, zi);
+                szz[q][j] = A::mad(szz[q][j], a.dt, d2[q][j]);
+                if (PML && zi >= 0 && ix < sh.nxp)
+                    szz[q][j] = pml_correct<T, MODE>(szz[q][j], a.dt, d2[q][j], sh.psiz[2] + zrow * sh.nxp + ix, a.pml,
+                                                     a.lpml, zb, zi);
             }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) sh.f[E2_VZ][o + j] = v[j];
+            if (fsrow) szz[q][j] = T(0);
         }
     }
 }
 
-// Stress half-step.  Forward (lib/waves.cpp:1571-1735):
-//   d = Dx-Vx: Sxx += dt*L2M*d, Szz += dt*L*d  [x PML psi2] ;
-//   d = Dz-Vz: Sxx += dt*L*d,   Szz += dt*L2M*d [z PML psi2] ; free surface Szz=0 ;
-//   Sxz += dt*M*Dx+Vz [x stag psi3] ; Sxz += dt*M*Dz+Vx [z stag psi3]
-// Adjoint (lib/waves.cpp:1916-2080): Sxx += dt*Dx-Vx, Szz += dt*Dz-Vz, Sxz as
-// above without the modulus.
-template <typename T, bool EXACT, bool ADJ, int TX, int TZ, int RZ>
-__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT)
-e2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs)
+// Stress half-step.  Forward (lib/waves.cpp:1571-1735): normal stresses as
+// above, then Sxz += dt*M*Dx+Vz [x stag psi3] ; Sxz += dt*M*Dz+Vx [z stag psi3].
+// Adjoint (lib/waves.cpp:1916-2080): Sxz without the modulus.
+template <typename T, int MODE, int TX, int TZ, int RZ, bool ADJ>
+__device__ __forceinline__ void e2d_stress_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
+                                                const T *sVx, const T *sVz, const CoefSet<T> &cs, uint64_t *bar,
+                                                int *err)
+{
+    RS_TILE_SETUP();
+    T d1[RZ][4], d2[RZ][4];
+    {
+        T sxx[RZ][4], szz[RZ][4], l[RZ][4], l2m[RZ][4];
+        load_block_rw<T, RZ>(sh.f[E2_SXX], o0, pitch, sxx);
+        load_block_rw<T, RZ>(sh.f[E2_SZZ], o0, pitch, szz);
+        if (!ADJ) {
+            load_block<T, RZ>(sh.m[M_L], o0, pitch, l);
+            load_block<T, RZ>(sh.m[M_L2M], o0, pitch, l2m);
+        }
+        // warm the shear-stress inputs of the second pass into L1/L2 meanwhile
+#pragma unroll
+        for (int q = 0; q < RZ; q++) {
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(sh.f[E2_SXZ] + o0 + q * pitch));
+            if (!ADJ) asm volatile("prefetch.global.L2 [%0];" ::"l"(sh.m[M_M] + o0 + q * pitch));
+        }
+        if (bar && !mbar_wait_bounded(bar, 0, err)) return;
+#pragma unroll
+        for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sVx, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+        block_dz<T, MODE, TX, TZ, RZ, false>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+        if (pml) update_normal<T, MODE, RZ, true, ADJ>(sxx, szz, l, l2m, d1, d2, sh, a, gx, gz);
+        else update_normal<T, MODE, RZ, false, ADJ>(sxx, szz, l, l2m, d1, d2, sh, a, gx, gz);
+        store_block<T, RZ>(sh.f[E2_SXX], o0, pitch, sxx);
+        store_block<T, RZ>(sh.f[E2_SZZ], o0, pitch, szz);
+    }
+    {
+        T F[RZ][4], M[RZ][4];
+        load_block_rw<T, RZ>(sh.f[E2_SXZ], o0, pitch, F);
+        if (!ADJ) load_block<T, RZ>(sh.m[M_M], o0, pitch, M);
+#pragma unroll
+        for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sVz, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+        block_dz<T, MODE, TX, TZ, RZ, true>(sVx, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+        update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[3], 3, sh.psiz[3], 3, ADJ);
+        store_block<T, RZ>(sh.f[E2_SXZ], o0, pitch, F);
+    }
+}
+
+// ------------------------------------------------------------------ kernels
+
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB>
+__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
+a2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
+{
+    using S = Smem2D<T, TX, TZ, RZ>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sm + S::coef_off(1));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::bar_off(1));
+    const Tile2D tl = a.tiles[blockIdx.x];
+    const Shot2D<T> &sh = a.shots[tl.shot];
+    const int which[1] = {tl.shot * NMAP + A2_P};
+    tma_stage<T, TX, TZ, RZ>(sm, bar, maps, which, 1, tl.x0, tl.z0);
+    load_coefs(cs, coefs);
+    __syncthreads();
+    const T *sP = reinterpret_cast<const T *>(sm);
+    a2d_velocity_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, sP, cs, err, bar);
+}
+
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB>
+__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
+a2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
 {
     using G = Geo2D<T, TX, TZ, RZ>;
-    using A = Ar<T, EXACT>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    T *sVx = reinterpret_cast<T *>(smraw);
-    T *sVz = sVx + G::H * G::W;
-    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sVz + G::H * G::W);
-    load_coefs(cs, *coefs);
-    const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-        const Tile2D tl = a.tiles[t];
-        const Shot2D<T> &sh = a.shots[tl.shot];
-        __syncthreads();
-        load_tile<T, TX, TZ, G::NT>(sVx, sh.f[E2_VX], sh.pitch, tl.x0, tl.z0);
-        load_tile<T, TX, TZ, G::NT>(sVz, sh.f[E2_VZ], sh.pitch, tl.x0, tl.z0);
-        __syncthreads();
-        const int xq = 4 * tx, zr = tz * RZ;
-        const int gx = tl.x0 + xq, gz = tl.z0 + zr;
-        const bool xe = tl.flags & TILE_XEDGE, ze = tl.flags & TILE_ZEDGE;
-        const T *cx[4], *cz[RZ];
-        T d1[RZ][4], d2[RZ][4];
-        // normal stresses: Dx- Vx, Dz- Vz
-        coef_rows<T, RZ>(cs, xe, ze, false, false, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, false, G::W>(sVx, zr + r + GUARD, xq, cx, a.dx, d1[r]);
-        dz_block<T, EXACT, false, G::W, RZ>(sVz, zr, xq, cz, a.dz, d2);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T sxx[4], szz[4], l[4], l2m[4];
-            ld4(sh.f[E2_SXX] + o, sxx); ld4(sh.f[E2_SZZ] + o, szz);
-            if (!ADJ) { ld4(sh.m[M_L] + o, l); ld4(sh.m[M_L2M] + o, l2m); }
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
-            const bool fsrow = sh.fs && iz == a.lpml;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                int xb = 0, xcol = 0;
-                const int xi = (tl.flags & TILE_XPML) ? xstrip(ix, sh.nxp, a.lpml, xb, xcol) : -1;
-                if (!ADJ) {
-                    const T a2 = A::mul(a.dt, l2m[j]), a1 = A::mul(a.dt, l[j]);
-                    sxx[j] = A::add(sxx[j], A::mul(a2, d1[r][j]));
-                    szz[j] = A::add(szz[j], A::mul(a1, d1[r][j]));
-                    if (xi >= 0) {
-                        // one psi update shared by both corrections (lib/waves.cpp:1625-1627)
-                        T *ps = sh.psix[2] + (long)iz * 2 * a.lpml + xcol;
-                        const T tA = a.pml[(xb + PT_A) * a.lpml + xi], tB = a.pml[(xb + PT_B) * a.lpml + xi],
-                                tC = a.pml[(xb + PT_C) * a.lpml + xi];
-                        T p = A::add(A::mul(tB, *ps), A::mul(tA, d1[r][j]));
-                        *ps = p;
-                        const T q = A::add(p, A::mul(tC, d1[r][j]));
-                        sxx[j] = A::sub(sxx[j], A::mul(a2, q));
-                        szz[j] = A::sub(szz[j], A::mul(a1, q));
-                    }
-                    sxx[j] = A::add(sxx[j], A::mul(a1, d2[r][j]));
-                    szz[j] = A::add(szz[j], A::mul(a2, d2[r][j]));
-                    if (zi >= 0 && ix < sh.nxp) {
-                        T *ps = sh.psiz[2] + (long)zrow * sh.nxp + ix;
-                        const T tA = a.pml[(zb + PT_A) * a.lpml + zi], tB = a.pml[(zb + PT_B) * a.lpml + zi],
-                                tC = a.pml[(zb + PT_C) * a.lpml + zi];
-                        T p = A::add(A::mul(tB, *ps), A::mul(tA, d2[r][j]));
-                        *ps = p;
-                        const T q = A::add(p, A::mul(tC, d2[r][j]));
-                        sxx[j] = A::sub(sxx[j], A::mul(a1, q));
-                        szz[j] = A::sub(szz[j], A::mul(a2, q));
-                    }
-                } else {
-                    sxx[j] = A::add(sxx[j], A::mul(a.dt, d1[r][j]));
-                    if (xi >= 0)
-                        sxx[j] = pml_correct<T, EXACT>(sxx[j], a.dt, d1[r][j], sh.psix[2] + (long)iz * 2 * a.lpml + xcol,
-                                                       a.pml, a.lpml, xb, xi);
-                    szz[j] = A::add(szz[j], A::mul(a.dt, d2[r][j]));
-                    if (zi >= 0 && ix < sh.nxp)
-                        szz[j] = pml_correct<T, EXACT>(szz[j], a.dt, d2[r][j], sh.psiz[2] + (long)zrow * sh.nxp + ix,
-                                                       a.pml, a.lpml, zb, zi);
-                }
-                if (fsrow) szz[j] = T(0);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) { sh.f[E2_SXX][o + j] = sxx[j]; sh.f[E2_SZZ][o + j] = szz[j]; }
-        }
-        // shear stress: Dx+ Vz, Dz+ Vx
-        coef_rows<T, RZ>(cs, xe, ze, true, true, gx, gz, sh.nxp, sh.nzp, a.order, cx, cz);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) dx_quad<T, EXACT, true, G::W>(sVz, zr + r + GUARD, xq, cx, a.dx, d1[r]);
-        dz_block<T, EXACT, true, G::W, RZ>(sVx, zr, xq, cz, a.dz, d2);
-#pragma unroll
-        for (int r = 0; r < RZ; r++) {
-            const int iz = gz + r;
-            if (iz >= sh.nzp) break;
-            const long o = (long)iz * sh.pitch + gx;
-            T sxz[4], mm[4];
-            ld4(sh.f[E2_SXZ] + o, sxz);
-            if (!ADJ) ld4(sh.m[M_M] + o, mm);
-            int zb, zrow; const int zi = (tl.flags & TILE_ZPML) ? zstrip(iz, sh.nzp, a.lpml, zb, zrow) : -1;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int ix = gx + j;
-                const T am = ADJ ? a.dt : A::mul(a.dt, mm[j]);
-                sxz[j] = A::add(sxz[j], A::mul(am, d1[r][j]));
-                if (tl.flags & TILE_XPML) {
-                    int xb, xcol; const int xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
-                    if (xi >= 0)
-                        sxz[j] = pml_correct<T, EXACT>(sxz[j], am, d1[r][j], sh.psix[3] + (long)iz * 2 * a.lpml + xcol,
-                                                       a.pml, a.lpml, xb + 3, xi);
-                }
-                sxz[j] = A::add(sxz[j], A::mul(am, d2[r][j]));
-                if (zi >= 0 && ix < sh.nxp)
-                    sxz[j] = pml_correct<T, EXACT>(sxz[j], am, d2[r][j], sh.psiz[3] + (long)zrow * sh.nxp + ix,
-                                                   a.pml, a.lpml, zb + 3, zi);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (gx + j < sh.nxp) sh.f[E2_SXZ][o + j] = sxz[j];
-        }
+    using S = Smem2D<T, TX, TZ, RZ>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sm + S::coef_off(2));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::bar_off(2));
+    const Tile2D tl = a.tiles[blockIdx.x];
+    const Shot2D<T> &sh = a.shots[tl.shot];
+    const int which[2] = {tl.shot * NMAP + A2_VX, tl.shot * NMAP + A2_VZ};
+    tma_stage<T, TX, TZ, RZ>(sm, bar, maps, which, 2, tl.x0, tl.z0);
+    load_coefs(cs, coefs);
+    __syncthreads();
+    const T *sVx = reinterpret_cast<const T *>(sm), *sVz = reinterpret_cast<const T *>(sm + G::TILE_STRIDE);
+    a2d_stress_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, sVx, sVz, cs, err, bar);
+}
+
+// Adjoint work arrays in place: wrk1 = L2M*Sxx + L*Szz, wrk3 = L*Sxx + L2M*Szz,
+// wrk2 = M*Sxz (lib/waves.cpp:1774, 1812, 1885), over the whole halo'd tile.
+template <typename T, int MODE, int TX, int TZ, int RZ>
+__device__ __forceinline__ void adjoint_work(T *sXX, T *sZZ, T *sXZ, const Shot2D<T> &sh, int x0, int z0)
+{
+    using G = Geo2D<T, TX, TZ, RZ>;
+    using A = Ar<T, MODE>;
+    const long off0 = (long)(z0 - GUARD) * sh.pitch + (x0 - GUARD);
+    for (int q = threadIdx.x; q < G::W * G::H; q += G::NT) {
+        const int rr = q / G::W, c = q - rr * G::W;
+        const long o = off0 + (long)rr * sh.pitch + c;
+        const T sxx = sXX[q], szz = sZZ[q], l = sh.m[M_L][o], l2m = sh.m[M_L2M][o], m = sh.m[M_M][o];
+        sXX[q] = A::add(A::mul(l2m, sxx), A::mul(l, szz));
+        sZZ[q] = A::add(A::mul(l, sxx), A::mul(l2m, szz));
+        sXZ[q] = A::mul(m, sXZ[q]);
     }
+}
+
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, bool ADJ>
+__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
+e2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
+{
+    using G = Geo2D<T, TX, TZ, RZ>;
+    using S = Smem2D<T, TX, TZ, RZ>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sm + S::coef_off(3));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::bar_off(3));
+    const Tile2D tl = a.tiles[blockIdx.x];
+    const Shot2D<T> &sh = a.shots[tl.shot];
+    const int which[3] = {tl.shot * NMAP + E2_SXX, tl.shot * NMAP + E2_SZZ, tl.shot * NMAP + E2_SXZ};
+    tma_stage<T, TX, TZ, RZ>(sm, bar, maps, which, 3, tl.x0, tl.z0);
+    load_coefs(cs, coefs);
+    __syncthreads();
+    T *sXX = reinterpret_cast<T *>(sm), *sZZ = reinterpret_cast<T *>(sm + G::TILE_STRIDE),
+      *sXZ = reinterpret_cast<T *>(sm + 2 * G::TILE_STRIDE);
+    uint64_t *wbar = bar;
+    if (ADJ) {
+        // every thread reaches the same barriers whether or not the wait succeeded
+        const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0, err));
+        if (!ok) return;
+        adjoint_work<T, MODE, TX, TZ, RZ>(sXX, sZZ, sXZ, sh, tl.x0, tl.z0);
+        __syncthreads();
+        wbar = nullptr;
+    }
+    e2d_velocity_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, sXX, sZZ, sXZ, cs, wbar, err);
+}
+
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, bool ADJ>
+__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
+e2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
+{
+    using G = Geo2D<T, TX, TZ, RZ>;
+    using S = Smem2D<T, TX, TZ, RZ>;
+    extern __shared__ __align__(128) unsigned char sm[];
+    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sm + S::coef_off(2));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::bar_off(2));
+    const Tile2D tl = a.tiles[blockIdx.x];
+    const Shot2D<T> &sh = a.shots[tl.shot];
+    const int which[2] = {tl.shot * NMAP + E2_VX, tl.shot * NMAP + E2_VZ};
+    tma_stage<T, TX, TZ, RZ>(sm, bar, maps, which, 2, tl.x0, tl.z0);
+    load_coefs(cs, coefs);
+    __syncthreads();
+    const T *sVx = reinterpret_cast<const T *>(sm), *sVz = reinterpret_cast<const T *>(sm + G::TILE_STRIDE);
+    e2d_stress_tile<T, MODE, TX, TZ, RZ, ADJ>(a, sh, tl, sVx, sVz, cs, bar, err);
 }
 
 // ---------------------------------------------------------------- sources and receivers
 // One CTA per shot.  Injection first (lib/waves.cpp:407-497, 2085-2174), then,
 // after a CTA barrier, recording (lib/waves.cpp:500-595, 2178-2288) of the same step.
-template <typename T, bool EXACT>
+template <typename T, int MODE>
 __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans, T dt, int it_base,
                                  const int *it_dev)
 {
-    using A = Ar<T, EXACT>;
+    using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
     const Shot2D<T> &sh = shots[blockIdx.x];
     const InjRec<T> &pl = plans[blockIdx.x];
     const int it = it_base + (it_dev ? *it_dev : 0);
     if (pl.kind_inj != INJ_NONE) {
         for (int q = threadIdx.x; q < pl.ninj; q += blockDim.x) {
             const int p = pl.inj_pt[q];
-            switch (pl.kind_inj) {
-            case INJ_A2_P: case INJ_A2_VX: case INJ_A2_VZ:
-            case INJ_E2_VX: case INJ_E2_VZ: {
-                T *F; const T *Mod;
-                if (pl.kind_inj == INJ_A2_P) { F = sh.f[A2_P]; Mod = sh.m[M_L]; }
-                else if (pl.kind_inj == INJ_A2_VX) { F = sh.f[A2_VX]; Mod = sh.m[M_RX]; }
-                else if (pl.kind_inj == INJ_A2_VZ) { F = sh.f[A2_VZ]; Mod = sh.m[M_RZ]; }
-                else if (pl.kind_inj == INJ_E2_VX) { F = sh.f[E2_VX]; Mod = sh.m[M_RX]; }
-                else { F = sh.f[E2_VZ]; Mod = sh.m[M_RZ]; }
-                T v = F[p];
-                const T dm = A::mul(dt, Mod[p]);
-                for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
-                    const T w = pl.wav[(long)pl.inj_trace[c] * pl.nt + it];
-                    v = A::add(v, A::mul(A::mul(A::mul(dm, w), pl.inj_wx[c]), pl.inj_wz[c]));
-                }
-                F[p] = v;
-                break;
-            }
-            case INJ_E2_P: {
+            if (pl.kind_inj == INJ_E2_P) {
                 T sxx = sh.f[E2_SXX][p], szz = sh.f[E2_SZZ][p];
                 for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
                     const T w = pl.wav[(long)pl.inj_trace[c] * pl.nt + it];
@@ -637,9 +816,24 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
                     sxx = A::sub(sxx, s);
                     szz = A::sub(szz, s);
                 }
-                sh.f[E2_SXX][p] = sxx; sh.f[E2_SZZ][p] = szz;
-                break;
-            }
+                sh.f[E2_SXX][p] = sxx;
+                sh.f[E2_SZZ][p] = szz;
+            } else {
+                T *F; const T *Mod;
+                switch (pl.kind_inj) {
+                case INJ_A2_P: F = sh.f[A2_P]; Mod = sh.m[M_L]; break;
+                case INJ_A2_VX: F = sh.f[A2_VX]; Mod = sh.m[M_RX]; break;
+                case INJ_A2_VZ: F = sh.f[A2_VZ]; Mod = sh.m[M_RZ]; break;
+                case INJ_E2_VX: F = sh.f[E2_VX]; Mod = sh.m[M_RX]; break;
+                default: F = sh.f[E2_VZ]; Mod = sh.m[M_RZ]; break;
+                }
+                T v = F[p];
+                const T dm = A::mul(dt, Mod[p]);
+                for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
+                    const T w = pl.wav[(long)pl.inj_trace[c] * pl.nt + it];
+                    v = A::add(v, A::mul(A::mul(A::mul(dm, w), pl.inj_wx[c]), pl.inj_wz[c]));
+                }
+                F[p] = v;
             }
         }
     }
@@ -688,67 +882,46 @@ static __global__ void advance_counter(int *it_dev, int by)
 }
 
 // ---------------------------------------------------------------- launchers
-template <typename T, bool EXACT, int TX, int TZ, int RZ>
+template <typename K>
+static cudaError_t set_smem(K k, size_t bytes)
+{
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB>
 cudaError_t launch_2d_cfg(int physics, int half, bool adj, const Step2DArgs<T> &a, const CoefSet<T> *coefs,
-                                 int grid, cudaStream_t st)
+                          const CUtensorMap *maps, int *err, int grid, cudaStream_t st)
 {
     using G = Geo2D<T, TX, TZ, RZ>;
-    const size_t tile = sizeof(T) * G::H * G::W;
-    const size_t cb = sizeof(CoefSet<T>);
+    using S = Smem2D<T, TX, TZ, RZ>;
     if (physics == PHYS_A2D) {
         if (half == 0) {
-            auto k = a2d_velocity<T, EXACT, TX, TZ, RZ>;
-            const size_t smem = tile + cb;
-            static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (attr != cudaSuccess) return attr;
-            k<<<grid, G::NT, smem, st>>>(a, coefs);
+            static const cudaError_t e = set_smem(a2d_velocity<T, MODE, TX, TZ, RZ, MINB>, S::bytes(1));
+            if (e != cudaSuccess) return e;
+            a2d_velocity<T, MODE, TX, TZ, RZ, MINB><<<grid, G::NT, S::bytes(1), st>>>(a, coefs, maps, err);
         } else {
-            auto k = a2d_stress<T, EXACT, TX, TZ, RZ>;
-            const size_t smem = 2 * tile + cb;
-            static const cudaError_t attr = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (attr != cudaSuccess) return attr;
-            k<<<grid, G::NT, smem, st>>>(a, coefs);
+            static const cudaError_t e = set_smem(a2d_stress<T, MODE, TX, TZ, RZ, MINB>, S::bytes(2));
+            if (e != cudaSuccess) return e;
+            a2d_stress<T, MODE, TX, TZ, RZ, MINB><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
         }
     } else {
         if (half == 0) {
-            const size_t smem = 3 * tile + cb;
-            auto k = adj ? e2d_velocity<T, EXACT, true, TX, TZ, RZ> : e2d_velocity<T, EXACT, false, TX, TZ, RZ>;
-            static const cudaError_t a0 = cudaFuncSetAttribute(e2d_velocity<T, EXACT, false, TX, TZ, RZ>,
-                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            static const cudaError_t a1 = cudaFuncSetAttribute(e2d_velocity<T, EXACT, true, TX, TZ, RZ>,
-                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (a0 != cudaSuccess) return a0;
-            if (a1 != cudaSuccess) return a1;
-            k<<<grid, G::NT, smem, st>>>(a, coefs);
+            static const cudaError_t e0 = set_smem(e2d_velocity<T, MODE, TX, TZ, RZ, MINB, false>, S::bytes(3));
+            static const cudaError_t e1 = set_smem(e2d_velocity<T, MODE, TX, TZ, RZ, MINB, true>, S::bytes(3));
+            if (e0 != cudaSuccess) return e0;
+            if (e1 != cudaSuccess) return e1;
+            if (adj) e2d_velocity<T, MODE, TX, TZ, RZ, MINB, true><<<grid, G::NT, S::bytes(3), st>>>(a, coefs, maps, err);
+            else e2d_velocity<T, MODE, TX, TZ, RZ, MINB, false><<<grid, G::NT, S::bytes(3), st>>>(a, coefs, maps, err);
         } else {
-            const size_t smem = 2 * tile + cb;
-            auto k = adj ? e2d_stress<T, EXACT, true, TX, TZ, RZ> : e2d_stress<T, EXACT, false, TX, TZ, RZ>;
-            static const cudaError_t a0 = cudaFuncSetAttribute(e2d_stress<T, EXACT, false, TX, TZ, RZ>,
-                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            static const cudaError_t a1 = cudaFuncSetAttribute(e2d_stress<T, EXACT, true, TX, TZ, RZ>,
-                                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (a0 != cudaSuccess) return a0;
-            if (a1 != cudaSuccess) return a1;
-            k<<<grid, G::NT, smem, st>>>(a, coefs);
+            static const cudaError_t e0 = set_smem(e2d_stress<T, MODE, TX, TZ, RZ, MINB, false>, S::bytes(2));
+            static const cudaError_t e1 = set_smem(e2d_stress<T, MODE, TX, TZ, RZ, MINB, true>, S::bytes(2));
+            if (e0 != cudaSuccess) return e0;
+            if (e1 != cudaSuccess) return e1;
+            if (adj) e2d_stress<T, MODE, TX, TZ, RZ, MINB, true><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
+            else e2d_stress<T, MODE, TX, TZ, RZ, MINB, false><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
         }
     }
     return cudaGetLastError();
-}
-
-template <typename T, bool EXACT>
-cudaError_t launch_2d_t(int cfg, int physics, int half, bool adj, const void *args, const void *coefs,
-                               int grid, cudaStream_t st)
-{
-    const Step2DArgs<T> &a = *static_cast<const Step2DArgs<T> *>(args);
-    const CoefSet<T> *c = static_cast<const CoefSet<T> *>(coefs);
-    switch (cfg) {
-    case TILECFG_64x32: return launch_2d_cfg<T, EXACT, 64, 32, 4>(physics, half, adj, a, c, grid, st);
-    case TILECFG_64x64: return launch_2d_cfg<T, EXACT, 64, 64, 4>(physics, half, adj, a, c, grid, st);
-    case TILECFG_32x32: return launch_2d_cfg<T, EXACT, 32, 32, 4>(physics, half, adj, a, c, grid, st);
-    case TILECFG_128x32: return launch_2d_cfg<T, EXACT, 128, 32, 4>(physics, half, adj, a, c, grid, st);
-    case TILECFG_32x16: return launch_2d_cfg<T, EXACT, 32, 16, 2>(physics, half, adj, a, c, grid, st);
-    default: return cudaErrorInvalidValue;
-    }
 }
 
 }  // namespace rsgpu

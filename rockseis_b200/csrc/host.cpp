@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "rsgpu.h"
@@ -82,6 +84,42 @@ static void build_coefs(int prec, double dx, double dz, std::vector<unsigned cha
 }
 
 int esize(int prec) { return prec == PREC_F64 ? 8 : 4; }
+
+// cuTensorMapEncodeTiled from the driver, fetched through the runtime so the
+// library needs no link-time dependency on libcuda.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// 2D tensor map over a whole pitched field allocation (guard cells included),
+// box = tile plus halo.
+static bool encode_field_map(CUtensorMap *m, void *base, int prec, int pitch, int rows, int boxw, int boxh)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const int es = esize(prec);
+    cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * es};
+    cuuint32_t box[2] = {(cuuint32_t)boxw, (cuuint32_t)boxh};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(m, prec == PREC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base,
+                     dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
 static int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 9; }
 static int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
 static int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
@@ -90,6 +128,9 @@ static int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 Plan::~Plan()
 {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto &row : tev)
+        for (auto &e : row)
+            if (e) cudaEventDestroy(e);
     if (arena) cudaFree(arena);
     if (d_meta) cudaFree(d_meta);
     if (stream) cudaStreamDestroy(stream);
@@ -147,7 +188,9 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     const int es = esize(prec);
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
-    tilecfg = (c->tile >= 0 && c->tile < TILECFG_COUNT_2D) ? c->tile : default_tile();
+    tilecfg = (c->tile >= 0 && c->tile < tile_count_2d()) ? c->tile : default_tile();
+    // the FP64 oracle propagator is built for two tile shapes only
+    if (prec == PREC_F64 && tilecfg != TILECFG_64x32 && tilecfg != TILECFG_32x16) tilecfg = TILECFG_64x32;
     const TileShape ts = tile_shape_2d(tilecfg);
     const int lp = cfg.lpml;
 
@@ -162,15 +205,18 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         L.pitch = (int)rup(GUARD + rup(L.nxp, 128) + GUARD, 32);
         L.rows = GUARD + (int)rup(L.nzp, 64) + GUARD;
         const size_t fbytes = (size_t)L.pitch * L.rows * es;
+        // state block first (zeroed by reset): wavefields, C-PML memory, traces
         for (int k = 0; k < nfields(phys); k++) L.f[k] = take(fbytes);
-        for (int k = 0; k < nparams(phys); k++) L.m[k] = take(fbytes);
         for (int k = 0; k < npsi(phys); k++) L.psix[k] = take((size_t)L.nzp * 2 * lp * es);
         for (int k = 0; k < npsi(phys); k++) L.psiz[k] = take((size_t)2 * lp * L.nxp * es);
         L.nrec = s[i].nrec;
         L.nsrc = s[i].nsrc;
         L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
-        L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
         L.field_begin = L.f[0];
+        L.state_end = off;
+        // constant inputs
+        for (int k = 0; k < nparams(phys); k++) L.m[k] = take(fbytes);
+        L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
     }
     state_end = off;   // everything above is state or data; plan tables follow
     // ---- injection / recording plans
@@ -319,7 +365,8 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     const size_t m_ir = rup(m_shots + ns * shot_bytes, 256);
     const size_t m_tiles = rup(m_ir + ns * ir_bytes, 256);
     const size_t m_coef = rup(m_tiles + tiles.size() * sizeof(Tile2D), 256);
-    const size_t m_it = rup(m_coef + coefs.size(), 256);
+    const size_t m_maps = rup(m_coef + coefs.size(), 256);
+    const size_t m_it = rup(m_maps + (size_t)ns * NMAP2D * sizeof(CUtensorMap), 256);
     const size_t m_end = m_it + 256;
     CU(cudaMalloc(&d_meta, m_end));
     std::vector<unsigned char> meta(m_end, 0);
@@ -335,12 +382,24 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     }
     std::memcpy(meta.data() + m_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
     std::memcpy(meta.data() + m_coef, coefs.data(), coefs.size());
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = shots[i];
+        for (int k = 0; k < nfields(phys); k++) {
+            CUtensorMap *m = reinterpret_cast<CUtensorMap *>(meta.data() + m_maps) + (size_t)i * NMAP2D + k;
+            if (!encode_field_map(m, A + L.f[k], prec, L.pitch, L.rows, ts.tx + 2 * GUARD, ts.tz + 2 * GUARD)) {
+                set_error("cuTensorMapEncodeTiled failed for shot %d field %d", i, k);
+                return RSGPU_ERR_CUDA;
+            }
+        }
+    }
     CU(cudaMemcpy(d_meta, meta.data(), m_end, cudaMemcpyHostToDevice));
     d_shots = (char *)d_meta + m_shots;
     d_injrec = (char *)d_meta + m_ir;
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
+    d_maps = (char *)d_meta + m_maps;
     d_it = (int *)((char *)d_meta + m_it);
+    d_err = d_it + 1;
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -390,16 +449,13 @@ int Plan::default_tile() const
     long pts = 0;
     for (const auto &L : shots) pts += (long)L.nxp * L.nzp;
     (void)pts;
-    return TILECFG_64x32;
+    return TILECFG_DEFAULT;
 }
 
 rsgpu_status Plan::reset()
 {
-    for (const auto &L : shots) {
-        const size_t es = esize(prec);
-        CU(cudaMemsetAsync((char *)arena + L.field_begin, 0, L.wav - L.field_begin, stream));
-        (void)es;
-    }
+    for (const auto &L : shots)
+        CU(cudaMemsetAsync((char *)arena + L.field_begin, 0, L.state_end - L.field_begin, stream));
     return RSGPU_OK;
 }
 
@@ -412,21 +468,26 @@ static void make_args(void *out, const Plan &p)
     a.ntiles = p.ntiles;
     a.order = p.cfg.order;
     a.dt = (T)p.cfg.dt; a.dx = (T)p.cfg.dx; a.dz = (T)p.cfg.dz;
+    a.rdx = (T)1 / a.dx; a.rdz = (T)1 / a.dz;
     a.pml = (const T *)p.d_pml;
     a.lpml = p.cfg.lpml;
     static_assert(sizeof a <= 128, "argument block");
     std::memcpy(out, &a, sizeof a);
 }
 
-rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj)
+rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj, cudaEvent_t *ev)
 {
     alignas(16) unsigned char args[128];
     if (prec == PREC_F64) make_args<double>(args, *this);
     else make_args<float>(args, *this);
     const int grid = ntiles;
     cudaError_t e;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 0, adj, args, d_coefs, grid, stream)) != cudaSuccess) goto fail;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 1, adj, args, d_coefs, grid, stream)) != cudaSuccess) goto fail;
+    // external records so the events become timestamp nodes of a captured graph
+    if (ev && (e = cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 0, adj, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if (ev && (e = cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 1, adj, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if (ev && (e = cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
     if ((e = launch_injrec_2d(prec, d_shots, d_injrec, nshots, cfg.dt, it_base, it_dev, stream)) != cudaSuccess) goto fail;
     launches += 3;
     return RSGPU_OK;
@@ -445,7 +506,8 @@ rsgpu_status Plan::run(int it0, int nsteps)
             cudaGraph_t g;
             CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             rsgpu_status st = RSGPU_OK;
-            for (int s = 0; s < G && st == RSGPU_OK; s++) st = launch_step(s, d_it, false);
+            for (int s = 0; s < G && st == RSGPU_OK; s++)
+                st = launch_step(s, d_it, false, (time_kernels && s < NTIMED) ? tev[s] : nullptr);
             if (st == RSGPU_OK) {
                 cudaError_t e = launch_advance(d_it, G, stream);
                 if (e != cudaSuccess) { set_error("launch_advance: %s", cudaGetErrorString(e)); st = RSGPU_ERR_CUDA; }
@@ -472,6 +534,45 @@ rsgpu_status Plan::run(int it0, int nsteps)
     return RSGPU_OK;
 }
 
+// Device-side error word (bounded waits that gave up); read after a sync.
+rsgpu_status Plan::check_device_error()
+{
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    if (e != 0) {
+        set_error("a device-side wait exceeded its time limit (code %d)", e);
+        return (rsgpu_status)e;
+    }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::enable_timing()
+{
+    if (time_kernels) return RSGPU_OK;
+    for (auto &row : tev)
+        for (auto &e : row) CU(cudaEventCreate(&e));
+    time_kernels = true;
+    if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::kernel_times(float *ms_vel, float *ms_str)
+{
+    if (!time_kernels || !graph_exec) { set_error("kernel timing needs enable_timing() and one graph replay"); return RSGPU_ERR_STATE; }
+    CU(cudaStreamSynchronize(stream));
+    float v = 0, w = 0;
+    for (int s = 0; s < NTIMED; s++) {
+        float a, b;
+        CU(cudaEventElapsedTime(&a, tev[s][0], tev[s][1]));
+        CU(cudaEventElapsedTime(&b, tev[s][1], tev[s][2]));
+        v += a; w += b;
+    }
+    *ms_vel = v / NTIMED;
+    *ms_str = w / NTIMED;
+    return RSGPU_OK;
+}
+
 rsgpu_status Plan::read_traces(int shot, void *host_out)
 {
     if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
@@ -482,6 +583,7 @@ rsgpu_status Plan::read_traces(int shot, void *host_out)
     std::vector<unsigned char> tmp(n * es);
     CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.traces, n * es, cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
+    if (rsgpu_status st = check_device_error()) return st;
     if (es == 8) { double *o = (double *)host_out; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
     else { float *o = (float *)host_out; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
     return RSGPU_OK;
@@ -556,9 +658,19 @@ rsgpu_status rsgpu_plan_sync(rsgpu_plan *p)
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
     cudaError_t e = cudaStreamSynchronize(p->p->stream);
     if (e != cudaSuccess) { set_error("stream sync: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-    return RSGPU_OK;
+    return p->p->check_device_error();
 }
 void *rsgpu_plan_stream(rsgpu_plan *p) { return p ? (void *)p->p->stream : nullptr; }
+rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *p)
+{
+    if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
+    return p->p->enable_timing();
+}
+rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *p, float *ms_velocity, float *ms_stress)
+{
+    if (!p || !ms_velocity || !ms_stress) { set_error("null argument"); return RSGPU_ERR_ARG; }
+    return p->p->kernel_times(ms_velocity, ms_stress);
+}
 long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? p->p->launches : 0; }
 void rsgpu_plan_destroy(rsgpu_plan *p) { delete p; }
 

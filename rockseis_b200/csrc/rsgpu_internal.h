@@ -106,6 +106,7 @@ struct Step2DArgs {
     int ntiles;
     int order;
     T dt, dx, dz;
+    T rdx, rdz;        // RN(1/dx), RN(1/dz): reciprocal-division mode only
     const T *pml;      // 12*lpml C-PML tables
     int lpml;
 };

@@ -17,6 +17,7 @@ struct ShotLayout {
     size_t f[9] = {}, m[8] = {}, psix[4] = {}, psiz[4] = {};
     size_t traces = 0, wav = 0;
     size_t field_begin = 0;   // first byte of the zero-initialised state block
+    size_t state_end = 0;     // one past its last byte (wavefields, C-PML memory, traces)
 };
 
 class Plan {
@@ -27,7 +28,10 @@ public:
     rsgpu_status run(int it0, int nsteps);
     rsgpu_status read_traces(int shot, void *host_out);
     rsgpu_status read_field(int shot, int field, void *host_out);
-    rsgpu_status launch_step(int it_base, const int *it_dev, bool adj);
+    rsgpu_status launch_step(int it_base, const int *it_dev, bool adj, cudaEvent_t *ev = nullptr);
+    rsgpu_status enable_timing();
+    rsgpu_status kernel_times(float *ms_vel, float *ms_str);
+    rsgpu_status check_device_error();
 
     rsgpu_config cfg{};
     int prec = 0, phys = 0, nshots = 0, tilecfg = 0, ntiles = 0;
@@ -36,12 +40,19 @@ public:
     size_t arena_bytes = 0, state_end = 0;
     void *d_meta = nullptr;
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
-    int *d_it = nullptr;
+    void *d_maps = nullptr;    // [nshots][NMAP2D] CUtensorMap
+    int *d_it = nullptr;       // step counter read by graph-replayed kernels
+    int *d_err = nullptr;      // device error word (bounded waits)
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool use_graph = true;
     int graph_steps = 32;
     long long launches = 0;
+    // CUDA events recorded inside the graph around the half-step kernels of the
+    // first NTIMED steps of every replayed chunk (kernel durations for rooflines)
+    static const int NTIMED = 4;
+    bool time_kernels = false;
+    cudaEvent_t tev[NTIMED][3] = {};
 
 private:
     rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s);

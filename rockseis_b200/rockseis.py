@@ -327,6 +327,13 @@ class Plan:
     def sync(self): check(abi.lib.rsgpu_plan_sync(self.h))
     def stream(self) -> int: return abi.lib.rsgpu_plan_stream(self.h) or 0
     def launch_count(self) -> int: return abi.lib.rsgpu_plan_launch_count(self.h)
+    def enable_timing(self): check(abi.lib.rsgpu_plan_enable_timing(self.h))
+
+    def kernel_times(self):
+        """Mean (velocity, stress) half-step kernel durations in ms from the last graph replay."""
+        v, s_ = C.c_float(), C.c_float()
+        check(abi.lib.rsgpu_plan_kernel_times(self.h, C.byref(v), C.byref(s_)))
+        return v.value, s_.value
 
     def read_traces(self, i, out=None):
         r = self.receivers[i]

@@ -34,7 +34,7 @@ def run_gpu(case, precision=None, tile=-1):
 
 
 @pytest.mark.parametrize("fs", [0, 1])
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("tile", list(range(10)))
 def test_acoustic2d_exact_bitwise(require_gpu, fs, tile):
     c = Case2D(abi.ACOUSTIC2D, fs=fs)
     gpu = run_gpu(c, tile=tile)
