@@ -150,6 +150,26 @@ rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *plan, float *ms_velocity, float
 rsgpu_status rsgpu_plan_read_field(rsgpu_plan *plan, int shot, int field, void *host_out);
 void rsgpu_plan_destroy(rsgpu_plan *plan);
 
+/* Forward modelling of ONE acoustic 2D shot that allocates no device memory.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc/cudaFree -- an application whose device memory belongs to another
+ * allocator or to a fixed budget, or one that cannot accept the device-wide
+ * synchronisation those calls imply while its other streams run.  Such a caller
+ * passes DEVICE buffers it owns for shot->model[0..2] (Rx, Rz, L, padded
+ * reference layout), shot->wavelet (nsrc*nt) and shot->rec_out (nrec*nt,
+ * accumulated); maps and shifts stay in host memory.  All working memory
+ * (wavefields, C-PML memory, staged parameters, plans) lives in one static
+ * 32 MiB device array per GPU, held by every GPU that loads the library until
+ * the process exits; a grid that needs more is rejected with RSGPU_ERR_ARG.
+ * Float precisions only; results equal rsgpu_modelling's.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Every call shares the array and clears
+ * what must start at zero; calls are serialised by a process-wide lock and each
+ * waits for its work on `stream` (a cudaStream_t, 0 = default) before returning,
+ * so work from two calls must not be made to overlap on the GPU: overlapping
+ * calls would race on the array. */
+rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, const rsgpu_shot *shot, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Host preprocessing (restatements of the reference's host-side code; callers
  * that hold reference objects pass the reference's own arrays instead)

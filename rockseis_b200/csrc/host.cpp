@@ -124,6 +124,17 @@ static int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 
 static int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
 static int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 
+// Shared with other host translation units (no-allocation entry point).
+void coef_table_host(int prec, double dx, double dz, std::vector<unsigned char> &out)
+{
+    if (prec == PREC_F64) build_coefs<double>(prec, dx, dz, out);
+    else build_coefs<float>(prec, dx, dz, out);
+}
+bool encode_field_map_host(void *map, void *base, int prec, int pitch, int rows, int boxw, int boxh)
+{
+    return encode_field_map(static_cast<CUtensorMap *>(map), base, prec, pitch, rows, boxw, boxh);
+}
+
 // ---------------------------------------------------------------- plan
 Plan::~Plan()
 {

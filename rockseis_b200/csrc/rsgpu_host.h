@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstddef>
 #include <string>
+#include <vector>
 #include "rsgpu_kernels.h"
 
 namespace rsgpu {
@@ -15,6 +16,8 @@ int stagger_host(int physics, int nx, int ny, int nz, int l, int fs, int prec, c
                  const void *rho, void *const *out);
 template <typename T>
 int stagger_e3d_host(int nx, int ny, int nz, int l, int fs, const T *vp, const T *vs, const T *rho, T *const *out);
+void coef_table_host(int prec, double dx, double dz, std::vector<unsigned char> &out);
+bool encode_field_map_host(void *map, void *base, int prec, int pitch, int rows, int boxw, int boxh);
 void make_map_host(int dim, int prec, int ntr, const double *coords, const int *n, const double *o, const double *d,
                    const double *gshift, int *map, void *shift);
 
