@@ -53,9 +53,9 @@ def workload_inputs(seed_model=2, seed_shots=3):
     return vp, vs, rho, sx, wav, gc
 
 
-def config_dict(ngpus, precision_name):
-    return {"workload": "elastic2d_forward_16shots_801x401_nt4000", "nx": NX, "nz": NZ, "dx": DX, "lpml": LPML,
-            "order": ORDER, "nt": NT, "dt": DT, "shots_per_gpu": NSHOTS, "receivers": NREC,
+def config_dict(ngpus, precision_name, nt=NT):
+    return {"workload": f"elastic2d_forward_16shots_801x401_nt{nt}", "nx": NX, "nz": NZ, "dx": DX, "lpml": LPML,
+            "order": ORDER, "nt": nt, "dt": DT, "shots_per_gpu": NSHOTS, "receivers": NREC,
             "padded_points_per_shot": (NX + 2 * LPML) * (NZ + 2 * LPML), "arithmetic": precision_name,
             "l2": "working set 254 MB per GPU > 126 MB L2 (no flush needed)", "parallelism": f"shots x{ngpus}"}
 
@@ -169,8 +169,6 @@ def build_batch(precision, vp, vs, rho, sx, wav, gc, nt=NT, pinned=False):
     if pinned:
         import torch
         for m in models:
-            for k, a in m._padded.items() if m._padded else []:
-                pass
             pads = m.padded()
             pinned_pads = []
             for a in pads:
@@ -233,16 +231,17 @@ def run_gpu(args, rank, world, device):
     from rockseis_b200.rockseis import Plan, make_config, make_shot
     precision = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
     vp, vs, rho, sx, wav, gc = workload_inputs()
-    models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc)
+    nt = args.nt
+    models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt)
     torch.cuda.set_device(device)
     plan = Plan(models, srcs, recs, ORDER, precision, args.tile)
     plan.enable_timing()
     st = torch.cuda.ExternalStream(plan.stream())
-    pts_per_step = sum(m.getNx_pml() * m.getNz_pml() for m in models) * NT
+    pts_per_step = sum(m.getNx_pml() * m.getNz_pml() for m in models) * nt
 
     def one_step():
         plan.reset()
-        plan.run(0, NT)
+        plan.run(0, nt)
 
     for _ in range(args.warmup):
         one_step()
@@ -277,12 +276,15 @@ def run_gpu(args, rank, world, device):
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": b_dom, "ms_per_launch": round(ms_dom, 5),
                 "ms_velocity": round(ms_vel, 5), "ms_stress": round(ms_str, 5),
-                "step_bytes_fraction": round(((b_vel + b_str) * NT / (ms_step / 1e3) / 1e9) / peak, 4)}
+                "step_bytes_fraction": round(((b_vel + b_str) * nt / (ms_step / 1e3) / 1e9) / peak, 4)}
     plan.close()
+    if args.no_e2e:
+        return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=None,
+                    clocks=clk.summary())
 
     # end to end through the C ABI from pinned host buffers
-    models_p, srcs_p, recs_p = build_batch(precision, vp, vs, rho, sx, wav, gc, pinned=True)
-    cfg = make_config(models_p[0], ORDER, NT, DT, precision, args.tile)
+    models_p, srcs_p, recs_p = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt, pinned=True)
+    cfg = make_config(models_p[0], ORDER, nt, DT, precision, args.tile)
     keep: list = []
     shots = (abi.Shot * NSHOTS)(*[make_shot(m, s, r, keep) for m, s, r in zip(models_p, srcs_p, recs_p)])
     h2d = sum(sum(a.nbytes for a in m.padded()) for m in models_p) + sum(s.data.nbytes + s.smap.nbytes +
@@ -346,10 +348,13 @@ def main():
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
     ap.add_argument("--tile", type=int, default=-1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
     args = ap.parse_args()
-    rank, world, local = dist_init(args)
 
     if args.impl == "reference":
+        # CPU only: rank 0 times the reference, the other ranks exit without work.
+        rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
         if rank == 0:
             per = []
             for _ in range(args.steps):
@@ -366,9 +371,9 @@ def main():
                     "cpu_baseline": r, "e2e": {"value": round(val, 5), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
                                                "d2h_bytes_per_step": 0}}
             print(json.dumps(line))
-        dist_barrier(world)
         return
 
+    rank, world, local = dist_init(args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference()   # before the first CUDA call of this process (spawned workers)
@@ -378,7 +383,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded layered elastic model with lenses, Ricker source)",
-                "config": config_dict(world, args.precision), "gpu_launches": int(r["launches"]),
+                "config": config_dict(world, args.precision, args.nt), "gpu_launches": int(r["launches"]),
                 "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
                 "cpu_baseline": cpu}
         print(json.dumps(line))

@@ -89,6 +89,7 @@ def ref() -> C.CDLL:
         _ref.ref_stagger_a3d_f.argtypes = [G, V, V, V, V, V, V]
         _ref.ref_stagger_e3d_f.argtypes = [G, V, V, V] + [V] * 8
         _ref.ref_makemap2d_f.argtypes = [G, I, V, I, V, V]
+        _ref.ref_makemap2d_field_f.argtypes = [G, I, V, I, I, V, V]
         _ref.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
         _ref.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
         _ref.ref_revolve_numforw.argtypes = [I, I]

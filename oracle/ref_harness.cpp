@@ -269,17 +269,22 @@ void ref_stagger_e3d_f(const ref_grid *g, const float *vp, const float *vs, cons
 }
 
 /* Geometry2D::makeMap (lib/geometry.cpp:137-230), T=float coordinates. */
-void ref_makemap2d_f(const ref_grid *g, int ntr, const double *coords, int which, int *map, float *shift)
+void ref_makemap2d_field_f(const ref_grid *g, int ntr, const double *coords, int which, int field, int *map,
+                           float *shift)
 {
     auto m = std::make_shared<ModelAcoustic2D<float>>(g->nx, g->nz, g->lpml, (float)g->dx, (float)g->dz,
                                                       (float)g->ox, (float)g->oz, g->fs != 0);
-    auto d = make_data2d<float>(ntr, g, coords, PRESSURE, which != 0, m->getGeom(), nullptr);
+    auto d = make_data2d<float>(ntr, g, coords, field, which != 0, m->getGeom(), nullptr);
     Point2D<int> *mp = which ? d->getGeom()->getGmap() : d->getGeom()->getSmap();
     Point2D<float> *sh = which ? d->getGeom()->getGshift() : d->getGeom()->getSshift();
     for (int i = 0; i < ntr; i++) {
         map[2 * i] = mp[i].x; map[2 * i + 1] = mp[i].y;
         shift[2 * i] = sh[i].x; shift[2 * i + 1] = sh[i].y;
     }
+}
+void ref_makemap2d_f(const ref_grid *g, int ntr, const double *coords, int which, int *map, float *shift)
+{
+    ref_makemap2d_field_f(g, ntr, coords, which, PRESSURE, map, shift);
 }
 void ref_makemap3d_f(const ref_grid *g, int ntr, const double *coords, int which, int *map, float *shift)
 {
