@@ -1,0 +1,186 @@
+"""Pins of the CPU oracle and of the host preprocessing (no GPU needed).
+
+tests/golden/reference_2d.npz holds outputs of the unmodified reference library
+on seeded inputs (generated by tests/golden/make_golden.py).  Here:
+
+* the C restatement (oracle/rs_oracle.c) must reproduce them bit for bit:
+  Der stencils (lib/der.cpp), acoustic and elastic 2D shot gathers
+  (lib/modelling.cpp:197-291, 545-645), the acoustic FWI gradient
+  (lib/fwi.cpp:1150-1332) and the extended RTM image (lib/rtm.cpp:423-545);
+* this library's host preprocessing (include/rsgpu.h: rsgpu_pml_tables,
+  rsgpu_stagger_model, rsgpu_make_map, rsgpu_revolve_trace) must reproduce
+  Pml::computeABC, Model*::staggerModels, Data2D::makeMap and Revolve bit for
+  bit, since the GPU path consumes exactly those arrays;
+* where the reference library is built here (oracle/_ref), the oracle is also
+  compared with it live on inputs not in the fixtures.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracle import api
+from rockseis_b200 import abi, synth
+from rockseis_b200.rockseis import Data2D, ModelAcoustic2D, ModelElastic2D
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_2d.npz"))
+SHOT = dict(nx=41, nz=31, lpml=8, dx=10.0, dt=1e-3, nt=150, order=8)
+
+
+def problem(fs, vp, rho, vs=None):
+    s = SHOT
+    return api.Problem2D(s["nx"], s["nz"], s["dx"], s["dx"], s["lpml"], s["order"], fs, s["dt"], s["nt"], vp, rho, vs)
+
+
+# ---------------------------------------------------------------- oracle vs reference fixtures
+@pytest.mark.parametrize("order", range(1, 9))
+def test_oracle_der_matches_reference(order):
+    f = GOLD["der_in"]
+    dx, dz = GOLD["der_dx_dz"]
+    nz, nx = f.shape
+    for k, which in enumerate((0, 2, 3, 5)):
+        out = np.zeros_like(f)
+        api.oracle().orc_der2d(nx, nz, order, float(dx), float(dz), which, f.ctypes.data, out.ctypes.data)
+        assert np.array_equal(out, GOLD["der_out"][order - 1, k]), f"which={which}"
+
+
+@pytest.mark.parametrize("case", [str(c) for c in GOLD["mod_cases"]])
+def test_oracle_shot_gather_matches_reference(case):
+    g = lambda k: GOLD[f"{case}_{k}"]  # noqa: E731
+    elastic, fs, sf, rf = (int(x) for x in g("meta"))
+    pb = problem(fs, g("vp"), g("rho"), g("vs") if elastic else None)
+    models = list(g("models"))
+    args = (pb, models, g("tab"), g("smap"), g("sshift"), g("wav"), sf, g("gmap"), g("gshift"), rf)
+    out = api.orc_modelling_e2d(*args) if elastic else api.orc_modelling_a2d(*args)
+    ref = g("traces")
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(out, ref), f"max abs diff {np.abs(out - ref).max()}"
+
+
+def test_oracle_fwi_gradient_matches_reference():
+    g = lambda k: GOLD[f"fwi_{k}"]  # noqa: E731
+    pb = problem(0, g("vp"), g("rho"))
+    r = api.orc_fwi_a2d(pb, list(g("models")), g("tab"), g("smap"), g("sshift"), g("wav"), g("gmap"), g("gshift"),
+                        g("obs"))
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        ref = g(f"out_{k}")
+        assert np.abs(ref).max() > 0, k
+        assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
+    assert r["misfit"] == float(g("out_misfit"))
+
+
+def test_oracle_rtm_image_matches_reference():
+    g = lambda k: GOLD[f"fwi_{k}"]  # noqa: E731
+    pb = problem(0, g("vp"), g("rho"))
+    img = api.orc_rtm_a2d(pb, list(g("models")), g("tab"), g("smap"), g("sshift"), g("wav"), g("gmap"), g("gshift"),
+                          g("obs"), nhx=3, nhz=1)
+    ref = GOLD["rtm_image_h3"]
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(img, ref), f"max abs diff {np.abs(img - ref).max()}"
+
+
+# ---------------------------------------------------------------- host preprocessing vs reference fixtures
+@pytest.mark.parametrize("lpml", [10, 30])
+def test_pml_tables_match_reference(lpml):
+    t = np.zeros(12 * lpml, np.float32)
+    abi.check(abi.lib.rsgpu_pml_tables(lpml, float(GOLD[f"pml_{lpml}_dt"][0]), abi.F32_EXACT, t.ctypes.data))
+    assert np.array_equal(t, GOLD[f"pml_{lpml}"])
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_stagger_models_match_reference(fs):
+    vp, vs, rho = GOLD["stag_vp"], GOLD["stag_vs"], GOLD["stag_rho"]
+    nz, nx = vp.shape
+    a = ModelAcoustic2D(nx, nz, 5, 10.0, 10.0, 0.0, 0.0, fs)
+    a.createModel()
+    a.Vp[:], a.R[:] = vp, rho
+    for got, ref in zip(a.padded(), GOLD[f"stag_a2d_fs{fs}"]):
+        assert np.array_equal(got, ref)
+    e = ModelElastic2D(nx, nz, 5, 10.0, 10.0, 0.0, 0.0, fs)
+    e.createModel()
+    e.Vp[:], e.Vs[:], e.R[:] = vp, vs, rho
+    for name, got, ref in zip(e.names, e.padded(), GOLD[f"stag_e2d_fs{fs}"]):
+        assert np.array_equal(got, ref), name
+
+
+@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("field", [abi.PRESSURE, abi.VX, abi.VZ])
+def test_make_map_matches_reference(which, field):
+    nx, nz, lpml, dx, dz, ox, oz = GOLD["map_grid"]
+    m = ModelAcoustic2D(int(nx), int(nz), int(lpml), dx, dz, ox, oz, 0)
+    coords = GOLD["map_coords"]
+    d = Data2D(len(coords), 10, 1e-3, 0.0)
+    (d.scoords if which == 0 else d.gcoords)[:] = coords
+    d.setField(field)
+    d.makeMap(m, which)
+    mp, sh = (d.smap, d.sshift) if which == 0 else (d.gmap, d.gshift)
+    ref_map, ref_shift = GOLD[f"map_w{which}_f{field}"], GOLD[f"shift_w{which}_f{field}"]
+    assert (ref_map[:, 0] < 0).any() and (ref_map[:, 0] >= 0).any()     # off-grid and on-grid traces covered
+    on = ref_map[:, 0] >= 0
+    assert np.array_equal(mp[:, 0] >= 0, on)
+    assert np.array_equal(mp[on], ref_map[on])
+    assert np.array_equal(sh[on], ref_shift[on])
+
+
+@pytest.mark.parametrize("pair", [tuple(int(x) for x in p) for p in GOLD["rev_pairs"]])
+def test_revolve_schedule_matches_reference(pair):
+    nt, nc = pair
+    ref = GOLD[f"rev_{nt}_{nc}"]
+    n = ref.shape[1]
+    a, c, k = (np.zeros(n + 8, np.int32) for _ in range(3))
+    cnt = C.c_int()
+    ip = C.POINTER(C.c_int)
+    abi.check(abi.lib.rsgpu_revolve_trace(nt, nc, n + 8, a.ctypes.data_as(ip), c.ctypes.data_as(ip),
+                                          k.ctypes.data_as(ip), C.byref(cnt)))
+    assert cnt.value == n
+    assert np.array_equal(np.stack([a[:n], c[:n], k[:n]]), ref)
+    assert abi.lib.rsgpu_revolve_numforw(nt, nc) == int(GOLD[f"rev_numforw_{nt}_{nc}"][0])
+
+
+# ---------------------------------------------------------------- oracle vs the reference library, live
+needs_ref = pytest.mark.skipif(not api.ref_available(), reason="reference library oracle/_ref not built here")
+
+
+def _live_case(seed, elastic, fs, sf, rf):
+    s = SHOT
+    vp = synth.layered_vp(s["nx"], s["nz"], s["dx"], 1600, 3200, 4, 0.08, 40, seed)
+    rho = synth.gardner(vp)
+    vs = (vp / 1.9).astype(np.float32) if elastic else None
+    prec = abi.F32_EXACT
+    m = (ModelElastic2D if elastic else ModelAcoustic2D)(s["nx"], s["nz"], s["lpml"], s["dx"], s["dx"], 0.0, 0.0, fs)
+    m.createModel()
+    m.Vp[:], m.R[:] = vp, rho
+    if elastic:
+        m.Vs[:] = vs
+    rng = np.random.default_rng(seed)
+    sc = np.array([[rng.uniform(50, 350), rng.uniform(5, 250)]])
+    gc = synth.surface_line(9, rng.uniform(0, 20), 41.0, rng.uniform(0, 30)).astype(np.float32).astype(np.float64)
+    wav = synth.ricker(s["nt"], s["dt"], 18.0)[None, :]
+    src, rec = Data2D(1, s["nt"], s["dt"], 0.0, prec), Data2D(len(gc), s["nt"], s["dt"], 0.0, prec)
+    src.scoords[:], rec.gcoords[:] = sc, gc
+    src.setField(sf)
+    rec.setField(rf)
+    src.makeMap(m, 0)
+    rec.makeMap(m, 1)
+    tab = np.zeros(12 * s["lpml"], np.float32)
+    abi.check(abi.lib.rsgpu_pml_tables(s["lpml"], s["dt"], prec, tab.ctypes.data))
+    pb = problem(fs, vp, rho, vs)
+    return pb, m, src, rec, tab, sc, gc, wav
+
+
+@needs_ref
+@pytest.mark.parametrize("seed,elastic,fs,sf,rf", [(101, False, 0, abi.PRESSURE, abi.VZ),
+                                                   (102, False, 1, abi.VX, abi.PRESSURE),
+                                                   (103, True, 1, abi.PRESSURE, abi.PRESSURE),
+                                                   (104, True, 0, abi.VZ, abi.VX)])
+def test_oracle_with_library_preprocessing_matches_reference_live(seed, elastic, fs, sf, rf):
+    """Oracle fed by this library's host preprocessing vs the reference run end to end."""
+    pb, m, src, rec, tab, sc, gc, wav = _live_case(seed, elastic, fs, sf, rf)
+    args = (pb, m.padded(), tab, src.smap, src.sshift, wav, sf, rec.gmap, rec.gshift, rf)
+    if elastic:
+        out, ref = api.orc_modelling_e2d(*args), api.ref_modelling_e2d(pb, sc, wav, sf, gc, rf)
+    else:
+        out, ref = api.orc_modelling_a2d(*args), api.ref_modelling_a2d(pb, sc, wav, sf, gc, rf)
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(out, ref), f"max abs diff {np.abs(out - ref).max()}"
