@@ -171,6 +171,71 @@ void rsgpu_plan_destroy(rsgpu_plan *plan);
 rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, const rsgpu_shot *shot, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * FWI gradient and RTM image (adjoint path with Revolve checkpointing)
+ * ------------------------------------------------------------------------- */
+/* How the gradient / image and the misfit are summed over the nt adjoint steps:
+ *   ACCUM_REFERENCE: in the propagator's element type, in the reference's order
+ *                    (with RSGPU_F32_EXACT: bit-identical to the reference);
+ *   ACCUM_F64      : per-step contributions added in double on the GPU, misfit
+ *                    summed in double (fixed-order tree). */
+enum { RSGPU_ACCUM_REFERENCE = 0, RSGPU_ACCUM_F64 = 1 };
+
+typedef struct {
+    int ncheck;          /* Revolve snapshots (Fwi::setNcheck / Rtm::setNcheck); values outside
+                            [2, nt] fall back to Revolve::adjust(nt) like the reference */
+    int ckpt_precision;  /* RSGPU_CKPT_NATIVE (lossless) / RSGPU_CKPT_F16 / RSGPU_CKPT_BF16: the
+                            checkpoint slots hold the state as 16-bit values with a power-of-two
+                            scale per array */
+    int accum;           /* RSGPU_ACCUM_* */
+    int misfit;          /* RSGPU_MISFIT_DIFFERENCE (others: RSGPU_ERR_UNSUPPORTED) */
+    int nhx, nhz;        /* RTM extended-image lags (Rtm::setNhx/setNhz; odd, 1 = zero lag) */
+    int reserved[10];
+} rsgpu_adjoint_opts;
+
+/* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332) or
+ * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545).  `shot` carries the padded
+ * model, the source (wavelet, SMAP maps) and the receiver maps (GMAP) exactly
+ * as for rsgpu_modelling; src_field and rec_field must be RSGPU_PRESSURE.
+ * Every output is ACCUMULATED (+=) and may be NULL when not wanted. */
+typedef struct {
+    rsgpu_shot shot;      /* shot.rec_out: FWI modelled data (datamodP), nrec*nt */
+    const void *vp;       /* FWI: unpadded vp, nz*nx (ModelAcoustic2D::getVp) */
+    const void *rho;      /* FWI: unpadded density, nz*nx (getR) */
+    const void *data;     /* FWI: recorded data (datarecP); RTM: the data to migrate; nrec*nt */
+    void *vpgrad;         /* FWI: nz*nx (vpgrad image) */
+    void *rhograd;        /* FWI: nz*nx */
+    void *wavgrad;        /* FWI: nsrc*nt wavelet gradient (SMAP recording of the adjoint P) */
+    void *datares;        /* FWI: nrec*nt residuals (dataresP) */
+    double *misfit;       /* FWI: one value, accumulated */
+    void *image;          /* RTM: nhz*nhx*nz*nx (pimage, Image2D layout) */
+} rsgpu_adjoint_shot;
+
+/* FwiAcoustic2D<float>::run_optimal for a batch of shots (DIFFERENCE misfit). */
+rsgpu_status rsgpu_fwi_gradient(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
+                                const rsgpu_adjoint_shot *shots);
+/* RtmAcoustic2D<float>::run_optimal for a batch of shots. */
+rsgpu_status rsgpu_rtm_image(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
+                             const rsgpu_adjoint_shot *shots);
+
+/* The same drivers with the batch resident on the device between runs (no
+ * counterpart in the reference; for repeated gradients of one batch):
+ * create uploads models, maps and data; run computes one gradient / image of
+ * every shot on the device; read adds the results of the last run into the
+ * host outputs of `shots` (the same array that create received, or one with the
+ * same shapes); stats reports the work of the last run. */
+typedef struct rsgpu_adjoint rsgpu_adjoint;
+enum { RSGPU_KIND_FWI = 0, RSGPU_KIND_RTM = 1 };
+rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int kind, int nshots,
+                                  const rsgpu_adjoint_shot *shots, rsgpu_adjoint **adj);
+rsgpu_status rsgpu_adjoint_run(rsgpu_adjoint *adj);
+rsgpu_status rsgpu_adjoint_read(rsgpu_adjoint *adj, int nshots, const rsgpu_adjoint_shot *shots);
+/* forward steps, adjoint steps, checkpoint bytes written + read, kernel launches */
+rsgpu_status rsgpu_adjoint_stats(rsgpu_adjoint *adj, long long *fw_steps, long long *bw_steps,
+                                 long long *ckpt_bytes, long long *launches);
+void *rsgpu_adjoint_stream(rsgpu_adjoint *adj);
+void rsgpu_adjoint_destroy(rsgpu_adjoint *adj);
+
+/* ---------------------------------------------------------------------------
  * Host preprocessing (restatements of the reference's host-side code; callers
  * that hold reference objects pass the reference's own arrays instead)
  * ------------------------------------------------------------------------- */

@@ -24,6 +24,9 @@ F32_EXACT, F32_FAST, F64 = 0, 1, 2
 PRESSURE, VX, VY, VZ, SXX, SYY, SZZ, SYZ, SXZ, SXY = range(10)
 CKPT_NATIVE, CKPT_F16, CKPT_BF16 = 0, 1, 2
 ADVANCE, TAKESHOT, RESTORE, FIRSTURN, YOUTURN, TERMINATE, ERROR = range(7)
+ACCUM_REFERENCE, ACCUM_F64 = 0, 1
+MISFIT_DIFFERENCE, MISFIT_CORRELATION = 0, 1
+KIND_FWI, KIND_RTM = 0, 1
 
 
 class RsgpuError(RuntimeError):
@@ -43,6 +46,17 @@ class Shot(C.Structure):
                 ("nsrc", C.c_int), ("smap", C.c_void_p), ("sshift", C.c_void_p), ("wavelet", C.c_void_p),
                 ("src_field", C.c_int), ("nrec", C.c_int), ("gmap", C.c_void_p), ("gshift", C.c_void_p),
                 ("rec_field", C.c_int), ("rec_factor", C.c_void_p), ("rec_out", C.c_void_p)]
+
+
+class AdjointOpts(C.Structure):
+    _fields_ = [("ncheck", C.c_int), ("ckpt_precision", C.c_int), ("accum", C.c_int), ("misfit", C.c_int),
+                ("nhx", C.c_int), ("nhz", C.c_int), ("reserved", C.c_int * 10)]
+
+
+class AdjointShot(C.Structure):
+    _fields_ = [("shot", Shot), ("vp", C.c_void_p), ("rho", C.c_void_p), ("data", C.c_void_p),
+                ("vpgrad", C.c_void_p), ("rhograd", C.c_void_p), ("wavgrad", C.c_void_p), ("datares", C.c_void_p),
+                ("misfit", C.POINTER(C.c_double)), ("image", C.c_void_p)]
 
 
 def _load() -> C.CDLL:
@@ -72,6 +86,14 @@ def _load() -> C.CDLL:
         "rsgpu_make_map": (I, [I, I, I, P(D), P(I), P(D), P(D), P(D), P(I), V]),
         "rsgpu_revolve_trace": (I, [I, I, I, P(I), P(I), P(I), P(I)]),
         "rsgpu_revolve_numforw": (I, [I, I]),
+        "rsgpu_fwi_gradient": (I, [P(Config), P(AdjointOpts), I, P(AdjointShot)]),
+        "rsgpu_rtm_image": (I, [P(Config), P(AdjointOpts), I, P(AdjointShot)]),
+        "rsgpu_adjoint_create": (I, [P(Config), P(AdjointOpts), I, I, P(AdjointShot), P(V)]),
+        "rsgpu_adjoint_run": (I, [V]),
+        "rsgpu_adjoint_read": (I, [V, I, P(AdjointShot)]),
+        "rsgpu_adjoint_stats": (I, [V] + [P(C.c_longlong)] * 4),
+        "rsgpu_adjoint_stream": (V, [V]),
+        "rsgpu_adjoint_destroy": (None, [V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

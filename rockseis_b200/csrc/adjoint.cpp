@@ -1,0 +1,512 @@
+// FWI gradient and RTM image drivers (host runtime behind rsgpu_fwi_gradient,
+// rsgpu_rtm_image and rsgpu_adjoint_*).
+//
+// The reference's FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332) and
+// RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545) drive a forward and an
+// adjoint propagator with a Revolve checkpoint schedule.  Here the same schedule
+// (RevolveSchedule, csrc/revolve.cpp) drives two batched plans that share one
+// stream:
+//   fw : the shots as given; records the modelled data during the first sweep
+//   bw : the adjoint wavefield, run forward in reversed time (it' = nt-1-it):
+//        its sources are the receivers (residuals or data injected as pressure
+//        at GMAP), its receivers the sources (wavelet gradient at SMAP).
+// Actions:
+//   ADVANCE   fw steps oldcapo..capo-1 (inject, and record until FIRSTURN)
+//   TAKESHOT  all shots' wavefields + C-PML memory -> checkpoint slot `check`
+//   RESTORE   slot `check` -> fw state
+//   FIRSTURN  fw step nt-1 (inject, record); residuals + misfit; bw injection at
+//             nt-1 without propagation; correlation at nt-1
+//   YOUTURN   bw step at it = capo (propagate, inject, record); correlation of
+//             the bw state with the fw state at capo, i.e. the forward state
+//             after step capo-1 (the reference's pairing)
+// Every correlation launch covers all shots.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "rsgpu.h"
+#include "rsgpu_adjoint.h"
+#include "rsgpu_host.h"
+#include "rsgpu_internal.h"
+#include "rsgpu_plan.h"
+
+namespace rsgpu {
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return RSGPU_ERR_CUDA;                                                        \
+        }                                                                                 \
+    } while (0)
+#define ST(call)                                 \
+    do {                                         \
+        rsgpu_status s_ = (call);                \
+        if (s_ != RSGPU_OK) return s_;           \
+    } while (0)
+
+static inline size_t rup(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+class Adjoint {
+public:
+    ~Adjoint();
+    rsgpu_status create(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
+                        const rsgpu_adjoint_shot *s);
+    rsgpu_status run();
+    rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
+
+    int kind = RSGPU_KIND_FWI, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhz = 1;
+    int ncheck = 0, nslots = 0, nxmax = 0, nzmax = 0;
+    rsgpu_config cfg{};
+    std::unique_ptr<Plan> fw, bw;
+    cudaStream_t stream = nullptr;
+    void *dbuf = nullptr, *ckpt = nullptr;
+    size_t slot_elems = 0, ck_es = 4;
+    std::vector<CkptSeg> segs;
+    std::vector<size_t> o_vp, o_rho, o_obs, o_g0, o_g1;
+    size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    std::vector<int> nx, nz, nrec, nsrc;
+    long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
+    bool ran = false;
+
+private:
+    rsgpu_status correlate();
+    rsgpu_status save(int slot);
+    rsgpu_status load(int slot);
+    template <typename T>
+    void build_desc(std::vector<unsigned char> &corr, std::vector<unsigned char> &res);
+    char *D(size_t o) const { return (char *)dbuf + o; }
+};
+
+Adjoint::~Adjoint()
+{
+    fw.reset();
+    bw.reset();
+    if (dbuf) cudaFree(dbuf);
+    if (ckpt) cudaFree(ckpt);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
+                                  const rsgpu_adjoint_shot *s)
+{
+    if (!c || !o || !s || ns < 1) { set_error("null config/options/shots or nshots < 1"); return RSGPU_ERR_ARG; }
+    if (kind != RSGPU_KIND_FWI && kind != RSGPU_KIND_RTM) { set_error("bad driver kind %d", kind); return RSGPU_ERR_ARG; }
+    if (c->physics != RSGPU_ACOUSTIC2D) {
+        set_error("the gradient/image drivers are built for acoustic 2D physics only");
+        return RSGPU_ERR_UNSUPPORTED;
+    }
+    if (o->misfit != RSGPU_MISFIT_DIFFERENCE) { set_error("only the DIFFERENCE misfit is built"); return RSGPU_ERR_UNSUPPORTED; }
+    if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
+        set_error("bad checkpoint precision %d", o->ckpt_precision);
+        return RSGPU_ERR_ARG;
+    }
+    if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
+    if (kind == RSGPU_KIND_RTM && (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || o->nhz % 2 == 0)) {
+        set_error("nhx and nhz must be odd and positive");
+        return RSGPU_ERR_ARG;
+    }
+    for (int i = 0; i < ns; i++) {
+        const rsgpu_shot &sh = s[i].shot;
+        if (sh.src_field != RSGPU_PRESSURE || (sh.nrec > 0 && sh.rec_field != RSGPU_PRESSURE)) {
+            set_error("shot %d: the acoustic gradient/image drivers take pressure sources and receivers", i);
+            return RSGPU_ERR_UNSUPPORTED;
+        }
+        if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
+        if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
+        if (kind == RSGPU_KIND_FWI && (!s[i].vp || !s[i].rho)) { set_error("shot %d: vp/rho are null", i); return RSGPU_ERR_ARG; }
+    }
+    return RSGPU_OK;
+}
+
+rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int k, int ns,
+                             const rsgpu_adjoint_shot *s)
+{
+    ST(check_adjoint(c, o, k, ns, s));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        set_error("no CUDA device");
+        return RSGPU_ERR_NODEVICE;
+    }
+    kind = k;
+    cfg = *c;
+    nshots = ns;
+    prec = c->precision;
+    es = esize(prec);
+    acc = o->accum == RSGPU_ACCUM_F64 ? ACC_F64 : ACC_REF;
+    ck = o->ckpt_precision;
+    ck_es = ck == CK_NATIVE ? (size_t)es : 2;
+    nhx = kind == RSGPU_KIND_RTM ? o->nhx : 1;
+    nhz = kind == RSGPU_KIND_RTM ? o->nhz : 1;
+    {
+        RevolveSchedule probe(c->nt, o->ncheck);
+        ncheck = probe.snaps();
+    }
+    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+    // forward plan: the shots as given, recording switched off after FIRSTURN
+    std::vector<rsgpu_shot> fs(ns), bs(ns);
+    for (int i = 0; i < ns; i++) {
+        fs[i] = s[i].shot;
+        fs[i].rec_out = nullptr;
+        bs[i] = s[i].shot;
+        // adjoint plan: receivers become sources, sources become receivers
+        bs[i].nsrc = s[i].shot.nrec;
+        bs[i].smap = s[i].shot.gmap;
+        bs[i].sshift = s[i].shot.gshift;
+        bs[i].wavelet = s[i].data;          // RTM: the data; FWI: replaced by the residuals
+        bs[i].src_field = RSGPU_PRESSURE;
+        bs[i].nrec = kind == RSGPU_KIND_FWI ? s[i].shot.nsrc : 0;
+        bs[i].gmap = s[i].shot.smap;
+        bs[i].gshift = s[i].shot.sshift;
+        bs[i].rec_field = RSGPU_PRESSURE;
+        bs[i].rec_factor = nullptr;
+        bs[i].rec_out = nullptr;
+    }
+    fw.reset(new Plan());
+    fw->gated_recording = true;
+    fw->shared_stream = stream;
+    ST(fw->create(c, ns, fs.data()));
+    bw.reset(new Plan());
+    bw->reverse_time = true;
+    bw->shared_stream = stream;
+    ST(bw->create(c, ns, bs.data()));
+
+    // device buffer: models, data, outputs, descriptors, checkpoint tables
+    const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t r = off; off = rup(off + std::max<size_t>(bytes, 1), 256); return r; };
+    o_vp.assign(ns, 0); o_rho.assign(ns, 0); o_obs.assign(ns, 0); o_g0.assign(ns, 0); o_g1.assign(ns, 0);
+    nx.resize(ns); nz.resize(ns); nrec.resize(ns); nsrc.resize(ns);
+    for (int i = 0; i < ns; i++) {
+        nx[i] = s[i].shot.nx; nz[i] = s[i].shot.nz; nrec[i] = s[i].shot.nrec; nsrc[i] = s[i].shot.nsrc;
+        nxmax = std::max(nxmax, nx[i]);
+        nzmax = std::max(nzmax, nz[i]);
+        const size_t n2 = (size_t)nx[i] * nz[i];
+        if (kind == RSGPU_KIND_FWI) {
+            o_vp[i] = take(n2 * es);
+            o_rho[i] = take(n2 * es);
+            o_obs[i] = take((size_t)nrec[i] * cfg.nt * es);
+            o_g0[i] = take(n2 * gs);
+            o_g1[i] = take(n2 * gs);
+        } else {
+            o_g0[i] = take(n2 * nhx * nhz * gs);
+        }
+    }
+    o_misfit = take(sizeof(double) * ns);
+    const size_t corr_bytes = prec == PREC_F64 ? sizeof(Corr2D<double>) : sizeof(Corr2D<float>);
+    const size_t res_bytes = prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>);
+    o_corr = take(corr_bytes * ns);
+    o_res = take(res_bytes * ns);
+    // checkpoint blocks: per shot the wavefields (interior of the pitched arrays)
+    // and the C-PML memory strips
+    segs.clear();
+    slot_elems = 0;
+    for (int i = 0; i < ns; i++) {
+        const ShotLayout &L = fw->shots[i];
+        const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
+        auto add = [&](size_t byte_off, int rows, int cols, int pitch) {
+            CkptSeg g;
+            g.src = (char *)fw->arena + byte_off;
+            g.rows = rows; g.cols = cols; g.pitch = pitch;
+            g.dst = (long long)slot_elems;
+            slot_elems += (size_t)rows * cols;
+            slot_elems = rup(slot_elems, 64);   // keep every block 128-byte aligned in 16-bit slots
+            segs.push_back(g);
+        };
+        for (int f = 0; f < nfields(PHYS_A2D); f++) add(L.f[f] + org, L.nzp, L.nxp, L.pitch);
+        for (int p = 0; p < npsi(PHYS_A2D); p++) add(L.psix[p], L.nzp, 2 * cfg.lpml, 2 * cfg.lpml);
+        for (int p = 0; p < npsi(PHYS_A2D); p++) add(L.psiz[p], 2 * cfg.lpml, L.nxp, L.nxp);
+    }
+    o_segs = take(sizeof(CkptSeg) * segs.size());
+    o_scales = take(sizeof(float) * segs.size() * ncheck);
+    o_maxbits = take(sizeof(unsigned) * segs.size());
+    if (cudaMalloc(&dbuf, off) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of %zu bytes failed", off);
+        return RSGPU_ERR_NOMEM;
+    }
+    nslots = ncheck;
+    const size_t ck_bytes = slot_elems * ck_es * (size_t)nslots;
+    if (cudaMalloc(&ckpt, ck_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("checkpoint allocation of %zu bytes (%d slots) failed", ck_bytes, nslots);
+        return RSGPU_ERR_NOMEM;
+    }
+    CU(cudaMemsetAsync(dbuf, 0, off, stream));
+    for (int i = 0; i < ns && kind == RSGPU_KIND_FWI; i++) {
+        const size_t n2 = (size_t)nx[i] * nz[i];
+        CU(cudaMemcpyAsync(D(o_vp[i]), s[i].vp, n2 * es, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(D(o_rho[i]), s[i].rho, n2 * es, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(D(o_obs[i]), s[i].data, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+    }
+    CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
+    std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
+    if (prec == PREC_F64) build_desc<double>(corr, res);
+    else build_desc<float>(corr, res);
+    CU(cudaMemcpyAsync(D(o_corr), corr.data(), corr.size(), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(D(o_res), res.data(), res.size(), cudaMemcpyHostToDevice, stream));
+    CU(cudaStreamSynchronize(stream));
+    return RSGPU_OK;
+}
+
+template <typename T>
+void Adjoint::build_desc(std::vector<unsigned char> &corr, std::vector<unsigned char> &res)
+{
+    for (int i = 0; i < nshots; i++) {
+        const ShotLayout &F = fw->shots[i], &B = bw->shots[i];
+        const size_t org = ((size_t)GUARD * F.pitch + GUARD) * es;
+        char *fa = (char *)fw->arena, *ba = (char *)bw->arena;
+        Corr2D<T> c{};
+        c.wsp = (const T *)(fa + F.f[A2_P] + org);
+        c.wrp = (const T *)(ba + B.f[A2_P] + org);
+        c.wrx = (const T *)(ba + B.f[A2_VX] + org);
+        c.wrz = (const T *)(ba + B.f[A2_VZ] + org);
+        c.rx = (const T *)(fa + F.m[M_RX] + org);
+        c.rz = (const T *)(fa + F.m[M_RZ] + org);
+        c.vp = kind == RSGPU_KIND_FWI ? (const T *)D(o_vp[i]) : nullptr;
+        c.rho = kind == RSGPU_KIND_FWI ? (const T *)D(o_rho[i]) : nullptr;
+        c.g0 = D(o_g0[i]);
+        c.g1 = kind == RSGPU_KIND_FWI ? D(o_g1[i]) : nullptr;
+        c.nx = nx[i]; c.nz = nz[i]; c.pitch = F.pitch; c.lpml = cfg.lpml;
+        std::memcpy(corr.data() + i * sizeof c, &c, sizeof c);
+        Resid2D<T> r{};
+        if (kind == RSGPU_KIND_FWI) {
+            r.mod = (const T *)(fa + F.traces);
+            r.obs = (const T *)D(o_obs[i]);
+            r.res = (T *)(ba + B.wav);
+            // the forward plan's receiver plan marks off-grid receivers with -1
+            r.rec_pt = (const int *)(fa + fw->rec_pt_offsets[i]);
+        }
+        r.nrec = nrec[i];
+        r.nt = cfg.nt;
+        std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+    }
+}
+
+rsgpu_status Adjoint::save(int slot)
+{
+    if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
+    cudaError_t e = launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(),
+                                     (char *)ckpt + (size_t)slot * slot_elems * ck_es,
+                                     (float *)D(o_scales) + (size_t)slot * segs.size(), (unsigned *)D(o_maxbits), stream);
+    if (e != cudaSuccess) { set_error("checkpoint save: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += ck == CK_NATIVE ? 1 : 2;
+    ckpt_bytes += (long long)(slot_elems * ck_es);
+    return RSGPU_OK;
+}
+
+rsgpu_status Adjoint::load(int slot)
+{
+    if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
+    cudaError_t e = launch_ckpt_load(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(),
+                                     (const char *)ckpt + (size_t)slot * slot_elems * ck_es,
+                                     (const float *)D(o_scales) + (size_t)slot * segs.size(), stream);
+    if (e != cudaSuccess) { set_error("checkpoint restore: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += 1;
+    ckpt_bytes += (long long)(slot_elems * ck_es);
+    return RSGPU_OK;
+}
+
+rsgpu_status Adjoint::correlate()
+{
+    cudaError_t e = kind == RSGPU_KIND_FWI
+                        ? launch_corr_fwi_a2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, cfg.dx, cfg.dz, stream)
+                        : launch_corr_rtm_a2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, nhx, nhz, stream);
+    if (e != cudaSuccess) { set_error("correlation launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += 1;
+    return RSGPU_OK;
+}
+
+rsgpu_status Adjoint::run()
+{
+    const int nt = cfg.nt;
+    const long long l0 = fw->launches + bw->launches;
+    launches = 0;
+    fw_steps = bw_steps = ckpt_bytes = 0;
+    ST(fw->reset());
+    ST(bw->reset());
+    for (int i = 0; i < nshots; i++) {
+        const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
+        const size_t n2 = (size_t)nx[i] * nz[i];
+        CU(cudaMemsetAsync(D(o_g0[i]), 0, n2 * (kind == RSGPU_KIND_FWI ? 1 : (size_t)nhx * nhz) * gs, stream));
+        if (kind == RSGPU_KIND_FWI) CU(cudaMemsetAsync(D(o_g1[i]), 0, n2 * gs, stream));
+    }
+    ST(fw->set_recording(true));
+    RevolveSchedule rev(nt, ncheck);
+    for (;;) {
+        const int oldcapo = rev.capo();
+        const int a = rev.next();
+        const int capo = rev.capo();
+        if (a == RSGPU_ADVANCE) {
+            ST(fw->run(oldcapo, capo - oldcapo));
+            fw_steps += capo - oldcapo;
+        } else if (a == RSGPU_TAKESHOT) {
+            ST(save(rev.check()));
+        } else if (a == RSGPU_RESTORE) {
+            ST(load(rev.check()));
+        } else if (a == RSGPU_FIRSTURN) {
+            // the last forward step, then the first adjoint time level (nt-1)
+            ST(fw->run(capo, 1));
+            fw_steps += 1;
+            ST(fw->set_recording(false));
+            if (kind == RSGPU_KIND_FWI) {
+                cudaError_t e = launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+                launches += 1;
+            }
+            ST(bw->inject_record_only(nt - 1 - capo));
+            ST(correlate());
+        } else if (a == RSGPU_YOUTURN) {
+            ST(bw->run(nt - 1 - capo, 1));
+            bw_steps += 1;
+            ST(correlate());
+        } else if (a == RSGPU_TERMINATE) {
+            break;
+        } else {
+            set_error("revolve schedule error (info %d)", rev.info());
+            return RSGPU_ERR_REVOLVE;
+        }
+    }
+    launches += fw->launches + bw->launches - l0;
+    CU(cudaStreamSynchronize(stream));
+    ST(fw->check_device_error());
+    ST(bw->check_device_error());
+    ran = true;
+    return RSGPU_OK;
+}
+
+template <typename T, typename G>
+static void add_into(void *host, const std::vector<unsigned char> &dev, size_t n)
+{
+    T *o = (T *)host;
+    const G *d = (const G *)dev.data();
+    for (size_t k = 0; k < n; k++) o[k] = (T)((G)o[k] + d[k]);
+}
+
+rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
+{
+    if (!ran) { set_error("no run to read"); return RSGPU_ERR_STATE; }
+    if (ns != nshots || !s) { set_error("read expects the %d shots of the batch", nshots); return RSGPU_ERR_ARG; }
+    const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
+    std::vector<unsigned char> tmp;
+    auto fetch = [&](size_t o, size_t bytes) -> rsgpu_status {
+        tmp.resize(bytes);
+        CU(cudaMemcpyAsync(tmp.data(), D(o), bytes, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        return RSGPU_OK;
+    };
+    // accumulate a device array of accumulator type into a host array of the element type
+    auto accumulate = [&](void *host, size_t n) {
+        if (es == 8) add_into<double, double>(host, tmp, n);
+        else if (gs == 8) add_into<float, double>(host, tmp, n);
+        else add_into<float, float>(host, tmp, n);
+    };
+    std::vector<double> mis(nshots, 0.0);
+    if (kind == RSGPU_KIND_FWI) {
+        CU(cudaMemcpyAsync(mis.data(), D(o_misfit), sizeof(double) * nshots, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+    }
+    for (int i = 0; i < nshots; i++) {
+        const size_t n2 = (size_t)nx[i] * nz[i];
+        if (kind == RSGPU_KIND_RTM) {
+            if (s[i].image) { ST(fetch(o_g0[i], n2 * nhx * nhz * gs)); accumulate(s[i].image, n2 * nhx * nhz); }
+            continue;
+        }
+        if (s[i].vpgrad) { ST(fetch(o_g0[i], n2 * gs)); accumulate(s[i].vpgrad, n2); }
+        if (s[i].rhograd) { ST(fetch(o_g1[i], n2 * gs)); accumulate(s[i].rhograd, n2); }
+        if (s[i].shot.rec_out) ST(fw->read_traces(i, s[i].shot.rec_out));
+        if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
+        if (s[i].datares) {
+            const size_t n = (size_t)nrec[i] * cfg.nt;
+            tmp.resize(n * es);
+            CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wav, n * es, cudaMemcpyDeviceToHost, stream));
+            CU(cudaStreamSynchronize(stream));
+            if (es == 8) add_into<double, double>(s[i].datares, tmp, n);
+            else add_into<float, float>(s[i].datares, tmp, n);
+        }
+        if (s[i].misfit) {
+            // the reference keeps the misfit in T
+            if (acc == ACC_REF && es == 4) *s[i].misfit = (double)(float)((float)*s[i].misfit + (float)mis[i]);
+            else *s[i].misfit += mis[i];
+        }
+    }
+    return RSGPU_OK;
+}
+
+}  // namespace rsgpu
+
+using namespace rsgpu;
+
+struct rsgpu_adjoint { std::unique_ptr<Adjoint> a; };
+
+extern "C" {
+
+rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int kind, int nshots,
+                                  const rsgpu_adjoint_shot *shots, rsgpu_adjoint **adj)
+{
+    if (!adj) { set_error("handle pointer is null"); return RSGPU_ERR_ARG; }
+    *adj = nullptr;
+    std::unique_ptr<rsgpu_adjoint> h(new rsgpu_adjoint);
+    h->a.reset(new Adjoint());
+    rsgpu_status st = h->a->create(cfg, opts, kind, nshots, shots);
+    if (st != RSGPU_OK) return st;
+    *adj = h.release();
+    return RSGPU_OK;
+}
+
+rsgpu_status rsgpu_adjoint_run(rsgpu_adjoint *adj)
+{
+    if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
+    return adj->a->run();
+}
+
+rsgpu_status rsgpu_adjoint_read(rsgpu_adjoint *adj, int nshots, const rsgpu_adjoint_shot *shots)
+{
+    if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
+    return adj->a->read(nshots, shots);
+}
+
+rsgpu_status rsgpu_adjoint_stats(rsgpu_adjoint *adj, long long *fw_steps, long long *bw_steps, long long *ckpt_bytes,
+                                 long long *launches)
+{
+    if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
+    if (fw_steps) *fw_steps = adj->a->fw_steps;
+    if (bw_steps) *bw_steps = adj->a->bw_steps;
+    if (ckpt_bytes) *ckpt_bytes = adj->a->ckpt_bytes;
+    if (launches) *launches = adj->a->launches;
+    return RSGPU_OK;
+}
+
+void *rsgpu_adjoint_stream(rsgpu_adjoint *adj) { return adj ? (void *)adj->a->stream : nullptr; }
+void rsgpu_adjoint_destroy(rsgpu_adjoint *adj) { delete adj; }
+
+static rsgpu_status one_call(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int kind, int nshots,
+                             const rsgpu_adjoint_shot *shots)
+{
+    rsgpu_adjoint *h = nullptr;
+    rsgpu_status st = rsgpu_adjoint_create(cfg, opts, kind, nshots, shots, &h);
+    if (st == RSGPU_OK) st = rsgpu_adjoint_run(h);
+    if (st == RSGPU_OK) st = rsgpu_adjoint_read(h, nshots, shots);
+    rsgpu_adjoint_destroy(h);
+    return st;
+}
+
+rsgpu_status rsgpu_fwi_gradient(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
+                                const rsgpu_adjoint_shot *shots)
+{
+    return one_call(cfg, opts, RSGPU_KIND_FWI, nshots, shots);
+}
+
+rsgpu_status rsgpu_rtm_image(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
+                             const rsgpu_adjoint_shot *shots)
+{
+    return one_call(cfg, opts, RSGPU_KIND_RTM, nshots, shots);
+}
+
+}  // extern "C"

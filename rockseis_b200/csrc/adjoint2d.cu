@@ -1,0 +1,344 @@
+// Kernels of the 2D FWI gradient and RTM image drivers:
+//   * the gradient correlation of FwiAcoustic2D::crossCorr (lib/fwi.cpp:511-571),
+//   * the (extended) image correlation of RtmAcoustic2D::crossCorr (lib/rtm.cpp:191-219),
+//   * residuals and misfit of FwiAcoustic2D::computeResiduals / computeMisfit
+//     with the DIFFERENCE misfit (lib/fwi.cpp:597-611, 798-806),
+//   * checkpoint slot save/restore (the in-core checkpoints of Revolve,
+//     lib/revolve.cpp:648-818), optionally as FP16/BF16 with a power-of-two scale
+//     per block.
+// All of them are memory-bound elementwise passes; one launch covers every shot
+// of the batch (blockIdx.z or blockIdx.y selects the shot / block).
+//
+// Exact mode reproduces the reference's float expression evaluation: C's usual
+// arithmetic conversions evaluate `0.5 * a * b * (c - d) / dx` in double when
+// a..d are float, and `-2.0 / vp` in double rounded to float; every such operation
+// is written out with explicitly rounded intrinsics.
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "rsgpu_adjoint.h"
+#include "rsgpu_kernels.h"
+
+namespace rsgpu {
+namespace {
+
+template <typename T> struct X;   // explicitly rounded operations of the element type
+template <> struct X<float> {
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    static __device__ __forceinline__ float rnd(double a) { return __double2float_rn(a); }
+};
+template <> struct X<double> {
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    static __device__ __forceinline__ double rnd(double a) { return a; }
+};
+
+// ---------------------------------------------------------------- FWI gradient correlation
+// vpgrad -= (-2/vp) * Pfw * (dx- Vx_adj + dz- Vz_adj)
+// rhograd -= (-1/rho) * Pfw * (same)
+// rhograd += 1/2 [ Vx_adj Rx dx+ Pfw ] averaged over the two staggered x-faces (and z)
+// on the interior 1..n-2 of the unpadded window.  G is the accumulator type.
+template <typename T, bool EXACT, typename G>
+__global__ void __launch_bounds__(256) corr_fwi_a2d(const Corr2D<T> *desc, T dx, T dz)
+{
+    const Corr2D<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix < 1 || iz < 1 || ix >= c.nx - 1 || iz >= c.nz - 1) return;
+    const long q = (long)(iz + c.lpml) * c.pitch + ix + c.lpml;
+    const long u = (long)iz * c.nx + ix;
+    const int P = c.pitch;
+    const T ws = c.wsp[q], wsl = c.wsp[q - 1], wsr = c.wsp[q + 1], wsu = c.wsp[q - P], wsd = c.wsp[q + P];
+    const T wx0 = c.wrx[q], wx1 = c.wrx[q - 1], wz0 = c.wrz[q], wz1 = c.wrz[q - P];
+    const T rx0 = c.rx[q], rx1 = c.rx[q - 1], rz0 = c.rz[q], rz1 = c.rz[q - P];
+    const T vp = c.vp[u], rho = c.rho[u];
+    G *vg = (G *)c.g0 + u;
+    G *rg = (G *)c.g1 + u;
+    T a, b, uder;
+    if (EXACT) {
+        using O = X<T>;
+        const T vpscale = O::rnd(__ddiv_rn(-2.0, (double)vp));
+        const T rhoscale1 = O::rnd(__ddiv_rn(-1.0, (double)rho));
+        const T mrxx = O::div(O::sub(wx0, wx1), dx);
+        const T mrzz = O::div(O::sub(wz0, wz1), dz);
+        const T s = O::add(mrxx, mrzz);
+        a = O::mul(O::mul(vpscale, ws), s);
+        b = O::mul(O::mul(rhoscale1, ws), s);
+        const double DX = (double)dx, DZ = (double)dz;
+        T ux = O::rnd(__ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)wx0), (double)rx0), (double)O::sub(wsr, ws)), DX));
+        ux = O::rnd(__dadd_rn((double)ux,
+                              __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)wx1), (double)rx1), (double)O::sub(ws, wsl)), DX)));
+        T uz = O::rnd(__ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)wz0), (double)rz0), (double)O::sub(wsd, ws)), DZ));
+        uz = O::rnd(__dadd_rn((double)uz,
+                              __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)wz1), (double)rz1), (double)O::sub(ws, wsu)), DZ)));
+        uder = O::add(ux, uz);
+    } else {
+        const T rdx = T(1) / dx, rdz = T(1) / dz;
+        const T s = (wx0 - wx1) * rdx + (wz0 - wz1) * rdz;
+        a = (T(-2) / vp) * ws * s;
+        b = (T(-1) / rho) * ws * s;
+        uder = T(0.5) * ((wx0 * rx0 * (wsr - ws) + wx1 * rx1 * (ws - wsl)) * rdx +
+                         (wz0 * rz0 * (wsd - ws) + wz1 * rz1 * (ws - wsu)) * rdz);
+    }
+    if (sizeof(G) == sizeof(T)) {
+        // accumulate in the element type, in the reference's order
+        using O = X<T>;
+        *(T *)vg = EXACT ? O::sub(*(T *)vg, a) : *(T *)vg - a;
+        const T r1 = EXACT ? O::sub(*(T *)rg, b) : *(T *)rg - b;
+        *(T *)rg = EXACT ? O::add(r1, uder) : r1 + uder;
+    } else {
+        *vg = __dsub_rn((double)*vg, (double)a);
+        *rg = __dadd_rn(__dsub_rn((double)*rg, (double)b), (double)uder);
+    }
+}
+
+// ---------------------------------------------------------------- RTM image correlation
+// image[ihz][ihx][iz][ix] += Pfw(ix-hx, iz-hz) * Padj(ix+hx, iz+hz) for lags
+// hx = ihx - (nhx-1)/2, hz likewise, where both points lie in the window.
+template <typename T, bool EXACT, typename G>
+__global__ void __launch_bounds__(256) corr_rtm_a2d(const Corr2D<T> *desc, int nhx, int nhz)
+{
+    const Corr2D<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= c.nx || iz >= c.nz) return;
+    const int L = c.lpml, P = c.pitch;
+    for (int ihx = 0; ihx < nhx; ihx++) {
+        const int hx = -(nhx - 1) / 2 + ihx;
+        if (ix - hx < 0 || ix - hx >= c.nx || ix + hx < 0 || ix + hx >= c.nx) continue;
+        for (int ihz = 0; ihz < nhz; ihz++) {
+            const int hz = -(nhz - 1) / 2 + ihz;
+            if (iz - hz < 0 || iz - hz >= c.nz || iz + hz < 0 || iz + hz >= c.nz) continue;
+            const T ws = c.wsp[(long)(iz - hz + L) * P + (ix - hx + L)];
+            const T wr = c.wrp[(long)(iz + hz + L) * P + (ix + hx + L)];
+            G *img = (G *)c.g0 + (((long)ihz * nhx + ihx) * c.nz + iz) * c.nx + ix;
+            if (sizeof(G) == sizeof(T)) {
+                using O = X<T>;
+                *(T *)img = EXACT ? O::add(*(T *)img, O::mul(ws, wr)) : *(T *)img + ws * wr;
+            } else {
+                *img = __dadd_rn((double)*img, __dmul_rn((double)ws, (double)wr));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- residuals and misfit
+template <typename T, int ACC>
+__global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, double *misfit)
+{
+    const Resid2D<T> d = desc[blockIdx.x];
+    const long n = (long)d.nrec * d.nt;
+    for (long k = threadIdx.x; k < n; k += blockDim.x) d.res[k] = X<T>::sub(d.mod[k], d.obs[k]);
+    if (ACC == ACC_REF) {
+        __syncthreads();
+        if (threadIdx.x != 0) return;
+        // mis += 0.5*r*r with a T-typed accumulator, traces then samples
+        T mis = 0;
+        for (int tr = 0; tr < d.nrec; tr++) {
+            if (d.rec_pt[tr] < 0) continue;
+            const T *r = d.res + (long)tr * d.nt;
+            for (int it = 0; it < d.nt; it++) {
+                const double rr = (double)r[it];
+                mis = X<T>::rnd(__dadd_rn((double)mis, __dmul_rn(__dmul_rn(0.5, rr), rr)));
+            }
+        }
+        misfit[blockIdx.x] = (double)mis;
+    } else {
+        double acc = 0.0;
+        for (long k = threadIdx.x; k < n; k += blockDim.x) {
+            if (d.rec_pt[k / d.nt] < 0) continue;
+            const double r = (double)X<T>::sub(d.mod[k], d.obs[k]);
+            acc = fma(0.5 * r, r, acc);
+        }
+        __shared__ double red[256];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) misfit[blockIdx.x] = red[0];
+    }
+}
+
+// ---------------------------------------------------------------- checkpoints
+template <typename S> struct Store;
+template <> struct Store<__half> {
+    static __device__ __forceinline__ __half to(float x) { return __float2half_rn(x); }
+    static __device__ __forceinline__ float from(__half h) { return __half2float(h); }
+};
+template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ __nv_bfloat16 to(float x) { return __float2bfloat16_rn(x); }
+    static __device__ __forceinline__ float from(__nv_bfloat16 h) { return __bfloat162float(h); }
+};
+
+// Power-of-two scale that maps the block's largest magnitude below 2^15 (exact
+// scaling; FP16's largest finite value is 65504).
+__device__ __forceinline__ float pow2_scale(unsigned maxbits)
+{
+    const float m = __uint_as_float(maxbits);
+    if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
+    int e;
+    frexpf(m, &e);          // m < 2^e
+    return ldexpf(1.0f, e - 15);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ckpt_copy_out(const CkptSeg *segs, T *slot)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    const T *src = (const T *)s.src;
+    T *dst = slot + s.dst;
+    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.cols + c] = src[(long)r * s.pitch + c];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ckpt_copy_in(const CkptSeg *segs, const T *slot)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    T *dst = (T *)s.src;
+    const T *src = slot + s.dst;
+    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.pitch + c] = src[(long)r * s.cols + c];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ckpt_maxabs(const CkptSeg *segs, unsigned *maxbits)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    const T *src = (const T *)s.src;
+    float m = 0.0f;
+    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) m = fmaxf(m, fabsf((float)src[(long)r * s.pitch + c]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(&maxbits[blockIdx.y], __float_as_uint(m));
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) ckpt_pack(const CkptSeg *segs, S *slot, const unsigned *maxbits, float *scales)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    const float scale = pow2_scale(maxbits[blockIdx.y]);
+    const float inv = 1.0f / scale;            // exact: a power of two
+    if (blockIdx.x == 0 && threadIdx.x == 0) scales[blockIdx.y] = scale;
+    const T *src = (const T *)s.src;
+    S *dst = slot + s.dst;
+    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
+            dst[(long)r * s.cols + c] = Store<S>::to((float)src[(long)r * s.pitch + c] * inv);
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) ckpt_unpack(const CkptSeg *segs, const S *slot, const float *scales)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    const float scale = scales[blockIdx.y];
+    T *dst = (T *)s.src;
+    const S *src = slot + s.dst;
+    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
+            dst[(long)r * s.pitch + c] = (T)(Store<S>::from(src[(long)r * s.cols + c]) * scale);
+}
+
+constexpr int CK_BLOCKS = 64;   // row-blocks per segment (grid.x)
+
+template <typename T>
+cudaError_t ckpt_save_t(int ck, const CkptSeg *segs, int nseg, void *slot, float *scales, unsigned *maxbits,
+                        cudaStream_t st)
+{
+    const dim3 grid(CK_BLOCKS, nseg);
+    if (ck == CK_NATIVE) {
+        ckpt_copy_out<T><<<grid, 256, 0, st>>>(segs, (T *)slot);
+        return cudaGetLastError();
+    }
+    cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * nseg, st);
+    if (e != cudaSuccess) return e;
+    ckpt_maxabs<T><<<grid, 256, 0, st>>>(segs, maxbits);
+    if (ck == CK_F16) ckpt_pack<T, __half><<<grid, 256, 0, st>>>(segs, (__half *)slot, maxbits, scales);
+    else ckpt_pack<T, __nv_bfloat16><<<grid, 256, 0, st>>>(segs, (__nv_bfloat16 *)slot, maxbits, scales);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t ckpt_load_t(int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales, cudaStream_t st)
+{
+    const dim3 grid(CK_BLOCKS, nseg);
+    if (ck == CK_NATIVE) ckpt_copy_in<T><<<grid, 256, 0, st>>>(segs, (const T *)slot);
+    else if (ck == CK_F16) ckpt_unpack<T, __half><<<grid, 256, 0, st>>>(segs, (const __half *)slot, scales);
+    else ckpt_unpack<T, __nv_bfloat16><<<grid, 256, 0, st>>>(segs, (const __nv_bfloat16 *)slot, scales);
+    return cudaGetLastError();
+}
+
+template <typename T, bool EXACT>
+cudaError_t corr_fwi_t(int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx, double dz,
+                       cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nzmax + 7) / 8, nshots);
+    if (acc == ACC_F64)
+        corr_fwi_a2d<T, EXACT, double><<<grid, block, 0, st>>>((const Corr2D<T> *)desc, (T)dx, (T)dz);
+    else
+        corr_fwi_a2d<T, EXACT, T><<<grid, block, 0, st>>>((const Corr2D<T> *)desc, (T)dx, (T)dz);
+    return cudaGetLastError();
+}
+
+template <typename T, bool EXACT>
+cudaError_t corr_rtm_t(int acc, const void *desc, int nshots, int nxmax, int nzmax, int nhx, int nhz, cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nzmax + 7) / 8, nshots);
+    if (acc == ACC_F64) corr_rtm_a2d<T, EXACT, double><<<grid, block, 0, st>>>((const Corr2D<T> *)desc, nhx, nhz);
+    else corr_rtm_a2d<T, EXACT, T><<<grid, block, 0, st>>>((const Corr2D<T> *)desc, nhx, nhz);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_corr_fwi_a2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
+                                double dz, cudaStream_t st)
+{
+    if (prec == PREC_F64) return corr_fwi_t<double, true>(acc, desc, nshots, nxmax, nzmax, dx, dz, st);
+    if (prec == PREC_F32_EXACT) return corr_fwi_t<float, true>(acc, desc, nshots, nxmax, nzmax, dx, dz, st);
+    return corr_fwi_t<float, false>(acc, desc, nshots, nxmax, nzmax, dx, dz, st);
+}
+
+cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, int nhx,
+                                int nhz, cudaStream_t st)
+{
+    if (prec == PREC_F64) return corr_rtm_t<double, true>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
+    if (prec == PREC_F32_EXACT) return corr_rtm_t<float, true>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
+    return corr_rtm_t<float, false>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
+}
+
+cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st)
+{
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) residual_misfit<double, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2D<double> *)desc, misfit);
+        else residual_misfit<double, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2D<double> *)desc, misfit);
+    } else {
+        if (acc == ACC_F64) residual_misfit<float, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
+        else residual_misfit<float, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,
+                             unsigned *maxbits, cudaStream_t st)
+{
+    return prec == PREC_F64 ? ckpt_save_t<double>(ck, segs, nseg, slot, scales, maxbits, st)
+                            : ckpt_save_t<float>(ck, segs, nseg, slot, scales, maxbits, st);
+}
+
+cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales,
+                             cudaStream_t st)
+{
+    return prec == PREC_F64 ? ckpt_load_t<double>(ck, segs, nseg, slot, scales, st)
+                            : ckpt_load_t<float>(ck, segs, nseg, slot, scales, st);
+}
+
+}  // namespace rsgpu

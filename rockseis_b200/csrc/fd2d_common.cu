@@ -36,6 +36,12 @@ cudaError_t launch_advance(int *it_dev, int by, cudaStream_t st)
     return cudaGetLastError();
 }
 
+cudaError_t launch_set_counter(int *it_dev, int value, cudaStream_t st)
+{
+    set_counter<<<1, 32, 0, st>>>(it_dev, value);
+    return cudaGetLastError();
+}
+
 size_t coefset_bytes(int prec) { return prec == PREC_F64 ? sizeof(CoefSet<double>) : sizeof(CoefSet<float>); }
 int coef_row_stride() { return CROW; }
 

@@ -804,7 +804,8 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
     using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
     const Shot2D<T> &sh = shots[blockIdx.x];
     const InjRec<T> &pl = plans[blockIdx.x];
-    const int it = it_base + (it_dev ? *it_dev : 0);
+    const int it_step = it_base + (it_dev ? *it_dev : 0);
+    const int it = pl.rev ? pl.nt - 1 - it_step : it_step;
     if (pl.kind_inj != INJ_NONE) {
         for (int q = threadIdx.x; q < pl.ninj; q += blockDim.x) {
             const int p = pl.inj_pt[q];
@@ -837,7 +838,7 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
             }
         }
     }
-    if (pl.kind_rec == REC_NONE) return;
+    if (pl.kind_rec == REC_NONE || (pl.rec_gate && *pl.rec_gate == 0)) return;
     __syncthreads();
     for (int tr = threadIdx.x; tr < pl.nrec; tr += blockDim.x) {
         const int p = pl.rec_pt[tr];
@@ -879,6 +880,11 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
 static __global__ void advance_counter(int *it_dev, int by)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) *it_dev += by;
+}
+
+static __global__ void set_counter(int *it_dev, int value)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *it_dev = value;
 }
 
 // ---------------------------------------------------------------- launchers

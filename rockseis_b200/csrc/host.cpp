@@ -120,9 +120,6 @@ static bool encode_field_map(CUtensorMap *m, void *base, int prec, int pitch, in
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
-static int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 9; }
-static int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
-static int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 
 // Shared with other host translation units (no-allocation entry point).
 void coef_table_host(int prec, double dx, double dz, std::vector<unsigned char> &out)
@@ -144,7 +141,7 @@ Plan::~Plan()
             if (e) cudaEventDestroy(e);
     if (arena) cudaFree(arena);
     if (d_meta) cudaFree(d_meta);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
 rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s)
@@ -197,7 +194,8 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     phys = c->physics;
     nshots = ns;
     const int es = esize(prec);
-    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (shared_stream) stream = shared_stream;
+    else CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
     tilecfg = (c->tile >= 0 && c->tile < tile_count_2d()) ? c->tile : default_tile();
     // the FP64 oracle propagator is built for two tile shapes only
@@ -220,6 +218,7 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         for (int k = 0; k < nfields(phys); k++) L.f[k] = take(fbytes);
         for (int k = 0; k < npsi(phys); k++) L.psix[k] = take((size_t)L.nzp * 2 * lp * es);
         for (int k = 0; k < npsi(phys); k++) L.psiz[k] = take((size_t)2 * lp * L.nxp * es);
+        L.psi_end = off;
         L.nrec = s[i].nrec;
         L.nsrc = s[i].nsrc;
         L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
@@ -300,6 +299,7 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         o_rec_fac[i] = take(std::max<size_t>(1, rec_fac[i].size()) * es);
     }
     const size_t o_pml = take((size_t)12 * lp * es);
+    rec_pt_offsets = o_rec_pt;
     arena_bytes = off;
     if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -380,7 +380,11 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     const size_t m_it = rup(m_maps + (size_t)ns * NMAP2D * sizeof(CUtensorMap), 256);
     const size_t m_end = m_it + 256;
     CU(cudaMalloc(&d_meta, m_end));
+    d_it = (int *)((char *)d_meta + m_it);
+    d_err = d_it + 1;
+    d_gate = d_it + 2;
     std::vector<unsigned char> meta(m_end, 0);
+    reinterpret_cast<int *>(meta.data() + m_it)[2] = 1;   // recording on
     for (int i = 0; i < ns; i++) {
         const ShotLayout &L = shots[i];
         const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
@@ -409,8 +413,6 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
     d_maps = (char *)d_meta + m_maps;
-    d_it = (int *)((char *)d_meta + m_it);
-    d_err = d_it + 1;
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -451,6 +453,8 @@ void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L,
     r.rec_factor = (const T *)(A + o_rf);
     r.rec_out = (T *)(A + L.traces);
     r.nt = cfg.nt;
+    r.rev = reverse_time ? 1 : 0;
+    r.rec_gate = gated_recording ? d_gate : nullptr;
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -530,8 +534,9 @@ rsgpu_status Plan::run(int it0, int nsteps)
             cudaGraphDestroy(g);
             launches -= 3L * G;   // captured launches are counted at replay
         }
-        CU(cudaMemcpyAsync(d_it, &it0, sizeof(int), cudaMemcpyHostToDevice, stream));
-        CU(cudaStreamSynchronize(stream));
+        cudaError_t e = launch_set_counter(d_it, it0, stream);
+        if (e != cudaSuccess) { set_error("launch_set_counter: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+        launches += 1;
         while (nsteps - done >= G) {
             CU(cudaGraphLaunch(graph_exec, stream));
             launches += 3L * G;
@@ -542,6 +547,22 @@ rsgpu_status Plan::run(int it0, int nsteps)
         rsgpu_status st = launch_step(it0 + done, nullptr, false);
         if (st != RSGPU_OK) return st;
     }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::inject_record_only(int it)
+{
+    if (it < 0 || it >= cfg.nt) { set_error("step %d outside [0,%d)", it, cfg.nt); return RSGPU_ERR_ARG; }
+    cudaError_t e = launch_injrec_2d(prec, d_shots, d_injrec, nshots, cfg.dt, it, nullptr, stream);
+    if (e != cudaSuccess) { set_error("kernel launch failed: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += 1;
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::set_recording(bool on)
+{
+    if (!gated_recording) { set_error("plan was created without gated recording"); return RSGPU_ERR_STATE; }
+    CU(cudaMemsetAsync(d_gate, on ? 1 : 0, sizeof(int), stream));
     return RSGPU_OK;
 }
 

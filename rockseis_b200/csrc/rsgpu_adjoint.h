@@ -1,0 +1,57 @@
+// Kernels of the FWI-gradient and RTM-image drivers (host runtime internals, not ABI).
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace rsgpu {
+
+// Correlation inputs of one shot.  Field and parameter pointers are the origins
+// (element (0,0) of the padded grid) of the pitched plan arrays; vp, rho and the
+// outputs are dense [nz][nx] arrays of the unpadded window.
+template <typename T>
+struct Corr2D {
+    const T *wsp;               // forward pressure
+    const T *wrp, *wrx, *wrz;   // adjoint pressure, vx, vz
+    const T *rx, *rz;           // staggered inverse densities of the forward plan
+    const T *vp, *rho;          // unpadded models (FWI gradient scaling)
+    void *g0, *g1;              // FWI: vpgrad, rhograd; RTM: g0 = image [nhz][nhx][nz][nx]
+    int nx, nz, pitch, lpml;
+};
+
+// Residual and misfit of one shot (DIFFERENCE misfit).
+template <typename T>
+struct Resid2D {
+    const T *mod;               // modelled data [nrec][nt] (forward plan traces)
+    const T *obs;               // observed data [nrec][nt]
+    T *res;                     // residual [nrec][nt] (adjoint plan source traces)
+    const int *rec_pt;          // -1 for receivers off the grid (excluded from the misfit)
+    int nrec, nt;
+};
+
+// One contiguous 2D block of state copied into / out of a checkpoint slot.
+struct CkptSeg {
+    void *src;                  // first element
+    int rows, cols, pitch;      // pitch in elements
+    long long dst;              // element offset of the block inside a slot
+};
+
+enum { ACC_REF = 0, ACC_F64 = 1 };
+enum { CK_NATIVE = 0, CK_F16 = 1, CK_BF16 = 2 };
+
+// Gradient/image correlation of one adjoint time step over all shots.
+cudaError_t launch_corr_fwi_a2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
+                                double dz, cudaStream_t st);
+cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, int nhx,
+                                int nhz, cudaStream_t st);
+// Residuals (mod - obs) and per-shot misfit (sum of r^2/2 over on-grid traces):
+// ACC_REF in the element type, sequentially in the reference's order; ACC_F64 in
+// double by a fixed-order tree reduction.
+cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
+// Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
+// for the 16-bit formats (written by save, read by load).
+cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,
+                             unsigned *maxbits, cudaStream_t st);
+cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales,
+                             cudaStream_t st);
+
+}  // namespace rsgpu

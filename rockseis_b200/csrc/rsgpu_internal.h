@@ -82,6 +82,9 @@ struct InjRec {
     const T *rec_factor;    // [nrec] reciprocity divisor for elastic pressure (or null)
     T *rec_out;             // [nrec * nt] trace-major output (accumulated with +=)
     int nt;
+    int rev;                // 1: step `it` reads wav[nt-1-it] and writes rec_out[nt-1-it]
+                            //    (adjoint propagation run forward in reversed time)
+    const int *rec_gate;    // if non-null, recording happens only while *rec_gate != 0
 };
 enum InjKind {
     INJ_NONE = 0,

@@ -29,6 +29,7 @@ Launch2DFn launch_2d_table(const char *variant, int cfg);
 cudaError_t launch_injrec_2d(int prec, const void *shots, const void *plans, int nshots, double dt, int it_base,
                              const int *it_dev, cudaStream_t st);
 cudaError_t launch_advance(int *it_dev, int by, cudaStream_t st);
+cudaError_t launch_set_counter(int *it_dev, int value, cudaStream_t st);
 size_t coefset_bytes(int prec);
 int coef_row_stride();
 

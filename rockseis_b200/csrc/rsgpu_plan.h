@@ -9,6 +9,9 @@
 namespace rsgpu {
 
 int esize(int prec);
+inline int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 9; }
+inline int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
+inline int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 
 // Byte offsets of one shot's arrays inside the plan arena.
 struct ShotLayout {
@@ -16,6 +19,7 @@ struct ShotLayout {
     int nrec = 0, nsrc = 0;
     size_t f[9] = {}, m[8] = {}, psix[4] = {}, psiz[4] = {};
     size_t traces = 0, wav = 0;
+    size_t psi_end = 0;       // end of the wavefields + C-PML memory (a checkpoint's extent)
     size_t field_begin = 0;   // first byte of the zero-initialised state block
     size_t state_end = 0;     // one past its last byte (wavefields, C-PML memory, traces)
 };
@@ -32,10 +36,20 @@ public:
     rsgpu_status enable_timing();
     rsgpu_status kernel_times(float *ms_vel, float *ms_str);
     rsgpu_status check_device_error();
+    // adjoint drivers: injection/recording of step `it` without propagation, and
+    // switching the trace recording on/off in stream order
+    rsgpu_status inject_record_only(int it);
+    rsgpu_status set_recording(bool on);
+
+    // options read by create()
+    bool reverse_time = false;           // wavelet/trace index nt-1-it at step it
+    bool gated_recording = false;        // recording obeys set_recording()
+    cudaStream_t shared_stream = nullptr;  // run on this caller-owned stream
 
     rsgpu_config cfg{};
     int prec = 0, phys = 0, nshots = 0, tilecfg = 0, ntiles = 0;
     std::vector<ShotLayout> shots;
+    std::vector<size_t> rec_pt_offsets;   // per shot: arena offset of the receiver points (-1 = off grid)
     void *arena = nullptr;
     size_t arena_bytes = 0, state_end = 0;
     void *d_meta = nullptr;
@@ -43,6 +57,7 @@ public:
     void *d_maps = nullptr;    // [nshots][NMAP2D] CUtensorMap
     int *d_it = nullptr;       // step counter read by graph-replayed kernels
     int *d_err = nullptr;      // device error word (bounded waits)
+    int *d_gate = nullptr;     // recording switch (gated_recording)
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool use_graph = true;

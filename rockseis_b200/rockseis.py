@@ -357,3 +357,194 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- FWI gradient / RTM image
+class Image2D:
+    """Image container (Image2D<T>, include/image.h): imagedata[ihz, ihx, iz, ix]."""
+
+    def __init__(self, imagefile, model: _Model, nhx=1, nhz=1, precision=None):
+        self.imagefile = imagefile
+        self.nx, self.nz, self.nhx, self.nhz = model.nx, model.nz, int(nhx), int(nhz)
+        self.dx, self.dz, self.ox, self.oz = model.dx, model.dz, model.ox, model.oz
+        self.dtype = abi.real_dtype(model.precision if precision is None else precision)
+        self.imagedata = None
+
+    def allocateImage(self):
+        if self.imagedata is None:
+            self.imagedata = np.zeros((self.nhz, self.nhx, self.nz, self.nx), self.dtype)
+
+    def getImagedata(self):
+        self.allocateImage()
+        return self.imagedata
+
+    def getNhx(self): return self.nhx
+    def getNhz(self): return self.nhz
+
+
+class _Adjoint:
+    """Settings shared by FwiAcoustic2D and RtmAcoustic2D (the reference's Fwi / Rtm bases)."""
+    cls = "FwiAcoustic2D"
+
+    def __init__(self, model, source, dataP, order=4, snapinc=1, precision=None):
+        self.model, self.source, self.dataP = model, source, dataP
+        self.order = int(order) if 1 < int(order) < 9 else 4
+        self.snapinc = snapinc if snapinc > 0 else 1
+        self.precision = precision if precision is not None else model.precision
+        self.ncheck = 0
+        self.ckpt_precision = abi.CKPT_NATIVE
+        self.accum = abi.ACCUM_REFERENCE
+        self.misfit_type = abi.MISFIT_DIFFERENCE
+        self.tile = -1
+
+    def setModel(self, m): self.model = m
+    def setSource(self, s): self.source = s
+    def setDataP(self, d): self.dataP = d
+    def setNcheck(self, n): self.ncheck = int(n)
+    def setMisfit_type(self, t): self.misfit_type = int(t)
+    def setCheckpointPrecision(self, p): self.ckpt_precision = int(p)   # no reference counterpart
+    def setAccumulation(self, a): self.accum = int(a)                  # no reference counterpart
+
+    def checkStability(self):
+        check_stability(self.model, self.source.dt, self.cls)
+        return True
+
+    def _opts(self, nhx=1, nhz=1) -> abi.AdjointOpts:
+        o = abi.AdjointOpts()
+        o.ncheck, o.ckpt_precision, o.accum, o.misfit, o.nhx, o.nhz = (self.ncheck, self.ckpt_precision, self.accum,
+                                                                        self.misfit_type, nhx, nhz)
+        return o
+
+    def _adjoint_shot(self, keep: list) -> abi.AdjointShot:
+        a = abi.AdjointShot()
+        a.shot = make_shot(self.model, self.source, self.dataP, keep)
+        a.shot.rec_out = None
+        data = np.ascontiguousarray(self.dataP.data)
+        keep.append(data)
+        a.data = ptr(data)
+        return a
+
+
+class FwiAcoustic2D(_Adjoint):
+    """FwiAcoustic2D<T> (include/fwi.h:128-182): gradient of the DIFFERENCE misfit
+    with respect to vp and rho (and the source wavelet), run on the GPU."""
+    cls = "FwiAcoustic2D"
+
+    def __init__(self, model=None, source=None, dataP=None, order=4, snapinc=1, precision=None):
+        super().__init__(model, source, dataP, order, snapinc, precision)
+        self.vpgrad = self.rhograd = self.wavgrad = self.datamodP = self.dataresP = None
+        self.misfit = 0.0
+
+    def setVpgrad(self, img): self.vpgrad = img
+    def setRhograd(self, img): self.rhograd = img
+    def setWavgrad(self, d): self.wavgrad = d
+    def setDatamodP(self, d): self.datamodP = d
+    def setDataresP(self, d): self.dataresP = d
+    def getMisfit(self): return self.misfit
+
+    def _adjoint_shot(self, keep):
+        a = super()._adjoint_shot(keep)
+        vp, rho = np.ascontiguousarray(self.model.Vp), np.ascontiguousarray(self.model.R)
+        keep.extend([vp, rho])
+        a.vp, a.rho = ptr(vp), ptr(rho)
+        a.vpgrad = ptr(self.vpgrad.getImagedata()) if self.vpgrad is not None else None
+        a.rhograd = ptr(self.rhograd.getImagedata()) if self.rhograd is not None else None
+        a.wavgrad = ptr(self.wavgrad.data) if self.wavgrad is not None else None
+        a.datares = ptr(self.dataresP.data) if self.dataresP is not None else None
+        a.shot.rec_out = ptr(self.datamodP.data) if self.datamodP is not None else None
+        self._mis = C.c_double(0.0)
+        a.misfit = C.pointer(self._mis)
+        return a
+
+    def run_optimal(self):
+        return fwi_gradient_batch([self])
+
+
+class RtmAcoustic2D(_Adjoint):
+    """RtmAcoustic2D<T> (include/rtm.h:97-127): (extended) cross-correlation image."""
+    cls = "RtmAcoustic2D"
+
+    def __init__(self, model=None, pimage=None, source=None, dataP=None, order=4, snapinc=1, precision=None):
+        super().__init__(model, source, dataP, order, snapinc, precision)
+        self.pimage = pimage
+
+    def setImage(self, img): self.pimage = img
+
+    def _adjoint_shot(self, keep):
+        a = super()._adjoint_shot(keep)
+        a.image = ptr(self.pimage.getImagedata())
+        return a
+
+    def run_optimal(self):
+        return rtm_image_batch([self])
+
+
+def _adjoint_batch(jobs, fn):
+    j0 = jobs[0]
+    j0.checkStability()
+    cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
+    nhx = j0.pimage.getNhx() if isinstance(j0, RtmAcoustic2D) else 1
+    nhz = j0.pimage.getNhz() if isinstance(j0, RtmAcoustic2D) else 1
+    opts = j0._opts(nhx, nhz)
+    keep: list = []
+    shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
+    check(fn(C.byref(cfg), C.byref(opts), len(jobs), shots))
+    for j in jobs:
+        if isinstance(j, FwiAcoustic2D):
+            j.misfit += j._mis.value
+    return FWI_OK
+
+
+def fwi_gradient_batch(jobs):
+    """Many FwiAcoustic2D shots (each with its own model window) in one batched
+    gradient computation; per-shot outputs accumulate like run_optimal's."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_fwi_gradient)
+
+
+def rtm_image_batch(jobs):
+    """Many RtmAcoustic2D shots imaged in one batched run."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_rtm_image)
+
+
+class AdjointBatch:
+    """Device-resident gradient/image batch (rsgpu_adjoint_*): create once, run many times."""
+
+    def __init__(self, jobs, kind=abi.KIND_FWI):
+        j0 = jobs[0]
+        self.jobs = jobs
+        self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
+        nhx = j0.pimage.getNhx() if kind == abi.KIND_RTM else 1
+        nhz = j0.pimage.getNhz() if kind == abi.KIND_RTM else 1
+        self.opts = j0._opts(nhx, nhz)
+        self._keep: list = []
+        self.shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(self._keep) for j in jobs])
+        self.h = C.c_void_p()
+        check(abi.lib.rsgpu_adjoint_create(C.byref(self.cfg), C.byref(self.opts), kind, len(jobs), self.shots,
+                                           C.byref(self.h)))
+
+    def run(self): check(abi.lib.rsgpu_adjoint_run(self.h))
+
+    def read(self):
+        check(abi.lib.rsgpu_adjoint_read(self.h, len(self.jobs), self.shots))
+        for j in self.jobs:
+            if isinstance(j, FwiAcoustic2D):
+                j.misfit += j._mis.value
+                j._mis.value = 0.0
+
+    def stats(self):
+        v = [C.c_longlong() for _ in range(4)]
+        check(abi.lib.rsgpu_adjoint_stats(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("fw_steps", "bw_steps", "ckpt_bytes", "launches"), [x.value for x in v]))
+
+    def stream(self) -> int: return abi.lib.rsgpu_adjoint_stream(self.h) or 0
+
+    def close(self):
+        if self.h:
+            abi.lib.rsgpu_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -59,3 +59,35 @@ def rel_l2(a, b) -> float:
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def fwi_case(nx=81, nz=61, nt=300, seed=1, precision=abi.F32_EXACT, scoord=(400.3, 23.7), dlens=0.92, **kw):
+    """A Case2D in the starting model plus 'observed' data modelled (by the oracle)
+    in a model with a slow lens, so residuals and gradients are nonzero."""
+    from rockseis_b200.rockseis import ModelAcoustic2D
+    c = Case2D(abi.ACOUSTIC2D, nx=nx, nz=nz, nt=nt, seed=seed, precision=precision, scoord=scoord, **kw)
+    vt = c.vp.copy()
+    vt[nz // 3: nz // 3 + 8, nx // 3: nx // 3 + 12] *= dlens
+    # the observed data are always modelled in float, so cases of every precision share them
+    mt = ModelAcoustic2D(nx, nz, c.model.lpml, c.model.dx, c.model.dz, c.model.ox, c.model.oz, c.model.fs)
+    mt.createModel()
+    mt.Vp[:], mt.R[:] = vt, c.rho
+    pbt = api.Problem2D(nx, nz, c.model.dx, c.model.dz, c.model.lpml, c.order, c.model.fs, c.dt, nt, vt, c.rho)
+    dtype = abi.real_dtype(precision)
+    tab32 = np.zeros(12 * c.model.lpml, np.float32)
+    abi.check(abi.lib.rsgpu_pml_tables(c.model.lpml, c.dt, abi.F32_EXACT, tab32.ctypes.data))
+    obs = api.orc_modelling_a2d(pbt, mt.padded(), tab32, c.src.smap, c.src.sshift,
+                                synth.ricker(nt, c.dt, 15.0)[None, :], abi.PRESSURE, c.rec.gmap, c.rec.gshift,
+                                abi.PRESSURE)
+    c.obs = obs.astype(dtype)
+    return c
+
+
+def oracle_fwi(c):
+    return api.orc_fwi_a2d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, c.src.smap, c.src.sshift,
+                           c.src.data, c.rec.gmap, c.rec.gshift, c.obs)
+
+
+def oracle_rtm(c, data, nhx=1, nhz=1):
+    return api.orc_rtm_a2d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, c.src.smap, c.src.sshift,
+                           c.src.data, c.rec.gmap, c.rec.gshift, data, nhx, nhz)
