@@ -308,6 +308,185 @@ def run_gpu(args, rank, world, device):
     return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary())
 
 
+# ---------------------------------------------------------------- FWI gradient workload
+FWI = dict(nx=601, nz=201, dx=10.0, lpml=20, order=8, nt=3000, dt=1e-3, nshots=64, ncheck=50, f0=10.0, sz=20.0,
+           nrec=601, plain_sample=4)
+
+
+def fwi_problem(precision, nshots, nt=None, start=True, f=FWI):
+    """Models, sources and receiver sets of the FWI workload (one Data2D pair per shot)."""
+    from rockseis_b200 import abi, synth
+    from rockseis_b200.rockseis import Data2D, ModelAcoustic2D
+    nt = nt or f["nt"]
+    vt, vs = synth.fwi_models(f["nx"], f["nz"], f["dx"])
+    m = ModelAcoustic2D(f["nx"], f["nz"], f["lpml"], f["dx"], f["dx"], 0.0, 0.0, 0, precision)
+    m.createModel()
+    m.Vp[:] = vs if start else vt
+    m.R[:] = synth.gardner(m.Vp)
+    wav = synth.ricker(nt, f["dt"], f["f0"], abi.real_dtype(precision))
+    sx = np.linspace(60.0, (f["nx"] - 1) * f["dx"] - 60.0, f["nshots"])[:nshots]
+    gc = synth.surface_line(f["nrec"], 0.0, f["dx"], 0.0)
+    srcs, recs = [], []
+    for x in sx:
+        s_ = Data2D(1, nt, f["dt"], 0.0, precision)
+        s_.scoords[:] = [[x, f["sz"]]]
+        s_.data[:] = wav[None, :]
+        s_.makeMap(m, 0)
+        r = Data2D(f["nrec"], nt, f["dt"], 0.0, precision)
+        r.gcoords[:] = gc
+        r.makeMap(m, 1)
+        srcs.append(s_)
+        recs.append(r)
+    return m, srcs, recs
+
+
+def fwi_jobs(m, srcs, obs, precision, ckpt, accum, f=FWI):
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import Data2D, FwiAcoustic2D, Image2D
+    jobs = []
+    for s_, o in zip(srcs, obs):
+        j = FwiAcoustic2D(m, s_, o, f["order"], 1, precision=precision)
+        j.setNcheck(f["ncheck"])
+        j.setCheckpointPrecision(ckpt)
+        j.setAccumulation(accum)
+        j.setVpgrad(Image2D("vpgrad", m, 1, 1, precision))
+        j.setRhograd(Image2D("rhograd", m, 1, 1, precision))
+        j.setWavgrad(Data2D(s_.ntrace, s_.nt, s_.dt, 0.0, precision))
+        jobs.append(j)
+    return jobs
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _fwi_ref_sample(args):
+    """One process: the reference's FwiAcoustic2D::run_optimal on one shot, shortened time axis."""
+    shot, nt = args
+    sys.path.insert(0, ROOT)
+    from oracle import api
+    from rockseis_b200 import synth
+    f = FWI
+    vt, vs = synth.fwi_models(f["nx"], f["nz"], f["dx"])
+    rho = synth.gardner(vs)
+    pb = api.Problem2D(f["nx"], f["nz"], f["dx"], f["dx"], f["lpml"], f["order"], 0, f["dt"], nt, vs, rho)
+    sx = np.linspace(60.0, (f["nx"] - 1) * f["dx"] - 60.0, f["nshots"])[shot % f["nshots"]]
+    gc = synth.surface_line(f["nrec"], 0.0, f["dx"], 0.0)
+    wav = synth.ricker(nt, f["dt"], f["f0"])[None, :]
+    obs = np.zeros((f["nrec"], nt), np.float32)
+    t0 = time.perf_counter()
+    api.ref_fwi_a2d(pb, np.array([[sx, f["sz"]]]), wav, gc, obs, f["ncheck"])
+    return time.perf_counter() - t0
+
+
+def cpu_fwi_reference(nt_sample=300, procs=None, f=FWI):
+    """The reference's CPU gradient, one shot per process on all host cores, on the full
+    grid with a shortened time axis, extrapolated to nt by the propagation work
+    (Revolve forward steps + adjoint steps + correlations)."""
+    import multiprocessing as mp
+    from oracle import api
+    from rockseis_b200 import abi
+    if not api.ref_available():
+        return None
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        times = pool.map(_fwi_ref_sample, [(i, nt_sample) for i in range(procs)])
+
+    def work(nt):
+        return abi.lib.rsgpu_revolve_numforw(nt, f["ncheck"]) + 1 + 2 * nt
+    t_shot = max(times) * work(f["nt"]) / work(nt_sample)
+    return {"value": round(procs / t_shot, 5), "unit": "shots/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x 1 shot, full 641x241 padded grid, nt={nt_sample} (ncheck "
+                      f"{f['ncheck']}), extrapolated to nt={f['nt']} by Revolve forward + adjoint + "
+                      f"correlation steps", "max_process_s": round(max(times), 3)}
+
+
+def _timed_runs(batch, steps):
+    import torch
+    st = torch.cuda.ExternalStream(batch.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(steps):
+        batch.run()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def fwi_config(f=FWI):
+    return {"workload": "acoustic2d_fwi_gradient_64shots_601x201_nt3000_ncheck50", "nx": f["nx"], "nz": f["nz"],
+            "dx": f["dx"], "lpml": f["lpml"], "order": f["order"], "nt": f["nt"], "dt": f["dt"],
+            "shots": f["nshots"], "receivers": f["nrec"], "ncheck": f["ncheck"],
+            "l2": "working set > 126 MB L2 (no flush needed)"}
+
+
+def run_fwi(args, device=0, f=FWI):
+    """Shots/s of the checkpointed FWI gradient: all shots batched vs one shot at a time."""
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import AdjointBatch, fwi_gradient_batch, modelling_batch
+    ns = f["nshots"]
+    prec, ckpt, accum = abi.F32_FAST, abi.CKPT_F16, abi.ACCUM_F64
+    # observed data: modelled in the true model on the GPU
+    mt, srcs, obs = fwi_problem(prec, ns, start=False)
+    modelling_batch([mt] * ns, srcs, obs, f["order"], prec)
+    m, srcs, _ = fwi_problem(prec, ns)
+    jobs = fwi_jobs(m, srcs, obs, prec, ckpt, accum)
+    batch = AdjointBatch(jobs)
+    batch.run()                                   # warm-up (graph capture, first touch)
+    with ClockSampler(device) as clk:
+        t_batch = _timed_runs(batch, max(1, args.fwi_steps))
+    stats = batch.stats()
+    batch.read()
+    g0 = jobs[0].vpgrad.getImagedata()[0, 0].copy()
+    batch.close()
+    # one shot at a time, same settings (sample of the shots)
+    t_plain = []
+    for j in jobs[:f["plain_sample"]]:
+        b1 = AdjointBatch([j])
+        b1.run()
+        t_plain.append(_timed_runs(b1, 1))
+        b1.close()
+    plain = len(t_plain) / sum(t_plain)
+    # accuracy of shot 0 against the FP64 propagator (lossless checkpoints, FP64 accumulation)
+    m64, s64, o64 = fwi_problem(abi.F64, 1)
+    o64[0].data = obs[0].data.astype(np.float64)
+    j64 = fwi_jobs(m64, s64, o64, abi.F64, abi.CKPT_NATIVE, abi.ACCUM_F64)
+    b64 = AdjointBatch(j64)
+    b64.run()
+    b64.read()
+    g64 = j64[0].vpgrad.getImagedata()[0, 0]
+    b64.close()
+    err = rel_l2(g0, g64)
+    pts = (f["nx"] + 2 * f["lpml"]) * (f["nz"] + 2 * f["lpml"])
+    # end to end: one rsgpu_fwi_gradient call from host buffers (plan creation, upload of
+    # models, maps, wavelets and observed data, the gradient, read-back of all outputs)
+    e2e = None
+    if not args.no_e2e:
+        for j in jobs:
+            for img in (j.vpgrad, j.rhograd):
+                img.getImagedata()[:] = 0
+            j.wavgrad.data[:] = 0
+        t0 = time.perf_counter()
+        fwi_gradient_batch(jobs)
+        t_e2e = time.perf_counter() - t0
+        h2d = sum(m_.nbytes for m_ in m.padded()) * ns + sum(o.data.nbytes + o.gmap.nbytes + o.gshift.nbytes
+                                                                for o in obs)
+        h2d += ns * (m.Vp.nbytes + m.R.nbytes) + sum(s_.data.nbytes for s_ in srcs)
+        d2h = ns * (2 * m.Vp.nbytes + srcs[0].data.nbytes)
+        e2e = {"value": round(ns / t_e2e, 3), "unit": "shots/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "path": "rsgpu_fwi_gradient (C ABI) from host buffers"}
+    return {"metric": "FWI gradient shots/s", "shots_per_s_batched": round(ns / t_batch, 3),
+            "shots_per_s_plain": round(plain, 3), "batched_over_plain": round((ns / t_batch) / plain, 2),
+            "s_per_batch": round(t_batch, 4), "plain_sample_shots": len(t_plain),
+            "gradient_rel_l2_vs_fp64": float("%.3g" % err), "arithmetic": "FMA f32, FP16-scaled checkpoints, "
+            "FP64 accumulation", "forward_steps": stats["fw_steps"], "adjoint_steps": stats["bw_steps"],
+            "checkpoint_bytes": stats["ckpt_bytes"], "gpu_launches": stats["launches"],
+            "gpts_per_s_propagation": round(ns * pts * (stats["fw_steps"] + stats["bw_steps"]) / t_batch / 1e9, 3),
+            "config": fwi_config(), "e2e": e2e, "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------- distributed plumbing
 def dist_init(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -350,7 +529,26 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
+    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "fwi"],
+                    help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
+                         "fwi: the FWI gradient line alone")
+    ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
+    ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
     args = ap.parse_args()
+
+    if args.impl == "reference" and args.workload == "fwi":
+        if int(os.environ.get("RANK", "0")) == 0:
+            r = cpu_fwi_reference()
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                return
+            print(json.dumps({"metric": "FWI gradient shots/s", "value": r["value"], "unit": "shots/s",
+                              "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1,
+                              "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f32", "data": "synthetic", "config": fwi_config(), "cpu_baseline": r,
+                              "e2e": {"value": r["value"], "unit": "shots/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return
 
     if args.impl == "reference":
         # CPU only: rank 0 times the reference, the other ranks exit without work.
@@ -374,10 +572,33 @@ def main():
         return
 
     rank, world, local = dist_init(args)
+    if args.workload == "fwi":
+        if world > 1:
+            raise SystemExit("the FWI gradient line is a one-GPU measurement")
+        cpu = None if args.no_cpu_baseline else cpu_fwi_reference()
+        import torch
+        torch.cuda.set_device(local)
+        r = run_fwi(args, device=local)
+        line = {"metric": "FWI gradient shots/s", "value": r["shots_per_s_batched"], "unit": "shots/s", "n_gpus": 1,
+                "steps": args.fwi_steps, "warmup": 1, "ms_per_step": round(r["s_per_batch"] * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded smooth background + Gaussian anomalies; start model smoothed)",
+                "config": r["config"], "gpu_launches": r["gpu_launches"], "fwi_gradient": r, "e2e": r.get("e2e"),
+                "clocks": r["clocks"], "cpu_baseline": cpu}
+        print(json.dumps(line))
+        return
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference()   # before the first CUDA call of this process (spawned workers)
     r = run_gpu(args, rank, world, local)
+    fwi = None
+    if rank == 0 and world == 1 and not args.no_fwi:
+        try:
+            fwi = run_fwi(args)
+            if not args.no_cpu_baseline:
+                fwi["cpu_baseline"] = cpu_fwi_reference()
+        except Exception as exc:          # keep the forward line if the gradient part fails
+            fwi = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         line = {"metric": "Gpts/s", "value": round(r["value"], 3), "unit": "Gpts/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
@@ -386,6 +607,8 @@ def main():
                 "config": config_dict(world, args.precision, args.nt), "gpu_launches": int(r["launches"]),
                 "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
                 "cpu_baseline": cpu}
+        if fwi is not None:
+            line["fwi_gradient"] = fwi
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -65,3 +65,33 @@ def elastic_model(nx: int, nz: int, dx: float, seed=2, vclip=4450.0, nlenses=6, 
 def surface_line(n: int, x0: float, dxr: float, z: float) -> np.ndarray:
     """n positions (x, z) starting at x0 with spacing dxr at depth z."""
     return np.stack([x0 + dxr * np.arange(n), np.full(n, z)], axis=1)
+
+
+def _gauss_smooth(a: np.ndarray, sigma_cells: float) -> np.ndarray:
+    """Gaussian smoothing with reflected edges (Fourier domain on the mirrored array)."""
+    nz, nx = a.shape
+    m = np.concatenate([a, a[::-1]], axis=0)
+    m = np.concatenate([m, m[:, ::-1]], axis=1)
+    kz = np.fft.fftfreq(2 * nz)[:, None]
+    kx = np.fft.fftfreq(2 * nx)[None, :]
+    g = np.exp(-2 * (np.pi * sigma_cells) ** 2 * (kz ** 2 + kx ** 2))
+    return np.real(np.fft.ifft2(np.fft.fft2(m) * g))[:nz, :nx]
+
+
+def fwi_models(nx: int, nz: int, dx: float, seed=4, nanom=8, amp=0.08, smooth_m=200.0, vmin=1500.0, vmax=3500.0,
+               dtype=np.float32):
+    """True model = smooth depth-increasing background + `nanom` Gaussian anomalies of
+    +-amp (seeded); starting model = the true model smoothed with sigma = smooth_m.
+    Returns (vp_true, vp_start); density follows Gardner's relation in both."""
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz)[:, None] / max(1, nz - 1)
+    bg = vmin + (vmax - vmin) * z * np.ones((1, nx))
+    zz, xx = np.mgrid[0:nz, 0:nx]
+    pert = np.zeros((nz, nx))
+    for _ in range(nanom):
+        cx, cz = rng.uniform(0.1, 0.9) * nx, rng.uniform(0.2, 0.85) * nz
+        r = rng.uniform(0.03, 0.08) * min(nx, 3 * nz)
+        pert += rng.choice([-1.0, 1.0]) * amp * np.exp(-(((xx - cx) ** 2 + (zz - cz) ** 2) / (2 * r * r)))
+    vt = bg * (1.0 + pert)
+    vs = _gauss_smooth(vt, smooth_m / dx)
+    return vt.astype(dtype), vs.astype(dtype)
