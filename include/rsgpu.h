@@ -77,8 +77,9 @@ typedef struct {
     const void *pml;    /* 12*lpml C-PML tables in the order A,B,C ltf; A,B,C ltf_stag;
                            A,B,C rbb; A,B,C rbb_stag (include/pml.h:31-81).  NULL: computed
                            by rsgpu_pml_tables with Smax = 1200. */
-    int tile;           /* kernel tile shape, -1 = autotuned/default */
-    int reserved[7];
+    int tile;           /* 2D kernel tile shape, -1 = autotuned/default */
+    int zchunk;         /* 3D: planes marched by one CTA (0 = 64) */
+    int reserved[6];
 } rsgpu_config;
 
 /* One shot (work item) of a batch.  nx/ny/nz are the UNPADDED window the

@@ -32,6 +32,12 @@ class OrcGrid(C.Structure):
                 ("dx", C.c_float), ("dz", C.c_float), ("dt", C.c_float), ("nt", C.c_int)]
 
 
+class OrcGrid3(C.Structure):
+    _fields_ = [("nxp", C.c_int), ("nyp", C.c_int), ("nzp", C.c_int), ("lpml", C.c_int), ("order", C.c_int),
+                ("fs", C.c_int), ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float),
+                ("nt", C.c_int)]
+
+
 class RefGrid(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("lpml", C.c_int), ("order", C.c_int),
                 ("fs", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("ox", C.c_double),
@@ -60,6 +66,7 @@ def oracle() -> C.CDLL:
                                                                                   V, V, V]
         _oracle.orc_rtm_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 4 + [I, V, V, V, I, V, V, V, I, I, V]
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
+        _oracle.orc_mod_a3d.argtypes = [C.POINTER(OrcGrid3)] + [V] * 5 + [I, V, V, V, I, I, V, V, I, V, I, V]
     return _oracle
 
 
@@ -91,6 +98,7 @@ def ref() -> C.CDLL:
         _ref.ref_makemap2d_f.argtypes = [G, I, V, I, V, V]
         _ref.ref_makemap2d_field_f.argtypes = [G, I, V, I, I, V, V]
         _ref.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
+        _ref.ref_makemap3d_field_f.argtypes = [G, I, V, I, I, V, V]
         _ref.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
         _ref.ref_revolve_numforw.argtypes = [I, I]
         _ref.ref_revolve_adjust.argtypes = [I]
@@ -244,3 +252,64 @@ def orc_rtm_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, data, nhx=1, n
                              len(gm), _p(gm), _p(gs), _p(d), nhx, nhz, _p(img))
     assert r == 0
     return img
+
+
+# ---------------------------------------------------------------- 3D
+class Problem3D:
+    """One 3D shot: unpadded models [nz][ny][nx] and the grid."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, lpml, order, fs, dt, nt, vp, rho, vs=None, ox=0.0, oy=0.0, oz=0.0):
+        self.nx, self.ny, self.nz, self.dx, self.dy, self.dz = nx, ny, nz, dx, dy, dz
+        self.lpml, self.order, self.fs, self.dt, self.nt = lpml, order, fs, dt, nt
+        self.vp, self.rho, self.vs, self.ox, self.oy, self.oz = vp, rho, vs, ox, oy, oz
+
+    def ref_grid(self) -> RefGrid:
+        return RefGrid(self.nx, self.ny, self.nz, self.lpml, self.order, int(self.fs), self.dx, self.dy, self.dz,
+                       self.ox, self.oy, self.oz, self.dt, self.nt)
+
+    def orc_grid(self) -> OrcGrid3:
+        L = self.lpml
+        return OrcGrid3(self.nx + 2 * L, self.ny + 2 * L, self.nz + 2 * L, L, min(max(self.order, 1), 8),
+                        int(self.fs), self.dx, self.dy, self.dz, self.dt, self.nt)
+
+
+def ref_modelling_a3d(pb, scoords, wav, sfield, gcoords, rfield):
+    out = np.zeros((len(gcoords), pb.nt), np.float32)
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    vp, rho, w = _keep(pb.vp, pb.rho, wav, dtype=np.float32)
+    r = ref().ref_mod_a3d_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), sfield, len(gc), _p(gc), rfield,
+                            _p(out))
+    assert r == 1
+    return out
+
+
+def ref_stagger_a3d(pb):
+    g = pb.ref_grid()
+    L = pb.lpml
+    n = (pb.nx + 2 * L) * (pb.ny + 2 * L) * (pb.nz + 2 * L)
+    out = np.zeros((4, n), np.float32)
+    vp, rho = _keep(pb.vp, pb.rho, dtype=np.float32)
+    ref().ref_stagger_a3d_f(C.byref(g), _p(vp), _p(rho), *[out[k].ctypes.data for k in range(4)])
+    return out.reshape(4, pb.nz + 2 * L, pb.ny + 2 * L, pb.nx + 2 * L)
+
+
+def ref_makemap3d(pb, coords, which, field=0):
+    g = pb.ref_grid()
+    c = np.ascontiguousarray(coords, np.float64)
+    mp = np.zeros((len(c), 3), np.int32)
+    sh = np.zeros((len(c), 3), np.float32)
+    ref().ref_makemap3d_field_f(C.byref(g), len(c), _p(c), which, field, _p(mp), _p(sh))
+    return mp, sh
+
+
+def orc_modelling_a3d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, rfield, nsteps=None, want_state=False):
+    g = pb.orc_grid()
+    nr = len(gmap)
+    out = np.zeros((nr, pb.nt), np.float32)
+    st = np.zeros((4, g.nzp, g.nyp, g.nxp), np.float32) if want_state else None
+    Rx, Ry, Rz, L, tb, ss, w, gs = _keep(*padded, tab, sshift, wav, gshift, dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    oracle().orc_mod_a3d(C.byref(g), _p(Rx), _p(Ry), _p(Rz), _p(L), _p(tb), len(sm), _p(sm), _p(ss), _p(w), sfield,
+                         nr, _p(gm), _p(gs), rfield, _p(out), pb.nt if nsteps is None else nsteps, _p(st))
+    return (out, st) if want_state else out

@@ -286,18 +286,23 @@ void ref_makemap2d_f(const ref_grid *g, int ntr, const double *coords, int which
 {
     ref_makemap2d_field_f(g, ntr, coords, which, PRESSURE, map, shift);
 }
-void ref_makemap3d_f(const ref_grid *g, int ntr, const double *coords, int which, int *map, float *shift)
+void ref_makemap3d_field_f(const ref_grid *g, int ntr, const double *coords, int which, int field, int *map,
+                           float *shift)
 {
     auto m = std::make_shared<ModelAcoustic3D<float>>(g->nx, g->ny, g->nz, g->lpml, (float)g->dx,
                                                       (float)g->dy, (float)g->dz, (float)g->ox,
                                                       (float)g->oy, (float)g->oz, g->fs != 0);
-    auto d = make_data3d<float>(ntr, g, coords, PRESSURE, which != 0, m->getGeom(), nullptr);
+    auto d = make_data3d<float>(ntr, g, coords, field, which != 0, m->getGeom(), nullptr);
     Point3D<int> *mp = which ? d->getGeom()->getGmap() : d->getGeom()->getSmap();
     Point3D<float> *sh = which ? d->getGeom()->getGshift() : d->getGeom()->getSshift();
     for (int i = 0; i < ntr; i++) {
         map[3 * i] = mp[i].x; map[3 * i + 1] = mp[i].y; map[3 * i + 2] = mp[i].z;
         shift[3 * i] = sh[i].x; shift[3 * i + 1] = sh[i].y; shift[3 * i + 2] = sh[i].z;
     }
+}
+void ref_makemap3d_f(const ref_grid *g, int ntr, const double *coords, int which, int *map, float *shift)
+{
+    ref_makemap3d_field_f(g, ntr, coords, which, PRESSURE, map, shift);
 }
 
 /* Revolve::revolve action trace (lib/revolve.cpp:150-305).  Returns the number of

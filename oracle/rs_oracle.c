@@ -518,3 +518,148 @@ int orc_rtm_a2d(const orc_grid *g, int nx, int nz, const float *Rx, const float 
 }
 
 long orc_state_size(int nxp, int nzp, int elastic) { return (long)nxp * nzp * (elastic ? 5 : 3); }
+
+/* ================================================================== acoustic 3D
+ * WavesAcoustic3D::forwardstepVelocity/Stress (lib/waves.cpp:710-998),
+ * insertSource/recordData (lib/waves.cpp:999-1190), ModellingAcoustic3D::run
+ * (lib/modelling.cpp:363-474).  Arrays a[(iz*nyp + iy)*nxp + ix]; C-PML memory
+ * per face pair: x [nzp][nyp][2L], y [nzp][2L][nxp], z [2L][nyp][nxp]. */
+typedef struct {
+    int nxp, nyp, nzp;
+    int lpml, order, fs;
+    float dx, dy, dz, dt;
+    int nt;
+} orc_grid3;
+
+typedef struct {
+    orc_grid3 g;
+    float *f[4];            /* P, Vx, Vy, Vz */
+    float *px[2], *py[2], *pz[2];   /* [0] velocity step (P), [1] stress step (Vxx, Vyy, Vzz) */
+} orc_state3;
+
+static void st3_alloc(orc_state3 *s, const orc_grid3 *g)
+{
+    s->g = *g;
+    long n = (long)g->nxp * g->nyp * g->nzp;
+    for (int k = 0; k < 4; k++) s->f[k] = calloc(n, sizeof(float));
+    for (int k = 0; k < 2; k++) {
+        s->px[k] = calloc((long)g->nzp * g->nyp * 2 * g->lpml, sizeof(float));
+        s->py[k] = calloc((long)g->nzp * 2 * g->lpml * g->nxp, sizeof(float));
+        s->pz[k] = calloc((long)2 * g->lpml * g->nyp * g->nxp, sizeof(float));
+    }
+}
+static void st3_free(orc_state3 *s)
+{
+    for (int k = 0; k < 4; k++) free(s->f[k]);
+    for (int k = 0; k < 2; k++) { free(s->px[k]); free(s->py[k]); free(s->pz[k]); }
+}
+
+static void a3d_step(orc_state3 *s, const float *Rx, const float *Ry, const float *Rz, const float *Lm,
+                     const float *tab)
+{
+    const orc_grid3 *g = &s->g;
+    const int nx = g->nxp, ny = g->nyp, nz = g->nzp, L = g->lpml, o = g->order;
+    const long sy = nx, sz = (long)nx * ny;
+    float *P = s->f[0], *Vx = s->f[1], *Vy = s->f[2], *Vz = s->f[3];
+    int b, sl, t;
+    for (int iz = 0; iz < nz; iz++)
+        for (int iy = 0; iy < ny; iy++)
+            for (int ix = 0; ix < nx; ix++) {
+                long p = iz * sz + iy * sy + ix;
+                float d = d_fw(P, p, 1, ix, nx, o, g->dx), a = g->dt * Rx[p];
+                Vx[p] += a * d;
+                if ((t = strip(ix, nx, L, &b, &sl)) >= 0)
+                    Vx[p] = cpml(Vx[p], a, d, &s->px[0][((long)iz * ny + iy) * 2 * L + sl], tab, L, b + 3, t);
+                d = d_fw(P, p, sy, iy, ny, o, g->dy);
+                a = g->dt * Ry[p];
+                Vy[p] += a * d;
+                if ((t = strip(iy, ny, L, &b, &sl)) >= 0)
+                    Vy[p] = cpml(Vy[p], a, d, &s->py[0][((long)iz * 2 * L + sl) * nx + ix], tab, L, b + 3, t);
+                d = d_fw(P, p, sz, iz, nz, o, g->dz);
+                a = g->dt * Rz[p];
+                Vz[p] += a * d;
+                if ((t = strip(iz, nz, L, &b, &sl)) >= 0)
+                    Vz[p] = cpml(Vz[p], a, d, &s->pz[0][((long)sl * ny + iy) * nx + ix], tab, L, b + 3, t);
+            }
+    for (int iz = 0; iz < nz; iz++)
+        for (int iy = 0; iy < ny; iy++)
+            for (int ix = 0; ix < nx; ix++) {
+                long p = iz * sz + iy * sy + ix;
+                float al = g->dt * Lm[p];
+                float d = d_bw(Vx, p, 1, ix, nx, o, g->dx);
+                P[p] += al * d;
+                if ((t = strip(ix, nx, L, &b, &sl)) >= 0)
+                    P[p] = cpml(P[p], al, d, &s->px[1][((long)iz * ny + iy) * 2 * L + sl], tab, L, b, t);
+                d = d_bw(Vy, p, sy, iy, ny, o, g->dy);
+                P[p] += al * d;
+                if ((t = strip(iy, ny, L, &b, &sl)) >= 0)
+                    P[p] = cpml(P[p], al, d, &s->py[1][((long)iz * 2 * L + sl) * nx + ix], tab, L, b, t);
+                d = d_bw(Vz, p, sz, iz, nz, o, g->dz);
+                P[p] += al * d;
+                if ((t = strip(iz, nz, L, &b, &sl)) >= 0)
+                    P[p] = cpml(P[p], al, d, &s->pz[1][((long)sl * ny + iy) * nx + ix], tab, L, b, t);
+            }
+}
+
+/* field codes: 0 PRESSURE, 1 VX, 2 VY, 3 VZ; maps (x,y,z) */
+static void inject3(orc_state3 *s, const float *Mod, int field, int ntr, const int *map, const float *shift,
+                    const float *wav, int it)
+{
+    const orc_grid3 *g = &s->g;
+    const int nx = g->nxp, ny = g->nyp, L = g->lpml;
+    float *F = s->f[field == 0 ? 0 : field];
+    for (int i = 0; i < ntr; i++) {
+        const int *m = map + 3 * i;
+        const float *sh = shift + 3 * i;
+        if (m[0] < 0 || m[1] < 0 || m[2] < 0) continue;
+        float xt[2] = {1 - sh[0], sh[0]}, yt[2] = {1 - sh[1], sh[1]}, zt[2] = {1 - sh[2], sh[2]};
+        float w = wav[it + (long)i * g->nt];
+        for (int i1 = 0; i1 < 2; i1++)
+            for (int i2 = 0; i2 < 2; i2++)
+                for (int i3 = 0; i3 < 2; i3++) {
+                    long p = ((long)(L + m[2] + i1) * ny + (L + m[1] + i2)) * nx + (L + m[0] + i3);
+                    F[p] += g->dt * Mod[p] * w * xt[i3] * yt[i2] * zt[i1];
+                }
+    }
+}
+
+static void record3(const orc_state3 *s, int field, int ntr, const int *map, const float *shift, float *out, int it)
+{
+    const orc_grid3 *g = &s->g;
+    const int nx = g->nxp, ny = g->nyp, L = g->lpml;
+    const float *F = s->f[field == 0 ? 0 : field];
+    for (int i = 0; i < ntr; i++) {
+        const int *m = map + 3 * i;
+        const float *sh = shift + 3 * i;
+        if (m[0] < 0 || m[1] < 0 || m[2] < 0) continue;
+        float xt[2] = {1 - sh[0], sh[0]}, yt[2] = {1 - sh[1], sh[1]}, zt[2] = {1 - sh[2], sh[2]};
+        float *o = &out[it + (long)i * g->nt];
+        for (int i1 = 0; i1 < 2; i1++)
+            for (int i2 = 0; i2 < 2; i2++)
+                for (int i3 = 0; i3 < 2; i3++) {
+                    long p = ((long)(L + m[2] + i1) * ny + (L + m[1] + i2)) * nx + (L + m[0] + i3);
+                    *o += xt[i3] * yt[i2] * zt[i1] * F[p];
+                }
+    }
+}
+
+/* ModellingAcoustic3D::run for one shot.  models: Rx, Ry, Rz, L (padded). */
+int orc_mod_a3d(const orc_grid3 *g, const float *Rx, const float *Ry, const float *Rz, const float *Lm,
+                const float *tab, int ns, const int *smap, const float *sshift, const float *wav, int sfield, int nr,
+                const int *gmap, const float *gshift, int rfield, float *out, int nsteps, float *state_out)
+{
+    orc_state3 s;
+    st3_alloc(&s, g);
+    const float *smod = sfield == 0 ? Lm : sfield == 1 ? Rx : sfield == 2 ? Ry : Rz;
+    for (int it = 0; it < nsteps; it++) {
+        a3d_step(&s, Rx, Ry, Rz, Lm, tab);
+        inject3(&s, smod, sfield, ns, smap, sshift, wav, it);
+        record3(&s, rfield, nr, gmap, gshift, out, it);
+    }
+    if (state_out) {
+        long n = (long)g->nxp * g->nyp * g->nzp;
+        for (int k = 0; k < 4; k++) memcpy(state_out + k * n, s.f[k], n * sizeof(float));
+    }
+    st3_free(&s);
+    return 0;
+}

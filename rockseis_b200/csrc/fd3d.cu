@@ -1,0 +1,300 @@
+// 3D acoustic staggered-grid propagator (WavesAcoustic3D, lib/waves.cpp:710-1190).
+//
+// Each CTA owns a TX3 x TY3 block of (x, y) columns of one shot and marches up
+// the z axis through a chunk of planes.  Per plane:
+//   - the z-derivative comes from a 16-plane register window per column
+//     (fw: planes z-7..z+8, bw: z-8..z+7), shifted by one plane per step, so a
+//     column's stencil values are loaded from HBM once;
+//   - the x- and y-derivatives come from the plane tile staged in shared memory
+//     with an 8-cell x/y halo (the centre from the register window, the halo
+//     from L2-resident neighbours);
+//   - the C-PML memory-variable update and correction of each face pair are fused
+//     into the same pass.
+// Arithmetic follows the reference operation by operation (MODE_IEEE: separately
+// rounded ops and IEEE division; MODE_FAST: FMA, coefficients pre-divided).  Near
+// the array ends the reference's reduced-order stencils are evaluated by
+// stencil_k (the same rules as in 2D).  One launch covers all tiles of all shots.
+#include "fd2d_kernels.cuh"
+#include "rsgpu_3d.h"
+
+namespace rsgpu {
+namespace {
+
+template <typename T>
+__device__ __forceinline__ void load_coefs3(CoefSet3<T> &s, const CoefSet3<T> *g)
+{
+    const T *src = reinterpret_cast<const T *>(g);
+    T *dst = reinterpret_cast<T *>(&s);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int i = tid; i < (int)(sizeof(CoefSet3<T>) / sizeof(T)); i += blockDim.x * blockDim.y) dst[i] = src[i];
+}
+
+// Staggered derivative with all NCOEF taps around b[7] (fw: b[0] = f[i-7]) or
+// b[8] (bw: b[0] = f[i-8]); in both cases sum_k (b[8+k*s] - b[7-k*s]) c_k.
+template <typename T, int MODE>
+__device__ __forceinline__ T taps(const T *b, int s, const T (&cu)[NCOEF], T d, T r)
+{
+    using A = Ar<T, MODE>;
+    T acc = A::mul(A::sub(b[8 * s], b[7 * s]), cu[0]);
+#pragma unroll
+    for (int k = 1; k < NCOEF; k++) acc = A::mad(acc, A::sub(b[(8 + k) * s], b[(7 - k) * s]), cu[k]);
+    return (MODE == MODE_FAST) ? acc : A::div(acc, d, r);
+}
+template <typename T, int MODE>
+__device__ __forceinline__ T taps_reg(const T (&q)[16], const T (&cu)[NCOEF], T d, T r)
+{
+    using A = Ar<T, MODE>;
+    T acc = A::mul(A::sub(q[8], q[7]), cu[0]);
+#pragma unroll
+    for (int k = 1; k < NCOEF; k++) acc = A::mad(acc, A::sub(q[8 + k], q[7 - k]), cu[k]);
+    return (MODE == MODE_FAST) ? acc : A::div(acc, d, r);
+}
+
+// Velocity half-step (lib/waves.cpp:710-851):
+//   Vx += dt*Rx*Dx+P [x C-PML, staggered tables], Vy likewise in y, Vz in z.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, const CoefSet3<T> *coefs)
+{
+    using A = Ar<T, MODE>;
+    __shared__ CoefSet3<T> cs;
+    __shared__ T sP[TY3 + 16][TX3 + 16];
+    load_coefs3(cs, coefs);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    const int ix = tl.x0 + tx, iy = tl.y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const long long plane = sh.plane;
+    const int col = iy * pitch + ix;
+    const T *P = sh.f[A3_P];
+    T *Vx = sh.f[A3_VX], *Vy = sh.f[A3_VY], *Vz = sh.f[A3_VZ];
+    const T *Rx = sh.m[M3_RX], *Ry = sh.m[M3_RY], *Rz = sh.m[M3_RZ];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kx = kfw(ix, nxp, order), Ky = kfw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    T q[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) q[j] = P[(z0 - 7 + j) * plane + col];
+    __syncthreads();
+    T cux[NCOEF], cuy[NCOEF], cuz[NCOEF];
+#pragma unroll
+    for (int k = 0; k < NCOEF; k++) {
+        cux[k] = cs.cx[order * CROW3 + k];
+        cuy[k] = cs.cy[order * CROW3 + k];
+        cuz[k] = cs.cz[order * CROW3 + k];
+    }
+    for (int iz = z0; iz < ze; iz++) {
+        const long long o = iz * plane + col;
+        T vx = Vx[o], vy = Vy[o], vz = Vz[o];
+        const T rx = __ldg(Rx + o), ry = __ldg(Ry + o), rz = __ldg(Rz + o);
+        __syncthreads();
+        sP[ty + 8][tx + 8] = q[7];
+        if (tx < 8) {
+            sP[ty + 8][tx] = P[o - 8];
+            sP[ty + 8][tx + TX3 + 8] = P[o + TX3];
+        }
+        if (ty < 8) {
+            sP[ty][tx + 8] = P[o - 8 * pitch];
+            sP[ty + TY3 + 8][tx + 8] = P[o + TY3 * pitch];
+        }
+        __syncthreads();
+        const T *cx = &sP[ty + 8][tx + 8];
+        const T dfx = (Kx == order) ? taps<T, MODE>(cx - 7, 1, cux, a.dx, a.rdx)
+                                    : stencil_k<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, true, a.dx, a.rdx);
+        const T dfy = (Ky == order) ? taps<T, MODE>(cx - 7 * (TX3 + 16), TX3 + 16, cuy, a.dy, a.rdy)
+                                    : stencil_k<T, MODE>(cx, TX3 + 16, Ky, cs.cy + Ky * CROW3, true, a.dy, a.rdy);
+        const int Kz = kfw(iz, nzp, order);
+        const T dfz = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
+                                    : stencil_k<T, MODE>(P + o, (int)plane, Kz, cs.cz + Kz * CROW3, true, a.dz, a.rdz);
+        T am = A::mul(a.dt, rx);
+        vx = A::mad(vx, am, dfx);
+        if (xi >= 0)
+            vx = pml_correct<T, MODE>(vx, am, dfx, sh.psix[0] + ((long long)iz * nyp + iy) * 2 * L + xc, a.pml, L,
+                                      xb + 3, xi);
+        Vx[o] = vx;
+        am = A::mul(a.dt, ry);
+        vy = A::mad(vy, am, dfy);
+        if (yi >= 0)
+            vy = pml_correct<T, MODE>(vy, am, dfy, sh.psiy[0] + ((long long)iz * 2 * L + yc) * nxp + ix, a.pml, L,
+                                      yb + 3, yi);
+        Vy[o] = vy;
+        am = A::mul(a.dt, rz);
+        vz = A::mad(vz, am, dfz);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        if (zi >= 0)
+            vz = pml_correct<T, MODE>(vz, am, dfz, sh.psiz[0] + ((long long)zc * nyp + iy) * nxp + ix, a.pml, L,
+                                      zb + 3, zi);
+        Vz[o] = vz;
+#pragma unroll
+        for (int j = 0; j < 15; j++) q[j] = q[j + 1];
+        q[15] = P[o + 9 * plane];
+    }
+}
+
+// Stress half-step (lib/waves.cpp:854-998):
+//   P += dt*L*Dx-Vx [x C-PML]; P += dt*L*Dy-Vy [y]; P += dt*L*Dz-Vz [z].
+template <typename T, int MODE>
+__global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const CoefSet3<T> *coefs)
+{
+    using A = Ar<T, MODE>;
+    __shared__ CoefSet3<T> cs;
+    __shared__ T sVx[TY3][TX3 + 16];
+    __shared__ T sVy[TY3 + 16][TX3];
+    load_coefs3(cs, coefs);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    const int ix = tl.x0 + tx, iy = tl.y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const long long plane = sh.plane;
+    const int col = iy * pitch + ix;
+    T *P = sh.f[A3_P];
+    const T *Vx = sh.f[A3_VX], *Vy = sh.f[A3_VY], *Vz = sh.f[A3_VZ];
+    const T *Lm = sh.m[M3_L];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kx = kbw(ix, nxp, order), Ky = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    T q[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) q[j] = Vz[(z0 - 8 + j) * plane + col];
+    __syncthreads();
+    T cux[NCOEF], cuy[NCOEF], cuz[NCOEF];
+#pragma unroll
+    for (int k = 0; k < NCOEF; k++) {
+        cux[k] = cs.cx[order * CROW3 + k];
+        cuy[k] = cs.cy[order * CROW3 + k];
+        cuz[k] = cs.cz[order * CROW3 + k];
+    }
+    for (int iz = z0; iz < ze; iz++) {
+        const long long o = iz * plane + col;
+        T p = P[o];
+        const T lm = __ldg(Lm + o);
+        const T vxc = Vx[o], vyc = Vy[o];
+        __syncthreads();
+        sVx[ty][tx + 8] = vxc;
+        sVy[ty + 8][tx] = vyc;
+        if (tx < 8) {
+            sVx[ty][tx] = Vx[o - 8];
+            sVx[ty][tx + TX3 + 8] = Vx[o + TX3];
+        }
+        if (ty < 8) {
+            sVy[ty][tx] = Vy[o - 8 * pitch];
+            sVy[ty + TY3 + 8][tx] = Vy[o + TY3 * pitch];
+        }
+        __syncthreads();
+        const T *cx = &sVx[ty][tx + 8];
+        const T *cy = &sVy[ty + 8][tx];
+        const T d1 = (Kx == order) ? taps<T, MODE>(cx - 8, 1, cux, a.dx, a.rdx)
+                                   : stencil_k<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, false, a.dx, a.rdx);
+        const T d2 = (Ky == order) ? taps<T, MODE>(cy - 8 * TX3, TX3, cuy, a.dy, a.rdy)
+                                   : stencil_k<T, MODE>(cy, TX3, Ky, cs.cy + Ky * CROW3, false, a.dy, a.rdy);
+        const int Kz = kbw(iz, nzp, order);
+        const T d3 = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
+                                   : stencil_k<T, MODE>(Vz + o, (int)plane, Kz, cs.cz + Kz * CROW3, false, a.dz, a.rdz);
+        const T am = A::mul(a.dt, lm);
+        p = A::mad(p, am, d1);
+        if (xi >= 0)
+            p = pml_correct<T, MODE>(p, am, d1, sh.psix[1] + ((long long)iz * nyp + iy) * 2 * L + xc, a.pml, L, xb,
+                                     xi);
+        p = A::mad(p, am, d2);
+        if (yi >= 0)
+            p = pml_correct<T, MODE>(p, am, d2, sh.psiy[1] + ((long long)iz * 2 * L + yc) * nxp + ix, a.pml, L, yb,
+                                     yi);
+        p = A::mad(p, am, d3);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        if (zi >= 0)
+            p = pml_correct<T, MODE>(p, am, d3, sh.psiz[1] + ((long long)zc * nyp + iy) * nxp + ix, a.pml, L, zb,
+                                     zi);
+        P[o] = p;
+#pragma unroll
+        for (int j = 0; j < 15; j++) q[j] = q[j + 1];
+        q[15] = Vz[o + 8 * plane];
+    }
+}
+
+// Source injection then receiver recording of one step, one CTA per shot
+// (lib/waves.cpp:999-1190).
+template <typename T, int MODE>
+__global__ void inject_record_3d(const Shot3D<T> *shots, const InjRec3<T> *plans, T dt, int it)
+{
+    using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
+    const Shot3D<T> &sh = shots[blockIdx.x];
+    const InjRec3<T> &pl = plans[blockIdx.x];
+    if (pl.kind_inj != INJ3_NONE) {
+        T *F = sh.f[pl.kind_inj == INJ3_P ? A3_P : pl.kind_inj == INJ3_VX ? A3_VX : pl.kind_inj == INJ3_VY ? A3_VY : A3_VZ];
+        const T *Mod = sh.m[pl.kind_inj == INJ3_P ? M3_L : pl.kind_inj == INJ3_VX ? M3_RX : pl.kind_inj == INJ3_VY ? M3_RY : M3_RZ];
+        for (int q = threadIdx.x; q < pl.ninj; q += blockDim.x) {
+            const long long p = pl.inj_pt[q];
+            T v = F[p];
+            const T dm = A::mul(dt, Mod[p]);
+            for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
+                const T w = pl.wav[(long long)pl.inj_trace[c] * pl.nt + it];
+                v = A::add(v, A::mul(A::mul(A::mul(A::mul(dm, w), pl.inj_w[3 * c]), pl.inj_w[3 * c + 1]),
+                                     pl.inj_w[3 * c + 2]));
+            }
+            F[p] = v;
+        }
+    }
+    if (pl.kind_rec == REC3_NONE) return;
+    __syncthreads();
+    const T *F = sh.f[pl.kind_rec == REC3_P ? A3_P : pl.kind_rec == REC3_VX ? A3_VX : pl.kind_rec == REC3_VY ? A3_VY : A3_VZ];
+    for (int tr = threadIdx.x; tr < pl.nrec; tr += blockDim.x) {
+        const long long p = pl.rec_pt[tr];
+        if (p < 0) continue;
+        const T *w = pl.rec_w + 6 * tr;
+        T *out = pl.rec_out + (long long)tr * pl.nt + it;
+        T acc = *out;
+        for (int i1 = 0; i1 < 2; i1++)
+            for (int i2 = 0; i2 < 2; i2++)
+                for (int i3 = 0; i3 < 2; i3++)
+                    acc = A::add(acc, A::mul(A::mul(A::mul(w[i3], w[2 + i2]), w[4 + i1]),
+                                             F[p + i1 * sh.plane + (long long)i2 * sh.pitch + i3]));
+        *out = acc;
+    }
+}
+
+template <typename T, int MODE>
+cudaError_t step3(int half, const void *args, const void *coefs, int grid, cudaStream_t st)
+{
+    const Step3DArgs<T> &a = *reinterpret_cast<const Step3DArgs<T> *>(args);
+    const dim3 block(TX3, TY3);
+    if (half == 0) a3d_velocity<T, MODE><<<grid, block, 0, st>>>(a, (const CoefSet3<T> *)coefs);
+    else a3d_stress<T, MODE><<<grid, block, 0, st>>>(a, (const CoefSet3<T> *)coefs);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_step_3d(int prec, int physics, int half, const void *args, const void *coefs, int grid,
+                           cudaStream_t st)
+{
+    if (physics != PHYS_A3D) return cudaErrorInvalidValue;
+    if (prec == PREC_F64) return step3<double, MODE_IEEE>(half, args, coefs, grid, st);
+    if (prec == PREC_F32_EXACT) return step3<float, MODE_IEEE>(half, args, coefs, grid, st);
+    return step3<float, MODE_FAST>(half, args, coefs, grid, st);
+}
+
+cudaError_t launch_injrec_3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
+                             cudaStream_t st)
+{
+    if (prec == PREC_F64)
+        inject_record_3d<double, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot3D<double> *)shots,
+                                                                    (const InjRec3<double> *)plans, dt, it);
+    else if (prec == PREC_F32_EXACT)
+        inject_record_3d<float, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot3D<float> *)shots,
+                                                                   (const InjRec3<float> *)plans, (float)dt, it);
+    else
+        inject_record_3d<float, MODE_FAST><<<nshots, 256, 0, st>>>((const Shot3D<float> *)shots,
+                                                                   (const InjRec3<float> *)plans, (float)dt, it);
+    return cudaGetLastError();
+}
+
+}  // namespace rsgpu

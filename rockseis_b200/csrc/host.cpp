@@ -21,6 +21,7 @@
 #include "rsgpu_host.h"
 #include "rsgpu_internal.h"
 #include "rsgpu_plan.h"
+#include "rsgpu_plan3d.h"
 
 namespace rsgpu {
 
@@ -641,7 +642,10 @@ rsgpu_status Plan::read_field(int shot, int field, void *host_out)
 
 using namespace rsgpu;
 
-struct rsgpu_plan { std::unique_ptr<Plan> p; };
+struct rsgpu_plan {
+    std::unique_ptr<Plan> p;        // 2D physics
+    std::unique_ptr<Plan3D> p3;     // 3D physics
+};
 
 extern "C" {
 
@@ -658,9 +662,19 @@ rsgpu_status rsgpu_plan_create(const rsgpu_config *cfg, int nshots, const rsgpu_
 {
     if (!plan) { set_error("plan pointer is null"); return RSGPU_ERR_ARG; }
     *plan = nullptr;
+    if (!cfg) { set_error("null config"); return RSGPU_ERR_ARG; }
     auto h = std::unique_ptr<rsgpu_plan>(new rsgpu_plan);
-    h->p.reset(new Plan());
-    rsgpu_status st = h->p->create(cfg, nshots, shots);
+    rsgpu_status st;
+    if (cfg->physics == RSGPU_ACOUSTIC3D) {
+        h->p3.reset(new Plan3D());
+        st = h->p3->create(cfg, nshots, shots);
+    } else if (cfg->physics == RSGPU_ELASTIC3D) {
+        set_error("elastic 3D propagation is not built");
+        st = RSGPU_ERR_UNSUPPORTED;
+    } else {
+        h->p.reset(new Plan());
+        st = h->p->create(cfg, nshots, shots);
+    }
     if (st != RSGPU_OK) return st;
     *plan = h.release();
     return RSGPU_OK;
@@ -668,42 +682,44 @@ rsgpu_status rsgpu_plan_create(const rsgpu_config *cfg, int nshots, const rsgpu_
 rsgpu_status rsgpu_plan_reset(rsgpu_plan *p)
 {
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
-    return p->p->reset();
+    return p->p3 ? p->p3->reset() : p->p->reset();
 }
 rsgpu_status rsgpu_plan_run(rsgpu_plan *p, int it0, int nsteps)
 {
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
-    return p->p->run(it0, nsteps);
+    return p->p3 ? p->p3->run(it0, nsteps) : p->p->run(it0, nsteps);
 }
 rsgpu_status rsgpu_plan_read_traces(rsgpu_plan *p, int shot, void *out)
 {
     if (!p || !out) { set_error("null plan/output"); return RSGPU_ERR_ARG; }
-    return p->p->read_traces(shot, out);
+    return p->p3 ? p->p3->read_traces(shot, out) : p->p->read_traces(shot, out);
 }
 rsgpu_status rsgpu_plan_read_field(rsgpu_plan *p, int shot, int field, void *out)
 {
     if (!p || !out) { set_error("null plan/output"); return RSGPU_ERR_ARG; }
-    return p->p->read_field(shot, field, out);
+    return p->p3 ? p->p3->read_field(shot, field, out) : p->p->read_field(shot, field, out);
 }
 rsgpu_status rsgpu_plan_sync(rsgpu_plan *p)
 {
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
-    cudaError_t e = cudaStreamSynchronize(p->p->stream);
+    cudaError_t e = cudaStreamSynchronize(p->p3 ? p->p3->stream : p->p->stream);
     if (e != cudaSuccess) { set_error("stream sync: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-    return p->p->check_device_error();
+    return p->p3 ? RSGPU_OK : p->p->check_device_error();
 }
-void *rsgpu_plan_stream(rsgpu_plan *p) { return p ? (void *)p->p->stream : nullptr; }
+void *rsgpu_plan_stream(rsgpu_plan *p) { return p ? (void *)(p->p3 ? p->p3->stream : p->p->stream) : nullptr; }
 rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *p)
 {
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
+    if (p->p3) { set_error("kernel timing is recorded by 2D plans only"); return RSGPU_ERR_UNSUPPORTED; }
     return p->p->enable_timing();
 }
 rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *p, float *ms_velocity, float *ms_stress)
 {
     if (!p || !ms_velocity || !ms_stress) { set_error("null argument"); return RSGPU_ERR_ARG; }
+    if (p->p3) { set_error("kernel timing is recorded by 2D plans only"); return RSGPU_ERR_UNSUPPORTED; }
     return p->p->kernel_times(ms_velocity, ms_stress);
 }
-long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? p->p->launches : 0; }
+long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? (p->p3 ? p->p3->launches : p->p->launches) : 0; }
 void rsgpu_plan_destroy(rsgpu_plan *p) { delete p; }
 
 rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_shot *shots)

@@ -1,0 +1,80 @@
+// 3D propagation: device descriptors and launchers (host runtime internals, not ABI).
+//
+// Device layout of one 3D shot: every field and parameter is a pitched array of
+// planes with a zero guard of GUARD cells on every side in x and y and GUARD
+// planes below and GUARD+2 above in z, so that a z-marching column with its
+// 16-plane register window and its x/y halos never leaves the allocation.
+//   element (ix, iy, iz) = origin[iz * plane + iy * pitch + ix],  plane = pitch * rows
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "rsgpu_internal.h"
+
+namespace rsgpu {
+
+constexpr int TX3 = 32;   // x columns per CTA (one warp row)
+constexpr int TY3 = 8;    // y rows per CTA
+
+enum { A3_P = 0, A3_VX = 1, A3_VY = 2, A3_VZ = 3 };
+enum { M3_RX = 0, M3_RY = 1, M3_RZ = 2, M3_L = 3 };
+
+template <typename T>
+struct Shot3D {
+    int nxp, nyp, nzp, pitch;
+    int rows, lpml, fs, pad_;
+    long long plane;          // elements per plane
+    T *f[4];                  // P, Vx, Vy, Vz
+    const T *m[4];            // Rx, Ry, Rz, L
+    // C-PML memory, [0] velocity step (P derivatives), [1] stress step (Vx, Vy, Vz derivatives):
+    //   x [nzp][nyp][2L], y [nzp][2L][nxp], z [2L][nyp][nxp]
+    T *psix[2], *psiy[2], *psiz[2];
+};
+
+// One CTA: a TX3 x TY3 column block of one shot, marching planes [z0, z0 + zc).
+struct Tile3D {
+    int shot, x0, y0, z0;
+};
+
+template <typename T>
+struct Step3DArgs {
+    const Shot3D<T> *shots;
+    const Tile3D *tiles;
+    int ntiles, order, zc, lpml;
+    T dt, dx, dy, dz;
+    T rdx, rdy, rdz;
+    const T *pml;
+};
+
+constexpr int CROW3 = 9;
+template <typename T>
+struct CoefSet3 {
+    T cx[9 * CROW3];
+    T cy[9 * CROW3];
+    T cz[9 * CROW3];
+};
+
+// Source injection / receiver recording (trilinear, 8 corners), one CTA per shot.
+// Contributions are kept in the reference's loop order: trace, z, y, x corner.
+template <typename T>
+struct InjRec3 {
+    int ninj, kind_inj;
+    const long long *inj_pt;   // [ninj] element offset from the field origin
+    const int *inj_start;      // [ninj+1]
+    const int *inj_trace;      // [ncontrib]
+    const T *inj_w;            // [ncontrib][3] x, y, z weights
+    const T *wav;              // [ntr * nt]
+    int nrec, kind_rec;
+    const long long *rec_pt;   // [nrec] offset of the (x0, y0, z0) corner, -1 off the grid
+    const T *rec_w;            // [nrec][6] x0 x1 y0 y1 z0 z1
+    T *rec_out;                // [nrec * nt], accumulated
+    int nt, pad_;
+};
+enum { INJ3_NONE = 0, INJ3_P = 1, INJ3_VX = 2, INJ3_VY = 3, INJ3_VZ = 4 };
+enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4 };
+
+cudaError_t launch_step_3d(int prec, int physics, int half, const void *args, const void *coefs, int grid,
+                           cudaStream_t st);
+cudaError_t launch_injrec_3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
+                             cudaStream_t st);
+
+}  // namespace rsgpu

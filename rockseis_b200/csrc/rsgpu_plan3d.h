@@ -1,0 +1,46 @@
+// 3D batch plan behind the opaque rsgpu_plan handle (host runtime, not ABI).
+#pragma once
+#include <cstddef>
+#include <vector>
+#include <cuda_runtime.h>
+#include "rsgpu.h"
+#include "rsgpu_kernels.h"
+
+namespace rsgpu {
+
+// Byte offsets of one 3D shot's arrays inside the plan arena.
+struct Layout3D {
+    int nxp = 0, nyp = 0, nzp = 0, pitch = 0, rows = 0, planes = 0;
+    long long plane = 0;
+    int nrec = 0, nsrc = 0;
+    size_t f[4] = {}, m[4] = {}, psix[2] = {}, psiy[2] = {}, psiz[2] = {};
+    size_t psi_end = 0, traces = 0, state_end = 0, wav = 0;
+};
+
+class Plan3D {
+public:
+    ~Plan3D();
+    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    rsgpu_status reset();
+    rsgpu_status run(int it0, int nsteps);
+    rsgpu_status step(int it);
+    rsgpu_status read_traces(int shot, void *host_out);
+    rsgpu_status read_field(int shot, int field, void *host_out);
+    size_t origin_bytes(const Layout3D &L) const;
+
+    rsgpu_config cfg{};
+    int prec = 0, nshots = 0, es = 4, zc = 64, ntiles = 0;
+    std::vector<Layout3D> shots;
+    void *arena = nullptr, *d_meta = nullptr;
+    size_t arena_bytes = 0;
+    void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+
+private:
+    template <typename T>
+    void fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu_shot &s, size_t o_ip, size_t o_is,
+                   size_t o_it, size_t o_iw, size_t o_rp, size_t o_rw, int ninj, int nrec);
+};
+
+}  // namespace rsgpu

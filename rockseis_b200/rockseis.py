@@ -136,6 +136,29 @@ class ModelElastic2D(_Model):
     def getM(self): return self.padded()[4]
 
 
+class ModelAcoustic3D(_Model):
+    """ModelAcoustic3D<T> (include/model.h): arrays [nz][ny][nx]."""
+    dim = 3
+    physics = abi.ACOUSTIC3D
+    names = ("Rx", "Ry", "Rz", "L")
+
+    def __init__(self, nx, ny, nz, lpml, dx, dy, dz, ox, oy, oz, fs, precision=abi.F32_EXACT):
+        super().__init__(nx, ny, nz, lpml, dx, dy, dz, ox, oy, oz, fs, precision)
+
+    def createModel(self):
+        self.Vp = np.zeros(self._shape(), self.dtype)
+        self.R = np.zeros(self._shape(), self.dtype)
+        self.realized = True
+
+    def getVp(self): return self.Vp
+    def getR(self): return self.R
+    def getDy(self): return self.dy
+    def getRx(self): return self.padded()[0]
+    def getRy(self): return self.padded()[1]
+    def getRz(self): return self.padded()[2]
+    def getL(self): return self.padded()[3]
+
+
 class Data2D:
     """Trace container (Data2D<T>): data[itr, it] == reference data[it + itr*nt]."""
     dim = 2
@@ -188,6 +211,11 @@ class Data2D:
                 self.smap, self.sshift = mp, sh
             else:
                 self.gmap, self.gshift = mp, sh
+
+
+class Data3D(Data2D):
+    """Trace container (Data3D<T>): coordinates and maps (x, y, z)."""
+    dim = 3
 
 
 def check_stability(model: _Model, dt: float, cls: str) -> None:
@@ -264,13 +292,15 @@ class _Modelling:
         self.order = int(order) if 1 < int(order) < 9 else 4   # Modelling<T>::Modelling (lib/modelling.cpp:17-22)
         self.snapinc = snapinc if snapinc > 0 else 1
         self.precision = precision if precision is not None else (model.precision if model else abi.F32_EXACT)
-        self.recP = self.recVx = self.recVz = None
+        self.recP = self.recVx = self.recVy = self.recVz = None
         self.tile = -1
+        self.zchunk = 0
 
     def setModel(self, m): self.model = m
     def setSource(self, s): self.source = s
     def setRecP(self, d): self.recP = d
     def setRecVx(self, d): self.recVx = d
+    def setRecVy(self, d): self.recVy = d
     def setRecVz(self, d): self.recVz = d
     def getOrder(self): return self.order
 
@@ -280,8 +310,9 @@ class _Modelling:
 
     def run(self):
         self.checkStability()
-        recs = [r for r in (self.recP, self.recVx, self.recVz) if r is not None]
+        recs = [r for r in (self.recP, self.recVx, self.recVy, self.recVz) if r is not None]
         cfg = make_config(self.model, self.order, self.source.nt, self.source.dt, self.precision, self.tile)
+        cfg.zchunk = int(self.zchunk)
         keep: list = []
         # one shot per recorded field; the wavefield computation is shared by
         # the reference, here each receiver set is a separate batch entry
@@ -297,6 +328,10 @@ class ModellingAcoustic2D(_Modelling):
 
 class ModellingElastic2D(_Modelling):
     physics_name = "ModellingElastic2D"
+
+
+class ModellingAcoustic3D(_Modelling):
+    physics_name = "ModellingAcoustic3D"
 
 
 def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):

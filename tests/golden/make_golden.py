@@ -1,11 +1,11 @@
-"""Generate the golden fixtures of the 2D path from the reference library itself.
+"""Generate the golden fixtures of the propagation path from the reference library itself.
 
 Run where the reference sources are present (the reference library is built
 from them into oracle/_ref by `make -C oracle ref`):
 
     python tests/golden/make_golden.py
 
-Every array in reference_2d.npz is an output of the unmodified reference code
+Every array in reference.npz is an output of the unmodified reference code
 (oracle/_ref/librsref.so driving Der, Pml, Model*::staggerModels,
 Data2D::makeMap, Revolve, ModellingAcoustic2D/ModellingElastic2D::run,
 FwiAcoustic2D::run_optimal and RtmAcoustic2D::run_optimal) on seeded inputs
@@ -29,7 +29,7 @@ from oracle import api  # noqa: E402
 from rockseis_b200 import synth  # noqa: E402
 
 PRESSURE, VX, VZ = 0, 1, 3
-OUT = os.path.join(HERE, "reference_2d.npz")
+OUT = os.path.join(HERE, "reference.npz")
 
 
 def grid(nx, nz, lpml, dx, dz, dt, nt, order=8, fs=0, ox=0.0, oz=0.0):
@@ -187,6 +187,31 @@ def adjoint_cases(g):
     g["rtm_image_h3"] = img
 
 
+def a3d_cases(g):
+    """Acoustic 3D shots (ModellingAcoustic3D::run) with reference-made inputs."""
+    nx, ny, nz, L, nt, dx = 15, 13, 14, 4, 70, 10.0
+    vp = np.stack([synth.layered_vp(nx, nz, dx, 1500, 3000, 3, 0.05, 40, 60 + k) for k in range(ny)], 1)
+    vp = np.ascontiguousarray(vp.astype(np.float32))
+    rho = synth.gardner(vp)
+    sc = np.array([[71.3, 63.9, 52.2]])
+    gc = np.stack([np.linspace(4.0, 131.0, 6), np.linspace(9.0, 111.0, 6), np.full(6, 7.3)], 1)
+    gc = gc.astype(np.float32).astype(np.float64)
+    wav = synth.ricker(nt, 1e-3, 30.0)[None, :]
+    g["a3d_vp"], g["a3d_rho"], g["a3d_sc"], g["a3d_gc"], g["a3d_wav"] = vp, rho, sc, gc, wav
+    g["a3d_grid"] = np.array([nx, ny, nz, L, nt, dx])
+    tab = np.zeros(12 * L, np.float32)
+    api.ref().ref_pml_tables_f(L, 1e-3, tab.ctypes.data)
+    g["a3d_tab"] = tab
+    for fs, sf, rf in ((0, PRESSURE, PRESSURE), (1, PRESSURE, VZ), (0, VX, PRESSURE)):
+        key = f"a3d_fs{fs}_s{sf}_r{rf}"
+        pb = api.Problem3D(nx, ny, nz, dx, dx, dx, L, 8, fs, 1e-3, nt, vp, rho)
+        g[f"{key}_traces"] = api.ref_modelling_a3d(pb, sc, wav, sf, gc, rf)
+        g[f"{key}_models"] = api.ref_stagger_a3d(pb)
+        g[f"{key}_smap"], g[f"{key}_sshift"] = api.ref_makemap3d(pb, sc, 0, sf)
+        g[f"{key}_gmap"], g[f"{key}_gshift"] = api.ref_makemap3d(pb, gc, 1, rf)
+    g["a3d_cases"] = np.array([f"a3d_fs{fs}_s{sf}_r{rf}" for fs, sf, rf in ((0, 0, 0), (1, 0, 3), (0, 1, 0))])
+
+
 def main():
     if not api.ref_available():
         raise SystemExit("oracle/_ref/librsref.so is missing: build it with `make -C oracle ref`")
@@ -198,6 +223,7 @@ def main():
     revolve_cases(g)
     modelling_cases(g)
     adjoint_cases(g)
+    a3d_cases(g)
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {len(g)} arrays, {os.path.getsize(OUT)} bytes")
 

@@ -1,6 +1,6 @@
 """Pins of the CPU oracle and of the host preprocessing (no GPU needed).
 
-tests/golden/reference_2d.npz holds outputs of the unmodified reference library
+tests/golden/reference.npz holds outputs of the unmodified reference library
 on seeded inputs (generated by tests/golden/make_golden.py).  Here:
 
 * the C restatement (oracle/rs_oracle.c) must reproduce them bit for bit:
@@ -24,7 +24,7 @@ from oracle import api
 from rockseis_b200 import abi, synth
 from rockseis_b200.rockseis import Data2D, ModelAcoustic2D, ModelElastic2D
 
-GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_2d.npz"))
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference.npz"))
 SHOT = dict(nx=41, nz=31, lpml=8, dx=10.0, dt=1e-3, nt=150, order=8)
 
 
@@ -184,3 +184,48 @@ def test_oracle_with_library_preprocessing_matches_reference_live(seed, elastic,
         out, ref = api.orc_modelling_a2d(*args), api.ref_modelling_a2d(pb, sc, wav, sf, gc, rf)
     assert np.abs(ref).max() > 0
     assert np.array_equal(out, ref), f"max abs diff {np.abs(out - ref).max()}"
+
+
+# ---------------------------------------------------------------- acoustic 3D
+def _a3d_key(case):
+    """'a3d_fs<fs>_s<src field>_r<rec field>' -> (fs, src field, rec field)."""
+    _, f, s_, r = case.split("_")
+    return int(f[2:]), int(s_[1:]), int(r[1:])
+
+
+def _a3d_problem(fs):
+    nx, ny, nz, L, nt, dx = (GOLD["a3d_grid"][k] for k in range(6))
+    return api.Problem3D(int(nx), int(ny), int(nz), dx, dx, dx, int(L), 8, fs, 1e-3, int(nt), GOLD["a3d_vp"],
+                         GOLD["a3d_rho"])
+
+
+@pytest.mark.parametrize("case", [str(c) for c in GOLD["a3d_cases"]])
+def test_oracle_3d_shot_gather_matches_reference(case):
+    fs, sf, rf = _a3d_key(case)
+    pb = _a3d_problem(fs)
+    g = lambda k: GOLD[f"{case}_{k}"]  # noqa: E731
+    out = api.orc_modelling_a3d(pb, list(g("models")), GOLD["a3d_tab"], g("smap"), g("sshift"), GOLD["a3d_wav"], sf,
+                                g("gmap"), g("gshift"), rf)
+    ref = g("traces")
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(out, ref), f"max abs diff {np.abs(out - ref).max()}"
+
+
+@pytest.mark.parametrize("case", [str(c) for c in GOLD["a3d_cases"]])
+def test_3d_host_preprocessing_matches_reference(case):
+    from rockseis_b200.rockseis import Data3D, ModelAcoustic3D
+    fs, sf, rf = _a3d_key(case)
+    nx, ny, nz, L, nt, dx = (GOLD["a3d_grid"][k] for k in range(6))
+    m = ModelAcoustic3D(int(nx), int(ny), int(nz), int(L), dx, dx, dx, 0.0, 0.0, 0.0, fs)
+    m.createModel()
+    m.Vp[:], m.R[:] = GOLD["a3d_vp"], GOLD["a3d_rho"]
+    for got, ref in zip(m.padded(), GOLD[f"{case}_models"]):
+        assert np.array_equal(got, ref)
+    for which, coords, field, key in ((0, GOLD["a3d_sc"], sf, "s"), (1, GOLD["a3d_gc"], rf, "g")):
+        d = Data3D(len(coords), int(nt), 1e-3, 0.0)
+        (d.scoords if which == 0 else d.gcoords)[:] = coords
+        d.setField(field)
+        d.makeMap(m, which)
+        mp, sh = (d.smap, d.sshift) if which == 0 else (d.gmap, d.gshift)
+        assert np.array_equal(mp, GOLD[f"{case}_{key}map"])
+        assert np.array_equal(sh, GOLD[f"{case}_{key}shift"])
