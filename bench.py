@@ -487,6 +487,143 @@ def run_fwi(args, device=0, f=FWI):
             "config": fwi_config(), "e2e": e2e, "clocks": clk.summary()}
 
 
+# ---------------------------------------------------------------- 3D acoustic workload
+A3D = dict(nx=400, ny=400, nz=300, dx=12.5, lpml=20, order=8, nt=2500, dt=1e-3, nshots=32, chunk=20, nrec=201,
+           f0=12.0, sz=25.0)
+
+
+def a3d_config(f=A3D):
+    return {"workload": "acoustic3d_forward_32shots_400x400x300_windows_nt2500", "nx": f["nx"], "ny": f["ny"],
+            "nz": f["nz"], "dx": f["dx"], "lpml": f["lpml"], "order": f["order"], "nt": f["nt"], "dt": f["dt"],
+            "shots": f["nshots"], "time_steps_per_bench_step": f["chunk"],
+            "windows": "per-shot aperture windows (apertures uniform in [1500, 5000] m, seed 6)",
+            "l2": "working set tens of GB > 126 MB L2 (no flush needed)"}
+
+
+def a3d_batch(precision, f=A3D):
+    """The 32 windowed shots of the 3D workload: (local models, sources, receivers)."""
+    from rockseis_b200 import abi, synth
+    from rockseis_b200.rockseis import SMAP, Data3D, ModelAcoustic3D
+    vp = synth.dipping_vp_3d(f["nx"], f["ny"], f["nz"], f["dx"], seed=5, vclip=4550.0)
+    big = ModelAcoustic3D(f["nx"], f["ny"], f["nz"], f["lpml"], f["dx"], f["dx"], f["dx"], 0.0, 0.0, 0.0, 0, precision)
+    big.createModel()
+    big.Vp[:] = vp
+    big.R[:] = synth.gardner(vp)
+    del vp
+    rng = np.random.default_rng(6)
+    ext = (f["nx"] - 1) * f["dx"], (f["ny"] - 1) * f["dx"]
+    gx, gy = np.meshgrid(np.linspace(0.1, 0.9, 8), np.linspace(0.15, 0.85, 4))
+    pos = np.stack([gx.ravel() * ext[0], gy.ravel() * ext[1]], 1) + rng.uniform(-150, 150, (f["nshots"], 2))
+    apert = rng.uniform(1500.0, 5000.0, (f["nshots"], 2))
+    wav = synth.ricker(f["nt"], f["dt"], f["f0"], abi.real_dtype(precision))
+    models, srcs, recs = [], [], []
+    for k in range(f["nshots"]):
+        sx, sy = pos[k]
+        s_ = Data3D(1, f["nt"], f["dt"], 0.0, precision)
+        s_.scoords[:] = [[sx, sy, f["sz"]]]
+        xs = np.clip(sx + np.linspace(-1250.0, 1250.0, f["nrec"]), 0.0, ext[0])
+        r = Data3D(f["nrec"], f["nt"], f["dt"], 0.0, precision)
+        r.gcoords[:] = np.stack([xs, np.full(f["nrec"], sy), np.zeros(f["nrec"])], 1)
+        s_.gcoords[:] = [[sx, sy, 0.0]]
+        m = big.getLocal(s_, apert[k, 0], apert[k, 1], SMAP)
+        s_.data[:] = wav[None, :]
+        s_.makeMap(m, 0)
+        r.makeMap(m, 1)
+        models.append(m)
+        srcs.append(s_)
+        recs.append(r)
+    return models, srcs, recs
+
+
+def _a3d_ref_sample(args):
+    """One process: the reference's ModellingAcoustic3D::run on one mean-size window, few steps."""
+    nxw, nyw, nsteps = args
+    sys.path.insert(0, ROOT)
+    from oracle import api
+    from rockseis_b200 import synth
+    f = A3D
+    vp = synth.dipping_vp_3d(nxw, nyw, f["nz"], f["dx"], seed=5, vclip=4550.0)
+    pb = api.Problem3D(nxw, nyw, f["nz"], f["dx"], f["dx"], f["dx"], f["lpml"], f["order"], 0, f["dt"], nsteps, vp,
+                       synth.gardner(vp))
+    wav = synth.ricker(nsteps, f["dt"], f["f0"])[None, :]
+    c = nxw * f["dx"] / 2
+    t0 = time.perf_counter()
+    api.ref_modelling_a3d(pb, np.array([[c, c, f["sz"]]]), wav, 0, np.array([[c, c, 0.0]]), 0)
+    return time.perf_counter() - t0
+
+
+def cpu_a3d_reference(models, nsteps=6, procs=None, f=A3D):
+    """Reference CPU 3D modelling, one mean-size window per process, first nsteps steps."""
+    import multiprocessing as mp
+    from oracle import api
+    if not api.ref_available():
+        return None
+    procs = procs or min(8, os.cpu_count() or 1)
+    nxw = int(round(np.mean([m.nx for m in models])))
+    nyw = int(round(np.mean([m.ny for m in models])))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        times = pool.map(_a3d_ref_sample, [(nxw, nyw, nsteps)] * procs)
+    L = f["lpml"]
+    pts = (nxw + 2 * L) * (nyw + 2 * L) * (f["nz"] + 2 * L) * nsteps * procs
+    return {"value": round(pts / max(times) / 1e9, 5), "unit": "Gpts/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x one {nxw}x{nyw}x{f['nz']} window (the batch's mean), first {nsteps} "
+                      f"steps", "max_process_s": round(max(times), 3)}
+
+
+def run_a3d(args, device=0, f=A3D):
+    """Gpts/s of the windowed 3D batch: chunks of time steps of all 32 shots."""
+    import ctypes as C
+    import torch
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import make_config, make_shot
+    prec = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
+    models, srcs, recs = a3d_batch(prec)
+    cfg = make_config(models[0], f["order"], f["nt"], f["dt"], prec)
+    keep: list = []
+    shots = (abi.Shot * len(models))(*[make_shot(m, s_, r, keep) for m, s_, r in zip(models, srcs, recs)])
+    h = C.c_void_p()
+    abi.check(abi.lib.rsgpu_plan_create(C.byref(cfg), len(models), shots, C.byref(h)))
+    L = f["lpml"]
+    pts = sum((m.nx + 2 * L) * (m.ny + 2 * L) * (m.nz + 2 * L) for m in models)
+    win = [(m.nx, m.ny) for m in models]
+    del keep, shots
+    for m in models:
+        m._padded = {}
+    st = torch.cuda.ExternalStream(abi.lib.rsgpu_plan_stream(h))
+    ch = f["chunk"]
+    it = 0
+    for _ in range(args.warmup):
+        abi.check(abi.lib.rsgpu_plan_run(h, it, ch))
+        it += ch
+    abi.check(abi.lib.rsgpu_plan_sync(h))
+    l0 = abi.lib.rsgpu_plan_launch_count(h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            abi.check(abi.lib.rsgpu_plan_run(h, it, ch))
+            it += ch
+        e1.record(st)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    abi.check(abi.lib.rsgpu_plan_sync(h))
+    launches = abi.lib.rsgpu_plan_launch_count(h) - l0
+    abi.lib.rsgpu_plan_destroy(h)
+    value = pts * ch / (ms / 1e3) / 1e9
+    # algorithmic bytes per time step: velocity reads P,Vx,Vy,Vz,Rx,Ry,Rz, writes Vx,Vy,Vz (40 B);
+    # stress reads Vx,Vy,Vz,P,L, writes P (24 B)
+    peak, peak_kind = measured_peak()
+    achieved = 64.0 * pts * ch / (ms / 1e3) / 1e9
+    return {"metric": "Gpts/s", "value": round(value, 3), "unit": "Gpts/s", "ms_per_step": round(ms, 3),
+            "gpu_launches": int(launches), "padded_points_per_step": int(pts),
+            "window_sizes": {"min": min(win), "max": max(win)},
+            "roofline": {"bound": "hbm", "kernel": "a3d_velocity + a3d_stress (whole step)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_point_step": 64},
+            "clocks": clk.summary(), "models": models}
+
+
 # ---------------------------------------------------------------- distributed plumbing
 def dist_init(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -529,7 +666,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
-    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "fwi"],
+    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "fwi", "acoustic3d"],
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "fwi: the FWI gradient line alone")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
@@ -571,7 +708,37 @@ def main():
             print(json.dumps(line))
         return
 
+    if args.impl == "reference" and args.workload == "acoustic3d":
+        if int(os.environ.get("RANK", "0")) == 0:
+            from rockseis_b200 import abi
+            models, _, _ = a3d_batch(abi.F32_EXACT)
+            r = cpu_a3d_reference(models)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                return
+            print(json.dumps({"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "impl": "reference",
+                              "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1, "warmup": 0,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic", "config": a3d_config(), "cpu_baseline": r,
+                              "e2e": {"value": r["value"], "unit": "Gpts/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return
+
     rank, world, local = dist_init(args)
+    if args.workload == "acoustic3d":
+        import torch
+        torch.cuda.set_device(local)
+        r = run_a3d(args, device=local)
+        models = r.pop("models")
+        cpu = None if args.no_cpu_baseline else cpu_a3d_reference(models)
+        line = {"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dipping layers, windowed shots)",
+                "config": a3d_config(), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "clocks": r["clocks"], "acoustic3d": {k: v for k, v in r.items() if k not in ("roofline", "clocks")},
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+        return
     if args.workload == "fwi":
         if world > 1:
             raise SystemExit("the FWI gradient line is a one-GPU measurement")

@@ -93,6 +93,53 @@ class _Model:
     def getVpmax(self):
         return float(self.Vp.max())
 
+    # ---- aperture windows (Model::getLocalsize2d/3d, lib/model.cpp:272-470)
+    def _local_axis(self, s, g, aperture, use_src, d, o):
+        """Start and size of the local window along one axis.  The reference rounds
+        with rintf, i.e. in float after double arithmetic; so does this."""
+        f32 = np.float32
+        s = np.asarray(s, np.float64)
+        g = np.asarray(g, np.float64)
+        dd, oo, ap = float(f32(d)), float(f32(o)), float(f32(aperture))
+        if ap >= 0:
+            v = s if use_src else g
+            mn, mx = float(v.min()), float(v.max())
+            off = float(np.abs(g - s).max())
+            if ap > 0:
+                size = int(f32(np.rint(f32((mx - mn + ap) / dd))) + f32(1))
+                if size % 2 == 0:
+                    size += 1
+            else:
+                size = int(f32(2) * f32(np.rint(f32(off / dd))) + f32(1))
+            start = int(f32(np.rint(f32((mn - oo) / dd))) - f32((size - 1) // 2))
+        else:
+            mn, mx = float(min(s.min(), g.min())), float(max(s.max(), g.max()))
+            size = int(f32(np.rint(f32((mx - mn + 2 * abs(ap)) / dd))) + f32(2))
+            start = int(f32(np.rint(f32((mn - oo) / dd))) - f32(np.rint(f32(abs(ap / dd))))) - 1
+        return start, size
+
+    def getLocalsize2d(self, data, aperture, map_):
+        """(start, size) of the x window (Model::getLocalsize2d, lib/model.cpp:272-343)."""
+        return self._local_axis(data.scoords[:, 0], data.gcoords[:, 0], aperture, map_ == SMAP, self.dx, self.ox)
+
+    def getLocalsize3d(self, data, aperture_x, aperture_y, map_):
+        """((start_x, size_x), (start_y, size_y)) (Model::getLocalsize3d, lib/model.cpp:345-470)."""
+        return (self._local_axis(data.scoords[:, 0], data.gcoords[:, 0], aperture_x, map_ == SMAP, self.dx, self.ox),
+                self._local_axis(data.scoords[:, 1], data.gcoords[:, 1], aperture_y, map_ == SMAP, self.dy, self.oy))
+
+    def _origin(self, o, start, d):
+        """Origin of a local window, o + start*d evaluated in T as the reference does."""
+        t = self.dtype
+        return float(t(t(o) + t(t(start) * t(d))))
+
+    def _window(self, arr, sx, nxw, sy=0, nyw=1):
+        """Edge-clamped copy of a window (the copy loops of Model*::getLocal)."""
+        ix = np.clip(np.arange(sx, sx + nxw), 0, self.nx - 1)
+        if self.dim == 3:
+            iy = np.clip(np.arange(sy, sy + nyw), 0, self.ny - 1)
+            return np.ascontiguousarray(arr[:, iy][:, :, ix])
+        return np.ascontiguousarray(arr[:, ix])
+
 
 class ModelAcoustic2D(_Model):
     physics = abi.ACOUSTIC2D
@@ -111,6 +158,16 @@ class ModelAcoustic2D(_Model):
     def getRx(self): return self.padded()[0]
     def getRz(self): return self.padded()[1]
     def getL(self): return self.padded()[2]
+
+    def getLocal(self, data, aperture, map_):
+        """Local model around a shot's sources or receivers (ModelAcoustic2D::getLocal,
+        lib/model.cpp:1443-1509): window from getLocalsize2d, edge-clamped copy."""
+        sx, nxw = self.getLocalsize2d(data, aperture, map_)
+        m = ModelAcoustic2D(nxw, self.nz, self.lpml, self.dx, self.dz, self._origin(self.ox, sx, self.dx), self.oz,
+                            self.fs, self.precision)
+        m.createModel()
+        m.Vp[:], m.R[:] = self._window(self.Vp, sx, nxw), self._window(self.R, sx, nxw)
+        return m
 
 
 class ModelElastic2D(_Model):
@@ -135,6 +192,15 @@ class ModelElastic2D(_Model):
     def getL2M(self): return self.padded()[3]
     def getM(self): return self.padded()[4]
 
+    def getLocal(self, data, aperture, map_):
+        """ModelElastic2D::getLocal (lib/model.cpp:2840-2910)."""
+        sx, nxw = self.getLocalsize2d(data, aperture, map_)
+        m = ModelElastic2D(nxw, self.nz, self.lpml, self.dx, self.dz, self._origin(self.ox, sx, self.dx), self.oz,
+                           self.fs, self.precision)
+        m.createModel()
+        m.Vp[:], m.Vs[:], m.R[:] = (self._window(a, sx, nxw) for a in (self.Vp, self.Vs, self.R))
+        return m
+
 
 class ModelAcoustic3D(_Model):
     """ModelAcoustic3D<T> (include/model.h): arrays [nz][ny][nx]."""
@@ -157,6 +223,16 @@ class ModelAcoustic3D(_Model):
     def getRy(self): return self.padded()[1]
     def getRz(self): return self.padded()[2]
     def getL(self): return self.padded()[3]
+
+    def getLocal(self, data, aperture_x, aperture_y, map_):
+        """ModelAcoustic3D::getLocal (lib/model.cpp:2369-2450)."""
+        (sx, nxw), (sy, nyw) = self.getLocalsize3d(data, aperture_x, aperture_y, map_)
+        m = ModelAcoustic3D(nxw, nyw, self.nz, self.lpml, self.dx, self.dy, self.dz,
+                            self._origin(self.ox, sx, self.dx), self._origin(self.oy, sy, self.dy), self.oz,
+                            self.fs, self.precision)
+        m.createModel()
+        m.Vp[:], m.R[:] = self._window(self.Vp, sx, nxw, sy, nyw), self._window(self.R, sx, nxw, sy, nyw)
+        return m
 
 
 class Data2D:

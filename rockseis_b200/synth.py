@@ -95,3 +95,23 @@ def fwi_models(nx: int, nz: int, dx: float, seed=4, nanom=8, amp=0.08, smooth_m=
     vt = bg * (1.0 + pert)
     vs = _gauss_smooth(vt, smooth_m / dx)
     return vt.astype(dtype), vs.astype(dtype)
+
+
+def dipping_vp_3d(nx: int, ny: int, nz: int, dx: float, seed=5, vmin=1500.0, vmax=5000.0, ninterfaces=3,
+                  vclip=None, dtype=np.float32) -> np.ndarray:
+    """Layered 3D velocity [nz][ny][nx]: ninterfaces planar interfaces with seeded
+    dips, velocity stepping from vmin to vmax across them (clipped at vclip)."""
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz)[:, None, None] * dx
+    y = np.arange(ny)[None, :, None] * dx
+    x = np.arange(nx)[None, None, :] * dx
+    depth = nz * dx
+    layer = np.zeros((nz, ny, nx), np.int32)
+    for k in range(ninterfaces):
+        z0 = depth * (k + 1) / (ninterfaces + 1)
+        gx, gy = rng.uniform(-0.15, 0.15, 2)
+        layer += (z > z0 + gx * (x - nx * dx / 2) + gy * (y - ny * dx / 2)).astype(np.int32)
+    vp = vmin + (vmax - vmin) * layer / ninterfaces
+    if vclip is not None:
+        vp = np.minimum(vp, vclip)
+    return vp.astype(dtype)
