@@ -193,11 +193,15 @@ typedef struct {
     int reserved[10];
 } rsgpu_adjoint_opts;
 
-/* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332) or
- * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545).  `shot` carries the padded
- * model, the source (wavelet, SMAP maps) and the receiver maps (GMAP) exactly
- * as for rsgpu_modelling; src_field and rec_field must be RSGPU_PRESSURE.
- * Every output is ACCUMULATED (+=) and may be NULL when not wanted. */
+/* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332),
+ * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545) or FwiElastic2D::run_optimal
+ * (lib/fwi.cpp:3937-4143).  `shot` carries the padded model, the source
+ * (wavelet, SMAP maps) and the receiver maps (GMAP) exactly as for
+ * rsgpu_modelling.  Acoustic: src_field and rec_field are RSGPU_PRESSURE.
+ * Elastic: shot.rec_field is RSGPU_PRESSURE (the P data set) and the Ux/Uz sets
+ * (VX/VZ maps of the same receivers) are given by the *_vx / *_vz members; the
+ * reference requires all three data sets.  Every output is ACCUMULATED (+=) and
+ * may be NULL when not wanted. */
 typedef struct {
     rsgpu_shot shot;      /* shot.rec_out: FWI modelled data (datamodP), nrec*nt */
     const void *vp;       /* FWI: unpadded vp, nz*nx (ModelAcoustic2D::getVp) */
@@ -209,9 +213,19 @@ typedef struct {
     void *datares;        /* FWI: nrec*nt residuals (dataresP) */
     double *misfit;       /* FWI: one value, accumulated */
     void *image;          /* RTM: nhz*nhx*nz*nx (pimage, Image2D layout) */
+    /* elastic 2D only */
+    const int *gmap_vx, *gmap_vz;          /* GMAP of the Ux (VX) and Uz (VZ) data sets */
+    const void *gshift_vx, *gshift_vz;
+    const void *data_vx, *data_vz;         /* recorded Ux / Uz data, nrec*nt */
+    const void *vs;                        /* unpadded vs, nz*nx (scaleGrad) */
+    void *vsgrad;                          /* nz*nx */
+    void *datamod_vx, *datamod_vz;         /* modelled Ux / Uz data */
+    void *datares_vx, *datares_vz;         /* Ux / Uz residuals */
 } rsgpu_adjoint_shot;
 
-/* FwiAcoustic2D<float>::run_optimal for a batch of shots (DIFFERENCE misfit). */
+/* FwiAcoustic2D<float>::run_optimal (cfg->physics RSGPU_ACOUSTIC2D) or
+ * FwiElastic2D<float>::run_optimal (RSGPU_ELASTIC2D) for a batch of shots
+ * (DIFFERENCE misfit). */
 rsgpu_status rsgpu_fwi_gradient(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
                                 const rsgpu_adjoint_shot *shots);
 /* RtmAcoustic2D<float>::run_optimal for a batch of shots. */

@@ -144,6 +144,53 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     return r;
 }
 
+/* FwiElastic2D::run_optimal (lib/fwi.cpp:3937-4143) with P, Ux (VX) and Uz (VZ) data. */
+template <typename T>
+int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, const double *sc, const T *wav,
+            int sfield, int nr, const double *gc, const T *obsp, const T *obsx, const T *obsz, int ncheck, T *vpgrad,
+            T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit)
+{
+    auto model = make_e2d<T>(g, vp, vs, rho);
+    auto geom = model->getGeom();
+    auto src = make_data2d<T>(ns, g, sc, sfield, SMAP, geom, wav);
+    auto dp = make_data2d<T>(nr, g, gc, PRESSURE, GMAP, geom, obsp);
+    auto dx = make_data2d<T>(nr, g, gc, VX, GMAP, geom, obsx);
+    auto dz = make_data2d<T>(nr, g, gc, VZ, GMAP, geom, obsz);
+    const int fields[3] = {PRESSURE, VX, VZ};
+    std::shared_ptr<Data2D<T>> dm[3], dr[3];
+    for (int k = 0; k < 3; k++) {
+        dm[k] = make_data2d<T>(nr, g, gc, fields[k], GMAP, geom, nullptr);
+        dr[k] = make_data2d<T>(nr, g, gc, fields[k], GMAP, geom, nullptr);
+    }
+    auto wg = make_data2d<T>(ns, g, sc, sfield, SMAP, geom, nullptr);
+    std::shared_ptr<Image2D<T>> img[3];
+    for (int k = 0; k < 3; k++) {
+        img[k] = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
+        img[k]->allocateImage();
+    }
+    FwiElastic2D<T> fwi(model, src, dp, dx, dz, g->order, 1);
+    fwi.setDatamodP(dm[0]); fwi.setDatamodUx(dm[1]); fwi.setDatamodUz(dm[2]);
+    fwi.setDataresP(dr[0]); fwi.setDataresUx(dr[1]); fwi.setDataresUz(dr[2]);
+    fwi.setVpgrad(img[0]); fwi.setVsgrad(img[1]); fwi.setRhograd(img[2]);
+    fwi.setWavgrad(wg);
+    fwi.setMisfit_type(DIFFERENCE);
+    fwi.setNcheck(ncheck);
+    fwi.setIncore(true);
+    fwi.setSnapfile(tmpname("fwie2d"));
+    int r = fwi.run_optimal();
+    size_t n = (size_t)g->nx * g->nz, nd = (size_t)nr * g->nt;
+    std::memcpy(vpgrad, img[0]->getImagedata(), sizeof(T) * n);
+    std::memcpy(vsgrad, img[1]->getImagedata(), sizeof(T) * n);
+    std::memcpy(rhograd, img[2]->getImagedata(), sizeof(T) * n);
+    std::memcpy(wavgrad, wg->getData(), sizeof(T) * (size_t)ns * g->nt);
+    for (int k = 0; k < 3; k++) {
+        std::memcpy(mods + k * nd, dm[k]->getData(), sizeof(T) * nd);
+        std::memcpy(ress + k * nd, dr[k]->getData(), sizeof(T) * nd);
+    }
+    *misfit = (double)fwi.getMisfit();
+    return r;
+}
+
 /* nsteps of forwardstepVelocity / forwardstepStress / insertSource on a fresh
  * wavefield, state copied out field by field (step-level parity). */
 template <typename T>
@@ -358,6 +405,14 @@ int ref_mod_e3d_f(const ref_grid *g, const float *vp, const float *vs, const flo
                   float *out)
 { return mod_e3d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, rfield, out); }
 
+int ref_fwi_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
+                  const float *wav, int sfield, int nr, const double *gc, const float *obsp, const float *obsx,
+                  const float *obsz, int ncheck, float *vpgrad, float *vsgrad, float *rhograd, float *wavgrad,
+                  float *mods, float *ress, double *misfit)
+{
+    return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
+                          rhograd, wavgrad, mods, ress, misfit);
+}
 int ref_fwi_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                   const float *wav, int nr, const double *gc, const float *obs, int ncheck,
                   int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod,

@@ -663,3 +663,131 @@ int orc_mod_a3d(const orc_grid3 *g, const float *Rx, const float *Ry, const floa
     st3_free(&s);
     return 0;
 }
+
+/* ================================================================== elastic 2D FWI gradient
+ * FwiElastic2D::crossCorr (lib/fwi.cpp:2591-2775) on the interior 1..n-2 of the
+ * unpadded window: fw = forward Vx,Vz,Sxx,Szz,Sxz, bw = adjoint fields.  vpg holds
+ * the lambda correlation, vsg the mu correlation until scaleGrad. */
+static void e2d_corr(const orc_grid *g, int nx, int nz, const float *Rx, const float *Rz, float *const *fw,
+                     float *const *bw, float *vpg, float *vsg, float *rhog, int sfield, int ns, const int *smap,
+                     const float *sshift, float *wavgrad, int it)
+{
+    const int L = g->lpml, P = g->nxp;
+    const float dx = g->dx, dz = g->dz;
+    const float *wsx = fw[0], *wsz = fw[1], *wsxx = fw[2], *wszz = fw[3], *wsxz = fw[4];
+    const float *wrx = bw[0], *wrz = bw[1], *rsxx = bw[2], *rszz = bw[3], *rsxz = bw[4];
+    for (int ix = 1; ix < nx - 1; ix++)
+        for (int iz = 1; iz < nz - 1; iz++) {
+            long q = (long)(iz + L) * P + (ix + L), u = (long)iz * nx + ix;
+            float msxx = (wsx[q] - wsx[q - 1]) / dx;
+            float mszz = (wsz[q] - wsz[q - P]) / dz;
+            vpg[u] -= (msxx + mszz) * (rsxx[q] + rszz[q]);
+            float msxz1 = (wsx[q - 1] - wsx[q - 1 - P]) / dz + (wsz[q - P] - wsz[q - 1 - P]) / dx;
+            float msxz2 = (wsx[q] - wsx[q - P]) / dz + (wsz[q + 1 - P] - wsz[q - P]) / dx;
+            float msxz3 = (wsx[q - 1 + P] - wsx[q - 1]) / dz + (wsz[q] - wsz[q - 1]) / dx;
+            float msxz4 = (wsx[q + P] - wsx[q]) / dz + (wsz[q + 1] - wsz[q]) / dx;
+            float mrxz1 = rsxz[q - 1 - P], mrxz2 = rsxz[q - P], mrxz3 = rsxz[q - 1], mrxz4 = rsxz[q];
+            vsg[u] += (2.0) * (msxx * rszz[q] + mszz * rsxx[q]) -
+                      0.25 * (msxz1 * mrxz1 + msxz2 * mrxz2 + msxz3 * mrxz3 + msxz4 * mrxz4);
+            for (int i = 0; i < ns && wavgrad; i++) {
+                if (smap[2 * i] != ix || smap[2 * i + 1] != iz) continue;
+                float xt[2] = {1 - sshift[2 * i], sshift[2 * i]}, zt[2] = {1 - sshift[2 * i + 1], sshift[2 * i + 1]};
+                for (int i1 = 0; i1 < 2; i1++)
+                    for (int i2 = 0; i2 < 2; i2++) {
+                        long r = q + (long)i1 * P + i2;
+                        float v = sfield == 0 ? rsxx[r] + rszz[r] : sfield == 1 ? wrx[r] : wrz[r];
+                        wavgrad[it + (long)i * g->nt] += xt[i2] * zt[i1] * v;
+                    }
+            }
+            float uderx = 0.5 * wrx[q] * Rx[q] * (wsxx[q + 1] - wsxx[q]) / dx;
+            uderx += 0.5 * wrx[q - 1] * Rx[q - 1] * (wsxx[q] - wsxx[q - 1]) / dx;
+            uderx += 0.5 * wrx[q] * Rx[q] * (wsxz[q] - wsxz[q - P]) / dz;
+            uderx += 0.5 * wrx[q - 1] * Rx[q - 1] * (wsxz[q - 1] - wsxz[q - 1 - P]) / dz;
+            float uderz = 0.5 * wrz[q] * Rz[q] * (wsxz[q] - wsxz[q - 1]) / dx;
+            uderz += 0.5 * wrz[q - P] * Rz[q - P] * (wsxz[q - P] - wsxz[q - 1 - P]) / dx;
+            uderz += 0.5 * wrz[q] * Rz[q] * (wszz[q + P] - wszz[q]) / dz;
+            uderz += 0.5 * wrz[q - P] * Rz[q - P] * (wszz[q] - wszz[q - P]) / dz;
+            rhog[u] -= (uderx + uderz);
+        }
+}
+
+/* FwiElastic2D::scaleGrad (lib/fwi.cpp:2778-2849) */
+static void e2d_scale(int nx, int nz, const float *Vp, const float *Vs, const float *Rho, float *vpg, float *vsg,
+                      float *rhog)
+{
+    for (int ix = 0; ix < nx; ix++)
+        for (int iz = 0; iz < nz; iz++) {
+            long u = (long)iz * nx + ix;
+            float vpscale = 2.0 * Rho[u] * Vp[u];
+            float vsscale = 2.0 * Rho[u] * Vs[u];
+            float rhoscale1 = Vp[u] * Vp[u] - 2.0 * Vs[u] * Vs[u];
+            float rhoscale2 = Vs[u] * Vs[u];
+            float lambda = vpg[u], mu = vsg[u];
+            vpg[u] = vpscale * lambda;
+            vsg[u] = vsscale * mu - 2.0 * vsscale * lambda;
+            float rho = rhog[u];
+            rhog[u] = rhoscale1 * lambda + rhoscale2 * mu + rho;
+        }
+}
+
+/* FwiElastic2D::run_optimal with the DIFFERENCE misfit: P, Ux (VX) and Uz (VZ)
+ * data at the receivers; all forward states kept in memory.  maps: gmap[3] /
+ * gshift[3] for the P, VX and VZ trace sets; obs/mods/ress: [3][nr][nt]. */
+int orc_fwi_e2d(const orc_grid *g, int nx, int nz, const float *vp, const float *vs, const float *rho,
+                const float *Rx, const float *Rz, const float *Lm, const float *L2M, const float *M, const float *tab,
+                int ns, const int *smap, const float *sshift, const float *wav, int sfield, int nr,
+                const int *const *gmap, const float *const *gshift, const float *obs, float *vpg, float *vsg,
+                float *rhog, float *wavgrad, float *mods, float *ress, double *misfit)
+{
+    const int nt = g->nt;
+    const long n = (long)g->nxp * g->nzp, nd = (long)nr * nt;
+    float *Ps = malloc((size_t)nt * 5 * n * sizeof(float));
+    if (!Ps) return -1;
+    orc_state fw, bw;
+    st_alloc(&fw, g, 1);
+    st_alloc(&bw, g, 1);
+    const float *smod = sfield == 1 ? Rx : Rz;
+    for (int it = 0; it < nt; it++) {
+        e2d_vel(&fw, Rx, Rz, Lm, L2M, M, tab, 0);
+        e2d_str(&fw, Lm, L2M, M, tab, 0);
+        inject(&fw, smod, sfield, ns, smap, sshift, wav, it);
+        record(&fw, 0, nr, gmap[0], gshift[0], NULL, mods, it);
+        record(&fw, 1, nr, gmap[1], gshift[1], NULL, mods + nd, it);
+        record(&fw, 3, nr, gmap[2], gshift[2], NULL, mods + 2 * nd, it);
+        for (int k = 0; k < 5; k++) memcpy(Ps + ((size_t)it * 5 + k) * n, fw.f[k], n * sizeof(float));
+    }
+    /* computeMisfit / computeResiduals (lib/fwi.cpp:2852-2905, 3227-3290), DIFFERENCE */
+    float mis = 0.0f;
+    for (int tr = 0; tr < nr; tr++) {
+        const int valid = gmap[1][2 * tr] >= 0 && gmap[1][2 * tr + 1] >= 0;
+        for (int it = 0; it < nt; it++) {
+            long k = it + (long)tr * nt;
+            float rp = mods[k] - obs[k], rx = mods[nd + k] - obs[nd + k], rz = mods[2 * nd + k] - obs[2 * nd + k];
+            if (valid) mis += 0.5 * (rp * rp + rx * rx + rz * rz);
+            ress[k] = rp;
+            ress[nd + k] = rx;
+            ress[2 * nd + k] = rz;
+        }
+    }
+    *misfit = mis;
+    float *zero = calloc(5 * n, sizeof(float));
+    for (int it = nt - 1; it >= 0; it--) {
+        if (it < nt - 1) {
+            e2d_vel(&bw, Rx, Rz, Lm, L2M, M, tab, 1);
+            e2d_str(&bw, Lm, L2M, M, tab, 1);
+        }
+        inject(&bw, NULL, 0, nr, gmap[0], gshift[0], ress, it);
+        inject(&bw, Rx, 1, nr, gmap[1], gshift[1], ress + nd, it);
+        inject(&bw, Rz, 3, nr, gmap[2], gshift[2], ress + 2 * nd, it);
+        const float *st = it == nt - 1 ? Ps + (size_t)it * 5 * n : it == 0 ? zero : Ps + (size_t)(it - 1) * 5 * n;
+        float *fwf[5];
+        for (int k = 0; k < 5; k++) fwf[k] = (float *)st + k * n;
+        e2d_corr(g, nx, nz, Rx, Rz, fwf, bw.f, vpg, vsg, rhog, sfield, ns, smap, sshift, wavgrad, it);
+    }
+    e2d_scale(nx, nz, vp, vs, rho, vpg, vsg, rhog);
+    free(zero);
+    st_free(&fw);
+    st_free(&bw);
+    free(Ps);
+    return 0;
+}

@@ -57,7 +57,11 @@ class AdjointOpts(C.Structure):
 class AdjointShot(C.Structure):
     _fields_ = [("shot", Shot), ("vp", C.c_void_p), ("rho", C.c_void_p), ("data", C.c_void_p),
                 ("vpgrad", C.c_void_p), ("rhograd", C.c_void_p), ("wavgrad", C.c_void_p), ("datares", C.c_void_p),
-                ("misfit", C.POINTER(C.c_double)), ("image", C.c_void_p)]
+                ("misfit", C.POINTER(C.c_double)), ("image", C.c_void_p),
+                ("gmap_vx", C.c_void_p), ("gmap_vz", C.c_void_p), ("gshift_vx", C.c_void_p), ("gshift_vz", C.c_void_p),
+                ("data_vx", C.c_void_p), ("data_vz", C.c_void_p), ("vs", C.c_void_p), ("vsgrad", C.c_void_p),
+                ("datamod_vx", C.c_void_p), ("datamod_vz", C.c_void_p), ("datares_vx", C.c_void_p),
+                ("datares_vz", C.c_void_p)]
 
 
 def _load() -> C.CDLL:

@@ -281,7 +281,7 @@ void Adjoint::build_desc(std::vector<unsigned char> &corr, std::vector<unsigned 
             r.obs = (const T *)D(o_obs[i]);
             r.res = (T *)(ba + B.wav);
             // the forward plan's receiver plan marks off-grid receivers with -1
-            r.rec_pt = (const int *)(fa + fw->rec_pt_offsets[i]);
+            r.rec_pt = (const int *)(fa + fw->rec_pt_offsets[(size_t)i * MAXSETS]);
         }
         r.nrec = nrec[i];
         r.nt = cfg.nt;

@@ -167,6 +167,159 @@ __global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, d
     }
 }
 
+// ---------------------------------------------------------------- elastic FWI
+// 0.5 * w * r * dd / h  in double, rounded to T (the reference's mixed-type expression)
+template <typename T>
+__device__ __forceinline__ double half_term(T w, T r, T dd, double h)
+{
+    return __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)w), (double)r), (double)dd), h);
+}
+
+// FwiElastic2D::crossCorr (lib/fwi.cpp:2591-2775) on the interior 1..n-2:
+//   g0 -= (Dx Vx_fw + Dz Vz_fw) (Sxx_bw + Szz_bw)                     (lambda)
+//   g1 += 2 (Dx Vx Szz + Dz Vz Sxx) - 1/4 sum of 4 Sxz corner products (mu)
+//   g2 -= sum of staggered velocity-stress products                     (rho)
+template <typename T, bool EXACT, typename G>
+__global__ void __launch_bounds__(256) corr_fwi_e2d(const Corr2DE<T> *desc, T dx, T dz)
+{
+    const Corr2DE<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix < 1 || iz < 1 || ix >= c.nx - 1 || iz >= c.nz - 1) return;
+    const long q = (long)(iz + c.lpml) * c.pitch + ix + c.lpml;
+    const long u = (long)iz * c.nx + ix;
+    const int P = c.pitch;
+    const T *wsx = c.ws[0], *wsz = c.ws[1], *wsxx = c.ws[2], *wszz = c.ws[3], *wsxz = c.ws[4];
+    const T *wrx = c.wr[0], *wrz = c.wr[1], *rsxx = c.wr[2], *rszz = c.wr[3], *rsxz = c.wr[4];
+    G *g0 = (G *)c.g[0] + u, *g1 = (G *)c.g[1] + u, *g2 = (G *)c.g[2] + u;
+    T a, rh;
+    double mu;
+    if (EXACT) {
+        using O = X<T>;
+        const T msxx = O::div(O::sub(wsx[q], wsx[q - 1]), dx);
+        const T mszz = O::div(O::sub(wsz[q], wsz[q - P]), dz);
+        a = O::mul(O::add(msxx, mszz), O::add(rsxx[q], rszz[q]));
+        const T m1 = O::add(O::div(O::sub(wsx[q - 1], wsx[q - 1 - P]), dz), O::div(O::sub(wsz[q - P], wsz[q - 1 - P]), dx));
+        const T m2 = O::add(O::div(O::sub(wsx[q], wsx[q - P]), dz), O::div(O::sub(wsz[q + 1 - P], wsz[q - P]), dx));
+        const T m3 = O::add(O::div(O::sub(wsx[q - 1 + P], wsx[q - 1]), dz), O::div(O::sub(wsz[q], wsz[q - 1]), dx));
+        const T m4 = O::add(O::div(O::sub(wsx[q + P], wsx[q]), dz), O::div(O::sub(wsz[q + 1], wsz[q]), dx));
+        const T t1 = O::add(O::mul(msxx, rszz[q]), O::mul(mszz, rsxx[q]));
+        const T t2 = O::add(O::add(O::add(O::mul(m1, rsxz[q - 1 - P]), O::mul(m2, rsxz[q - P])), O::mul(m3, rsxz[q - 1])),
+                            O::mul(m4, rsxz[q]));
+        mu = __dsub_rn(__dmul_rn(2.0, (double)t1), __dmul_rn(0.25, (double)t2));
+        const double DX = (double)dx, DZ = (double)dz;
+        T ux = O::rnd(half_term(wrx[q], c.rx[q], O::sub(wsxx[q + 1], wsxx[q]), DX));
+        ux = O::rnd(__dadd_rn((double)ux, half_term(wrx[q - 1], c.rx[q - 1], O::sub(wsxx[q], wsxx[q - 1]), DX)));
+        ux = O::rnd(__dadd_rn((double)ux, half_term(wrx[q], c.rx[q], O::sub(wsxz[q], wsxz[q - P]), DZ)));
+        ux = O::rnd(__dadd_rn((double)ux, half_term(wrx[q - 1], c.rx[q - 1], O::sub(wsxz[q - 1], wsxz[q - 1 - P]), DZ)));
+        T uz = O::rnd(half_term(wrz[q], c.rz[q], O::sub(wsxz[q], wsxz[q - 1]), DX));
+        uz = O::rnd(__dadd_rn((double)uz, half_term(wrz[q - P], c.rz[q - P], O::sub(wsxz[q - P], wsxz[q - 1 - P]), DX)));
+        uz = O::rnd(__dadd_rn((double)uz, half_term(wrz[q], c.rz[q], O::sub(wszz[q + P], wszz[q]), DZ)));
+        uz = O::rnd(__dadd_rn((double)uz, half_term(wrz[q - P], c.rz[q - P], O::sub(wszz[q], wszz[q - P]), DZ)));
+        rh = O::add(ux, uz);
+    } else {
+        const T rdx = T(1) / dx, rdz = T(1) / dz;
+        const T msxx = (wsx[q] - wsx[q - 1]) * rdx, mszz = (wsz[q] - wsz[q - P]) * rdz;
+        a = (msxx + mszz) * (rsxx[q] + rszz[q]);
+        const T m1 = (wsx[q - 1] - wsx[q - 1 - P]) * rdz + (wsz[q - P] - wsz[q - 1 - P]) * rdx;
+        const T m2 = (wsx[q] - wsx[q - P]) * rdz + (wsz[q + 1 - P] - wsz[q - P]) * rdx;
+        const T m3 = (wsx[q - 1 + P] - wsx[q - 1]) * rdz + (wsz[q] - wsz[q - 1]) * rdx;
+        const T m4 = (wsx[q + P] - wsx[q]) * rdz + (wsz[q + 1] - wsz[q]) * rdx;
+        mu = (double)(T(2) * (msxx * rszz[q] + mszz * rsxx[q]) -
+                      T(0.25) * (m1 * rsxz[q - 1 - P] + m2 * rsxz[q - P] + m3 * rsxz[q - 1] + m4 * rsxz[q]));
+        const T ux = wrx[q] * c.rx[q] * ((wsxx[q + 1] - wsxx[q]) * rdx + (wsxz[q] - wsxz[q - P]) * rdz) +
+                     wrx[q - 1] * c.rx[q - 1] * ((wsxx[q] - wsxx[q - 1]) * rdx + (wsxz[q - 1] - wsxz[q - 1 - P]) * rdz);
+        const T uz = wrz[q] * c.rz[q] * ((wsxz[q] - wsxz[q - 1]) * rdx + (wszz[q + P] - wszz[q]) * rdz) +
+                     wrz[q - P] * c.rz[q - P] * ((wsxz[q - P] - wsxz[q - 1 - P]) * rdx + (wszz[q] - wszz[q - P]) * rdz);
+        rh = T(0.5) * (ux + uz);
+    }
+    if (sizeof(G) == sizeof(T)) {
+        using O = X<T>;
+        *(T *)g0 = EXACT ? O::sub(*(T *)g0, a) : *(T *)g0 - a;
+        *(T *)g1 = O::rnd(__dadd_rn((double)*(T *)g1, mu));
+        *(T *)g2 = EXACT ? O::sub(*(T *)g2, rh) : *(T *)g2 - rh;
+    } else {
+        *g0 = __dsub_rn((double)*g0, (double)a);
+        *g1 = __dadd_rn((double)*g1, mu);
+        *g2 = __dsub_rn((double)*g2, (double)rh);
+    }
+}
+
+// FwiElastic2D::scaleGrad (lib/fwi.cpp:2778-2849): lambda/mu/rho correlations to
+// vp/vs/rho gradients, over the whole window.
+template <typename T, typename G>
+__global__ void __launch_bounds__(256) scale_grad_e2d(const Corr2DE<T> *desc)
+{
+    const Corr2DE<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= c.nx || iz >= c.nz) return;
+    const long u = (long)iz * c.nx + ix;
+    const T vp = c.vp[u], vs = c.vs[u], rho = c.rho[u];
+    G *g0 = (G *)c.g[0] + u, *g1 = (G *)c.g[1] + u, *g2 = (G *)c.g[2] + u;
+    if (sizeof(G) == sizeof(T)) {
+        using O = X<T>;
+        const T vpscale = O::rnd(__dmul_rn(__dmul_rn(2.0, (double)rho), (double)vp));
+        const T vsscale = O::rnd(__dmul_rn(__dmul_rn(2.0, (double)rho), (double)vs));
+        const T rs1 = O::rnd(__dsub_rn((double)O::mul(vp, vp), __dmul_rn(__dmul_rn(2.0, (double)vs), (double)vs)));
+        const T rs2 = O::mul(vs, vs);
+        const T lambda = *(T *)g0, mu = *(T *)g1, r = *(T *)g2;
+        *(T *)g0 = O::mul(vpscale, lambda);
+        *(T *)g1 = O::rnd(__dsub_rn((double)O::mul(vsscale, mu), __dmul_rn(__dmul_rn(2.0, (double)vsscale), (double)lambda)));
+        *(T *)g2 = O::add(O::add(O::mul(rs1, lambda), O::mul(rs2, mu)), r);
+    } else {
+        const double dvp = vp, dvs = vs, drho = rho;
+        const double vpscale = 2.0 * drho * dvp, vsscale = 2.0 * drho * dvs;
+        const double lambda = *g0, mu = *g1, r = *g2;
+        *g0 = vpscale * lambda;
+        *g1 = vsscale * mu - 2.0 * vsscale * lambda;
+        *g2 = (dvp * dvp - 2.0 * dvs * dvs) * lambda + dvs * dvs * mu + r;
+    }
+}
+
+// FwiElastic2D::computeResiduals / computeMisfit, DIFFERENCE (lib/fwi.cpp:2852-2905, 3227-3290)
+template <typename T, int ACC>
+__global__ void __launch_bounds__(256) residual_misfit_e2d(const Resid2DE<T> *desc, double *misfit)
+{
+    const Resid2DE<T> d = desc[blockIdx.x];
+    const long n = (long)d.nrec * d.nt;
+    for (int k = 0; k < 3; k++)
+        for (long j = threadIdx.x; j < n; j += blockDim.x) d.res[k][j] = X<T>::sub(d.mod[k][j], d.obs[k][j]);
+    if (ACC == ACC_REF) {
+        __syncthreads();
+        if (threadIdx.x != 0) return;
+        // misfit += 0.5*(rp*rp + rx*rx + rz*rz): squares summed in T, then added in double
+        T mis = 0;
+        for (int tr = 0; tr < d.nrec; tr++) {
+            if (d.rec_pt_vx[tr] < 0) continue;
+            for (int it = 0; it < d.nt; it++) {
+                const long j = (long)tr * d.nt + it;
+                const T rp = d.res[0][j], rx = d.res[1][j], rz = d.res[2][j];
+                const T s = X<T>::add(X<T>::add(X<T>::mul(rp, rp), X<T>::mul(rx, rx)), X<T>::mul(rz, rz));
+                mis = X<T>::rnd(__dadd_rn((double)mis, __dmul_rn(0.5, (double)s)));
+            }
+        }
+        misfit[blockIdx.x] = (double)mis;
+    } else {
+        double acc = 0.0;
+        for (long j = threadIdx.x; j < n; j += blockDim.x) {
+            if (d.rec_pt_vx[j / d.nt] < 0) continue;
+            for (int k = 0; k < 3; k++) {
+                const double r = (double)X<T>::sub(d.mod[k][j], d.obs[k][j]);
+                acc = fma(0.5 * r, r, acc);
+            }
+        }
+        __shared__ double red[256];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) misfit[blockIdx.x] = red[0];
+    }
+}
+
 // ---------------------------------------------------------------- checkpoints
 template <typename S> struct Store;
 template <> struct Store<__half> {
@@ -323,6 +476,44 @@ cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, dou
     } else {
         if (acc == ACC_F64) residual_misfit<float, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
         else residual_misfit<float, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_fwi_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
+                                double dz, cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nzmax + 7) / 8, nshots);
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) corr_fwi_e2d<double, true, double><<<grid, block, 0, st>>>((const Corr2DE<double> *)desc, dx, dz);
+        else corr_fwi_e2d<double, true, double><<<grid, block, 0, st>>>((const Corr2DE<double> *)desc, dx, dz);
+    } else if (prec == PREC_F32_EXACT) {
+        if (acc == ACC_F64) corr_fwi_e2d<float, true, double><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc, (float)dx, (float)dz);
+        else corr_fwi_e2d<float, true, float><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc, (float)dx, (float)dz);
+    } else {
+        if (acc == ACC_F64) corr_fwi_e2d<float, false, double><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc, (float)dx, (float)dz);
+        else corr_fwi_e2d<float, false, float><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc, (float)dx, (float)dz);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nzmax + 7) / 8, nshots);
+    if (prec == PREC_F64) scale_grad_e2d<double, double><<<grid, block, 0, st>>>((const Corr2DE<double> *)desc);
+    else if (acc == ACC_F64) scale_grad_e2d<float, double><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc);
+    else scale_grad_e2d<float, float><<<grid, block, 0, st>>>((const Corr2DE<float> *)desc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_e2d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st)
+{
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) residual_misfit_e2d<double, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2DE<double> *)desc, misfit);
+        else residual_misfit_e2d<double, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2DE<double> *)desc, misfit);
+    } else {
+        if (acc == ACC_F64) residual_misfit_e2d<float, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2DE<float> *)desc, misfit);
+        else residual_misfit_e2d<float, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2DE<float> *)desc, misfit);
     }
     return cudaGetLastError();
 }

@@ -806,14 +806,17 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
     const InjRec<T> &pl = plans[blockIdx.x];
     const int it_step = it_base + (it_dev ? *it_dev : 0);
     const int it = pl.rev ? pl.nt - 1 - it_step : it_step;
-    if (pl.kind_inj != INJ_NONE) {
-        for (int q = threadIdx.x; q < pl.ninj; q += blockDim.x) {
-            const int p = pl.inj_pt[q];
-            if (pl.kind_inj == INJ_E2_P) {
+    for (int set = 0; set < pl.ninjsets; set++) {
+        const InjSet<T> &q = pl.inj[set];
+        if (q.kind == INJ_NONE) continue;
+        if (set > 0) __syncthreads();   // sets that touch the same field add in set order
+        for (int j = threadIdx.x; j < q.ninj; j += blockDim.x) {
+            const int p = q.pt[j];
+            if (q.kind == INJ_E2_P) {
                 T sxx = sh.f[E2_SXX][p], szz = sh.f[E2_SZZ][p];
-                for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
-                    const T w = pl.wav[(long)pl.inj_trace[c] * pl.nt + it];
-                    const T s = A::mul(A::mul(A::mul(dt, w), pl.inj_wx[c]), pl.inj_wz[c]);
+                for (int c = q.start[j]; c < q.start[j + 1]; c++) {
+                    const T w = q.wav[(long)q.trace[c] * pl.nt + it];
+                    const T s = A::mul(A::mul(A::mul(dt, w), q.wx[c]), q.wz[c]);
                     sxx = A::sub(sxx, s);
                     szz = A::sub(szz, s);
                 }
@@ -821,7 +824,7 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
                 sh.f[E2_SZZ][p] = szz;
             } else {
                 T *F; const T *Mod;
-                switch (pl.kind_inj) {
+                switch (q.kind) {
                 case INJ_A2_P: F = sh.f[A2_P]; Mod = sh.m[M_L]; break;
                 case INJ_A2_VX: F = sh.f[A2_VX]; Mod = sh.m[M_RX]; break;
                 case INJ_A2_VZ: F = sh.f[A2_VZ]; Mod = sh.m[M_RZ]; break;
@@ -830,49 +833,61 @@ __global__ void inject_record_2d(const Shot2D<T> *shots, const InjRec<T> *plans,
                 }
                 T v = F[p];
                 const T dm = A::mul(dt, Mod[p]);
-                for (int c = pl.inj_start[q]; c < pl.inj_start[q + 1]; c++) {
-                    const T w = pl.wav[(long)pl.inj_trace[c] * pl.nt + it];
-                    v = A::add(v, A::mul(A::mul(A::mul(dm, w), pl.inj_wx[c]), pl.inj_wz[c]));
+                for (int c = q.start[j]; c < q.start[j + 1]; c++) {
+                    const T w = q.wav[(long)q.trace[c] * pl.nt + it];
+                    v = A::add(v, A::mul(A::mul(A::mul(dm, w), q.wx[c]), q.wz[c]));
                 }
                 F[p] = v;
             }
         }
     }
-    if (pl.kind_rec == REC_NONE || (pl.rec_gate && *pl.rec_gate == 0)) return;
+    if (pl.nrecsets == 0 || (pl.rec_gate && *pl.rec_gate == 0)) return;
     __syncthreads();
-    for (int tr = threadIdx.x; tr < pl.nrec; tr += blockDim.x) {
-        const int p = pl.rec_pt[tr];
-        if (p < 0) continue;
-        const T wx0 = pl.rec_w[4 * tr], wx1 = pl.rec_w[4 * tr + 1];
-        const T wz0 = pl.rec_w[4 * tr + 2], wz1 = pl.rec_w[4 * tr + 3];
-        const int off[4] = {0, 1, sh.pitch, sh.pitch + 1};
-        const T wx[4] = {wx0, wx1, wx0, wx1}, wz[4] = {wz0, wz0, wz1, wz1};
-        T *out = pl.rec_out + (long)tr * pl.nt + it;
-        if (pl.kind_rec == REC_E2_P) {
-            // (1./2.)*xtri*ytri*F/factor is evaluated in double by the reference and
-            // added to the T-typed trace sample (lib/waves.cpp:2240-2241)
-            const double fac = pl.rec_factor ? (double)pl.rec_factor[tr] : 1.0;
-            T acc = *out;
+    for (int set = 0; set < pl.nrecsets; set++) {
+        const RecSet<T> &q = pl.rec[set];
+        if (q.kind == REC_NONE) continue;
+        for (int tr = threadIdx.x; tr < q.nrec; tr += blockDim.x) {
+            const int p = q.pt[tr];
+            if (p < 0) continue;
+            const T wx0 = q.w[4 * tr], wx1 = q.w[4 * tr + 1];
+            const T wz0 = q.w[4 * tr + 2], wz1 = q.w[4 * tr + 3];
+            const int off[4] = {0, 1, sh.pitch, sh.pitch + 1};
+            const T wx[4] = {wx0, wx1, wx0, wx1}, wz[4] = {wz0, wz0, wz1, wz1};
+            T *out = q.out + (long)tr * pl.nt + it;
+            if (q.kind == REC_E2_P) {
+                // (1./2.)*xtri*ytri*F/factor is evaluated in double by the reference and
+                // added to the T-typed trace sample (lib/waves.cpp:2238-2239)
+                const double fac = (double)q.factor[tr];
+                T acc = *out;
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const double w = __dmul_rn(__dmul_rn(0.5, (double)wx[c]), (double)wz[c]);
-                acc = (T)__dadd_rn((double)acc, __ddiv_rn(__dmul_rn(w, (double)sh.f[E2_SXX][p + off[c]]), fac));
-                acc = (T)__dadd_rn((double)acc, __ddiv_rn(__dmul_rn(w, (double)sh.f[E2_SZZ][p + off[c]]), fac));
-            }
-            *out = acc;
-        } else {
-            const T *F;
-            switch (pl.kind_rec) {
-            case REC_A2_P: F = sh.f[A2_P]; break;
-            case REC_A2_VX: F = sh.f[A2_VX]; break;
-            case REC_A2_VZ: F = sh.f[A2_VZ]; break;
-            case REC_E2_VX: F = sh.f[E2_VX]; break;
-            default: F = sh.f[E2_VZ]; break;
-            }
-            T acc = *out;
+                for (int c = 0; c < 4; c++) {
+                    const double w = __dmul_rn(__dmul_rn(0.5, (double)wx[c]), (double)wz[c]);
+                    acc = (T)__dadd_rn((double)acc, __ddiv_rn(__dmul_rn(w, (double)sh.f[E2_SXX][p + off[c]]), fac));
+                    acc = (T)__dadd_rn((double)acc, __ddiv_rn(__dmul_rn(w, (double)sh.f[E2_SZZ][p + off[c]]), fac));
+                }
+                *out = acc;
+            } else {
+                if (q.kind == REC_E2_PSUM) {
+                    T acc = *out;
 #pragma unroll
-            for (int c = 0; c < 4; c++) acc = A::add(acc, A::mul(A::mul(wx[c], wz[c]), F[p + off[c]]));
-            *out = acc;
+                    for (int c = 0; c < 4; c++)
+                        acc = A::add(acc, A::mul(A::mul(wx[c], wz[c]), A::add(sh.f[E2_SXX][p + off[c]], sh.f[E2_SZZ][p + off[c]])));
+                    *out = acc;
+                    continue;
+                }
+                const T *F;
+                switch (q.kind) {
+                case REC_A2_P: F = sh.f[A2_P]; break;
+                case REC_A2_VX: F = sh.f[A2_VX]; break;
+                case REC_A2_VZ: F = sh.f[A2_VZ]; break;
+                case REC_E2_VX: F = sh.f[E2_VX]; break;
+                default: F = sh.f[E2_VZ]; break;
+                }
+                T acc = *out;
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc = A::add(acc, A::mul(A::mul(wx[c], wz[c]), F[p + off[c]]));
+                *out = acc;
+            }
         }
     }
 }

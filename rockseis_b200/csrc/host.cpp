@@ -145,7 +145,7 @@ Plan::~Plan()
     if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
-rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s)
+rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s, bool sets_given)
 {
     if (!c || !s || ns < 1) { set_error("null config/shots or nshots < 1"); return RSGPU_ERR_ARG; }
     if (c->physics < 0 || c->physics > 3) { set_error("bad physics %d", c->physics); return RSGPU_ERR_ARG; }
@@ -163,6 +163,7 @@ rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot 
         if (nxp <= order || nzp <= order) { set_error("shot %d: padded grid smaller than stencil", i); return RSGPU_ERR_ARG; }
         for (int k = 0; k < nparams(c->physics); k++)
             if (!s[i].model[k]) { set_error("shot %d: model parameter %d is null", i, k); return RSGPU_ERR_ARG; }
+        if (sets_given) continue;   // trace sets are checked by check_sets
         if (s[i].nsrc < 0 || s[i].nrec < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
         if (s[i].nsrc > 0 && (!s[i].smap || !s[i].sshift || !s[i].wavelet)) {
             set_error("shot %d: source arrays missing", i);
@@ -180,12 +181,52 @@ rsgpu_status Plan::check_config(const rsgpu_config *c, int ns, const rsgpu_shot 
 }
 
 // Build the device arena layout and upload everything.
-rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
+// Trace sets of one shot as the plan consumes them: the rsgpu_shot's single source
+// and receiver set, or the sets an adjoint driver supplies.
+static ShotSets sets_of(const rsgpu_shot &s)
 {
-    rsgpu_status st = check_config(c, ns, s);
+    ShotSets t;
+    t.nsrc = 1;
+    t.src[0].n = s.nsrc; t.src[0].map = s.smap; t.src[0].shift = s.sshift; t.src[0].field = s.src_field;
+    t.src[0].data = s.wavelet;
+    if (s.nrec > 0) {
+        t.nrec = 1;
+        t.rec[0].n = s.nrec; t.rec[0].map = s.gmap; t.rec[0].shift = s.gshift; t.rec[0].field = s.rec_field;
+        t.rec[0].factor = s.rec_factor;
+    }
+    return t;
+}
+
+static rsgpu_status check_sets(int i, const ShotSets &t)
+{
+    if (t.nsrc < 0 || t.nsrc > MAXSETS || t.nrec < 0 || t.nrec > MAXSETS) { set_error("shot %d: bad trace-set count", i); return RSGPU_ERR_ARG; }
+    for (int k = 0; k < t.nsrc; k++) {
+        const TraceSet &q = t.src[k];
+        if (q.n < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
+        if (q.n > 0 && (!q.map || !q.shift || !q.data)) { set_error("shot %d: source arrays missing", i); return RSGPU_ERR_ARG; }
+        if (q.field != RSGPU_PRESSURE && q.field != RSGPU_VX && q.field != RSGPU_VZ) { set_error("shot %d: bad source field", i); return RSGPU_ERR_ARG; }
+    }
+    for (int k = 0; k < t.nrec; k++) {
+        const TraceSet &q = t.rec[k];
+        if (q.n < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
+        if (q.n > 0 && (!q.map || !q.shift)) { set_error("shot %d: receiver arrays missing", i); return RSGPU_ERR_ARG; }
+        if (q.field != RSGPU_PRESSURE && q.field != RSGPU_VX && q.field != RSGPU_VZ) { set_error("shot %d: bad receiver field", i); return RSGPU_ERR_ARG; }
+    }
+    return RSGPU_OK;
+}
+
+rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, const ShotSets *sets_in)
+{
+    rsgpu_status st = check_config(c, ns, s, sets_in != nullptr);
     if (st != RSGPU_OK) return st;
+    std::vector<ShotSets> sets(ns);
+    for (int i = 0; i < ns; i++) {
+        sets[i] = sets_in ? sets_in[i] : sets_of(s[i]);
+        if ((st = check_sets(i, sets[i])) != RSGPU_OK) return st;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
         set_error("no CUDA device");
         return RSGPU_ERR_NODEVICE;
     }
@@ -207,9 +248,10 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     // ---- per-shot layout (byte offsets into the arena)
     shots.resize(ns);
     size_t off = 0;
-    auto take = [&](size_t bytes) { size_t o = off; off = rup(off + bytes, 256); return o; };
+    auto take = [&](size_t bytes) { size_t o = off; off = rup(off + std::max<size_t>(bytes, 1), 256); return o; };
     for (int i = 0; i < ns; i++) {
         ShotLayout &L = shots[i];
+        const ShotSets &t = sets[i];
         L.nx = s[i].nx; L.nz = s[i].nz;
         L.nxp = s[i].nx + 2 * lp; L.nzp = s[i].nz + 2 * lp;
         L.pitch = (int)rup(GUARD + rup(L.nxp, 128) + GUARD, 32);
@@ -220,87 +262,106 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         for (int k = 0; k < npsi(phys); k++) L.psix[k] = take((size_t)L.nzp * 2 * lp * es);
         for (int k = 0; k < npsi(phys); k++) L.psiz[k] = take((size_t)2 * lp * L.nxp * es);
         L.psi_end = off;
-        L.nrec = s[i].nrec;
-        L.nsrc = s[i].nsrc;
-        L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
+        L.nrecsets = t.nrec;
+        L.nsrcsets = t.nsrc;
+        for (int k = 0; k < t.nrec; k++) {
+            L.nrecs[k] = t.rec[k].n;
+            L.tracesk[k] = take((size_t)t.rec[k].n * cfg.nt * es);
+        }
+        if (t.nrec == 0) L.tracesk[0] = take(0);
+        L.nrec = t.nrec > 0 ? t.rec[0].n : 0;
+        L.traces = L.tracesk[0];
         L.field_begin = L.f[0];
         L.state_end = off;
         // constant inputs
         for (int k = 0; k < nparams(phys); k++) L.m[k] = take(fbytes);
-        L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
+        for (int k = 0; k < t.nsrc; k++) {
+            L.nsrcs[k] = t.src[k].n;
+            L.wavk[k] = take((size_t)t.src[k].n * cfg.nt * es);
+        }
+        if (t.nsrc == 0) L.wavk[0] = take(0);
+        L.nsrc = t.nsrc > 0 ? t.src[0].n : 0;
+        L.wav = L.wavk[0];
     }
     state_end = off;   // everything above is state or data; plan tables follow
-    // ---- injection / recording plans
-    std::vector<std::vector<int>> inj_pt(ns), inj_start(ns), inj_tr(ns), rec_pt(ns);
-    std::vector<std::vector<double>> inj_wx(ns), inj_wz(ns), rec_w(ns), rec_fac(ns);
+    // ---- injection / recording plans, one per trace set
+    struct InjPlan { std::vector<int> pt, start, tr; std::vector<double> wx, wz; };
+    struct RecPlan { std::vector<int> pt; std::vector<double> w, fac; };
+    std::vector<InjPlan> inj((size_t)ns * MAXSETS);
+    std::vector<RecPlan> rec((size_t)ns * MAXSETS);
+    auto shift_at = [&](const void *p, int k) -> double {
+        return prec == PREC_F64 ? ((const double *)p)[k] : (double)((const float *)p)[k];
+    };
+    auto tri = [&](double sft, double *w) {
+        if (prec == PREC_F64) { w[0] = 1 - sft; w[1] = sft; }
+        else { w[0] = (float)(1 - (float)sft); w[1] = (float)sft; }
+    };
     for (int i = 0; i < ns; i++) {
         const ShotLayout &L = shots[i];
-        // contributions in reference loop order: trace, z-corner, x-corner
-        std::map<int, std::vector<std::pair<int, std::pair<double, double>>>> per_pt;
-        std::vector<int> order_pts;
-        for (int t = 0; t < s[i].nsrc; t++) {
-            const int mx = s[i].smap[2 * t], mz = s[i].smap[2 * t + 1];
-            if (mx < 0 || mz < 0) continue;
-            double sx, sz;
-            if (prec == PREC_F64) { sx = ((const double *)s[i].sshift)[2 * t]; sz = ((const double *)s[i].sshift)[2 * t + 1]; }
-            else { sx = ((const float *)s[i].sshift)[2 * t]; sz = ((const float *)s[i].sshift)[2 * t + 1]; }
-            double xt[2], zt[2];
-            if (prec == PREC_F64) { xt[0] = 1 - sx; xt[1] = sx; zt[0] = 1 - sz; zt[1] = sz; }
-            else { xt[0] = (float)(1 - (float)sx); xt[1] = (float)sx; zt[0] = (float)(1 - (float)sz); zt[1] = (float)sz; }
-            for (int i1 = 0; i1 < 2; i1++)
-                for (int i2 = 0; i2 < 2; i2++) {
-                    const int ix = lp + mx + i2, iz = lp + mz + i1;
-                    if (ix >= L.nxp || iz >= L.nzp) { set_error("shot %d: source %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
-                    const int p = iz * L.pitch + ix;
-                    if (!per_pt.count(p)) order_pts.push_back(p);
-                    per_pt[p].push_back({t, {xt[i2], zt[i1]}});
-                }
-        }
-        inj_start[i].push_back(0);
-        for (int p : order_pts) {
-            inj_pt[i].push_back(p);
-            for (auto &cw : per_pt[p]) {
-                inj_tr[i].push_back(cw.first);
-                inj_wx[i].push_back(cw.second.first);
-                inj_wz[i].push_back(cw.second.second);
+        for (int k = 0; k < sets[i].nsrc; k++) {
+            const TraceSet &q = sets[i].src[k];
+            InjPlan &P = inj[(size_t)i * MAXSETS + k];
+            // contributions in reference loop order: trace, z-corner, x-corner
+            std::map<int, std::vector<std::pair<int, std::pair<double, double>>>> per_pt;
+            std::vector<int> order_pts;
+            for (int t = 0; t < q.n; t++) {
+                const int mx = q.map[2 * t], mz = q.map[2 * t + 1];
+                if (mx < 0 || mz < 0) continue;
+                double xt[2], zt[2];
+                tri(shift_at(q.shift, 2 * t), xt);
+                tri(shift_at(q.shift, 2 * t + 1), zt);
+                for (int i1 = 0; i1 < 2; i1++)
+                    for (int i2 = 0; i2 < 2; i2++) {
+                        const int ix = lp + mx + i2, iz = lp + mz + i1;
+                        if (ix >= L.nxp || iz >= L.nzp) { set_error("shot %d: source %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
+                        const int p = iz * L.pitch + ix;
+                        if (!per_pt.count(p)) order_pts.push_back(p);
+                        per_pt[p].push_back({t, {xt[i2], zt[i1]}});
+                    }
             }
-            inj_start[i].push_back((int)inj_tr[i].size());
+            P.start.push_back(0);
+            for (int p : order_pts) {
+                P.pt.push_back(p);
+                for (auto &cw : per_pt[p]) {
+                    P.tr.push_back(cw.first);
+                    P.wx.push_back(cw.second.first);
+                    P.wz.push_back(cw.second.second);
+                }
+                P.start.push_back((int)P.tr.size());
+            }
         }
-        for (int t = 0; t < s[i].nrec; t++) {
-            const int mx = s[i].gmap[2 * t], mz = s[i].gmap[2 * t + 1];
-            if (mx < 0 || mz < 0) { rec_pt[i].push_back(-1); for (int k = 0; k < 4; k++) rec_w[i].push_back(0); }
-            else {
-                if (lp + mx + 1 >= L.nxp || lp + mz + 1 >= L.nzp) { set_error("shot %d: receiver %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
-                rec_pt[i].push_back((lp + mz) * L.pitch + lp + mx);
-                double sx, sz;
-                if (prec == PREC_F64) { sx = ((const double *)s[i].gshift)[2 * t]; sz = ((const double *)s[i].gshift)[2 * t + 1]; }
-                else { sx = ((const float *)s[i].gshift)[2 * t]; sz = ((const float *)s[i].gshift)[2 * t + 1]; }
-                if (prec == PREC_F64) { rec_w[i].push_back(1 - sx); rec_w[i].push_back(sx); rec_w[i].push_back(1 - sz); rec_w[i].push_back(sz); }
+        for (int k = 0; k < sets[i].nrec; k++) {
+            const TraceSet &q = sets[i].rec[k];
+            RecPlan &R = rec[(size_t)i * MAXSETS + k];
+            for (int t = 0; t < q.n; t++) {
+                const int mx = q.map[2 * t], mz = q.map[2 * t + 1];
+                if (mx < 0 || mz < 0) { R.pt.push_back(-1); for (int j = 0; j < 4; j++) R.w.push_back(0); }
                 else {
-                    rec_w[i].push_back((float)(1 - (float)sx)); rec_w[i].push_back((float)sx);
-                    rec_w[i].push_back((float)(1 - (float)sz)); rec_w[i].push_back((float)sz);
+                    if (lp + mx + 1 >= L.nxp || lp + mz + 1 >= L.nzp) { set_error("shot %d: receiver %d maps outside the grid", i, t); return RSGPU_ERR_ARG; }
+                    R.pt.push_back((lp + mz) * L.pitch + lp + mx);
+                    double w[2];
+                    tri(shift_at(q.shift, 2 * t), w);
+                    R.w.push_back(w[0]); R.w.push_back(w[1]);
+                    tri(shift_at(q.shift, 2 * t + 1), w);
+                    R.w.push_back(w[0]); R.w.push_back(w[1]);
                 }
+                R.fac.push_back(q.factor ? shift_at(q.factor, t) : 1.0);
             }
-            double fac = 1.0;
-            if (s[i].rec_factor) fac = prec == PREC_F64 ? ((const double *)s[i].rec_factor)[t] : ((const float *)s[i].rec_factor)[t];
-            rec_fac[i].push_back(fac);
         }
     }
     // plan tables in the same arena
-    std::vector<size_t> o_inj_pt(ns), o_inj_start(ns), o_inj_tr(ns), o_inj_wx(ns), o_inj_wz(ns), o_rec_pt(ns), o_rec_w(ns),
-        o_rec_fac(ns);
-    for (int i = 0; i < ns; i++) {
-        o_inj_pt[i] = take(std::max<size_t>(1, inj_pt[i].size()) * 4);
-        o_inj_start[i] = take(inj_start[i].size() * 4);
-        o_inj_tr[i] = take(std::max<size_t>(1, inj_tr[i].size()) * 4);
-        o_inj_wx[i] = take(std::max<size_t>(1, inj_wx[i].size()) * es);
-        o_inj_wz[i] = take(std::max<size_t>(1, inj_wz[i].size()) * es);
-        o_rec_pt[i] = take(std::max<size_t>(1, rec_pt[i].size()) * 4);
-        o_rec_w[i] = take(std::max<size_t>(1, rec_w[i].size()) * es);
-        o_rec_fac[i] = take(std::max<size_t>(1, rec_fac[i].size()) * es);
+    struct InjOff { size_t pt, start, tr, wx, wz; };
+    struct RecOff { size_t pt, w, fac; };
+    std::vector<InjOff> io((size_t)ns * MAXSETS);
+    std::vector<RecOff> ro((size_t)ns * MAXSETS);
+    for (size_t j = 0; j < io.size(); j++) {
+        io[j] = {take(inj[j].pt.size() * 4), take(std::max<size_t>(1, inj[j].start.size()) * 4), take(inj[j].tr.size() * 4),
+                 take(inj[j].wx.size() * es), take(inj[j].wz.size() * es)};
+        ro[j] = {take(rec[j].pt.size() * 4), take(rec[j].w.size() * es), take(rec[j].fac.size() * es)};
     }
     const size_t o_pml = take((size_t)12 * lp * es);
-    rec_pt_offsets = o_rec_pt;
+    rec_pt_offsets.assign((size_t)ns * MAXSETS, 0);
+    for (size_t j = 0; j < ro.size(); j++) rec_pt_offsets[j] = ro[j].pt;
     arena_bytes = off;
     if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -333,16 +394,21 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         for (int k = 0; k < nparams(phys); k++)
             CU(cudaMemcpy2DAsync(A + L.m[k] + org, (size_t)L.pitch * es, s[i].model[k], (size_t)L.nxp * es,
                                  (size_t)L.nxp * es, L.nzp, cudaMemcpyHostToDevice, stream));
-        if (s[i].nsrc > 0)
-            CU(cudaMemcpyAsync(A + L.wav, s[i].wavelet, (size_t)s[i].nsrc * cfg.nt * es, cudaMemcpyHostToDevice, stream));
-        if ((st = upload_vec_int(o_inj_pt[i], inj_pt[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_int(o_inj_start[i], inj_start[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_int(o_inj_tr[i], inj_tr[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_real(o_inj_wx[i], inj_wx[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_real(o_inj_wz[i], inj_wz[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_int(o_rec_pt[i], rec_pt[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_real(o_rec_w[i], rec_w[i])) != RSGPU_OK) return st;
-        if ((st = upload_vec_real(o_rec_fac[i], rec_fac[i])) != RSGPU_OK) return st;
+        for (int k = 0; k < sets[i].nsrc; k++)
+            if (sets[i].src[k].n > 0)
+                CU(cudaMemcpyAsync(A + L.wavk[k], sets[i].src[k].data, (size_t)sets[i].src[k].n * cfg.nt * es,
+                                   cudaMemcpyHostToDevice, stream));
+        for (int k = 0; k < MAXSETS; k++) {
+            const size_t j = (size_t)i * MAXSETS + k;
+            if ((st = upload_vec_int(io[j].pt, inj[j].pt)) != RSGPU_OK) return st;
+            if ((st = upload_vec_int(io[j].start, inj[j].start)) != RSGPU_OK) return st;
+            if ((st = upload_vec_int(io[j].tr, inj[j].tr)) != RSGPU_OK) return st;
+            if ((st = upload_vec_real(io[j].wx, inj[j].wx)) != RSGPU_OK) return st;
+            if ((st = upload_vec_real(io[j].wz, inj[j].wz)) != RSGPU_OK) return st;
+            if ((st = upload_vec_int(ro[j].pt, rec[j].pt)) != RSGPU_OK) return st;
+            if ((st = upload_vec_real(ro[j].w, rec[j].w)) != RSGPU_OK) return st;
+            if ((st = upload_vec_real(ro[j].fac, rec[j].fac)) != RSGPU_OK) return st;
+        }
     }
     {
         std::vector<unsigned char> tab((size_t)12 * lp * es);
@@ -389,12 +455,13 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     for (int i = 0; i < ns; i++) {
         const ShotLayout &L = shots[i];
         const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
-        if (prec == PREC_F64) fill_desc<double>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org,
-                                                o_inj_pt[i], o_inj_start[i], o_inj_tr[i], o_inj_wx[i], o_inj_wz[i], o_rec_pt[i],
-                                                o_rec_w[i], o_rec_fac[i], (int)inj_pt[i].size(), s[i]);
-        else fill_desc<float>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org,
-                              o_inj_pt[i], o_inj_start[i], o_inj_tr[i], o_inj_wx[i], o_inj_wz[i], o_rec_pt[i],
-                              o_rec_w[i], o_rec_fac[i], (int)inj_pt[i].size(), s[i]);
+        std::vector<SetOffsets> so(MAXSETS);
+        for (int k = 0; k < MAXSETS; k++) {
+            const size_t j = (size_t)i * MAXSETS + k;
+            so[k] = {io[j].pt, io[j].start, io[j].tr, io[j].wx, io[j].wz, (int)inj[j].pt.size(), ro[j].pt, ro[j].w, ro[j].fac};
+        }
+        if (prec == PREC_F64) fill_desc<double>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org, so.data(), sets[i]);
+        else fill_desc<float>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, L, org, so.data(), sets[i]);
     }
     std::memcpy(meta.data() + m_tiles, tiles.data(), tiles.size() * sizeof(Tile2D));
     std::memcpy(meta.data() + m_coef, coefs.data(), coefs.size());
@@ -418,10 +485,20 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     return RSGPU_OK;
 }
 
+static int inj_kind(int phys, int field)
+{
+    if (phys == PHYS_A2D) return field == RSGPU_PRESSURE ? INJ_A2_P : field == RSGPU_VX ? INJ_A2_VX : INJ_A2_VZ;
+    return field == RSGPU_PRESSURE ? INJ_E2_P : field == RSGPU_VX ? INJ_E2_VX : INJ_E2_VZ;
+}
+static int rec_kind(int phys, int field)
+{
+    if (phys == PHYS_A2D) return field == RSGPU_PRESSURE ? REC_A2_P : field == RSGPU_VX ? REC_A2_VX : REC_A2_VZ;
+    return field == RSGPU_PRESSURE ? REC_E2_P : field == RSGPU_VX ? REC_E2_VX : REC_E2_VZ;
+}
+
 template <typename T>
-void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, size_t o_ip, size_t o_is,
-                     size_t o_it, size_t o_wx, size_t o_wz, size_t o_rp, size_t o_rw, size_t o_rf, int ninj,
-                     const rsgpu_shot &s)
+void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, const SetOffsets *so,
+                     const ShotSets &t)
 {
     char *A = (char *)arena;
     Shot2D<T> d{};
@@ -431,31 +508,31 @@ void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L,
     for (int k = 0; k < npsi(phys); k++) { d.psix[k] = (T *)(A + L.psix[k]); d.psiz[k] = (T *)(A + L.psiz[k]); }
     std::memcpy(sd, &d, sizeof d);
     InjRec<T> r{};
-    r.ninj = ninj;
-    r.kind_inj = INJ_NONE;
-    if (ninj > 0) {
-        if (phys == PHYS_A2D) r.kind_inj = s.src_field == RSGPU_PRESSURE ? INJ_A2_P : s.src_field == RSGPU_VX ? INJ_A2_VX : INJ_A2_VZ;
-        else r.kind_inj = s.src_field == RSGPU_PRESSURE ? INJ_E2_P : s.src_field == RSGPU_VX ? INJ_E2_VX : INJ_E2_VZ;
-    }
-    r.inj_pt = (const int *)(A + o_ip);
-    r.inj_start = (const int *)(A + o_is);
-    r.inj_trace = (const int *)(A + o_it);
-    r.inj_wx = (const T *)(A + o_wx);
-    r.inj_wz = (const T *)(A + o_wz);
-    r.wav = (const T *)(A + L.wav);
-    r.nrec = L.nrec;
-    r.kind_rec = REC_NONE;
-    if (L.nrec > 0) {
-        if (phys == PHYS_A2D) r.kind_rec = s.rec_field == RSGPU_PRESSURE ? REC_A2_P : s.rec_field == RSGPU_VX ? REC_A2_VX : REC_A2_VZ;
-        else r.kind_rec = s.rec_field == RSGPU_PRESSURE ? REC_E2_P : s.rec_field == RSGPU_VX ? REC_E2_VX : REC_E2_VZ;
-    }
-    r.rec_pt = (const int *)(A + o_rp);
-    r.rec_w = (const T *)(A + o_rw);
-    r.rec_factor = (const T *)(A + o_rf);
-    r.rec_out = (T *)(A + L.traces);
     r.nt = cfg.nt;
     r.rev = reverse_time ? 1 : 0;
     r.rec_gate = gated_recording ? d_gate : nullptr;
+    r.ninjsets = t.nsrc;
+    for (int k = 0; k < t.nsrc; k++) {
+        InjSet<T> &q = r.inj[k];
+        q.ninj = so[k].ninj;
+        q.kind = q.ninj > 0 ? inj_kind(phys, t.src[k].field) : INJ_NONE;
+        q.pt = (const int *)(A + so[k].ipt);
+        q.start = (const int *)(A + so[k].istart);
+        q.trace = (const int *)(A + so[k].itr);
+        q.wx = (const T *)(A + so[k].iwx);
+        q.wz = (const T *)(A + so[k].iwz);
+        q.wav = (const T *)(A + L.wavk[k]);
+    }
+    r.nrecsets = t.nrec;
+    for (int k = 0; k < t.nrec; k++) {
+        RecSet<T> &q = r.rec[k];
+        q.nrec = L.nrecs[k];
+        q.kind = q.nrec > 0 ? (t.rec[k].psum ? REC_E2_PSUM : rec_kind(phys, t.rec[k].field)) : REC_NONE;
+        q.pt = (const int *)(A + so[k].rpt);
+        q.w = (const T *)(A + so[k].rw);
+        q.factor = (const T *)(A + so[k].rfac);
+        q.out = (T *)(A + L.tracesk[k]);
+    }
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -523,7 +600,7 @@ rsgpu_status Plan::run(int it0, int nsteps)
             CU(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
             rsgpu_status st = RSGPU_OK;
             for (int s = 0; s < G && st == RSGPU_OK; s++)
-                st = launch_step(s, d_it, false, (time_kernels && s < NTIMED) ? tev[s] : nullptr);
+                st = launch_step(s, d_it, adjoint_steps, (time_kernels && s < NTIMED) ? tev[s] : nullptr);
             if (st == RSGPU_OK) {
                 cudaError_t e = launch_advance(d_it, G, stream);
                 if (e != cudaSuccess) { set_error("launch_advance: %s", cudaGetErrorString(e)); st = RSGPU_ERR_CUDA; }
@@ -545,7 +622,7 @@ rsgpu_status Plan::run(int it0, int nsteps)
         }
     }
     for (; done < nsteps; done++) {
-        rsgpu_status st = launch_step(it0 + done, nullptr, false);
+        rsgpu_status st = launch_step(it0 + done, nullptr, adjoint_steps);
         if (st != RSGPU_OK) return st;
     }
     return RSGPU_OK;
@@ -606,15 +683,16 @@ rsgpu_status Plan::kernel_times(float *ms_vel, float *ms_str)
     return RSGPU_OK;
 }
 
-rsgpu_status Plan::read_traces(int shot, void *host_out)
+rsgpu_status Plan::read_traces(int shot, void *host_out, int set)
 {
     if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
     const ShotLayout &L = shots[shot];
-    if (L.nrec == 0) return RSGPU_OK;
+    if (set < 0 || set >= std::max(1, L.nrecsets)) { set_error("bad receiver set %d", set); return RSGPU_ERR_ARG; }
+    if (L.nrecsets == 0 || L.nrecs[set] == 0) return RSGPU_OK;
     const int es = esize(prec);
-    const size_t n = (size_t)L.nrec * cfg.nt;
+    const size_t n = (size_t)L.nrecs[set] * cfg.nt;
     std::vector<unsigned char> tmp(n * es);
-    CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.traces, n * es, cudaMemcpyDeviceToHost, stream));
+    CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.tracesk[set], n * es, cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
     if (rsgpu_status st = check_device_error()) return st;
     if (es == 8) { double *o = (double *)host_out; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }

@@ -196,16 +196,20 @@ extern "C" rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, con
     for (int k = 0; k < 2; k++) { sd.psix[k] = (float *)(S + o_px[k]); sd.psiz[k] = (float *)(S + o_pz[k]); }
     std::memcpy(at(o_shot), &sd, sizeof sd);
     InjRec<float> ir{};
-    ir.ninj = (int)inj_pt.size();
-    ir.kind_inj = ir.ninj == 0 ? INJ_NONE : sf == RSGPU_PRESSURE ? INJ_A2_P : sf == RSGPU_VX ? INJ_A2_VX : INJ_A2_VZ;
-    ir.inj_pt = (const int *)(S + o_ip); ir.inj_start = (const int *)(S + o_is); ir.inj_trace = (const int *)(S + o_it);
-    ir.inj_wx = (const float *)(S + o_wx); ir.inj_wz = (const float *)(S + o_wz);
-    ir.wav = static_cast<const float *>(shot->wavelet);
-    ir.nrec = shot->nrec;
-    ir.kind_rec = shot->nrec == 0 ? REC_NONE : rf == RSGPU_PRESSURE ? REC_A2_P : rf == RSGPU_VX ? REC_A2_VX : REC_A2_VZ;
-    ir.rec_pt = (const int *)(S + o_rp); ir.rec_w = (const float *)(S + o_rw); ir.rec_factor = nullptr;
-    ir.rec_out = static_cast<float *>(shot->rec_out);
     ir.nt = nt;
+    ir.ninjsets = 1;
+    InjSet<float> &q = ir.inj[0];
+    q.ninj = (int)inj_pt.size();
+    q.kind = q.ninj == 0 ? INJ_NONE : sf == RSGPU_PRESSURE ? INJ_A2_P : sf == RSGPU_VX ? INJ_A2_VX : INJ_A2_VZ;
+    q.pt = (const int *)(S + o_ip); q.start = (const int *)(S + o_is); q.trace = (const int *)(S + o_it);
+    q.wx = (const float *)(S + o_wx); q.wz = (const float *)(S + o_wz);
+    q.wav = static_cast<const float *>(shot->wavelet);
+    ir.nrecsets = shot->nrec > 0 ? 1 : 0;
+    RecSet<float> &r = ir.rec[0];
+    r.nrec = shot->nrec;
+    r.kind = shot->nrec == 0 ? REC_NONE : rf == RSGPU_PRESSURE ? REC_A2_P : rf == RSGPU_VX ? REC_A2_VX : REC_A2_VZ;
+    r.pt = (const int *)(S + o_rp); r.w = (const float *)(S + o_rw); r.factor = nullptr;
+    r.out = static_cast<float *>(shot->rec_out);
     std::memcpy(at(o_ir), &ir, sizeof ir);
     std::memcpy(at(o_tiles), tiles.data(), tiles.size() * sizeof(Tile2D));
     std::memcpy(at(o_coef), coefs.data(), coefs.size());

@@ -18,6 +18,27 @@ struct Corr2D {
     int nx, nz, pitch, lpml;
 };
 
+// Elastic 2D correlation inputs of one shot (FwiElastic2D::crossCorr and scaleGrad).
+template <typename T>
+struct Corr2DE {
+    const T *ws[5];             // forward Vx, Vz, Sxx, Szz, Sxz (origins)
+    const T *wr[5];             // adjoint Vx, Vz, Sxx, Szz, Sxz
+    const T *rx, *rz;
+    const T *vp, *vs, *rho;     // unpadded models
+    void *g[3];                 // lambda -> vp, mu -> vs, rho gradients [nz][nx]
+    int nx, nz, pitch, lpml;
+};
+
+// Residuals of the three elastic data types (P, Ux, Uz) of one shot.
+template <typename T>
+struct Resid2DE {
+    const T *mod[3];
+    const T *obs[3];
+    T *res[3];
+    const int *rec_pt_vx;       // validity of a trace for the misfit: the Ux set's map
+    int nrec, nt;
+};
+
 // Residual and misfit of one shot (DIFFERENCE misfit).
 template <typename T>
 struct Resid2D {
@@ -47,6 +68,11 @@ cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots,
 // ACC_REF in the element type, sequentially in the reference's order; ACC_F64 in
 // double by a fixed-order tree reduction.
 cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
+cudaError_t launch_corr_fwi_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
+                                double dz, cudaStream_t st);
+cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax,
+                                  cudaStream_t st);
+cudaError_t launch_residual_e2d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
 // Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
 // for the 16-bit formats (written by save, read by load).
 cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,

@@ -62,29 +62,42 @@ enum { PT_A = 0, PT_B = 1, PT_C = 2 };
 enum { PT_LTF = 0, PT_LTF_STAG = 3, PT_RBB = 6, PT_RBB_STAG = 9 };
 
 // Source injection / receiver recording plan for one shot (all device pointers).
-// Injection: a CSR list over unique target points, contributions in the
-// reference's loop order (trace, then z-corner, then x-corner), so that several
-// traces hitting one cell add in the same order as on the CPU.
+// A shot has up to MAXSETS source sets and MAXSETS receiver sets (e.g. the P, Vx
+// and Vz residuals an elastic adjoint injects, or the three data types its forward
+// records).  Injection: per set a CSR list over unique target points,
+// contributions in the reference's loop order (trace, then z-corner, then
+// x-corner), so that several traces hitting one cell add in the same order as on
+// the CPU.  Sets are injected one after another, then recorded.
+constexpr int MAXSETS = 3;
+template <typename T>
+struct InjSet {
+    int ninj;               // unique injection target points
+    int kind;               // see InjKind
+    const int *pt;          // [ninj] linear offset (iz*pitch + ix) from field origin
+    const int *start;       // [ninj+1] CSR into contributions
+    const int *trace;       // [ncontrib] trace index
+    const T *wx;            // [ncontrib] xtri weight (1 - shift.x or shift.x)
+    const T *wz;            // [ncontrib] ytri weight
+    const T *wav;           // [ntr * nt] trace-major wavelet / residual
+};
+template <typename T>
+struct RecSet {
+    int nrec;               // receiver traces
+    int kind;               // see RecKind
+    const int *pt;          // [nrec] offset of the (ix,iz) corner, or -1 if off-grid
+    const T *w;             // [nrec*4] weights x0, x1, z0, z1
+    const T *factor;        // [nrec] reciprocity divisor for elastic pressure
+    T *out;                 // [nrec * nt] trace-major output (accumulated with +=)
+};
 template <typename T>
 struct InjRec {
-    int ninj;               // unique injection target points
-    int kind_inj;           // see InjKind
-    const int *inj_pt;      // [ninj] linear offset (iz*pitch + ix) from field origin
-    const int *inj_start;   // [ninj+1] CSR into contributions
-    const int *inj_trace;   // [ncontrib] trace index
-    const T *inj_wx;        // [ncontrib] xtri weight (1 - shift.x or shift.x)
-    const T *inj_wz;        // [ncontrib] ytri weight
-    const T *wav;           // [ntr_src * nt] trace-major wavelet / residual
-    int nrec;               // receiver traces
-    int kind_rec;           // see RecKind
-    const int *rec_pt;      // [nrec] offset of the (ix,iz) corner, or -1 if off-grid
-    const T *rec_w;         // [nrec*4] weights (x0z0, x1z0, x0z1, x1z1) pre-split as wx,wz pairs
-    const T *rec_factor;    // [nrec] reciprocity divisor for elastic pressure (or null)
-    T *rec_out;             // [nrec * nt] trace-major output (accumulated with +=)
+    int ninjsets, nrecsets;
     int nt;
-    int rev;                // 1: step `it` reads wav[nt-1-it] and writes rec_out[nt-1-it]
+    int rev;                // 1: step `it` reads wav[nt-1-it] and writes out[nt-1-it]
                             //    (adjoint propagation run forward in reversed time)
     const int *rec_gate;    // if non-null, recording happens only while *rec_gate != 0
+    InjSet<T> inj[MAXSETS];
+    RecSet<T> rec[MAXSETS];
 };
 enum InjKind {
     INJ_NONE = 0,
@@ -99,6 +112,7 @@ enum RecKind {
     REC_NONE = 0,
     REC_A2_P = 1, REC_A2_VX = 2, REC_A2_VZ = 3,
     REC_E2_P = 4, REC_E2_VX = 5, REC_E2_VZ = 6,
+    REC_E2_PSUM = 7,  // xtri*ytri*(Sxx + Szz) in T: the elastic wavelet gradient (lib/fwi.cpp:2681-2697)
 };
 
 // Arguments of one 2D half-step launch (passed by value).

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include "rsgpu.h"
 #include "rsgpu_kernels.h"
+#include "rsgpu_internal.h"
 
 namespace rsgpu {
 
@@ -13,10 +14,34 @@ inline int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 
 inline int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
 inline int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 
+// One source or receiver trace set of a shot (host arrays).
+struct TraceSet {
+    int n = 0;
+    const int *map = nullptr;       // n*2 ints, -1 = off the grid
+    const void *shift = nullptr;    // n*2 reals
+    int field = RSGPU_PRESSURE;
+    const void *data = nullptr;     // sources: n*nt wavelet / residual reals
+    const void *factor = nullptr;   // receivers: elastic pressure divisor per trace, or null
+    bool psum = false;              // receivers, elastic PRESSURE: record (Sxx + Szz) unhalved
+};
+struct ShotSets {
+    int nsrc = 0, nrec = 0;
+    TraceSet src[MAXSETS], rec[MAXSETS];
+};
+// Arena offsets of one set's injection and recording plans.
+struct SetOffsets {
+    size_t ipt, istart, itr, iwx, iwz;
+    int ninj;
+    size_t rpt, rw, rfac;
+};
+
 // Byte offsets of one shot's arrays inside the plan arena.
 struct ShotLayout {
     int nx = 0, nz = 0, nxp = 0, nzp = 0, pitch = 0, rows = 0;
-    int nrec = 0, nsrc = 0;
+    int nrec = 0, nsrc = 0;         // traces of set 0
+    int nrecsets = 0, nsrcsets = 0;
+    int nrecs[MAXSETS] = {}, nsrcs[MAXSETS] = {};
+    size_t tracesk[MAXSETS] = {}, wavk[MAXSETS] = {};
     size_t f[9] = {}, m[8] = {}, psix[4] = {}, psiz[4] = {};
     size_t traces = 0, wav = 0;
     size_t psi_end = 0;       // end of the wavefields + C-PML memory (a checkpoint's extent)
@@ -27,10 +52,11 @@ struct ShotLayout {
 class Plan {
 public:
     ~Plan();
-    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    // sets: per shot the source/receiver trace sets; null = the rsgpu_shot's own
+    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s, const ShotSets *sets = nullptr);
     rsgpu_status reset();
     rsgpu_status run(int it0, int nsteps);
-    rsgpu_status read_traces(int shot, void *host_out);
+    rsgpu_status read_traces(int shot, void *host_out, int set = 0);
     rsgpu_status read_field(int shot, int field, void *host_out);
     rsgpu_status launch_step(int it_base, const int *it_dev, bool adj, cudaEvent_t *ev = nullptr);
     rsgpu_status enable_timing();
@@ -43,13 +69,14 @@ public:
 
     // options read by create()
     bool reverse_time = false;           // wavelet/trace index nt-1-it at step it
+    bool adjoint_steps = false;          // propagate with the adjoint (backwardstep*) kernels
     bool gated_recording = false;        // recording obeys set_recording()
     cudaStream_t shared_stream = nullptr;  // run on this caller-owned stream
 
     rsgpu_config cfg{};
     int prec = 0, phys = 0, nshots = 0, tilecfg = 0, ntiles = 0;
     std::vector<ShotLayout> shots;
-    std::vector<size_t> rec_pt_offsets;   // per shot: arena offset of the receiver points (-1 = off grid)
+    std::vector<size_t> rec_pt_offsets;   // [shot*MAXSETS + set]: arena offset of the receiver points (-1 = off grid)
     void *arena = nullptr;
     size_t arena_bytes = 0, state_end = 0;
     void *d_meta = nullptr;
@@ -70,12 +97,11 @@ public:
     cudaEvent_t tev[NTIMED][3] = {};
 
 private:
-    rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s, bool sets_given);
     int default_tile() const;
     template <typename T>
-    void fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, size_t o_ip, size_t o_is,
-                   size_t o_it, size_t o_wx, size_t o_wz, size_t o_rp, size_t o_rw, size_t o_rf, int ninj,
-                   const rsgpu_shot &s);
+    void fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, const SetOffsets *so,
+                   const ShotSets &t);
 };
 
 }  // namespace rsgpu
