@@ -59,7 +59,8 @@ public:
     rsgpu_status run();
     rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
 
-    int kind = RSGPU_KIND_FWI, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhz = 1;
+    int kind = RSGPU_KIND_FWI, phys = PHYS_A2D, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE;
+    int nhx = 1, nhz = 1;
     int ncheck = 0, nslots = 0, nxmax = 0, nzmax = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan> fw, bw;
@@ -67,7 +68,7 @@ public:
     void *dbuf = nullptr, *ckpt = nullptr;
     size_t slot_elems = 0, ck_es = 4;
     std::vector<CkptSeg> segs;
-    std::vector<size_t> o_vp, o_rho, o_obs, o_g0, o_g1;
+    std::vector<size_t> o_vp, o_vs, o_rho, o_obs, o_obsx, o_obsz, o_g0, o_g1, o_g2;
     size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
     std::vector<int> nx, nz, nrec, nsrc;
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
@@ -79,6 +80,9 @@ private:
     rsgpu_status load(int slot);
     template <typename T>
     void build_desc(std::vector<unsigned char> &corr, std::vector<unsigned char> &res);
+    template <typename T>
+    void build_desc_e2d(std::vector<unsigned char> &corr, std::vector<unsigned char> &res);
+    bool elastic() const { return phys == PHYS_E2D; }
     char *D(size_t o) const { return (char *)dbuf + o; }
 };
 
@@ -96,10 +100,11 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
 {
     if (!c || !o || !s || ns < 1) { set_error("null config/options/shots or nshots < 1"); return RSGPU_ERR_ARG; }
     if (kind != RSGPU_KIND_FWI && kind != RSGPU_KIND_RTM) { set_error("bad driver kind %d", kind); return RSGPU_ERR_ARG; }
-    if (c->physics != RSGPU_ACOUSTIC2D) {
-        set_error("the gradient/image drivers are built for acoustic 2D physics only");
+    if (c->physics != RSGPU_ACOUSTIC2D && !(c->physics == RSGPU_ELASTIC2D && kind == RSGPU_KIND_FWI)) {
+        set_error("the gradient/image drivers are built for acoustic 2D (FWI, RTM) and elastic 2D (FWI)");
         return RSGPU_ERR_UNSUPPORTED;
     }
+    const bool el = c->physics == RSGPU_ELASTIC2D;
     if (o->misfit != RSGPU_MISFIT_DIFFERENCE) { set_error("only the DIFFERENCE misfit is built"); return RSGPU_ERR_UNSUPPORTED; }
     if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
         set_error("bad checkpoint precision %d", o->ckpt_precision);
@@ -112,9 +117,15 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
     }
     for (int i = 0; i < ns; i++) {
         const rsgpu_shot &sh = s[i].shot;
-        if (sh.src_field != RSGPU_PRESSURE || (sh.nrec > 0 && sh.rec_field != RSGPU_PRESSURE)) {
-            set_error("shot %d: the acoustic gradient/image drivers take pressure sources and receivers", i);
+        if ((!el && sh.src_field != RSGPU_PRESSURE) || (sh.nrec > 0 && sh.rec_field != RSGPU_PRESSURE)) {
+            set_error("shot %d: the gradient/image drivers take pressure %s and a pressure receiver set", i,
+                      el ? "data" : "sources");
             return RSGPU_ERR_UNSUPPORTED;
+        }
+        if (el && (!s[i].gmap_vx || !s[i].gmap_vz || !s[i].gshift_vx || !s[i].gshift_vz || !s[i].data_vx ||
+                   !s[i].data_vz || !s[i].vs)) {
+            set_error("shot %d: elastic FWI needs the Ux and Uz data sets (maps, shifts, data) and vs", i);
+            return RSGPU_ERR_ARG;
         }
         if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
         if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
@@ -149,6 +160,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     }
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
+    phys = c->physics == RSGPU_ELASTIC2D ? PHYS_E2D : PHYS_A2D;
     // forward plan: the shots as given, recording switched off after FIRSTURN
     std::vector<rsgpu_shot> fs(ns), bs(ns);
     for (int i = 0; i < ns; i++) {
@@ -168,20 +180,52 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         bs[i].rec_factor = nullptr;
         bs[i].rec_out = nullptr;
     }
+    // elastic: the forward plan records P, Ux and Uz; the adjoint plan injects the
+    // three residuals and records the wavelet gradient at sources inside the
+    // interior 1..n-2 (FwiElastic2D::crossCorr records it inside its interior loop)
+    std::vector<ShotSets> fsets, bsets;
+    std::vector<std::vector<int>> wmaps(ns);
+    if (elastic()) {
+        fsets.resize(ns);
+        bsets.resize(ns);
+        for (int i = 0; i < ns; i++) {
+            const rsgpu_adjoint_shot &a = s[i];
+            ShotSets &F = fsets[i], &B = bsets[i];
+            F.nsrc = 1;
+            F.src[0] = {a.shot.nsrc, a.shot.smap, a.shot.sshift, a.shot.src_field, a.shot.wavelet, nullptr, false};
+            F.nrec = 3;
+            F.rec[0] = {a.shot.nrec, a.shot.gmap, a.shot.gshift, RSGPU_PRESSURE, nullptr, nullptr, false};
+            F.rec[1] = {a.shot.nrec, a.gmap_vx, a.gshift_vx, RSGPU_VX, nullptr, nullptr, false};
+            F.rec[2] = {a.shot.nrec, a.gmap_vz, a.gshift_vz, RSGPU_VZ, nullptr, nullptr, false};
+            B.nsrc = 3;
+            B.src[0] = {a.shot.nrec, a.shot.gmap, a.shot.gshift, RSGPU_PRESSURE, a.data, nullptr, false};
+            B.src[1] = {a.shot.nrec, a.gmap_vx, a.gshift_vx, RSGPU_VX, a.data_vx, nullptr, false};
+            B.src[2] = {a.shot.nrec, a.gmap_vz, a.gshift_vz, RSGPU_VZ, a.data_vz, nullptr, false};
+            std::vector<int> &wm = wmaps[i];
+            wm.assign(a.shot.smap, a.shot.smap + 2 * a.shot.nsrc);
+            for (int t = 0; t < a.shot.nsrc; t++)
+                if (wm[2 * t] < 1 || wm[2 * t] > a.shot.nx - 2 || wm[2 * t + 1] < 1 || wm[2 * t + 1] > a.shot.nz - 2)
+                    wm[2 * t] = wm[2 * t + 1] = -1;
+            B.nrec = 1;
+            B.rec[0] = {a.shot.nsrc, wm.data(), a.shot.sshift, a.shot.src_field, nullptr, nullptr,
+                        a.shot.src_field == RSGPU_PRESSURE};
+        }
+    }
     fw.reset(new Plan());
     fw->gated_recording = true;
     fw->shared_stream = stream;
-    ST(fw->create(c, ns, fs.data()));
+    ST(fw->create(c, ns, fs.data(), elastic() ? fsets.data() : nullptr));
     bw.reset(new Plan());
     bw->reverse_time = true;
+    bw->adjoint_steps = elastic();
     bw->shared_stream = stream;
-    ST(bw->create(c, ns, bs.data()));
+    ST(bw->create(c, ns, bs.data(), elastic() ? bsets.data() : nullptr));
 
     // device buffer: models, data, outputs, descriptors, checkpoint tables
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off = rup(off + std::max<size_t>(bytes, 1), 256); return r; };
-    o_vp.assign(ns, 0); o_rho.assign(ns, 0); o_obs.assign(ns, 0); o_g0.assign(ns, 0); o_g1.assign(ns, 0);
+    for (auto *v : {&o_vp, &o_vs, &o_rho, &o_obs, &o_obsx, &o_obsz, &o_g0, &o_g1, &o_g2}) v->assign(ns, 0);
     nx.resize(ns); nz.resize(ns); nrec.resize(ns); nsrc.resize(ns);
     for (int i = 0; i < ns; i++) {
         nx[i] = s[i].shot.nx; nz[i] = s[i].shot.nz; nrec[i] = s[i].shot.nrec; nsrc[i] = s[i].shot.nsrc;
@@ -194,13 +238,21 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
             o_obs[i] = take((size_t)nrec[i] * cfg.nt * es);
             o_g0[i] = take(n2 * gs);
             o_g1[i] = take(n2 * gs);
+            if (elastic()) {
+                o_vs[i] = take(n2 * es);
+                o_obsx[i] = take((size_t)nrec[i] * cfg.nt * es);
+                o_obsz[i] = take((size_t)nrec[i] * cfg.nt * es);
+                o_g2[i] = take(n2 * gs);
+            }
         } else {
             o_g0[i] = take(n2 * nhx * nhz * gs);
         }
     }
     o_misfit = take(sizeof(double) * ns);
-    const size_t corr_bytes = prec == PREC_F64 ? sizeof(Corr2D<double>) : sizeof(Corr2D<float>);
-    const size_t res_bytes = prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>);
+    const size_t corr_bytes = elastic() ? (prec == PREC_F64 ? sizeof(Corr2DE<double>) : sizeof(Corr2DE<float>))
+                                        : (prec == PREC_F64 ? sizeof(Corr2D<double>) : sizeof(Corr2D<float>));
+    const size_t res_bytes = elastic() ? (prec == PREC_F64 ? sizeof(Resid2DE<double>) : sizeof(Resid2DE<float>))
+                                       : (prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>));
     o_corr = take(corr_bytes * ns);
     o_res = take(res_bytes * ns);
     // checkpoint blocks: per shot the wavefields (interior of the pitched arrays)
@@ -219,9 +271,9 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
             slot_elems = rup(slot_elems, 64);   // keep every block 128-byte aligned in 16-bit slots
             segs.push_back(g);
         };
-        for (int f = 0; f < nfields(PHYS_A2D); f++) add(L.f[f] + org, L.nzp, L.nxp, L.pitch);
-        for (int p = 0; p < npsi(PHYS_A2D); p++) add(L.psix[p], L.nzp, 2 * cfg.lpml, 2 * cfg.lpml);
-        for (int p = 0; p < npsi(PHYS_A2D); p++) add(L.psiz[p], 2 * cfg.lpml, L.nxp, L.nxp);
+        for (int f = 0; f < nfields(phys); f++) add(L.f[f] + org, L.nzp, L.nxp, L.pitch);
+        for (int p = 0; p < npsi(phys); p++) add(L.psix[p], L.nzp, 2 * cfg.lpml, 2 * cfg.lpml);
+        for (int p = 0; p < npsi(phys); p++) add(L.psiz[p], 2 * cfg.lpml, L.nxp, L.nxp);
     }
     o_segs = take(sizeof(CkptSeg) * segs.size());
     o_scales = take(sizeof(float) * segs.size() * ncheck);
@@ -244,11 +296,21 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         CU(cudaMemcpyAsync(D(o_vp[i]), s[i].vp, n2 * es, cudaMemcpyHostToDevice, stream));
         CU(cudaMemcpyAsync(D(o_rho[i]), s[i].rho, n2 * es, cudaMemcpyHostToDevice, stream));
         CU(cudaMemcpyAsync(D(o_obs[i]), s[i].data, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        if (elastic()) {
+            CU(cudaMemcpyAsync(D(o_vs[i]), s[i].vs, n2 * es, cudaMemcpyHostToDevice, stream));
+            CU(cudaMemcpyAsync(D(o_obsx[i]), s[i].data_vx, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+            CU(cudaMemcpyAsync(D(o_obsz[i]), s[i].data_vz, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        }
     }
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
     std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
-    if (prec == PREC_F64) build_desc<double>(corr, res);
-    else build_desc<float>(corr, res);
+    if (elastic()) {
+        if (prec == PREC_F64) build_desc_e2d<double>(corr, res);
+        else build_desc_e2d<float>(corr, res);
+    } else {
+        if (prec == PREC_F64) build_desc<double>(corr, res);
+        else build_desc<float>(corr, res);
+    }
     CU(cudaMemcpyAsync(D(o_corr), corr.data(), corr.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(D(o_res), res.data(), res.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
@@ -289,6 +351,42 @@ void Adjoint::build_desc(std::vector<unsigned char> &corr, std::vector<unsigned 
     }
 }
 
+template <typename T>
+void Adjoint::build_desc_e2d(std::vector<unsigned char> &corr, std::vector<unsigned char> &res)
+{
+    for (int i = 0; i < nshots; i++) {
+        const ShotLayout &F = fw->shots[i], &B = bw->shots[i];
+        const size_t org = ((size_t)GUARD * F.pitch + GUARD) * es;
+        char *fa = (char *)fw->arena, *ba = (char *)bw->arena;
+        Corr2DE<T> c{};
+        for (int k = 0; k < 5; k++) {
+            c.ws[k] = (const T *)(fa + F.f[k] + org);
+            c.wr[k] = (const T *)(ba + B.f[k] + org);
+        }
+        c.rx = (const T *)(fa + F.m[M_RX] + org);
+        c.rz = (const T *)(fa + F.m[M_RZ] + org);
+        c.vp = (const T *)D(o_vp[i]);
+        c.vs = (const T *)D(o_vs[i]);
+        c.rho = (const T *)D(o_rho[i]);
+        c.g[0] = D(o_g0[i]);
+        c.g[1] = D(o_g1[i]);
+        c.g[2] = D(o_g2[i]);
+        c.nx = nx[i]; c.nz = nz[i]; c.pitch = F.pitch; c.lpml = cfg.lpml;
+        std::memcpy(corr.data() + i * sizeof c, &c, sizeof c);
+        Resid2DE<T> r{};
+        const size_t obs[3] = {o_obs[i], o_obsx[i], o_obsz[i]};
+        for (int k = 0; k < 3; k++) {
+            r.mod[k] = (const T *)(fa + F.tracesk[k]);
+            r.obs[k] = (const T *)D(obs[k]);
+            r.res[k] = (T *)(ba + B.wavk[k]);
+        }
+        r.rec_pt_vx = (const int *)(fa + fw->rec_pt_offsets[(size_t)i * MAXSETS + 1]);
+        r.nrec = nrec[i];
+        r.nt = cfg.nt;
+        std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+    }
+}
+
 rsgpu_status Adjoint::save(int slot)
 {
     if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
@@ -315,7 +413,8 @@ rsgpu_status Adjoint::load(int slot)
 
 rsgpu_status Adjoint::correlate()
 {
-    cudaError_t e = kind == RSGPU_KIND_FWI
+    cudaError_t e = elastic() ? launch_corr_fwi_e2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, cfg.dx, cfg.dz, stream)
+                    : kind == RSGPU_KIND_FWI
                         ? launch_corr_fwi_a2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, cfg.dx, cfg.dz, stream)
                         : launch_corr_rtm_a2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, nhx, nhz, stream);
     if (e != cudaSuccess) { set_error("correlation launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
@@ -336,6 +435,7 @@ rsgpu_status Adjoint::run()
         const size_t n2 = (size_t)nx[i] * nz[i];
         CU(cudaMemsetAsync(D(o_g0[i]), 0, n2 * (kind == RSGPU_KIND_FWI ? 1 : (size_t)nhx * nhz) * gs, stream));
         if (kind == RSGPU_KIND_FWI) CU(cudaMemsetAsync(D(o_g1[i]), 0, n2 * gs, stream));
+        if (elastic()) CU(cudaMemsetAsync(D(o_g2[i]), 0, n2 * gs, stream));
     }
     ST(fw->set_recording(true));
     RevolveSchedule rev(nt, ncheck);
@@ -356,7 +456,8 @@ rsgpu_status Adjoint::run()
             fw_steps += 1;
             ST(fw->set_recording(false));
             if (kind == RSGPU_KIND_FWI) {
-                cudaError_t e = launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                cudaError_t e = elastic() ? launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
+                                          : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
                 launches += 1;
             }
@@ -372,6 +473,12 @@ rsgpu_status Adjoint::run()
             set_error("revolve schedule error (info %d)", rev.info());
             return RSGPU_ERR_REVOLVE;
         }
+    }
+    if (elastic()) {
+        // FwiElastic2D::scaleGrad after the time loop
+        cudaError_t e = launch_scale_grad_e2d(prec, acc, D(o_corr), nshots, nxmax, nzmax, stream);
+        if (e != cudaSuccess) { set_error("gradient scaling launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+        launches += 1;
     }
     launches += fw->launches + bw->launches - l0;
     CU(cudaStreamSynchronize(stream));
@@ -419,17 +526,27 @@ rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
             continue;
         }
         if (s[i].vpgrad) { ST(fetch(o_g0[i], n2 * gs)); accumulate(s[i].vpgrad, n2); }
-        if (s[i].rhograd) { ST(fetch(o_g1[i], n2 * gs)); accumulate(s[i].rhograd, n2); }
-        if (s[i].shot.rec_out) ST(fw->read_traces(i, s[i].shot.rec_out));
-        if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
-        if (s[i].datares) {
+        if (elastic()) {
+            if (s[i].vsgrad) { ST(fetch(o_g1[i], n2 * gs)); accumulate(s[i].vsgrad, n2); }
+            if (s[i].rhograd) { ST(fetch(o_g2[i], n2 * gs)); accumulate(s[i].rhograd, n2); }
+        } else if (s[i].rhograd) {
+            ST(fetch(o_g1[i], n2 * gs));
+            accumulate(s[i].rhograd, n2);
+        }
+        void *mods[3] = {s[i].shot.rec_out, elastic() ? s[i].datamod_vx : nullptr, elastic() ? s[i].datamod_vz : nullptr};
+        void *ress[3] = {s[i].datares, elastic() ? s[i].datares_vx : nullptr, elastic() ? s[i].datares_vz : nullptr};
+        for (int k = 0; k < 3; k++) {
+            if (mods[k]) ST(fw->read_traces(i, mods[k], k));
+            if (!ress[k]) continue;
             const size_t n = (size_t)nrec[i] * cfg.nt;
             tmp.resize(n * es);
-            CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wav, n * es, cudaMemcpyDeviceToHost, stream));
+            CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wavk[k], n * es, cudaMemcpyDeviceToHost,
+                               stream));
             CU(cudaStreamSynchronize(stream));
-            if (es == 8) add_into<double, double>(s[i].datares, tmp, n);
-            else add_into<float, float>(s[i].datares, tmp, n);
+            if (es == 8) add_into<double, double>(ress[k], tmp, n);
+            else add_into<float, float>(ress[k], tmp, n);
         }
+        if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
         if (s[i].misfit) {
             // the reference keeps the misfit in T
             if (acc == ACC_REF && es == 4) *s[i].misfit = (double)(float)((float)*s[i].misfit + (float)mis[i]);

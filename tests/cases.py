@@ -91,3 +91,58 @@ def oracle_fwi(c):
 def oracle_rtm(c, data, nhx=1, nhz=1):
     return api.orc_rtm_a2d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, c.src.smap, c.src.sshift,
                            c.src.data, c.rec.gmap, c.rec.gshift, data, nhx, nhz)
+
+
+class ElasticFwiCase:
+    """Elastic 2D FWI problem: starting model, source, P/Ux/Uz receiver sets and
+    observed data modelled by the oracle in a model with a slow lens."""
+
+    def __init__(self, nx=61, nz=47, lpml=10, dx=10.0, dt=1e-3, nt=250, fs=0, seed=7, sfield=abi.PRESSURE,
+                 scoord=(301.7, 28.3), nrec=20, rx0=13.0, rdx=30.0, rz=14.7, precision=abi.F32_EXACT):
+        from rockseis_b200.rockseis import ModelElastic2D
+        self.nt, self.dt, self.order, self.precision, self.sfield = nt, dt, 8, precision, sfield
+        t = abi.real_dtype(precision)
+        vp = synth.layered_vp(nx, nz, dx, 1800, 3200, 3, 0.05, 60, seed)
+        vs = (vp / 1.8).astype(np.float32)
+        rho = synth.gardner(vp)
+        vt = vp.copy()
+        vt[nz // 3: nz // 3 + 10, nx // 3: nx // 3 + 15] *= 0.93
+        self.vp, self.vs, self.rho = vp, vs, rho
+        m = ModelElastic2D(nx, nz, lpml, dx, dx, 0.0, 0.0, fs, precision)
+        m.createModel()
+        m.Vp[:], m.Vs[:], m.R[:] = vp, vs, rho
+        self.model = m
+        src = Data2D(1, nt, dt, 0.0, precision)
+        src.scoords[:] = [scoord]
+        src.data[:] = synth.ricker(nt, dt, 20.0, t)[None, :]
+        src.setField(sfield)
+        src.makeMap(m, 0)
+        self.src = src
+        gc = synth.surface_line(nrec, rx0, rdx, rz)
+        self.recs = []
+        for f in (abi.PRESSURE, abi.VX, abi.VZ):
+            r = Data2D(nrec, nt, dt, 0.0, precision)
+            r.gcoords[:] = gc
+            r.setField(f)
+            r.makeMap(m, 1)
+            self.recs.append(r)
+        self.tab = np.zeros(12 * lpml, t)
+        abi.check(abi.lib.rsgpu_pml_tables(lpml, dt, precision, self.tab.ctypes.data))
+        self.pb = api.Problem2D(nx, nz, dx, dx, lpml, 8, fs, dt, nt, vp, rho, vs)
+        # observed data: float oracle modelling in the true model
+        mt = ModelElastic2D(nx, nz, lpml, dx, dx, 0.0, 0.0, fs)
+        mt.createModel()
+        mt.Vp[:], mt.Vs[:], mt.R[:] = vt, vs, rho
+        pbt = api.Problem2D(nx, nz, dx, dx, lpml, 8, fs, dt, nt, vt, rho, vs)
+        tab32 = np.zeros(12 * lpml, np.float32)
+        abi.check(abi.lib.rsgpu_pml_tables(lpml, dt, abi.F32_EXACT, tab32.ctypes.data))
+        wav32 = synth.ricker(nt, dt, 20.0)[None, :]
+        self.obs = [api.orc_modelling_e2d(pbt, mt.padded(), tab32, src.smap, src.sshift.astype(np.float32), wav32,
+                                          sfield, r.gmap, r.gshift.astype(np.float32), r.field).astype(t)
+                    for r in self.recs]
+
+    def oracle(self):
+        return api.orc_fwi_e2d(self.pb, [a.astype(np.float32) for a in self.model.padded()],
+                               self.tab.astype(np.float32), self.src.smap, self.src.sshift, self.src.data, self.sfield,
+                               [r.gmap for r in self.recs], [r.gshift for r in self.recs],
+                               [o.astype(np.float32) for o in self.obs])
