@@ -20,6 +20,9 @@
 namespace rsgpu {
 namespace {
 
+static_assert(TX3 >= 16 && TY3 >= 8, "the halo fetch assigns one x-halo column per thread tx < 16 and two y-halo rows "
+                                     "per thread ty < 8");
+
 template <typename T>
 __device__ __forceinline__ void load_coefs3(CoefSet3<T> &s, const CoefSet3<T> *g)
 {
@@ -30,9 +33,11 @@ __device__ __forceinline__ void load_coefs3(CoefSet3<T> &s, const CoefSet3<T> *g
 }
 
 // Staggered derivative with all NCOEF taps around b[7] (fw: b[0] = f[i-7]) or
-// b[8] (bw: b[0] = f[i-8]); in both cases sum_k (b[8+k*s] - b[7-k*s]) c_k.
+// b[8] (bw: b[0] = f[i-8]); in both cases sum_k (b[8+k*s] - b[7-k*s]) c_k.  The
+// coefficients are read from shared memory (one broadcast per tap), which keeps
+// them out of the register file.
 template <typename T, int MODE>
-__device__ __forceinline__ T taps(const T *b, int s, const T (&cu)[NCOEF], T d, T r)
+__device__ __forceinline__ T taps(const T *b, int s, const T *cu, T d, T r)
 {
     using A = Ar<T, MODE>;
     T acc = A::mul(A::sub(b[8 * s], b[7 * s]), cu[0]);
@@ -41,7 +46,7 @@ __device__ __forceinline__ T taps(const T *b, int s, const T (&cu)[NCOEF], T d, 
     return (MODE == MODE_FAST) ? acc : A::div(acc, d, r);
 }
 template <typename T, int MODE>
-__device__ __forceinline__ T taps_reg(const T (&q)[16], const T (&cu)[NCOEF], T d, T r)
+__device__ __forceinline__ T taps_reg(const T (&q)[16], const T *cu, T d, T r)
 {
     using A = Ar<T, MODE>;
     T acc = A::mul(A::sub(q[8], q[7]), cu[0]);
@@ -52,6 +57,10 @@ __device__ __forceinline__ T taps_reg(const T (&q)[16], const T (&cu)[NCOEF], T 
 
 // Velocity half-step (lib/waves.cpp:710-851):
 //   Vx += dt*Rx*Dx+P [x C-PML, staggered tables], Vy likewise in y, Vz in z.
+// Software pipelined: the point-wise inputs and the x/y halo of plane iz+1 are
+// requested while plane iz is computed, so their latency overlaps the arithmetic.
+// (Plane ze, read by the last prefetch, lies inside the allocation; a value read
+// there belongs to the next z-chunk and is not used.)
 template <typename T, int MODE>
 __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, const CoefSet3<T> *coefs)
 {
@@ -75,30 +84,33 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, con
     const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
     const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
     const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    // x halo: threads tx < 16 fetch one column each (tx < 8 left, 8..15 right);
+    // y halo: threads ty < 8 fetch one row below and one above the block
+    const int hx = tx < 8 ? -8 : TX3 - 8;
     T q[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) q[j] = P[(z0 - 7 + j) * plane + col];
-    __syncthreads();
-    T cux[NCOEF], cuy[NCOEF], cuz[NCOEF];
-#pragma unroll
-    for (int k = 0; k < NCOEF; k++) {
-        cux[k] = cs.cx[order * CROW3 + k];
-        cuy[k] = cs.cy[order * CROW3 + k];
-        cuz[k] = cs.cz[order * CROW3 + k];
-    }
-    for (int iz = z0; iz < ze; iz++) {
-        const long long o = iz * plane + col;
-        T vx = Vx[o], vy = Vy[o], vz = Vz[o];
-        const T rx = __ldg(Rx + o), ry = __ldg(Ry + o), rz = __ldg(Rz + o);
+    long long o = (long long)z0 * plane + col;
+    T vx = Vx[o], vy = Vy[o], vz = Vz[o], rx = __ldg(Rx + o), ry = __ldg(Ry + o), rz = __ldg(Rz + o);
+    T hxv = tx < 16 ? P[o + hx] : T(0);
+    T hy0 = ty < 8 ? P[o - 8 * pitch] : T(0), hy1 = ty < 8 ? P[o + TY3 * pitch] : T(0);
+    const T *cux = cs.cx + order * CROW3, *cuy = cs.cy + order * CROW3, *cuz = cs.cz + order * CROW3;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
         __syncthreads();
         sP[ty + 8][tx + 8] = q[7];
-        if (tx < 8) {
-            sP[ty + 8][tx] = P[o - 8];
-            sP[ty + 8][tx + TX3 + 8] = P[o + TX3];
-        }
+        if (tx < 16) sP[ty + 8][tx < 8 ? tx : tx + TX3] = hxv;
         if (ty < 8) {
-            sP[ty][tx + 8] = P[o - 8 * pitch];
-            sP[ty + TY3 + 8][tx + 8] = P[o + TY3 * pitch];
+            sP[ty][tx + 8] = hy0;
+            sP[ty + TY3 + 8][tx + 8] = hy1;
+        }
+        // next plane's inputs
+        const long long on = o + plane;
+        const T nvx = Vx[on], nvy = Vy[on], nvz = Vz[on];
+        const T nrx = __ldg(Rx + on), nry = __ldg(Ry + on), nrz = __ldg(Rz + on);
+        if (tx < 16) hxv = P[on + hx];
+        if (ty < 8) {
+            hy0 = P[on - 8 * pitch];
+            hy1 = P[on + TY3 * pitch];
         }
         __syncthreads();
         const T *cx = &sP[ty + 8][tx + 8];
@@ -132,11 +144,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, con
 #pragma unroll
         for (int j = 0; j < 15; j++) q[j] = q[j + 1];
         q[15] = P[o + 9 * plane];
+        vx = nvx; vy = nvy; vz = nvz; rx = nrx; ry = nry; rz = nrz;
     }
 }
 
 // Stress half-step (lib/waves.cpp:854-998):
 //   P += dt*L*Dx-Vx [x C-PML]; P += dt*L*Dy-Vy [y]; P += dt*L*Dz-Vz [z].
+// Pipelined like the velocity half-step.
 template <typename T, int MODE>
 __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const CoefSet3<T> *coefs)
 {
@@ -161,32 +175,30 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const
     const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
     const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
     const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    const int hx = tx < 8 ? -8 : TX3 - 8;
     T q[16];
 #pragma unroll
     for (int j = 0; j < 16; j++) q[j] = Vz[(z0 - 8 + j) * plane + col];
-    __syncthreads();
-    T cux[NCOEF], cuy[NCOEF], cuz[NCOEF];
-#pragma unroll
-    for (int k = 0; k < NCOEF; k++) {
-        cux[k] = cs.cx[order * CROW3 + k];
-        cuy[k] = cs.cy[order * CROW3 + k];
-        cuz[k] = cs.cz[order * CROW3 + k];
-    }
-    for (int iz = z0; iz < ze; iz++) {
-        const long long o = iz * plane + col;
-        T p = P[o];
-        const T lm = __ldg(Lm + o);
-        const T vxc = Vx[o], vyc = Vy[o];
+    long long o = (long long)z0 * plane + col;
+    T p = P[o], lm = __ldg(Lm + o), vxc = Vx[o], vyc = Vy[o];
+    T hxv = tx < 16 ? Vx[o + hx] : T(0);
+    T hy0 = ty < 8 ? Vy[o - 8 * pitch] : T(0), hy1 = ty < 8 ? Vy[o + TY3 * pitch] : T(0);
+    const T *cux = cs.cx + order * CROW3, *cuy = cs.cy + order * CROW3, *cuz = cs.cz + order * CROW3;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
         __syncthreads();
         sVx[ty][tx + 8] = vxc;
         sVy[ty + 8][tx] = vyc;
-        if (tx < 8) {
-            sVx[ty][tx] = Vx[o - 8];
-            sVx[ty][tx + TX3 + 8] = Vx[o + TX3];
-        }
+        if (tx < 16) sVx[ty][tx < 8 ? tx : tx + TX3] = hxv;
         if (ty < 8) {
-            sVy[ty][tx] = Vy[o - 8 * pitch];
-            sVy[ty + TY3 + 8][tx] = Vy[o + TY3 * pitch];
+            sVy[ty][tx] = hy0;
+            sVy[ty + TY3 + 8][tx] = hy1;
+        }
+        const long long on = o + plane;
+        const T np_ = P[on], nlm = __ldg(Lm + on), nvx = Vx[on], nvy = Vy[on];
+        if (tx < 16) hxv = Vx[on + hx];
+        if (ty < 8) {
+            hy0 = Vy[on - 8 * pitch];
+            hy1 = Vy[on + TY3 * pitch];
         }
         __syncthreads();
         const T *cx = &sVx[ty][tx + 8];
@@ -217,6 +229,7 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const
 #pragma unroll
         for (int j = 0; j < 15; j++) q[j] = q[j + 1];
         q[15] = Vz[o + 8 * plane];
+        p = np_; lm = nlm; vxc = nvx; vyc = nvy;
     }
 }
 
