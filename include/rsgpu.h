@@ -190,7 +190,8 @@ typedef struct {
     int accum;           /* RSGPU_ACCUM_* */
     int misfit;          /* RSGPU_MISFIT_DIFFERENCE (others: RSGPU_ERR_UNSUPPORTED) */
     int nhx, nhz;        /* RTM extended-image lags (Rtm::setNhx/setNhz; odd, 1 = zero lag) */
-    int reserved[10];
+    int nhy;             /* 3D RTM y lags (Rtm::setNhy; odd, 0 or 1 = zero lag) */
+    int reserved[9];
 } rsgpu_adjoint_opts;
 
 /* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332),
@@ -212,7 +213,7 @@ typedef struct {
     void *wavgrad;        /* FWI: nsrc*nt wavelet gradient (SMAP recording of the adjoint P) */
     void *datares;        /* FWI: nrec*nt residuals (dataresP) */
     double *misfit;       /* FWI: one value, accumulated */
-    void *image;          /* RTM: nhz*nhx*nz*nx (pimage, Image2D layout) */
+    void *image;          /* RTM: nhz*nhx*nz*nx (pimage, Image2D layout); 3D: nhz*nhy*nhx*nz*ny*nx */
     /* elastic 2D only */
     const int *gmap_vx, *gmap_vz;          /* GMAP of the Ux (VX) and Uz (VZ) data sets */
     const void *gshift_vx, *gshift_vz;
@@ -228,7 +229,8 @@ typedef struct {
  * (DIFFERENCE misfit). */
 rsgpu_status rsgpu_fwi_gradient(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
                                 const rsgpu_adjoint_shot *shots);
-/* RtmAcoustic2D<float>::run_optimal for a batch of shots. */
+/* RtmAcoustic2D<float>::run_optimal (RSGPU_ACOUSTIC2D) or RtmAcoustic3D<float>::run_optimal
+ * (RSGPU_ACOUSTIC3D, lib/rtm.cpp:735-859) for a batch of shots. */
 rsgpu_status rsgpu_rtm_image(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
                              const rsgpu_adjoint_shot *shots);
 

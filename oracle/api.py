@@ -68,6 +68,7 @@ def oracle() -> C.CDLL:
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
         _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V] + \
             [V] * 4 + [V, V, V]
+        _oracle.orc_rtm_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 5 + [I, V, V, V, I, V, V, V, I, I, I, V]
         _oracle.orc_mod_a3d.argtypes = [C.POINTER(OrcGrid3)] + [V] * 5 + [I, V, V, V, I, I, V, V, I, V, I, V]
     return _oracle
 
@@ -93,6 +94,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+        _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
         _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
         _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
         _ref.ref_stagger_e2d_f.argtypes = [G, V, V, V, V, V, V, V, V]
@@ -361,3 +363,25 @@ def orc_fwi_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmaps, gshifts, obs3
     assert r == 0
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out
+
+
+def ref_rtm_a3d(pb, scoords, wav, gcoords, data, ncheck, nhx=1, nhy=1, nhz=1):
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    img = np.zeros((nhz, nhy, nhx, pb.nz, pb.ny, pb.nx), np.float32)
+    vp, rho, w, d = _keep(pb.vp, pb.rho, wav, data, dtype=np.float32)
+    r = ref().ref_rtm_a3d_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d), ncheck,
+                            nhx, nhy, nhz, _p(img))
+    assert r == 1
+    return img
+
+
+def orc_rtm_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, data, nhx=1, nhy=1, nhz=1):
+    g = pb.orc_grid()
+    img = np.zeros((nhz, nhy, nhx, pb.nz, pb.ny, pb.nx), np.float32)
+    Rx, Ry, Rz, L, tb, ss, w, gs, d = _keep(*padded, tab, sshift, wav, gshift, data, dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    r = oracle().orc_rtm_a3d(C.byref(g), pb.nx, pb.ny, pb.nz, _p(Rx), _p(Ry), _p(Rz), _p(L), _p(tb), len(sm), _p(sm),
+                             _p(ss), _p(w), len(gm), _p(gm), _p(gs), _p(d), nhx, nhy, nhz, _p(img))
+    assert r == 0
+    return img

@@ -28,9 +28,33 @@ int rtm_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     return r;
 }
 
+/* RtmAcoustic3D::run_optimal (lib/rtm.cpp:735-859); image [nhz][nhy][nhx][nz][ny][nx] */
+template <typename T>
+int rtm_a3d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav,
+            int nr, const double *gc, const T *data, int ncheck, int nhx, int nhy, int nhz, T *image)
+{
+    auto model = make_a3d<T>(g, vp, rho);
+    auto src = make_data3d<T>(ns, g, sc, PRESSURE, SMAP, model->getGeom(), wav);
+    auto drec = make_data3d<T>(nr, g, gc, PRESSURE, GMAP, model->getGeom(), data);
+    auto img = std::make_shared<Image3D<T>>(g->nx, g->ny, g->nz, nhx, nhy, nhz, (T)g->dx, (T)g->dy, (T)g->dz,
+                                            (T)g->ox, (T)g->oy, (T)g->oz);
+    RtmAcoustic3D<T> rtm(model, img, src, drec, g->order, 1);
+    rtm.setNcheck(ncheck);
+    rtm.setIncore(true);
+    rtm.setSnapfile(tmpname("rtma3d"));
+    int r = rtm.run_optimal();
+    std::memcpy(image, img->getImagedata(), sizeof(T) * (size_t)g->nx * g->ny * g->nz * nhx * nhy * nhz);
+    return r;
+}
+
 } // namespace
 
 extern "C" {
+int ref_rtm_a3d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                  const float *wav, int nr, const double *gc, const float *data, int ncheck, int nhx, int nhy,
+                  int nhz, float *image)
+{ return rtm_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, data, ncheck, nhx, nhy, nhz, image); }
+
 int ref_rtm_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                   const float *wav, int nr, const double *gc, const float *data, int ncheck, int nhx,
                   int nhz, float *image)

@@ -791,3 +791,59 @@ int orc_fwi_e2d(const orc_grid *g, int nx, int nz, const float *vp, const float 
     free(Ps);
     return 0;
 }
+
+/* RtmAcoustic3D::run_optimal with (nhx, nhy, nhz) lags (lib/rtm.cpp:601-637, 735-859),
+ * forward pressure kept for every step; pairing as fw_state_at().
+ * image [nhz][nhy][nhx][nz][ny][nx]. */
+int orc_rtm_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *Rx, const float *Ry, const float *Rz,
+                const float *Lm, const float *tab, int ns, const int *smap, const float *sshift, const float *wav,
+                int nr, const int *gmap, const float *gshift, const float *data, int nhx, int nhy, int nhz,
+                float *image)
+{
+    const int nt = g->nt, L = g->lpml, nxp = g->nxp, nyp = g->nyp;
+    const long n = (long)g->nxp * g->nyp * g->nzp;
+    float *Ps = malloc((size_t)nt * n * sizeof(float));
+    if (!Ps) return -1;
+    orc_state3 fw, bw;
+    st3_alloc(&fw, g);
+    st3_alloc(&bw, g);
+    for (int it = 0; it < nt; it++) {
+        a3d_step(&fw, Rx, Ry, Rz, Lm, tab);
+        inject3(&fw, Lm, 0, ns, smap, sshift, wav, it);
+        memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
+    }
+    float *zero = calloc(n, sizeof(float));
+    for (int it = nt - 1; it >= 0; it--) {
+        if (it < nt - 1) a3d_step(&bw, Rx, Ry, Rz, Lm, tab);
+        inject3(&bw, Lm, 0, nr, gmap, gshift, data, it);
+        const float *ws = fw_state_at(Ps, zero, n, nt, it), *wr = bw.f[0];
+        for (int ihx = 0; ihx < nhx; ihx++) {
+            int hx = -(nhx - 1) / 2 + ihx;
+            for (int ihy = 0; ihy < nhy; ihy++) {
+                int hy = -(nhy - 1) / 2 + ihy;
+                for (int ihz = 0; ihz < nhz; ihz++) {
+                    int hz = -(nhz - 1) / 2 + ihz;
+                    for (int ix = 0; ix < nx; ix++) {
+                        if (ix - hx < 0 || ix - hx >= nx || ix + hx < 0 || ix + hx >= nx) continue;
+                        for (int iy = 0; iy < ny; iy++) {
+                            if (iy - hy < 0 || iy - hy >= ny || iy + hy < 0 || iy + hy >= ny) continue;
+                            for (int iz = 0; iz < nz; iz++) {
+                                if (iz - hz < 0 || iz - hz >= nz || iz + hz < 0 || iz + hz >= nz) continue;
+                                long ii = ((((long)ihz * nhy + ihy) * nhx + ihx) * nz + iz) * (long)nx * ny +
+                                          (long)iy * nx + ix;
+                                long ps = ((long)(iz - hz + L) * nyp + (iy - hy + L)) * nxp + (ix - hx + L);
+                                long pr = ((long)(iz + hz + L) * nyp + (iy + hy + L)) * nxp + (ix + hx + L);
+                                image[ii] += ws[ps] * wr[pr];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    free(zero);
+    st3_free(&fw);
+    st3_free(&bw);
+    free(Ps);
+    return 0;
+}

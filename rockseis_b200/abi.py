@@ -51,7 +51,7 @@ class Shot(C.Structure):
 
 class AdjointOpts(C.Structure):
     _fields_ = [("ncheck", C.c_int), ("ckpt_precision", C.c_int), ("accum", C.c_int), ("misfit", C.c_int),
-                ("nhx", C.c_int), ("nhz", C.c_int), ("reserved", C.c_int * 10)]
+                ("nhx", C.c_int), ("nhz", C.c_int), ("nhy", C.c_int), ("reserved", C.c_int * 9)]
 
 
 class AdjointShot(C.Structure):

@@ -29,6 +29,7 @@
 
 #include "rsgpu.h"
 #include "rsgpu_adjoint.h"
+#include "rsgpu_adjoint3d.h"
 #include "rsgpu_host.h"
 #include "rsgpu_internal.h"
 #include "rsgpu_plan.h"
@@ -263,7 +264,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         const ShotLayout &L = fw->shots[i];
         const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
         auto add = [&](size_t byte_off, int rows, int cols, int pitch) {
-            CkptSeg g;
+            CkptSeg g{};
             g.src = (char *)fw->arena + byte_off;
             g.rows = rows; g.cols = cols; g.pitch = pitch;
             g.dst = (long long)slot_elems;
@@ -560,7 +561,10 @@ rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
 
 using namespace rsgpu;
 
-struct rsgpu_adjoint { std::unique_ptr<Adjoint> a; };
+struct rsgpu_adjoint {
+    std::unique_ptr<Adjoint> a;       // 2D physics
+    std::unique_ptr<Adjoint3D> a3;    // 3D physics
+};
 
 extern "C" {
 
@@ -570,8 +574,14 @@ rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_o
     if (!adj) { set_error("handle pointer is null"); return RSGPU_ERR_ARG; }
     *adj = nullptr;
     std::unique_ptr<rsgpu_adjoint> h(new rsgpu_adjoint);
-    h->a.reset(new Adjoint());
-    rsgpu_status st = h->a->create(cfg, opts, kind, nshots, shots);
+    rsgpu_status st;
+    if (cfg && cfg->physics == RSGPU_ACOUSTIC3D) {
+        h->a3.reset(new Adjoint3D());
+        st = h->a3->create(cfg, opts, kind, nshots, shots);
+    } else {
+        h->a.reset(new Adjoint());
+        st = h->a->create(cfg, opts, kind, nshots, shots);
+    }
     if (st != RSGPU_OK) return st;
     *adj = h.release();
     return RSGPU_OK;
@@ -580,27 +590,30 @@ rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_o
 rsgpu_status rsgpu_adjoint_run(rsgpu_adjoint *adj)
 {
     if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
-    return adj->a->run();
+    return adj->a3 ? adj->a3->run() : adj->a->run();
 }
 
 rsgpu_status rsgpu_adjoint_read(rsgpu_adjoint *adj, int nshots, const rsgpu_adjoint_shot *shots)
 {
     if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
-    return adj->a->read(nshots, shots);
+    return adj->a3 ? adj->a3->read(nshots, shots) : adj->a->read(nshots, shots);
 }
 
 rsgpu_status rsgpu_adjoint_stats(rsgpu_adjoint *adj, long long *fw_steps, long long *bw_steps, long long *ckpt_bytes,
                                  long long *launches)
 {
     if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
-    if (fw_steps) *fw_steps = adj->a->fw_steps;
-    if (bw_steps) *bw_steps = adj->a->bw_steps;
-    if (ckpt_bytes) *ckpt_bytes = adj->a->ckpt_bytes;
-    if (launches) *launches = adj->a->launches;
+    if (fw_steps) *fw_steps = adj->a3 ? adj->a3->fw_steps : adj->a->fw_steps;
+    if (bw_steps) *bw_steps = adj->a3 ? adj->a3->bw_steps : adj->a->bw_steps;
+    if (ckpt_bytes) *ckpt_bytes = adj->a3 ? adj->a3->ckpt_bytes : adj->a->ckpt_bytes;
+    if (launches) *launches = adj->a3 ? adj->a3->launches : adj->a->launches;
     return RSGPU_OK;
 }
 
-void *rsgpu_adjoint_stream(rsgpu_adjoint *adj) { return adj ? (void *)adj->a->stream : nullptr; }
+void *rsgpu_adjoint_stream(rsgpu_adjoint *adj)
+{
+    return adj ? (void *)(adj->a3 ? adj->a3->stream : adj->a->stream) : nullptr;
+}
 void rsgpu_adjoint_destroy(rsgpu_adjoint *adj) { delete adj; }
 
 static rsgpu_status one_call(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int kind, int nshots,

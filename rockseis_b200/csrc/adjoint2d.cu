@@ -128,6 +128,44 @@ __global__ void __launch_bounds__(256) corr_rtm_a2d(const Corr2D<T> *desc, int n
     }
 }
 
+// 3D: image[ihz][ihy][ihx][iz][iy][ix] += Pfw(x-h) * Padj(x+h) (lib/rtm.cpp:601-637);
+// one thread per (x, y) column, marching z.
+template <typename T, bool EXACT, typename G>
+__global__ void __launch_bounds__(256) corr_rtm_a3d(const Corr3D<T> *desc, int nhx, int nhy, int nhz)
+{
+    const Corr3D<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= c.nx || iy >= c.ny) return;
+    const int L = c.lpml;
+    const long long n3 = (long long)c.nx * c.ny * c.nz;
+    for (int ihx = 0; ihx < nhx; ihx++) {
+        const int hx = -(nhx - 1) / 2 + ihx;
+        if (ix - hx < 0 || ix - hx >= c.nx || ix + hx < 0 || ix + hx >= c.nx) continue;
+        for (int ihy = 0; ihy < nhy; ihy++) {
+            const int hy = -(nhy - 1) / 2 + ihy;
+            if (iy - hy < 0 || iy - hy >= c.ny || iy + hy < 0 || iy + hy >= c.ny) continue;
+            for (int ihz = 0; ihz < nhz; ihz++) {
+                const int hz = -(nhz - 1) / 2 + ihz;
+                G *img = (G *)c.img + (((long long)ihz * nhy + ihy) * nhx + ihx) * n3 + (long long)iy * c.nx + ix;
+                const T *ws = c.wsp + (long long)(iy - hy + L) * c.pitch + (ix - hx + L);
+                const T *wr = c.wrp + (long long)(iy + hy + L) * c.pitch + (ix + hx + L);
+                const int z0 = max(hz, -hz), z1 = c.nz - max(hz, -hz);
+                for (int iz = z0; iz < z1; iz++) {
+                    const T a = ws[(long long)(iz - hz + L) * c.plane], b = wr[(long long)(iz + hz + L) * c.plane];
+                    G *o = img + (long long)iz * c.nx * c.ny;
+                    if (sizeof(G) == sizeof(T)) {
+                        using O = X<T>;
+                        *(T *)o = EXACT ? O::add(*(T *)o, O::mul(a, b)) : *(T *)o + a * b;
+                    } else {
+                        *o = __dadd_rn((double)*o, __dmul_rn((double)a, (double)b));
+                    }
+                }
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------- residuals and misfit
 template <typename T, int ACC>
 __global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, double *misfit)
@@ -342,6 +380,14 @@ __device__ __forceinline__ float pow2_scale(unsigned maxbits)
     return ldexpf(1.0f, e - 15);
 }
 
+// Element offset of row r of a block (rows of a 3D block run plane by plane).
+__device__ __forceinline__ long long seg_row(const CkptSeg &s, int r)
+{
+    if (s.prow <= 0) return (long long)r * s.pitch;
+    const int pl = r / s.prow;
+    return pl * s.pstride + (long long)(r - pl * s.prow) * s.pitch;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) ckpt_copy_out(const CkptSeg *segs, T *slot)
 {
@@ -349,7 +395,7 @@ __global__ void __launch_bounds__(256) ckpt_copy_out(const CkptSeg *segs, T *slo
     const T *src = (const T *)s.src;
     T *dst = slot + s.dst;
     for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.cols + c] = src[(long)r * s.pitch + c];
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.cols + c] = src[seg_row(s, r) + c];
 }
 
 template <typename T>
@@ -359,7 +405,7 @@ __global__ void __launch_bounds__(256) ckpt_copy_in(const CkptSeg *segs, const T
     T *dst = (T *)s.src;
     const T *src = slot + s.dst;
     for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.pitch + c] = src[(long)r * s.cols + c];
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[seg_row(s, r) + c] = src[(long)r * s.cols + c];
 }
 
 template <typename T>
@@ -369,7 +415,7 @@ __global__ void __launch_bounds__(256) ckpt_maxabs(const CkptSeg *segs, unsigned
     const T *src = (const T *)s.src;
     float m = 0.0f;
     for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) m = fmaxf(m, fabsf((float)src[(long)r * s.pitch + c]));
+        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) m = fmaxf(m, fabsf((float)src[seg_row(s, r) + c]));
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(&maxbits[blockIdx.y], __float_as_uint(m));
 }
@@ -385,7 +431,7 @@ __global__ void __launch_bounds__(256) ckpt_pack(const CkptSeg *segs, S *slot, c
     S *dst = slot + s.dst;
     for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
         for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
-            dst[(long)r * s.cols + c] = Store<S>::to((float)src[(long)r * s.pitch + c] * inv);
+            dst[(long)r * s.cols + c] = Store<S>::to((float)src[seg_row(s, r) + c] * inv);
 }
 
 template <typename T, typename S>
@@ -397,7 +443,7 @@ __global__ void __launch_bounds__(256) ckpt_unpack(const CkptSeg *segs, const S 
     const S *src = slot + s.dst;
     for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
         for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
-            dst[(long)r * s.pitch + c] = (T)(Store<S>::from(src[(long)r * s.cols + c]) * scale);
+            dst[seg_row(s, r) + c] = (T)(Store<S>::from(src[(long)r * s.cols + c]) * scale);
 }
 
 constexpr int CK_BLOCKS = 64;   // row-blocks per segment (grid.x)
@@ -466,6 +512,21 @@ cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots,
     if (prec == PREC_F64) return corr_rtm_t<double, true>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
     if (prec == PREC_F32_EXACT) return corr_rtm_t<float, true>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
     return corr_rtm_t<float, false>(acc, desc, nshots, nxmax, nzmax, nhx, nhz, st);
+}
+
+cudaError_t launch_corr_rtm_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, int nhx,
+                                int nhy, int nhz, cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nymax + 7) / 8, nshots);
+    if (prec == PREC_F64) corr_rtm_a3d<double, true, double><<<grid, block, 0, st>>>((const Corr3D<double> *)desc, nhx, nhy, nhz);
+    else if (acc == ACC_F64) {
+        if (prec == PREC_F32_EXACT) corr_rtm_a3d<float, true, double><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
+        else corr_rtm_a3d<float, false, double><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
+    } else {
+        if (prec == PREC_F32_EXACT) corr_rtm_a3d<float, true, float><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
+        else corr_rtm_a3d<float, false, float><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st)

@@ -241,6 +241,7 @@ __global__ void inject_record_3d(const Shot3D<T> *shots, const InjRec3<T> *plans
     using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
     const Shot3D<T> &sh = shots[blockIdx.x];
     const InjRec3<T> &pl = plans[blockIdx.x];
+    it = pl.rev ? pl.nt - 1 - it : it;
     if (pl.kind_inj != INJ3_NONE) {
         T *F = sh.f[pl.kind_inj == INJ3_P ? A3_P : pl.kind_inj == INJ3_VX ? A3_VX : pl.kind_inj == INJ3_VY ? A3_VY : A3_VZ];
         const T *Mod = sh.m[pl.kind_inj == INJ3_P ? M3_L : pl.kind_inj == INJ3_VX ? M3_RX : pl.kind_inj == INJ3_VY ? M3_RY : M3_RZ];

@@ -37,7 +37,7 @@ Plan3D::~Plan3D()
 {
     if (arena) cudaFree(arena);
     if (d_meta) cudaFree(d_meta);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
 rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
@@ -77,7 +77,8 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     nshots = ns;
     es = prec == PREC_F64 ? 8 : 4;
     zc = c->zchunk > 0 ? c->zchunk : 64;      // planes per z-chunk
-    CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (shared_stream) stream = shared_stream;
+    else CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     const int lp = cfg.lpml;
 
     shots.resize(ns);
@@ -309,6 +310,7 @@ void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu
     r.rec_w = (const T *)(A + o_rw);
     r.rec_out = (T *)(A + L.traces);
     r.nt = cfg.nt;
+    r.rev = reverse_time ? 1 : 0;
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -348,6 +350,15 @@ rsgpu_status Plan3D::step(int it)
 fail:
     set_error("3D kernel launch failed: %s", cudaGetErrorString(e));
     return RSGPU_ERR_CUDA;
+}
+
+rsgpu_status Plan3D::inject_record_only(int it)
+{
+    if (it < 0 || it >= cfg.nt) { set_error("step %d outside [0,%d)", it, cfg.nt); return RSGPU_ERR_ARG; }
+    cudaError_t e = launch_injrec_3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream);
+    if (e != cudaSuccess) { set_error("3D kernel launch failed: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += 1;
+    return RSGPU_OK;
 }
 
 rsgpu_status Plan3D::run(int it0, int nsteps)

@@ -67,7 +67,8 @@ struct InjRec3 {
     const long long *rec_pt;   // [nrec] offset of the (x0, y0, z0) corner, -1 off the grid
     const T *rec_w;            // [nrec][6] x0 x1 y0 y1 z0 z1
     T *rec_out;                // [nrec * nt], accumulated
-    int nt, pad_;
+    int nt;
+    int rev;                   // 1: step it reads wav[nt-1-it] and writes rec_out[nt-1-it]
 };
 enum { INJ3_NONE = 0, INJ3_P = 1, INJ3_VX = 2, INJ3_VY = 3, INJ3_VZ = 4 };
 enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4 };

@@ -39,6 +39,15 @@ struct Resid2DE {
     int nrec, nt;
 };
 
+// 3D image correlation inputs of one shot (RtmAcoustic3D::crossCorr).
+template <typename T>
+struct Corr3D {
+    const T *wsp, *wrp;         // forward and adjoint pressure (origins of the pitched 3D arrays)
+    void *img;                  // [nhz][nhy][nhx][nz][ny][nx]
+    int nx, ny, nz, pitch, lpml, pad_;
+    long long plane;            // elements per plane of the pitched arrays
+};
+
 // Residual and misfit of one shot (DIFFERENCE misfit).
 template <typename T>
 struct Resid2D {
@@ -54,6 +63,8 @@ struct CkptSeg {
     void *src;                  // first element
     int rows, cols, pitch;      // pitch in elements
     long long dst;              // element offset of the block inside a slot
+    int prow;                   // 3D: rows per plane (0 = one 2D block)
+    long long pstride;          // 3D: elements between planes
 };
 
 enum { ACC_REF = 0, ACC_F64 = 1 };
@@ -73,6 +84,8 @@ cudaError_t launch_corr_fwi_e2d(int prec, int acc, const void *desc, int nshots,
 cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax,
                                   cudaStream_t st);
 cudaError_t launch_residual_e2d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
+cudaError_t launch_corr_rtm_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, int nhx,
+                                int nhy, int nhz, cudaStream_t st);
 // Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
 // for the 16-bit formats (written by save, read by load).
 cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,

@@ -1,0 +1,40 @@
+// 3D RTM driver behind the rsgpu_adjoint handle (host runtime, not ABI).
+#pragma once
+#include <memory>
+#include <vector>
+#include <cuda_runtime.h>
+#include "rsgpu.h"
+#include "rsgpu_adjoint.h"
+#include "rsgpu_plan3d.h"
+
+namespace rsgpu {
+
+class Adjoint3D {
+public:
+    ~Adjoint3D();
+    rsgpu_status create(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
+                        const rsgpu_adjoint_shot *s);
+    rsgpu_status run();
+    rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
+
+    int nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
+    int ncheck = 0, nxmax = 0, nymax = 0;
+    rsgpu_config cfg{};
+    std::unique_ptr<Plan3D> fw, bw;
+    cudaStream_t stream = nullptr;
+    void *dbuf = nullptr, *ckpt = nullptr;
+    size_t slot_elems = 0, ck_es = 4;
+    std::vector<CkptSeg> segs;
+    std::vector<size_t> o_img;
+    size_t o_corr = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    std::vector<int> nx, ny, nz;
+    long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
+    bool ran = false;
+
+private:
+    rsgpu_status slot_io(bool save, int slot);
+    rsgpu_status correlate();
+    char *D(size_t o) const { return (char *)dbuf + o; }
+};
+
+}  // namespace rsgpu

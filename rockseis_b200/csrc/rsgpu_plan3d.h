@@ -27,6 +27,11 @@ public:
     rsgpu_status read_traces(int shot, void *host_out);
     rsgpu_status read_field(int shot, int field, void *host_out);
     size_t origin_bytes(const Layout3D &L) const;
+    rsgpu_status inject_record_only(int it);   // injection/recording of step it without propagation
+
+    // options read by create()
+    bool reverse_time = false;                 // wavelet/trace index nt-1-it at step it
+    cudaStream_t shared_stream = nullptr;      // run on this caller-owned stream
 
     rsgpu_config cfg{};
     int prec = 0, nshots = 0, es = 4, zc = 64, ntiles = 0;

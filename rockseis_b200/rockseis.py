@@ -493,6 +493,29 @@ class Image2D:
     def getNhz(self): return self.nhz
 
 
+class Image3D:
+    """Image container (Image3D<T>, include/image.h): imagedata[ihz, ihy, ihx, iz, iy, ix]."""
+
+    def __init__(self, imagefile, model: _Model, nhx=1, nhy=1, nhz=1, precision=None):
+        self.imagefile = imagefile
+        self.nx, self.ny, self.nz = model.nx, model.ny, model.nz
+        self.nhx, self.nhy, self.nhz = int(nhx), int(nhy), int(nhz)
+        self.dtype = abi.real_dtype(model.precision if precision is None else precision)
+        self.imagedata = None
+
+    def allocateImage(self):
+        if self.imagedata is None:
+            self.imagedata = np.zeros((self.nhz, self.nhy, self.nhx, self.nz, self.ny, self.nx), self.dtype)
+
+    def getImagedata(self):
+        self.allocateImage()
+        return self.imagedata
+
+    def getNhx(self): return self.nhx
+    def getNhy(self): return self.nhy
+    def getNhz(self): return self.nhz
+
+
 class _Adjoint:
     """Settings shared by FwiAcoustic2D and RtmAcoustic2D (the reference's Fwi / Rtm bases)."""
     cls = "FwiAcoustic2D"
@@ -520,10 +543,11 @@ class _Adjoint:
         check_stability(self.model, self.source.dt, self.cls)
         return True
 
-    def _opts(self, nhx=1, nhz=1) -> abi.AdjointOpts:
+    def _opts(self, nhx=1, nhz=1, nhy=1) -> abi.AdjointOpts:
         o = abi.AdjointOpts()
         o.ncheck, o.ckpt_precision, o.accum, o.misfit, o.nhx, o.nhz = (self.ncheck, self.ckpt_precision, self.accum,
                                                                         self.misfit_type, nhx, nhz)
+        o.nhy = nhy
         return o
 
     def _adjoint_shot(self, keep: list) -> abi.AdjointShot:
@@ -646,13 +670,37 @@ class RtmAcoustic2D(_Adjoint):
         return rtm_image_batch([self])
 
 
+class RtmAcoustic3D(_Adjoint):
+    """RtmAcoustic3D<T> (include/rtm.h:128-160): (extended) 3D cross-correlation image."""
+    cls = "RtmAcoustic3D"
+
+    def __init__(self, model=None, pimage=None, source=None, dataP=None, order=4, snapinc=1, precision=None):
+        super().__init__(model, source, dataP, order, snapinc, precision)
+        self.pimage = pimage
+
+    def setImage(self, img): self.pimage = img
+
+    def _adjoint_shot(self, keep):
+        a = super()._adjoint_shot(keep)
+        a.image = ptr(self.pimage.getImagedata())
+        return a
+
+    def run_optimal(self):
+        return rtm_image_batch([self])
+
+
+def _lags(j0):
+    if isinstance(j0, (RtmAcoustic2D, RtmAcoustic3D)):
+        img = j0.pimage
+        return img.getNhx(), img.getNhz(), img.getNhy() if isinstance(img, Image3D) else 1
+    return 1, 1, 1
+
+
 def _adjoint_batch(jobs, fn):
     j0 = jobs[0]
     j0.checkStability()
     cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
-    nhx = j0.pimage.getNhx() if isinstance(j0, RtmAcoustic2D) else 1
-    nhz = j0.pimage.getNhz() if isinstance(j0, RtmAcoustic2D) else 1
-    opts = j0._opts(nhx, nhz)
+    opts = j0._opts(*_lags(j0))
     keep: list = []
     shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
     check(fn(C.byref(cfg), C.byref(opts), len(jobs), shots))
@@ -680,9 +728,7 @@ class AdjointBatch:
         j0 = jobs[0]
         self.jobs = jobs
         self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
-        nhx = j0.pimage.getNhx() if kind == abi.KIND_RTM else 1
-        nhz = j0.pimage.getNhz() if kind == abi.KIND_RTM else 1
-        self.opts = j0._opts(nhx, nhz)
+        self.opts = j0._opts(*_lags(j0))
         self._keep: list = []
         self.shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(self._keep) for j in jobs])
         self.h = C.c_void_p()

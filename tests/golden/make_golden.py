@@ -209,6 +209,9 @@ def a3d_cases(g):
         g[f"{key}_models"] = api.ref_stagger_a3d(pb)
         g[f"{key}_smap"], g[f"{key}_sshift"] = api.ref_makemap3d(pb, sc, 0, sf)
         g[f"{key}_gmap"], g[f"{key}_gshift"] = api.ref_makemap3d(pb, gc, 1, rf)
+    # extended 3D RTM image of the first case's gather
+    pb = api.Problem3D(nx, ny, nz, dx, dx, dx, L, 8, 0, 1e-3, nt, vp, rho)
+    g["a3d_rtm_image"] = api.ref_rtm_a3d(pb, sc, wav, gc, g["a3d_fs0_s0_r0_traces"], 5, 3, 1, 3)
     g["a3d_cases"] = np.array([f"a3d_fs{fs}_s{sf}_r{rf}" for fs, sf, rf in ((0, 0, 0), (1, 0, 3), (0, 1, 0))])
 
 

@@ -95,3 +95,64 @@ def test_acoustic3d_fast_within_fp32_tolerance(require_gpu):
     ref = c.oracle()
     got = c.gpu(precision=abi.F32_FAST)
     assert rel_l2(got, ref) <= 1e-5
+
+
+# ---------------------------------------------------------------- RtmAcoustic3D::run_optimal
+def rtm_inputs(c):
+    """Data to migrate: the oracle's pressure gather of the case's shot."""
+    return c.oracle().astype(np.float32)
+
+
+def oracle_rtm3d(c, data, nhx, nhy, nhz):
+    s, r = c.src, c.rec
+    return api.orc_rtm_a3d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, s.smap, s.sshift,
+                           s.data.astype(np.float32), r.gmap, r.gshift, data, nhx, nhy, nhz)
+
+
+def gpu_rtm3d(c, data, nhx, nhy, nhz, ncheck=5, precision=None, ckpt=abi.CKPT_NATIVE, accum=abi.ACCUM_REFERENCE):
+    from rockseis_b200.rockseis import Image3D, RtmAcoustic3D
+    prec = c.precision if precision is None else precision
+    c.rec.data = np.ascontiguousarray(data.astype(abi.real_dtype(prec)))
+    img = Image3D("pimage", c.model, nhx, nhy, nhz, prec)
+    r = RtmAcoustic3D(c.model, img, c.src, c.rec, c.order, 1, precision=prec)
+    r.setNcheck(ncheck)
+    r.setCheckpointPrecision(ckpt)
+    r.setAccumulation(accum)
+    assert r.run_optimal() == 1
+    return img.getImagedata()
+
+
+@pytest.mark.parametrize("lags,ncheck", [((1, 1, 1), 5), ((3, 1, 3), 9), ((1, 3, 1), 120)])
+def test_rtm3d_exact_bitwise(require_gpu, lags, ncheck):
+    c = Case3D(nx=29, ny=27, nz=25)
+    data = rtm_inputs(c)
+    ref = oracle_rtm3d(c, data, *lags)
+    got = gpu_rtm3d(c, data, *lags, ncheck=ncheck)
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(got, ref), f"max abs diff {np.abs(got - ref).max()}"
+
+
+def test_rtm3d_batched_windows_bitwise(require_gpu):
+    from rockseis_b200.rockseis import Image3D, RtmAcoustic3D, rtm_image_batch
+    cases = [Case3D(nx=29, ny=27, nz=25, seed=5), Case3D(nx=23, ny=31, nz=27, seed=9, scoord=(120.4, 200.8, 97.0))]
+    jobs, refs = [], []
+    for c in cases:
+        data = rtm_inputs(c)
+        refs.append(oracle_rtm3d(c, data, 1, 1, 1))
+        c.rec.data = np.ascontiguousarray(data)
+        r = RtmAcoustic3D(c.model, Image3D("pimage", c.model, 1, 1, 1), c.src, c.rec, c.order, 1)
+        r.setNcheck(6)
+        jobs.append(r)
+    rtm_image_batch(jobs)
+    for r, ref in zip(jobs, refs):
+        assert np.array_equal(r.pimage.getImagedata(), ref)
+
+
+def test_rtm3d_fast_fp16_checkpoints_within_tolerance(require_gpu):
+    c = Case3D(nx=29, ny=27, nz=25)
+    data = rtm_inputs(c)
+    ref = oracle_rtm3d(c, data, 1, 1, 1)
+    got = gpu_rtm3d(c, data, 1, 1, 1, ncheck=8, precision=abi.F32_FAST, ckpt=abi.CKPT_F16, accum=abi.ACCUM_F64)
+    err = rel_l2(got, ref)
+    print(f"3D RTM image, FMA + FP16 checkpoints + FP64 accumulation vs exact: {err:.3g}")
+    assert err <= 1e-3

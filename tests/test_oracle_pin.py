@@ -229,3 +229,14 @@ def test_3d_host_preprocessing_matches_reference(case):
         mp, sh = (d.smap, d.sshift) if which == 0 else (d.gmap, d.gshift)
         assert np.array_equal(mp, GOLD[f"{case}_{key}map"])
         assert np.array_equal(sh, GOLD[f"{case}_{key}shift"])
+
+
+def test_oracle_3d_rtm_image_matches_reference():
+    case = "a3d_fs0_s0_r0"
+    pb = _a3d_problem(0)
+    g = lambda k: GOLD[f"{case}_{k}"]  # noqa: E731
+    img = api.orc_rtm_a3d(pb, list(g("models")), GOLD["a3d_tab"], g("smap"), g("sshift"), GOLD["a3d_wav"], g("gmap"),
+                          g("gshift"), g("traces"), 3, 1, 3)
+    ref = GOLD["a3d_rtm_image"]
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(img, ref), f"max abs diff {np.abs(img - ref).max()}"
