@@ -79,7 +79,9 @@ typedef struct {
                            by rsgpu_pml_tables with Smax = 1200. */
     int tile;           /* 2D kernel tile shape, -1 = autotuned/default */
     int zchunk;         /* 3D: planes marched by one CTA (0 = 64) */
-    int reserved[6];
+    int launch_mode;    /* 2D elastic forward: 0 = one CTA per tile (the faster on B200),
+                           1 = persistent CTAs with double-buffered tile stages */
+    int reserved[5];
 } rsgpu_config;
 
 /* One shot (work item) of a batch.  nx/ny/nz are the UNPADDED window the

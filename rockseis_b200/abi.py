@@ -39,7 +39,7 @@ class Config(C.Structure):
     _fields_ = [("physics", C.c_int), ("precision", C.c_int), ("lpml", C.c_int), ("order", C.c_int),
                 ("fs", C.c_int), ("nt", C.c_int), ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
                 ("dt", C.c_double), ("pml", C.c_void_p), ("tile", C.c_int), ("zchunk", C.c_int),
-                ("reserved", C.c_int * 6)]
+                ("launch_mode", C.c_int), ("reserved", C.c_int * 5)]
 
 
 class Shot(C.Structure):

@@ -80,9 +80,9 @@ def _generate() -> list[str]:
                 continue
             fn = f"launch_2d_{name}_{tx}x{tz}r{rz}m{mb}"
             src = ("// generated by rockseis_b200/build.py\n#include \"fd2d_kernels.cuh\"\nnamespace rsgpu {\n"
-                   f"cudaError_t {fn}(int physics, int half, bool adj, const void *args, const void *coefs, "
+                   f"cudaError_t {fn}(int physics, int half, int flags, const void *args, const void *coefs, "
                    "const void *maps, int *err, int grid, cudaStream_t st)\n{\n"
-                   f"    return launch_2d_cfg<{t}, {mode}, {tx}, {tz}, {rz}, {mb}>(physics, half, adj, "
+                   f"    return launch_2d_cfg<{t}, {mode}, {tx}, {tz}, {rz}, {mb}>(physics, half, flags, "
                    f"*static_cast<const Step2DArgs<{t}> *>(args), static_cast<const CoefSet<{t}> *>(coefs), "
                    "static_cast<const CUtensorMap *>(maps), err, grid, st);\n}\n}  // namespace rsgpu\n")
             path = os.path.join(gen, fn + ".cu")
@@ -91,7 +91,7 @@ def _generate() -> list[str]:
                     f.write(src)
             out.append(path)
             table.append((name, idx, fn))
-    decl = "".join(f"cudaError_t {fn}(int, int, bool, const void *, const void *, const void *, int *, int, "
+    decl = "".join(f"cudaError_t {fn}(int, int, int, const void *, const void *, const void *, int *, int, "
                    "cudaStream_t);\n" for _, _, fn in table)
     cases = ""
     for name in [v[0] for v in VARIANTS_2D]:

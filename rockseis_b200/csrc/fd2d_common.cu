@@ -6,13 +6,13 @@ namespace rsgpu {
 
 static_assert(NMAP2D == NMAP, "tensor-map slots per shot");
 
-cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, bool adj, const void *args, const void *coefs,
+cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, int flags, const void *args, const void *coefs,
                            const void *maps, int *err, int grid, cudaStream_t st)
 {
     const char *v = prec == PREC_F32_EXACT ? "f32x" : prec == PREC_F32_FAST ? "f32f" : "f64";
     Launch2DFn fn = launch_2d_table(v, cfg);
     if (!fn) return cudaErrorInvalidValue;
-    return fn(physics, half, adj, args, coefs, maps, err, grid, st);
+    return fn(physics, half, flags, args, coefs, maps, err, grid, st);
 }
 
 cudaError_t launch_injrec_2d(int prec, const void *shots, const void *plans, int nshots, double dt, int it_base,

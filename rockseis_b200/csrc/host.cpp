@@ -574,12 +574,13 @@ rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj, cudaEve
     if (prec == PREC_F64) make_args<double>(args, *this);
     else make_args<float>(args, *this);
     const int grid = ntiles;
+    const int flags = (adj ? LAUNCH_ADJ : 0) | (cfg.launch_mode == 1 ? LAUNCH_PERSISTENT : 0);
     cudaError_t e;
     // external records so the events become timestamp nodes of a captured graph
     if (ev && (e = cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 0, adj, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 0, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
     if (ev && (e = cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 1, adj, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = launch_step_2d(prec, tilecfg, phys, 1, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
     if (ev && (e = cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
     if ((e = launch_injrec_2d(prec, d_shots, d_injrec, nshots, cfg.dt, it_base, it_dev, stream)) != cudaSuccess) goto fail;
     launches += 3;

@@ -249,7 +249,7 @@ extern "C" rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, con
     int *derr = (int *)(S + o_err);
     for (int it = 0; it < nt; it++) {
         for (int half = 0; half < 2; half++)
-            NA_CU(launch_step_2d(prec, cfgi, PHYS_A2D, half, false, &a, S + o_coef, S + o_maps, derr, a.ntiles, st));
+            NA_CU(launch_step_2d(prec, cfgi, PHYS_A2D, half, 0, &a, S + o_coef, S + o_maps, derr, a.ntiles, st));
         NA_CU(launch_injrec_2d(prec, S + o_shot, S + o_ir, 1, cfg->dt, it, nullptr, st));
     }
     NA_CU(cudaStreamSynchronize(st));

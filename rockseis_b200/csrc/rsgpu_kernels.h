@@ -17,12 +17,15 @@ enum { TILECFG_64x32 = 0, TILECFG_32x16 = 3, TILECFG_DEFAULT = 6 };
 
 // One half-step (half = 0 velocity, 1 stress) of every tile in args.
 // maps: per shot NMAP2D CUtensorMaps of the halo-loaded fields; err: device error word.
-cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, bool adj, const void *args, const void *coefs,
+// flags: LAUNCH_ADJ (adjoint kernels), LAUNCH_PERSISTENT (elastic forward only:
+// one persistent CTA set walking all tiles with double-buffered TMA stages)
+enum { LAUNCH_ADJ = 1, LAUNCH_PERSISTENT = 2 };
+cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, int flags, const void *args, const void *coefs,
                            const void *maps, int *err, int grid, cudaStream_t st);
 constexpr int NMAP2D = 5;
 // Kernel instantiation table (generated at build time): variant "f32x" (exact),
 // "f32f" (fast), "f64"; nullptr if the tile config is not built for the variant.
-using Launch2DFn = cudaError_t (*)(int physics, int half, bool adj, const void *args, const void *coefs,
+using Launch2DFn = cudaError_t (*)(int physics, int half, int flags, const void *args, const void *coefs,
                                    const void *maps, int *err, int grid, cudaStream_t st);
 Launch2DFn launch_2d_table(const char *variant, int cfg);
 // Source injection followed by receiver recording, one CTA per shot.
