@@ -492,16 +492,17 @@ A3D = dict(nx=400, ny=400, nz=300, dx=12.5, lpml=20, order=8, nt=2500, dt=1e-3, 
            f0=12.0, sz=25.0)
 
 
-def a3d_config(f=A3D):
-    return {"workload": "acoustic3d_forward_32shots_400x400x300_windows_nt2500", "nx": f["nx"], "ny": f["ny"],
+def a3d_config(nshots=None, f=A3D):
+    ns = f["nshots"] if nshots is None else min(nshots, f["nshots"])
+    return {"workload": f"acoustic3d_forward_{ns}shots_400x400x300_windows_nt2500", "nx": f["nx"], "ny": f["ny"],
             "nz": f["nz"], "dx": f["dx"], "lpml": f["lpml"], "order": f["order"], "nt": f["nt"], "dt": f["dt"],
-            "shots": f["nshots"], "time_steps_per_bench_step": f["chunk"],
+            "shots": ns, "time_steps_per_bench_step": f["chunk"],
             "windows": "per-shot aperture windows (apertures uniform in [1500, 5000] m, seed 6)",
             "l2": "working set tens of GB > 126 MB L2 (no flush needed)"}
 
 
-def a3d_batch(precision, f=A3D):
-    """The 32 windowed shots of the 3D workload: (local models, sources, receivers)."""
+def a3d_batch(precision, f=A3D, nshots=None):
+    """The windowed shots of the 3D workload (the first nshots of 32): (local models, sources, receivers)."""
     from rockseis_b200 import abi, synth
     from rockseis_b200.rockseis import SMAP, Data3D, ModelAcoustic3D
     vp = synth.dipping_vp_3d(f["nx"], f["ny"], f["nz"], f["dx"], seed=5, vclip=4550.0)
@@ -517,7 +518,7 @@ def a3d_batch(precision, f=A3D):
     apert = rng.uniform(1500.0, 5000.0, (f["nshots"], 2))
     wav = synth.ricker(f["nt"], f["dt"], f["f0"], abi.real_dtype(precision))
     models, srcs, recs = [], [], []
-    for k in range(f["nshots"]):
+    for k in range(f["nshots"] if nshots is None else min(nshots, f["nshots"])):
         sx, sy = pos[k]
         s_ = Data3D(1, f["nt"], f["dt"], 0.0, precision)
         s_.scoords[:] = [[sx, sy, f["sz"]]]
@@ -577,7 +578,7 @@ def run_a3d(args, device=0, f=A3D):
     from rockseis_b200 import abi
     from rockseis_b200.rockseis import make_config, make_shot
     prec = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
-    models, srcs, recs = a3d_batch(prec)
+    models, srcs, recs = a3d_batch(prec, nshots=args.shots)
     cfg = make_config(models[0], f["order"], f["nt"], f["dt"], prec)
     keep: list = []
     shots = (abi.Shot * len(models))(*[make_shot(m, s_, r, keep) for m, s_, r in zip(models, srcs, recs)])
@@ -671,6 +672,8 @@ def main():
                          "fwi: the FWI gradient line alone")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
+    ap.add_argument("--shots", type=int, default=None,
+                    help="acoustic3d: model only the first N windows (profiling runs)")
     args = ap.parse_args()
 
     if args.impl == "reference" and args.workload == "fwi":
@@ -734,7 +737,7 @@ def main():
         line = {"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded dipping layers, windowed shots)",
-                "config": a3d_config(), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "config": a3d_config(args.shots), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
                 "clocks": r["clocks"], "acoustic3d": {k: v for k, v in r.items() if k not in ("roofline", "clocks")},
                 "cpu_baseline": cpu}
         print(json.dumps(line))

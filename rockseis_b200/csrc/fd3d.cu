@@ -62,11 +62,11 @@ __device__ __forceinline__ T taps_reg(const T (&q)[16], const T *cu, T d, T r)
 // (Plane ze, read by the last prefetch, lies inside the allocation; a value read
 // there belongs to the next z-chunk and is not used.)
 template <typename T, int MODE>
-__global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, const CoefSet3<T> *coefs)
+__global__ void __launch_bounds__(TX3 *TY3, 3) a3d_velocity(Step3DArgs<T> a, const CoefSet3<T> *coefs)
 {
     using A = Ar<T, MODE>;
     __shared__ CoefSet3<T> cs;
-    __shared__ T sP[TY3 + 16][TX3 + 16];
+    __shared__ T sPb[2][TY3 + 16][TX3 + 16];   // ping-pong: one barrier per plane
     load_coefs3(cs, coefs);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const Tile3D tl = a.tiles[blockIdx.x];
@@ -96,7 +96,9 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, con
     T hy0 = ty < 8 ? P[o - 8 * pitch] : T(0), hy1 = ty < 8 ? P[o + TY3 * pitch] : T(0);
     const T *cux = cs.cx + order * CROW3, *cuy = cs.cy + order * CROW3, *cuz = cs.cz + order * CROW3;
     for (int iz = z0; iz < ze; iz++, o += plane) {
-        __syncthreads();
+        // the buffer written here was last read two planes ago, before the
+        // previous plane's barrier
+        T (*sP)[TX3 + 16] = sPb[(iz - z0) & 1];
         sP[ty + 8][tx + 8] = q[7];
         if (tx < 16) sP[ty + 8][tx < 8 ? tx : tx + TX3] = hxv;
         if (ty < 8) {
@@ -152,12 +154,12 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_velocity(Step3DArgs<T> a, con
 //   P += dt*L*Dx-Vx [x C-PML]; P += dt*L*Dy-Vy [y]; P += dt*L*Dz-Vz [z].
 // Pipelined like the velocity half-step.
 template <typename T, int MODE>
-__global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const CoefSet3<T> *coefs)
+__global__ void __launch_bounds__(TX3 *TY3, 3) a3d_stress(Step3DArgs<T> a, const CoefSet3<T> *coefs)
 {
     using A = Ar<T, MODE>;
     __shared__ CoefSet3<T> cs;
-    __shared__ T sVx[TY3][TX3 + 16];
-    __shared__ T sVy[TY3 + 16][TX3];
+    __shared__ T sVxb[2][TY3][TX3 + 16];       // ping-pong: one barrier per plane
+    __shared__ T sVyb[2][TY3 + 16][TX3];
     load_coefs3(cs, coefs);
     const int tx = threadIdx.x, ty = threadIdx.y;
     const Tile3D tl = a.tiles[blockIdx.x];
@@ -185,7 +187,8 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) a3d_stress(Step3DArgs<T> a, const
     T hy0 = ty < 8 ? Vy[o - 8 * pitch] : T(0), hy1 = ty < 8 ? Vy[o + TY3 * pitch] : T(0);
     const T *cux = cs.cx + order * CROW3, *cuy = cs.cy + order * CROW3, *cuz = cs.cz + order * CROW3;
     for (int iz = z0; iz < ze; iz++, o += plane) {
-        __syncthreads();
+        T (*sVx)[TX3 + 16] = sVxb[(iz - z0) & 1];
+        T (*sVy)[TX3] = sVyb[(iz - z0) & 1];
         sVx[ty][tx + 8] = vxc;
         sVy[ty + 8][tx] = vyc;
         if (tx < 16) sVx[ty][tx < 8 ? tx : tx + TX3] = hxv;

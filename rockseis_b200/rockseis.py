@@ -371,6 +371,7 @@ class _Modelling:
         self.recP = self.recVx = self.recVy = self.recVz = None
         self.tile = -1
         self.zchunk = 0
+        self.launch_mode = 0
 
     def setModel(self, m): self.model = m
     def setSource(self, s): self.source = s
@@ -389,6 +390,7 @@ class _Modelling:
         recs = [r for r in (self.recP, self.recVx, self.recVy, self.recVz) if r is not None]
         cfg = make_config(self.model, self.order, self.source.nt, self.source.dt, self.precision, self.tile)
         cfg.zchunk = int(self.zchunk)
+        cfg.launch_mode = int(self.launch_mode)
         keep: list = []
         # one shot per recorded field; the wavefield computation is shared by
         # the reference, here each receiver set is a separate batch entry
