@@ -68,6 +68,8 @@ def oracle() -> C.CDLL:
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
         _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V] + \
             [V] * 4 + [V, V, V]
+        _oracle.orc_fwi_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 7 + [I, V, V, V, I, V, V, V] + \
+            [V] * 5 + [V]
         _oracle.orc_rtm_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 5 + [I, V, V, V, I, V, V, V, I, I, I, V]
         _oracle.orc_mod_a3d.argtypes = [C.POINTER(OrcGrid3)] + [V] * 5 + [I, V, V, V, I, I, V, V, I, V, I, V]
     return _oracle
@@ -94,6 +96,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+        _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
         _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
         _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
@@ -385,3 +388,39 @@ def orc_rtm_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, data, nhx=1, n
                              _p(ss), _p(w), len(gm), _p(gm), _p(gs), _p(d), nhx, nhy, nhz, _p(img))
     assert r == 0
     return img
+
+
+def ref_fwi_a3d(pb, scoords, wav, gcoords, obs, ncheck):
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    ns, nr = len(sc), len(gc)
+    o = {k: np.zeros((pb.nz, pb.ny, pb.nx), np.float32) for k in ("vpgrad", "rhograd")}
+    wg = np.zeros((ns, pb.nt), np.float32)
+    dm = np.zeros((nr, pb.nt), np.float32)
+    dr = np.zeros((nr, pb.nt), np.float32)
+    mis = C.c_double()
+    vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=np.float32)
+    r = ref().ref_fwi_a3d_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
+                            _p(o["vpgrad"]), _p(o["rhograd"]), _p(wg), _p(dm), _p(dr), C.byref(mis))
+    assert r == 1
+    o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
+    return o
+
+
+def orc_fwi_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
+    g = pb.orc_grid()
+    ns, nr = len(smap), len(gmap)
+    o = {k: np.zeros((pb.nz, pb.ny, pb.nx), np.float32) for k in ("vpgrad", "rhograd")}
+    wg = np.zeros((ns, pb.nt), np.float32)
+    dm = np.zeros((nr, pb.nt), np.float32)
+    dr = np.zeros((nr, pb.nt), np.float32)
+    mis = C.c_double()
+    Rx, Ry, Rz, L, tb, ss, w, gs, ob, vp, rho = _keep(*padded, tab, sshift, wav, gshift, obs, pb.vp, pb.rho,
+                                                      dtype=np.float32)
+    sm, gm = _keep(smap, gmap, dtype=np.int32)
+    r = oracle().orc_fwi_a3d(C.byref(g), pb.nx, pb.ny, pb.nz, _p(vp), _p(rho), _p(Rx), _p(Ry), _p(Rz), _p(L), _p(tb),
+                             ns, _p(sm), _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), _p(o["vpgrad"]), _p(o["rhograd"]),
+                             _p(wg), _p(dm), _p(dr), C.byref(mis))
+    assert r == 0
+    o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
+    return o

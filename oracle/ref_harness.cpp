@@ -191,6 +191,44 @@ int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
     return r;
 }
 
+/* FwiAcoustic3D::run_optimal (lib/fwi.cpp:1991-2160), DIFFERENCE misfit. */
+template <typename T>
+int fwi_a3d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav, int nr,
+            const double *gc, const T *obs, int ncheck, T *vpgrad, T *rhograd, T *wavgrad, T *datamod, T *datares,
+            double *misfit)
+{
+    auto model = make_a3d<T>(g, vp, rho);
+    auto geom = model->getGeom();
+    auto src = make_data3d<T>(ns, g, sc, PRESSURE, SMAP, geom, wav);
+    auto dobs = make_data3d<T>(nr, g, gc, PRESSURE, GMAP, geom, obs);
+    auto dmod = make_data3d<T>(nr, g, gc, PRESSURE, GMAP, geom, nullptr);
+    auto dres = make_data3d<T>(nr, g, gc, PRESSURE, GMAP, geom, nullptr);
+    auto wg = make_data3d<T>(ns, g, sc, PRESSURE, SMAP, geom, nullptr);
+    auto ivp = std::make_shared<Image3D<T>>(g->nx, g->ny, g->nz, 1, 1, 1, (T)g->dx, (T)g->dy, (T)g->dz, (T)g->ox,
+                                            (T)g->oy, (T)g->oz);
+    auto irho = std::make_shared<Image3D<T>>(g->nx, g->ny, g->nz, 1, 1, 1, (T)g->dx, (T)g->dy, (T)g->dz, (T)g->ox,
+                                             (T)g->oy, (T)g->oz);
+    FwiAcoustic3D<T> fwi(model, src, dobs, g->order, 1);
+    fwi.setDatamodP(dmod);
+    fwi.setDataresP(dres);
+    fwi.setVpgrad(ivp);
+    fwi.setRhograd(irho);
+    fwi.setWavgrad(wg);
+    fwi.setMisfit_type(DIFFERENCE);
+    fwi.setNcheck(ncheck);
+    fwi.setIncore(true);
+    fwi.setSnapfile(tmpname("fwia3d"));
+    int r = fwi.run_optimal();
+    size_t n = (size_t)g->nx * g->ny * g->nz;
+    std::memcpy(vpgrad, ivp->getImagedata(), sizeof(T) * n);
+    std::memcpy(rhograd, irho->getImagedata(), sizeof(T) * n);
+    std::memcpy(wavgrad, wg->getData(), sizeof(T) * (size_t)ns * g->nt);
+    std::memcpy(datamod, dmod->getData(), sizeof(T) * (size_t)nr * g->nt);
+    std::memcpy(datares, dres->getData(), sizeof(T) * (size_t)nr * g->nt);
+    *misfit = (double)fwi.getMisfit();
+    return r;
+}
+
 /* nsteps of forwardstepVelocity / forwardstepStress / insertSource on a fresh
  * wavefield, state copied out field by field (step-level parity). */
 template <typename T>
@@ -405,6 +443,13 @@ int ref_mod_e3d_f(const ref_grid *g, const float *vp, const float *vs, const flo
                   float *out)
 { return mod_e3d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, rfield, out); }
 
+int ref_fwi_a3d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc, const float *wav,
+                  int nr, const double *gc, const float *obs, int ncheck, float *vpgrad, float *rhograd,
+                  float *wavgrad, float *datamod, float *datares, double *misfit)
+{
+    return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
+                          misfit);
+}
 int ref_fwi_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                   const float *wav, int sfield, int nr, const double *gc, const float *obsp, const float *obsx,
                   const float *obsz, int ncheck, float *vpgrad, float *vsgrad, float *rhograd, float *wavgrad,

@@ -847,3 +847,81 @@ int orc_rtm_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *Rx, con
     free(Ps);
     return 0;
 }
+
+/* FwiAcoustic3D::crossCorr (lib/fwi.cpp:1403-1466) on 1..n-1 of the unpadded window.
+ * The reference's last z-term uses the adjoint Vz of the cell below in y (iy-1),
+ * with Rz of the cell above in z (iz-1); that is restated as it is. */
+static void a3d_corr(const orc_grid3 *g, int nx, int ny, int nz, const float *Vp, const float *Rho, const float *Rx,
+                     const float *Ry, const float *Rz, const float *wsp, const float *wrx, const float *wry,
+                     const float *wrz, float *vpgrad, float *rhograd)
+{
+    const int L = g->lpml;
+    const long sy = g->nxp, sz = (long)g->nxp * g->nyp;
+    const float dx = g->dx, dy = g->dy, dz = g->dz;
+    for (int ix = 1; ix < nx; ix++)
+        for (int iy = 1; iy < ny; iy++)
+            for (int iz = 1; iz < nz; iz++) {
+                long q = (iz + L) * sz + (iy + L) * sy + (ix + L);
+                long u = ((long)iz * ny + iy) * nx + ix;
+                float vpscale = -2.0 / (Vp[u]);
+                float rhoscale1 = -1.0 / (Rho[u]);
+                float mrxx = (wrx[q] - wrx[q - 1]) / dx;
+                float mryy = (wry[q] - wry[q - sy]) / dy;
+                float mrzz = (wrz[q] - wrz[q - sz]) / dz;
+                vpgrad[u] -= vpscale * wsp[q] * (mrxx + mryy + mrzz);
+                rhograd[u] -= rhoscale1 * wsp[q] * (mrxx + mryy + mrzz);
+                float uderx = (0.5) * wrx[q] * Rx[q] * (wsp[q + 1] - wsp[q]) / dx;
+                uderx += (0.5) * wrx[q - 1] * Rx[q - 1] * (wsp[q] - wsp[q - 1]) / dx;
+                float udery = (0.5) * wry[q] * Ry[q] * (wsp[q + sy] - wsp[q]) / dy;
+                udery += (0.5) * wry[q - sy] * Ry[q - sy] * (wsp[q] - wsp[q - sy]) / dy;
+                float uderz = (0.5) * wrz[q] * Rz[q] * (wsp[q + sz] - wsp[q]) / dz;
+                uderz += (0.5) * wrz[q - sy] * Rz[q - sz] * (wsp[q] - wsp[q - sz]) / dz;
+                rhograd[u] += (uderx + udery + uderz);
+            }
+}
+
+/* FwiAcoustic3D::run_optimal with the DIFFERENCE misfit and pressure data, one shot,
+ * all forward pressures kept (pairing as fw_state_at()). */
+int orc_fwi_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *vp, const float *rho, const float *Rx,
+                const float *Ry, const float *Rz, const float *Lm, const float *tab, int ns, const int *smap,
+                const float *sshift, const float *wav, int nr, const int *gmap, const float *gshift, const float *obs,
+                float *vpgrad, float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
+{
+    const int nt = g->nt;
+    const long n = (long)g->nxp * g->nyp * g->nzp;
+    float *Ps = malloc((size_t)nt * n * sizeof(float));
+    if (!Ps) return -1;
+    orc_state3 fw, bw;
+    st3_alloc(&fw, g);
+    st3_alloc(&bw, g);
+    for (int it = 0; it < nt; it++) {
+        a3d_step(&fw, Rx, Ry, Rz, Lm, tab);
+        inject3(&fw, Lm, 0, ns, smap, sshift, wav, it);
+        record3(&fw, 0, nr, gmap, gshift, datamod, it);
+        memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
+    }
+    float mis = 0.0f;
+    for (int tr = 0; tr < nr; tr++) {
+        const int valid = gmap[3 * tr] >= 0 && gmap[3 * tr + 1] >= 0 && gmap[3 * tr + 2] >= 0;
+        for (int it = 0; it < nt; it++) {
+            long k = it + (long)tr * nt;
+            float r = datamod[k] - obs[k];
+            if (valid) mis += 0.5 * r * r;
+            datares[k] = 1 * (datamod[k] - obs[k]);
+        }
+    }
+    *misfit = mis;
+    float *zero = calloc(n, sizeof(float));
+    for (int it = nt - 1; it >= 0; it--) {
+        if (it < nt - 1) a3d_step(&bw, Rx, Ry, Rz, Lm, tab);
+        inject3(&bw, Lm, 0, nr, gmap, gshift, datares, it);
+        a3d_corr(g, nx, ny, nz, vp, rho, Rx, Ry, Rz, fw_state_at(Ps, zero, n, nt, it), bw.f[1], bw.f[2], bw.f[3],
+                 vpgrad, rhograd);
+        record3(&bw, 0, ns, smap, sshift, wavgrad, it);
+    }
+    free(zero);
+    st3_free(&fw);
+    st3_free(&bw);
+    free(Ps);
+    return 0;
+}

@@ -283,6 +283,64 @@ __global__ void __launch_bounds__(256) corr_fwi_e2d(const Corr2DE<T> *desc, T dx
     }
 }
 
+// FwiAcoustic3D::crossCorr (lib/fwi.cpp:1403-1466) on 1..n-1 of the unpadded
+// window, one thread per (x, y) column marching z.  The reference's second z term
+// takes the adjoint Vz of the cell at y-1 with Rz of the cell at z-1 (as written
+// there); it is reproduced as it is.
+template <typename T, bool EXACT, typename G>
+__global__ void __launch_bounds__(256) corr_fwi_a3d(const Corr3DF<T> *desc, T dx, T dy, T dz)
+{
+    const Corr3DF<T> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix < 1 || iy < 1 || ix >= c.nx || iy >= c.ny) return;
+    const long long P = c.pitch, PL = c.plane;
+    const int L = c.lpml;
+    for (int iz = 1; iz < c.nz; iz++) {
+        const long long q = (long long)(iz + L) * PL + (long long)(iy + L) * P + (ix + L);
+        const long long u = ((long long)iz * c.ny + iy) * c.nx + ix;
+        const T ws = c.wsp[q];
+        G *vg = (G *)c.g0 + u, *rg = (G *)c.g1 + u;
+        T a, b, ud;
+        if (EXACT) {
+            using O = X<T>;
+            const T vpscale = O::rnd(__ddiv_rn(-2.0, (double)c.vp[u]));
+            const T rhoscale1 = O::rnd(__ddiv_rn(-1.0, (double)c.rho[u]));
+            const T mrxx = O::div(O::sub(c.wrx[q], c.wrx[q - 1]), dx);
+            const T mryy = O::div(O::sub(c.wry[q], c.wry[q - P]), dy);
+            const T mrzz = O::div(O::sub(c.wrz[q], c.wrz[q - PL]), dz);
+            const T s = O::add(O::add(mrxx, mryy), mrzz);
+            a = O::mul(O::mul(vpscale, ws), s);
+            b = O::mul(O::mul(rhoscale1, ws), s);
+            const double DX = (double)dx, DY = (double)dy, DZ = (double)dz;
+            T ux = O::rnd(half_term(c.wrx[q], c.rx[q], O::sub(c.wsp[q + 1], ws), DX));
+            ux = O::rnd(__dadd_rn((double)ux, half_term(c.wrx[q - 1], c.rx[q - 1], O::sub(ws, c.wsp[q - 1]), DX)));
+            T uy = O::rnd(half_term(c.wry[q], c.ry[q], O::sub(c.wsp[q + P], ws), DY));
+            uy = O::rnd(__dadd_rn((double)uy, half_term(c.wry[q - P], c.ry[q - P], O::sub(ws, c.wsp[q - P]), DY)));
+            T uz = O::rnd(half_term(c.wrz[q], c.rz[q], O::sub(c.wsp[q + PL], ws), DZ));
+            uz = O::rnd(__dadd_rn((double)uz, half_term(c.wrz[q - P], c.rz[q - PL], O::sub(ws, c.wsp[q - PL]), DZ)));
+            ud = O::add(O::add(ux, uy), uz);
+        } else {
+            const T rdx = T(1) / dx, rdy = T(1) / dy, rdz = T(1) / dz;
+            const T s = (c.wrx[q] - c.wrx[q - 1]) * rdx + (c.wry[q] - c.wry[q - P]) * rdy + (c.wrz[q] - c.wrz[q - PL]) * rdz;
+            a = (T(-2) / c.vp[u]) * ws * s;
+            b = (T(-1) / c.rho[u]) * ws * s;
+            ud = T(0.5) * ((c.wrx[q] * c.rx[q] * (c.wsp[q + 1] - ws) + c.wrx[q - 1] * c.rx[q - 1] * (ws - c.wsp[q - 1])) * rdx +
+                           (c.wry[q] * c.ry[q] * (c.wsp[q + P] - ws) + c.wry[q - P] * c.ry[q - P] * (ws - c.wsp[q - P])) * rdy +
+                           (c.wrz[q] * c.rz[q] * (c.wsp[q + PL] - ws) + c.wrz[q - P] * c.rz[q - PL] * (ws - c.wsp[q - PL])) * rdz);
+        }
+        if (sizeof(G) == sizeof(T)) {
+            using O = X<T>;
+            *(T *)vg = EXACT ? O::sub(*(T *)vg, a) : *(T *)vg - a;
+            const T r1 = EXACT ? O::sub(*(T *)rg, b) : *(T *)rg - b;
+            *(T *)rg = EXACT ? O::add(r1, ud) : r1 + ud;
+        } else {
+            *vg = __dsub_rn((double)*vg, (double)a);
+            *rg = __dadd_rn(__dsub_rn((double)*rg, (double)b), (double)ud);
+        }
+    }
+}
+
 // FwiElastic2D::scaleGrad (lib/fwi.cpp:2778-2849): lambda/mu/rho correlations to
 // vp/vs/rho gradients, over the whole window.
 template <typename T, typename G>
@@ -525,6 +583,22 @@ cudaError_t launch_corr_rtm_a3d(int prec, int acc, const void *desc, int nshots,
     } else {
         if (prec == PREC_F32_EXACT) corr_rtm_a3d<float, true, float><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
         else corr_rtm_a3d<float, false, float><<<grid, block, 0, st>>>((const Corr3D<float> *)desc, nhx, nhy, nhz);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_corr_fwi_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, double dx,
+                                double dy, double dz, cudaStream_t st)
+{
+    const dim3 block(32, 8), grid((nxmax + 31) / 32, (nymax + 7) / 8, nshots);
+    if (prec == PREC_F64)
+        corr_fwi_a3d<double, true, double><<<grid, block, 0, st>>>((const Corr3DF<double> *)desc, dx, dy, dz);
+    else if (prec == PREC_F32_EXACT) {
+        if (acc == ACC_F64) corr_fwi_a3d<float, true, double><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
+        else corr_fwi_a3d<float, true, float><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
+    } else {
+        if (acc == ACC_F64) corr_fwi_a3d<float, false, double><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
+        else corr_fwi_a3d<float, false, float><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
     }
     return cudaGetLastError();
 }

@@ -1,8 +1,9 @@
-// RTM image driver for 3D acoustic shots (host runtime behind rsgpu_rtm_image and
-// rsgpu_adjoint_* for RSGPU_ACOUSTIC3D).
+// RTM image and FWI gradient drivers for 3D acoustic shots (host runtime behind
+// rsgpu_rtm_image, rsgpu_fwi_gradient and rsgpu_adjoint_* for RSGPU_ACOUSTIC3D).
 //
 // The reference's RtmAcoustic3D::run_optimal (lib/rtm.cpp:735-859) runs the same
-// Revolve-driven loop as the 2D drivers: a forward propagator checkpointed in
+// Revolve-driven loop as the 2D drivers (FwiAcoustic3D::run_optimal,
+// lib/fwi.cpp:1991-2160, likewise): a forward propagator checkpointed in
 // `ncheck` slots, an adjoint propagator fed with the recorded data, and a
 // correlation of both pressures at every adjoint time level.  Here the forward and
 // adjoint wavefields of all shots are two batched 3D plans (z-marching kernels)
@@ -12,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -50,12 +52,16 @@ Adjoint3D::~Adjoint3D()
     if (stream) cudaStreamDestroy(stream);
 }
 
-rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
+rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int k_, int ns,
                                const rsgpu_adjoint_shot *s)
 {
     if (!c || !o || !s || ns < 1) { set_error("null config/options/shots or nshots < 1"); return RSGPU_ERR_ARG; }
-    if (c->physics != RSGPU_ACOUSTIC3D || kind != RSGPU_KIND_RTM) {
-        set_error("the 3D adjoint driver is built for acoustic RTM images");
+    if (c->physics != RSGPU_ACOUSTIC3D || (k_ != RSGPU_KIND_RTM && k_ != RSGPU_KIND_FWI)) {
+        set_error("the 3D adjoint driver is built for acoustic RTM images and FWI gradients");
+        return RSGPU_ERR_UNSUPPORTED;
+    }
+    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE) {
+        set_error("only the DIFFERENCE misfit is built");
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
@@ -64,7 +70,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     }
     if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
     const int hy = o->nhy > 0 ? o->nhy : 1;
-    if (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || hy % 2 == 0 || o->nhz % 2 == 0) {
+    if (k_ == RSGPU_KIND_RTM && (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || hy % 2 == 0 || o->nhz % 2 == 0)) {
         set_error("nhx, nhy and nhz must be odd and positive");
         return RSGPU_ERR_ARG;
     }
@@ -76,6 +82,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
         if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
         if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
+        if (k_ == RSGPU_KIND_FWI && (!s[i].vp || !s[i].rho)) { set_error("shot %d: vp/rho are null", i); return RSGPU_ERR_ARG; }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
@@ -83,6 +90,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         set_error("no CUDA device");
         return RSGPU_ERR_NODEVICE;
     }
+    kind = k_;
     cfg = *c;
     nshots = ns;
     prec = c->precision;
@@ -90,7 +98,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     acc = o->accum == RSGPU_ACCUM_F64 ? ACC_F64 : ACC_REF;
     ck = o->ckpt_precision;
     ck_es = ck == CK_NATIVE ? (size_t)es : 2;
-    nhx = o->nhx; nhy = hy; nhz = o->nhz;
+    nhx = fwi() ? 1 : o->nhx;
+    nhy = fwi() ? 1 : hy;
+    nhz = fwi() ? 1 : o->nhz;
     {
         RevolveSchedule probe(c->nt, o->ncheck);
         ncheck = probe.snaps();
@@ -100,18 +110,21 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     std::vector<rsgpu_shot> fs(ns), bs(ns);
     for (int i = 0; i < ns; i++) {
         fs[i] = s[i].shot;
-        fs[i].nrec = 0;                      // the forward run records nothing
+        if (!fwi()) fs[i].nrec = 0;          // RTM: the forward run records nothing
         fs[i].rec_out = nullptr;
         bs[i] = s[i].shot;
         bs[i].nsrc = s[i].shot.nrec;         // the data, injected at the receivers
         bs[i].smap = s[i].shot.gmap;
         bs[i].sshift = s[i].shot.gshift;
-        bs[i].wavelet = s[i].data;
-        bs[i].nrec = 0;
+        bs[i].wavelet = s[i].data;           // FWI: replaced by the residuals
+        bs[i].nrec = fwi() ? s[i].shot.nsrc : 0;   // FWI: the wavelet gradient at the sources
+        bs[i].gmap = s[i].shot.smap;
+        bs[i].gshift = s[i].shot.sshift;
         bs[i].rec_out = nullptr;
     }
     fw.reset(new Plan3D());
     fw->shared_stream = stream;
+    fw->gated_recording = fwi();
     ST(fw->create(c, ns, fs.data()));
     bw.reset(new Plan3D());
     bw->shared_stream = stream;
@@ -121,16 +134,28 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off = rupa(off + std::max<size_t>(bytes, 1), 256); return r; };
-    o_img.assign(ns, 0);
-    nx.resize(ns); ny.resize(ns); nz.resize(ns);
+    for (auto *v : {&o_img, &o_vp, &o_rho, &o_obs, &o_g1, &o_valid}) v->assign(ns, 0);
+    nx.resize(ns); ny.resize(ns); nz.resize(ns); nrec.resize(ns);
     for (int i = 0; i < ns; i++) {
-        nx[i] = s[i].shot.nx; ny[i] = s[i].shot.ny; nz[i] = s[i].shot.nz;
+        nx[i] = s[i].shot.nx; ny[i] = s[i].shot.ny; nz[i] = s[i].shot.nz; nrec[i] = s[i].shot.nrec;
         nxmax = std::max(nxmax, nx[i]);
         nymax = std::max(nymax, ny[i]);
-        o_img[i] = take((size_t)nx[i] * ny[i] * nz[i] * nhx * nhy * nhz * gs);
+        const size_t n3 = (size_t)nx[i] * ny[i] * nz[i];
+        o_img[i] = take(n3 * nhx * nhy * nhz * gs);     // RTM image, or FWI vp gradient
+        if (fwi()) {
+            o_vp[i] = take(n3 * es);
+            o_rho[i] = take(n3 * es);
+            o_obs[i] = take((size_t)nrec[i] * cfg.nt * es);
+            o_g1[i] = take(n3 * gs);
+            o_valid[i] = take(sizeof(int) * nrec[i]);
+        }
     }
-    const size_t corr_bytes = prec == PREC_F64 ? sizeof(Corr3D<double>) : sizeof(Corr3D<float>);
+    const size_t corr_bytes = fwi() ? (prec == PREC_F64 ? sizeof(Corr3DF<double>) : sizeof(Corr3DF<float>))
+                                    : (prec == PREC_F64 ? sizeof(Corr3D<double>) : sizeof(Corr3D<float>));
+    const size_t res_bytes = prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>);
     o_corr = take(corr_bytes * ns);
+    o_res = take(res_bytes * ns);
+    o_misfit = take(sizeof(double) * ns);
     segs.clear();
     slot_elems = 0;
     for (int i = 0; i < ns; i++) {
@@ -168,8 +193,62 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     }
     CU(cudaMemsetAsync(dbuf, 0, off, stream));
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
-    std::vector<unsigned char> corr(corr_bytes * ns);
-    for (int i = 0; i < ns; i++) {
+    std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
+    std::vector<std::vector<int>> valids(ns);   // host copies stay alive until the stream sync below
+    for (int i = 0; i < ns && fwi(); i++) {
+        const size_t n3 = (size_t)nx[i] * ny[i] * nz[i];
+        CU(cudaMemcpyAsync(D(o_vp[i]), s[i].vp, n3 * es, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(D(o_rho[i]), s[i].rho, n3 * es, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(D(o_obs[i]), s[i].data, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        // misfit mask: a receiver counts when its map lies on the grid (lib/fwi.cpp:1500)
+        std::vector<int> &valid = valids[i];
+        valid.resize(nrec[i]);
+        for (int t = 0; t < nrec[i]; t++) {
+            const int *m = s[i].shot.gmap + 3 * t;
+            valid[t] = (m[0] >= 0 && m[1] >= 0 && m[2] >= 0) ? 0 : -1;
+        }
+        CU(cudaMemcpyAsync(D(o_valid[i]), valid.data(), sizeof(int) * valid.size(), cudaMemcpyHostToDevice, stream));
+    }
+    for (int i = 0; i < ns && fwi(); i++) {
+        const Layout3D &F = fw->shots[i], &B = bw->shots[i];
+        char *fa = (char *)fw->arena, *ba = (char *)bw->arena;
+        const size_t fo = fw->origin_bytes(F), bo = bw->origin_bytes(B);
+        auto fill = [&](auto *d, auto *r) {
+            using T = typename std::remove_const<typename std::remove_pointer<decltype(d->wsp)>::type>::type;
+            d->wsp = (const T *)(fa + F.f[A3_P] + fo);
+            d->wrx = (const T *)(ba + B.f[A3_VX] + bo);
+            d->wry = (const T *)(ba + B.f[A3_VY] + bo);
+            d->wrz = (const T *)(ba + B.f[A3_VZ] + bo);
+            d->rx = (const T *)(fa + F.m[M3_RX] + fo);
+            d->ry = (const T *)(fa + F.m[M3_RY] + fo);
+            d->rz = (const T *)(fa + F.m[M3_RZ] + fo);
+            d->vp = (const T *)D(o_vp[i]);
+            d->rho = (const T *)D(o_rho[i]);
+            d->g0 = D(o_img[i]);
+            d->g1 = D(o_g1[i]);
+            d->nx = nx[i]; d->ny = ny[i]; d->nz = nz[i]; d->pitch = F.pitch; d->lpml = cfg.lpml; d->plane = F.plane;
+            r->mod = (const T *)(fa + F.traces);
+            r->obs = (const T *)D(o_obs[i]);
+            r->res = (T *)(ba + B.wav);
+            r->rec_pt = (const int *)D(o_valid[i]);
+            r->nrec = nrec[i];
+            r->nt = cfg.nt;
+        };
+        if (prec == PREC_F64) {
+            Corr3DF<double> d{};
+            Resid2D<double> r{};
+            fill(&d, &r);
+            std::memcpy(corr.data() + i * sizeof d, &d, sizeof d);
+            std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+        } else {
+            Corr3DF<float> d{};
+            Resid2D<float> r{};
+            fill(&d, &r);
+            std::memcpy(corr.data() + i * sizeof d, &d, sizeof d);
+            std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+        }
+    }
+    for (int i = 0; i < ns && !fwi(); i++) {
         const Layout3D &F = fw->shots[i], &B = bw->shots[i];
         if (prec == PREC_F64) {
             Corr3D<double> d{};
@@ -188,6 +267,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
     }
     CU(cudaMemcpyAsync(D(o_corr), corr.data(), corr.size(), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(D(o_res), res.data(), res.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -208,7 +288,8 @@ rsgpu_status Adjoint3D::slot_io(bool save, int slot)
 
 rsgpu_status Adjoint3D::correlate()
 {
-    cudaError_t e = launch_corr_rtm_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, nhx, nhy, nhz, stream);
+    cudaError_t e = fwi() ? launch_corr_fwi_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, cfg.dx, cfg.dy, cfg.dz, stream)
+                          : launch_corr_rtm_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, nhx, nhy, nhz, stream);
     if (e != cudaSuccess) { set_error("correlation launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
     launches += 1;
     return RSGPU_OK;
@@ -223,8 +304,11 @@ rsgpu_status Adjoint3D::run()
     ST(fw->reset());
     ST(bw->reset());
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
-    for (int i = 0; i < nshots; i++)
+    for (int i = 0; i < nshots; i++) {
         CU(cudaMemsetAsync(D(o_img[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * nhx * nhy * nhz * gs, stream));
+        if (fwi()) CU(cudaMemsetAsync(D(o_g1[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * gs, stream));
+    }
+    if (fwi()) ST(fw->set_recording(true));
     RevolveSchedule rev(nt, ncheck);
     for (;;) {
         const int oldcapo = rev.capo();
@@ -240,6 +324,12 @@ rsgpu_status Adjoint3D::run()
         } else if (a == RSGPU_FIRSTURN) {
             ST(fw->run(capo, 1));
             fw_steps += 1;
+            if (fwi()) {
+                ST(fw->set_recording(false));
+                cudaError_t e = launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+                launches += 1;
+            }
             ST(bw->inject_record_only(nt - 1 - capo));
             ST(correlate());
         } else if (a == RSGPU_YOUTURN) {
@@ -265,6 +355,52 @@ rsgpu_status Adjoint3D::read(int ns, const rsgpu_adjoint_shot *s)
     if (ns != nshots || !s) { set_error("read expects the %d shots of the batch", nshots); return RSGPU_ERR_ARG; }
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
     std::vector<unsigned char> tmp;
+    // add a device array of the accumulator type into a host array of the element type
+    auto add_from = [&](void *host, size_t o, size_t n) -> rsgpu_status {
+        tmp.resize(n * gs);
+        CU(cudaMemcpyAsync(tmp.data(), D(o), n * gs, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        if (es == 8) {
+            double *h = (double *)host;
+            const double *t = (const double *)tmp.data();
+            for (size_t k = 0; k < n; k++) h[k] += t[k];
+        } else if (gs == 8) {
+            float *h = (float *)host;
+            const double *t = (const double *)tmp.data();
+            for (size_t k = 0; k < n; k++) h[k] = (float)((double)h[k] + t[k]);
+        } else {
+            float *h = (float *)host;
+            const float *t = (const float *)tmp.data();
+            for (size_t k = 0; k < n; k++) h[k] += t[k];
+        }
+        return RSGPU_OK;
+    };
+    if (fwi()) {
+        std::vector<double> mis(nshots, 0.0);
+        CU(cudaMemcpyAsync(mis.data(), D(o_misfit), sizeof(double) * nshots, cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        for (int i = 0; i < nshots; i++) {
+            const size_t n3 = (size_t)nx[i] * ny[i] * nz[i];
+            if (s[i].vpgrad) ST(add_from(s[i].vpgrad, o_img[i], n3));
+            if (s[i].rhograd) ST(add_from(s[i].rhograd, o_g1[i], n3));
+            if (s[i].shot.rec_out) ST(fw->read_traces(i, s[i].shot.rec_out));
+            if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
+            if (s[i].datares) {
+                const size_t n = (size_t)nrec[i] * cfg.nt;
+                tmp.resize(n * es);
+                CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wav, n * es, cudaMemcpyDeviceToHost,
+                                   stream));
+                CU(cudaStreamSynchronize(stream));
+                if (es == 8) { double *h = (double *)s[i].datares; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) h[k] += t[k]; }
+                else { float *h = (float *)s[i].datares; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) h[k] += t[k]; }
+            }
+            if (s[i].misfit) {
+                if (acc == ACC_REF && es == 4) *s[i].misfit = (double)(float)((float)*s[i].misfit + (float)mis[i]);
+                else *s[i].misfit += mis[i];
+            }
+        }
+        return RSGPU_OK;
+    }
     for (int i = 0; i < nshots; i++) {
         if (!s[i].image) continue;
         const size_t n = (size_t)nx[i] * ny[i] * nz[i] * nhx * nhy * nhz;

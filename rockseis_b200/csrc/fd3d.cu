@@ -260,7 +260,7 @@ __global__ void inject_record_3d(const Shot3D<T> *shots, const InjRec3<T> *plans
             F[p] = v;
         }
     }
-    if (pl.kind_rec == REC3_NONE) return;
+    if (pl.kind_rec == REC3_NONE || (pl.rec_gate && *pl.rec_gate == 0)) return;
     __syncthreads();
     const T *F = sh.f[pl.kind_rec == REC3_P ? A3_P : pl.kind_rec == REC3_VX ? A3_VX : pl.kind_rec == REC3_VY ? A3_VY : A3_VZ];
     for (int tr = threadIdx.x; tr < pl.nrec; tr += blockDim.x) {

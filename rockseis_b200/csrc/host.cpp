@@ -369,6 +369,9 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
         return RSGPU_ERR_NOMEM;
     }
     CU(cudaMemsetAsync(arena, 0, arena_bytes, stream));
+    // the plan tables below go up with synchronous copies, which do not wait for the
+    // plan's non-blocking stream: let the clearing finish first
+    CU(cudaStreamSynchronize(stream));
     char *A = (char *)arena;
 
     // ---- uploads

@@ -182,6 +182,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         o_rw[i] = take(rec_w[i].size() * es);
     }
     const size_t o_pml = take((size_t)12 * lp * es);
+    rec_pt_offsets = o_rp;
     arena_bytes = off;
     if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -189,6 +190,9 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         return RSGPU_ERR_NOMEM;
     }
     CU(cudaMemsetAsync(arena, 0, arena_bytes, stream));
+    // the plan tables below go up with synchronous copies, which do not wait for the
+    // plan's non-blocking stream: let the clearing finish first
+    CU(cudaStreamSynchronize(stream));
     char *A = (char *)arena;
     std::vector<unsigned char> hb;
     auto put_real = [&](size_t o, const std::vector<double> &v) -> rsgpu_status {
@@ -252,9 +256,12 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     const size_t shot_bytes = prec == PREC_F64 ? sizeof(Shot3D<double>) : sizeof(Shot3D<float>);
     const size_t ir_bytes = prec == PREC_F64 ? sizeof(InjRec3<double>) : sizeof(InjRec3<float>);
     const size_t m_shots = 0, m_ir = rup3(ns * shot_bytes, 256), m_tiles = rup3(m_ir + ns * ir_bytes, 256);
-    const size_t m_coef = rup3(m_tiles + tiles.size() * sizeof(Tile3D), 256), m_end = m_coef + coefs.size();
+    const size_t m_coef = rup3(m_tiles + tiles.size() * sizeof(Tile3D), 256);
+    const size_t m_gate = rup3(m_coef + coefs.size(), 256), m_end = m_gate + 256;
     CU(cudaMalloc(&d_meta, m_end));
+    d_gate = reinterpret_cast<int *>((char *)d_meta + m_gate);
     std::vector<unsigned char> meta(m_end, 0);
+    reinterpret_cast<int *>(meta.data() + m_gate)[0] = 1;   // recording on
     for (int i = 0; i < ns; i++) {
         if (prec == PREC_F64) fill_desc<double>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes,
                                                 i, s[i], o_ip[i], o_is[i], o_it[i], o_iw[i], o_rp[i], o_rw[i],
@@ -311,6 +318,7 @@ void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu
     r.rec_out = (T *)(A + L.traces);
     r.nt = cfg.nt;
     r.rev = reverse_time ? 1 : 0;
+    r.rec_gate = gated_recording ? d_gate : nullptr;
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -350,6 +358,13 @@ rsgpu_status Plan3D::step(int it)
 fail:
     set_error("3D kernel launch failed: %s", cudaGetErrorString(e));
     return RSGPU_ERR_CUDA;
+}
+
+rsgpu_status Plan3D::set_recording(bool on)
+{
+    if (!gated_recording) { set_error("plan was created without gated recording"); return RSGPU_ERR_STATE; }
+    CU(cudaMemsetAsync(d_gate, on ? 1 : 0, sizeof(int), stream));
+    return RSGPU_OK;
 }
 
 rsgpu_status Plan3D::inject_record_only(int it)

@@ -69,6 +69,7 @@ struct InjRec3 {
     T *rec_out;                // [nrec * nt], accumulated
     int nt;
     int rev;                   // 1: step it reads wav[nt-1-it] and writes rec_out[nt-1-it]
+    const int *rec_gate;       // if non-null, recording happens only while *rec_gate != 0
 };
 enum { INJ3_NONE = 0, INJ3_P = 1, INJ3_VX = 2, INJ3_VY = 3, INJ3_VZ = 4 };
 enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4 };

@@ -48,6 +48,18 @@ struct Corr3D {
     long long plane;            // elements per plane of the pitched arrays
 };
 
+// 3D FWI gradient correlation inputs of one shot (FwiAcoustic3D::crossCorr).
+template <typename T>
+struct Corr3DF {
+    const T *wsp;               // forward pressure
+    const T *wrx, *wry, *wrz;   // adjoint velocities
+    const T *rx, *ry, *rz;      // staggered inverse densities
+    const T *vp, *rho;          // unpadded models [nz][ny][nx]
+    void *g0, *g1;              // vpgrad, rhograd [nz][ny][nx]
+    int nx, ny, nz, pitch, lpml, pad_;
+    long long plane;
+};
+
 // Residual and misfit of one shot (DIFFERENCE misfit).
 template <typename T>
 struct Resid2D {
@@ -86,6 +98,8 @@ cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshot
 cudaError_t launch_residual_e2d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
 cudaError_t launch_corr_rtm_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, int nhx,
                                 int nhy, int nhz, cudaStream_t st);
+cudaError_t launch_corr_fwi_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, double dx,
+                                double dy, double dz, cudaStream_t st);
 // Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
 // for the 16-bit formats (written by save, read by load).
 cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,

@@ -17,7 +17,7 @@ public:
     rsgpu_status run();
     rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
 
-    int nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
+    int kind = RSGPU_KIND_RTM, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
     int ncheck = 0, nxmax = 0, nymax = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan3D> fw, bw;
@@ -25,9 +25,10 @@ public:
     void *dbuf = nullptr, *ckpt = nullptr;
     size_t slot_elems = 0, ck_es = 4;
     std::vector<CkptSeg> segs;
-    std::vector<size_t> o_img;
-    size_t o_corr = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
-    std::vector<int> nx, ny, nz;
+    std::vector<size_t> o_img, o_vp, o_rho, o_obs, o_g1, o_valid;
+    size_t o_corr = 0, o_res = 0, o_misfit = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    std::vector<int> nx, ny, nz, nrec;
+    bool fwi() const { return kind == RSGPU_KIND_FWI; }
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
     bool ran = false;
 

@@ -31,11 +31,15 @@ public:
 
     // options read by create()
     bool reverse_time = false;                 // wavelet/trace index nt-1-it at step it
+    bool gated_recording = false;              // recording obeys set_recording()
+    rsgpu_status set_recording(bool on);
+    int *d_gate = nullptr;                     // recording switch (gated_recording)
     cudaStream_t shared_stream = nullptr;      // run on this caller-owned stream
 
     rsgpu_config cfg{};
     int prec = 0, nshots = 0, es = 4, zc = 64, ntiles = 0;
     std::vector<Layout3D> shots;
+    std::vector<size_t> rec_pt_offsets;        // per shot: arena offset of the receiver points (long long, -1 off grid)
     void *arena = nullptr, *d_meta = nullptr;
     size_t arena_bytes = 0;
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;

@@ -597,6 +597,12 @@ class FwiAcoustic2D(_Adjoint):
         return fwi_gradient_batch([self])
 
 
+class FwiAcoustic3D(FwiAcoustic2D):
+    """FwiAcoustic3D<T> (include/fwi.h:186-236): vp/rho gradients of the DIFFERENCE
+    misfit on a 3D window (gradients in Image3D containers)."""
+    cls = "FwiAcoustic3D"
+
+
 class FwiElastic2D(_Adjoint):
     """FwiElastic2D<T> (include/fwi.h:240-300): vp/vs/rho (and wavelet) gradients of
     the DIFFERENCE misfit of P, Ux and Uz data, run on the GPU with the adjoint

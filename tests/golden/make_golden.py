@@ -212,6 +212,14 @@ def a3d_cases(g):
     # extended 3D RTM image of the first case's gather
     pb = api.Problem3D(nx, ny, nz, dx, dx, dx, L, 8, 0, 1e-3, nt, vp, rho)
     g["a3d_rtm_image"] = api.ref_rtm_a3d(pb, sc, wav, gc, g["a3d_fs0_s0_r0_traces"], 5, 3, 1, 3)
+    # FWI gradient against an observed gather from a model with a slow block
+    vt = vp.copy()
+    vt[5:9, 4:8, 5:10] *= 0.92
+    pbt = api.Problem3D(nx, ny, nz, dx, dx, dx, L, 8, 0, 1e-3, nt, vt, rho)
+    obs = api.ref_modelling_a3d(pbt, sc, wav, PRESSURE, gc, PRESSURE)
+    g["a3d_fwi_obs"] = obs
+    for k, v in api.ref_fwi_a3d(pb, sc, wav, gc, obs, 5).items():
+        g[f"a3d_fwi_{k}"] = np.asarray(v)
     g["a3d_cases"] = np.array([f"a3d_fs{fs}_s{sf}_r{rf}" for fs, sf, rf in ((0, 0, 0), (1, 0, 3), (0, 1, 0))])
 
 

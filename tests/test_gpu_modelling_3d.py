@@ -156,3 +156,65 @@ def test_rtm3d_fast_fp16_checkpoints_within_tolerance(require_gpu):
     err = rel_l2(got, ref)
     print(f"3D RTM image, FMA + FP16 checkpoints + FP64 accumulation vs exact: {err:.3g}")
     assert err <= 1e-3
+
+
+# ---------------------------------------------------------------- FwiAcoustic3D::run_optimal
+def fwi3d_case(**kw):
+    c = Case3D(nx=27, ny=25, nz=23, nt=110, **kw)
+    # observed data: the oracle's gather in a model with a slow block
+    vt = c.pb.vp.copy()
+    vt[8:14, 7:13, 9:16] *= 0.92
+    from rockseis_b200.rockseis import ModelAcoustic3D
+    m = c.model
+    mt = ModelAcoustic3D(m.nx, m.ny, m.nz, m.lpml, m.dx, m.dy, m.dz, 0.0, 0.0, 0.0, m.fs)
+    mt.createModel()
+    mt.Vp[:], mt.R[:] = vt, c.pb.rho
+    pbt = api.Problem3D(m.nx, m.ny, m.nz, m.dx, m.dy, m.dz, m.lpml, c.order, m.fs, c.dt, c.nt, vt, c.pb.rho)
+    s, r = c.src, c.rec
+    c.obs = api.orc_modelling_a3d(pbt, mt.padded(), c.tab, s.smap, s.sshift, s.data.astype(np.float32), 0, r.gmap,
+                                  r.gshift, 0)
+    return c
+
+
+def oracle_fwi3d(c):
+    s, r = c.src, c.rec
+    return api.orc_fwi_a3d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, s.smap, s.sshift,
+                           s.data.astype(np.float32), r.gmap, r.gshift, c.obs)
+
+
+def gpu_fwi3d(c, ncheck=6, precision=None, ckpt=abi.CKPT_NATIVE, accum=abi.ACCUM_REFERENCE):
+    from rockseis_b200.rockseis import Data3D, FwiAcoustic3D, Image3D
+    prec = c.precision if precision is None else precision
+    c.rec.data = np.ascontiguousarray(c.obs.astype(abi.real_dtype(prec)))
+    f = FwiAcoustic3D(c.model, c.src, c.rec, c.order, 1, precision=prec)
+    f.setNcheck(ncheck)
+    f.setCheckpointPrecision(ckpt)
+    f.setAccumulation(accum)
+    f.setVpgrad(Image3D("vp", c.model, 1, 1, 1, prec))
+    f.setRhograd(Image3D("rho", c.model, 1, 1, 1, prec))
+    f.setWavgrad(Data3D(c.src.ntrace, c.nt, c.dt, 0.0, prec))
+    f.setDatamodP(Data3D(c.rec.ntrace, c.nt, c.dt, 0.0, prec))
+    f.setDataresP(Data3D(c.rec.ntrace, c.nt, c.dt, 0.0, prec))
+    assert f.run_optimal() == 1
+    return dict(vpgrad=f.vpgrad.getImagedata()[0, 0, 0], rhograd=f.rhograd.getImagedata()[0, 0, 0],
+                wavgrad=f.wavgrad.data, datamod=f.datamodP.data, datares=f.dataresP.data, misfit=f.getMisfit())
+
+
+@pytest.mark.parametrize("ncheck", [4, 110])
+def test_fwi3d_exact_bitwise(require_gpu, ncheck):
+    c = fwi3d_case()
+    ref = oracle_fwi3d(c)
+    got = gpu_fwi3d(c, ncheck=ncheck)
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        assert np.abs(ref[k]).max() > 0, k
+        assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
+    assert got["misfit"] == ref["misfit"]
+
+
+def test_fwi3d_fast_fp16_checkpoints_close_to_exact(require_gpu):
+    c = fwi3d_case()
+    ref = oracle_fwi3d(c)
+    got = gpu_fwi3d(c, ncheck=8, precision=abi.F32_FAST, ckpt=abi.CKPT_F16, accum=abi.ACCUM_F64)
+    err = {k: rel_l2(got[k], ref[k]) for k in ("vpgrad", "rhograd", "wavgrad")}
+    print(f"3D FWI gradient, FMA + FP16 checkpoints + FP64 accumulation vs exact: {err}")
+    assert max(err.values()) <= 1e-3, err

@@ -240,3 +240,16 @@ def test_oracle_3d_rtm_image_matches_reference():
     ref = GOLD["a3d_rtm_image"]
     assert np.abs(ref).max() > 0
     assert np.array_equal(img, ref), f"max abs diff {np.abs(img - ref).max()}"
+
+
+def test_oracle_3d_fwi_gradient_matches_reference():
+    case = "a3d_fs0_s0_r0"
+    pb = _a3d_problem(0)
+    g = lambda k: GOLD[f"{case}_{k}"]  # noqa: E731
+    r = api.orc_fwi_a3d(pb, list(g("models")), GOLD["a3d_tab"], g("smap"), g("sshift"), GOLD["a3d_wav"], g("gmap"),
+                        g("gshift"), GOLD["a3d_fwi_obs"])
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        ref = GOLD[f"a3d_fwi_{k}"]
+        assert np.abs(ref).max() > 0, k
+        assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
+    assert r["misfit"] == float(GOLD["a3d_fwi_misfit"])
