@@ -580,6 +580,7 @@ def run_a3d(args, device=0, f=A3D):
     prec = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
     models, srcs, recs = a3d_batch(prec, nshots=args.shots)
     cfg = make_config(models[0], f["order"], f["nt"], f["dt"], prec)
+    cfg.zchunk = int(args.zchunk)
     keep: list = []
     shots = (abi.Shot * len(models))(*[make_shot(m, s_, r, keep) for m, s_, r in zip(models, srcs, recs)])
     h = C.c_void_p()
@@ -672,6 +673,7 @@ def main():
                          "fwi: the FWI gradient line alone")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
+    ap.add_argument("--zchunk", type=int, default=0, help="acoustic3d: planes per z-march (0 = library default)")
     ap.add_argument("--shots", type=int, default=None,
                     help="acoustic3d: model only the first N windows (profiling runs)")
     args = ap.parse_args()
