@@ -692,6 +692,22 @@ def main():
                                       "d2h_bytes_per_step": 0}}))
         return
 
+    if args.impl == "reference" and args.workload == "acoustic3d":
+        if int(os.environ.get("RANK", "0")) == 0:
+            from rockseis_b200 import abi
+            models, _, _ = a3d_batch(abi.F32_EXACT)
+            r = cpu_a3d_reference(models)
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                return
+            print(json.dumps({"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "impl": "reference",
+                              "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1, "warmup": 0,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic", "config": a3d_config(), "cpu_baseline": r,
+                              "e2e": {"value": r["value"], "unit": "Gpts/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return
+
     if args.impl == "reference":
         # CPU only: rank 0 times the reference, the other ranks exit without work.
         rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
@@ -711,22 +727,6 @@ def main():
                     "cpu_baseline": r, "e2e": {"value": round(val, 5), "unit": "Gpts/s", "h2d_bytes_per_step": 0,
                                                "d2h_bytes_per_step": 0}}
             print(json.dumps(line))
-        return
-
-    if args.impl == "reference" and args.workload == "acoustic3d":
-        if int(os.environ.get("RANK", "0")) == 0:
-            from rockseis_b200 import abi
-            models, _, _ = a3d_batch(abi.F32_EXACT)
-            r = cpu_a3d_reference(models)
-            if r is None:
-                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
-                return
-            print(json.dumps({"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "impl": "reference",
-                              "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1, "warmup": 0,
-                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                              "data": "synthetic", "config": a3d_config(), "cpu_baseline": r,
-                              "e2e": {"value": r["value"], "unit": "Gpts/s", "h2d_bytes_per_step": 0,
-                                      "d2h_bytes_per_step": 0}}))
         return
 
     rank, world, local = dist_init(args)
