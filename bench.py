@@ -234,7 +234,11 @@ def run_gpu(args, rank, world, device):
     nt = args.nt
     models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt)
     torch.cuda.set_device(device)
-    plan = Plan(models, srcs, recs, ORDER, precision, args.tile)
+    from rockseis_b200.autotune import tile_shapes, tune_tile
+    # tile shape: the autotuner's pick (cached in JSON), measured before the timed region
+    tile = tune_tile(models, srcs, recs, ORDER, precision) if args.tile == -2 else args.tile
+    tile_desc = list(tile_shapes(precision).get(tile, ())) if tile >= 0 else "library default"
+    plan = Plan(models, srcs, recs, ORDER, precision, tile)
     plan.enable_timing()
     st = torch.cuda.ExternalStream(plan.stream())
     pts_per_step = sum(m.getNx_pml() * m.getNz_pml() for m in models) * nt
@@ -280,11 +284,11 @@ def run_gpu(args, rank, world, device):
     plan.close()
     if args.no_e2e:
         return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=None,
-                    clocks=clk.summary())
+                    clocks=clk.summary(), tile=tile_desc)
 
     # end to end through the C ABI from pinned host buffers
     models_p, srcs_p, recs_p = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt, pinned=True)
-    cfg = make_config(models_p[0], ORDER, nt, DT, precision, args.tile)
+    cfg = make_config(models_p[0], ORDER, nt, DT, precision, tile)
     keep: list = []
     shots = (abi.Shot * NSHOTS)(*[make_shot(m, s, r, keep) for m, s, r in zip(models_p, srcs_p, recs_p)])
     h2d = sum(sum(a.nbytes for a in m.padded()) for m in models_p) + sum(s.data.nbytes + s.smap.nbytes +
@@ -305,7 +309,8 @@ def run_gpu(args, rank, world, device):
     e2e = {"value": round(pts_per_step * world / e2e_s / 1e9, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
            "path": "rsgpu_modelling (C ABI): plan create + upload, nt steps, trace read-back, destroy"}
-    return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary())
+    return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary(),
+                tile=tile_desc)
 
 
 # ---------------------------------------------------------------- FWI gradient workload
@@ -340,13 +345,14 @@ def fwi_problem(precision, nshots, nt=None, start=True, f=FWI):
     return m, srcs, recs
 
 
-def fwi_jobs(m, srcs, obs, precision, ckpt, accum, f=FWI):
+def fwi_jobs(m, srcs, obs, precision, ckpt, accum, f=FWI, tile=-1):
     from rockseis_b200 import abi
     from rockseis_b200.rockseis import Data2D, FwiAcoustic2D, Image2D
     jobs = []
     for s_, o in zip(srcs, obs):
         j = FwiAcoustic2D(m, s_, o, f["order"], 1, precision=precision)
         j.setNcheck(f["ncheck"])
+        j.tile = tile
         j.setCheckpointPrecision(ckpt)
         j.setAccumulation(accum)
         j.setVpgrad(Image2D("vpgrad", m, 1, 1, precision))
@@ -432,7 +438,8 @@ def run_fwi(args, device=0, f=FWI):
     mt, srcs, obs = fwi_problem(prec, ns, start=False)
     modelling_batch([mt] * ns, srcs, obs, f["order"], prec)
     m, srcs, _ = fwi_problem(prec, ns)
-    jobs = fwi_jobs(m, srcs, obs, prec, ckpt, accum)
+    # tile shape: autotuned per batch shape (-2) unless --tile names one
+    jobs = fwi_jobs(m, srcs, obs, prec, ckpt, accum, tile=getattr(args, "tile", -1))
     batch = AdjointBatch(jobs)
     batch.run()                                   # warm-up (graph capture, first touch)
     with ClockSampler(device) as clk:
@@ -664,7 +671,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fast", choices=["fast", "exact"])
-    ap.add_argument("--tile", type=int, default=-1)
+    ap.add_argument("--tile", type=int, default=-2,
+                    help="2D tile shape index; -2 = autotuned (cached in JSON), -1 = library default")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
@@ -776,7 +784,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded layered elastic model with lenses, Ricker source)",
-                "config": config_dict(world, args.precision, args.nt), "gpu_launches": int(r["launches"]),
+                "config": {**config_dict(world, args.precision, args.nt), "tile": r["tile"]},
+                "gpu_launches": int(r["launches"]),
                 "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
                 "cpu_baseline": cpu}
         if fwi is not None:

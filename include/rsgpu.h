@@ -77,7 +77,7 @@ typedef struct {
     const void *pml;    /* 12*lpml C-PML tables in the order A,B,C ltf; A,B,C ltf_stag;
                            A,B,C rbb; A,B,C rbb_stag (include/pml.h:31-81).  NULL: computed
                            by rsgpu_pml_tables with Smax = 1200. */
-    int tile;           /* 2D kernel tile shape, -1 = autotuned/default */
+    int tile;           /* 2D kernel tile shape index (rsgpu_tile_shape), -1 = built-in default */
     int zchunk;         /* 3D: planes marched by one CTA (0 = 64) */
     int launch_mode;    /* 2D elastic forward: 0 = one CTA per tile (the faster on B200),
                            1 = persistent CTAs with double-buffered tile stages */
@@ -258,6 +258,15 @@ void rsgpu_adjoint_destroy(rsgpu_adjoint *adj);
  * Host preprocessing (restatements of the reference's host-side code; callers
  * that hold reference objects pass the reference's own arrays instead)
  * ------------------------------------------------------------------------- */
+
+/* 2D kernel tile shapes, the search space of the tile autotuner (no counterpart in
+ * the reference, whose loops have no tiles).  rsgpu_tile_count returns how many
+ * shapes the library holds for `precision`; rsgpu_tile_shape gives shape `idx`:
+ * the tile's x and z extent, the rows each thread updates and the CTAs per SM the
+ * kernel is compiled for.  Index i is the value of rsgpu_config.tile that selects
+ * it.  FP64 holds shapes 0 and 3 only; other indices return RSGPU_ERR_ARG there. */
+int rsgpu_tile_count(int precision);
+rsgpu_status rsgpu_tile_shape(int precision, int idx, int *tx, int *tz, int *rows_per_thread, int *ctas_per_sm);
 
 /* Pml::computeABC with Amax=0, Kmax=2, Smax=1200 (lib/pml.cpp:79-126). */
 rsgpu_status rsgpu_pml_tables(int lpml, double dt, int precision, void *out12);

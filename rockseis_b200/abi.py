@@ -86,6 +86,8 @@ def _load() -> C.CDLL:
         "rsgpu_plan_kernel_times": (I, [V, P(C.c_float), P(C.c_float)]),
         "rsgpu_plan_destroy": (None, [V]),
         "rsgpu_modelling_a2d_noalloc": (I, [P(Config), P(Shot), V]),
+        "rsgpu_tile_count": (I, [I]),
+        "rsgpu_tile_shape": (I, [I, I, P(I), P(I), P(I), P(I)]),
         "rsgpu_pml_tables": (I, [I, D, I, V]),
         "rsgpu_stagger_model": (I, [I, I, I, I, I, I, I, V, V, V, P(V)]),
         "rsgpu_make_map": (I, [I, I, I, P(D), P(I), P(D), P(D), P(D), P(I), V]),

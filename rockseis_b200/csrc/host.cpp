@@ -819,6 +819,24 @@ rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_sh
     return st;
 }
 
+int rsgpu_tile_count(int precision)
+{
+    return (precision == PREC_F64) ? TILECFG_32x16 + 1 : tile_count_2d();
+}
+
+rsgpu_status rsgpu_tile_shape(int precision, int idx, int *tx, int *tz, int *rows_per_thread, int *ctas_per_sm)
+{
+    if (!tx || !tz || !rows_per_thread || !ctas_per_sm) { set_error("null argument"); return RSGPU_ERR_ARG; }
+    const bool f64 = precision == PREC_F64;
+    if (idx < 0 || idx >= tile_count_2d() || (f64 && idx != TILECFG_64x32 && idx != TILECFG_32x16)) {
+        set_error("tile shape %d is not built for precision %d", idx, precision);
+        return RSGPU_ERR_ARG;
+    }
+    const TileShape t = tile_shape_2d(idx);
+    *tx = t.tx; *tz = t.tz; *rows_per_thread = t.rz; *ctas_per_sm = t.minb;
+    return RSGPU_OK;
+}
+
 rsgpu_status rsgpu_pml_tables(int lpml, double dt, int precision, void *out12)
 {
     if (lpml < 1 || !out12 || precision < 0 || precision > 2) { set_error("bad arguments"); return RSGPU_ERR_ARG; }

@@ -310,6 +310,16 @@ def check_stability(model: _Model, dt: float, cls: str) -> None:
                              f"stability criteria (limit {float(dt_stab)}).")
 
 
+def _tile(tile, models, sources, receivers, order, precision) -> int:
+    """The tile index to build with: `tile`, or the autotuner's pick for tile == -2 (2D only)."""
+    if int(tile) != -2:
+        return int(tile)
+    if models[0].dim == 3:
+        return -1
+    from .autotune import tune_tile
+    return tune_tile(models, sources, receivers, order, precision)
+
+
 def make_config(model: _Model, order: int, nt: int, dt: float, precision: int, tile: int = -1) -> abi.Config:
     cfg = abi.Config()
     cfg.physics = model.physics
@@ -388,7 +398,9 @@ class _Modelling:
     def run(self):
         self.checkStability()
         recs = [r for r in (self.recP, self.recVx, self.recVy, self.recVz) if r is not None]
-        cfg = make_config(self.model, self.order, self.source.nt, self.source.dt, self.precision, self.tile)
+        tile = _tile(self.tile, [self.model] * len(recs or [None]), [self.source] * len(recs or [None]), recs or [None],
+                     self.order, self.precision)
+        cfg = make_config(self.model, self.order, self.source.nt, self.source.dt, self.precision, tile)
         cfg.zchunk = int(self.zchunk)
         cfg.launch_mode = int(self.launch_mode)
         keep: list = []
@@ -415,6 +427,7 @@ class ModellingAcoustic3D(_Modelling):
 def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
     """Many shots, each with its own model window, advanced together in one plan
     (the batched form of Modelling*::run).  Traces accumulate into receivers[i].data."""
+    tile = _tile(tile, models, sources, receivers, order, precision)
     cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
     keep: list = []
     shots = (abi.Shot * len(models))(*[make_shot(m, s, r, keep) for m, s, r in zip(models, sources, receivers)])
@@ -426,6 +439,7 @@ class Plan:
     """Device-resident batch (rsgpu_plan): upload once, run steps, read traces."""
 
     def __init__(self, models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
+        tile = _tile(tile, models, sources, receivers, order, precision)
         self.cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
         self._keep: list = []
         self.n = len(models)
@@ -704,10 +718,17 @@ def _lags(j0):
     return 1, 1, 1
 
 
+def _adjoint_tile(jobs) -> int:
+    # the adjoint reuses the forward kernels: tune on the forward modelling of the batch
+    j0 = jobs[0]
+    return _tile(j0.tile, [j.model for j in jobs], [j.source for j in jobs], [j.dataP for j in jobs], j0.order,
+                 j0.precision)
+
+
 def _adjoint_batch(jobs, fn):
     j0 = jobs[0]
     j0.checkStability()
-    cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
+    cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
     opts = j0._opts(*_lags(j0))
     keep: list = []
     shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
@@ -735,7 +756,7 @@ class AdjointBatch:
     def __init__(self, jobs, kind=abi.KIND_FWI):
         j0 = jobs[0]
         self.jobs = jobs
-        self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, j0.tile)
+        self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
         self.opts = j0._opts(*_lags(j0))
         self._keep: list = []
         self.shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(self._keep) for j in jobs])
