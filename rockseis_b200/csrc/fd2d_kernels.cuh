@@ -27,6 +27,7 @@
 #pragma once
 #include <cuda.h>
 #include <cstdint>
+#include <type_traits>
 #include "rsgpu.h"
 #include "rsgpu_internal.h"
 #include "rsgpu_kernels.h"
@@ -386,21 +387,64 @@ __device__ __forceinline__ void row_dx(const T *tile, int row, int xq, const Coe
     }
 }
 
+// FAST-mode z-derivatives of the thread's 4 columns x RZ rows, streamed: each
+// of the RZ+16 window rows is read once as a 128-bit shared load and scattered
+// into the RZ accumulators with paired FMAs (c*w+ and -c*w- as separate terms),
+// so neither the window nor a difference is held in registers.  Same taps and
+// coefficients as dz_pair; only the summation order differs.
+template <int W, int RZ, bool FW>
+__device__ __forceinline__ void dz_stream_f32(const float *s, int zr, int col, const float (&cu)[NCOEF],
+                                              float (&out)[RZ][4])
+{
+    float2 lo[RZ], hi[RZ];
+#pragma unroll
+    for (int rr = 0; rr < RZ; rr++) { lo[rr] = make_float2(0.f, 0.f); hi[rr] = lo[rr]; }
+#pragma unroll
+    for (int q = 0; q < RZ + 16; q++) {
+        const float4 w = *reinterpret_cast<const float4 *>(s + (zr + q) * W + col);
+        const float2 wl = make_float2(w.x, w.y), wh = make_float2(w.z, w.w);
+#pragma unroll
+        for (int rr = 0; rr < RZ; rr++) {
+            // forward: d = sum_k c_k (w[rr+9+k] - w[rr+8-k]); backward: (w[rr+8+k] - w[rr+7-k])
+            const int kp = FW ? q - rr - 9 : q - rr - 8;
+            const int km = FW ? rr + 8 - q : rr + 7 - q;
+            if (kp >= 0 && kp < NCOEF) {
+                const float2 c = make_float2(cu[kp], cu[kp]);
+                lo[rr] = __ffma2_rn(wl, c, lo[rr]);
+                hi[rr] = __ffma2_rn(wh, c, hi[rr]);
+            }
+            if (km >= 0 && km < NCOEF) {
+                const float2 c = make_float2(-cu[km], -cu[km]);
+                lo[rr] = __ffma2_rn(wl, c, lo[rr]);
+                hi[rr] = __ffma2_rn(wh, c, hi[rr]);
+            }
+        }
+    }
+#pragma unroll
+    for (int rr = 0; rr < RZ; rr++) {
+        out[rr][0] = lo[rr].x; out[rr][1] = lo[rr].y; out[rr][2] = hi[rr].x; out[rr][3] = hi[rr].y;
+    }
+}
+
 template <typename T, int MODE, int TX, int TZ, int RZ, bool FW>
 __device__ __forceinline__ void block_dz(const T *tile, int zr, int xq, const CoefSet<T> &cs, const T (&cu)[NCOEF],
                                          bool zedge, int gz, int nzp, int order, T d, T r, T (&out)[RZ][4])
 {
     using G = Geo2D<T, TX, TZ, RZ>;
     using P = typename Pair<T>::t;
-    const T *ce[RZ];
+    if constexpr (MODE == MODE_FAST && std::is_same<T, float>::value) {
+        dz_stream_f32<G::W, RZ, FW>(tile, zr, xq + GUARD, cu, out);
+    } else {
+        const T *ce[RZ];
 #pragma unroll
-    for (int q = 0; q < RZ; q++) ce[q] = nullptr;
+        for (int q = 0; q < RZ; q++) ce[q] = nullptr;
 #pragma unroll
-    for (int cp = 0; cp < 2; cp++) {
-        P o[RZ];
-        dz_pair<T, MODE, FW, false, G::W, RZ>(tile, zr, xq + GUARD + 2 * cp, cu, ce, d, r, o);
+        for (int cp = 0; cp < 2; cp++) {
+            P o[RZ];
+            dz_pair<T, MODE, FW, false, G::W, RZ>(tile, zr, xq + GUARD + 2 * cp, cu, ce, d, r, o);
 #pragma unroll
-        for (int q = 0; q < RZ; q++) { out[q][2 * cp] = o[q].x; out[q][2 * cp + 1] = o[q].y; }
+            for (int q = 0; q < RZ; q++) { out[q][2 * cp] = o[q].x; out[q][2 * cp + 1] = o[q].y; }
+        }
     }
     if (zedge) {
 #pragma unroll
