@@ -172,3 +172,15 @@ def test_fwi_16bit_checkpoints_against_fp64_propagator(require_gpu, fp64_and_exa
     err = _rel(outputs(f), ref64)
     print(f"checkpoint format {ckpt}: relative L2 against the FP64 propagator {err}")
     assert max(err.values()) <= tol, err
+
+
+def test_sharded_stack_on_one_rank_equals_sum_of_shots(require_gpu):
+    from rockseis_b200.distributed import fwi_gradient_sharded
+    cases = [fwi_case(scoord=(sx, 23.7), seed=1) for sx in (150.9, 400.3, 610.2)]
+    refs = [oracle_fwi(c) for c in cases]
+    jobs = [make_fwi(c, ncheck=6) for c in cases]
+    vp, rho, mis = fwi_gradient_sharded(jobs, 0, 1)
+    assert vp.shape == jobs[0].vpgrad.getImagedata().shape      # (nhx, nhz, nz, nx) like the images
+    assert np.array_equal(vp[0, 0], sum(r["vpgrad"].astype(np.float64) for r in refs))
+    assert np.array_equal(rho[0, 0], sum(r["rhograd"].astype(np.float64) for r in refs))
+    assert mis == sum(float(r["misfit"]) for r in refs)
