@@ -259,6 +259,13 @@ void rsgpu_adjoint_destroy(rsgpu_adjoint *adj);
  * that hold reference objects pass the reference's own arrays instead)
  * ------------------------------------------------------------------------- */
 
+/* Failure-detection self test (no counterpart in the reference): launches one CTA
+ * that waits on a barrier nothing completes.  The kernel's bounded wait (the same
+ * one every TMA stage uses) gives up after 2 s, records the time-out in a device
+ * error word and returns, so the call returns RSGPU_ERR_TIMEOUT and the device stays
+ * usable for further calls.  Any other status means the failure path is broken. */
+rsgpu_status rsgpu_selftest_bounded_wait(void);
+
 /* 2D kernel tile shapes, the search space of the tile autotuner (no counterpart in
  * the reference, whose loops have no tiles).  rsgpu_tile_count returns how many
  * shapes the library holds for `precision`; rsgpu_tile_shape gives shape `idx`:

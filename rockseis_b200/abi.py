@@ -86,6 +86,7 @@ def _load() -> C.CDLL:
         "rsgpu_plan_kernel_times": (I, [V, P(C.c_float), P(C.c_float)]),
         "rsgpu_plan_destroy": (None, [V]),
         "rsgpu_modelling_a2d_noalloc": (I, [P(Config), P(Shot), V]),
+        "rsgpu_selftest_bounded_wait": (I, []),
         "rsgpu_tile_count": (I, [I]),
         "rsgpu_tile_shape": (I, [I, I, P(I), P(I), P(I), P(I)]),
         "rsgpu_pml_tables": (I, [I, D, I, V]),

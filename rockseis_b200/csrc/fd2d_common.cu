@@ -42,6 +42,24 @@ cudaError_t launch_set_counter(int *it_dev, int value, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Failure-detection self test: one CTA waits on a shared-memory barrier that
+// expects one arrival that never comes.  The bounded wait gives up after its
+// wall-clock limit, records RSGPU_ERR_TIMEOUT in the error word and the kernel
+// returns normally, leaving the context usable.
+static __global__ void wait_for_nothing(int *err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    mbar_wait_bounded(&bar, 0, err);
+}
+
+cudaError_t launch_wait_for_nothing(int *err, cudaStream_t st)
+{
+    wait_for_nothing<<<1, 32, 0, st>>>(err);
+    return cudaGetLastError();
+}
+
 size_t coefset_bytes(int prec) { return prec == PREC_F64 ? sizeof(CoefSet<double>) : sizeof(CoefSet<float>); }
 int coef_row_stride() { return CROW; }
 

@@ -819,6 +819,31 @@ rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_sh
     return st;
 }
 
+rsgpu_status rsgpu_selftest_bounded_wait(void)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        set_error("no CUDA device");
+        return RSGPU_ERR_NODEVICE;
+    }
+    int *d_err = nullptr, h_err = 0;
+    cudaStream_t st = nullptr;
+    CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaError_t e = cudaMallocAsync((void **)&d_err, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = launch_wait_for_nothing(d_err, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (d_err) cudaFreeAsync(d_err, st);
+    const cudaError_t es = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e == cudaSuccess) e = es;
+    if (e != cudaSuccess) { set_error("self test: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    if (h_err == RSGPU_ERR_TIMEOUT) { set_error("a device-side wait exceeded its time limit (self test)"); return RSGPU_ERR_TIMEOUT; }
+    set_error("self test: the bounded wait did not report its time-out (code %d)", h_err);
+    return RSGPU_ERR_STATE;
+}
+
 int rsgpu_tile_count(int precision)
 {
     return (precision == PREC_F64) ? TILECFG_32x16 + 1 : tile_count_2d();

@@ -33,6 +33,7 @@ cudaError_t launch_injrec_2d(int prec, const void *shots, const void *plans, int
                              const int *it_dev, cudaStream_t st);
 cudaError_t launch_advance(int *it_dev, int by, cudaStream_t st);
 cudaError_t launch_set_counter(int *it_dev, int value, cudaStream_t st);
+cudaError_t launch_wait_for_nothing(int *err, cudaStream_t st);
 size_t coefset_bytes(int prec);
 int coef_row_stride();
 

@@ -60,3 +60,7 @@ def test_compute_without_device_fails_loudly():
         mod.run()
     assert e.value.status == abi.ERR_NODEVICE
     assert not c.rec.data.any()
+
+
+def test_failure_self_test_without_device_fails_loudly():
+    assert abi.lib.rsgpu_selftest_bounded_wait() == abi.ERR_NODEVICE
