@@ -62,8 +62,8 @@ def oracle() -> C.CDLL:
         _oracle.orc_mod_a2d.argtypes = [C.POINTER(OrcGrid)] + [V] * 4 + [I, V, V, V, I, I, V, V, I, V, I, V]
         _oracle.orc_mod_e2d.argtypes = [C.POINTER(OrcGrid)] + [V] * 6 + [I, V, V, V, I, I, V, V, I, V, V, I, V]
         _oracle.orc_e2d_adjoint_steps.argtypes = [C.POINTER(OrcGrid)] + [V] * 6 + [I, V]
-        _oracle.orc_fwi_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 6 + [I, V, V, V, I, V, V, V, V, V, V,
-                                                                                  V, V, V]
+        _oracle.orc_fwi_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 6 + [I, V, V, V, I, V, V, V, I, V, V,
+                                                                                  V, V, V, V]
         _oracle.orc_rtm_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 4 + [I, V, V, V, I, V, V, V, I, I, V]
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
         _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V] + \
@@ -164,7 +164,7 @@ def _keep(*arrs, dtype=None):
     return [None if a is None else np.ascontiguousarray(a, dtype if dtype is not None else a.dtype) for a in arrs]
 
 
-def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32):
+def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit=0):
     t = "f" if dtype == np.float32 else "d"
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
@@ -177,7 +177,7 @@ def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32):
     mis = C.c_double()
     vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=dtype)
     r = getattr(ref(), f"ref_fwi_a2d_{t}")(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
-                                           ncheck, 0, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
+                                           ncheck, misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 1
     return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
 
@@ -232,7 +232,7 @@ def orc_modelling_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, 
     return (out, st) if want_state else out
 
 
-def orc_fwi_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
+def orc_fwi_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs, misfit=0):
     g = pb.orc_grid()
     ns, nr = len(smap), len(gmap)
     vpg = np.zeros((pb.nz, pb.nx), np.float32)
@@ -245,7 +245,8 @@ def orc_fwi_a2d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
                                                   dtype=np.float32)
     sm, gm = _keep(smap, gmap, dtype=np.int32)
     r = oracle().orc_fwi_a2d(C.byref(g), pb.nx, pb.nz, _p(vp), _p(rho), _p(Rx), _p(Rz), _p(L), _p(tb), ns, _p(sm),
-                             _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr),
+                             _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), misfit, _p(vpg), _p(rhog), _p(wg), _p(dm),
+                             _p(dr),
                              C.byref(mis))
     assert r == 0
     return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)

@@ -425,15 +425,21 @@ static void a2d_corr(const orc_grid *g, int nx, int nz, const float *Vp, const f
         }
 }
 
-/* FwiAcoustic2D::run_optimal with the DIFFERENCE misfit and pressure data, one shot.
+static int cmp_float(const void *a, const void *b)
+{
+    const float x = *(const float *)a, y = *(const float *)b;
+    return (x > y) - (x < y);
+}
+
+/* FwiAcoustic2D::run_optimal with the DIFFERENCE (misfit_type 0) or CORRELATION (1) misfit and pressure data, one shot.
  * The forward states are kept for every step instead of being recomputed from
  * checkpoints; recomputation is deterministic, so the gradient is the same.
  * The pairing of forward and adjoint time levels follows fw_state_at().
  * vp, rho: unpadded models [nz][nx]; outputs accumulate (+=) like the reference. */
 int orc_fwi_a2d(const orc_grid *g, int nx, int nz, const float *vp, const float *rho, const float *Rx,
                 const float *Rz, const float *Lm, const float *tab, int ns, const int *smap, const float *sshift,
-                const float *wav, int nr, const int *gmap, const float *gshift, const float *obs, float *vpgrad,
-                float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
+                const float *wav, int nr, const int *gmap, const float *gshift, const float *obs, int misfit_type,
+                float *vpgrad, float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
 {
     const int nt = g->nt;
     const long n = (long)g->nxp * g->nzp;
@@ -448,15 +454,51 @@ int orc_fwi_a2d(const orc_grid *g, int nx, int nz, const float *vp, const float 
         record(&fw, 0, nr, gmap, gshift, NULL, datamod, it);
         memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
     }
-    /* computeMisfit / computeResiduals, DIFFERENCE (lib/fwi.cpp:597-611, 798-806) */
     float mis = 0.0f;
-    for (int tr = 0; tr < nr; tr++) {
-        if (gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0)
+    if (misfit_type == 0) {
+        /* computeMisfit / computeResiduals, DIFFERENCE (lib/fwi.cpp:597-611, 798-806) */
+        for (int tr = 0; tr < nr; tr++) {
+            if (gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0)
+                for (int it = 0; it < nt; it++) {
+                    float r = datamod[it + (long)tr * nt] - obs[it + (long)tr * nt];
+                    mis += 0.5 * r * r;
+                }
+            for (int it = 0; it < nt; it++) datares[it + (long)tr * nt] = 1 * (datamod[it + (long)tr * nt] - obs[it + (long)tr * nt]);
+        }
+    } else {
+        /* CORRELATION (lib/fwi.cpp:617-645, 808-849): per-trace norms in float, the
+         * misfit over traces on the grid, residuals of every trace, then residuals
+         * at or above the 97th-percentile magnitude of the shot set to zero */
+        for (int tr = 0; tr < nr; tr++) {
+            const float *m = datamod + (long)tr * nt, *o = obs + (long)tr * nt;
+            float n1 = 0.0f, n2 = 0.0f, n3 = 0.0f;
             for (int it = 0; it < nt; it++) {
-                float r = datamod[it + (long)tr * nt] - obs[it + (long)tr * nt];
-                mis += 0.5 * r * r;
+                n1 += m[it] * m[it];
+                n2 += o[it] * o[it];
+                n3 += m[it] * o[it];
             }
-        for (int it = 0; it < nt; it++) datares[it + (long)tr * nt] = 1 * (datamod[it + (long)tr * nt] - obs[it + (long)tr * nt]);
+            n1 = sqrtf(n1);
+            n2 = sqrtf(n2);
+            if (n1 == 0) n1 = 1.0f;
+            if (n2 == 0) n2 = 1.0f;
+            if (gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0)
+                for (int it = 0; it < nt; it++) {
+                    float v = (float)((-1.0) * (m[it] * o[it] / (n1 * n2)));
+                    mis += v;
+                }
+            n3 /= (n1 * n2);
+            float *r = datares + (long)tr * nt;
+            for (int it = 0; it < nt; it++) r[it] = (float)((-1.0) * 1 * ((o[it] / (n1 * n2)) - (m[it] / (n1 * n1)) * n3));
+        }
+        const long tot = (long)nt * nr;
+        float *fres = malloc(tot * sizeof(float));
+        if (!fres) return -1;
+        for (long k = 0; k < tot; k++) fres[k] = fabsf(datares[k]);
+        qsort(fres, tot, sizeof(float), cmp_float);
+        const float pclip = fres[(long)((97ul * (unsigned long)nt * (unsigned long)nr) / 100ul)];
+        for (long k = 0; k < tot; k++)
+            if (fabsf(datares[k]) >= pclip) datares[k] = 0.0f;
+        free(fres);
     }
     *misfit = mis;
     float *zero = calloc(n, sizeof(float));

@@ -63,6 +63,7 @@ public:
     int kind = RSGPU_KIND_FWI, phys = PHYS_A2D, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE;
     int nhx = 1, nhz = 1;
     int ncheck = 0, nslots = 0, nxmax = 0, nzmax = 0;
+    int misfit_type = RSGPU_MISFIT_DIFFERENCE, nrec_max = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan> fw, bw;
     cudaStream_t stream = nullptr;
@@ -106,7 +107,18 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_UNSUPPORTED;
     }
     const bool el = c->physics == RSGPU_ELASTIC2D;
-    if (o->misfit != RSGPU_MISFIT_DIFFERENCE) { set_error("only the DIFFERENCE misfit is built"); return RSGPU_ERR_UNSUPPORTED; }
+    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && !(o->misfit == RSGPU_MISFIT_CORRELATION && !el)) {
+        set_error("misfit %d: DIFFERENCE is built for every driver, CORRELATION for acoustic 2D FWI", o->misfit);
+        return RSGPU_ERR_UNSUPPORTED;
+    }
+    if (o->misfit == RSGPU_MISFIT_CORRELATION && kind == RSGPU_KIND_FWI) {
+        const int lim = 49152 / (c->precision == RSGPU_F64 ? 8 : 4);
+        for (int i = 0; i < ns; i++)
+            if (s[i].shot.nrec > lim) {
+                set_error("shot %d: the CORRELATION misfit takes at most %d receivers per shot", i, lim);
+                return RSGPU_ERR_UNSUPPORTED;
+            }
+    }
     if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
         set_error("bad checkpoint precision %d", o->ckpt_precision);
         return RSGPU_ERR_ARG;
@@ -151,6 +163,8 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     prec = c->precision;
     es = esize(prec);
     acc = o->accum == RSGPU_ACCUM_F64 ? ACC_F64 : ACC_REF;
+    misfit_type = o->misfit;
+    for (int i = 0; i < ns; i++) nrec_max = std::max(nrec_max, s[i].shot.nrec);
     ck = o->ckpt_precision;
     ck_es = ck == CK_NATIVE ? (size_t)es : 2;
     nhx = kind == RSGPU_KIND_RTM ? o->nhx : 1;
@@ -458,7 +472,9 @@ rsgpu_status Adjoint::run()
             ST(fw->set_recording(false));
             if (kind == RSGPU_KIND_FWI) {
                 cudaError_t e = elastic() ? launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
-                                          : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                                : misfit_type == RSGPU_MISFIT_CORRELATION
+                                    ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream)
+                                    : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
                 launches += 1;
             }

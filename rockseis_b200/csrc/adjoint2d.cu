@@ -13,6 +13,8 @@
 // arithmetic conversions evaluate `0.5 * a * b * (c - d) / dx` in double when
 // a..d are float, and `-2.0 / vp` in double rounded to float; every such operation
 // is written out with explicitly rounded intrinsics.
+#include <algorithm>
+#include <cstring>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -203,6 +205,106 @@ __global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, d
         }
         if (threadIdx.x == 0) misfit[blockIdx.x] = red[0];
     }
+}
+
+// ---------------------------------------------------------------- CORRELATION misfit
+// FwiAcoustic2D::computeMisfit / computeResiduals, CORRELATION (lib/fwi.cpp:617-645,
+// 808-849), pressure data.  Per trace, in the element type and the reference's
+// order: n1 = sqrt(sum m*m), n2 = sqrt(sum o*o) (zero -> 1), n3 = sum m*o / (n1*n2);
+// residual -(o/(n1*n2) - (m/(n1*n1))*n3) for every trace; misfit += -(m*o/(n1*n2))
+// over the traces on the grid.  Then the residuals whose magnitude reaches the
+// 97th-percentile value of all |residual| samples of the shot (the element at
+// index (97*nt*nrec)/100 of the ascending sort) are zeroed.  The order statistic
+// comes from a radix select on the magnitude bit patterns, which order like the
+// non-negative values.  One CTA per shot; dynamic shared memory holds n1*n2 of
+// every trace.
+template <typename T> struct Bits;
+template <> struct Bits<float> { using U = unsigned int; static constexpr int NB = 32; };
+template <> struct Bits<double> { using U = unsigned long long; static constexpr int NB = 64; };
+
+template <typename T> __device__ __forceinline__ T sqrt_rn(T x);
+template <> __device__ __forceinline__ float sqrt_rn<float>(float x) { return __fsqrt_rn(x); }
+template <> __device__ __forceinline__ double sqrt_rn<double>(double x) { return __dsqrt_rn(x); }
+
+template <typename T>
+__device__ __forceinline__ typename Bits<T>::U mag_bits(T x)
+{
+    using U = typename Bits<T>::U;
+    U u;
+    memcpy(&u, &x, sizeof u);
+    return u & ~((U)1 << (Bits<T>::NB - 1));
+}
+
+template <typename T, int ACC>
+__global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, double *misfit)
+{
+    using U = typename Bits<T>::U;
+    extern __shared__ __align__(16) unsigned char corr_smem[];
+    T *nn = reinterpret_cast<T *>(corr_smem);            // n1*n2 per trace
+    const Resid2D<T> d = desc[blockIdx.x];
+    const long n = (long)d.nrec * d.nt;
+    for (int tr = threadIdx.x; tr < d.nrec; tr += blockDim.x) {
+        const T *m = d.mod + (long)tr * d.nt, *o = d.obs + (long)tr * d.nt;
+        T n1 = 0, n2 = 0, n3 = 0;
+        for (int it = 0; it < d.nt; it++) {
+            n1 = X<T>::add(n1, X<T>::mul(m[it], m[it]));
+            n2 = X<T>::add(n2, X<T>::mul(o[it], o[it]));
+            n3 = X<T>::add(n3, X<T>::mul(m[it], o[it]));
+        }
+        n1 = sqrt_rn(n1);
+        n2 = sqrt_rn(n2);
+        if (n1 == T(0)) n1 = T(1);
+        if (n2 == T(0)) n2 = T(1);
+        const T n12 = X<T>::mul(n1, n2), n11 = X<T>::mul(n1, n1);
+        n3 = X<T>::div(n3, n12);
+        nn[tr] = n12;
+        T *r = d.res + (long)tr * d.nt;
+        for (int it = 0; it < d.nt; it++)
+            r[it] = -X<T>::sub(X<T>::div(o[it], n12), X<T>::mul(X<T>::div(m[it], n11), n3));
+    }
+    __syncthreads();
+    // radix select of the k-th smallest magnitude, most significant digit first
+    __shared__ unsigned int hist[256];
+    __shared__ U prefix_s;
+    __shared__ long rank_s;
+    if (threadIdx.x == 0) { prefix_s = 0; rank_s = (long)((97ull * (unsigned long long)d.nt * (unsigned long long)d.nrec) / 100ull); }
+    U mask = 0;
+    for (int shift = Bits<T>::NB - 8; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        const U prefix = prefix_s;
+        for (long k = threadIdx.x; k < n; k += blockDim.x) {
+            const U u = mag_bits(d.res[k]);
+            if ((u & mask) == prefix) atomicAdd(&hist[(unsigned)(u >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long r = rank_s;
+            int b = 0;
+            while (b < 255 && r >= (long)hist[b]) { r -= hist[b]; b++; }
+            rank_s = r;
+            prefix_s = prefix | ((U)b << shift);
+        }
+        mask |= (U)255 << shift;
+        __syncthreads();
+    }
+    const U clip = prefix_s;
+    for (long k = threadIdx.x; k < n; k += blockDim.x)
+        if (mag_bits(d.res[k]) >= clip) d.res[k] = T(0);
+    if (threadIdx.x != 0) return;
+    // misfit, traces then samples, on the traces inside the grid
+    T mis = 0;
+    double mis64 = 0.0;
+    for (int tr = 0; tr < d.nrec; tr++) {
+        if (d.rec_pt[tr] < 0) continue;
+        const T *m = d.mod + (long)tr * d.nt, *o = d.obs + (long)tr * d.nt;
+        for (int it = 0; it < d.nt; it++) {
+            const T v = -X<T>::div(X<T>::mul(m[it], o[it]), nn[tr]);
+            if (ACC == ACC_REF) mis = X<T>::add(mis, v);
+            else mis64 += (double)v;
+        }
+    }
+    misfit[blockIdx.x] = ACC == ACC_REF ? (double)mis : mis64;
 }
 
 // ---------------------------------------------------------------- elastic FWI
@@ -599,6 +701,20 @@ cudaError_t launch_corr_fwi_a3d(int prec, int acc, const void *desc, int nshots,
     } else {
         if (acc == ACC_F64) corr_fwi_a3d<float, false, double><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
         else corr_fwi_a3d<float, false, float><<<grid, block, 0, st>>>((const Corr3DF<float> *)desc, (float)dx, (float)dy, (float)dz);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
+                                 cudaStream_t st)
+{
+    const size_t sm = (size_t)std::max(nrec_max, 1) * (prec == PREC_F64 ? 8 : 4);
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) residual_corr<double, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
+        else residual_corr<double, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
+    } else {
+        if (acc == ACC_F64) residual_corr<float, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
+        else residual_corr<float, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
     }
     return cudaGetLastError();
 }

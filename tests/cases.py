@@ -83,9 +83,9 @@ def fwi_case(nx=81, nz=61, nt=300, seed=1, precision=abi.F32_EXACT, scoord=(400.
     return c
 
 
-def oracle_fwi(c):
+def oracle_fwi(c, misfit=0):
     return api.orc_fwi_a2d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, c.src.smap, c.src.sshift,
-                           c.src.data, c.rec.gmap, c.rec.gshift, c.obs)
+                           c.src.data, c.rec.gmap, c.rec.gshift, c.obs, misfit)
 
 
 def oracle_rtm(c, data, nhx=1, nhz=1):

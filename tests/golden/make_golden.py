@@ -183,6 +183,9 @@ def adjoint_cases(g):
     prep(g, "fwi", 0, vp, None, rho, sc, gc, PRESSURE, PRESSURE)
     for k, v in fwi.items():
         g[f"fwi_out_{k}"] = np.asarray(v)
+    # the CORRELATION misfit (misfit type 1) on the same shot
+    for k, v in api.ref_fwi_a2d(pb, sc, wav, gc, obs, 5, misfit=1).items():
+        g[f"fwi_corr_out_{k}"] = np.asarray(v)
     img = api.ref_rtm_a2d(pb, sc, wav, gc, obs, 5, nhx=3, nhz=1)
     g["rtm_image_h3"] = img
 

@@ -184,3 +184,42 @@ def test_sharded_stack_on_one_rank_equals_sum_of_shots(require_gpu):
     assert np.array_equal(vp[0, 0], sum(r["vpgrad"].astype(np.float64) for r in refs))
     assert np.array_equal(rho[0, 0], sum(r["rhograd"].astype(np.float64) for r in refs))
     assert mis == sum(float(r["misfit"]) for r in refs)
+
+
+@pytest.mark.parametrize("ncheck", [4, 11])
+def test_fwi_correlation_misfit_exact_bitwise(require_gpu, ncheck):
+    # CORRELATION misfit: per-trace normalised correlation, its residuals and the
+    # 97th-percentile residual clip (radix select on the GPU, a sort in the oracle)
+    c = fwi_case()
+    ref = oracle_fwi(c, misfit=abi.MISFIT_CORRELATION)
+    assert (ref["datares"] == 0).mean() >= 0.03
+    f = make_fwi(c, ncheck=ncheck)
+    f.setMisfit_type(abi.MISFIT_CORRELATION)
+    assert f.run_optimal() == 1
+    assert_same(outputs(f), ref)
+
+
+def test_fwi_correlation_batched_windows_bitwise(require_gpu):
+    cases = [fwi_case(nx=81, nz=61, seed=1, scoord=(400.3, 23.7), fs=1),
+             fwi_case(nx=97, nz=53, seed=2, scoord=(150.9, 31.2), nrec=41, rx0=-17.0),
+             fwi_case(nx=64, nz=70, seed=3, scoord=(322.0, 12.5))]
+    refs = [oracle_fwi(c, misfit=abi.MISFIT_CORRELATION) for c in cases]
+    jobs = [make_fwi(c, ncheck=6) for c in cases]
+    for j in jobs:
+        j.setMisfit_type(abi.MISFIT_CORRELATION)
+    assert fwi_gradient_batch(jobs) == 1
+    for f, ref in zip(jobs, refs):
+        assert_same(outputs(f), ref)
+
+
+def test_fwi_correlation_fp64_accumulation_close(require_gpu):
+    c = fwi_case()
+    ref = oracle_fwi(c, misfit=abi.MISFIT_CORRELATION)
+    f = make_fwi(c, ncheck=8, accum=abi.ACCUM_F64)
+    f.setMisfit_type(abi.MISFIT_CORRELATION)
+    f.run_optimal()
+    got = outputs(f)
+    assert np.array_equal(got["datares"], ref["datares"])            # residuals do not depend on the accumulator
+    assert abs(got["misfit"] - ref["misfit"]) <= 1e-5 * abs(ref["misfit"])
+    for k in GRAD:
+        assert rel_l2(got[k], ref[k]) <= 1e-5, k

@@ -70,6 +70,20 @@ def test_oracle_fwi_gradient_matches_reference():
     assert r["misfit"] == float(g("out_misfit"))
 
 
+def test_oracle_correlation_misfit_gradient_matches_reference():
+    g = lambda k: GOLD[f"fwi_{k}"]  # noqa: E731
+    pb = problem(0, g("vp"), g("rho"))
+    r = api.orc_fwi_a2d(pb, list(g("models")), g("tab"), g("smap"), g("sshift"), g("wav"), g("gmap"), g("gshift"),
+                        g("obs"), misfit=1)
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        ref = g(f"corr_out_{k}")
+        assert np.abs(ref).max() > 0, k
+        assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
+    assert r["misfit"] == float(g("corr_out_misfit")) and r["misfit"] < 0
+    # the 97th-percentile clip zeroed at least 3 % of the residual samples
+    assert (r["datares"] == 0).mean() >= 0.03
+
+
 def test_oracle_rtm_image_matches_reference():
     g = lambda k: GOLD[f"fwi_{k}"]  # noqa: E731
     pb = problem(0, g("vp"), g("rho"))
