@@ -68,7 +68,7 @@ def oracle() -> C.CDLL:
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
         _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V] + \
             [V] * 4 + [V, V, V]
-        _oracle.orc_fwi_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 7 + [I, V, V, V, I, V, V, V] + \
+        _oracle.orc_fwi_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 7 + [I, V, V, V, I, V, V, V, I] + \
             [V] * 5 + [V]
         _oracle.orc_rtm_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 5 + [I, V, V, V, I, V, V, V, I, I, I, V]
         _oracle.orc_mod_a3d.argtypes = [C.POINTER(OrcGrid3)] + [V] * 5 + [I, V, V, V, I, I, V, V, I, V, I, V]
@@ -97,6 +97,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
+        _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
         _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
         _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
@@ -391,7 +392,7 @@ def orc_rtm_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, data, nhx=1, n
     return img
 
 
-def ref_fwi_a3d(pb, scoords, wav, gcoords, obs, ncheck):
+def ref_fwi_a3d(pb, scoords, wav, gcoords, obs, ncheck, misfit=0):
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     ns, nr = len(sc), len(gc)
@@ -401,14 +402,15 @@ def ref_fwi_a3d(pb, scoords, wav, gcoords, obs, ncheck):
     dr = np.zeros((nr, pb.nt), np.float32)
     mis = C.c_double()
     vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=np.float32)
-    r = ref().ref_fwi_a3d_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
-                            _p(o["vpgrad"]), _p(o["rhograd"]), _p(wg), _p(dm), _p(dr), C.byref(mis))
+    fn = ref().ref_fwi_a3d_corr_f if misfit == 1 else ref().ref_fwi_a3d_f
+    r = fn(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
+           _p(o["vpgrad"]), _p(o["rhograd"]), _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 1
     o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
     return o
 
 
-def orc_fwi_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
+def orc_fwi_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs, misfit=0):
     g = pb.orc_grid()
     ns, nr = len(smap), len(gmap)
     o = {k: np.zeros((pb.nz, pb.ny, pb.nx), np.float32) for k in ("vpgrad", "rhograd")}
@@ -420,7 +422,8 @@ def orc_fwi_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs):
                                                       dtype=np.float32)
     sm, gm = _keep(smap, gmap, dtype=np.int32)
     r = oracle().orc_fwi_a3d(C.byref(g), pb.nx, pb.ny, pb.nz, _p(vp), _p(rho), _p(Rx), _p(Ry), _p(Rz), _p(L), _p(tb),
-                             ns, _p(sm), _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), _p(o["vpgrad"]), _p(o["rhograd"]),
+                             ns, _p(sm), _p(ss), _p(w), nr, _p(gm), _p(gs), _p(ob), misfit, _p(o["vpgrad"]),
+                             _p(o["rhograd"]),
                              _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 0
     o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)

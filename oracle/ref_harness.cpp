@@ -191,11 +191,11 @@ int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
     return r;
 }
 
-/* FwiAcoustic3D::run_optimal (lib/fwi.cpp:1991-2160), DIFFERENCE misfit. */
+/* FwiAcoustic3D::run_optimal (lib/fwi.cpp:1991-2160), DIFFERENCE (0) or CORRELATION (1) misfit. */
 template <typename T>
 int fwi_a3d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav, int nr,
             const double *gc, const T *obs, int ncheck, T *vpgrad, T *rhograd, T *wavgrad, T *datamod, T *datares,
-            double *misfit)
+            double *misfit, int misfit_type = 0)
 {
     auto model = make_a3d<T>(g, vp, rho);
     auto geom = model->getGeom();
@@ -214,7 +214,7 @@ int fwi_a3d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     fwi.setVpgrad(ivp);
     fwi.setRhograd(irho);
     fwi.setWavgrad(wg);
-    fwi.setMisfit_type(DIFFERENCE);
+    fwi.setMisfit_type((rs_fwimisfit)misfit_type);
     fwi.setNcheck(ncheck);
     fwi.setIncore(true);
     fwi.setSnapfile(tmpname("fwia3d"));
@@ -449,6 +449,13 @@ int ref_fwi_a3d_f(const ref_grid *g, const float *vp, const float *rho, int ns, 
 {
     return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
                           misfit);
+}
+int ref_fwi_a3d_corr_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                       const float *wav, int nr, const double *gc, const float *obs, int ncheck, float *vpgrad,
+                       float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
+{
+    return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
+                          misfit, 1);
 }
 int ref_fwi_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                   const float *wav, int sfield, int nr, const double *gc, const float *obsp, const float *obsx,

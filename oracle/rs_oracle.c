@@ -431,6 +431,50 @@ static int cmp_float(const void *a, const void *b)
     return (x > y) - (x < y);
 }
 
+/* CORRELATION misfit and residuals of one shot's pressure traces, shared by the 2D
+ * and 3D drivers (FwiAcoustic2D: lib/fwi.cpp:617-645, 808-849; FwiAcoustic3D:
+ * lib/fwi.cpp:1511-1540, 1696-1722).  Per trace in float: n1 = sqrt(sum m*m),
+ * n2 = sqrt(sum o*o) (zero -> 1), n3 = sum m*o / (n1*n2); the misfit adds
+ * -(m*o/(n1*n2)) over the traces on the grid; every trace's residual is
+ * -(o/(n1*n2) - (m/(n1*n1))*n3).  With `clip` (2D only) the residuals at or above
+ * the magnitude at index 97*nt*nr/100 of the ascending sort are set to zero. */
+static int corr_misfit(int nr, int nt, const int *valid, const float *datamod, const float *obs, int clip,
+                       float *datares, float *mis)
+{
+    for (int tr = 0; tr < nr; tr++) {
+        const float *m = datamod + (long)tr * nt, *o = obs + (long)tr * nt;
+        float n1 = 0.0f, n2 = 0.0f, n3 = 0.0f;
+        for (int it = 0; it < nt; it++) {
+            n1 += m[it] * m[it];
+            n2 += o[it] * o[it];
+            n3 += m[it] * o[it];
+        }
+        n1 = sqrtf(n1);
+        n2 = sqrtf(n2);
+        if (n1 == 0) n1 = 1.0f;
+        if (n2 == 0) n2 = 1.0f;
+        if (valid[tr])
+            for (int it = 0; it < nt; it++) {
+                float v = (float)((-1.0) * (m[it] * o[it] / (n1 * n2)));
+                *mis += v;
+            }
+        n3 /= (n1 * n2);
+        float *r = datares + (long)tr * nt;
+        for (int it = 0; it < nt; it++) r[it] = (float)((-1.0) * 1 * ((o[it] / (n1 * n2)) - (m[it] / (n1 * n1)) * n3));
+    }
+    if (!clip) return 0;
+    const long tot = (long)nt * nr;
+    float *fres = malloc(tot * sizeof(float));
+    if (!fres) return -1;
+    for (long k = 0; k < tot; k++) fres[k] = fabsf(datares[k]);
+    qsort(fres, tot, sizeof(float), cmp_float);
+    const float pclip = fres[(long)((97ul * (unsigned long)nt * (unsigned long)nr) / 100ul)];
+    for (long k = 0; k < tot; k++)
+        if (fabsf(datares[k]) >= pclip) datares[k] = 0.0f;
+    free(fres);
+    return 0;
+}
+
 /* FwiAcoustic2D::run_optimal with the DIFFERENCE (misfit_type 0) or CORRELATION (1) misfit and pressure data, one shot.
  * The forward states are kept for every step instead of being recomputed from
  * checkpoints; recomputation is deterministic, so the gradient is the same.
@@ -466,39 +510,13 @@ int orc_fwi_a2d(const orc_grid *g, int nx, int nz, const float *vp, const float 
             for (int it = 0; it < nt; it++) datares[it + (long)tr * nt] = 1 * (datamod[it + (long)tr * nt] - obs[it + (long)tr * nt]);
         }
     } else {
-        /* CORRELATION (lib/fwi.cpp:617-645, 808-849): per-trace norms in float, the
-         * misfit over traces on the grid, residuals of every trace, then residuals
-         * at or above the 97th-percentile magnitude of the shot set to zero */
-        for (int tr = 0; tr < nr; tr++) {
-            const float *m = datamod + (long)tr * nt, *o = obs + (long)tr * nt;
-            float n1 = 0.0f, n2 = 0.0f, n3 = 0.0f;
-            for (int it = 0; it < nt; it++) {
-                n1 += m[it] * m[it];
-                n2 += o[it] * o[it];
-                n3 += m[it] * o[it];
-            }
-            n1 = sqrtf(n1);
-            n2 = sqrtf(n2);
-            if (n1 == 0) n1 = 1.0f;
-            if (n2 == 0) n2 = 1.0f;
-            if (gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0)
-                for (int it = 0; it < nt; it++) {
-                    float v = (float)((-1.0) * (m[it] * o[it] / (n1 * n2)));
-                    mis += v;
-                }
-            n3 /= (n1 * n2);
-            float *r = datares + (long)tr * nt;
-            for (int it = 0; it < nt; it++) r[it] = (float)((-1.0) * 1 * ((o[it] / (n1 * n2)) - (m[it] / (n1 * n1)) * n3));
-        }
-        const long tot = (long)nt * nr;
-        float *fres = malloc(tot * sizeof(float));
-        if (!fres) return -1;
-        for (long k = 0; k < tot; k++) fres[k] = fabsf(datares[k]);
-        qsort(fres, tot, sizeof(float), cmp_float);
-        const float pclip = fres[(long)((97ul * (unsigned long)nt * (unsigned long)nr) / 100ul)];
-        for (long k = 0; k < tot; k++)
-            if (fabsf(datares[k]) >= pclip) datares[k] = 0.0f;
-        free(fres);
+        /* CORRELATION (lib/fwi.cpp:617-645, 808-849), with the percentile clip */
+        int *valid = malloc(nr * sizeof(int));
+        if (!valid) return -1;
+        for (int tr = 0; tr < nr; tr++) valid[tr] = gmap[2 * tr] >= 0 && gmap[2 * tr + 1] >= 0;
+        const int rc = corr_misfit(nr, nt, valid, datamod, obs, 1, datares, &mis);
+        free(valid);
+        if (rc) return rc;
     }
     *misfit = mis;
     float *zero = calloc(n, sizeof(float));
@@ -922,12 +940,13 @@ static void a3d_corr(const orc_grid3 *g, int nx, int ny, int nz, const float *Vp
             }
 }
 
-/* FwiAcoustic3D::run_optimal with the DIFFERENCE misfit and pressure data, one shot,
+/* FwiAcoustic3D::run_optimal with the DIFFERENCE (misfit_type 0) or CORRELATION (1, no clip in 3D) misfit and pressure data, one shot,
  * all forward pressures kept (pairing as fw_state_at()). */
 int orc_fwi_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *vp, const float *rho, const float *Rx,
                 const float *Ry, const float *Rz, const float *Lm, const float *tab, int ns, const int *smap,
                 const float *sshift, const float *wav, int nr, const int *gmap, const float *gshift, const float *obs,
-                float *vpgrad, float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit)
+                int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod, float *datares,
+                double *misfit)
 {
     const int nt = g->nt;
     const long n = (long)g->nxp * g->nyp * g->nzp;
@@ -943,14 +962,23 @@ int orc_fwi_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *vp, con
         memcpy(Ps + (size_t)it * n, fw.f[0], n * sizeof(float));
     }
     float mis = 0.0f;
-    for (int tr = 0; tr < nr; tr++) {
-        const int valid = gmap[3 * tr] >= 0 && gmap[3 * tr + 1] >= 0 && gmap[3 * tr + 2] >= 0;
-        for (int it = 0; it < nt; it++) {
-            long k = it + (long)tr * nt;
-            float r = datamod[k] - obs[k];
-            if (valid) mis += 0.5 * r * r;
-            datares[k] = 1 * (datamod[k] - obs[k]);
+    if (misfit_type == 0) {
+        for (int tr = 0; tr < nr; tr++) {
+            const int valid = gmap[3 * tr] >= 0 && gmap[3 * tr + 1] >= 0 && gmap[3 * tr + 2] >= 0;
+            for (int it = 0; it < nt; it++) {
+                long k = it + (long)tr * nt;
+                float r = datamod[k] - obs[k];
+                if (valid) mis += 0.5 * r * r;
+                datares[k] = 1 * (datamod[k] - obs[k]);
+            }
         }
+    } else {
+        int *valid = malloc(nr * sizeof(int));
+        if (!valid) return -1;
+        for (int tr = 0; tr < nr; tr++) valid[tr] = gmap[3 * tr] >= 0 && gmap[3 * tr + 1] >= 0 && gmap[3 * tr + 2] >= 0;
+        const int rc = corr_misfit(nr, nt, valid, datamod, obs, 0, datares, &mis);
+        free(valid);
+        if (rc) return rc;
     }
     *misfit = mis;
     float *zero = calloc(n, sizeof(float));

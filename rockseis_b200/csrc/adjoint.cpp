@@ -473,7 +473,7 @@ rsgpu_status Adjoint::run()
             if (kind == RSGPU_KIND_FWI) {
                 cudaError_t e = elastic() ? launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
                                 : misfit_type == RSGPU_MISFIT_CORRELATION
-                                    ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream)
+                                    ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream, true)
                                     : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
                 launches += 1;

@@ -214,7 +214,8 @@ __global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, d
 // residual -(o/(n1*n2) - (m/(n1*n1))*n3) for every trace; misfit += -(m*o/(n1*n2))
 // over the traces on the grid.  Then the residuals whose magnitude reaches the
 // 97th-percentile value of all |residual| samples of the shot (the element at
-// index (97*nt*nrec)/100 of the ascending sort) are zeroed.  The order statistic
+// index (97*nt*nrec)/100 of the ascending sort) are zeroed (CLIP; the 3D
+// driver, FwiAcoustic3D lib/fwi.cpp:1696-1722, has no clip).  The order statistic
 // comes from a radix select on the magnitude bit patterns, which order like the
 // non-negative values.  One CTA per shot; dynamic shared memory holds n1*n2 of
 // every trace.
@@ -235,7 +236,7 @@ __device__ __forceinline__ typename Bits<T>::U mag_bits(T x)
     return u & ~((U)1 << (Bits<T>::NB - 1));
 }
 
-template <typename T, int ACC>
+template <typename T, int ACC, bool CLIP>
 __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, double *misfit)
 {
     using U = typename Bits<T>::U;
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, dou
             r[it] = -X<T>::sub(X<T>::div(o[it], n12), X<T>::mul(X<T>::div(m[it], n11), n3));
     }
     __syncthreads();
+    if (CLIP) {
     // radix select of the k-th smallest magnitude, most significant digit first
     __shared__ unsigned int hist[256];
     __shared__ U prefix_s;
@@ -291,6 +293,7 @@ __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, dou
     const U clip = prefix_s;
     for (long k = threadIdx.x; k < n; k += blockDim.x)
         if (mag_bits(d.res[k]) >= clip) d.res[k] = T(0);
+    }
     if (threadIdx.x != 0) return;
     // misfit, traces then samples, on the traces inside the grid
     T mis = 0;
@@ -705,17 +708,24 @@ cudaError_t launch_corr_fwi_a3d(int prec, int acc, const void *desc, int nshots,
     return cudaGetLastError();
 }
 
+template <bool CLIP>
+static void launch_corr(int prec, int acc, const void *desc, int nshots, size_t sm, double *misfit, cudaStream_t st)
+{
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) residual_corr<double, ACC_F64, CLIP><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
+        else residual_corr<double, ACC_REF, CLIP><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
+    } else {
+        if (acc == ACC_F64) residual_corr<float, ACC_F64, CLIP><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
+        else residual_corr<float, ACC_REF, CLIP><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
+    }
+}
+
 cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
-                                 cudaStream_t st)
+                                 cudaStream_t st, bool clip)
 {
     const size_t sm = (size_t)std::max(nrec_max, 1) * (prec == PREC_F64 ? 8 : 4);
-    if (prec == PREC_F64) {
-        if (acc == ACC_F64) residual_corr<double, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
-        else residual_corr<double, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2D<double> *)desc, misfit);
-    } else {
-        if (acc == ACC_F64) residual_corr<float, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
-        else residual_corr<float, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2D<float> *)desc, misfit);
-    }
+    if (clip) launch_corr<true>(prec, acc, desc, nshots, sm, misfit, st);
+    else launch_corr<false>(prec, acc, desc, nshots, sm, misfit, st);
     return cudaGetLastError();
 }
 

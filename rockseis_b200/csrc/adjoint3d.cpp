@@ -60,10 +60,20 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         set_error("the 3D adjoint driver is built for acoustic RTM images and FWI gradients");
         return RSGPU_ERR_UNSUPPORTED;
     }
-    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE) {
-        set_error("only the DIFFERENCE misfit is built");
+    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION) {
+        set_error("misfit %d: DIFFERENCE and CORRELATION are built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
+    if (k_ == RSGPU_KIND_FWI && o->misfit == RSGPU_MISFIT_CORRELATION) {
+        const int lim = 49152 / (c->precision == RSGPU_F64 ? 8 : 4);
+        for (int i = 0; i < ns; i++)
+            if (s[i].shot.nrec > lim) {
+                set_error("shot %d: the CORRELATION misfit takes at most %d receivers per shot", i, lim);
+                return RSGPU_ERR_UNSUPPORTED;
+            }
+    }
+    misfit_type = o->misfit;
+    for (int i = 0; i < ns; i++) nrec_max = std::max(nrec_max, s[i].shot.nrec);
     if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
         set_error("bad checkpoint precision %d", o->ckpt_precision);
         return RSGPU_ERR_ARG;
@@ -326,7 +336,10 @@ rsgpu_status Adjoint3D::run()
             fw_steps += 1;
             if (fwi()) {
                 ST(fw->set_recording(false));
-                cudaError_t e = launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                cudaError_t e = misfit_type == RSGPU_MISFIT_CORRELATION
+                                    ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit),
+                                                           stream, false)
+                                    : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
                 launches += 1;
             }

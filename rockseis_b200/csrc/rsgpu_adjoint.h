@@ -91,10 +91,11 @@ cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots,
 // ACC_REF in the element type, sequentially in the reference's order; ACC_F64 in
 // double by a fixed-order tree reduction.
 cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
-// CORRELATION misfit (normalised zero-lag correlation per trace) and its residuals
-// with the 97th-percentile magnitude clip; nrec_max bounds the shared memory.
+// CORRELATION misfit (normalised zero-lag correlation per trace) and its residuals,
+// with the 97th-percentile magnitude clip of the 2D driver when `clip`; nrec_max
+// bounds the shared memory.
 cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
-                                 cudaStream_t st);
+                                 cudaStream_t st, bool clip);
 cudaError_t launch_corr_fwi_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
                                 double dz, cudaStream_t st);
 cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax,

@@ -19,6 +19,7 @@ public:
 
     int kind = RSGPU_KIND_RTM, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
     int ncheck = 0, nxmax = 0, nymax = 0;
+    int misfit_type = 0, nrec_max = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan3D> fw, bw;
     cudaStream_t stream = nullptr;

@@ -223,6 +223,8 @@ def a3d_cases(g):
     g["a3d_fwi_obs"] = obs
     for k, v in api.ref_fwi_a3d(pb, sc, wav, gc, obs, 5).items():
         g[f"a3d_fwi_{k}"] = np.asarray(v)
+    for k, v in api.ref_fwi_a3d(pb, sc, wav, gc, obs, 5, misfit=1).items():
+        g[f"a3d_fwi_corr_{k}"] = np.asarray(v)
     g["a3d_cases"] = np.array([f"a3d_fs{fs}_s{sf}_r{rf}" for fs, sf, rf in ((0, 0, 0), (1, 0, 3), (0, 1, 0))])
 
 

@@ -176,13 +176,13 @@ def fwi3d_case(**kw):
     return c
 
 
-def oracle_fwi3d(c):
+def oracle_fwi3d(c, misfit=0):
     s, r = c.src, c.rec
     return api.orc_fwi_a3d(c.pb, [a.astype(np.float32) for a in c.model.padded()], c.tab, s.smap, s.sshift,
-                           s.data.astype(np.float32), r.gmap, r.gshift, c.obs)
+                           s.data.astype(np.float32), r.gmap, r.gshift, c.obs, misfit)
 
 
-def gpu_fwi3d(c, ncheck=6, precision=None, ckpt=abi.CKPT_NATIVE, accum=abi.ACCUM_REFERENCE):
+def gpu_fwi3d(c, ncheck=6, precision=None, ckpt=abi.CKPT_NATIVE, accum=abi.ACCUM_REFERENCE, misfit=0):
     from rockseis_b200.rockseis import Data3D, FwiAcoustic3D, Image3D
     prec = c.precision if precision is None else precision
     c.rec.data = np.ascontiguousarray(c.obs.astype(abi.real_dtype(prec)))
@@ -190,6 +190,7 @@ def gpu_fwi3d(c, ncheck=6, precision=None, ckpt=abi.CKPT_NATIVE, accum=abi.ACCUM
     f.setNcheck(ncheck)
     f.setCheckpointPrecision(ckpt)
     f.setAccumulation(accum)
+    f.setMisfit_type(misfit)
     f.setVpgrad(Image3D("vp", c.model, 1, 1, 1, prec))
     f.setRhograd(Image3D("rho", c.model, 1, 1, 1, prec))
     f.setWavgrad(Data3D(c.src.ntrace, c.nt, c.dt, 0.0, prec))
@@ -218,3 +219,13 @@ def test_fwi3d_fast_fp16_checkpoints_close_to_exact(require_gpu):
     err = {k: rel_l2(got[k], ref[k]) for k in ("vpgrad", "rhograd", "wavgrad")}
     print(f"3D FWI gradient, FMA + FP16 checkpoints + FP64 accumulation vs exact: {err}")
     assert max(err.values()) <= 1e-3, err
+
+
+def test_fwi3d_correlation_misfit_exact_bitwise(require_gpu):
+    c = fwi3d_case()
+    ref = oracle_fwi3d(c, misfit=abi.MISFIT_CORRELATION)
+    got = gpu_fwi3d(c, ncheck=5, misfit=abi.MISFIT_CORRELATION)
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        assert np.abs(ref[k]).max() > 0, k
+        assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
+    assert got["misfit"] == ref["misfit"] and got["misfit"] < 0

@@ -267,3 +267,17 @@ def test_oracle_3d_fwi_gradient_matches_reference():
         assert np.abs(ref).max() > 0, k
         assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
     assert r["misfit"] == float(GOLD["a3d_fwi_misfit"])
+
+
+def test_oracle_3d_correlation_misfit_matches_reference():
+    # FwiAcoustic3D's CORRELATION residuals carry no percentile clip
+    case = "a3d_fs0_s0_r0"
+    pb = _a3d_problem(0)
+    g = lambda k: GOLD[f"{case}_{k}"]  # noqa: E731
+    r = api.orc_fwi_a3d(pb, list(g("models")), GOLD["a3d_tab"], g("smap"), g("sshift"), GOLD["a3d_wav"], g("gmap"),
+                        g("gshift"), GOLD["a3d_fwi_obs"], misfit=1)
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        ref = GOLD[f"a3d_fwi_corr_{k}"]
+        assert np.abs(ref).max() > 0, k
+        assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
+    assert r["misfit"] == float(GOLD["a3d_fwi_corr_misfit"])
