@@ -190,6 +190,30 @@ def adjoint_cases(g):
     g["rtm_image_h3"] = img
 
 
+def e2d_fwi_cases(g):
+    """FwiElastic2D::run_optimal (P, Ux, Uz data) on the small shot, observed data
+    modelled by the reference in a model with a slow lens."""
+    vp, vs, rho, sc, gc, wav = shot_inputs(41, True)
+    vtrue = vp.copy()
+    vtrue[10:18, 15:26] *= 0.93
+    pbt = problem(0, vtrue, vs, rho)
+    obs3 = [api.ref_modelling_e2d(pbt, sc, wav, PRESSURE, gc, f) for f in (PRESSURE, VX, VZ)]
+    pb = problem(0, vp, vs, rho)
+    g["e2dfwi_vp"], g["e2dfwi_vs"], g["e2dfwi_rho"], g["e2dfwi_wav"] = vp, vs, rho, wav
+    g["e2dfwi_sc"], g["e2dfwi_gc"], g["e2dfwi_obs"] = sc, gc, np.stack(obs3)
+    prep(g, "e2dfwi", 0, vp, vs, rho, sc, gc, PRESSURE, PRESSURE)
+    s = SHOT
+    rg = grid(s["nx"], s["nz"], s["lpml"], s["dx"], s["dx"], s["dt"], s["nt"], s["order"], 0)
+    for name, field in (("vx", VX), ("vz", VZ)):
+        mp = np.zeros((len(gc), 2), np.int32)
+        sh = np.zeros((len(gc), 2), np.float32)
+        api.ref().ref_makemap2d_field_f(C.byref(rg), len(gc), np.ascontiguousarray(gc).ctypes.data, 1, field,
+                                        mp.ctypes.data, sh.ctypes.data)
+        g[f"e2dfwi_gmap_{name}"], g[f"e2dfwi_gshift_{name}"] = mp, sh
+    for k, v in api.ref_fwi_e2d(pb, sc, wav, PRESSURE, gc, obs3, 5).items():
+        g[f"e2dfwi_out_{k}"] = np.asarray(v)
+
+
 def a3d_cases(g):
     """Acoustic 3D shots (ModellingAcoustic3D::run) with reference-made inputs."""
     nx, ny, nz, L, nt, dx = 15, 13, 14, 4, 70, 10.0
@@ -239,6 +263,7 @@ def main():
     revolve_cases(g)
     modelling_cases(g)
     adjoint_cases(g)
+    e2d_fwi_cases(g)
     a3d_cases(g)
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {len(g)} arrays, {os.path.getsize(OUT)} bytes")
