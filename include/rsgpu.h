@@ -190,9 +190,10 @@ typedef struct {
                             checkpoint slots hold the state as 16-bit values with a power-of-two
                             scale per array */
     int accum;           /* RSGPU_ACCUM_* */
-    int misfit;          /* RSGPU_MISFIT_DIFFERENCE; RSGPU_MISFIT_CORRELATION for acoustic 2D and 3D FWI
-                            (lib/fwi.cpp:617-645, 808-849 with the 97th-percentile residual clip;
-                            3D :1511-1540, 1696-1722 without it) */
+    int misfit;          /* RSGPU_MISFIT_DIFFERENCE; RSGPU_MISFIT_CORRELATION for the FWI drivers
+                            (acoustic 2D lib/fwi.cpp:617-645, 808-849 with the 97th-percentile
+                            residual clip; acoustic 3D :1511-1540, 1696-1722 without it;
+                            elastic 2D :2939-3001, 3309-3426 with the x/z and P clips) */
     int nhx, nhz;        /* RTM extended-image lags (Rtm::setNhx/setNhz; odd, 1 = zero lag) */
     int nhy;             /* 3D RTM y lags (Rtm::setNhy; odd, 0 or 1 = zero lag) */
     int reserved[9];

@@ -66,7 +66,7 @@ def oracle() -> C.CDLL:
                                                                                   V, V, V, V]
         _oracle.orc_rtm_a2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 4 + [I, V, V, V, I, V, V, V, I, I, V]
         _oracle.orc_der2d.argtypes = [I, I, I, C.c_float, C.c_float, I, V, V]
-        _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V] + \
+        _oracle.orc_fwi_e2d.argtypes = [C.POINTER(OrcGrid), I, I] + [V] * 3 + [V] * 6 + [I, V, V, V, I, I, V, V, V, I] + \
             [V] * 4 + [V, V, V]
         _oracle.orc_fwi_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 7 + [I, V, V, V, I, V, V, V, I] + \
             [V] * 5 + [V]
@@ -96,6 +96,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+        _ref.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
@@ -326,7 +327,7 @@ def orc_modelling_a3d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, 
 
 
 # ---------------------------------------------------------------- elastic FWI
-def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck):
+def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
     """FwiElastic2D::run_optimal; obs3 = [P, Ux, Uz] observed data, each [nr][nt]."""
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
@@ -337,15 +338,16 @@ def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck):
     ress = np.zeros((3, nr, pb.nt), np.float32)
     mis = C.c_double()
     vp, vs, rho, w, op, ox, oz = _keep(pb.vp, pb.vs, pb.rho, wav, obs3[0], obs3[1], obs3[2], dtype=np.float32)
-    r = ref().ref_fwi_e2d_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
-                            _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]), _p(wg),
-                            _p(mods), _p(ress), C.byref(mis))
+    fn = ref().ref_fwi_e2d_corr_f if misfit == 1 else ref().ref_fwi_e2d_f
+    r = fn(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
+           _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]), _p(wg),
+           _p(mods), _p(ress), C.byref(mis))
     assert r == 1
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out
 
 
-def orc_fwi_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmaps, gshifts, obs3):
+def orc_fwi_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmaps, gshifts, obs3, misfit=0):
     g = pb.orc_grid()
     ns, nr = len(smap), len(gmaps[0])
     out = {k: np.zeros((pb.nz, pb.nx), np.float32) for k in ("vpgrad", "vsgrad", "rhograd")}
@@ -362,7 +364,7 @@ def orc_fwi_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmaps, gshifts, obs3
     gmp = (C.c_void_p * 3)(*[m.ctypes.data for m in gm])
     gsp = (C.c_void_p * 3)(*[s.ctypes.data for s in gs])
     r = oracle().orc_fwi_e2d(C.byref(g), pb.nx, pb.nz, _p(vp), _p(vs), _p(rho), _p(Rx), _p(Rz), _p(L), _p(L2M),
-                             _p(M), _p(tb), ns, _p(sm), _p(ss), _p(w), sfield, nr, gmp, gsp, _p(ob),
+                             _p(M), _p(tb), ns, _p(sm), _p(ss), _p(w), sfield, nr, gmp, gsp, _p(ob), misfit,
                              _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]), _p(wg), _p(mods), _p(ress),
                              C.byref(mis))
     assert r == 0

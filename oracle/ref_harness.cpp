@@ -148,7 +148,7 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
 template <typename T>
 int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, const double *sc, const T *wav,
             int sfield, int nr, const double *gc, const T *obsp, const T *obsx, const T *obsz, int ncheck, T *vpgrad,
-            T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit)
+            T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit, int misfit_type = 0)
 {
     auto model = make_e2d<T>(g, vp, vs, rho);
     auto geom = model->getGeom();
@@ -173,7 +173,7 @@ int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
     fwi.setDataresP(dr[0]); fwi.setDataresUx(dr[1]); fwi.setDataresUz(dr[2]);
     fwi.setVpgrad(img[0]); fwi.setVsgrad(img[1]); fwi.setRhograd(img[2]);
     fwi.setWavgrad(wg);
-    fwi.setMisfit_type(DIFFERENCE);
+    fwi.setMisfit_type((rs_fwimisfit)misfit_type);
     fwi.setNcheck(ncheck);
     fwi.setIncore(true);
     fwi.setSnapfile(tmpname("fwie2d"));
@@ -464,6 +464,14 @@ int ref_fwi_e2d_f(const ref_grid *g, const float *vp, const float *vs, const flo
 {
     return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
                           rhograd, wavgrad, mods, ress, misfit);
+}
+int ref_fwi_e2d_corr_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns,
+                       const double *sc, const float *wav, int sfield, int nr, const double *gc, const float *obsp,
+                       const float *obsx, const float *obsz, int ncheck, float *vpgrad, float *vsgrad, float *rhograd,
+                       float *wavgrad, float *mods, float *ress, double *misfit)
+{
+    return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
+                          rhograd, wavgrad, mods, ress, misfit, 1);
 }
 int ref_fwi_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                   const float *wav, int nr, const double *gc, const float *obs, int ncheck,

@@ -790,14 +790,88 @@ static void e2d_scale(int nx, int nz, const float *Vp, const float *Vs, const fl
         }
 }
 
-/* FwiElastic2D::run_optimal with the DIFFERENCE misfit: P, Ux (VX) and Uz (VZ)
+/* FwiElastic2D CORRELATION misfit and residuals (lib/fwi.cpp:2939-3001, 3309-3426)
+ * for the P, Ux, Uz components (c = 0, 1, 2 at offsets c*nr*nt): per trace and
+ * component, norms in float as in the acoustic case; the misfit adds
+ * (rp + rx + rz) with non-finite terms set to zero, over the traces whose Ux map
+ * is on the grid; residuals for every trace.  Clips: x and z share the larger of
+ * their two 97th-percentile magnitudes, and a sample whose x residual reaches it
+ * loses both its x and z residual; P has its own clip; non-finite residuals are
+ * set to zero. */
+static int fin(float v) { return !isnan(v) && !isinf(v); }
+
+static float kth_mag(const float *r, long tot, long pos, float *buf)
+{
+    for (long k = 0; k < tot; k++) buf[k] = fabsf(r[k]);
+    qsort(buf, tot, sizeof(float), cmp_float);
+    return buf[pos];
+}
+
+static int e2d_corr_misfit(int nr, int nt, const int *gmap_vx, const float *mods, const float *obs, float *ress, float *mis)
+{
+    const long nd = (long)nr * nt;
+    for (int tr = 0; tr < nr; tr++) {
+        float n1[3], n2[3], n3[3];
+        for (int c = 0; c < 3; c++) {
+            const float *m = mods + c * nd + (long)tr * nt, *o = obs + c * nd + (long)tr * nt;
+            n1[c] = n2[c] = n3[c] = 0.0f;
+            for (int it = 0; it < nt; it++) {
+                n1[c] += m[it] * m[it];
+                n2[c] += o[it] * o[it];
+                n3[c] += m[it] * o[it];
+            }
+            n1[c] = sqrtf(n1[c]);
+            n2[c] = sqrtf(n2[c]);
+            if (n1[c] == 0) n1[c] = 1.0f;
+            if (n2[c] == 0) n2[c] = 1.0f;
+        }
+        if (gmap_vx[2 * tr] >= 0 && gmap_vx[2 * tr + 1] >= 0)
+            for (int it = 0; it < nt; it++) {
+                float r[3];
+                for (int c = 0; c < 3; c++) {
+                    const long k = c * nd + (long)tr * nt + it;
+                    r[c] = (float)((-1.0) * (mods[k] * obs[k] / (n1[c] * n2[c])));
+                    if (!fin(r[c])) r[c] = 0.0f;
+                }
+                *mis += (r[0] + r[1] + r[2]);
+            }
+        for (int c = 0; c < 3; c++) {
+            n3[c] /= (n1[c] * n2[c]);
+            for (int it = 0; it < nt; it++) {
+                const long k = c * nd + (long)tr * nt + it;
+                ress[k] = (float)((-1.0) * ((obs[k] / (n1[c] * n2[c])) - (mods[k] / (n1[c] * n1[c])) * n3[c]));
+            }
+        }
+    }
+    float *buf = malloc(nd * sizeof(float));
+    if (!buf) return -1;
+    const long pos = (long)((97ul * (unsigned long)nt * (unsigned long)nr) / 100ul);
+    float *rp = ress, *rx = ress + nd, *rz = ress + 2 * nd;
+    float pclip = kth_mag(rx, nd, pos, buf);
+    const float zclip = kth_mag(rz, nd, pos, buf);
+    if (zclip > pclip) pclip = zclip;
+    for (long k = 0; k < nd; k++) {
+        if (fabsf(rx[k]) >= pclip) { rx[k] = 0.0f; rz[k] = 0.0f; }
+        if (!fin(rx[k])) rx[k] = 0.0f;
+        if (!fin(rz[k])) rz[k] = 0.0f;
+    }
+    pclip = kth_mag(rp, nd, pos, buf);
+    for (long k = 0; k < nd; k++) {
+        if (fabsf(rp[k]) >= pclip) rp[k] = 0.0f;
+        if (!fin(rp[k])) rp[k] = 0.0f;
+    }
+    free(buf);
+    return 0;
+}
+
+/* FwiElastic2D::run_optimal with the DIFFERENCE (misfit_type 0) or CORRELATION (1) misfit: P, Ux (VX) and Uz (VZ)
  * data at the receivers; all forward states kept in memory.  maps: gmap[3] /
  * gshift[3] for the P, VX and VZ trace sets; obs/mods/ress: [3][nr][nt]. */
 int orc_fwi_e2d(const orc_grid *g, int nx, int nz, const float *vp, const float *vs, const float *rho,
                 const float *Rx, const float *Rz, const float *Lm, const float *L2M, const float *M, const float *tab,
                 int ns, const int *smap, const float *sshift, const float *wav, int sfield, int nr,
-                const int *const *gmap, const float *const *gshift, const float *obs, float *vpg, float *vsg,
-                float *rhog, float *wavgrad, float *mods, float *ress, double *misfit)
+                const int *const *gmap, const float *const *gshift, const float *obs, int misfit_type, float *vpg,
+                float *vsg, float *rhog, float *wavgrad, float *mods, float *ress, double *misfit)
 {
     const int nt = g->nt;
     const long n = (long)g->nxp * g->nzp, nd = (long)nr * nt;
@@ -816,18 +890,22 @@ int orc_fwi_e2d(const orc_grid *g, int nx, int nz, const float *vp, const float 
         record(&fw, 3, nr, gmap[2], gshift[2], NULL, mods + 2 * nd, it);
         for (int k = 0; k < 5; k++) memcpy(Ps + ((size_t)it * 5 + k) * n, fw.f[k], n * sizeof(float));
     }
-    /* computeMisfit / computeResiduals (lib/fwi.cpp:2852-2905, 3227-3290), DIFFERENCE */
     float mis = 0.0f;
-    for (int tr = 0; tr < nr; tr++) {
-        const int valid = gmap[1][2 * tr] >= 0 && gmap[1][2 * tr + 1] >= 0;
-        for (int it = 0; it < nt; it++) {
-            long k = it + (long)tr * nt;
-            float rp = mods[k] - obs[k], rx = mods[nd + k] - obs[nd + k], rz = mods[2 * nd + k] - obs[2 * nd + k];
-            if (valid) mis += 0.5 * (rp * rp + rx * rx + rz * rz);
-            ress[k] = rp;
-            ress[nd + k] = rx;
-            ress[2 * nd + k] = rz;
+    if (misfit_type == 0) {
+        /* computeMisfit / computeResiduals (lib/fwi.cpp:2852-2905, 3227-3290), DIFFERENCE */
+        for (int tr = 0; tr < nr; tr++) {
+            const int valid = gmap[1][2 * tr] >= 0 && gmap[1][2 * tr + 1] >= 0;
+            for (int it = 0; it < nt; it++) {
+                long k = it + (long)tr * nt;
+                float rp = mods[k] - obs[k], rx = mods[nd + k] - obs[nd + k], rz = mods[2 * nd + k] - obs[2 * nd + k];
+                if (valid) mis += 0.5 * (rp * rp + rx * rx + rz * rz);
+                ress[k] = rp;
+                ress[nd + k] = rx;
+                ress[2 * nd + k] = rz;
+            }
         }
+    } else if (e2d_corr_misfit(nr, nt, gmap[1], mods, obs, ress, &mis)) {
+        return -1;
     }
     *misfit = mis;
     float *zero = calloc(5 * n, sizeof(float));

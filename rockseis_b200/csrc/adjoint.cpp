@@ -107,12 +107,12 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_UNSUPPORTED;
     }
     const bool el = c->physics == RSGPU_ELASTIC2D;
-    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && !(o->misfit == RSGPU_MISFIT_CORRELATION && !el)) {
-        set_error("misfit %d: DIFFERENCE is built for every driver, CORRELATION for acoustic 2D FWI", o->misfit);
+    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION) {
+        set_error("misfit %d: DIFFERENCE and CORRELATION are built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (o->misfit == RSGPU_MISFIT_CORRELATION && kind == RSGPU_KIND_FWI) {
-        const int lim = 49152 / (c->precision == RSGPU_F64 ? 8 : 4);
+        const int lim = 49152 / ((el ? 3 : 1) * (c->precision == RSGPU_F64 ? 8 : 4));
         for (int i = 0; i < ns; i++)
             if (s[i].shot.nrec > lim) {
                 set_error("shot %d: the CORRELATION misfit takes at most %d receivers per shot", i, lim);
@@ -471,8 +471,12 @@ rsgpu_status Adjoint::run()
             fw_steps += 1;
             ST(fw->set_recording(false));
             if (kind == RSGPU_KIND_FWI) {
-                cudaError_t e = elastic() ? launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
-                                : misfit_type == RSGPU_MISFIT_CORRELATION
+                const bool corr = misfit_type == RSGPU_MISFIT_CORRELATION;
+                cudaError_t e = elastic()
+                                ? (corr ? launch_residual_corr_e2d(prec, acc, D(o_res), nshots, nrec_max,
+                                                                   (double *)D(o_misfit), stream)
+                                        : launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream))
+                                : corr
                                     ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream, true)
                                     : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }

@@ -236,6 +236,53 @@ __device__ __forceinline__ typename Bits<T>::U mag_bits(T x)
     return u & ~((U)1 << (Bits<T>::NB - 1));
 }
 
+// Magnitude bit pattern of the k-th smallest |r[i]|, i < n (k < n), found by the
+// whole CTA with four (float) or eight (double) 8-bit histogram passes.
+template <typename T>
+__device__ typename Bits<T>::U kth_mag_bits(const T *r, long n, long k)
+{
+    using U = typename Bits<T>::U;
+    __shared__ unsigned int hist[256];
+    __shared__ U prefix_s;
+    __shared__ long rank_s;
+    __syncthreads();
+    if (threadIdx.x == 0) { prefix_s = 0; rank_s = k; }
+    U mask = 0;
+    for (int shift = Bits<T>::NB - 8; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        const U prefix = prefix_s;
+        for (long i = threadIdx.x; i < n; i += blockDim.x) {
+            const U u = mag_bits(r[i]);
+            if ((u & mask) == prefix) atomicAdd(&hist[(unsigned)(u >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long rr = rank_s;
+            int b = 0;
+            while (b < 255 && rr >= (long)hist[b]) { rr -= hist[b]; b++; }
+            rank_s = rr;
+            prefix_s = prefix | ((U)b << shift);
+        }
+        mask |= (U)255 << shift;
+        __syncthreads();
+    }
+    const U out = prefix_s;
+    __syncthreads();
+    return out;
+}
+
+template <typename T>
+__device__ __forceinline__ T from_bits(typename Bits<T>::U u)
+{
+    T x;
+    memcpy(&x, &u, sizeof x);
+    return x;
+}
+
+__device__ __forceinline__ bool finite_f(float v) { return isfinite(v); }
+__device__ __forceinline__ bool finite_f(double v) { return isfinite(v); }
+
 template <typename T, int ACC, bool CLIP>
 __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, double *misfit)
 {
@@ -265,34 +312,10 @@ __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, dou
     }
     __syncthreads();
     if (CLIP) {
-    // radix select of the k-th smallest magnitude, most significant digit first
-    __shared__ unsigned int hist[256];
-    __shared__ U prefix_s;
-    __shared__ long rank_s;
-    if (threadIdx.x == 0) { prefix_s = 0; rank_s = (long)((97ull * (unsigned long long)d.nt * (unsigned long long)d.nrec) / 100ull); }
-    U mask = 0;
-    for (int shift = Bits<T>::NB - 8; shift >= 0; shift -= 8) {
-        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
-        __syncthreads();
-        const U prefix = prefix_s;
-        for (long k = threadIdx.x; k < n; k += blockDim.x) {
-            const U u = mag_bits(d.res[k]);
-            if ((u & mask) == prefix) atomicAdd(&hist[(unsigned)(u >> shift) & 255u], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            long r = rank_s;
-            int b = 0;
-            while (b < 255 && r >= (long)hist[b]) { r -= hist[b]; b++; }
-            rank_s = r;
-            prefix_s = prefix | ((U)b << shift);
-        }
-        mask |= (U)255 << shift;
-        __syncthreads();
-    }
-    const U clip = prefix_s;
-    for (long k = threadIdx.x; k < n; k += blockDim.x)
-        if (mag_bits(d.res[k]) >= clip) d.res[k] = T(0);
+        const long pos = (long)((97ull * (unsigned long long)d.nt * (unsigned long long)d.nrec) / 100ull);
+        const U clip = kth_mag_bits(d.res, n, pos);
+        for (long k = threadIdx.x; k < n; k += blockDim.x)
+            if (mag_bits(d.res[k]) >= clip) d.res[k] = T(0);
     }
     if (threadIdx.x != 0) return;
     // misfit, traces then samples, on the traces inside the grid
@@ -305,6 +328,80 @@ __global__ void __launch_bounds__(256) residual_corr(const Resid2D<T> *desc, dou
             const T v = -X<T>::div(X<T>::mul(m[it], o[it]), nn[tr]);
             if (ACC == ACC_REF) mis = X<T>::add(mis, v);
             else mis64 += (double)v;
+        }
+    }
+    misfit[blockIdx.x] = ACC == ACC_REF ? (double)mis : mis64;
+}
+
+// FwiElastic2D CORRELATION (lib/fwi.cpp:2939-3001, 3309-3426): the acoustic
+// per-trace formulas for the P, Ux and Uz components; the misfit adds
+// (rp + rx + rz) with non-finite terms zeroed over the traces whose Ux map is on
+// the grid.  Clips: x and z share the larger of their 97th-percentile magnitudes
+// and a sample whose x residual reaches it loses its x and z residual; P has its
+// own; non-finite residuals become zero.  Comparisons are float comparisons, as in
+// the reference.  Dynamic shared memory: n1*n2 per component and trace.
+template <typename T, int ACC>
+__global__ void __launch_bounds__(256) residual_corr_e2d(const Resid2DE<T> *desc, double *misfit)
+{
+    extern __shared__ __align__(16) unsigned char corr_smem[];
+    T *nn = reinterpret_cast<T *>(corr_smem);            // [3][nrec]
+    const Resid2DE<T> d = desc[blockIdx.x];
+    const long n = (long)d.nrec * d.nt;
+    for (int tr = threadIdx.x; tr < d.nrec; tr += blockDim.x)
+        for (int c = 0; c < 3; c++) {
+            const T *m = d.mod[c] + (long)tr * d.nt, *o = d.obs[c] + (long)tr * d.nt;
+            T n1 = 0, n2 = 0, n3 = 0;
+            for (int it = 0; it < d.nt; it++) {
+                n1 = X<T>::add(n1, X<T>::mul(m[it], m[it]));
+                n2 = X<T>::add(n2, X<T>::mul(o[it], o[it]));
+                n3 = X<T>::add(n3, X<T>::mul(m[it], o[it]));
+            }
+            n1 = sqrt_rn(n1);
+            n2 = sqrt_rn(n2);
+            if (n1 == T(0)) n1 = T(1);
+            if (n2 == T(0)) n2 = T(1);
+            const T n12 = X<T>::mul(n1, n2), n11 = X<T>::mul(n1, n1);
+            n3 = X<T>::div(n3, n12);
+            nn[c * d.nrec + tr] = n12;
+            T *r = d.res[c] + (long)tr * d.nt;
+            for (int it = 0; it < d.nt; it++)
+                r[it] = -X<T>::sub(X<T>::div(o[it], n12), X<T>::mul(X<T>::div(m[it], n11), n3));
+        }
+    __syncthreads();
+    const long pos = (long)((97ull * (unsigned long long)d.nt * (unsigned long long)d.nrec) / 100ull);
+    T cx = from_bits<T>(kth_mag_bits(d.res[1], n, pos));
+    const T cz = from_bits<T>(kth_mag_bits(d.res[2], n, pos));
+    if (cz > cx) cx = cz;
+    for (long k = threadIdx.x; k < n; k += blockDim.x) {
+        T rx = d.res[1][k], rz = d.res[2][k];
+        if (fabs(rx) >= cx) { rx = T(0); rz = T(0); }
+        if (!finite_f(rx)) rx = T(0);
+        if (!finite_f(rz)) rz = T(0);
+        d.res[1][k] = rx;
+        d.res[2][k] = rz;
+    }
+    const T cp = from_bits<T>(kth_mag_bits(d.res[0], n, pos));
+    for (long k = threadIdx.x; k < n; k += blockDim.x) {
+        T rp = d.res[0][k];
+        if (fabs(rp) >= cp) rp = T(0);
+        if (!finite_f(rp)) rp = T(0);
+        d.res[0][k] = rp;
+    }
+    if (threadIdx.x != 0) return;
+    T mis = 0;
+    double mis64 = 0.0;
+    for (int tr = 0; tr < d.nrec; tr++) {
+        if (d.rec_pt_vx[tr] < 0) continue;
+        for (int it = 0; it < d.nt; it++) {
+            const long j = (long)tr * d.nt + it;
+            T r[3];
+            for (int c = 0; c < 3; c++) {
+                r[c] = -X<T>::div(X<T>::mul(d.mod[c][j], d.obs[c][j]), nn[c * d.nrec + tr]);
+                if (!finite_f(r[c])) r[c] = T(0);
+            }
+            const T s = X<T>::add(X<T>::add(r[0], r[1]), r[2]);
+            if (ACC == ACC_REF) mis = X<T>::add(mis, s);
+            else mis64 += (double)s;
         }
     }
     misfit[blockIdx.x] = ACC == ACC_REF ? (double)mis : mis64;
@@ -726,6 +823,20 @@ cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots
     const size_t sm = (size_t)std::max(nrec_max, 1) * (prec == PREC_F64 ? 8 : 4);
     if (clip) launch_corr<true>(prec, acc, desc, nshots, sm, misfit, st);
     else launch_corr<false>(prec, acc, desc, nshots, sm, misfit, st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
+                                     cudaStream_t st)
+{
+    const size_t sm = 3 * (size_t)std::max(nrec_max, 1) * (prec == PREC_F64 ? 8 : 4);
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) residual_corr_e2d<double, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2DE<double> *)desc, misfit);
+        else residual_corr_e2d<double, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2DE<double> *)desc, misfit);
+    } else {
+        if (acc == ACC_F64) residual_corr_e2d<float, ACC_F64><<<nshots, 256, sm, st>>>((const Resid2DE<float> *)desc, misfit);
+        else residual_corr_e2d<float, ACC_REF><<<nshots, 256, sm, st>>>((const Resid2DE<float> *)desc, misfit);
+    }
     return cudaGetLastError();
 }
 

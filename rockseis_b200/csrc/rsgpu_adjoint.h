@@ -96,6 +96,9 @@ cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, dou
 // bounds the shared memory.
 cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
                                  cudaStream_t st, bool clip);
+// The elastic CORRELATION misfit and residuals (P, Ux, Uz) with the reference's clips.
+cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
+                                     cudaStream_t st);
 cudaError_t launch_corr_fwi_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax, double dx,
                                 double dz, cudaStream_t st);
 cudaError_t launch_scale_grad_e2d(int prec, int acc, const void *desc, int nshots, int nxmax, int nzmax,

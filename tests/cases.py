@@ -141,8 +141,8 @@ class ElasticFwiCase:
                                           sfield, r.gmap, r.gshift.astype(np.float32), r.field).astype(t)
                     for r in self.recs]
 
-    def oracle(self):
+    def oracle(self, misfit=0):
         return api.orc_fwi_e2d(self.pb, [a.astype(np.float32) for a in self.model.padded()],
                                self.tab.astype(np.float32), self.src.smap, self.src.sshift, self.src.data, self.sfield,
                                [r.gmap for r in self.recs], [r.gshift for r in self.recs],
-                               [o.astype(np.float32) for o in self.obs])
+                               [o.astype(np.float32) for o in self.obs], misfit)

@@ -212,6 +212,8 @@ def e2d_fwi_cases(g):
         g[f"e2dfwi_gmap_{name}"], g[f"e2dfwi_gshift_{name}"] = mp, sh
     for k, v in api.ref_fwi_e2d(pb, sc, wav, PRESSURE, gc, obs3, 5).items():
         g[f"e2dfwi_out_{k}"] = np.asarray(v)
+    for k, v in api.ref_fwi_e2d(pb, sc, wav, PRESSURE, gc, obs3, 5, misfit=1).items():
+        g[f"e2dfwi_corr_{k}"] = np.asarray(v)
 
 
 def a3d_cases(g):

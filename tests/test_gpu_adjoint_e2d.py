@@ -90,3 +90,17 @@ def test_elastic_fwi_fast_mode_as_accurate_as_reference_float(require_gpu):
         base, err = rel_l2(exact[k], ref64[k]), rel_l2(got[k], ref64[k])
         print(f"{k}: FMA+FP16 checkpoints {err:.3g}, reference float {base:.3g} (vs FP64)")
         assert err <= max(1.25 * base + 1e-5, 1e-3), k
+
+
+@pytest.mark.parametrize("ncheck", [4, 9])
+def test_elastic_fwi_correlation_misfit_exact_bitwise(require_gpu, ncheck):
+    # CORRELATION misfit of P, Ux and Uz with the reference's x/z and P residual clips
+    c = ElasticFwiCase()
+    ref = c.oracle(misfit=abi.MISFIT_CORRELATION)
+    f = make_job(c, ncheck=ncheck)
+    f.setMisfit_type(abi.MISFIT_CORRELATION)
+    assert f.run_optimal() == 1
+    got = outputs(f)
+    assert_same(got, ref)
+    assert got["misfit"] < 0
+    assert (ref["datares"][0] == 0).mean() >= 0.03 and (ref["datares"][1] == 0).any()

@@ -295,3 +295,16 @@ def test_oracle_elastic_fwi_gradient_matches_reference():
         assert np.abs(ref).max() > 0, k
         assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
     assert r["misfit"] == float(g("out_misfit"))
+
+
+def test_oracle_elastic_correlation_misfit_matches_reference():
+    g = lambda k: GOLD[f"e2dfwi_{k}"]  # noqa: E731
+    pb = problem(0, g("vp"), g("rho"), g("vs"))
+    r = api.orc_fwi_e2d(pb, list(g("models")), g("tab"), g("smap"), g("sshift"), g("wav"), abi.PRESSURE,
+                        [g("gmap"), g("gmap_vx"), g("gmap_vz")], [g("gshift"), g("gshift_vx"), g("gshift_vz")],
+                        list(g("obs")), misfit=1)
+    for k in ("vpgrad", "vsgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        ref = g(f"corr_{k}")
+        assert np.abs(ref).max() > 0, k
+        assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
+    assert r["misfit"] == float(g("corr_misfit")) and r["misfit"] < 0
