@@ -57,6 +57,7 @@ enum { RSGPU_F32_EXACT = 0, RSGPU_F32_FAST = 1, RSGPU_F64 = 2 };
 enum { RSGPU_PRESSURE = 0, RSGPU_VX = 1, RSGPU_VY = 2, RSGPU_VZ = 3 };
 /* misfit codes: identical to rs_fwimisfit (include/utils.h:26) */
 enum { RSGPU_MISFIT_DIFFERENCE = 0, RSGPU_MISFIT_CORRELATION = 1 };
+enum { RSGPU_INTERP_LINEAR = 0, RSGPU_INTERP_BSPLINE = 1, RSGPU_INTERP_SINC = 2 };   /* rs_interpmode */
 /* checkpoint storage precision of the FWI/RTM gradient drivers */
 enum { RSGPU_CKPT_NATIVE = 0, RSGPU_CKPT_F16 = 1, RSGPU_CKPT_BF16 = 2 };
 /* revolve actions: identical to revolve_action (include/revolve.h:25) */
@@ -261,6 +262,15 @@ void rsgpu_adjoint_destroy(rsgpu_adjoint *adj);
  * Host preprocessing (restatements of the reference's host-side code; callers
  * that hold reference objects pass the reference's own arrays instead)
  * ------------------------------------------------------------------------- */
+
+/* Interp<T>::interp (lib/interp.cpp:123-186, Data2D and Data3D alike): resample
+ * ntr traces of n1 samples (origin o1, interval d1, trace-major [ntr][n1]) onto n2
+ * samples (o2, d2) with the reference's LINEAR, BSPLINE (4-tap) or SINC (6-tap)
+ * kernel; samples whose stencil leaves the input trace are zero.  Host arrays of
+ * the precision's element type.  LINEAR and BSPLINE are bit-identical to the
+ * reference; SINC evaluates sin on the GPU (equal after rounding in practice). */
+rsgpu_status rsgpu_interp_traces(int precision, int mode, int ntr, int n1, double o1, double d1, const void *in,
+                                 int n2, double o2, double d2, void *out);
 
 /* Failure-detection self test (no counterpart in the reference): launches one CTA
  * that waits on a barrier nothing completes.  The kernel's bounded wait (the same

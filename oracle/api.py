@@ -70,6 +70,7 @@ def oracle() -> C.CDLL:
             [V] * 4 + [V, V, V]
         _oracle.orc_fwi_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 7 + [I, V, V, V, I, V, V, V, I] + \
             [V] * 5 + [V]
+        _oracle.orc_interp.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
         _oracle.orc_rtm_a3d.argtypes = [C.POINTER(OrcGrid3), I, I, I] + [V] * 5 + [I, V, V, V, I, V, V, V, I, I, I, V]
         _oracle.orc_mod_a3d.argtypes = [C.POINTER(OrcGrid3)] + [V] * 5 + [I, V, V, V, I, I, V, V, I, V, I, V]
     return _oracle
@@ -99,6 +100,7 @@ def ref() -> C.CDLL:
         _ref.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
+        _ref.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
         _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
         _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
         _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
@@ -430,3 +432,18 @@ def orc_fwi_a3d(pb, padded, tab, smap, sshift, wav, gmap, gshift, obs, misfit=0)
     assert r == 0
     o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
     return o
+
+
+def ref_interp(mode, data, o1, d1, n2, o2, d2):
+    """Interp<float>::interp of trace-major data [ntr][n1] onto n2 samples."""
+    d = np.ascontiguousarray(data, np.float32)
+    out = np.zeros((d.shape[0], n2), np.float32)
+    assert ref().ref_interp_f(mode, d.shape[0], d.shape[1], o1, d1, _p(d), n2, o2, d2, _p(out)) == 1
+    return out
+
+
+def orc_interp(mode, data, o1, d1, n2, o2, d2):
+    d = np.ascontiguousarray(data, np.float32)
+    out = np.zeros((d.shape[0], n2), np.float32)
+    assert oracle().orc_interp(mode, d.shape[0], d.shape[1], o1, d1, _p(d), n2, o2, d2, _p(out)) == 0
+    return out

@@ -5,6 +5,7 @@
  */
 #include "ref_harness_common.h"
 #include "fwi.h"
+#include "interp.h"
 
 using namespace rockseis;
 using namespace refh;
@@ -287,6 +288,19 @@ int steps_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double
 } // namespace
 
 extern "C" {
+
+/* Interp<float>::interp (lib/interp.cpp:123-186) on trace-major float arrays. */
+int ref_interp_f(int mode, int ntr, int n1, float o1, float d1, const float *in, int n2, float o2, float d2,
+                 float *out)
+{
+    auto from = std::make_shared<rockseis::Data2D<float>>(ntr, n1, d1, o1);
+    auto to = std::make_shared<rockseis::Data2D<float>>(ntr, n2, d2, o2);
+    std::memcpy(from->getData(), in, sizeof(float) * (size_t)ntr * n1);
+    rockseis::Interp<float> ip((rockseis::rs_interpmode)mode);
+    ip.interp(from, to);
+    std::memcpy(out, to->getData(), sizeof(float) * (size_t)ntr * n2);
+    return 1;
+}
 
 int ref_steps_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                     const float *wav, int sfield, int nsteps, int adjoint, float *state)

@@ -1073,3 +1073,43 @@ int orc_fwi_a3d(const orc_grid3 *g, int nx, int ny, int nz, const float *vp, con
     free(Ps);
     return 0;
 }
+
+/* Interp<float>::interp (lib/interp.cpp:38-186) for trace-major float traces:
+ * mode 0 LINEAR (pad 1), 1 BSPLINE (pad 2), 2 SINC (pad 3); the C expressions
+ * keep the reference's float/double mix (double literals promote). */
+static float orc_sinc(float x)
+{
+    if (x == 0.0) return 1.0f;
+    return (float)(sin(3.14159265358979323846 * x) / (3.14159265358979323846 * x));
+}
+
+int orc_interp(int mode, int ntr, int n1, float o1, float d1, const float *in, int n2, float o2, float d2, float *out)
+{
+    const int pad = mode == 0 ? 1 : mode == 1 ? 2 : 3;
+    for (int i = 0; i < ntr; i++)
+        for (long j = 0; j < n2; j++) {
+            const float val = o2 + (float)j * d2;
+            const long i0 = (long)((val - o1) / d1) - (pad - 1);
+            float *o = out + (long)i * n2 + j;
+            if (i0 < 0 || i0 + (2 * pad) - 1 > (long)n1 - 1) { *o = 0.0f; continue; }
+            const float x0 = o1 + (float)(i0 + (pad - 1)) * d1;
+            const float d = (val - x0) / d1;
+            const float *m = in + (long)i * n1 + i0;
+            if (mode == 0) {
+                *o = (float)((1.0 - d) * m[0] + d * m[1]);
+            } else if (mode == 1) {
+                const float xp = (float)(d + 1.0), om = (float)(1.0 - d);
+                const float a0 = (float)(((-(1.0 / 6.0) * xp + 1.0) * xp - 2.0) * xp + (4.0 / 3.0));
+                const float a1 = (float)((0.5 * d - 1.0) * d * d + (2.0 / 3.0));
+                const float a2 = (float)((0.5 * om - 1.0) * om * om + (2.0 / 3.0));
+                const float a3 = (float)(1.0 - a0 - a1 - a2);
+                *o = a0 * m[0] + a1 * m[1] + a2 * m[2] + a3 * m[3];
+            } else {
+                float acc = 0.0f;
+                for (int k = 0; k < 6; k++)
+                    acc = acc + m[k] * orc_sinc((float)((2.0 - k) + d)) * orc_sinc((float)(((2.0 - k) + d) / 3.0));
+                *o = acc;
+            }
+        }
+    return 0;
+}

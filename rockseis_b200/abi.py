@@ -26,6 +26,7 @@ CKPT_NATIVE, CKPT_F16, CKPT_BF16 = 0, 1, 2
 ADVANCE, TAKESHOT, RESTORE, FIRSTURN, YOUTURN, TERMINATE, ERROR = range(7)
 ACCUM_REFERENCE, ACCUM_F64 = 0, 1
 MISFIT_DIFFERENCE, MISFIT_CORRELATION = 0, 1
+INTERP_LINEAR, INTERP_BSPLINE, INTERP_SINC = 0, 1, 2
 KIND_FWI, KIND_RTM = 0, 1
 
 
@@ -87,6 +88,7 @@ def _load() -> C.CDLL:
         "rsgpu_plan_destroy": (None, [V]),
         "rsgpu_modelling_a2d_noalloc": (I, [P(Config), P(Shot), V]),
         "rsgpu_selftest_bounded_wait": (I, []),
+        "rsgpu_interp_traces": (I, [I, I, I, I, D, D, V, I, D, D, V]),
         "rsgpu_tile_count": (I, [I]),
         "rsgpu_tile_shape": (I, [I, I, P(I), P(I), P(I), P(I)]),
         "rsgpu_pml_tables": (I, [I, D, I, V]),

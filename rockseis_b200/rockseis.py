@@ -790,3 +790,20 @@ class AdjointBatch:
             self.close()
         except Exception:
             pass
+
+
+class Interp:
+    """Interp<T> (include/interp.h, lib/interp.cpp): resample a Data2D/Data3D onto
+    another's time axis (its nt, dt, ot) on the GPU; coordinates are copied."""
+
+    def __init__(self, mode=abi.INTERP_LINEAR):
+        self.mode = int(mode)
+
+    def interp(self, frm: Data2D, to: Data2D):
+        if frm.ntrace != to.ntrace:
+            raise abi.RsgpuError(abi.ERR_ARG, "Interp::interp: Number of traces in the two datasets mismatch.")
+        to.scoords[:] = frm.scoords
+        to.gcoords[:] = frm.gcoords
+        src = np.ascontiguousarray(frm.data.astype(to.dtype))
+        check(abi.lib.rsgpu_interp_traces(to.precision, self.mode, frm.ntrace, frm.nt, float(frm.ot), float(frm.dt),
+                                          ptr(src), to.nt, float(to.ot), float(to.dt), ptr(to.data)))

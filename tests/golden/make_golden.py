@@ -216,6 +216,24 @@ def e2d_fwi_cases(g):
         g[f"e2dfwi_corr_{k}"] = np.asarray(v)
 
 
+INTERP_AXES = ((800, 0.0, 1e-3), (333, 0.0103, 2.37e-3), (120, -0.05, 7e-3))
+
+
+def interp_cases(g):
+    """Interp<float>::interp, LINEAR / BSPLINE / SINC, onto finer, irregular-ratio and
+    coarser time axes (the last one starting before the input trace)."""
+    rng = np.random.default_rng(3)
+    n1, d1 = 400, 2e-3
+    data = np.stack([synth.ricker(n1, d1, 25.0) * (k + 1) for k in range(5)]).astype(np.float32)
+    data += (rng.standard_normal((5, n1)) * 0.01).astype(np.float32)
+    g["interp_in"] = data
+    g["interp_axis_in"] = np.array([n1, 0.0, d1])
+    for mode in (0, 1, 2):
+        for a, (n2, o2, d2) in enumerate(INTERP_AXES):
+            g[f"interp_m{mode}_a{a}"] = api.ref_interp(mode, data, np.float32(0.0), np.float32(d1), n2,
+                                                       np.float32(o2), np.float32(d2))
+
+
 def a3d_cases(g):
     """Acoustic 3D shots (ModellingAcoustic3D::run) with reference-made inputs."""
     nx, ny, nz, L, nt, dx = 15, 13, 14, 4, 70, 10.0
@@ -266,6 +284,7 @@ def main():
     modelling_cases(g)
     adjoint_cases(g)
     e2d_fwi_cases(g)
+    interp_cases(g)
     a3d_cases(g)
     np.savez_compressed(OUT, **g)
     print(f"wrote {OUT}: {len(g)} arrays, {os.path.getsize(OUT)} bytes")

@@ -308,3 +308,17 @@ def test_oracle_elastic_correlation_misfit_matches_reference():
         assert np.abs(ref).max() > 0, k
         assert np.array_equal(r[k], ref), f"{k}: max abs diff {np.abs(r[k] - ref).max()}"
     assert r["misfit"] == float(g("corr_misfit")) and r["misfit"] < 0
+
+
+INTERP_AXES = ((800, 0.0, 1e-3), (333, 0.0103, 2.37e-3), (120, -0.05, 7e-3))
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_oracle_interp_matches_reference(mode):
+    n1, o1, d1 = GOLD["interp_axis_in"]
+    for a, (n2, o2, d2) in enumerate(INTERP_AXES):
+        got = api.orc_interp(mode, GOLD["interp_in"], np.float32(o1), np.float32(d1), n2, np.float32(o2),
+                             np.float32(d2))
+        ref = GOLD[f"interp_m{mode}_a{a}"]
+        assert np.abs(ref).max() > 0
+        assert np.array_equal(got, ref), (mode, a, np.abs(got - ref).max())
