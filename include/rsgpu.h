@@ -3,8 +3,7 @@
  *
  * This is the drop-in boundary beneath RockSeis's C++ drivers.  Each entry
  * point replaces the body of one reference method; the comment beside it cites
- * the reference interface (paths relative to the RockSeis source tree).  The
- * reference-side bindings a maintainer adds are shown in INTEGRATION.md.
+ * the reference interface (paths relative to the RockSeis source tree).
  *
  * Conventions
  *  - Plain pointers and sizes only.  Array layouts are the reference's:
@@ -165,13 +164,14 @@ void rsgpu_plan_destroy(rsgpu_plan *plan);
  * (wavefields, C-PML memory, staged parameters, plans) lives in one static
  * 32 MiB device array per GPU, held by every GPU that loads the library until
  * the process exits; a grid that needs more is rejected with RSGPU_ERR_ARG.
- * Float precisions only; results equal rsgpu_modelling's.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  Every call shares the array and clears
- * what must start at zero; calls are serialised by a process-wide lock and each
- * waits for its work on `stream` (a cudaStream_t, 0 = default) before returning,
- * so work from two calls must not be made to overlap on the GPU: overlapping
- * calls would race on the array. */
+ * Float precisions only; results equal rsgpu_modelling's.  Every call, the
+ * first on a device included, looks up the array's device address on the
+ * current device (cudaGetSymbolAddress, which allocates nothing), so make each
+ * call outside stream capture.  The call blocks: it waits for its work on
+ * `stream` (a cudaStream_t, 0 = default) to finish before it returns.  Every
+ * call shares the array and clears what must start at zero; calls are
+ * serialised by a process-wide lock, and work from two calls must not be made
+ * to overlap on the GPU: overlapping calls would race on the array. */
 rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, const rsgpu_shot *shot, void *stream);
 
 /* ---------------------------------------------------------------------------

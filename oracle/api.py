@@ -18,12 +18,16 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "librsoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "librsref.so")
-REFSRC = "/root/reference"
+# Root of the reference source tree, from the environment (the build recipe sets it);
+# without it only the C restatement is built.
+REFSRC_ENV = "RSGPU_REFERENCE_SRC"
 
 
 def build(ref: bool = True) -> None:
     """Build the checkers (the reference part only where its sources exist)."""
-    targets = ["oracle"] + (["ref"] if ref and os.path.isdir(REFSRC) else [])
+    refsrc = os.environ.get(REFSRC_ENV, "")
+    use_ref = ref and bool(refsrc) and os.path.isdir(refsrc)
+    targets = ["oracle"] + (["ref", f"REFSRC={refsrc}"] if use_ref else [])
     subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}"] + targets, check=True)
 
 

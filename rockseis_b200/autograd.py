@@ -86,14 +86,14 @@ class _ModelledData(torch.autograd.Function):
         traces = problem.model_traces(vp, rho)
         ctx.problem, ctx.traces = problem, traces
         ctx.save_for_backward(vp, rho)
-        return torch.from_numpy(traces).to(vp.dtype)
+        return torch.from_numpy(traces).to(device=vp.device, dtype=vp.dtype)
 
     @staticmethod
     def backward(ctx, g):
         vp, rho = ctx.saved_tensors
         gv, gr = ctx.problem.vjp(vp, rho, ctx.traces, g.detach().cpu().numpy())
-        return (torch.from_numpy(gv).to(vp.dtype).reshape(vp.shape),
-                torch.from_numpy(gr).to(rho.dtype).reshape(rho.shape), None)
+        return (torch.from_numpy(gv).to(device=vp.device, dtype=vp.dtype).reshape(vp.shape),
+                torch.from_numpy(gr).to(device=rho.device, dtype=rho.dtype).reshape(rho.shape), None)
 
 
 def modelled_data(vp: torch.Tensor, rho: torch.Tensor, problem: AcousticProblem2D) -> torch.Tensor:

@@ -33,31 +33,29 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 namespace {
 
-constexpr int kMaxDevices = 64;
 std::mutex g_lock;                        // one call at a time in this process
-unsigned char *g_scratch_dev[kMaxDevices] = {};
 
-// Device address of the scratch array for the current device.  In host code
-// g_noalloc_scratch names a host-side stand-in, so the address must come from
-// cudaGetSymbolAddress, once per device, with that device current.
+// Device address of the scratch array on the current device.  In host code
+// g_noalloc_scratch names a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress with the device current.  It is looked up on every call
+// (the lookup allocates nothing): a cached address would go stale when the
+// device's context is torn down and the module reloaded (cudaDeviceReset).
 rsgpu_status scratch_address(unsigned char **out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
         set_error("no usable CUDA device for the no-allocation entry point");
         return RSGPU_ERR_NODEVICE;
     }
-    if (!g_scratch_dev[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            set_error("cudaGetSymbolAddress of the scratch array failed: %s", cudaGetErrorString(e));
-            return RSGPU_ERR_CUDA;
-        }
-        g_scratch_dev[dev] = static_cast<unsigned char *>(p);
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        set_error("cudaGetSymbolAddress of the scratch array failed: %s", cudaGetErrorString(e));
+        return RSGPU_ERR_CUDA;
     }
-    *out = g_scratch_dev[dev];
+    *out = static_cast<unsigned char *>(p);
     return RSGPU_OK;
 }
 
@@ -247,14 +245,21 @@ extern "C" rsgpu_status rsgpu_modelling_a2d_noalloc(const rsgpu_config *cfg, con
     a.pml = (const float *)(S + o_pml);
     a.lpml = lp;
     int *derr = (int *)(S + o_err);
+    // The error word is read back every CHECK_EVERY steps, so a call whose bounded
+    // waits give up stops after at most that many more steps instead of queueing
+    // all nt of them (each could wait out its own limit again).
+    constexpr int CHECK_EVERY = 256;
+    int err = 0;
     for (int it = 0; it < nt; it++) {
         for (int half = 0; half < 2; half++)
             NA_CU(launch_step_2d(prec, cfgi, PHYS_A2D, half, 0, &a, S + o_coef, S + o_maps, derr, a.ntiles, st));
         NA_CU(launch_injrec_2d(prec, S + o_shot, S + o_ir, 1, cfg->dt, it, nullptr, st));
+        if ((it + 1) % CHECK_EVERY == 0 || it + 1 == nt) {
+            NA_CU(cudaMemcpyAsync(&err, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+            NA_CU(cudaStreamSynchronize(st));
+            if (err) break;
+        }
     }
-    NA_CU(cudaStreamSynchronize(st));
-    int err = 0;
-    NA_CU(cudaMemcpy(&err, derr, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) { set_error("a device-side wait exceeded its time limit (code %d)", err); return (rsgpu_status)err; }
     return RSGPU_OK;
 }
