@@ -78,9 +78,13 @@ typedef struct {
                            A,B,C rbb; A,B,C rbb_stag (include/pml.h:31-81).  NULL: computed
                            by rsgpu_pml_tables with Smax = 1200. */
     int tile;           /* 2D kernel tile shape index (rsgpu_tile_shape), -1 = built-in default */
-    int zchunk;         /* 3D: planes marched by one CTA (0 = 64) */
-    int launch_mode;    /* 2D elastic forward: 0 = one CTA per tile (the faster on B200),
-                           1 = persistent CTAs with double-buffered tile stages */
+    int zchunk;         /* 3D: planes marched by one CTA (0 = 64); 2D fused step: rows per
+                           work item (rounded up to 8; 0 = chosen from the batch size) */
+    int launch_mode;    /* 2D propagation: 0 = library choice (the fused step for forward
+                           propagation), 1 = persistent per-tile kernels (elastic forward),
+                           2 = per-tile velocity and stress kernels, 3 = fused z-marching step:
+                           velocity, stress and injection of a time step plus recording of
+                           the previous one in one launch */
     int reserved[5];
 } rsgpu_config;
 
@@ -148,6 +152,12 @@ long long rsgpu_plan_launch_count(rsgpu_plan *plan);
  * chunk; kernel_times returns their mean durations (ms) from the last replay. */
 rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *plan);
 rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *plan, float *ms_velocity, float *ms_stress);
+/* How a 2D plan propagates (no counterpart in the reference): the launch mode in
+ * use (3 = fused z-marching step, whose one launch per step rsgpu_plan_kernel_times
+ * reports as ms_velocity with ms_stress 0; 2 = per-tile velocity and stress
+ * kernels; 1 = persistent per-tile kernels), the fused step's work items and
+ * their height in rows (0 when not fused). */
+rsgpu_status rsgpu_plan_info(rsgpu_plan *plan, int *launch_mode, int *work_items, int *band_rows);
 /* Copy one wavefield (reference field code, SXX=4.. for elastic) of one shot to the host
  * in the reference's padded layout (for step-level parity tests). */
 rsgpu_status rsgpu_plan_read_field(rsgpu_plan *plan, int shot, int field, void *host_out);

@@ -137,6 +137,8 @@ bool encode_field_map_host(void *map, void *base, int prec, int pitch, int rows,
 Plan::~Plan()
 {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (zm_graph) cudaGraphExecDestroy(zm_graph);
+    if (d_zm) cudaFree(d_zm);
     for (auto &row : tev)
         for (auto &e : row)
             if (e) cudaEventDestroy(e);
@@ -244,6 +246,11 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     if (prec == PREC_F64 && tilecfg != TILECFG_64x32 && tilecfg != TILECFG_32x16) tilecfg = TILECFG_64x32;
     const TileShape ts = tile_shape_2d(tilecfg);
     const int lp = cfg.lpml;
+    // The fused z-marching step serves forward propagation (the forward operator;
+    // the acoustic adjoint is the forward operator run in reversed time).  The
+    // elastic adjoint steps and launch modes 1 and 2 use the per-tile kernels.
+    fused = (c->launch_mode == 0 || c->launch_mode == 3) && !adjoint_steps;
+    const int ztx = zm_strip_width();
 
     // ---- per-shot layout (byte offsets into the arena)
     shots.resize(ns);
@@ -254,7 +261,9 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
         const ShotSets &t = sets[i];
         L.nx = s[i].nx; L.nz = s[i].nz;
         L.nxp = s[i].nx + 2 * lp; L.nzp = s[i].nz + 2 * lp;
-        L.pitch = (int)rup(GUARD + rup(L.nxp, 128) + GUARD, 32);
+        // the fused step reads velocity columns up to 8 past its last strip
+        const size_t wide = fused ? std::max(rup(L.nxp, 128), rup(L.nxp, ztx) + 8) : rup(L.nxp, 128);
+        L.pitch = (int)rup(GUARD + wide + GUARD, 32);
         L.rows = GUARD + (int)rup(L.nzp, 64) + GUARD;
         const size_t fbytes = (size_t)L.pitch * L.rows * es;
         // state block first (zeroed by reset): wavefields, C-PML memory, traces
@@ -269,6 +278,13 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
             L.tracesk[k] = take((size_t)t.rec[k].n * cfg.nt * es);
         }
         if (t.nrec == 0) L.tracesk[0] = take(0);
+        if (fused) {
+            for (int k = 0; k < nfields(phys); k++) L.fb[k] = take(fbytes);
+            for (int k = 0; k < (phys == PHYS_E2D ? 2 : 1); k++) {
+                L.psixb[k] = take((size_t)L.nzp * 2 * lp * es);
+                L.psizb[k] = take((size_t)2 * lp * L.nxp * es);
+            }
+        }
         L.nrec = t.nrec > 0 ? t.rec[0].n : 0;
         L.traces = L.tracesk[0];
         L.field_begin = L.f[0];
@@ -484,6 +500,11 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
     d_maps = (char *)d_meta + m_maps;
+    if (fused) {
+        std::vector<std::vector<int>> inj_pts(inj.size());
+        for (size_t j = 0; j < inj.size(); j++) inj_pts[j] = inj[j].pt;
+        if ((st = setup_fused(inj_pts)) != RSGPU_OK) return st;
+    }
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -509,6 +530,13 @@ void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L,
     for (int k = 0; k < nfields(phys); k++) d.f[k] = (T *)(A + L.f[k] + org);
     for (int k = 0; k < nparams(phys); k++) d.m[k] = (const T *)(A + L.m[k] + org);
     for (int k = 0; k < npsi(phys); k++) { d.psix[k] = (T *)(A + L.psix[k]); d.psiz[k] = (T *)(A + L.psiz[k]); }
+    if (fused) {
+        for (int k = 0; k < nfields(phys); k++) d.fb[k] = (T *)(A + L.fb[k] + org);
+        for (int k = 0; k < (phys == PHYS_E2D ? 2 : 1); k++) {
+            d.psixb[k] = (T *)(A + L.psixb[k]);
+            d.psizb[k] = (T *)(A + L.psizb[k]);
+        }
+    }
     std::memcpy(sd, &d, sizeof d);
     InjRec<T> r{};
     r.nt = cfg.nt;
@@ -596,6 +624,7 @@ fail:
 rsgpu_status Plan::run(int it0, int nsteps)
 {
     if (it0 < 0 || nsteps < 0 || it0 + nsteps > cfg.nt) { set_error("step range [%d,%d) outside [0,%d)", it0, it0 + nsteps, cfg.nt); return RSGPU_ERR_ARG; }
+    if (fused && nsteps >= 2) return run_fused(it0, nsteps);
     int done = 0;
     const int G = graph_steps;
     if (use_graph && nsteps >= G) {
@@ -668,11 +697,25 @@ rsgpu_status Plan::enable_timing()
         for (auto &e : row) CU(cudaEventCreate(&e));
     time_kernels = true;
     if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+    if (zm_graph) { cudaGraphExecDestroy(zm_graph); zm_graph = nullptr; }
     return RSGPU_OK;
 }
 
 rsgpu_status Plan::kernel_times(float *ms_vel, float *ms_str)
 {
+    if (fused && zm_graph && time_kernels) {
+        // one fused launch per step: its duration, and no separate stress launch
+        CU(cudaStreamSynchronize(stream));
+        float v = 0;
+        for (int s = 0; s < NTIMED; s++) {
+            float a;
+            CU(cudaEventElapsedTime(&a, tev[s][0], tev[s][1]));
+            v += a;
+        }
+        *ms_vel = v / NTIMED;
+        *ms_str = 0;
+        return RSGPU_OK;
+    }
     if (!time_kernels || !graph_exec) { set_error("kernel timing needs enable_timing() and one graph replay"); return RSGPU_ERR_STATE; }
     CU(cudaStreamSynchronize(stream));
     float v = 0, w = 0;
@@ -800,6 +843,16 @@ rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *p, float *ms_velocity, float *m
     if (!p || !ms_velocity || !ms_stress) { set_error("null argument"); return RSGPU_ERR_ARG; }
     if (p->p3) { set_error("kernel timing is recorded by 2D plans only"); return RSGPU_ERR_UNSUPPORTED; }
     return p->p->kernel_times(ms_velocity, ms_stress);
+}
+rsgpu_status rsgpu_plan_info(rsgpu_plan *p, int *launch_mode, int *work_items, int *band_rows)
+{
+    if (!p || !launch_mode || !work_items || !band_rows) { set_error("null argument"); return RSGPU_ERR_ARG; }
+    if (p->p3) { set_error("3D plans have no 2D launch mode"); return RSGPU_ERR_UNSUPPORTED; }
+    const Plan &q = *p->p;
+    *launch_mode = q.fused ? 3 : (q.cfg.launch_mode == 1 ? 1 : 2);
+    *work_items = q.fused ? q.zm_nitems : 0;
+    *band_rows = q.fused ? q.zm_band : 0;
+    return RSGPU_OK;
 }
 long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? (p->p3 ? p->p3->launches : p->p->launches) : 0; }
 void rsgpu_plan_destroy(rsgpu_plan *p) { delete p; }

@@ -42,6 +42,12 @@ struct Shot2D {
     const T *m[5];
     T *psix[4];
     T *psiz[4];
+    // Second copy of the wavefields and of the velocity C-PML memory (psix/psiz 0
+    // and 1) for the fused z-marching step kernel, which reads one copy and writes
+    // the other (null when the plan does not use it).
+    T *fb[5];
+    T *psixb[2];
+    T *psizb[2];
 };
 
 // One CTA work item: shot index, tile origin and flags.
@@ -125,6 +131,32 @@ struct Step2DArgs {
     T dt, dx, dz;
     T rdx, rdz;        // RN(1/dx), RN(1/dz): reciprocal-division mode only
     const T *pml;      // 12*lpml C-PML tables
+    int lpml;
+};
+
+// ---- fused z-marching 2D step (fd2d_fused.cuh)
+// One work item: rows [z0, z1) (multiples of 8) of the strip [x0, x0+TX) of a shot,
+// and its injection entries per trace set, ie[s]..ie[s+1] in the item entry list.
+struct ZmItem {
+    int shot, x0, z0, z1, flags;
+    int ie[MAXSETS + 1];
+};
+enum { ZM_XEDGE = 1, ZM_ZEDGE = 2, ZM_XPML = 4, ZM_ZPML = 8 };
+
+template <typename T>
+struct Zm2DArgs {
+    const Shot2D<T> *shots;
+    const InjRec<T> *plans;       // per shot (injection and recording sets)
+    const ZmItem *items;
+    int nitems;
+    const int *inj;               // item injection entries: (set << 24) | CSR index
+    const int4 *recs;             // every receiver trace of the batch: (shot, set, trace, 0)
+    int nrecs;
+    const void *maps;             // CUtensorMap [shot][copy][ring field]
+    int order;
+    T dt, dx, dz;
+    T rdx, rdz;
+    const T *pml;                 // 12*lpml C-PML tables
     int lpml;
 };
 

@@ -34,6 +34,19 @@ cudaError_t launch_injrec_2d(int prec, const void *shots, const void *plans, int
 cudaError_t launch_advance(int *it_dev, int by, cudaStream_t st);
 cudaError_t launch_set_counter(int *it_dev, int value, cudaStream_t st);
 cudaError_t launch_wait_for_nothing(int *err, cudaStream_t st);
+// Fused z-marching 2D step (fd2d_fused.cuh): velocity, stress and injection of one
+// time step plus the recording of the previous one, in one launch over all shots.
+// args: Zm2DArgs<T>; ctl: device control words (step counter, error word, gate,
+// first step of the run, two work counters); cur: the wavefield copy read.
+int zm_strip_width();
+size_t zm_args_bytes(int prec);
+cudaError_t launch_zm_step_2d(int prec, int physics, const void *args, const void *coefs, int *ctl, int cur,
+                              int it_base, int use_dev_it, int nitems, cudaStream_t st);
+cudaError_t launch_zm_record_2d(int prec, const void *args, const int *ctl, int cur, int step, cudaStream_t st);
+// ctl[0] = ctl[3] = it0: the step counter of graph replays and the first step of a run
+cudaError_t launch_zm_set_run(int *ctl, int it0, cudaStream_t st);
+// CTAs of the fused step resident on the current device at once
+int zm_resident_ctas(int prec, int physics);
 size_t coefset_bytes(int prec);
 int coef_row_stride();
 

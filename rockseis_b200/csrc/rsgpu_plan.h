@@ -43,6 +43,7 @@ struct ShotLayout {
     int nrecs[MAXSETS] = {}, nsrcs[MAXSETS] = {};
     size_t tracesk[MAXSETS] = {}, wavk[MAXSETS] = {};
     size_t f[9] = {}, m[8] = {}, psix[4] = {}, psiz[4] = {};
+    size_t fb[5] = {}, psixb[2] = {}, psizb[2] = {};   // second copy (fused z-marching step)
     size_t traces = 0, wav = 0;
     size_t psi_end = 0;       // end of the wavefields + C-PML memory (a checkpoint's extent)
     size_t field_begin = 0;   // first byte of the zero-initialised state block
@@ -59,6 +60,9 @@ public:
     rsgpu_status read_traces(int shot, void *host_out, int set = 0);
     rsgpu_status read_field(int shot, int field, void *host_out);
     rsgpu_status launch_step(int it_base, const int *it_dev, bool adj, cudaEvent_t *ev = nullptr);
+    // fused z-marching step (one launch per time step, recording of the previous
+    // step included); cur = the wavefield copy it reads
+    rsgpu_status launch_fused(int it_base, bool dev_it, int cur, cudaEvent_t *ev = nullptr);
     rsgpu_status enable_timing();
     rsgpu_status kernel_times(float *ms_vel, float *ms_str);
     rsgpu_status check_device_error();
@@ -96,7 +100,18 @@ public:
     bool time_kernels = false;
     cudaEvent_t tev[NTIMED][3] = {};
 
+    // fused z-marching step (fd2d_fused.cuh): chosen at create() for 2D forward
+    // propagation unless launch_mode asks for the per-tile kernels
+    bool fused = false;
+    int zm_nitems = 0, zm_band = 0;
+    std::vector<unsigned char> zm_args;   // Zm2DArgs<T> with device pointers into d_zm
+    void *d_zm = nullptr;                 // items, injection entries, receiver list, tensor maps
+    cudaGraphExec_t zm_graph = nullptr;
+
 private:
+    rsgpu_status run_fused(int it0, int nsteps);
+    // builds the fused step's tables; inj_pts[shot*MAXSETS + set] = the set's CSR target offsets
+    rsgpu_status setup_fused(const std::vector<std::vector<int>> &inj_pts);
     rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s, bool sets_given);
     int default_tile() const;
     template <typename T>

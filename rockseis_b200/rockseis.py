@@ -424,11 +424,13 @@ class ModellingAcoustic3D(_Modelling):
     physics_name = "ModellingAcoustic3D"
 
 
-def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
+def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1, launch_mode=0, zchunk=0):
     """Many shots, each with its own model window, advanced together in one plan
-    (the batched form of Modelling*::run).  Traces accumulate into receivers[i].data."""
+    (the batched form of Modelling*::run).  Traces accumulate into receivers[i].data.
+    launch_mode / zchunk: rsgpu_config's (0 = the library's choice)."""
     tile = _tile(tile, models, sources, receivers, order, precision)
     cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
+    cfg.launch_mode, cfg.zchunk = int(launch_mode), int(zchunk)
     keep: list = []
     shots = (abi.Shot * len(models))(*[make_shot(m, s, r, keep) for m, s, r in zip(models, sources, receivers)])
     check(abi.lib.rsgpu_modelling(C.byref(cfg), len(models), shots))
@@ -438,9 +440,10 @@ def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, 
 class Plan:
     """Device-resident batch (rsgpu_plan): upload once, run steps, read traces."""
 
-    def __init__(self, models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1):
+    def __init__(self, models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1, launch_mode=0, zchunk=0):
         tile = _tile(tile, models, sources, receivers, order, precision)
         self.cfg = make_config(models[0], order, sources[0].nt, sources[0].dt, precision, tile)
+        self.cfg.launch_mode, self.cfg.zchunk = int(launch_mode), int(zchunk)
         self._keep: list = []
         self.n = len(models)
         self.receivers = receivers
@@ -461,6 +464,12 @@ class Plan:
         v, s_ = C.c_float(), C.c_float()
         check(abi.lib.rsgpu_plan_kernel_times(self.h, C.byref(v), C.byref(s_)))
         return v.value, s_.value
+
+    def info(self):
+        """(launch mode in use, fused work items, rows per work item)."""
+        m, n, b = C.c_int(), C.c_int(), C.c_int()
+        check(abi.lib.rsgpu_plan_info(self.h, C.byref(m), C.byref(n), C.byref(b)))
+        return m.value, n.value, b.value
 
     def read_traces(self, i, out=None):
         r = self.receivers[i]
