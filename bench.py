@@ -40,17 +40,17 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-NX, NZ, DX, LPML, ORDER, DT, NT, NSHOTS, NREC = 801, 401, 5.0, 30, 8, 5e-4, 4000, 16, 400
-CPU_SAMPLE_STEPS = 100
+from rockseis_b200 import workloads as W  # noqa: E402
+
+NX, NZ, DX, LPML, ORDER, DT, NT, NSHOTS, NREC = (W.C2[k] for k in ("nx", "nz", "dx", "lpml", "order", "dt", "nt",
+                                                                    "nshots", "nrec"))
+CPU_SAMPLE_STEPS = 100          # the reference arm: time steps of one bench step
+CPU_BASELINE_STEPS = 400        # the cpu_baseline object of our own line (10 % of nt)
 
 
-def workload_inputs(seed_model=2, seed_shots=3):
-    from rockseis_b200 import synth
-    vp, vs, rho = synth.elastic_model(NX, NZ, DX, seed=seed_model)
-    sx = np.sort(np.random.default_rng(seed_shots).uniform(200.0, (NX - 1) * DX - 200.0, NSHOTS))
-    wav = synth.ricker(NT, DT, 15.0)
-    gc = synth.surface_line(NREC, 0.0, 10.0, 0.0)
-    return vp, vs, rho, sx, wav, gc
+def workload_inputs():
+    """The elastic 2D workload (rockseis_b200.workloads.elastic2d_c2)."""
+    return W.elastic2d_c2()
 
 
 def config_dict(ngpus, precision_name, nt=NT):
@@ -145,17 +145,78 @@ def cpu_reference(nsteps=CPU_SAMPLE_STEPS, procs=None):
             "max_process_s": round(max(times), 3), "wall_s": round(wall, 3)}
 
 
+def c1_config(ngpus, precision_name):
+    c = W.C1
+    return {"workload": "acoustic2d_forward_1shot_501x301_nt2000", "nx": c["nx"], "nz": c["nz"], "dx": c["dx"],
+            "lpml": c["lpml"], "order": c["order"], "nt": c["nt"], "dt": c["dt"], "shots_per_gpu": 1,
+            "receivers": c["nrec"], "padded_points_per_shot": (c["nx"] + 2 * c["lpml"]) * (c["nz"] + 2 * c["lpml"]),
+            "arithmetic": precision_name, "vp_clip": c["vclip"],
+            "l2": "working set 6.6 MB: L2-resident; timed steps repeat the same shot without a flush",
+            "parallelism": f"shots x{ngpus}"}
+
+
+def _c1_ref_sample(nsteps):
+    sys.path.insert(0, ROOT)
+    from oracle import api
+    c = W.C1
+    vp, rho, src, wav, rec = W.acoustic2d_c1(nsteps)
+    pb = api.Problem2D(c["nx"], c["nz"], c["dx"], c["dx"], c["lpml"], c["order"], 0, c["dt"], nsteps, vp, rho)
+    t0 = time.perf_counter()
+    api.ref_modelling_a2d(pb, src, wav, 0, rec, 0)
+    return time.perf_counter() - t0
+
+
+def cpu_c1_reference(nsteps=500):
+    """The reference's ModellingAcoustic2D::run on the one shot (one process: the
+    reference parallelises only over shots), first nsteps of 2000."""
+    import multiprocessing as mp
+    from oracle import api
+    if not api.ref_available():
+        return None
+    with mp.get_context("spawn").Pool(1) as pool:
+        t = pool.map(_c1_ref_sample, [nsteps])[0]
+    c = W.C1
+    pts = (c["nx"] + 2 * c["lpml"]) * (c["nz"] + 2 * c["lpml"]) * nsteps
+    return {"value": round(pts / t / 1e9, 5), "unit": "Gpts/s", "cores": 1, "kind": "reference",
+            "sample": f"1 process (one shot) x first {nsteps} of {c['nt']} steps, full 541x341 padded grid",
+            "process_s": round(t, 3)}
+
+
 # ---------------------------------------------------------------- GPU arm
-def build_batch(precision, vp, vs, rho, sx, wav, gc, nt=NT, pinned=False):
+def _pin(models, srcs, recs):
+    """Move the batch's host arrays into pinned memory (the end-to-end measurement)."""
+    import torch
+    for m in models:
+        pinned_pads = []
+        for a in m.padded():
+            t = torch.empty(a.shape, dtype=torch.float32).pin_memory()
+            t.numpy()[:] = a
+            pinned_pads.append(t)
+        m._pinned = pinned_pads
+        m._padded = dict(zip(m.names, [t.numpy() for t in pinned_pads]))
+    for r in recs:
+        t = torch.zeros(r.data.shape, dtype=torch.float32).pin_memory()
+        r._pinned = t
+        r.data = t.numpy()
+    for s_ in srcs:
+        t = torch.empty(s_.data.shape, dtype=torch.float32).pin_memory()
+        t.numpy()[:] = s_.data
+        s_._pinned = t
+        s_.data = t.numpy()
+
+
+def build_batch(precision, vp, vs, rho, sx, wav, gc, nt=NT, pinned=False, shots=None):
+    """The elastic 2D batch: one model window per shot (the whole model), explosive
+    source at z = 10 m, Vx receivers at the surface."""
     from rockseis_b200 import abi
     from rockseis_b200.rockseis import Data2D, ModelElastic2D
     models, srcs, recs = [], [], []
-    for i in range(NSHOTS):
+    for i in (range(NSHOTS) if shots is None else shots):
         m = ModelElastic2D(NX, NZ, LPML, DX, DX, 0.0, 0.0, 0, precision)
         m.createModel()
         m.Vp[:], m.Vs[:], m.R[:] = vp, vs, rho
         s = Data2D(1, nt, DT, 0.0, precision)
-        s.scoords[:] = [[sx[i], 10.0]]
+        s.scoords[:] = [[sx[i], W.C2["sz"]]]
         s.data[:] = wav[None, :nt]
         s.setField(abi.PRESSURE)
         s.makeMap(m, 0)
@@ -167,46 +228,58 @@ def build_batch(precision, vp, vs, rho, sx, wav, gc, nt=NT, pinned=False):
         srcs.append(s)
         recs.append(r)
     if pinned:
-        import torch
-        for m in models:
-            pads = m.padded()
-            pinned_pads = []
-            for a in pads:
-                t = torch.empty(a.shape, dtype=torch.float32).pin_memory()
-                t.numpy()[:] = a
-                pinned_pads.append(t)
-            m._pinned = pinned_pads
-            m._padded = dict(zip(m.names, [t.numpy() for t in pinned_pads]))
-        for r in recs:
-            t = torch.zeros(r.data.shape, dtype=torch.float32).pin_memory()
-            r._pinned = t
-            r.data = t.numpy()
-        for s in srcs:
-            t = torch.empty(s.data.shape, dtype=torch.float32).pin_memory()
-            t.numpy()[:] = s.data
-            s._pinned = t
-            s.data = t.numpy()
+        _pin(models, srcs, recs)
     return models, srcs, recs
 
 
-def algorithmic_bytes(models):
-    """Algorithmic bytes of one velocity / stress launch over the batch (fp32).
+def build_c1(precision, nt=None, pinned=False):
+    """The acoustic 2D shot of rockseis_b200.workloads.acoustic2d_c1."""
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import Data2D, ModelAcoustic2D
+    c = W.C1
+    nt = nt or c["nt"]
+    vp, rho, src, wav, rec = W.acoustic2d_c1(nt)
+    m = ModelAcoustic2D(c["nx"], c["nz"], c["lpml"], c["dx"], c["dx"], 0.0, 0.0, 0, precision)
+    m.createModel()
+    m.Vp[:], m.R[:] = vp, rho
+    s = Data2D(1, nt, c["dt"], 0.0, precision)
+    s.scoords[:] = src
+    s.data[:] = wav
+    s.setField(abi.PRESSURE)
+    s.makeMap(m, 0)
+    r = Data2D(len(rec), nt, c["dt"], 0.0, precision)
+    r.gcoords[:] = rec
+    r.setField(abi.PRESSURE)
+    r.makeMap(m, 1)
+    models, srcs, recs = [m], [s], [r]
+    if pinned:
+        _pin(models, srcs, recs)
+    return models, srcs, recs
 
-    velocity: read Sxx,Szz,Sxz,Vx,Vz,Rx,Rz; write Vx,Vz  -> 36 B per padded point
-    stress:   read Vx,Vz,Sxx,Szz,Sxz,L,L2M,M; write Sxx,Szz,Sxz -> 44 B per point
-    plus the C-PML memory variables: 2 per strip point per launch, read+write (16 B).
-    """
+
+def algorithmic_bytes(models, physics="elastic2d"):
+    """Algorithmic bytes per launch over the batch (fp32) and the padded points.
+
+    elastic, fused step: read Vx,Vz,Sxx,Szz,Sxz,Rx,Rz,L,L2M,M; write the 5 fields
+      -> 60 B per padded point, plus 8 C-PML memory arrays (4 in the x strips, 4 in
+      the z strips), each read and written once: 32 B per strip point;
+    elastic, per-tile half-steps: velocity 36 B, stress 44 B, 16 B per strip point each;
+    acoustic, fused: read P,Vx,Vz,Rx,Rz,L, write P,Vx,Vz -> 36 B + 16 B per strip point;
+    acoustic, per-tile: velocity 28 B, stress 20 B, 8 B per strip point each.
+    Returns (fused, velocity, stress, points)."""
     pts = strip = 0
     for m in models:
         nxp, nzp, L = m.getNx_pml(), m.getNz_pml(), m.lpml
         pts += nxp * nzp
         strip += 2 * L * nzp + 2 * L * nxp
-    return 36 * pts + 16 * strip, 44 * pts + 16 * strip, pts
+    if physics == "elastic2d":
+        return 60 * pts + 32 * strip, 36 * pts + 16 * strip, 44 * pts + 16 * strip, pts
+    return 36 * pts + 16 * strip, 28 * pts + 8 * strip, 20 * pts + 8 * strip, pts
 
 
-def read_traffic(kernel):
+def read_traffic(kernel, workload="elastic2d_16shots"):
     """ncu DRAM bytes per launch recorded in profiles/ for the workload, if any."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_elastic2d_16shots.txt")
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.txt")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -224,21 +297,63 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def run_gpu(args, rank, world, device):
+def _shot0_traces(precision, physics, nt):
+    """Shot 0 of the workload alone, modelled in `precision` (parity figures)."""
+    from rockseis_b200.rockseis import modelling_batch
+    if physics == "elastic2d":
+        vp, vs, rho, sx, wav, gc = workload_inputs()
+        models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt, shots=[0])
+    else:
+        models, srcs, recs = build_c1(precision, nt)
+    modelling_batch(models, srcs, recs, ORDER, precision)
+    return recs[0].data.copy()
+
+
+def parity_figures(fast0, physics, nt):
+    """Errors of the timed FMA result (shot 0), computed outside the timed region:
+    against the EXACT GPU run, whose digest is compared with the reference's own
+    output at full length (tests/golden/fullsize.json), and against the FP64 GPU
+    propagator, beside the reference float's own error against FP64."""
+    from rockseis_b200 import abi
+    exact = _shot0_traces(abi.F32_EXACT, physics, nt)
+    f64 = _shot0_traces(abi.F64, physics, nt)
+    key = "c2_traces" if physics == "elastic2d" else "c1_traces"
+    equal = None
+    full_nt = NT if physics == "elastic2d" else W.C1["nt"]
+    if nt == full_nt:
+        gold = json.load(open(os.path.join(ROOT, "tests", "golden", "fullsize.json")))[key]
+        equal = W.digest(exact) == gold["sha256"]
+    return {"shot": 0, "exact_equals_reference": equal,
+            "rel_l2_vs_reference": float("%.3g" % rel_l2(fast0, exact)),
+            "rel_l2_vs_fp64_gpu": float("%.3g" % rel_l2(fast0, f64)),
+            "reference_float_rel_l2_vs_fp64_gpu": float("%.3g" % rel_l2(exact, f64)),
+            "how": "FMA traces of the timed run vs the EXACT GPU run (bit-identical to the reference "
+                   "when exact_equals_reference) and vs the FP64 GPU propagator"}
+
+
+def run_gpu(args, rank, world, device, physics="elastic2d"):
     import ctypes as C
     import torch
     from rockseis_b200 import abi
     from rockseis_b200.rockseis import Plan, make_config, make_shot
     precision = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
-    vp, vs, rho, sx, wav, gc = workload_inputs()
-    nt = args.nt
-    models, srcs, recs = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt)
+    nt = args.nt if physics == "elastic2d" else min(args.nt, W.C1["nt"])
+    if physics == "elastic2d":
+        vp, vs, rho, sx, wav, gc = workload_inputs()
+        build = lambda pinned: build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt, pinned=pinned)  # noqa: E731
+    else:
+        build = lambda pinned: build_c1(precision, nt, pinned=pinned)  # noqa: E731
+    models, srcs, recs = build(False)
     torch.cuda.set_device(device)
-    from rockseis_b200.autotune import tile_shapes, tune_tile
-    # tile shape: the autotuner's pick (cached in JSON), measured before the timed region
-    tile = tune_tile(models, srcs, recs, ORDER, precision) if args.tile == -2 else args.tile
-    tile_desc = list(tile_shapes(precision).get(tile, ())) if tile >= 0 else "library default"
-    plan = Plan(models, srcs, recs, ORDER, precision, tile)
+    plan = Plan(models, srcs, recs, ORDER, precision, args.tile if args.tile >= -1 else -1,
+                launch_mode=args.launch_mode, zchunk=args.zchunk)
+    mode, items, band = plan.info()
+    if mode != 3:
+        # per-tile kernels: the tile shape is the autotuner's pick (cached in JSON), measured before timing
+        plan.close()
+        from rockseis_b200.autotune import tune_tile
+        tile = tune_tile(models, srcs, recs, ORDER, precision) if args.tile == -2 else args.tile
+        plan = Plan(models, srcs, recs, ORDER, precision, tile, launch_mode=args.launch_mode)
     plan.enable_timing()
     st = torch.cuda.ExternalStream(plan.stream())
     pts_per_step = sum(m.getNx_pml() * m.getNz_pml() for m in models) * nt
@@ -263,54 +378,65 @@ def run_gpu(args, rank, world, device):
     ms_total = e0.elapsed_time(e1)
     plan.sync()
     launches = plan.launch_count() - l0
-    ms_vel, ms_str = plan.kernel_times()
+    ms_a, ms_b = plan.kernel_times()
+    fast0 = plan.read_traces(0)
+    plan.close()
     torch.cuda.synchronize()
     dist_barrier(world)
     ms_max = dist_max(ms_total, world)
     ms_step = ms_max / args.steps
     value = pts_per_step * world / (ms_step / 1e3) / 1e9
 
-    # roofline of the dominant half-step kernel
-    b_vel, b_str, _ = algorithmic_bytes(models)
+    # roofline of the dominant kernel (CUDA events recorded inside the replayed graph)
+    b_fused, b_vel, b_str, pts = algorithmic_bytes(models, physics)
     peak, peak_kind = measured_peak()
-    dom, ms_dom, b_dom = ("e2d_stress", ms_str, b_str) if ms_str >= ms_vel else ("e2d_velocity", ms_vel, b_vel)
+    tag = "elastic2d_16shots" if physics == "elastic2d" else "acoustic2d_1shot"
+    if mode == 3:
+        dom, ms_dom, b_dom = "zm_step_2d", ms_a, b_fused
+        extra = {"launch": "fused z-marching step (velocity + stress + injection + recording of the previous "
+                           "step)", "work_items": items, "rows_per_item": band}
+    else:
+        dom, ms_dom, b_dom = (("e2d_stress" if physics == "elastic2d" else "a2d_stress"), ms_b, b_str) \
+            if ms_b >= ms_a else (("e2d_velocity" if physics == "elastic2d" else "a2d_velocity"), ms_a, b_vel)
+        extra = {"launch": "per-tile velocity and stress kernels", "ms_velocity": round(ms_a, 5),
+                 "ms_stress": round(ms_b, 5)}
     achieved = b_dom / (ms_dom / 1e3) / 1e9
-    traffic = read_traffic(dom)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
+                "frac": round(achieved / peak, 4), "traffic": read_traffic(dom, tag), "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": b_dom, "ms_per_launch": round(ms_dom, 5),
-                "ms_velocity": round(ms_vel, 5), "ms_stress": round(ms_str, 5),
-                "step_bytes_fraction": round(((b_vel + b_str) * nt / (ms_step / 1e3) / 1e9) / peak, 4)}
-    plan.close()
+                "bytes_per_point_step": 60 if physics == "elastic2d" else 36,
+                "step_frac_of_peak": round((b_fused * nt / (ms_step / 1e3) / 1e9) / peak, 4), **extra}
+    parity = parity_figures(fast0, physics, nt) if (rank == 0 and args.precision == "fast") else None
     if args.no_e2e:
         return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=None,
-                    clocks=clk.summary(), tile=tile_desc)
+                    clocks=clk.summary(), parity=parity, mode=mode)
 
     # end to end through the C ABI from pinned host buffers
-    models_p, srcs_p, recs_p = build_batch(precision, vp, vs, rho, sx, wav, gc, nt=nt, pinned=True)
-    cfg = make_config(models_p[0], ORDER, nt, DT, precision, tile)
+    models_p, srcs_p, recs_p = build(True)
+    cfg = make_config(models_p[0], ORDER, nt, srcs_p[0].dt, precision, -1)
+    cfg.launch_mode, cfg.zchunk = int(args.launch_mode), int(args.zchunk)
     keep: list = []
-    shots = (abi.Shot * NSHOTS)(*[make_shot(m, s, r, keep) for m, s, r in zip(models_p, srcs_p, recs_p)])
+    ns = len(models_p)
+    shots = (abi.Shot * ns)(*[make_shot(m, s, r, keep) for m, s, r in zip(models_p, srcs_p, recs_p)])
     h2d = sum(sum(a.nbytes for a in m.padded()) for m in models_p) + sum(s.data.nbytes + s.smap.nbytes +
                                                                         s.sshift.nbytes for s in srcs_p)
     h2d += sum(r.gmap.nbytes + r.gshift.nbytes for r in recs_p)
     d2h = sum(r.data.nbytes for r in recs_p)
-    for _ in range(1):
-        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), NSHOTS, shots))
+    abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), ns, shots))
     dist_barrier(world)
     e2e_steps = max(1, min(args.steps, 3))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         for r in recs_p:
             r.data[:] = 0
-        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), NSHOTS, shots))
+        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), ns, shots))
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_s = dist_max(e2e_s * 1e3, world) / 1e3
     e2e = {"value": round(pts_per_step * world / e2e_s / 1e9, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
            "path": "rsgpu_modelling (C ABI): plan create + upload, nt steps, trace read-back, destroy"}
     return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary(),
-                tile=tile_desc)
+                parity=parity, mode=mode)
 
 
 # ---------------------------------------------------------------- FWI gradient workload
@@ -676,12 +802,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
-    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "fwi", "acoustic3d"],
+    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d"],
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
-                         "fwi: the FWI gradient line alone")
+                         "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
+    ap.add_argument("--launch-mode", type=int, default=0,
+                    help="2D: rsgpu_config.launch_mode (0 = library choice: the fused step, 2 = per-tile kernels)")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
-    ap.add_argument("--zchunk", type=int, default=0, help="acoustic3d: planes per z-march (0 = library default)")
+    ap.add_argument("--zchunk", type=int, default=0,
+                    help="acoustic3d: planes per z-march; 2D fused step: rows per work item (0 = library default)")
     ap.add_argument("--shots", type=int, default=None,
                     help="acoustic3d: model only the first N windows (profiling runs)")
     args = ap.parse_args()
@@ -767,9 +896,23 @@ def main():
                 "clocks": r["clocks"], "cpu_baseline": cpu}
         print(json.dumps(line))
         return
+    if args.workload == "acoustic2d":
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_c1_reference()
+        r = run_gpu(args, rank, world, local, physics="acoustic2d")
+        if rank == 0:
+            print(json.dumps({"metric": "Gpts/s", "value": round(r["value"], 3), "unit": "Gpts/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic (seeded layered model, 5 % smooth perturbation, Ricker source)",
+                              "config": c1_config(world, args.precision), "gpu_launches": int(r["launches"]),
+                              "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
+                              "parity": r["parity"], "cpu_baseline": cpu}))
+        return
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference()   # before the first CUDA call of this process (spawned workers)
+        cpu = cpu_reference(CPU_BASELINE_STEPS)   # before the first CUDA call of this process (spawned workers)
     r = run_gpu(args, rank, world, local)
     fwi = None
     if rank == 0 and world == 1 and not args.no_fwi:
@@ -784,10 +927,10 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms_step"], 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded layered elastic model with lenses, Ricker source)",
-                "config": {**config_dict(world, args.precision, args.nt), "tile": r["tile"]},
+                "config": config_dict(world, args.precision, args.nt),
                 "gpu_launches": int(r["launches"]),
                 "roofline": r["roofline"], "e2e": r["e2e"], "clocks": r["clocks"],
-                "cpu_baseline": cpu}
+                "parity": r["parity"], "cpu_baseline": cpu}
         if fwi is not None:
             line["fwi_gradient"] = fwi
         print(json.dumps(line))
