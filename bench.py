@@ -434,9 +434,35 @@ def run_gpu(args, rank, world, device, physics="elastic2d"):
     e2e_s = dist_max(e2e_s * 1e3, world) / 1e3
     e2e = {"value": round(pts_per_step * world / e2e_s / 1e9, 3), "unit": "Gpts/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-           "path": "rsgpu_modelling (C ABI): plan create + upload, nt steps, trace read-back, destroy"}
+           "path": "rsgpu_modelling (C ABI): plan create + upload, nt steps, trace read-back, destroy",
+           "phases_ms": e2e_phases(cfg, ns, shots, recs_p)}
     return dict(value=value, ms_step=ms_step, launches=launches, roofline=roofline, e2e=e2e, clocks=clk.summary(),
                 parity=parity, mode=mode)
+
+
+def e2e_phases(cfg, ns, shots, recs):
+    """The same work as one rsgpu_modelling call, split into its C ABI phases and
+    timed on the host: plan creation with the uploads, the nt steps, the trace
+    read-back into the host arrays, and the plan's destruction."""
+    import ctypes as C
+    from rockseis_b200 import abi
+    for r in recs:
+        r.data[:] = 0
+    h = C.c_void_p()
+    t0 = time.perf_counter()
+    abi.check(abi.lib.rsgpu_plan_create(C.byref(cfg), ns, shots, C.byref(h)))
+    abi.check(abi.lib.rsgpu_plan_sync(h))
+    t1 = time.perf_counter()
+    abi.check(abi.lib.rsgpu_plan_run(h, 0, cfg.nt))
+    abi.check(abi.lib.rsgpu_plan_sync(h))
+    t2 = time.perf_counter()
+    for i, r in enumerate(recs):
+        abi.check(abi.lib.rsgpu_plan_read_traces(h, i, r.data.ctypes.data))
+    t3 = time.perf_counter()
+    abi.lib.rsgpu_plan_destroy(h)
+    t4 = time.perf_counter()
+    return {"create_upload": round((t1 - t0) * 1e3, 2), "run": round((t2 - t1) * 1e3, 2),
+            "read_traces": round((t3 - t2) * 1e3, 2), "destroy": round((t4 - t3) * 1e3, 2)}
 
 
 # ---------------------------------------------------------------- FWI gradient workload

@@ -155,11 +155,60 @@ static int stagger_t(int physics, int nx, int ny, int nz, int l, int fs, const T
     return stagger_e3d_host(nx, ny, nz, l, fs, vp, vs, rho, out);
 }
 
-// Elastic 3D staggering is provided by the 3D module when it is built.
+// ModelElastic3D::staggerModels (lib/model.cpp:3371-3475).  out = Rx, Ry, Rz, L,
+// L2M, M_yz, M_xz, M_xy.  Moduli from the padded vp/vs/rho in the reference's
+// expression types (2.0 is a double literal there), the free-surface row gets
+// L = 0 and L2M = M before staggering, each shear modulus is averaged along its
+// two axes, the densities are averaged and inverted, and the free-surface row
+// doubles Rx and Ry.
 template <typename T>
-int stagger_e3d_host(int, int, int, int, int, const T *, const T *, const T *, T *const *)
+int stagger_e3d_host(int nx, int ny, int nz, int l, int fs, const T *vp, const T *vs, const T *rho, T *const *out)
 {
-    return -2;
+    const int nxp = nx + 2 * l, nyp = ny + 2 * l, nzp = nz + 2 * l;
+    const size_t n = (size_t)nxp * nyp * nzp;
+    T *Rx = out[0], *Ry = out[1], *Rz = out[2], *L = out[3], *L2M = out[4], *Myz = out[5], *Mxz = out[6], *Mxy = out[7];
+    auto idx = [&](int ix, int iy, int iz) { return ((size_t)iz * nyp + iy) * nxp + ix; };
+    pad3(Rx, rho, nx, ny, nz, l, true);
+    pad3(Ry, rho, nx, ny, nz, l, true);
+    pad3(Rz, rho, nx, ny, nz, l, true);
+    pad3(L, vp, nx, ny, nz, l, true);
+    pad3(Mxz, vs, nx, ny, nz, l, true);
+    for (size_t i = 0; i < n; i++) {
+        const T _vp = L[i], _vs = Mxz[i], _rho = Rx[i];
+        L2M[i] = _rho * _vp * _vp;
+        L[i] = _rho * _vp * _vp - 2.0 * _rho * _vs * _vs;
+        Mxz[i] = _rho * _vs * _vs;
+        Myz[i] = _rho * _vs * _vs;
+        Mxy[i] = _rho * _vs * _vs;
+    }
+    if (fs)
+        for (int ix = 0; ix < nxp; ix++)
+            for (int iy = 0; iy < nyp; iy++) {
+                L[idx(ix, iy, l)] = 0.0;
+                L2M[idx(ix, iy, l)] = Mxz[idx(ix, iy, l)];
+            }
+    stagger_axis(Rx, nxp, nyp, nzp, 0);
+    stagger_axis(Ry, nxp, nyp, nzp, 1);
+    stagger_axis(Rz, nxp, nyp, nzp, 2);
+    stagger_axis(Mxz, nxp, nyp, nzp, 0);
+    stagger_axis(Mxz, nxp, nyp, nzp, 2);
+    stagger_axis(Myz, nxp, nyp, nzp, 1);
+    stagger_axis(Myz, nxp, nyp, nzp, 2);
+    stagger_axis(Mxy, nxp, nyp, nzp, 0);
+    stagger_axis(Mxy, nxp, nyp, nzp, 1);
+    for (size_t i = 0; i < n; i++) {
+        if (Rx[i] == 0.0 || Ry[i] == 0.0 || Rz[i] == 0.0) return -1;
+        Rx[i] = 1.0 / Rx[i];
+        Ry[i] = 1.0 / Ry[i];
+        Rz[i] = 1.0 / Rz[i];
+    }
+    if (fs)
+        for (int ix = 0; ix < nxp; ix++)
+            for (int iy = 0; iy < nyp; iy++) {
+                Rx[idx(ix, iy, l)] *= 2.0;
+                Ry[idx(ix, iy, l)] *= 2.0;
+            }
+    return 0;
 }
 template int stagger_e3d_host<float>(int, int, int, int, int, const float *, const float *, const float *, float *const *);
 template int stagger_e3d_host<double>(int, int, int, int, int, const double *, const double *, const double *, double *const *);

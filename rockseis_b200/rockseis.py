@@ -235,6 +235,36 @@ class ModelAcoustic3D(_Model):
         return m
 
 
+class ModelElastic3D(_Model):
+    """ModelElastic3D<T> (include/model.h): arrays [nz][ny][nx]; staggered
+    parameters Rx, Ry, Rz, L, L2M, M_yz, M_xz, M_xy (lib/model.cpp:3371-3475)."""
+    dim = 3
+    physics = abi.ELASTIC3D
+    names = ("Rx", "Ry", "Rz", "L", "L2M", "M_yz", "M_xz", "M_xy")
+
+    def __init__(self, nx, ny, nz, lpml, dx, dy, dz, ox, oy, oz, fs, precision=abi.F32_EXACT):
+        super().__init__(nx, ny, nz, lpml, dx, dy, dz, ox, oy, oz, fs, precision)
+
+    def createModel(self):
+        self.Vp = np.zeros(self._shape(), self.dtype)
+        self.Vs = np.zeros(self._shape(), self.dtype)
+        self.R = np.zeros(self._shape(), self.dtype)
+        self.realized = True
+
+    def getVp(self): return self.Vp
+    def getVs(self): return self.Vs
+    def getR(self): return self.R
+    def getDy(self): return self.dy
+    def getRx(self): return self.padded()[0]
+    def getRy(self): return self.padded()[1]
+    def getRz(self): return self.padded()[2]
+    def getL(self): return self.padded()[3]
+    def getL2M(self): return self.padded()[4]
+    def getM_yz(self): return self.padded()[5]
+    def getM_xz(self): return self.padded()[6]
+    def getM_xy(self): return self.padded()[7]
+
+
 class Data2D:
     """Trace container (Data2D<T>): data[itr, it] == reference data[it + itr*nt]."""
     dim = 2

@@ -322,3 +322,28 @@ def test_oracle_interp_matches_reference(mode):
         ref = GOLD[f"interp_m{mode}_a{a}"]
         assert np.abs(ref).max() > 0
         assert np.array_equal(got, ref), (mode, a, np.abs(got - ref).max())
+
+
+@pytest.mark.parametrize("fs", [0, 1])
+def test_stagger_elastic3d_matches_reference(fs):
+    """ModelElastic3D::staggerModels restated on the host (rsgpu_stagger_model),
+    against the reference library itself (skipped where it is not built)."""
+    from oracle import api
+    from rockseis_b200.rockseis import ModelElastic3D
+    if not api.ref_available():
+        pytest.skip("reference library not built")
+    import ctypes as C
+    rng = np.random.default_rng(7)
+    nx, ny, nz, l = 9, 7, 6, 3
+    vp = rng.uniform(1500, 3000, (nz, ny, nx)).astype(np.float32)
+    vs = (vp / rng.uniform(1.6, 2.1, vp.shape)).astype(np.float32)
+    rho = rng.uniform(1000, 2500, vp.shape).astype(np.float32)
+    m = ModelElastic3D(nx, ny, nz, l, 10.0, 10.0, 10.0, 0.0, 0.0, 0.0, fs)
+    m.createModel()
+    m.Vp[:], m.Vs[:], m.R[:] = vp, vs, rho
+    g = api.RefGrid(nx, ny, nz, l, 8, fs, 10.0, 10.0, 10.0, 0.0, 0.0, 0.0, 1e-3, 10)
+    ref = [np.zeros((nz + 2 * l, ny + 2 * l, nx + 2 * l), np.float32) for _ in range(8)]
+    api.ref().ref_stagger_e3d_f(C.byref(g), vp.ctypes.data, vs.ctypes.data, rho.ctypes.data,
+                                *[a.ctypes.data for a in ref])
+    for name, got, r in zip(m.names, m.padded(), ref):
+        assert np.array_equal(got, r), name
