@@ -832,7 +832,7 @@ def main():
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
     ap.add_argument("--launch-mode", type=int, default=0,
-                    help="2D: rsgpu_config.launch_mode (0 = library choice: the fused step, 2 = per-tile kernels)")
+                    help="2D: rsgpu_config.launch_mode (0 = library choice: per-tile kernels, 3 = fused step)")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
     ap.add_argument("--zchunk", type=int, default=0,

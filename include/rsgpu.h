@@ -80,11 +80,11 @@ typedef struct {
     int tile;           /* 2D kernel tile shape index (rsgpu_tile_shape), -1 = built-in default */
     int zchunk;         /* 3D: planes marched by one CTA (0 = 64); 2D fused step: rows per
                            work item (rounded up to 8; 0 = chosen from the batch size) */
-    int launch_mode;    /* 2D propagation: 0 = library choice (the fused step for forward
-                           propagation), 1 = persistent per-tile kernels (elastic forward),
+    int launch_mode;    /* 2D propagation: 0 = library choice (the per-tile kernels, the
+                           faster on B200), 1 = persistent per-tile kernels (elastic forward),
                            2 = per-tile velocity and stress kernels, 3 = fused z-marching step:
                            velocity, stress and injection of a time step plus recording of
-                           the previous one in one launch */
+                           the previous one in one launch (forward propagation) */
     int reserved[5];
 } rsgpu_config;
 

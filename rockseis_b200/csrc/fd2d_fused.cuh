@@ -39,6 +39,13 @@
 // Arithmetic per point is the per-tile kernels' (fd2d_kernels.cuh): MODE_IEEE
 // reproduces the reference's float operations bit for bit, MODE_FAST uses FMA
 // and coefficients pre-divided by the spacing.
+//
+// Measured on B200 (16-shot 801 x 401 elastic batch): DRAM traffic is at the
+// algorithmic 60 B per point, but the step issues about as many instructions per
+// point as the per-tile kernels (~440) with two CTAs of four warps per SM (the
+// rings take 80 KB of shared memory, the block state ~240 registers per thread),
+// so it is issue-bound at 15-18 % issue efficiency and runs slower than the
+// per-tile kernels; it is selected by launch_mode 3 only.
 #pragma once
 #include "fd2d_kernels.cuh"
 
@@ -116,7 +123,9 @@ __device__ __forceinline__ void dz_ring(const T *s0, const T *s1, const T *s2, c
 {
     using P = typename Pair<T>::t;
     if constexpr (MODE == MODE_FAST && std::is_same<T, float>::value) {
-        float2 acc[4];
+        float2 acc[4], cp[NCOEF], cn[NCOEF];
+#pragma unroll
+        for (int k = 0; k < NCOEF; k++) { cp[k] = make_float2(cu[k], cu[k]); cn[k] = make_float2(-cu[k], -cu[k]); }
 #pragma unroll
         for (int rr = 0; rr < 4; rr++) acc[rr] = make_float2(0.f, 0.f);
 #pragma unroll
@@ -126,8 +135,8 @@ __device__ __forceinline__ void dz_ring(const T *s0, const T *s1, const T *s2, c
             for (int rr = 0; rr < 4; rr++) {
                 const int kp = FW ? q - rr - 9 : q - rr - 8;
                 const int km = FW ? rr + 8 - q : rr + 7 - q;
-                if (kp >= 0 && kp < NCOEF) acc[rr] = __ffma2_rn(w, make_float2(cu[kp], cu[kp]), acc[rr]);
-                if (km >= 0 && km < NCOEF) acc[rr] = __ffma2_rn(w, make_float2(-cu[km], -cu[km]), acc[rr]);
+                if (kp >= 0 && kp < NCOEF) acc[rr] = __ffma2_rn(w, cp[kp], acc[rr]);
+                if (km >= 0 && km < NCOEF) acc[rr] = __ffma2_rn(w, cn[km], acc[rr]);
             }
         }
 #pragma unroll
@@ -175,33 +184,6 @@ __device__ __noinline__ T stencil_k_ring(const T *s0, const T *s1, const T *s2, 
 __device__ __forceinline__ int kfw_in(int i, int n, int order) { return (i < 0 || i >= n) ? order : kfw(i, n, order); }
 __device__ __forceinline__ int kbw_in(int i, int n, int order) { return (i < 0 || i >= n) ? order : kbw(i, n, order); }
 
-// x fix-up of a pair of row outputs (columns gx, gx+1) whose coefficient count differs from `order`.
-template <typename T, int MODE>
-__device__ __forceinline__ void fix_x(T (&o)[2], const T *row_c8, int gx, int nxp, int order, const T *cx, bool fw, T d,
-                                      T r)
-{
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        const int K = fw ? kfw_in(gx + j, nxp, order) : kbw_in(gx + j, nxp, order);
-        if (K != order) o[j] = stencil_k<T, MODE>(row_c8 + 8 + j, 1, K, cx + K * CROW, fw, d, r);
-    }
-}
-// z fix-up of the thread's 4 x 2 outputs (rows gz0.., window rows 4h+8..).
-template <typename T, int MODE>
-__device__ __forceinline__ void fix_z(T (&o)[4][2], const T *s0, const T *s1, const T *s2, int rs, int h, int gz0,
-                                      int nzp, int order, const T *cz, bool fw, T d, T r)
-{
-#pragma unroll
-    for (int rr = 0; rr < 4; rr++) {
-        const int K = fw ? kfw_in(gz0 + rr, nzp, order) : kbw_in(gz0 + rr, nzp, order);
-        if (K != order) {
-#pragma unroll
-            for (int j = 0; j < 2; j++)
-                o[rr][j] = stencil_k_ring<T, MODE>(s0 + j, s1 + j, s2 + j, rs, 4 * h + rr + 8, K, cz + K * CROW, fw, d, r);
-        }
-    }
-}
-
 // z-derivative dispatch on the thread's row half (uniform per warp).
 template <typename T, int MODE, bool FW, int RS>
 __device__ __forceinline__ void dz_half(int h, const T *s0, const T *s1, const T *s2, const T (&cu)[NCOEF], T d, T r,
@@ -239,49 +221,193 @@ __device__ __forceinline__ int zstrip_in(int ix, int iz, int nxp, int nzp, int l
     return zstrip(iz, nzp, lp, tb, row);
 }
 
-// One field of an update at a 4 x 2 block (lib/waves.cpp:245-307):
-//   F += a*d1 [x strip: psi, F -= a*(psi + C*d1)] ; F += a*d2 [z strip likewise],
-// a = dt*modulus.  has1/has2 select the parts (acoustic velocities have one each).
+// Fast update of one field at a 4 x 2 block that touches no C-PML strip, no
+// reduced-order stencil and no free-surface row (lib/waves.cpp:245-307 without the
+// strip corrections): F += a*d1 ; F += a*d2 with a = dt*modulus.
 template <typename T, int MODE>
-__device__ __forceinline__ void blk_update(T (&F)[4][2], const T (&Mo)[4][2], const T (&d1)[4][2], const T (&d2)[4][2],
-                                           bool has1, bool has2, bool pml, const Shot2D<T> &sh, const Zm2DArgs<T> &a,
-                                           int gx, int gz0, const T *pxi, T *pxo, int xb_add, const T *pzi, T *pzo,
-                                           int zb_add, bool own)
+__device__ __forceinline__ void fast_update(T (&F)[4][2], const T (&Mo)[4][2], const T (&d1)[4][2],
+                                            const T (&d2)[4][2], bool has1, bool has2, T dt)
 {
     using A = Ar<T, MODE>;
 #pragma unroll
-    for (int rr = 0; rr < 4; rr++) {
-        const int iz = gz0 + rr;
+    for (int rr = 0; rr < 4; rr++)
 #pragma unroll
         for (int j = 0; j < 2; j++) {
-            const int ix = gx + j;
-            const T am = A::mul(a.dt, Mo[rr][j]);
-            if (has1) {
-                F[rr][j] = A::mad(F[rr][j], am, d1[rr][j]);
-                if (pml) {
-                    int xb, xc;
-                    const int xi = xstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, xb, xc);
-                    if (xi >= 0) {
-                        const int o = iz * 2 * a.lpml + xc;
-                        F[rr][j] = pml_pp<T, MODE>(F[rr][j], am, d1[rr][j], pxi + o, pxo + o, own, a.pml, a.lpml,
-                                                   xb + xb_add, xi);
-                    }
-                }
+            const T am = A::mul(dt, Mo[rr][j]);
+            if (has1) F[rr][j] = A::mad(F[rr][j], am, d1[rr][j]);
+            if (has2) F[rr][j] = A::mad(F[rr][j], am, d2[rr][j]);
+        }
+}
+
+// Do the index ranges [a, b] and [lo, hi) meet?
+__device__ __forceinline__ bool meets(int a, int b, int lo, int hi) { return a < hi && b >= lo; }
+
+// Does the block of columns [gx, gx+1] x rows [gz0, gz0+3] need the general
+// per-point path: a reduced-order stencil near an array end, a C-PML strip point
+// or (stress) the free-surface row?
+__device__ __forceinline__ bool block_special(int gx, int gz0, int nxp, int nzp, int order, int lp, bool fsrow_check,
+                                              bool fs)
+{
+    const int gx1 = gx + 1, gz1 = gz0 + 3;
+    const bool in_x = meets(gx, gx1, 0, nxp), in_z = meets(gz0, gz1, 0, nzp);
+    const bool edge = (in_z && (meets(gx, gx1, 0, order) || meets(gx, gx1, nxp - order - 1, nxp))) ||
+                      (in_x && (meets(gz0, gz1, 0, order) || meets(gz0, gz1, nzp - order - 1, nzp)));
+    const bool pml = (in_z && (meets(gx, gx1, 0, lp) || meets(gx, gx1, nxp - lp, nxp))) ||
+                     (in_x && (meets(gz0, gz1, 0, lp) || meets(gz0, gz1, nzp - lp, nzp)));
+    return edge || pml || (fsrow_check && fs && meets(gz0, gz1, lp, lp + 1));
+}
+
+// What the general per-point path needs to know about one field's update.
+template <typename T>
+struct ZmPoint {
+    const T *xrow;              // x-derivative field: row 0 of the block, column gx-8 (shared memory)
+    int xrs;                    // its row stride
+    const T *z0, *z1, *z2;      // z-derivative field at column gx, row 0 of slabs i-1, i, i+1
+    int zrs;
+    int h, gx, gz0;
+    bool fw1, fw2;              // forward (staggered) derivatives
+    const T *pxi, *pzi;         // C-PML memory read (x strip, z strip)
+    T *pxo, *pzo;               // ... and written (by the owner)
+    int xb_add, zb_add;         // 3 = staggered C-PML tables
+    bool own;
+};
+
+// The reference's reduced-order x / z stencils at one point of the block, where the
+// coefficient count differs from `order` (lib/der.cpp:155-540).
+template <typename T, int MODE>
+__device__ __forceinline__ T fix_dx_pt(T d, const ZmPoint<T> &q, int rr, int j, int nxp, const Zm2DArgs<T> &a,
+                                       const CoefSet<T> *cs)
+{
+    const int ix = q.gx + j;
+    const int K = q.fw1 ? kfw_in(ix, nxp, a.order) : kbw_in(ix, nxp, a.order);
+    if (K == a.order) return d;
+    return stencil_k<T, MODE>(q.xrow + rr * q.xrs + 8 + j, 1, K, cs->cx + K * CROW, q.fw1, a.dx, a.rdx);
+}
+template <typename T, int MODE>
+__device__ __forceinline__ T fix_dz_pt(T d, const ZmPoint<T> &q, int rr, int j, int nzp, const Zm2DArgs<T> &a,
+                                       const CoefSet<T> *cs)
+{
+    const int iz = q.gz0 + rr;
+    const int K = q.fw2 ? kfw_in(iz, nzp, a.order) : kbw_in(iz, nzp, a.order);
+    if (K == a.order) return d;
+    return stencil_k_ring<T, MODE>(q.z0 + j, q.z1 + j, q.z2 + j, q.zrs, 4 * q.h + rr + 8, K, cs->cz + K * CROW, q.fw2,
+                                   a.dz, a.rdz);
+}
+
+// General per-point update of one field (a loop over the block's 8 points, not
+// unrolled, so the code stays small): reduced-order derivatives where the
+// reference uses them, then F += a*d1 [x strip: psi = B*psi + A*d1,
+// F -= a*(psi + C*d1)] ; F += a*d2 [z strip likewise]  (lib/waves.cpp:245-307).
+template <typename T, int MODE>
+__device__ __noinline__ void general_update(T *F, const T *Mo, const T *d1, const T *d2, bool has1, bool has2,
+                                            const ZmPoint<T> &q, const Shot2D<T> &sh, const Zm2DArgs<T> &a,
+                                            const CoefSet<T> *cs)
+{
+    using A = Ar<T, MODE>;
+    for (int k = 0; k < 8; k++) {
+        const int rr = k >> 1, j = k & 1, ix = q.gx + j, iz = q.gz0 + rr;
+        const T am = A::mul(a.dt, Mo[k]);
+        if (has1) {
+            const T d = fix_dx_pt<T, MODE>(d1[k], q, rr, j, sh.nxp, a, cs);
+            F[k] = A::mad(F[k], am, d);
+            int xb, xc;
+            const int xi = xstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, xb, xc);
+            if (xi >= 0) {
+                const int o = iz * 2 * a.lpml + xc;
+                F[k] = pml_pp<T, MODE>(F[k], am, d, q.pxi + o, q.pxo + o, q.own, a.pml, a.lpml, xb + q.xb_add, xi);
             }
-            if (has2) {
-                F[rr][j] = A::mad(F[rr][j], am, d2[rr][j]);
-                if (pml) {
-                    int zb, zr;
-                    const int zi = zstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, zb, zr);
-                    if (zi >= 0) {
-                        const int o = zr * sh.nxp + ix;
-                        F[rr][j] = pml_pp<T, MODE>(F[rr][j], am, d2[rr][j], pzi + o, pzo + o, own, a.pml, a.lpml,
-                                                   zb + zb_add, zi);
-                    }
-                }
+        }
+        if (has2) {
+            const T d = fix_dz_pt<T, MODE>(d2[k], q, rr, j, sh.nzp, a, cs);
+            F[k] = A::mad(F[k], am, d);
+            int zb, zr;
+            const int zi = zstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, zb, zr);
+            if (zi >= 0) {
+                const int o = zr * sh.nxp + ix;
+                F[k] = pml_pp<T, MODE>(F[k], am, d, q.pzi + o, q.pzo + o, q.own, a.pml, a.lpml, zb + q.zb_add, zi);
             }
         }
     }
+}
+
+// General per-point update of the normal stresses (lib/waves.cpp:1596-1674):
+// d1 = Dx-Vx feeds Sxx with L2M and Szz with L and one x memory; d2 = Dz-Vz
+// likewise with one z memory; free surface Szz = 0 on row lpml.
+template <typename T, int MODE>
+__device__ __noinline__ void general_normal(T *sxx, T *szz, const T *l, const T *l2m, const T *d1, const T *d2,
+                                            const ZmPoint<T> &q, const Shot2D<T> &sh, const Zm2DArgs<T> &a,
+                                            const CoefSet<T> *cs)
+{
+    using A = Ar<T, MODE>;
+    for (int k = 0; k < 8; k++) {
+        const int rr = k >> 1, j = k & 1, ix = q.gx + j, iz = q.gz0 + rr;
+        const T a2 = A::mul(a.dt, l2m[k]), a1 = A::mul(a.dt, l[k]);
+        const T e1 = fix_dx_pt<T, MODE>(d1[k], q, rr, j, sh.nxp, a, cs);
+        const T e2 = fix_dz_pt<T, MODE>(d2[k], q, rr, j, sh.nzp, a, cs);
+        T xx = A::mad(sxx[k], a2, e1), zz = A::mad(szz[k], a1, e1);
+        int xb, xc;
+        const int xi = xstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, xb, xc);
+        if (xi >= 0) {
+            T *ps = sh.psix[2] + iz * 2 * a.lpml + xc;
+            const T tA = __ldg(a.pml + (xb + PT_A) * a.lpml + xi), tB = __ldg(a.pml + (xb + PT_B) * a.lpml + xi),
+                    tC = __ldg(a.pml + (xb + PT_C) * a.lpml + xi);
+            const T p = A::mad(A::mul(tB, *ps), tA, e1);
+            *ps = p;
+            const T cq = A::mad(p, tC, e1);
+            xx = A::msub(xx, a2, cq);
+            zz = A::msub(zz, a1, cq);
+        }
+        xx = A::mad(xx, a1, e2);
+        zz = A::mad(zz, a2, e2);
+        int zb, zr;
+        const int zi = zstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, zb, zr);
+        if (zi >= 0) {
+            T *ps = sh.psiz[2] + zr * sh.nxp + ix;
+            const T tA = __ldg(a.pml + (zb + PT_A) * a.lpml + zi), tB = __ldg(a.pml + (zb + PT_B) * a.lpml + zi),
+                    tC = __ldg(a.pml + (zb + PT_C) * a.lpml + zi);
+            const T p = A::mad(A::mul(tB, *ps), tA, e2);
+            *ps = p;
+            const T cq = A::mad(p, tC, e2);
+            xx = A::msub(xx, a1, cq);
+            zz = A::msub(zz, a2, cq);
+        }
+        if (sh.fs && iz == a.lpml) zz = T(0);
+        sxx[k] = xx;
+        szz[k] = zz;
+    }
+}
+
+// Register block <-> flat per-point arrays for the general path.
+template <typename T>
+__device__ __forceinline__ void flat(T *o, const T (&v)[4][2])
+{
+#pragma unroll
+    for (int k = 0; k < 8; k++) o[k] = v[k >> 1][k & 1];
+}
+template <typename T>
+__device__ __forceinline__ void unflat(T (&v)[4][2], const T *o)
+{
+#pragma unroll
+    for (int k = 0; k < 8; k++) v[k >> 1][k & 1] = o[k];
+}
+
+// One field's update: the fast path, or the general path through flat arrays.
+template <typename T, int MODE>
+__device__ __forceinline__ void field_update(bool special, T (&F)[4][2], const T (&Mo)[4][2], const T (&d1)[4][2],
+                                             const T (&d2)[4][2], bool has1, bool has2, const ZmPoint<T> &q,
+                                             const Shot2D<T> &sh, const Zm2DArgs<T> &a, const CoefSet<T> *cs)
+{
+    if (!special) {
+        fast_update<T, MODE>(F, Mo, d1, d2, has1, has2, a.dt);
+        return;
+    }
+    T f[8], m[8], e1[8], e2[8];
+    flat(f, F);
+    flat(m, Mo);
+    flat(e1, d1);
+    flat(e2, d2);
+    general_update<T, MODE>(f, m, e1, e2, has1, has2, q, sh, a, cs);
+    unflat(F, f);
 }
 
 // ------------------------------------------------------------------ point-wise inputs
@@ -473,6 +599,18 @@ struct ZmStep {
         }
     }
 
+    // Per-point context of one field's update for the general path.
+    __device__ ZmPoint<T> point(const T *xrow, int xrs, const T *z0, const T *z1, const T *z2, int zrs, int gx, int gz0,
+                                bool fw1, bool fw2, const T *pxi, T *pxo, int xb_add, const T *pzi, T *pzo, int zb_add,
+                                bool own)
+    {
+        ZmPoint<T> q;
+        q.xrow = xrow; q.xrs = xrs; q.z0 = z0; q.z1 = z1; q.z2 = z2; q.zrs = zrs;
+        q.h = h; q.gx = gx; q.gz0 = gz0; q.fw1 = fw1; q.fw2 = fw2;
+        q.pxi = pxi; q.pxo = pxo; q.xb_add = xb_add; q.pzi = pzi; q.pzo = pzo; q.zb_add = zb_add; q.own = own;
+        return q;
+    }
+
     // ---- velocity of slab i (columns x0-8 .. x0+TX+8)
     __device__ void velocity(const Zm2DArgs<T> &a, const Shot2D<T> &sh, const ZmItem &it, int cur, int i, VelIn<T> &v,
                              T *const *Fn, bool owned_rows)
@@ -480,55 +618,43 @@ struct ZmStep {
         const int vc = 2 * p, gx = it.x0 - 8 + vc, gz0 = it.z0 - 16 + ZM_RB * i + 4 * h;
         const T *s0 = slot_ptr(gslab + i - 1), *s1 = slot_ptr(gslab + i), *s2 = slot_ptr(gslab + i + 1);
         const int sc = vc + 8;                         // ring column of the pair
-        const bool xe = it.flags & ZM_XEDGE, ze = it.flags & ZM_ZEDGE;
-        const bool pml = it.flags & (ZM_XPML | ZM_ZPML);
+        const bool special = block_special(gx, gz0, sh.nxp, sh.nzp, a.order, a.lpml, false, false);
         const bool own = owned_rows && p >= 4 && p < 4 + G::NPS;
         T cux[NCOEF], cuz[NCOEF];
 #pragma unroll
         for (int k = 0; k < NCOEF; k++) { cux[k] = cs->cx[a.order * CROW + k]; cuz[k] = cs->cz[a.order * CROW + k]; }
         const int lo = cur, hi = cur ^ 1;   // psi copies read / written
         T d1[4][2], d2[4][2];
+        const T *rowbase = s1 + (4 * h) * SW + sc - 8;   // row 0 of the block, column gx-8, ring field 0
         if constexpr (PHYS == PHYS_E2D) {
             // Vx += dt*Rx*Dx+Sxx [x stag psi0] ; Vx += dt*Rx*Dz-Sxz [z psi0]   (lib/waves.cpp:1416-1490)
-            const T *rxx = s1 + R_SXX * G::SLAB, *rxz0 = s0 + R_SXZ * G::SLAB, *rxz1 = s1 + R_SXZ * G::SLAB,
-                    *rxz2 = s2 + R_SXZ * G::SLAB;
+            const T *rxz0 = s0 + R_SXZ * G::SLAB + sc, *rxz1 = s1 + R_SXZ * G::SLAB + sc, *rxz2 = s2 + R_SXZ * G::SLAB + sc;
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const T *row = rxx + (4 * h + rr) * SW + sc - 8;
-                dx_pair<T, MODE, true>(row, cux, a.dx, a.rdx, d1[rr]);
-                if (xe) fix_x<T, MODE>(d1[rr], row, gx, sh.nxp, a.order, cs->cx, true, a.dx, a.rdx);
-            }
-            dz_half<T, MODE, false, SW>(h, rxz0 + sc, rxz1 + sc, rxz2 + sc, cuz, a.dz, a.rdz, d2);
-            if (ze) fix_z<T, MODE>(d2, rxz0 + sc, rxz1 + sc, rxz2 + sc, SW, h, gz0, sh.nzp, a.order, cs->cz, false, a.dz, a.rdz);
-            blk_update<T, MODE>(v.f1, v.m1, d1, d2, true, true, pml, sh, a, gx, gz0, psi_x(sh, 0, lo), psi_x(sh, 0, hi),
-                                3, psi_z(sh, 0, lo), psi_z(sh, 0, hi), 0, own);
+            for (int rr = 0; rr < 4; rr++) dx_pair<T, MODE, true>(rowbase + R_SXX * G::SLAB + rr * SW, cux, a.dx, a.rdx, d1[rr]);
+            dz_half<T, MODE, false, SW>(h, rxz0, rxz1, rxz2, cuz, a.dz, a.rdz, d2);
+            field_update<T, MODE>(special, v.f1, v.m1, d1, d2, true, true,
+                                  point(rowbase + R_SXX * G::SLAB, SW, rxz0, rxz1, rxz2, SW, gx, gz0, true, false,
+                                        psi_x(sh, 0, lo), psi_x(sh, 0, hi), 3, psi_z(sh, 0, lo), psi_z(sh, 0, hi), 0, own),
+                                  sh, a, cs);
             // Vz += dt*Rz*Dx-Sxz [x psi1] ; Vz += dt*Rz*Dz+Szz [z stag psi1]   (lib/waves.cpp:1492-1566)
-            const T *rzz0 = s0 + R_SZZ * G::SLAB, *rzz1 = s1 + R_SZZ * G::SLAB, *rzz2 = s2 + R_SZZ * G::SLAB;
+            const T *rzz0 = s0 + R_SZZ * G::SLAB + sc, *rzz1 = s1 + R_SZZ * G::SLAB + sc, *rzz2 = s2 + R_SZZ * G::SLAB + sc;
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const T *row = rxz1 + (4 * h + rr) * SW + sc - 8;
-                dx_pair<T, MODE, false>(row, cux, a.dx, a.rdx, d1[rr]);
-                if (xe) fix_x<T, MODE>(d1[rr], row, gx, sh.nxp, a.order, cs->cx, false, a.dx, a.rdx);
-            }
-            dz_half<T, MODE, true, SW>(h, rzz0 + sc, rzz1 + sc, rzz2 + sc, cuz, a.dz, a.rdz, d2);
-            if (ze) fix_z<T, MODE>(d2, rzz0 + sc, rzz1 + sc, rzz2 + sc, SW, h, gz0, sh.nzp, a.order, cs->cz, true, a.dz, a.rdz);
-            blk_update<T, MODE>(v.f2, v.m2, d1, d2, true, true, pml, sh, a, gx, gz0, psi_x(sh, 1, lo), psi_x(sh, 1, hi),
-                                0, psi_z(sh, 1, lo), psi_z(sh, 1, hi), 3, own);
+            for (int rr = 0; rr < 4; rr++) dx_pair<T, MODE, false>(rowbase + R_SXZ * G::SLAB + rr * SW, cux, a.dx, a.rdx, d1[rr]);
+            dz_half<T, MODE, true, SW>(h, rzz0, rzz1, rzz2, cuz, a.dz, a.rdz, d2);
+            field_update<T, MODE>(special, v.f2, v.m2, d1, d2, true, true,
+                                  point(rowbase + R_SXZ * G::SLAB, SW, rzz0, rzz1, rzz2, SW, gx, gz0, false, true,
+                                        psi_x(sh, 1, lo), psi_x(sh, 1, hi), 0, psi_z(sh, 1, lo), psi_z(sh, 1, hi), 3, own),
+                                  sh, a, cs);
         } else {
             // Vx += dt*Rx*Dx+P [x stag psi0] ; Vz += dt*Rz*Dz+P [z stag psi0]   (lib/waves.cpp:217-310)
-            const T *rp0 = s0 + R_P * G::SLAB, *rp1 = s1 + R_P * G::SLAB, *rp2 = s2 + R_P * G::SLAB;
+            const T *rp0 = s0 + sc, *rp1 = s1 + sc, *rp2 = s2 + sc;
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const T *row = rp1 + (4 * h + rr) * SW + sc - 8;
-                dx_pair<T, MODE, true>(row, cux, a.dx, a.rdx, d1[rr]);
-                if (xe) fix_x<T, MODE>(d1[rr], row, gx, sh.nxp, a.order, cs->cx, true, a.dx, a.rdx);
-            }
-            blk_update<T, MODE>(v.f1, v.m1, d1, d1, true, false, pml, sh, a, gx, gz0, psi_x(sh, 0, lo), psi_x(sh, 0, hi),
-                                3, psi_z(sh, 0, lo), psi_z(sh, 0, hi), 3, own);
-            dz_half<T, MODE, true, SW>(h, rp0 + sc, rp1 + sc, rp2 + sc, cuz, a.dz, a.rdz, d2);
-            if (ze) fix_z<T, MODE>(d2, rp0 + sc, rp1 + sc, rp2 + sc, SW, h, gz0, sh.nzp, a.order, cs->cz, true, a.dz, a.rdz);
-            blk_update<T, MODE>(v.f2, v.m2, d2, d2, false, true, pml, sh, a, gx, gz0, psi_x(sh, 0, lo), psi_x(sh, 0, hi),
-                                3, psi_z(sh, 0, lo), psi_z(sh, 0, hi), 3, own);
+            for (int rr = 0; rr < 4; rr++) dx_pair<T, MODE, true>(rowbase + rr * SW, cux, a.dx, a.rdx, d1[rr]);
+            dz_half<T, MODE, true, SW>(h, rp0, rp1, rp2, cuz, a.dz, a.rdz, d2);
+            const ZmPoint<T> q = point(rowbase, SW, rp0, rp1, rp2, SW, gx, gz0, true, true, psi_x(sh, 0, lo),
+                                       psi_x(sh, 0, hi), 3, psi_z(sh, 0, lo), psi_z(sh, 0, hi), 3, own);
+            field_update<T, MODE>(special, v.f1, v.m1, d1, d1, true, false, q, sh, a, cs);
+            field_update<T, MODE>(special, v.f2, v.m2, d2, d2, false, true, q, sh, a, cs);
         }
         // velocity ring (all columns) and the new copy (owned points)
         T *vs = vslot_ptr(i);
@@ -545,28 +671,24 @@ struct ZmStep {
     __device__ void stress(const Zm2DArgs<T> &a, const Shot2D<T> &sh, const ZmItem &it, int j, const StrIn<T, PHYS> &m,
                            T *const *Fn)
     {
+        using A = Ar<T, MODE>;
         const int gx = it.x0 + 2 * p, gz0 = it.z0 - 16 + ZM_RB * j + 4 * h;
         const int vc = 2 * p + 8, sc = 2 * p + 16;
         const T *v0 = vslot_ptr(j - 1), *v1 = vslot_ptr(j), *v2 = vslot_ptr(j + 1);
         const T *so = slot_ptr(gslab + j) + (4 * h) * SW + sc;   // old stresses, row 4h of slab j
-        const bool xe = it.flags & ZM_XEDGE, ze = it.flags & ZM_ZEDGE;
-        const bool pml = it.flags & (ZM_XPML | ZM_ZPML);
+        const bool special = block_special(gx, gz0, sh.nxp, sh.nzp, a.order, a.lpml, true, sh.fs != 0);
         T cux[NCOEF], cuz[NCOEF];
 #pragma unroll
         for (int k = 0; k < NCOEF; k++) { cux[k] = cs->cx[a.order * CROW + k]; cuz[k] = cs->cz[a.order * CROW + k]; }
         const int o0 = gz0 * sh.pitch + gx;
         T d1[4][2], d2[4][2];
-        const T *vx0 = v0, *vx1 = v1, *vx2 = v2;                                  // Vx plane of each slab
-        const T *vz0 = v0 + G::VSLAB, *vz1 = v1 + G::VSLAB, *vz2 = v2 + G::VSLAB;   // Vz plane
+        const T *vx0 = v0 + vc, *vx1 = v1 + vc, *vx2 = v2 + vc;                                   // Vx plane
+        const T *vz0 = v0 + G::VSLAB + vc, *vz1 = v1 + G::VSLAB + vc, *vz2 = v2 + G::VSLAB + vc;   // Vz plane
+        const T *rowx = v1 + (4 * h) * VW + vc - 8, *rowz = rowx + G::VSLAB;   // row 0 of the block, column gx-8
         // d1 = Dx-Vx, d2 = Dz-Vz
 #pragma unroll
-        for (int rr = 0; rr < 4; rr++) {
-            const T *row = vx1 + (4 * h + rr) * VW + vc - 8;
-            dx_pair<T, MODE, false>(row, cux, a.dx, a.rdx, d1[rr]);
-            if (xe) fix_x<T, MODE>(d1[rr], row, gx, sh.nxp, a.order, cs->cx, false, a.dx, a.rdx);
-        }
-        dz_half<T, MODE, false, VW>(h, vz0 + vc, vz1 + vc, vz2 + vc, cuz, a.dz, a.rdz, d2);
-        if (ze) fix_z<T, MODE>(d2, vz0 + vc, vz1 + vc, vz2 + vc, VW, h, gz0, sh.nzp, a.order, cs->cz, false, a.dz, a.rdz);
+        for (int rr = 0; rr < 4; rr++) dx_pair<T, MODE, false>(rowx + rr * VW, cux, a.dx, a.rdx, d1[rr]);
+        dz_half<T, MODE, false, VW>(h, vz0, vz1, vz2, cuz, a.dz, a.rdz, d2);
         if constexpr (PHYS == PHYS_E2D) {
             T sxx[4][2], szz[4][2];
 #pragma unroll
@@ -576,25 +698,40 @@ struct ZmStep {
                     sxx[rr][c] = so[R_SXX * G::SLAB + rr * SW + c];
                     szz[rr][c] = so[R_SZZ * G::SLAB + rr * SW + c];
                 }
-            normal_update(sxx, szz, m, d1, d2, pml, sh, a, gx, gz0);
+            if (!special) {
+                // normal stresses (lib/waves.cpp:1596-1674), no strip, no free surface here
+#pragma unroll
+                for (int rr = 0; rr < 4; rr++)
+#pragma unroll
+                    for (int c = 0; c < 2; c++) {
+                        const T a2 = A::mul(a.dt, m.l2m[rr][c]), a1 = A::mul(a.dt, m.l[rr][c]);
+                        sxx[rr][c] = A::mad(A::mad(sxx[rr][c], a2, d1[rr][c]), a1, d2[rr][c]);
+                        szz[rr][c] = A::mad(A::mad(szz[rr][c], a1, d1[rr][c]), a2, d2[rr][c]);
+                    }
+            } else {
+                T fx[8], fz[8], l[8], l2m[8], e1[8], e2[8];
+                flat(fx, sxx); flat(fz, szz); flat(l, m.l); flat(l2m, m.l2m); flat(e1, d1); flat(e2, d2);
+                const ZmPoint<T> q = point(rowx, VW, vz0, vz1, vz2, VW, gx, gz0, false, false, nullptr, nullptr, 0,
+                                           nullptr, nullptr, 0, true);
+                general_normal<T, MODE>(fx, fz, l, l2m, e1, e2, q, sh, a, cs);
+                unflat(sxx, fx);
+                unflat(szz, fz);
+            }
             st_pair_rows(Fn[E2_SXX], o0, sh.pitch, sxx);
             st_pair_rows(Fn[E2_SZZ], o0, sh.pitch, szz);
             // Sxz += dt*M*Dx+Vz [x stag psi3] ; Sxz += dt*M*Dz+Vx [z stag psi3]   (lib/waves.cpp:1676-1735)
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                const T *row = vz1 + (4 * h + rr) * VW + vc - 8;
-                dx_pair<T, MODE, true>(row, cux, a.dx, a.rdx, d1[rr]);
-                if (xe) fix_x<T, MODE>(d1[rr], row, gx, sh.nxp, a.order, cs->cx, true, a.dx, a.rdx);
-            }
-            dz_half<T, MODE, true, VW>(h, vx0 + vc, vx1 + vc, vx2 + vc, cuz, a.dz, a.rdz, d2);
-            if (ze) fix_z<T, MODE>(d2, vx0 + vc, vx1 + vc, vx2 + vc, VW, h, gz0, sh.nzp, a.order, cs->cz, true, a.dz, a.rdz);
+            for (int rr = 0; rr < 4; rr++) dx_pair<T, MODE, true>(rowz + rr * VW, cux, a.dx, a.rdx, d1[rr]);
+            dz_half<T, MODE, true, VW>(h, vx0, vx1, vx2, cuz, a.dz, a.rdz, d2);
             T sxz[4][2];
 #pragma unroll
             for (int rr = 0; rr < 4; rr++)
 #pragma unroll
                 for (int c = 0; c < 2; c++) sxz[rr][c] = so[R_SXZ * G::SLAB + rr * SW + c];
-            blk_update<T, MODE>(sxz, m.m, d1, d2, true, true, pml, sh, a, gx, gz0, sh.psix[3], sh.psix[3], 3, sh.psiz[3],
-                                sh.psiz[3], 3, true);
+            field_update<T, MODE>(special, sxz, m.m, d1, d2, true, true,
+                                  point(rowz, VW, vx0, vx1, vx2, VW, gx, gz0, true, true, sh.psix[3], sh.psix[3], 3,
+                                        sh.psiz[3], sh.psiz[3], 3, true),
+                                  sh, a, cs);
             st_pair_rows(Fn[E2_SXZ], o0, sh.pitch, sxz);
         } else {
             // P += dt*L*Dx-Vx [x psi1] ; P += dt*L*Dz-Vz [z psi1]   (lib/waves.cpp:313-404)
@@ -603,60 +740,11 @@ struct ZmStep {
             for (int rr = 0; rr < 4; rr++)
 #pragma unroll
                 for (int c = 0; c < 2; c++) pp[rr][c] = so[R_P * G::SLAB + rr * SW + c];
-            blk_update<T, MODE>(pp, m.l, d1, d2, true, true, pml, sh, a, gx, gz0, sh.psix[1], sh.psix[1], 0, sh.psiz[1],
-                                sh.psiz[1], 0, true);
+            field_update<T, MODE>(special, pp, m.l, d1, d2, true, true,
+                                  point(rowx, VW, vz0, vz1, vz2, VW, gx, gz0, false, false, sh.psix[1], sh.psix[1], 0,
+                                        sh.psiz[1], sh.psiz[1], 0, true),
+                                  sh, a, cs);
             st_pair_rows(Fn[A2_P], o0, sh.pitch, pp);
-        }
-    }
-
-    // Normal stresses (lib/waves.cpp:1596-1674): d1 = Dx-Vx feeds Sxx with L2M and
-    // Szz with L and one x memory; d2 = Dz-Vz likewise with one z memory; free
-    // surface Szz = 0 on row lpml.
-    __device__ void normal_update(T (&sxx)[4][2], T (&szz)[4][2], const StrIn<T, PHYS> &m, const T (&d1)[4][2],
-                                  const T (&d2)[4][2], bool pml, const Shot2D<T> &sh, const Zm2DArgs<T> &a, int gx, int gz0)
-    {
-#pragma unroll
-        for (int rr = 0; rr < 4; rr++) {
-            const int iz = gz0 + rr;
-            const bool fsrow = sh.fs && iz == a.lpml;
-#pragma unroll
-            for (int j = 0; j < 2; j++) {
-                const int ix = gx + j;
-                const T a2 = A::mul(a.dt, m.l2m[rr][j]), a1 = A::mul(a.dt, m.l[rr][j]);
-                sxx[rr][j] = A::mad(sxx[rr][j], a2, d1[rr][j]);
-                szz[rr][j] = A::mad(szz[rr][j], a1, d1[rr][j]);
-                if (pml) {
-                    int xb, xc;
-                    const int xi = xstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, xb, xc);
-                    if (xi >= 0) {
-                        T *ps = sh.psix[2] + iz * 2 * a.lpml + xc;
-                        const T tA = __ldg(a.pml + (xb + PT_A) * a.lpml + xi), tB = __ldg(a.pml + (xb + PT_B) * a.lpml + xi),
-                                tC = __ldg(a.pml + (xb + PT_C) * a.lpml + xi);
-                        const T q = A::mad(A::mul(tB, *ps), tA, d1[rr][j]);
-                        *ps = q;
-                        const T cq = A::mad(q, tC, d1[rr][j]);
-                        sxx[rr][j] = A::msub(sxx[rr][j], a2, cq);
-                        szz[rr][j] = A::msub(szz[rr][j], a1, cq);
-                    }
-                }
-                sxx[rr][j] = A::mad(sxx[rr][j], a1, d2[rr][j]);
-                szz[rr][j] = A::mad(szz[rr][j], a2, d2[rr][j]);
-                if (pml) {
-                    int zb, zr;
-                    const int zi = zstrip_in(ix, iz, sh.nxp, sh.nzp, a.lpml, zb, zr);
-                    if (zi >= 0) {
-                        T *ps = sh.psiz[2] + zr * sh.nxp + ix;
-                        const T tA = __ldg(a.pml + (zb + PT_A) * a.lpml + zi), tB = __ldg(a.pml + (zb + PT_B) * a.lpml + zi),
-                                tC = __ldg(a.pml + (zb + PT_C) * a.lpml + zi);
-                        const T q = A::mad(A::mul(tB, *ps), tA, d2[rr][j]);
-                        *ps = q;
-                        const T cq = A::mad(q, tC, d2[rr][j]);
-                        sxx[rr][j] = A::msub(sxx[rr][j], a1, cq);
-                        szz[rr][j] = A::msub(szz[rr][j], a2, cq);
-                    }
-                }
-                if (fsrow) szz[rr][j] = T(0);
-            }
         }
     }
 

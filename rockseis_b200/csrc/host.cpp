@@ -246,10 +246,12 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     if (prec == PREC_F64 && tilecfg != TILECFG_64x32 && tilecfg != TILECFG_32x16) tilecfg = TILECFG_64x32;
     const TileShape ts = tile_shape_2d(tilecfg);
     const int lp = cfg.lpml;
-    // The fused z-marching step serves forward propagation (the forward operator;
-    // the acoustic adjoint is the forward operator run in reversed time).  The
-    // elastic adjoint steps and launch modes 1 and 2 use the per-tile kernels.
-    fused = (c->launch_mode == 0 || c->launch_mode == 3) && !adjoint_steps;
+    // The fused z-marching step (launch mode 3) serves forward propagation (the
+    // forward operator; the acoustic adjoint is the forward operator run in
+    // reversed time).  It is bit-identical to the per-tile kernels but measured
+    // slower on B200 (it issues as many instructions per point with a third of the
+    // resident warps), so the library's choice (mode 0) is the per-tile kernels.
+    fused = c->launch_mode == 3 && !adjoint_steps;
     const int ztx = zm_strip_width();
 
     // ---- per-shot layout (byte offsets into the arena)
