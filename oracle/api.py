@@ -120,6 +120,7 @@ def ref() -> C.CDLL:
         _ref.ref_revolve_adjust.argtypes = [I]
         _ref.ref_steps_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
         _ref.ref_steps_a2d_f.argtypes = [G, V, V, I, V, V, I, I, V]
+        _ref.ref_steps_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
     return _ref
 
 
@@ -451,3 +452,29 @@ def orc_interp(mode, data, o1, d1, n2, o2, d2):
     out = np.zeros((d.shape[0], n2), np.float32)
     assert oracle().orc_interp(mode, d.shape[0], d.shape[1], o1, d1, _p(d), n2, o2, d2, _p(out)) == 0
     return out
+
+
+def ref_modelling_e3d(pb, scoords, wav, sfield, gcoords, rfield):
+    """ModellingElastic3D<float>::run of the reference (traces [nrec][nt])."""
+    out = np.zeros((len(gcoords), pb.nt), np.float32)
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    vp, vs, rho, w = _keep(pb.vp, pb.vs, pb.rho, wav, dtype=np.float32)
+    r = ref().ref_mod_e3d_f(C.byref(g), _p(vp), _p(vs), _p(rho), len(sc), _p(sc), _p(w), sfield, len(gc), _p(gc),
+                            rfield, _p(out))
+    assert r == 1
+    return out
+
+
+def ref_steps_e3d(pb, scoords, wav, sfield, nsteps, state=None):
+    """The nine WavesElastic3D fields [9][nzp][nyp][nxp] after nsteps forward steps with
+    source injection, or (state given) after nsteps backwardstep* steps from it."""
+    shape = (9, pb.nz + 2 * pb.lpml, pb.ny + 2 * pb.lpml, pb.nx + 2 * pb.lpml)
+    st = np.zeros(shape, np.float32) if state is None else np.ascontiguousarray(state, np.float32).copy()
+    g = pb.ref_grid()
+    sc = np.ascontiguousarray(scoords, np.float64)
+    vp, vs, rho, w = _keep(pb.vp, pb.vs, pb.rho, wav, dtype=np.float32)
+    r = ref().ref_steps_e3d_f(C.byref(g), _p(vp), _p(vs), _p(rho), len(sc), _p(sc), _p(w), sfield, nsteps,
+                              0 if state is None else 1, _p(st))
+    assert r == 1
+    return st

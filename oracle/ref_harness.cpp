@@ -263,6 +263,41 @@ int steps_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns,
     return 1;
 }
 
+/* The nine WavesElastic3D fields after nsteps forward steps with source injection
+ * (or, with adjoint set, nsteps backwardstep* steps from the given state), in the
+ * order Vx, Vy, Vz, Sxx, Syy, Szz, Syz, Sxz, Sxy, each padded [nz][ny][nx]. */
+template <typename T>
+int steps_e3d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, const double *sc, const T *wav,
+              int sfield, int nsteps, int adjoint, T *state)
+{
+    auto model = make_e3d<T>(g, vp, vs, rho);
+    auto src = make_data3d<T>(ns, g, sc, sfield, SMAP, model->getGeom(), wav);
+    auto waves = std::make_shared<WavesElastic3D<T>>(model, g->nt, (T)g->dt, (T)0.0);
+    auto der = std::make_shared<Der<T>>(waves->getNx_pml(), waves->getNy_pml(), waves->getNz_pml(), waves->getDx(),
+                                        waves->getDy(), waves->getDz(), g->order);
+    waves->getPml()->setSmax(SMAX);
+    waves->getPml()->computeABC();
+    size_t n = (size_t)waves->getNx_pml() * waves->getNy_pml() * waves->getNz_pml();
+    T *f[9] = {waves->getVx(), waves->getVy(), waves->getVz(), waves->getSxx(), waves->getSyy(),
+               waves->getSzz(), waves->getSyz(), waves->getSxz(), waves->getSxy()};
+    if (adjoint) {
+        waves->setAdjoint();
+        for (int k = 0; k < 9; k++) std::memcpy(f[k], state + k * n, sizeof(T) * n);
+    }
+    for (int it = 0; it < nsteps; it++) {
+        if (adjoint) {
+            waves->backwardstepVelocity(model, der);
+            waves->backwardstepStress(model, der);
+        } else {
+            waves->forwardstepVelocity(model, der);
+            waves->forwardstepStress(model, der);
+            waves->insertSource(model, src, SMAP, it);
+        }
+    }
+    for (int k = 0; k < 9; k++) std::memcpy(state + k * n, f[k], sizeof(T) * n);
+    return 1;
+}
+
 template <typename T>
 int steps_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav, int sfield,
               int nsteps, T *state)
@@ -305,6 +340,9 @@ int ref_interp_f(int mode, int ntr, int n1, float o1, float d1, const float *in,
 int ref_steps_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                     const float *wav, int sfield, int nsteps, int adjoint, float *state)
 { return steps_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nsteps, adjoint, state); }
+int ref_steps_e3d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
+                    const float *wav, int sfield, int nsteps, int adjoint, float *state)
+{ return steps_e3d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nsteps, adjoint, state); }
 int ref_steps_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                     const float *wav, int sfield, int nsteps, float *state)
 { return steps_a2d<float>(g, vp, rho, ns, sc, wav, sfield, nsteps, state); }

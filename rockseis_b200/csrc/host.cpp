@@ -792,12 +792,9 @@ rsgpu_status rsgpu_plan_create(const rsgpu_config *cfg, int nshots, const rsgpu_
     if (!cfg) { set_error("null config"); return RSGPU_ERR_ARG; }
     auto h = std::unique_ptr<rsgpu_plan>(new rsgpu_plan);
     rsgpu_status st;
-    if (cfg->physics == RSGPU_ACOUSTIC3D) {
+    if (cfg->physics == RSGPU_ACOUSTIC3D || cfg->physics == RSGPU_ELASTIC3D) {
         h->p3.reset(new Plan3D());
         st = h->p3->create(cfg, nshots, shots);
-    } else if (cfg->physics == RSGPU_ELASTIC3D) {
-        set_error("elastic 3D propagation is not built");
-        st = RSGPU_ERR_UNSUPPORTED;
     } else {
         h->p.reset(new Plan());
         st = h->p->create(cfg, nshots, shots);

@@ -43,7 +43,8 @@ Plan3D::~Plan3D()
 rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
 {
     if (!c || !s || ns < 1) { set_error("null config/shots or nshots < 1"); return RSGPU_ERR_ARG; }
-    if (c->physics != RSGPU_ACOUSTIC3D) { set_error("Plan3D: physics %d is not acoustic 3D", c->physics); return RSGPU_ERR_UNSUPPORTED; }
+    if (c->physics != RSGPU_ACOUSTIC3D && c->physics != RSGPU_ELASTIC3D) { set_error("Plan3D: physics %d is not 3D", c->physics); return RSGPU_ERR_UNSUPPORTED; }
+    phys = c->physics == RSGPU_ELASTIC3D ? PHYS_E3D : PHYS_A3D;
     if (c->precision < 0 || c->precision > 2) { set_error("bad precision %d", c->precision); return RSGPU_ERR_ARG; }
     if (c->lpml < 1 || c->nt < 1 || !(c->dt > 0) || !(c->dx > 0) || !(c->dy > 0) || !(c->dz > 0)) {
         set_error("lpml, nt, dt, dx, dy, dz must be positive");
@@ -57,8 +58,13 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
             set_error("shot %d: padded grid smaller than stencil", i);
             return RSGPU_ERR_ARG;
         }
-        for (int k = 0; k < 4; k++)
+        for (int k = 0; k < np3(); k++)
             if (!sh.model[k]) { set_error("shot %d: model parameter %d is null", i, k); return RSGPU_ERR_ARG; }
+        if (phys == PHYS_E3D && sh.nrec > 0 && sh.rec_field == RSGPU_PRESSURE && !sh.rec_factor) {
+            set_error("shot %d: elastic 3D pressure receivers need rec_factor, (3*rho*vp^2 - 4*rho*vs^2)/3 at each "
+                      "receiver's map point (WavesElastic3D::recordData, lib/waves.cpp:4285)", i);
+            return RSGPU_ERR_ARG;
+        }
         if (sh.nsrc < 0 || sh.nrec < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
         if (sh.nsrc > 0 && (!sh.smap || !sh.sshift || !sh.wavelet)) { set_error("shot %d: source arrays missing", i); return RSGPU_ERR_ARG; }
         if (sh.nrec > 0 && (!sh.gmap || !sh.gshift)) { set_error("shot %d: receiver arrays missing", i); return RSGPU_ERR_ARG; }
@@ -93,8 +99,8 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         L.plane = (long long)L.pitch * L.rows;
         if ((long long)L.plane * 10 > 0x7fffffffLL) { set_error("shot %d: plane of %lld cells too large", i, L.plane); return RSGPU_ERR_ARG; }
         const size_t fbytes = (size_t)L.plane * L.planes * es;
-        for (int k = 0; k < 4; k++) L.f[k] = take(fbytes);
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < nf3(); k++) L.f[k] = take(fbytes);
+        for (int k = 0; k < npsi3(); k++) {
             L.psix[k] = take((size_t)L.nzp * L.nyp * 2 * lp * es);
             L.psiy[k] = take((size_t)L.nzp * 2 * lp * L.nxp * es);
             L.psiz[k] = take((size_t)2 * lp * L.nyp * L.nxp * es);
@@ -104,8 +110,9 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         L.nsrc = s[i].nsrc;
         L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
         L.state_end = off;
-        for (int k = 0; k < 4; k++) L.m[k] = take(fbytes);
+        for (int k = 0; k < np3(); k++) L.m[k] = take(fbytes);
         L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
+        L.rfac = take((size_t)std::max(1, s[i].nrec) * es);
     }
     // injection / recording plans (reference loop order: trace, z, y, x corner)
     std::vector<std::vector<long long>> inj_pt(ns), rec_pt(ns);
@@ -212,7 +219,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     rsgpu_status st;
     for (int i = 0; i < ns; i++) {
         const Layout3D &L = shots[i];
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < np3(); k++) {
             cudaMemcpy3DParms p = {};
             p.srcPtr = make_cudaPitchedPtr(const_cast<void *>(s[i].model[k]), (size_t)L.nxp * es, L.nxp, L.nyp);
             p.dstPtr = make_cudaPitchedPtr(A + L.m[k] + origin_bytes(L), (size_t)L.pitch * es, L.pitch, L.rows);
@@ -228,6 +235,11 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         if ((st = put_real(o_iw[i], inj_w[i])) != RSGPU_OK) return st;
         if ((st = put_raw(o_rp[i], rec_pt[i].data(), rec_pt[i].size() * 8)) != RSGPU_OK) return st;
         if ((st = put_real(o_rw[i], rec_w[i])) != RSGPU_OK) return st;
+        if (s[i].rec_factor && s[i].nrec > 0) {
+            std::vector<double> fac(s[i].nrec);
+            for (int t = 0; t < s[i].nrec; t++) fac[t] = shift_of(s[i].rec_factor, t);
+            if ((st = put_real(L.rfac, fac)) != RSGPU_OK) return st;
+        }
     }
     {
         std::vector<unsigned char> tab((size_t)12 * lp * es);
@@ -296,8 +308,9 @@ void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu
     Shot3D<T> d{};
     d.nxp = L.nxp; d.nyp = L.nyp; d.nzp = L.nzp; d.pitch = L.pitch; d.rows = L.rows;
     d.lpml = cfg.lpml; d.fs = cfg.fs; d.plane = L.plane;
-    for (int k = 0; k < 4; k++) { d.f[k] = (T *)(A + L.f[k] + org); d.m[k] = (const T *)(A + L.m[k] + org); }
-    for (int k = 0; k < 2; k++) {
+    for (int k = 0; k < nf3(); k++) d.f[k] = (T *)(A + L.f[k] + org);
+    for (int k = 0; k < np3(); k++) d.m[k] = (const T *)(A + L.m[k] + org);
+    for (int k = 0; k < npsi3(); k++) {
         d.psix[k] = (T *)(A + L.psix[k]);
         d.psiy[k] = (T *)(A + L.psiy[k]);
         d.psiz[k] = (T *)(A + L.psiz[k]);
@@ -319,6 +332,7 @@ void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu
     r.nt = cfg.nt;
     r.rev = reverse_time ? 1 : 0;
     r.rec_gate = gated_recording ? d_gate : nullptr;
+    r.rec_factor = (const T *)(A + L.rfac);
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -350,6 +364,13 @@ rsgpu_status Plan3D::step(int it)
     if (prec == PREC_F64) make_args3<double>(args, *this);
     else make_args3<float>(args, *this);
     cudaError_t e;
+    if (phys == PHYS_E3D) {
+        if ((e = launch_step_e3d(prec, 0, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_step_e3d(prec, 1, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_injrec_e3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream)) != cudaSuccess) goto fail;
+        launches += 3;
+        return RSGPU_OK;
+    }
     if ((e = launch_step_3d(prec, PHYS_A3D, 0, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
     if ((e = launch_step_3d(prec, PHYS_A3D, 1, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
     if ((e = launch_injrec_3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream)) != cudaSuccess) goto fail;
@@ -370,7 +391,8 @@ rsgpu_status Plan3D::set_recording(bool on)
 rsgpu_status Plan3D::inject_record_only(int it)
 {
     if (it < 0 || it >= cfg.nt) { set_error("step %d outside [0,%d)", it, cfg.nt); return RSGPU_ERR_ARG; }
-    cudaError_t e = launch_injrec_3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream);
+    cudaError_t e = phys == PHYS_E3D ? launch_injrec_e3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream)
+                                     : launch_injrec_3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream);
     if (e != cudaSuccess) { set_error("3D kernel launch failed: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
     launches += 1;
     return RSGPU_OK;
@@ -403,10 +425,12 @@ rsgpu_status Plan3D::read_traces(int shot, void *host_out)
 rsgpu_status Plan3D::read_field(int shot, int field, void *host_out)
 {
     if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
-    if (field < RSGPU_PRESSURE || field > RSGPU_VZ) { set_error("field %d not held by acoustic 3D", field); return RSGPU_ERR_ARG; }
+    // acoustic: PRESSURE, VX, VY, VZ = slots 0..3; elastic: VX..SXY (codes 1..9) = slots 0..8
+    const int slot = phys == PHYS_E3D ? field - 1 : field;
+    if (slot < 0 || slot >= nf3()) { set_error("field %d not held by this 3D physics", field); return RSGPU_ERR_ARG; }
     const Layout3D &L = shots[shot];
     cudaMemcpy3DParms p = {};
-    p.srcPtr = make_cudaPitchedPtr((char *)arena + L.f[field] + origin_bytes(L), (size_t)L.pitch * es, L.pitch, L.rows);
+    p.srcPtr = make_cudaPitchedPtr((char *)arena + L.f[slot] + origin_bytes(L), (size_t)L.pitch * es, L.pitch, L.rows);
     p.dstPtr = make_cudaPitchedPtr(host_out, (size_t)L.nxp * es, L.nxp, L.nyp);
     p.extent = make_cudaExtent((size_t)L.nxp * es, L.nyp, L.nzp);
     p.kind = cudaMemcpyDeviceToHost;

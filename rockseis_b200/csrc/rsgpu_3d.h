@@ -17,17 +17,23 @@ constexpr int TY3 = 8;    // y rows per CTA
 
 enum { A3_P = 0, A3_VX = 1, A3_VY = 2, A3_VZ = 3 };
 enum { M3_RX = 0, M3_RY = 1, M3_RZ = 2, M3_L = 3 };
+// Elastic 3D field slots (the reference's rs_field codes minus one) and parameters
+// (the rsgpu_shot.model order: ModelElastic3D::staggerModels, lib/model.cpp:3371).
+enum { E3_VX = 0, E3_VY = 1, E3_VZ = 2, E3_SXX = 3, E3_SYY = 4, E3_SZZ = 5, E3_SYZ = 6, E3_SXZ = 7, E3_SXY = 8 };
+enum { ME_RX = 0, ME_RY = 1, ME_RZ = 2, ME_L = 3, ME_L2M = 4, ME_MYZ = 5, ME_MXZ = 6, ME_MXY = 7 };
 
 template <typename T>
 struct Shot3D {
     int nxp, nyp, nzp, pitch;
     int rows, lpml, fs, pad_;
     long long plane;          // elements per plane
-    T *f[4];                  // P, Vx, Vy, Vz
-    const T *m[4];            // Rx, Ry, Rz, L
-    // C-PML memory, [0] velocity step (P derivatives), [1] stress step (Vx, Vy, Vz derivatives):
-    //   x [nzp][nyp][2L], y [nzp][2L][nxp], z [2L][nyp][nxp]
-    T *psix[2], *psiy[2], *psiz[2];
+    T *f[9];                  // acoustic: P, Vx, Vy, Vz; elastic: E3_* slots
+    const T *m[8];            // acoustic: Rx, Ry, Rz, L; elastic: ME_* slots
+    // C-PML memory per face pair, x [nzp][nyp][2L], y [nzp][2L][nxp], z [2L][nyp][nxp].
+    // Acoustic: [0] velocity step (P derivatives), [1] stress step.  Elastic: [0..2]
+    // the velocity step's Vx, Vy, Vz updates, [3] the normal stresses, [4] Sxz (x, z),
+    // Syz (y) ... see fd3d_elastic.cu for the assignment of each update.
+    T *psix[6], *psiy[6], *psiz[6];
 };
 
 // One CTA: a TX3 x TY3 column block of one shot, marching planes [z0, z0 + zc).
@@ -70,12 +76,20 @@ struct InjRec3 {
     int nt;
     int rev;                   // 1: step it reads wav[nt-1-it] and writes rec_out[nt-1-it]
     const int *rec_gate;       // if non-null, recording happens only while *rec_gate != 0
+    const T *rec_factor;       // elastic pressure: per-receiver divisor (3*rho*vp^2 - 4*rho*vs^2)/3
 };
 enum { INJ3_NONE = 0, INJ3_P = 1, INJ3_VX = 2, INJ3_VY = 3, INJ3_VZ = 4 };
 enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4 };
 
 cudaError_t launch_step_3d(int prec, int physics, int half, const void *args, const void *coefs, int grid,
                            cudaStream_t st);
+// Elastic 3D half-steps (fd3d_elastic.cu); adj selects backwardstepVelocity/Stress.
+cudaError_t launch_step_e3d(int prec, int half, int adj, const void *args, const void *coefs, int grid,
+                            cudaStream_t st);
+// Elastic 3D injection then recording (one CTA per shot); factor: per-receiver
+// divisor of the pressure recording.
+cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
+                              cudaStream_t st);
 cudaError_t launch_injrec_3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
                              cudaStream_t st);
 

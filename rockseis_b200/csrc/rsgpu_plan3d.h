@@ -13,8 +13,8 @@ struct Layout3D {
     int nxp = 0, nyp = 0, nzp = 0, pitch = 0, rows = 0, planes = 0;
     long long plane = 0;
     int nrec = 0, nsrc = 0;
-    size_t f[4] = {}, m[4] = {}, psix[2] = {}, psiy[2] = {}, psiz[2] = {};
-    size_t psi_end = 0, traces = 0, state_end = 0, wav = 0;
+    size_t f[9] = {}, m[8] = {}, psix[6] = {}, psiy[6] = {}, psiz[6] = {};
+    size_t psi_end = 0, traces = 0, state_end = 0, wav = 0, rfac = 0;
 };
 
 class Plan3D {
@@ -29,15 +29,21 @@ public:
     size_t origin_bytes(const Layout3D &L) const;
     rsgpu_status inject_record_only(int it);   // injection/recording of step it without propagation
 
+    // fields, parameters and C-PML memory arrays per face pair of the physics
+    int nf3() const { return phys == PHYS_E3D ? 9 : 4; }
+    int np3() const { return phys == PHYS_E3D ? 8 : 4; }
+    int npsi3() const { return phys == PHYS_E3D ? 6 : 2; }
+
     // options read by create()
     bool reverse_time = false;                 // wavelet/trace index nt-1-it at step it
+    bool adjoint_steps = false;                // elastic: propagate with backwardstep* (adjoint kernels)
     bool gated_recording = false;              // recording obeys set_recording()
     rsgpu_status set_recording(bool on);
     int *d_gate = nullptr;                     // recording switch (gated_recording)
     cudaStream_t shared_stream = nullptr;      // run on this caller-owned stream
 
     rsgpu_config cfg{};
-    int prec = 0, nshots = 0, es = 4, zc = 64, ntiles = 0;
+    int prec = 0, phys = PHYS_A3D, nshots = 0, es = 4, zc = 64, ntiles = 0;
     std::vector<Layout3D> shots;
     std::vector<size_t> rec_pt_offsets;        // per shot: arena offset of the receiver points (long long, -1 off grid)
     void *arena = nullptr, *d_meta = nullptr;

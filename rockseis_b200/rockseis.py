@@ -386,7 +386,23 @@ def make_shot(model: _Model, source: Data2D, rec: Data2D | None, keep: list) -> 
             fac = reciprocity_factor(model, rec)
             keep.append(fac)
             s.rec_factor = ptr(fac)
+        if model.physics == abi.ELASTIC3D and rec.field == abi.PRESSURE:
+            fac = pressure_factor_3d(model, rec)
+            keep.append(fac)
+            s.rec_factor = ptr(fac)
     return s
+
+
+def pressure_factor_3d(model: _Model, rec: Data2D) -> np.ndarray:
+    """(3*R*Vp*Vp - 4*R*Vs*Vs)/3 at each receiver's map point, evaluated in double
+    and stored in T: the divisor of WavesElastic3D::recordData's pressure
+    (lib/waves.cpp:4285)."""
+    fac = np.ones(rec.ntrace, model.dtype)
+    for i, (mx, my, mz) in enumerate(rec.gmap):
+        if mx >= 0 and my >= 0 and mz >= 0:
+            r, vp, vs = (float(a[mz, my, mx]) for a in (model.R, model.Vp, model.Vs))
+            fac[i] = (3.0 * r * vp * vp - 4.0 * r * vs * vs) / 3.0
+    return fac
 
 
 def reciprocity_factor(model: _Model, rec: Data2D) -> np.ndarray:
@@ -452,6 +468,11 @@ class ModellingElastic2D(_Modelling):
 
 class ModellingAcoustic3D(_Modelling):
     physics_name = "ModellingAcoustic3D"
+
+
+class ModellingElastic3D(_Modelling):
+    """ModellingElastic3D<T>::run (lib/modelling.cpp:727-850)."""
+    physics_name = "ModellingElastic3D"
 
 
 def modelling_batch(models, sources, receivers, order, precision=abi.F32_EXACT, tile=-1, launch_mode=0, zchunk=0):

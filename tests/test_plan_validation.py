@@ -34,7 +34,7 @@ def _create(cfg, shots, n=None):
     (lambda cfg, s: setattr(cfg, "lpml", 0), abi.ERR_ARG),
     (lambda cfg, s: setattr(cfg, "physics", 7), abi.ERR_ARG),
     (lambda cfg, s: setattr(cfg, "precision", 5), abi.ERR_ARG),
-    (lambda cfg, s: setattr(cfg, "physics", abi.ELASTIC3D), abi.ERR_UNSUPPORTED),
+    (lambda cfg, s: setattr(cfg, "physics", abi.ELASTIC3D), abi.ERR_ARG),     # a 2D batch lacks the 3D arrays
     (lambda cfg, s: setattr(s[1], "nx", 0), abi.ERR_ARG),                  # empty window
     (lambda cfg, s: (setattr(cfg, "lpml", 1), setattr(s[0], "nx", 2), setattr(s[0], "nz", 2)), abi.ERR_ARG),
     (lambda cfg, s: s[0].model.__setitem__(1, None), abi.ERR_ARG),         # missing parameter array
