@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define RSGPU_ABI_VERSION 1
+#define RSGPU_ABI_VERSION 2
 
 typedef enum {
     RSGPU_OK = 0,
@@ -211,14 +211,17 @@ typedef struct {
 } rsgpu_adjoint_opts;
 
 /* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332),
- * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545) or FwiElastic2D::run_optimal
- * (lib/fwi.cpp:3937-4143).  `shot` carries the padded model, the source
- * (wavelet, SMAP maps) and the receiver maps (GMAP) exactly as for
- * rsgpu_modelling.  Acoustic: src_field and rec_field are RSGPU_PRESSURE.
- * Elastic: shot.rec_field is RSGPU_PRESSURE (the P data set) and the Ux/Uz sets
- * (VX/VZ maps of the same receivers) are given by the *_vx / *_vz members; the
- * reference requires all three data sets.  Every output is ACCUMULATED (+=) and
- * may be NULL when not wanted. */
+ * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545), FwiElastic2D::run_optimal
+ * (lib/fwi.cpp:3937-4143) or FwiElastic3D::run_optimal (lib/fwi.cpp:6770-6990).
+ * `shot` carries the padded model, the source (wavelet, SMAP maps) and the
+ * receiver maps (GMAP) exactly as for rsgpu_modelling.  Acoustic: src_field and
+ * rec_field are RSGPU_PRESSURE.  Elastic 2D: shot.rec_field is RSGPU_PRESSURE (the
+ * P data set) and the Ux/Uz sets (VX/VZ maps of the same receivers) are given by
+ * the *_vx / *_vz members.  Elastic 3D: the shot's own receiver set is the Ux set
+ * (shot.rec_field RSGPU_VX: data, shot.rec_out, datares), the Uy and Uz sets are
+ * the *_vy and *_vz members (same trace count); vpgrad, vsgrad, rhograd and the
+ * models are [nz][ny][nx].  The reference requires every data set.  Every output
+ * is ACCUMULATED (+=) and may be NULL when not wanted. */
 typedef struct {
     rsgpu_shot shot;      /* shot.rec_out: FWI modelled data (datamodP), nrec*nt */
     const void *vp;       /* FWI: unpadded vp, nz*nx (ModelAcoustic2D::getVp) */
@@ -238,11 +241,17 @@ typedef struct {
     void *vsgrad;                          /* nz*nx */
     void *datamod_vx, *datamod_vz;         /* modelled Ux / Uz data */
     void *datares_vx, *datares_vz;         /* Ux / Uz residuals */
+    /* elastic 3D only: the Uy data set */
+    const int *gmap_vy;
+    const void *gshift_vy;
+    const void *data_vy;
+    void *datamod_vy, *datares_vy;
 } rsgpu_adjoint_shot;
 
-/* FwiAcoustic2D<float>::run_optimal (cfg->physics RSGPU_ACOUSTIC2D) or
- * FwiElastic2D<float>::run_optimal (RSGPU_ELASTIC2D) for a batch of shots
- * (DIFFERENCE misfit). */
+/* FwiAcoustic2D<float>::run_optimal (cfg->physics RSGPU_ACOUSTIC2D),
+ * FwiElastic2D<float>::run_optimal (RSGPU_ELASTIC2D), FwiAcoustic3D (RSGPU_ACOUSTIC3D)
+ * or FwiElastic3D<float>::run_optimal (RSGPU_ELASTIC3D, DIFFERENCE misfit) for a
+ * batch of shots. */
 rsgpu_status rsgpu_fwi_gradient(const rsgpu_config *cfg, const rsgpu_adjoint_opts *opts, int nshots,
                                 const rsgpu_adjoint_shot *shots);
 /* RtmAcoustic2D<float>::run_optimal (RSGPU_ACOUSTIC2D) or RtmAcoustic3D<float>::run_optimal

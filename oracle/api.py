@@ -102,6 +102,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+        _ref.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
@@ -349,6 +350,25 @@ def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
     r = fn(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
            _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]), _p(wg),
            _p(mods), _p(ress), C.byref(mis))
+    assert r == 1
+    out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
+    return out
+
+
+def ref_fwi_e3d(pb, scoords, wav, sfield, gcoords, obs3, ncheck):
+    """FwiElastic3D::run_optimal; obs3 = [Ux, Uy, Uz] observed data, each [nr][nt]."""
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    ns, nr = len(sc), len(gc)
+    out = {k: np.zeros((pb.nz, pb.ny, pb.nx), np.float32) for k in ("vpgrad", "vsgrad", "rhograd")}
+    wg = np.zeros((ns, pb.nt), np.float32)
+    mods = np.zeros((3, nr, pb.nt), np.float32)
+    ress = np.zeros((3, nr, pb.nt), np.float32)
+    mis = C.c_double()
+    vp, vs, rho, w, ox, oy, oz = _keep(pb.vp, pb.vs, pb.rho, wav, obs3[0], obs3[1], obs3[2], dtype=np.float32)
+    r = ref().ref_fwi_e3d_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(ox),
+                            _p(oy), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]),
+                            _p(wg), _p(mods), _p(ress), C.byref(mis))
     assert r == 1
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out

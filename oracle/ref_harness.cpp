@@ -230,6 +230,55 @@ int fwi_a3d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     return r;
 }
 
+/* FwiElastic3D::run_optimal (lib/fwi.cpp:6770-6990), DIFFERENCE misfit: Ux, Uy and
+ * Uz data of nr receivers (one coordinate set for all three), every gradient set. */
+template <typename T>
+int fwi_e3d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, const double *sc, const T *wav,
+            int sfield, int nr, const double *gc, const T *obsx, const T *obsy, const T *obsz, int ncheck,
+            T *vpgrad, T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit)
+{
+    auto model = make_e3d<T>(g, vp, vs, rho);
+    auto geom = model->getGeom();
+    auto src = make_data3d<T>(ns, g, sc, sfield, SMAP, geom, wav);
+    auto dx = make_data3d<T>(nr, g, gc, VX, GMAP, geom, obsx);
+    auto dy = make_data3d<T>(nr, g, gc, VY, GMAP, geom, obsy);
+    auto dz = make_data3d<T>(nr, g, gc, VZ, GMAP, geom, obsz);
+    const int fields[3] = {VX, VY, VZ};
+    std::shared_ptr<Data3D<T>> dm[3], dr[3];
+    for (int k = 0; k < 3; k++) {
+        dm[k] = make_data3d<T>(nr, g, gc, fields[k], GMAP, geom, nullptr);
+        dr[k] = make_data3d<T>(nr, g, gc, fields[k], GMAP, geom, nullptr);
+    }
+    auto wg = make_data3d<T>(ns, g, sc, sfield, SMAP, geom, nullptr);
+    std::shared_ptr<Image3D<T>> img[3];
+    for (int k = 0; k < 3; k++) {
+        img[k] = std::make_shared<Image3D<T>>(g->nx, g->ny, g->nz, 1, 1, 1, (T)g->dx, (T)g->dy, (T)g->dz, (T)g->ox,
+                                              (T)g->oy, (T)g->oz);
+        img[k]->allocateImage();
+    }
+    FwiElastic3D<T> fwi(model, src, dx, dy, dz, g->order, 1);
+    fwi.setDatamodUx(dm[0]); fwi.setDatamodUy(dm[1]); fwi.setDatamodUz(dm[2]);
+    fwi.setDataresUx(dr[0]); fwi.setDataresUy(dr[1]); fwi.setDataresUz(dr[2]);
+    fwi.setVpgrad(img[0]); fwi.setVsgrad(img[1]); fwi.setRhograd(img[2]);
+    fwi.setWavgrad(wg);
+    fwi.setMisfit_type(DIFFERENCE);
+    fwi.setNcheck(ncheck);
+    fwi.setIncore(true);
+    fwi.setSnapfile(tmpname("fwie3d"));
+    int r = fwi.run_optimal();
+    size_t n = (size_t)g->nx * g->ny * g->nz, nd = (size_t)nr * g->nt;
+    std::memcpy(vpgrad, img[0]->getImagedata(), sizeof(T) * n);
+    std::memcpy(vsgrad, img[1]->getImagedata(), sizeof(T) * n);
+    std::memcpy(rhograd, img[2]->getImagedata(), sizeof(T) * n);
+    std::memcpy(wavgrad, wg->getData(), sizeof(T) * (size_t)ns * g->nt);
+    for (int k = 0; k < 3; k++) {
+        std::memcpy(mods + k * nd, dm[k]->getData(), sizeof(T) * nd);
+        std::memcpy(ress + k * nd, dr[k]->getData(), sizeof(T) * nd);
+    }
+    *misfit = (double)fwi.getMisfit();
+    return r;
+}
+
 /* nsteps of forwardstepVelocity / forwardstepStress / insertSource on a fresh
  * wavefield, state copied out field by field (step-level parity). */
 template <typename T>
@@ -508,6 +557,14 @@ int ref_fwi_a3d_corr_f(const ref_grid *g, const float *vp, const float *rho, int
 {
     return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
                           misfit, 1);
+}
+int ref_fwi_e3d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
+                  const float *wav, int sfield, int nr, const double *gc, const float *obsx, const float *obsy,
+                  const float *obsz, int ncheck, float *vpgrad, float *vsgrad, float *rhograd, float *wavgrad,
+                  float *mods, float *ress, double *misfit)
+{
+    return fwi_e3d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsx, obsy, obsz, ncheck, vpgrad, vsgrad,
+                          rhograd, wavgrad, mods, ress, misfit);
 }
 int ref_fwi_e2d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                   const float *wav, int sfield, int nr, const double *gc, const float *obsp, const float *obsx,

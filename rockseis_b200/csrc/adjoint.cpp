@@ -595,7 +595,7 @@ rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_o
     *adj = nullptr;
     std::unique_ptr<rsgpu_adjoint> h(new rsgpu_adjoint);
     rsgpu_status st;
-    if (cfg && cfg->physics == RSGPU_ACOUSTIC3D) {
+    if (cfg && (cfg->physics == RSGPU_ACOUSTIC3D || cfg->physics == RSGPU_ELASTIC3D)) {
         h->a3.reset(new Adjoint3D());
         st = h->a3->create(cfg, opts, kind, nshots, shots);
     } else {

@@ -19,27 +19,12 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "adjoint_ops.cuh"
 #include "rsgpu_adjoint.h"
 #include "rsgpu_kernels.h"
 
 namespace rsgpu {
 namespace {
-
-template <typename T> struct X;   // explicitly rounded operations of the element type
-template <> struct X<float> {
-    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
-    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
-    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
-    static __device__ __forceinline__ float rnd(double a) { return __double2float_rn(a); }
-};
-template <> struct X<double> {
-    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
-    static __device__ __forceinline__ double rnd(double a) { return a; }
-};
 
 // ---------------------------------------------------------------- FWI gradient correlation
 // vpgrad -= (-2/vp) * Pfw * (dx- Vx_adj + dz- Vz_adj)
@@ -408,13 +393,6 @@ __global__ void __launch_bounds__(256) residual_corr_e2d(const Resid2DE<T> *desc
 }
 
 // ---------------------------------------------------------------- elastic FWI
-// 0.5 * w * r * dd / h  in double, rounded to T (the reference's mixed-type expression)
-template <typename T>
-__device__ __forceinline__ double half_term(T w, T r, T dd, double h)
-{
-    return __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(0.5, (double)w), (double)r), (double)dd), h);
-}
-
 // FwiElastic2D::crossCorr (lib/fwi.cpp:2591-2775) on the interior 1..n-2:
 //   g0 -= (Dx Vx_fw + Dz Vz_fw) (Sxx_bw + Szz_bw)                     (lambda)
 //   g1 += 2 (Dx Vx Szz + Dz Vz Sxx) - 1/4 sum of 4 Sxz corner products (mu)

@@ -1,5 +1,6 @@
-// RTM image and FWI gradient drivers for 3D acoustic shots (host runtime behind
-// rsgpu_rtm_image, rsgpu_fwi_gradient and rsgpu_adjoint_* for RSGPU_ACOUSTIC3D).
+// RTM image and FWI gradient drivers for 3D shots (host runtime behind
+// rsgpu_rtm_image, rsgpu_fwi_gradient and rsgpu_adjoint_* for RSGPU_ACOUSTIC3D and,
+// FWI only, RSGPU_ELASTIC3D).
 //
 // The reference's RtmAcoustic3D::run_optimal (lib/rtm.cpp:735-859) runs the same
 // Revolve-driven loop as the 2D drivers (FwiAcoustic3D::run_optimal,
@@ -7,9 +8,17 @@
 // `ncheck` slots, an adjoint propagator fed with the recorded data, and a
 // correlation of both pressures at every adjoint time level.  Here the forward and
 // adjoint wavefields of all shots are two batched 3D plans (z-marching kernels)
-// sharing one stream; the adjoint plan runs forward in reversed time.  Checkpoints
-// hold every shot's four wavefields (interior of the pitched arrays) and C-PML
-// memory, lossless or as FP16/BF16 with a power-of-two scale per block.
+// sharing one stream and one copy of the staggered parameters; the adjoint plan
+// runs forward in reversed time.  Checkpoints hold every shot's wavefields
+// (interior of the pitched arrays) and C-PML memory, lossless or as FP16/BF16 with
+// a power-of-two scale per block.
+//
+// FwiElastic3D::run_optimal (lib/fwi.cpp:6770-6990) is the same loop with the
+// elastic plans: the forward plan records the Ux, Uy and Uz data sets, the adjoint
+// plan (backwardstepVelocity / backwardstepStress kernels) injects the three
+// residuals at their receivers and records the wavelet gradient at the sources,
+// and the correlation is FwiElastic3D::crossCorr; scaleGrad follows the last
+// adjoint step.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -56,8 +65,14 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
                                const rsgpu_adjoint_shot *s)
 {
     if (!c || !o || !s || ns < 1) { set_error("null config/options/shots or nshots < 1"); return RSGPU_ERR_ARG; }
-    if (c->physics != RSGPU_ACOUSTIC3D || (k_ != RSGPU_KIND_RTM && k_ != RSGPU_KIND_FWI)) {
-        set_error("the 3D adjoint driver is built for acoustic RTM images and FWI gradients");
+    const bool el = c->physics == RSGPU_ELASTIC3D;
+    if ((c->physics != RSGPU_ACOUSTIC3D && !el) || (k_ != RSGPU_KIND_RTM && k_ != RSGPU_KIND_FWI) ||
+        (el && k_ != RSGPU_KIND_FWI)) {
+        set_error("the 3D adjoint driver is built for acoustic RTM images and FWI gradients and elastic FWI gradients");
+        return RSGPU_ERR_UNSUPPORTED;
+    }
+    if (el && o->misfit != RSGPU_MISFIT_DIFFERENCE) {
+        set_error("elastic 3D: misfit %d: DIFFERENCE is built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION) {
@@ -86,9 +101,18 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     }
     for (int i = 0; i < ns; i++) {
         const rsgpu_shot &sh = s[i].shot;
-        if (sh.src_field != RSGPU_PRESSURE || sh.rec_field != RSGPU_PRESSURE) {
-            set_error("shot %d: the acoustic RTM driver takes pressure sources and receivers", i);
+        if (!el && (sh.src_field != RSGPU_PRESSURE || sh.rec_field != RSGPU_PRESSURE)) {
+            set_error("shot %d: the acoustic 3D drivers take pressure sources and receivers", i);
             return RSGPU_ERR_UNSUPPORTED;
+        }
+        if (el && sh.rec_field != RSGPU_VX) {
+            set_error("shot %d: elastic 3D FWI: the shot's receiver set is the Ux (RSGPU_VX) data set", i);
+            return RSGPU_ERR_ARG;
+        }
+        if (el && (!s[i].gmap_vy || !s[i].gshift_vy || !s[i].data_vy || !s[i].gmap_vz || !s[i].gshift_vz ||
+                   !s[i].data_vz || !s[i].vs)) {
+            set_error("shot %d: elastic 3D FWI needs the Uy and Uz data sets (maps, shifts, data) and vs", i);
+            return RSGPU_ERR_ARG;
         }
         if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
         if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
@@ -101,6 +125,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         return RSGPU_ERR_NODEVICE;
     }
     kind = k_;
+    phys = el ? PHYS_E3D : PHYS_A3D;
     cfg = *c;
     nshots = ns;
     prec = c->precision;
@@ -132,19 +157,56 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         bs[i].gshift = s[i].shot.sshift;
         bs[i].rec_out = nullptr;
     }
+    // elastic: the forward plan records Ux, Uy and Uz; the adjoint plan injects the
+    // three residuals and records the wavelet gradient at sources inside the
+    // interior 1..n-2 of every axis (crossCorr records it inside its interior loop)
+    std::vector<ShotSets> fsets, bsets;
+    std::vector<std::vector<int>> wmaps(ns);
+    if (el) {
+        fsets.resize(ns);
+        bsets.resize(ns);
+        for (int i = 0; i < ns; i++) {
+            const rsgpu_adjoint_shot &a = s[i];
+            const int nr = a.shot.nrec;
+            ShotSets &F = fsets[i], &B = bsets[i];
+            F.nsrc = 1;
+            F.src[0] = {a.shot.nsrc, a.shot.smap, a.shot.sshift, a.shot.src_field, a.shot.wavelet, nullptr, false};
+            F.nrec = 3;
+            F.rec[0] = {nr, a.shot.gmap, a.shot.gshift, RSGPU_VX, nullptr, nullptr, false};
+            F.rec[1] = {nr, a.gmap_vy, a.gshift_vy, RSGPU_VY, nullptr, nullptr, false};
+            F.rec[2] = {nr, a.gmap_vz, a.gshift_vz, RSGPU_VZ, nullptr, nullptr, false};
+            B.nsrc = 3;
+            B.src[0] = {nr, a.shot.gmap, a.shot.gshift, RSGPU_VX, a.data, nullptr, false};
+            B.src[1] = {nr, a.gmap_vy, a.gshift_vy, RSGPU_VY, a.data_vy, nullptr, false};
+            B.src[2] = {nr, a.gmap_vz, a.gshift_vz, RSGPU_VZ, a.data_vz, nullptr, false};
+            std::vector<int> &wm = wmaps[i];
+            wm.assign(a.shot.smap, a.shot.smap + 3 * a.shot.nsrc);
+            for (int t = 0; t < a.shot.nsrc; t++) {
+                const int *m = &wm[3 * t];
+                if (m[0] < 1 || m[0] > a.shot.nx - 2 || m[1] < 1 || m[1] > a.shot.ny - 2 || m[2] < 1 ||
+                    m[2] > a.shot.nz - 2)
+                    wm[3 * t] = wm[3 * t + 1] = wm[3 * t + 2] = -1;
+            }
+            B.nrec = 1;
+            B.rec[0] = {a.shot.nsrc, wm.data(), a.shot.sshift, a.shot.src_field, nullptr, nullptr, false};
+            B.rec[0].at_point = true;
+        }
+    }
     fw.reset(new Plan3D());
     fw->shared_stream = stream;
     fw->gated_recording = fwi();
-    ST(fw->create(c, ns, fs.data()));
+    ST(fw->create(c, ns, fs.data(), el ? fsets.data() : nullptr));
     bw.reset(new Plan3D());
     bw->shared_stream = stream;
     bw->reverse_time = true;
-    ST(bw->create(c, ns, bs.data()));
+    bw->adjoint_steps = el;
+    bw->share_params = fw.get();
+    ST(bw->create(c, ns, bs.data(), el ? bsets.data() : nullptr));
 
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off = rupa(off + std::max<size_t>(bytes, 1), 256); return r; };
-    for (auto *v : {&o_img, &o_vp, &o_rho, &o_obs, &o_g1, &o_valid}) v->assign(ns, 0);
+    for (auto *v : {&o_img, &o_vp, &o_rho, &o_obs, &o_g1, &o_valid, &o_vs, &o_obsy, &o_obsz, &o_g2}) v->assign(ns, 0);
     nx.resize(ns); ny.resize(ns); nz.resize(ns); nrec.resize(ns);
     for (int i = 0; i < ns; i++) {
         nx[i] = s[i].shot.nx; ny[i] = s[i].shot.ny; nz[i] = s[i].shot.nz; nrec[i] = s[i].shot.nrec;
@@ -158,11 +220,19 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
             o_obs[i] = take((size_t)nrec[i] * cfg.nt * es);
             o_g1[i] = take(n3 * gs);
             o_valid[i] = take(sizeof(int) * nrec[i]);
+            if (el) {
+                o_vs[i] = take(n3 * es);
+                o_obsy[i] = take((size_t)nrec[i] * cfg.nt * es);
+                o_obsz[i] = take((size_t)nrec[i] * cfg.nt * es);
+                o_g2[i] = take(n3 * gs);
+            }
         }
     }
-    const size_t corr_bytes = fwi() ? (prec == PREC_F64 ? sizeof(Corr3DF<double>) : sizeof(Corr3DF<float>))
+    const size_t corr_bytes = el ? (prec == PREC_F64 ? sizeof(Corr3DE<double>) : sizeof(Corr3DE<float>))
+                            : fwi() ? (prec == PREC_F64 ? sizeof(Corr3DF<double>) : sizeof(Corr3DF<float>))
                                     : (prec == PREC_F64 ? sizeof(Corr3D<double>) : sizeof(Corr3D<float>));
-    const size_t res_bytes = prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>);
+    const size_t res_bytes = el ? (prec == PREC_F64 ? sizeof(Resid3E<double>) : sizeof(Resid3E<float>))
+                                : (prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>));
     o_corr = take(corr_bytes * ns);
     o_res = take(res_bytes * ns);
     o_misfit = take(sizeof(double) * ns);
@@ -179,9 +249,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
             segs.push_back(g);
         };
         const int l2 = 2 * cfg.lpml;
-        for (int f = 0; f < 4; f++)
+        for (int f = 0; f < fw->nf3(); f++)
             add(L.f[f] + fw->origin_bytes(L), L.nyp * L.nzp, L.nxp, L.pitch, L.nyp, L.plane);
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < fw->npsi3(); k++) {
             add(L.psix[k], L.nzp * L.nyp, l2, l2, 0, 0);
             add(L.psiy[k], L.nzp * l2, L.nxp, L.nxp, 0, 0);
             add(L.psiz[k], l2 * L.nyp, L.nxp, L.nxp, 0, 0);
@@ -210,6 +280,11 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         CU(cudaMemcpyAsync(D(o_vp[i]), s[i].vp, n3 * es, cudaMemcpyHostToDevice, stream));
         CU(cudaMemcpyAsync(D(o_rho[i]), s[i].rho, n3 * es, cudaMemcpyHostToDevice, stream));
         CU(cudaMemcpyAsync(D(o_obs[i]), s[i].data, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        if (el) {
+            CU(cudaMemcpyAsync(D(o_vs[i]), s[i].vs, n3 * es, cudaMemcpyHostToDevice, stream));
+            CU(cudaMemcpyAsync(D(o_obsy[i]), s[i].data_vy, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+            CU(cudaMemcpyAsync(D(o_obsz[i]), s[i].data_vz, (size_t)nrec[i] * cfg.nt * es, cudaMemcpyHostToDevice, stream));
+        }
         // misfit mask: a receiver counts when its map lies on the grid (lib/fwi.cpp:1500)
         std::vector<int> &valid = valids[i];
         valid.resize(nrec[i]);
@@ -219,7 +294,50 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
         CU(cudaMemcpyAsync(D(o_valid[i]), valid.data(), sizeof(int) * valid.size(), cudaMemcpyHostToDevice, stream));
     }
-    for (int i = 0; i < ns && fwi(); i++) {
+    for (int i = 0; i < ns && el; i++) {
+        const Layout3D &F = fw->shots[i], &B = bw->shots[i];
+        char *fa = (char *)fw->arena, *ba = (char *)bw->arena;
+        const size_t fo = fw->origin_bytes(F), bo = bw->origin_bytes(B);
+        auto fill = [&](auto *d, auto *r) {
+            using T = typename std::remove_const<typename std::remove_pointer<decltype(d->rx)>::type>::type;
+            for (int k = 0; k < 9; k++) {
+                d->ws[k] = (const T *)(fa + F.f[k] + fo);
+                d->wr[k] = (const T *)(ba + B.f[k] + bo);
+            }
+            d->rx = (const T *)fw->param_base(i, ME_RX);
+            d->ry = (const T *)fw->param_base(i, ME_RY);
+            d->rz = (const T *)fw->param_base(i, ME_RZ);
+            d->vp = (const T *)D(o_vp[i]);
+            d->vs = (const T *)D(o_vs[i]);
+            d->rho = (const T *)D(o_rho[i]);
+            d->g[0] = D(o_img[i]);
+            d->g[1] = D(o_g1[i]);
+            d->g[2] = D(o_g2[i]);
+            d->nx = nx[i]; d->ny = ny[i]; d->nz = nz[i]; d->pitch = F.pitch; d->lpml = cfg.lpml; d->plane = F.plane;
+            const size_t obs[3] = {o_obs[i], o_obsy[i], o_obsz[i]};
+            for (int k = 0; k < 3; k++) {
+                r->mod[k] = (const T *)(fa + F.tracesk[k]);
+                r->obs[k] = (const T *)D(obs[k]);
+                r->res[k] = (T *)(ba + B.wavk[k]);
+            }
+            r->nrec = nrec[i];
+            r->nt = cfg.nt;
+        };
+        if (prec == PREC_F64) {
+            Corr3DE<double> d{};
+            Resid3E<double> r{};
+            fill(&d, &r);
+            std::memcpy(corr.data() + i * sizeof d, &d, sizeof d);
+            std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+        } else {
+            Corr3DE<float> d{};
+            Resid3E<float> r{};
+            fill(&d, &r);
+            std::memcpy(corr.data() + i * sizeof d, &d, sizeof d);
+            std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+        }
+    }
+    for (int i = 0; i < ns && fwi() && !el; i++) {
         const Layout3D &F = fw->shots[i], &B = bw->shots[i];
         char *fa = (char *)fw->arena, *ba = (char *)bw->arena;
         const size_t fo = fw->origin_bytes(F), bo = bw->origin_bytes(B);
@@ -229,9 +347,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
             d->wrx = (const T *)(ba + B.f[A3_VX] + bo);
             d->wry = (const T *)(ba + B.f[A3_VY] + bo);
             d->wrz = (const T *)(ba + B.f[A3_VZ] + bo);
-            d->rx = (const T *)(fa + F.m[M3_RX] + fo);
-            d->ry = (const T *)(fa + F.m[M3_RY] + fo);
-            d->rz = (const T *)(fa + F.m[M3_RZ] + fo);
+            d->rx = (const T *)fw->param_base(i, M3_RX);
+            d->ry = (const T *)fw->param_base(i, M3_RY);
+            d->rz = (const T *)fw->param_base(i, M3_RZ);
             d->vp = (const T *)D(o_vp[i]);
             d->rho = (const T *)D(o_rho[i]);
             d->g0 = D(o_img[i]);
@@ -298,8 +416,9 @@ rsgpu_status Adjoint3D::slot_io(bool save, int slot)
 
 rsgpu_status Adjoint3D::correlate()
 {
-    cudaError_t e = fwi() ? launch_corr_fwi_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, cfg.dx, cfg.dy, cfg.dz, stream)
-                          : launch_corr_rtm_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, nhx, nhy, nhz, stream);
+    cudaError_t e = elastic() ? launch_corr_fwi_e3d(prec, acc, D(o_corr), nshots, nxmax, nymax, cfg.dx, cfg.dy, cfg.dz, stream)
+                    : fwi()   ? launch_corr_fwi_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, cfg.dx, cfg.dy, cfg.dz, stream)
+                              : launch_corr_rtm_a3d(prec, acc, D(o_corr), nshots, nxmax, nymax, nhx, nhy, nhz, stream);
     if (e != cudaSuccess) { set_error("correlation launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
     launches += 1;
     return RSGPU_OK;
@@ -317,6 +436,7 @@ rsgpu_status Adjoint3D::run()
     for (int i = 0; i < nshots; i++) {
         CU(cudaMemsetAsync(D(o_img[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * nhx * nhy * nhz * gs, stream));
         if (fwi()) CU(cudaMemsetAsync(D(o_g1[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * gs, stream));
+        if (elastic()) CU(cudaMemsetAsync(D(o_g2[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * gs, stream));
     }
     if (fwi()) ST(fw->set_recording(true));
     RevolveSchedule rev(nt, ncheck);
@@ -336,7 +456,8 @@ rsgpu_status Adjoint3D::run()
             fw_steps += 1;
             if (fwi()) {
                 ST(fw->set_recording(false));
-                cudaError_t e = misfit_type == RSGPU_MISFIT_CORRELATION
+                cudaError_t e = elastic() ? launch_residual_e3d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
+                                : misfit_type == RSGPU_MISFIT_CORRELATION
                                     ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit),
                                                            stream, false)
                                     : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
@@ -355,6 +476,11 @@ rsgpu_status Adjoint3D::run()
             set_error("revolve schedule error (info %d)", rev.info());
             return RSGPU_ERR_REVOLVE;
         }
+    }
+    if (elastic()) {
+        cudaError_t e = launch_scale_grad_e3d(prec, acc, D(o_corr), nshots, nxmax, nymax, stream);
+        if (e != cudaSuccess) { set_error("scaleGrad launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+        launches += 1;
     }
     launches += fw->launches + bw->launches - l0;
     CU(cudaStreamSynchronize(stream));
@@ -395,17 +521,27 @@ rsgpu_status Adjoint3D::read(int ns, const rsgpu_adjoint_shot *s)
         for (int i = 0; i < nshots; i++) {
             const size_t n3 = (size_t)nx[i] * ny[i] * nz[i];
             if (s[i].vpgrad) ST(add_from(s[i].vpgrad, o_img[i], n3));
-            if (s[i].rhograd) ST(add_from(s[i].rhograd, o_g1[i], n3));
-            if (s[i].shot.rec_out) ST(fw->read_traces(i, s[i].shot.rec_out));
+            if (elastic()) {
+                if (s[i].vsgrad) ST(add_from(s[i].vsgrad, o_g1[i], n3));
+                if (s[i].rhograd) ST(add_from(s[i].rhograd, o_g2[i], n3));
+            } else if (s[i].rhograd) {
+                ST(add_from(s[i].rhograd, o_g1[i], n3));
+            }
+            if (s[i].shot.rec_out) ST(fw->read_traces(i, s[i].shot.rec_out, 0));
+            if (elastic() && s[i].datamod_vy) ST(fw->read_traces(i, s[i].datamod_vy, 1));
+            if (elastic() && s[i].datamod_vz) ST(fw->read_traces(i, s[i].datamod_vz, 2));
             if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
-            if (s[i].datares) {
+            void *res_out[3] = {s[i].datares, elastic() ? s[i].datares_vy : nullptr,
+                                elastic() ? s[i].datares_vz : nullptr};
+            for (int k = 0; k < 3; k++) {
+                if (!res_out[k]) continue;
                 const size_t n = (size_t)nrec[i] * cfg.nt;
                 tmp.resize(n * es);
-                CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wav, n * es, cudaMemcpyDeviceToHost,
-                                   stream));
+                CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wavk[k], n * es,
+                                   cudaMemcpyDeviceToHost, stream));
                 CU(cudaStreamSynchronize(stream));
-                if (es == 8) { double *h = (double *)s[i].datares; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) h[k] += t[k]; }
-                else { float *h = (float *)s[i].datares; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) h[k] += t[k]; }
+                if (es == 8) { double *h = (double *)res_out[k]; const double *t = (const double *)tmp.data(); for (size_t j = 0; j < n; j++) h[j] += t[j]; }
+                else { float *h = (float *)res_out[k]; const float *t = (const float *)tmp.data(); for (size_t j = 0; j < n; j++) h[j] += t[j]; }
             }
             if (s[i].misfit) {
                 if (acc == ACC_REF && es == 4) *s[i].misfit = (double)(float)((float)*s[i].misfit + (float)mis[i]);

@@ -469,15 +469,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress(Step3DArgs<T> a, const
 }
 
 // ---------------------------------------------------------------- sources and receivers
-// One CTA per shot: injection (lib/waves.cpp:4104-4244) then, after a barrier,
-// recording (lib/waves.cpp:4247-4400) of the same step.
+// One CTA per shot: injection of every source set (lib/waves.cpp:4104-4244), then,
+// after a barrier, recording of every receiver set (lib/waves.cpp:4247-4400) of
+// the same step.
 template <typename T, int MODE>
-__global__ void inject_record_e3d(const Shot3D<T> *shots, const InjRec3<T> *plans, T dt, int it)
+__device__ void inject_set(const Shot3D<T> &sh, const InjRec3<T> &pl, T dt, int it)
 {
     using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
-    const Shot3D<T> &sh = shots[blockIdx.x];
-    const InjRec3<T> &pl = plans[blockIdx.x];
-    it = pl.rev ? pl.nt - 1 - it : it;
     if (pl.kind_inj == INJ3_P) {
         // Sxx, Syy, Szz -= dt*wav*xtri*ytri*ztri
         for (int q = threadIdx.x; q < pl.ninj; q += blockDim.x) {
@@ -507,13 +505,30 @@ __global__ void inject_record_e3d(const Shot3D<T> *shots, const InjRec3<T> *plan
             F[p] = v;
         }
     }
+}
+
+template <typename T, int MODE>
+__device__ void record_set(const Shot3D<T> &sh, const InjRec3<T> &pl, int it)
+{
+    using A = Ar<T, MODE == MODE_FAST ? MODE_FAST : MODE_IEEE>;
     if (pl.kind_rec == REC3_NONE || (pl.rec_gate && *pl.rec_gate == 0)) return;
-    __syncthreads();
     for (int tr = threadIdx.x; tr < pl.nrec; tr += blockDim.x) {
         const long long p = pl.rec_pt[tr];
         if (p < 0) continue;
-        const T *w = pl.rec_w + 6 * tr;
         T *out = pl.rec_out + (long long)tr * pl.nt + it;
+        if (pl.kind_rec >= REC3_WG_P) {
+            // wavelet gradient, assigned: 1.0*(Sxx + Syy + Szz) or 0.5*(v + v[-1]) in double
+            if (pl.kind_rec == REC3_WG_P) {
+                *out = A::add(A::add(sh.f[E3_SXX][p], sh.f[E3_SYY][p]), sh.f[E3_SZZ][p]);
+            } else {
+                const int k = pl.kind_rec - REC3_WG_VX;
+                const long long step = k == 0 ? 1 : k == 1 ? (long long)sh.pitch : sh.plane;
+                const T *F = sh.f[E3_VX + k];
+                *out = (T)__dmul_rn(0.5, (double)A::add(F[p], F[p - step]));
+            }
+            continue;
+        }
+        const T *w = pl.rec_w + 6 * tr;
         T acc = *out;
         if (pl.kind_rec == REC3_P) {
             // (1./3.)*xtri*ytri*ztri*F/factor in double, added to the T-typed sample, for
@@ -539,6 +554,20 @@ __global__ void inject_record_e3d(const Shot3D<T> *shots, const InjRec3<T> *plan
         }
         *out = acc;
     }
+}
+
+template <typename T, int MODE>
+__global__ void inject_record_e3d(const Shot3D<T> *shots, const InjRec3<T> *plans, int nsets, T dt, int it0)
+{
+    const Shot3D<T> &sh = shots[blockIdx.x];
+    const InjRec3<T> *pl = plans + (long long)blockIdx.x * nsets;
+    const int it = pl[0].rev ? pl[0].nt - 1 - it0 : it0;
+    for (int k = 0; k < nsets; k++) {
+        if (k) __syncthreads();
+        inject_set<T, MODE>(sh, pl[k], dt, it);
+    }
+    __syncthreads();
+    for (int k = 0; k < nsets; k++) record_set<T, MODE>(sh, pl[k], it);
 }
 
 template <typename T, int MODE, bool ADJ>
@@ -577,18 +606,20 @@ cudaError_t launch_step_e3d(int prec, int half, int adj, const void *args, const
                : step_e3<float, MODE_FAST, false>(half, args, coefs, grid, st);
 }
 
-cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
-                              cudaStream_t st)
+cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, int nsets, double dt,
+                              int it, cudaStream_t st)
 {
     if (prec == PREC_F64)
         inject_record_e3d<double, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot3D<double> *)shots,
-                                                                     (const InjRec3<double> *)plans, dt, it);
+                                                                     (const InjRec3<double> *)plans, nsets, dt, it);
     else if (prec == PREC_F32_EXACT)
         inject_record_e3d<float, MODE_IEEE><<<nshots, 256, 0, st>>>((const Shot3D<float> *)shots,
-                                                                    (const InjRec3<float> *)plans, (float)dt, it);
+                                                                    (const InjRec3<float> *)plans, nsets, (float)dt,
+                                                                    it);
     else
         inject_record_e3d<float, MODE_FAST><<<nshots, 256, 0, st>>>((const Shot3D<float> *)shots,
-                                                                    (const InjRec3<float> *)plans, (float)dt, it);
+                                                                    (const InjRec3<float> *)plans, nsets, (float)dt,
+                                                                    it);
     return cudaGetLastError();
 }
 

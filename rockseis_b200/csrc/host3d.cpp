@@ -40,7 +40,7 @@ Plan3D::~Plan3D()
     if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
-rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
+rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, const ShotSets *sets)
 {
     if (!c || !s || ns < 1) { set_error("null config/shots or nshots < 1"); return RSGPU_ERR_ARG; }
     if (c->physics != RSGPU_ACOUSTIC3D && c->physics != RSGPU_ELASTIC3D) { set_error("Plan3D: physics %d is not 3D", c->physics); return RSGPU_ERR_UNSUPPORTED; }
@@ -60,16 +60,53 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
         }
         for (int k = 0; k < np3(); k++)
             if (!sh.model[k]) { set_error("shot %d: model parameter %d is null", i, k); return RSGPU_ERR_ARG; }
-        if (phys == PHYS_E3D && sh.nrec > 0 && sh.rec_field == RSGPU_PRESSURE && !sh.rec_factor) {
-            set_error("shot %d: elastic 3D pressure receivers need rec_factor, (3*rho*vp^2 - 4*rho*vs^2)/3 at each "
-                      "receiver's map point (WavesElastic3D::recordData, lib/waves.cpp:4285)", i);
-            return RSGPU_ERR_ARG;
-        }
         if (sh.nsrc < 0 || sh.nrec < 0) { set_error("shot %d: negative trace count", i); return RSGPU_ERR_ARG; }
         if (sh.nsrc > 0 && (!sh.smap || !sh.sshift || !sh.wavelet)) { set_error("shot %d: source arrays missing", i); return RSGPU_ERR_ARG; }
         if (sh.nrec > 0 && (!sh.gmap || !sh.gshift)) { set_error("shot %d: receiver arrays missing", i); return RSGPU_ERR_ARG; }
         if (sh.src_field < RSGPU_PRESSURE || sh.src_field > RSGPU_VZ) { set_error("shot %d: bad source field", i); return RSGPU_ERR_ARG; }
         if (sh.nrec > 0 && (sh.rec_field < RSGPU_PRESSURE || sh.rec_field > RSGPU_VZ)) { set_error("shot %d: bad receiver field", i); return RSGPU_ERR_ARG; }
+    }
+    nsets = phys == PHYS_E3D ? MAXSETS : 1;
+    // the effective trace sets of every shot
+    std::vector<ShotSets> eff(ns);
+    for (int i = 0; i < ns; i++) {
+        ShotSets &e = eff[i];
+        if (sets) {
+            e = sets[i];
+        } else {
+            e.nsrc = 1;
+            e.src[0] = {s[i].nsrc, s[i].smap, s[i].sshift, s[i].src_field, s[i].wavelet, nullptr, false};
+            e.nrec = 1;
+            e.rec[0] = {s[i].nrec, s[i].gmap, s[i].gshift, s[i].rec_field, nullptr, s[i].rec_factor, false};
+        }
+        if (e.nsrc < 0 || e.nrec < 0 || e.nsrc > nsets || e.nrec > nsets) {
+            set_error("shot %d: %d source and %d receiver sets (at most %d)", i, e.nsrc, e.nrec, nsets);
+            return RSGPU_ERR_ARG;
+        }
+        for (int k = 0; k < e.nsrc; k++) {
+            const TraceSet &t = e.src[k];
+            if (t.n < 0 || (t.n > 0 && (!t.map || !t.shift || !t.data)) || t.field < RSGPU_PRESSURE || t.field > RSGPU_VZ) {
+                set_error("shot %d: source set %d is malformed", i, k);
+                return RSGPU_ERR_ARG;
+            }
+        }
+        for (int k = 0; k < e.nrec; k++) {
+            const TraceSet &t = e.rec[k];
+            if (t.n < 0 || (t.n > 0 && (!t.map || !t.shift)) || t.field < RSGPU_PRESSURE || t.field > RSGPU_VZ ||
+                (t.at_point && phys != PHYS_E3D)) {
+                set_error("shot %d: receiver set %d is malformed", i, k);
+                return RSGPU_ERR_ARG;
+            }
+            if (phys == PHYS_E3D && t.n > 0 && t.field == RSGPU_PRESSURE && !t.at_point && !t.factor) {
+                set_error("shot %d: elastic 3D pressure receivers need rec_factor, (3*rho*vp^2 - 4*rho*vs^2)/3 at "
+                          "each receiver's map point (WavesElastic3D::recordData, lib/waves.cpp:4285)", i);
+                return RSGPU_ERR_ARG;
+            }
+        }
+    }
+    if (share_params && (share_params->nshots != ns || share_params->phys != phys || share_params->prec != c->precision)) {
+        set_error("plans sharing parameters must hold the same shots");
+        return RSGPU_ERR_ARG;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
@@ -106,18 +143,32 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
             L.psiz[k] = take((size_t)2 * lp * L.nyp * L.nxp * es);
         }
         L.psi_end = off;
-        L.nrec = s[i].nrec;
-        L.nsrc = s[i].nsrc;
-        L.traces = take((size_t)std::max(1, s[i].nrec) * cfg.nt * es);
+        const ShotSets &e = eff[i];
+        L.nsrcsets = e.nsrc;
+        L.nrecsets = e.nrec;
+        for (int k = 0; k < e.nrec; k++) {
+            L.nrecs[k] = e.rec[k].n;
+            L.tracesk[k] = take((size_t)std::max(1, e.rec[k].n) * cfg.nt * es);
+        }
         L.state_end = off;
-        for (int k = 0; k < np3(); k++) L.m[k] = take(fbytes);
-        L.wav = take((size_t)std::max(1, s[i].nsrc) * cfg.nt * es);
-        L.rfac = take((size_t)std::max(1, s[i].nrec) * es);
+        if (!share_params)
+            for (int k = 0; k < np3(); k++) L.m[k] = take(fbytes);
+        for (int k = 0; k < e.nsrc; k++) {
+            L.nsrcs[k] = e.src[k].n;
+            L.wavk[k] = take((size_t)std::max(1, e.src[k].n) * cfg.nt * es);
+        }
+        for (int k = 0; k < e.nrec; k++) L.rfack[k] = take((size_t)std::max(1, e.rec[k].n) * es);
+        L.nrec = L.nrecs[0];
+        L.nsrc = L.nsrcs[0];
+        L.traces = L.tracesk[0];
+        L.wav = L.wavk[0];
+        L.rfac = L.rfack[0];
     }
-    // injection / recording plans (reference loop order: trace, z, y, x corner)
-    std::vector<std::vector<long long>> inj_pt(ns), rec_pt(ns);
-    std::vector<std::vector<int>> inj_start(ns), inj_tr(ns);
-    std::vector<std::vector<double>> inj_w(ns), rec_w(ns);
+    // injection / recording plans per (shot, set) (reference loop order: trace, z, y, x corner)
+    const int nps = ns * nsets;
+    std::vector<std::vector<long long>> inj_pt(nps), rec_pt(nps);
+    std::vector<std::vector<int>> inj_start(nps), inj_tr(nps);
+    std::vector<std::vector<double>> inj_w(nps), rec_w(nps);
     auto shift_of = [&](const void *p, int k) -> double {
         return prec == PREC_F64 ? ((const double *)p)[k] : (double)((const float *)p)[k];
     };
@@ -127,69 +178,82 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     };
     for (int i = 0; i < ns; i++) {
         const Layout3D &L = shots[i];
-        struct W3 { double v[3]; };
-        std::map<long long, std::vector<std::pair<int, W3>>> per_pt;
-        std::vector<long long> order_pts;
-        for (int t = 0; t < s[i].nsrc; t++) {
-            const int mx = s[i].smap[3 * t], my = s[i].smap[3 * t + 1], mz = s[i].smap[3 * t + 2];
-            if (mx < 0 || my < 0 || mz < 0) continue;
-            double xt[2], yt[2], zt[2];
-            tri(shift_of(s[i].sshift, 3 * t), xt);
-            tri(shift_of(s[i].sshift, 3 * t + 1), yt);
-            tri(shift_of(s[i].sshift, 3 * t + 2), zt);
-            for (int i1 = 0; i1 < 2; i1++)
-                for (int i2 = 0; i2 < 2; i2++)
-                    for (int i3 = 0; i3 < 2; i3++) {
-                        const int ix = lp + mx + i3, iy = lp + my + i2, iz = lp + mz + i1;
-                        if (ix >= L.nxp || iy >= L.nyp || iz >= L.nzp) {
-                            set_error("shot %d: source %d maps outside the grid", i, t);
-                            return RSGPU_ERR_ARG;
+        const ShotSets &e = eff[i];
+        for (int k = 0; k < e.nsrc; k++) {
+            const TraceSet &t = e.src[k];
+            const int j = i * nsets + k;
+            struct W3 { double v[3]; };
+            std::map<long long, std::vector<std::pair<int, W3>>> per_pt;
+            std::vector<long long> order_pts;
+            for (int tr = 0; tr < t.n; tr++) {
+                const int mx = t.map[3 * tr], my = t.map[3 * tr + 1], mz = t.map[3 * tr + 2];
+                if (mx < 0 || my < 0 || mz < 0) continue;
+                double xt[2], yt[2], zt[2];
+                tri(shift_of(t.shift, 3 * tr), xt);
+                tri(shift_of(t.shift, 3 * tr + 1), yt);
+                tri(shift_of(t.shift, 3 * tr + 2), zt);
+                for (int i1 = 0; i1 < 2; i1++)
+                    for (int i2 = 0; i2 < 2; i2++)
+                        for (int i3 = 0; i3 < 2; i3++) {
+                            const int ix = lp + mx + i3, iy = lp + my + i2, iz = lp + mz + i1;
+                            if (ix >= L.nxp || iy >= L.nyp || iz >= L.nzp) {
+                                set_error("shot %d: source %d of set %d maps outside the grid", i, tr, k);
+                                return RSGPU_ERR_ARG;
+                            }
+                            const long long p = iz * L.plane + (long long)iy * L.pitch + ix;
+                            if (!per_pt.count(p)) order_pts.push_back(p);
+                            per_pt[p].push_back({tr, W3{{xt[i3], yt[i2], zt[i1]}}});
                         }
-                        const long long p = iz * L.plane + (long long)iy * L.pitch + ix;
-                        if (!per_pt.count(p)) order_pts.push_back(p);
-                        per_pt[p].push_back({t, W3{{xt[i3], yt[i2], zt[i1]}}});
-                    }
+            }
+            inj_start[j].push_back(0);
+            for (long long p : order_pts) {
+                inj_pt[j].push_back(p);
+                for (auto &cw : per_pt[p]) {
+                    inj_tr[j].push_back(cw.first);
+                    for (int q = 0; q < 3; q++) inj_w[j].push_back(cw.second.v[q]);
+                }
+                inj_start[j].push_back((int)inj_tr[j].size());
+            }
         }
-        inj_start[i].push_back(0);
-        for (long long p : order_pts) {
-            inj_pt[i].push_back(p);
-            for (auto &cw : per_pt[p]) {
-                inj_tr[i].push_back(cw.first);
-                for (int k = 0; k < 3; k++) inj_w[i].push_back(cw.second.v[k]);
-            }
-            inj_start[i].push_back((int)inj_tr[i].size());
-        }
-        for (int t = 0; t < s[i].nrec; t++) {
-            const int mx = s[i].gmap[3 * t], my = s[i].gmap[3 * t + 1], mz = s[i].gmap[3 * t + 2];
-            if (mx < 0 || my < 0 || mz < 0) {
-                rec_pt[i].push_back(-1);
-                for (int k = 0; k < 6; k++) rec_w[i].push_back(0);
-                continue;
-            }
-            if (lp + mx + 1 >= L.nxp || lp + my + 1 >= L.nyp || lp + mz + 1 >= L.nzp) {
-                set_error("shot %d: receiver %d maps outside the grid", i, t);
-                return RSGPU_ERR_ARG;
-            }
-            rec_pt[i].push_back((long long)(lp + mz) * L.plane + (long long)(lp + my) * L.pitch + lp + mx);
-            double w[2];
-            for (int k = 0; k < 3; k++) {
-                tri(shift_of(s[i].gshift, 3 * t + k), w);
-                rec_w[i].push_back(w[0]);
-                rec_w[i].push_back(w[1]);
+        for (int k = 0; k < e.nrec; k++) {
+            const TraceSet &t = e.rec[k];
+            const int j = i * nsets + k;
+            for (int tr = 0; tr < t.n; tr++) {
+                const int mx = t.map[3 * tr], my = t.map[3 * tr + 1], mz = t.map[3 * tr + 2];
+                if (mx < 0 || my < 0 || mz < 0) {
+                    rec_pt[j].push_back(-1);
+                    for (int q = 0; q < 6; q++) rec_w[j].push_back(0);
+                    continue;
+                }
+                if (lp + mx + 1 >= L.nxp || lp + my + 1 >= L.nyp || lp + mz + 1 >= L.nzp) {
+                    set_error("shot %d: receiver %d of set %d maps outside the grid", i, tr, k);
+                    return RSGPU_ERR_ARG;
+                }
+                rec_pt[j].push_back((long long)(lp + mz) * L.plane + (long long)(lp + my) * L.pitch + lp + mx);
+                double w[2];
+                for (int q = 0; q < 3; q++) {
+                    tri(shift_of(t.shift, 3 * tr + q), w);
+                    rec_w[j].push_back(w[0]);
+                    rec_w[j].push_back(w[1]);
+                }
             }
         }
     }
-    std::vector<size_t> o_ip(ns), o_is(ns), o_it(ns), o_iw(ns), o_rp(ns), o_rw(ns);
-    for (int i = 0; i < ns; i++) {
-        o_ip[i] = take(inj_pt[i].size() * 8);
-        o_is[i] = take(inj_start[i].size() * 4);
-        o_it[i] = take(inj_tr[i].size() * 4);
-        o_iw[i] = take(inj_w[i].size() * es);
-        o_rp[i] = take(rec_pt[i].size() * 8);
-        o_rw[i] = take(rec_w[i].size() * es);
+    std::vector<SetTables> tabs(nps);
+    for (int j = 0; j < nps; j++) {
+        SetTables &t = tabs[j];
+        t.ip = take(inj_pt[j].size() * 8);
+        t.is = take(std::max<size_t>(1, inj_start[j].size()) * 4);
+        t.it = take(inj_tr[j].size() * 4);
+        t.iw = take(inj_w[j].size() * es);
+        t.rp = take(rec_pt[j].size() * 8);
+        t.rw = take(rec_w[j].size() * es);
+        t.ninj = (int)inj_pt[j].size();
+        t.nrec = (int)rec_pt[j].size();
     }
     const size_t o_pml = take((size_t)12 * lp * es);
-    rec_pt_offsets = o_rp;
+    rec_pt_offsets.assign(nps, 0);
+    for (int j = 0; j < nps; j++) rec_pt_offsets[j] = tabs[j].rp;
     arena_bytes = off;
     if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -219,7 +283,8 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     rsgpu_status st;
     for (int i = 0; i < ns; i++) {
         const Layout3D &L = shots[i];
-        for (int k = 0; k < np3(); k++) {
+        const ShotSets &e = eff[i];
+        for (int k = 0; k < np3() && !share_params; k++) {
             cudaMemcpy3DParms p = {};
             p.srcPtr = make_cudaPitchedPtr(const_cast<void *>(s[i].model[k]), (size_t)L.nxp * es, L.nxp, L.nyp);
             p.dstPtr = make_cudaPitchedPtr(A + L.m[k] + origin_bytes(L), (size_t)L.pitch * es, L.pitch, L.rows);
@@ -227,19 +292,26 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
             p.kind = cudaMemcpyHostToDevice;
             CU(cudaMemcpy3DAsync(&p, stream));
         }
-        if (s[i].nsrc > 0)
-            CU(cudaMemcpyAsync(A + L.wav, s[i].wavelet, (size_t)s[i].nsrc * cfg.nt * es, cudaMemcpyHostToDevice, stream));
-        if ((st = put_raw(o_ip[i], inj_pt[i].data(), inj_pt[i].size() * 8)) != RSGPU_OK) return st;
-        if ((st = put_raw(o_is[i], inj_start[i].data(), inj_start[i].size() * 4)) != RSGPU_OK) return st;
-        if ((st = put_raw(o_it[i], inj_tr[i].data(), inj_tr[i].size() * 4)) != RSGPU_OK) return st;
-        if ((st = put_real(o_iw[i], inj_w[i])) != RSGPU_OK) return st;
-        if ((st = put_raw(o_rp[i], rec_pt[i].data(), rec_pt[i].size() * 8)) != RSGPU_OK) return st;
-        if ((st = put_real(o_rw[i], rec_w[i])) != RSGPU_OK) return st;
-        if (s[i].rec_factor && s[i].nrec > 0) {
-            std::vector<double> fac(s[i].nrec);
-            for (int t = 0; t < s[i].nrec; t++) fac[t] = shift_of(s[i].rec_factor, t);
-            if ((st = put_real(L.rfac, fac)) != RSGPU_OK) return st;
+        for (int k = 0; k < e.nsrc; k++)
+            if (e.src[k].n > 0)
+                CU(cudaMemcpyAsync(A + L.wavk[k], e.src[k].data, (size_t)e.src[k].n * cfg.nt * es,
+                                   cudaMemcpyHostToDevice, stream));
+        for (int k = 0; k < nsets; k++) {
+            const int j = i * nsets + k;
+            const SetTables &t = tabs[j];
+            if ((st = put_raw(t.ip, inj_pt[j].data(), inj_pt[j].size() * 8)) != RSGPU_OK) return st;
+            if ((st = put_raw(t.is, inj_start[j].data(), inj_start[j].size() * 4)) != RSGPU_OK) return st;
+            if ((st = put_raw(t.it, inj_tr[j].data(), inj_tr[j].size() * 4)) != RSGPU_OK) return st;
+            if ((st = put_real(t.iw, inj_w[j])) != RSGPU_OK) return st;
+            if ((st = put_raw(t.rp, rec_pt[j].data(), rec_pt[j].size() * 8)) != RSGPU_OK) return st;
+            if ((st = put_real(t.rw, rec_w[j])) != RSGPU_OK) return st;
         }
+        for (int k = 0; k < e.nrec; k++)
+            if (e.rec[k].factor && e.rec[k].n > 0) {
+                std::vector<double> fac(e.rec[k].n);
+                for (int t = 0; t < e.rec[k].n; t++) fac[t] = shift_of(e.rec[k].factor, t);
+                if ((st = put_real(L.rfack[k], fac)) != RSGPU_OK) return st;
+            }
     }
     {
         std::vector<unsigned char> tab((size_t)12 * lp * es);
@@ -267,7 +339,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     std::memcpy(coefs.data() + 2 * half, cy.data(), half);
     const size_t shot_bytes = prec == PREC_F64 ? sizeof(Shot3D<double>) : sizeof(Shot3D<float>);
     const size_t ir_bytes = prec == PREC_F64 ? sizeof(InjRec3<double>) : sizeof(InjRec3<float>);
-    const size_t m_shots = 0, m_ir = rup3(ns * shot_bytes, 256), m_tiles = rup3(m_ir + ns * ir_bytes, 256);
+    const size_t m_shots = 0, m_ir = rup3(ns * shot_bytes, 256), m_tiles = rup3(m_ir + (size_t)nps * ir_bytes, 256);
     const size_t m_coef = rup3(m_tiles + tiles.size() * sizeof(Tile3D), 256);
     const size_t m_gate = rup3(m_coef + coefs.size(), 256), m_end = m_gate + 256;
     CU(cudaMalloc(&d_meta, m_end));
@@ -275,12 +347,16 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s)
     std::vector<unsigned char> meta(m_end, 0);
     reinterpret_cast<int *>(meta.data() + m_gate)[0] = 1;   // recording on
     for (int i = 0; i < ns; i++) {
-        if (prec == PREC_F64) fill_desc<double>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes,
-                                                i, s[i], o_ip[i], o_is[i], o_it[i], o_iw[i], o_rp[i], o_rw[i],
-                                                (int)inj_pt[i].size(), (int)rec_pt[i].size());
-        else fill_desc<float>(meta.data() + m_shots + i * shot_bytes, meta.data() + m_ir + i * ir_bytes, i, s[i],
-                              o_ip[i], o_is[i], o_it[i], o_iw[i], o_rp[i], o_rw[i], (int)inj_pt[i].size(),
-                              (int)rec_pt[i].size());
+        const ShotSets &e = eff[i];
+        if (prec == PREC_F64) fill_shot<double>(meta.data() + m_shots + i * shot_bytes, i);
+        else fill_shot<float>(meta.data() + m_shots + i * shot_bytes, i);
+        for (int k = 0; k < nsets; k++) {
+            const TraceSet none{};
+            const TraceSet &src = k < e.nsrc ? e.src[k] : none, &rec = k < e.nrec ? e.rec[k] : none;
+            unsigned char *irp = meta.data() + m_ir + (size_t)(i * nsets + k) * ir_bytes;
+            if (prec == PREC_F64) fill_set<double>(irp, i, k, src, rec, tabs[i * nsets + k]);
+            else fill_set<float>(irp, i, k, src, rec, tabs[i * nsets + k]);
+        }
     }
     std::memcpy(meta.data() + m_tiles, tiles.data(), tiles.size() * sizeof(Tile3D));
     std::memcpy(meta.data() + m_coef, coefs.data(), coefs.size());
@@ -298,9 +374,14 @@ size_t Plan3D::origin_bytes(const Layout3D &L) const
     return ((size_t)GUARD * L.plane + (size_t)GUARD * L.pitch + GUARD) * es;
 }
 
+const char *Plan3D::param_base(int i, int k) const
+{
+    const Plan3D &o = share_params ? *share_params : *this;
+    return (const char *)o.arena + o.shots[i].m[k] + o.origin_bytes(o.shots[i]);
+}
+
 template <typename T>
-void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu_shot &s, size_t o_ip, size_t o_is,
-                       size_t o_it, size_t o_iw, size_t o_rp, size_t o_rw, int ninj, int nrec)
+void Plan3D::fill_shot(unsigned char *sd, int i)
 {
     char *A = (char *)arena;
     const Layout3D &L = shots[i];
@@ -309,30 +390,37 @@ void Plan3D::fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu
     d.nxp = L.nxp; d.nyp = L.nyp; d.nzp = L.nzp; d.pitch = L.pitch; d.rows = L.rows;
     d.lpml = cfg.lpml; d.fs = cfg.fs; d.plane = L.plane;
     for (int k = 0; k < nf3(); k++) d.f[k] = (T *)(A + L.f[k] + org);
-    for (int k = 0; k < np3(); k++) d.m[k] = (const T *)(A + L.m[k] + org);
+    for (int k = 0; k < np3(); k++) d.m[k] = (const T *)param_base(i, k);
     for (int k = 0; k < npsi3(); k++) {
         d.psix[k] = (T *)(A + L.psix[k]);
         d.psiy[k] = (T *)(A + L.psiy[k]);
         d.psiz[k] = (T *)(A + L.psiz[k]);
     }
     std::memcpy(sd, &d, sizeof d);
+}
+
+template <typename T>
+void Plan3D::fill_set(unsigned char *irp, int i, int k, const TraceSet &src, const TraceSet &rec, const SetTables &t)
+{
+    char *A = (char *)arena;
+    const Layout3D &L = shots[i];
     InjRec3<T> r{};
-    r.ninj = ninj;
-    r.kind_inj = ninj > 0 ? INJ3_P + s.src_field : INJ3_NONE;    // PRESSURE, VX, VY, VZ -> 1..4
-    r.inj_pt = (const long long *)(A + o_ip);
-    r.inj_start = (const int *)(A + o_is);
-    r.inj_trace = (const int *)(A + o_it);
-    r.inj_w = (const T *)(A + o_iw);
-    r.wav = (const T *)(A + L.wav);
-    r.nrec = nrec;
-    r.kind_rec = nrec > 0 ? REC3_P + s.rec_field : REC3_NONE;
-    r.rec_pt = (const long long *)(A + o_rp);
-    r.rec_w = (const T *)(A + o_rw);
-    r.rec_out = (T *)(A + L.traces);
+    r.ninj = t.ninj;
+    r.kind_inj = t.ninj > 0 ? INJ3_P + src.field : INJ3_NONE;    // PRESSURE, VX, VY, VZ -> 1..4
+    r.inj_pt = (const long long *)(A + t.ip);
+    r.inj_start = (const int *)(A + t.is);
+    r.inj_trace = (const int *)(A + t.it);
+    r.inj_w = (const T *)(A + t.iw);
+    r.wav = (const T *)(A + (k < L.nsrcsets ? L.wavk[k] : L.wavk[0]));
+    r.nrec = t.nrec;
+    r.kind_rec = t.nrec > 0 ? (rec.at_point ? REC3_WG_P : REC3_P) + rec.field : REC3_NONE;
+    r.rec_pt = (const long long *)(A + t.rp);
+    r.rec_w = (const T *)(A + t.rw);
+    r.rec_out = (T *)(A + (k < L.nrecsets ? L.tracesk[k] : L.tracesk[0]));
     r.nt = cfg.nt;
     r.rev = reverse_time ? 1 : 0;
     r.rec_gate = gated_recording ? d_gate : nullptr;
-    r.rec_factor = (const T *)(A + L.rfac);
+    r.rec_factor = (const T *)(A + (k < L.nrecsets ? L.rfack[k] : L.rfack[0]));
     std::memcpy(irp, &r, sizeof r);
 }
 
@@ -367,7 +455,7 @@ rsgpu_status Plan3D::step(int it)
     if (phys == PHYS_E3D) {
         if ((e = launch_step_e3d(prec, 0, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
         if ((e = launch_step_e3d(prec, 1, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
-        if ((e = launch_injrec_e3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_injrec_e3d(prec, d_shots, d_injrec, nshots, nsets, cfg.dt, it, stream)) != cudaSuccess) goto fail;
         launches += 3;
         return RSGPU_OK;
     }
@@ -391,7 +479,7 @@ rsgpu_status Plan3D::set_recording(bool on)
 rsgpu_status Plan3D::inject_record_only(int it)
 {
     if (it < 0 || it >= cfg.nt) { set_error("step %d outside [0,%d)", it, cfg.nt); return RSGPU_ERR_ARG; }
-    cudaError_t e = phys == PHYS_E3D ? launch_injrec_e3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream)
+    cudaError_t e = phys == PHYS_E3D ? launch_injrec_e3d(prec, d_shots, d_injrec, nshots, nsets, cfg.dt, it, stream)
                                      : launch_injrec_3d(prec, d_shots, d_injrec, nshots, cfg.dt, it, stream);
     if (e != cudaSuccess) { set_error("3D kernel launch failed: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
     launches += 1;
@@ -408,14 +496,15 @@ rsgpu_status Plan3D::run(int it0, int nsteps)
     return RSGPU_OK;
 }
 
-rsgpu_status Plan3D::read_traces(int shot, void *host_out)
+rsgpu_status Plan3D::read_traces(int shot, void *host_out, int set)
 {
     if (shot < 0 || shot >= nshots) { set_error("bad shot %d", shot); return RSGPU_ERR_ARG; }
     const Layout3D &L = shots[shot];
-    if (L.nrec == 0) return RSGPU_OK;
-    const size_t n = (size_t)L.nrec * cfg.nt;
+    if (set < 0 || set >= std::max(1, L.nrecsets)) { set_error("bad receiver set %d", set); return RSGPU_ERR_ARG; }
+    if (set >= L.nrecsets || L.nrecs[set] == 0) return RSGPU_OK;
+    const size_t n = (size_t)L.nrecs[set] * cfg.nt;
     std::vector<unsigned char> tmp(n * es);
-    CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.traces, n * es, cudaMemcpyDeviceToHost, stream));
+    CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.tracesk[set], n * es, cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
     if (es == 8) { double *o = (double *)host_out; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
     else { float *o = (float *)host_out; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }

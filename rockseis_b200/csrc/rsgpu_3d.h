@@ -79,17 +79,22 @@ struct InjRec3 {
     const T *rec_factor;       // elastic pressure: per-receiver divisor (3*rho*vp^2 - 4*rho*vs^2)/3
 };
 enum { INJ3_NONE = 0, INJ3_P = 1, INJ3_VX = 2, INJ3_VY = 3, INJ3_VZ = 4 };
-enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4 };
+enum { REC3_NONE = 0, REC3_P = 1, REC3_VX = 2, REC3_VY = 3, REC3_VZ = 4,
+       // elastic 3D wavelet gradient (FwiElastic3D::crossCorr, lib/fwi.cpp:5217-5258):
+       // out[it] = value at the map point (rec_pt) of Sxx + Syy + Szz, or the average
+       // of the velocity and its lower neighbour along its own axis
+       REC3_WG_P = 5, REC3_WG_VX = 6, REC3_WG_VY = 7, REC3_WG_VZ = 8 };
 
 cudaError_t launch_step_3d(int prec, int physics, int half, const void *args, const void *coefs, int grid,
                            cudaStream_t st);
 // Elastic 3D half-steps (fd3d_elastic.cu); adj selects backwardstepVelocity/Stress.
 cudaError_t launch_step_e3d(int prec, int half, int adj, const void *args, const void *coefs, int grid,
                             cudaStream_t st);
-// Elastic 3D injection then recording (one CTA per shot); factor: per-receiver
-// divisor of the pressure recording.
-cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
-                              cudaStream_t st);
+// Elastic 3D injection then recording, one CTA per shot: plans[shot*nsets + k]
+// holds source set k and receiver set k; every set is injected, then every set
+// recorded.
+cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, int nsets, double dt,
+                              int it, cudaStream_t st);
 cudaError_t launch_injrec_3d(int prec, const void *shots, const void *plans, int nshots, double dt, int it,
                              cudaStream_t st);
 

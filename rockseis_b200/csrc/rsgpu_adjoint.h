@@ -60,6 +60,27 @@ struct Corr3DF {
     long long plane;
 };
 
+// Elastic 3D correlation inputs of one shot (FwiElastic3D::crossCorr and scaleGrad).
+template <typename T>
+struct Corr3DE {
+    const T *ws[9];             // forward Vx, Vy, Vz, Sxx, Syy, Szz, Syz, Sxz, Sxy (origins)
+    const T *wr[9];             // adjoint fields, same order
+    const T *rx, *ry, *rz;      // staggered inverse densities
+    const T *vp, *vs, *rho;     // unpadded models [nz][ny][nx]
+    void *g[3];                 // lambda -> vp, mu -> vs, rho gradients [nz][ny][nx]
+    int nx, ny, nz, pitch, lpml, pad_;
+    long long plane;
+};
+
+// Residuals of the three elastic 3D data types (Ux, Uy, Uz) of one shot.
+template <typename T>
+struct Resid3E {
+    const T *mod[3];
+    const T *obs[3];
+    T *res[3];
+    int nrec, nt;
+};
+
 // Residual and misfit of one shot (DIFFERENCE misfit).
 template <typename T>
 struct Resid2D {
@@ -108,6 +129,13 @@ cudaError_t launch_corr_rtm_a3d(int prec, int acc, const void *desc, int nshots,
                                 int nhy, int nhz, cudaStream_t st);
 cudaError_t launch_corr_fwi_a3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, double dx,
                                 double dy, double dz, cudaStream_t st);
+// Elastic 3D (adjoint3d_elastic.cu): FwiElastic3D::crossCorr of one adjoint step,
+// scaleGrad after the last one, and the DIFFERENCE residuals and misfit.
+cudaError_t launch_corr_fwi_e3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax, double dx,
+                                double dy, double dz, cudaStream_t st);
+cudaError_t launch_scale_grad_e3d(int prec, int acc, const void *desc, int nshots, int nxmax, int nymax,
+                                  cudaStream_t st);
+cudaError_t launch_residual_e3d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
 // Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
 // for the 16-bit formats (written by save, read by load).
 cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,

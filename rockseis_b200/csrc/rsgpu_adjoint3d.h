@@ -1,4 +1,5 @@
-// 3D RTM driver behind the rsgpu_adjoint handle (host runtime, not ABI).
+// 3D RTM image and FWI gradient drivers behind the rsgpu_adjoint handle (host
+// runtime, not ABI): acoustic RTM and FWI, elastic FWI.
 #pragma once
 #include <memory>
 #include <vector>
@@ -18,6 +19,7 @@ public:
     rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
 
     int kind = RSGPU_KIND_RTM, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
+    int phys = PHYS_A3D;
     int ncheck = 0, nxmax = 0, nymax = 0;
     int misfit_type = 0, nrec_max = 0;
     rsgpu_config cfg{};
@@ -27,9 +29,11 @@ public:
     size_t slot_elems = 0, ck_es = 4;
     std::vector<CkptSeg> segs;
     std::vector<size_t> o_img, o_vp, o_rho, o_obs, o_g1, o_valid;
+    std::vector<size_t> o_vs, o_obsy, o_obsz, o_g2;    // elastic: vs, Uy/Uz data, density gradient
     size_t o_corr = 0, o_res = 0, o_misfit = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
     std::vector<int> nx, ny, nz, nrec;
     bool fwi() const { return kind == RSGPU_KIND_FWI; }
+    bool elastic() const { return phys == PHYS_E3D; }
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
     bool ran = false;
 

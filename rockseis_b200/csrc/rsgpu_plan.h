@@ -14,15 +14,18 @@ inline int nfields(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 
 inline int nparams(int phys) { return phys == PHYS_A2D ? 3 : phys == PHYS_E2D ? 5 : phys == PHYS_A3D ? 4 : 8; }
 inline int npsi(int phys) { return phys == PHYS_A2D ? 2 : 4; }
 
-// One source or receiver trace set of a shot (host arrays).
+// One source or receiver trace set of a shot (host arrays; maps and shifts hold
+// dim = 2 or 3 values per trace).
 struct TraceSet {
     int n = 0;
-    const int *map = nullptr;       // n*2 ints, -1 = off the grid
-    const void *shift = nullptr;    // n*2 reals
+    const int *map = nullptr;       // n*dim ints, -1 = off the grid
+    const void *shift = nullptr;    // n*dim reals
     int field = RSGPU_PRESSURE;
     const void *data = nullptr;     // sources: n*nt wavelet / residual reals
     const void *factor = nullptr;   // receivers: elastic pressure divisor per trace, or null
     bool psum = false;              // receivers, elastic PRESSURE: record (Sxx + Szz) unhalved
+    bool at_point = false;          // receivers, elastic 3D: the adjoint wavelet gradient, read at
+                                    // the map point itself (no interpolation)
 };
 struct ShotSets {
     int nsrc = 0, nrec = 0;

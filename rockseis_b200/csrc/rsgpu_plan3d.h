@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include "rsgpu.h"
 #include "rsgpu_kernels.h"
+#include "rsgpu_plan.h"
 
 namespace rsgpu {
 
@@ -12,19 +13,25 @@ namespace rsgpu {
 struct Layout3D {
     int nxp = 0, nyp = 0, nzp = 0, pitch = 0, rows = 0, planes = 0;
     long long plane = 0;
-    int nrec = 0, nsrc = 0;
+    int nrec = 0, nsrc = 0;                       // traces of set 0
+    int nrecsets = 0, nsrcsets = 0;
+    int nrecs[MAXSETS] = {}, nsrcs[MAXSETS] = {};
     size_t f[9] = {}, m[8] = {}, psix[6] = {}, psiy[6] = {}, psiz[6] = {};
-    size_t psi_end = 0, traces = 0, state_end = 0, wav = 0, rfac = 0;
+    size_t psi_end = 0, state_end = 0;
+    size_t traces = 0, wav = 0, rfac = 0;         // set 0
+    size_t tracesk[MAXSETS] = {}, wavk[MAXSETS] = {}, rfack[MAXSETS] = {};
 };
 
 class Plan3D {
 public:
     ~Plan3D();
-    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s);
+    // sets: per shot the source/receiver trace sets (elastic: up to MAXSETS each);
+    // null = the rsgpu_shot's own
+    rsgpu_status create(const rsgpu_config *c, int ns, const rsgpu_shot *s, const ShotSets *sets = nullptr);
     rsgpu_status reset();
     rsgpu_status run(int it0, int nsteps);
     rsgpu_status step(int it);
-    rsgpu_status read_traces(int shot, void *host_out);
+    rsgpu_status read_traces(int shot, void *host_out, int set = 0);
     rsgpu_status read_field(int shot, int field, void *host_out);
     size_t origin_bytes(const Layout3D &L) const;
     rsgpu_status inject_record_only(int it);   // injection/recording of step it without propagation
@@ -38,24 +45,35 @@ public:
     bool reverse_time = false;                 // wavelet/trace index nt-1-it at step it
     bool adjoint_steps = false;                // elastic: propagate with backwardstep* (adjoint kernels)
     bool gated_recording = false;              // recording obeys set_recording()
+    const Plan3D *share_params = nullptr;      // use this plan's parameter arrays (same shots and
+                                               // grids) instead of uploading a copy
     rsgpu_status set_recording(bool on);
     int *d_gate = nullptr;                     // recording switch (gated_recording)
     cudaStream_t shared_stream = nullptr;      // run on this caller-owned stream
 
     rsgpu_config cfg{};
     int prec = 0, phys = PHYS_A3D, nshots = 0, es = 4, zc = 64, ntiles = 0;
+    int nsets = 1;                             // InjRec3 entries per shot (elastic: MAXSETS)
     std::vector<Layout3D> shots;
-    std::vector<size_t> rec_pt_offsets;        // per shot: arena offset of the receiver points (long long, -1 off grid)
+    std::vector<size_t> rec_pt_offsets;        // [shot*nsets + set]: arena offset of the receiver points (long long, -1 off grid)
     void *arena = nullptr, *d_meta = nullptr;
     size_t arena_bytes = 0;
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
     cudaStream_t stream = nullptr;
     long long launches = 0;
 
+    // device address of parameter k of shot i (this plan's arena, or the shared plan's)
+    const char *param_base(int i, int k) const;
+
 private:
+    struct SetTables {
+        size_t ip, is, it, iw, rp, rw;
+        int ninj, nrec;
+    };
     template <typename T>
-    void fill_desc(unsigned char *sd, unsigned char *irp, int i, const rsgpu_shot &s, size_t o_ip, size_t o_is,
-                   size_t o_it, size_t o_iw, size_t o_rp, size_t o_rw, int ninj, int nrec);
+    void fill_shot(unsigned char *sd, int i);
+    template <typename T>
+    void fill_set(unsigned char *irp, int i, int k, const TraceSet &src, const TraceSet &rec, const SetTables &t);
 };
 
 }  // namespace rsgpu

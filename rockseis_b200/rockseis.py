@@ -733,6 +733,64 @@ class FwiElastic2D(_Adjoint):
         return fwi_gradient_batch([self])
 
 
+class FwiElastic3D(_Adjoint):
+    """FwiElastic3D<T> (include/fwi.h:318-390): vp/vs/rho (and wavelet) gradients of
+    the DIFFERENCE misfit of the Ux, Uy and Uz data, run on the GPU with the
+    adjoint elastic 3D propagator and Revolve checkpointing (run_optimal,
+    lib/fwi.cpp:6770-6990).  Gradients are Image3D containers [1, 1, 1, nz, ny, nx]."""
+    cls = "FwiElastic3D"
+
+    def __init__(self, model=None, source=None, dataUx=None, dataUy=None, dataUz=None, order=4, snapinc=1,
+                 precision=None):
+        super().__init__(model, source, dataUx, order, snapinc, precision)
+        self.dataUy, self.dataUz = dataUy, dataUz
+        self.vpgrad = self.vsgrad = self.rhograd = self.wavgrad = None
+        self.datamodUx = self.datamodUy = self.datamodUz = None
+        self.dataresUx = self.dataresUy = self.dataresUz = None
+        self.misfit = 0.0
+
+    def setDataUx(self, d): self.dataP = d
+    def setDataUy(self, d): self.dataUy = d
+    def setDataUz(self, d): self.dataUz = d
+    def setVpgrad(self, img): self.vpgrad = img
+    def setVsgrad(self, img): self.vsgrad = img
+    def setRhograd(self, img): self.rhograd = img
+    def setWavgrad(self, d): self.wavgrad = d
+    def setDatamodUx(self, d): self.datamodUx = d
+    def setDatamodUy(self, d): self.datamodUy = d
+    def setDatamodUz(self, d): self.datamodUz = d
+    def setDataresUx(self, d): self.dataresUx = d
+    def setDataresUy(self, d): self.dataresUy = d
+    def setDataresUz(self, d): self.dataresUz = d
+    def getMisfit(self): return self.misfit
+
+    def _adjoint_shot(self, keep):
+        a = super()._adjoint_shot(keep)
+        m = self.model
+        vp, vs, rho = (np.ascontiguousarray(x) for x in (m.Vp, m.Vs, m.R))
+        keep.extend([vp, vs, rho])
+        a.vp, a.vs, a.rho = ptr(vp), ptr(vs), ptr(rho)
+        for d, mp, sh, dat in ((self.dataUy, "gmap_vy", "gshift_vy", "data_vy"),
+                               (self.dataUz, "gmap_vz", "gshift_vz", "data_vz")):
+            arrs = [np.ascontiguousarray(x) for x in (d.gmap, d.gshift, d.data)]
+            keep.extend(arrs)
+            setattr(a, mp, ptr(arrs[0]))
+            setattr(a, sh, ptr(arrs[1]))
+            setattr(a, dat, ptr(arrs[2]))
+        out = lambda o: ptr(o.getImagedata()) if o is not None else None  # noqa: E731
+        a.vpgrad, a.vsgrad, a.rhograd = out(self.vpgrad), out(self.vsgrad), out(self.rhograd)
+        dat = lambda o: ptr(o.data) if o is not None else None  # noqa: E731
+        a.wavgrad = dat(self.wavgrad)
+        a.shot.rec_out, a.datamod_vy, a.datamod_vz = dat(self.datamodUx), dat(self.datamodUy), dat(self.datamodUz)
+        a.datares, a.datares_vy, a.datares_vz = dat(self.dataresUx), dat(self.dataresUy), dat(self.dataresUz)
+        self._mis = C.c_double(0.0)
+        a.misfit = C.pointer(self._mis)
+        return a
+
+    def run_optimal(self):
+        return fwi_gradient_batch([self])
+
+
 class RtmAcoustic2D(_Adjoint):
     """RtmAcoustic2D<T> (include/rtm.h:97-127): (extended) cross-correlation image."""
     cls = "RtmAcoustic2D"
@@ -794,7 +852,7 @@ def _adjoint_batch(jobs, fn):
     shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
     check(fn(C.byref(cfg), C.byref(opts), len(jobs), shots))
     for j in jobs:
-        if isinstance(j, (FwiAcoustic2D, FwiElastic2D)):
+        if isinstance(j, (FwiAcoustic2D, FwiElastic2D, FwiElastic3D)):
             j.misfit += j._mis.value
     return FWI_OK
 
@@ -829,7 +887,7 @@ class AdjointBatch:
     def read(self):
         check(abi.lib.rsgpu_adjoint_read(self.h, len(self.jobs), self.shots))
         for j in self.jobs:
-            if isinstance(j, (FwiAcoustic2D, FwiElastic2D)):
+            if isinstance(j, (FwiAcoustic2D, FwiElastic2D, FwiElastic3D)):
                 j.misfit += j._mis.value
                 j._mis.value = 0.0
 
