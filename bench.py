@@ -785,6 +785,215 @@ def run_a3d(args, device=0, f=A3D):
             "clocks": clk.summary(), "models": models}
 
 
+# ---------------------------------------------------------------- 3D elastic FWI workload
+E3D = dict(W.C5, ncheck_max=40, nt_bench=200, plain_sample=1)
+
+
+def e3d_config(nt, ncheck, f=E3D):
+    return {"workload": f"elastic3d_fwi_gradient_16shots_256cubed_nt{nt}", "nx": f["nx"], "ny": f["ny"],
+            "nz": f["nz"], "dx": f["dx"], "lpml": f["lpml"], "order": f["order"], "dt": f["dt"], "nt": nt,
+            "nt_full": f["nt"], "shots": f["nshots"], "receivers": f["nrec_side"] ** 2, "ncheck": ncheck,
+            "checkpoints": "BF16, power-of-two scale per field array", "accumulation": "FP64",
+            "l2": "working set tens of GB > 126 MB L2 (no flush needed)"}
+
+
+def e3d_problem(precision, nt, true_model=False, nshots=None, f=E3D):
+    """Model, sources and Ux/Uy/Uz receiver sets of the elastic 3D FWI workload."""
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import Data3D, ModelElastic3D
+    vp, vs, rho, src, wav, rec = W.elastic3d_c5(nt, true_model)
+    m = ModelElastic3D(f["nx"], f["ny"], f["nz"], f["lpml"], f["dx"], f["dx"], f["dx"], 0.0, 0.0, 0.0, 0, precision)
+    m.createModel()
+    m.Vp[:], m.Vs[:], m.R[:] = vp, vs, rho
+    del vp, vs, rho
+    t = abi.real_dtype(precision)
+    srcs, recsets = [], []
+    for xyz in src[: nshots or f["nshots"]]:
+        s_ = Data3D(1, nt, f["dt"], 0.0, precision)
+        s_.scoords[:] = [xyz]
+        s_.data[:] = wav.astype(t)[None, :]
+        s_.makeMap(m, 0)
+        sets = []
+        for fld in (abi.VX, abi.VY, abi.VZ):
+            r = Data3D(len(rec), nt, f["dt"], 0.0, precision)
+            r.gcoords[:] = rec
+            r.setField(fld)
+            r.makeMap(m, 1)
+            sets.append(r)
+        srcs.append(s_)
+        recsets.append(sets)
+    return m, srcs, recsets
+
+
+def e3d_jobs(m, srcs, recsets, precision, ckpt, accum, ncheck, f=E3D):
+    from rockseis_b200.rockseis import Data3D, FwiElastic3D, Image3D
+    jobs = []
+    for s_, (rx, ry, rz) in zip(srcs, recsets):
+        j = FwiElastic3D(m, s_, rx, ry, rz, f["order"], 1, precision=precision)
+        j.setNcheck(ncheck)
+        j.setCheckpointPrecision(ckpt)
+        j.setAccumulation(accum)
+        j.setVpgrad(Image3D("vpgrad", m, 1, 1, 1, precision))
+        j.setVsgrad(Image3D("vsgrad", m, 1, 1, 1, precision))
+        j.setRhograd(Image3D("rhograd", m, 1, 1, 1, precision))
+        j.setWavgrad(Data3D(s_.ntrace, s_.nt, s_.dt, 0.0, precision))
+        jobs.append(j)
+    return jobs
+
+
+def _e3d_ref_sample(args):
+    """One process: the reference's FwiElastic3D::run_optimal for one shot on the full
+    256^3 grid (296^3 padded) with a time axis of nt steps."""
+    shot, nt, ncheck = args
+    sys.path.insert(0, ROOT)
+    from oracle import api
+    f = E3D
+    vp, vs, rho, src, wav, rec = W.elastic3d_c5(nt)
+    pb = api.Problem3D(f["nx"], f["ny"], f["nz"], f["dx"], f["dx"], f["dx"], f["lpml"], f["order"], 0, f["dt"], nt,
+                       vp, rho, vs)
+    obs = [np.zeros((len(rec), nt), np.float32)] * 3
+    t0 = time.perf_counter()
+    api.ref_fwi_e3d(pb, src[shot % len(src)][None, :], wav[None, :], 0, rec, obs, ncheck)
+    return time.perf_counter() - t0
+
+
+def cpu_e3d_reference(ncheck_full, nt_sample=4, procs=None, f=E3D):
+    """The reference's CPU gradient, one full-grid shot per process, nt_sample steps,
+    extrapolated to nt by the propagation work (Revolve forward steps + adjoint steps
+    + correlations) at the GPU run's snapshot count."""
+    import multiprocessing as mp
+    from oracle import api
+    from rockseis_b200 import abi
+    if not api.ref_available():
+        return None
+    procs = procs or max(1, min(4, (os.cpu_count() or 1)))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        times = pool.map(_e3d_ref_sample, [(i, nt_sample, 2) for i in range(procs)])
+
+    def work(nt, nc):
+        return abi.lib.rsgpu_revolve_numforw(nt, nc) + 1 + 2 * nt
+    t_shot = max(times) * work(f["nt"], ncheck_full) / work(nt_sample, 2)
+    return {"value": float("%.4g" % (procs / t_shot)), "unit": "shots/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x 1 shot, full 296^3 padded grid, nt={nt_sample} (ncheck 2), "
+                      f"extrapolated to nt={f['nt']} with ncheck {ncheck_full} by Revolve forward + adjoint + "
+                      f"correlation steps", "max_process_s": round(max(times), 3)}
+
+
+def run_e3d(args, device=0, f=E3D):
+    """Shots/s of the batched elastic 3D FWI gradient (FMA, BF16 checkpoints, FP64
+    accumulation) on a shortened time axis, the one-shot-at-a-time gradient beside it,
+    the FP64 error of shot 0, and the forward step's roofline."""
+    import ctypes as C
+    import torch
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import AdjointBatch, fwi_gradient_batch, make_config, make_shot
+    nt = int(args.e3d_nt)
+    ns = args.shots or f["nshots"]
+    prec, ckpt, accum = abi.F32_FAST, abi.CKPT_BF16, abi.ACCUM_F64
+    # observed data: the three components modelled in the true model (batched plans)
+    mt, srcs, recsets = e3d_problem(prec, nt, True, ns)
+    for k in range(3):
+        cfg = make_config(mt, f["order"], nt, f["dt"], prec)
+        keep: list = []
+        shots = (abi.Shot * ns)(*[make_shot(mt, s_, rs[k], keep) for s_, rs in zip(srcs, recsets)])
+        abi.check(abi.lib.rsgpu_modelling(C.byref(cfg), ns, shots))
+        del keep, shots
+    obs = [[r.data.copy() for r in rs] for rs in recsets]
+    del mt
+    m, srcs, recsets = e3d_problem(prec, nt, False, ns)
+    for rs, o in zip(recsets, obs):
+        for r, d in zip(rs, o):
+            r.data = d
+    # snapshots: as many as fit next to the two propagators of every shot
+    L = f["lpml"]
+    pts = (f["nx"] + 2 * L) * (f["ny"] + 2 * L) * (f["nz"] + 2 * L)
+    psi = 18 * 2 * L * (f["nx"] + 2 * L) * (f["ny"] + 2 * L)
+    slot = ns * (9 * pts + psi) * 2
+    free, _ = torch.cuda.mem_get_info(device)
+    need = ns * (2 * 9 * pts * 1.33 + 8 * pts * 1.33 + 2 * psi + 3 * f["nx"] * f["ny"] * f["nz"] * 2) * 4
+    ncheck = int(max(2, min(f["ncheck_max"], (free * 0.92 - need) // slot)))
+    jobs = e3d_jobs(m, srcs, recsets, prec, ckpt, accum, ncheck)
+    batch = AdjointBatch(jobs)
+    batch.run()                                   # warm-up
+    with ClockSampler(device) as clk:
+        t_batch = _timed_runs(batch, max(1, args.fwi_steps))
+    stats = batch.stats()
+    batch.read()
+    g0 = jobs[0].vpgrad.getImagedata()[0, 0, 0].copy()
+    batch.close()
+    torch.cuda.empty_cache()
+    t_plain = []
+    for j in jobs[: f["plain_sample"]]:
+        b1 = AdjointBatch([j])
+        b1.run()
+        t_plain.append(_timed_runs(b1, 1))
+        b1.close()
+    plain = len(t_plain) / sum(t_plain)
+    # FP64 gradient of shot 0 (lossless checkpoints, FP64 accumulation)
+    m64, s64, r64 = e3d_problem(abi.F64, nt, False, 1)
+    for r, d in zip(r64[0], obs[0]):
+        r.data = d.astype(np.float64)
+    j64 = e3d_jobs(m64, s64, r64, abi.F64, abi.CKPT_NATIVE, abi.ACCUM_F64, ncheck)
+    b64 = AdjointBatch(j64)
+    b64.run()
+    b64.read()
+    err = rel_l2(g0, j64[0].vpgrad.getImagedata()[0, 0, 0])
+    b64.close()
+    del m64, j64
+    torch.cuda.empty_cache()
+    # forward step of the batch alone: CUDA events around chunks of time steps
+    cfg = make_config(m, f["order"], nt, f["dt"], prec)
+    keep = []
+    shots = (abi.Shot * ns)(*[make_shot(m, s_, rs[0], keep) for s_, rs in zip(srcs, recsets)])
+    h = C.c_void_p()
+    abi.check(abi.lib.rsgpu_plan_create(C.byref(cfg), ns, shots, C.byref(h)))
+    st = torch.cuda.ExternalStream(abi.lib.rsgpu_plan_stream(h))
+    abi.check(abi.lib.rsgpu_plan_run(h, 0, 5))
+    ch = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    abi.check(abi.lib.rsgpu_plan_run(h, 5, ch))
+    e1.record(st)
+    e1.synchronize()
+    fw_ms = e0.elapsed_time(e1) / ch
+    abi.lib.rsgpu_plan_destroy(h)
+    del keep, shots
+    peak, peak_kind = measured_peak()
+    # algorithmic bytes per point and forward step: velocity reads 6 stresses, 3
+    # velocities, Rx/Ry/Rz and writes 3 velocities (60 B); stress reads 3 velocities,
+    # 6 stresses, 5 moduli and writes 6 stresses (80 B)
+    achieved = 140.0 * ns * pts / (fw_ms / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        for j in jobs:
+            for img in (j.vpgrad, j.vsgrad, j.rhograd):
+                img.getImagedata()[:] = 0
+            j.wavgrad.data[:] = 0
+        t0 = time.perf_counter()
+        fwi_gradient_batch(jobs)
+        t_e2e = time.perf_counter() - t0
+        h2d = ns * (sum(a.nbytes for a in m.padded()) + 3 * m.Vp.nbytes +
+                    sum(r.data.nbytes + r.gmap.nbytes + r.gshift.nbytes for r in recsets[0]) + srcs[0].data.nbytes)
+        d2h = ns * (3 * m.Vp.nbytes + srcs[0].data.nbytes)
+        e2e = {"value": float("%.4g" % (ns / t_e2e)), "unit": "shots/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "path": "rsgpu_fwi_gradient (C ABI) from host buffers"}
+    work_full = abi.lib.rsgpu_revolve_numforw(f["nt"], ncheck) + 1 + 2 * f["nt"]
+    work = stats["fw_steps"] + stats["bw_steps"] + 1
+    return {"shots_per_s_batched": float("%.4g" % (ns / t_batch)), "shots_per_s_plain": float("%.4g" % plain),
+            "batched_over_plain": round((ns / t_batch) / plain, 2), "s_per_batch": round(t_batch, 3),
+            "shots_per_s_at_full_nt_extrapolated": float("%.4g" % (ns / t_batch * work / work_full)),
+            "gradient_rel_l2_vs_fp64": float("%.3g" % err), "ncheck": ncheck,
+            "forward_steps": stats["fw_steps"], "adjoint_steps": stats["bw_steps"],
+            "checkpoint_bytes": stats["ckpt_bytes"], "gpu_launches": stats["launches"],
+            "gpts_per_s_propagation": round(ns * pts * (stats["fw_steps"] + stats["bw_steps"]) / t_batch / 1e9, 3),
+            "forward_step_ms": round(fw_ms, 3), "forward_gpts_per_s": round(ns * pts / fw_ms / 1e6, 3),
+            "roofline": {"bound": "hbm", "kernel": "e3d_velocity + e3d_stress + inject_record_e3d (forward step)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_point_step": 140, "traffic": None},
+            "config": e3d_config(nt, ncheck), "e2e": e2e, "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------- distributed plumbing
 def dist_init(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -828,7 +1037,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
-    ap.add_argument("--workload", default="elastic2d", choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d"],
+    ap.add_argument("--workload", default="elastic2d",
+                    choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d", "elastic3d_fwi"],
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
     ap.add_argument("--launch-mode", type=int, default=0,
@@ -838,7 +1048,9 @@ def main():
     ap.add_argument("--zchunk", type=int, default=0,
                     help="acoustic3d: planes per z-march; 2D fused step: rows per work item (0 = library default)")
     ap.add_argument("--shots", type=int, default=None,
-                    help="acoustic3d: model only the first N windows (profiling runs)")
+                    help="acoustic3d / elastic3d_fwi: only the first N shots (profiling runs)")
+    ap.add_argument("--e3d-nt", type=int, default=E3D["nt_bench"],
+                    help="elastic3d_fwi: time steps of the timed gradients (the full workload has 2000)")
     args = ap.parse_args()
 
     if args.impl == "reference" and args.workload == "fwi":
@@ -851,6 +1063,21 @@ def main():
                               "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1,
                               "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                               "dtype": "f32", "data": "synthetic", "config": fwi_config(), "cpu_baseline": r,
+                              "e2e": {"value": r["value"], "unit": "shots/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}))
+        return
+
+    if args.impl == "reference" and args.workload == "elastic3d_fwi":
+        if int(os.environ.get("RANK", "0")) == 0:
+            r = cpu_e3d_reference(E3D["ncheck_max"])
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                return
+            print(json.dumps({"metric": "FWI gradient shots/s", "value": r["value"], "unit": "shots/s",
+                              "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1,
+                              "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f32", "data": "synthetic",
+                              "config": e3d_config(E3D["nt"], E3D["ncheck_max"]), "cpu_baseline": r,
                               "e2e": {"value": r["value"], "unit": "shots/s", "h2d_bytes_per_step": 0,
                                       "d2h_bytes_per_step": 0}}))
         return
@@ -905,6 +1132,22 @@ def main():
                 "config": a3d_config(args.shots), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
                 "clocks": r["clocks"], "acoustic3d": {k: v for k, v in r.items() if k not in ("roofline", "clocks")},
                 "cpu_baseline": cpu}
+        print(json.dumps(line))
+        return
+    if args.workload == "elastic3d_fwi":
+        if world > 1:
+            raise SystemExit("the elastic 3D FWI gradient line is a one-GPU measurement")
+        import torch
+        torch.cuda.set_device(local)
+        r = run_e3d(args, device=local)
+        cpu = None if args.no_cpu_baseline else cpu_e3d_reference(r["ncheck"])
+        line = {"metric": "FWI gradient shots/s", "value": r["shots_per_s_batched"], "unit": "shots/s", "n_gpus": 1,
+                "steps": args.fwi_steps, "warmup": 1, "ms_per_step": round(r["s_per_batch"] * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded layers + Gaussian blobs; start model = the layers)",
+                "config": r["config"], "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "fwi_gradient": {k: v for k, v in r.items() if k not in ("roofline", "config", "e2e", "clocks")},
+                "e2e": r["e2e"], "clocks": r["clocks"], "cpu_baseline": cpu}
         print(json.dumps(line))
         return
     if args.workload == "fwi":

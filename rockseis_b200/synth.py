@@ -115,3 +115,30 @@ def dipping_vp_3d(nx: int, ny: int, nz: int, dx: float, seed=5, vmin=1500.0, vma
     if vclip is not None:
         vp = np.minimum(vp, vclip)
     return vp.astype(dtype)
+
+
+def elastic_blobs_3d(nx: int, ny: int, nz: int, dx: float, seed=7, vmin=1800.0, vmax=4000.0, nlayers=4, nblobs=12,
+                     blobs=True, dtype=np.float32):
+    """Elastic 3D model [nz][ny][nx]: flat layers from vmin to vmax, optionally with
+    nblobs seeded Gaussian blobs of +-8 % vp; vp/vs drawn per layer in [1.7, 2.0];
+    Gardner density.  Returns vp, vs, rho."""
+    rng = np.random.default_rng(seed)
+    z = np.arange(nz, dtype=np.float32) * dx
+    edges = np.sort(rng.uniform(0.1, 0.9, nlayers - 1)) * nz * dx
+    layer = np.searchsorted(edges, z)
+    v1 = (vmin + (vmax - vmin) * layer / max(1, nlayers - 1)).astype(np.float32)
+    ratio = rng.uniform(1.7, 2.0, nlayers).astype(np.float32)[layer]
+    vp = np.broadcast_to(v1[:, None, None], (nz, ny, nx)).copy()
+    vsr = np.broadcast_to(ratio[:, None, None], (nz, ny, nx))
+    centres = rng.uniform(0.15, 0.85, (nblobs, 3)) * np.array([nz, ny, nx])
+    radii = rng.uniform(0.04, 0.1, nblobs) * min(nx, ny, nz)
+    amps = rng.uniform(-0.08, 0.08, nblobs)
+    if blobs:
+        iz, iy, ix = (np.arange(n, dtype=np.float32) for n in (nz, ny, nx))
+        for (cz, cy, cx), r, a in zip(centres, radii, amps):
+            g = (np.exp(-((iz - cz) / r) ** 2)[:, None, None] * np.exp(-((iy - cy) / r) ** 2)[None, :, None] *
+                 np.exp(-((ix - cx) / r) ** 2)[None, None, :])
+            vp *= (1.0 + a * g).astype(np.float32)
+    vp = np.minimum(vp, vmax).astype(dtype)
+    vs = (vp / vsr).astype(dtype)
+    return vp, vs, gardner(vp).astype(dtype)

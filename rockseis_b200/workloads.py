@@ -19,6 +19,13 @@ benchmark all see identical inputs:
                   20-cell C-PML, dt = 1 ms, nt = 3000, Revolve with 50
                   snapshots; true model = smooth background + 8 anomalies,
                   starting model = the true model smoothed.
+  elastic3d_c5    elastic 3D FWI gradient, 16 shots, 256^3, dx = 10 m, 20-cell
+                  C-PML, dt = 0.8 ms, nt = 2000; four flat layers 1800 -> 4000
+                  m/s with vp/vs 1.7-2.0 per layer and Gardner density; true
+                  model = layers + 12 Gaussian blobs of +-8 % vp (seed 7),
+                  starting model = the layers; explosive sources on a 4 x 4 grid
+                  at z = 20 m; 20 x 20 receivers (Ux, Uy, Uz) every 120 m at
+                  z = 10 m.
 """
 from __future__ import annotations
 
@@ -32,6 +39,8 @@ C2 = dict(nx=801, nz=401, dx=5.0, lpml=30, order=8, dt=5e-4, nt=4000, nshots=16,
           sz=10.0)
 C3 = dict(nx=601, nz=201, dx=10.0, lpml=20, order=8, nt=3000, dt=1e-3, nshots=64, ncheck=50, f0=10.0, sz=20.0,
           nrec=601)
+C5 = dict(nx=256, ny=256, nz=256, dx=10.0, lpml=20, order=8, dt=8e-4, nt=2000, nshots=16, f0=10.0, sz=20.0,
+          nrec_side=20, drec=120.0, rz=10.0)
 
 
 def acoustic2d_c1(nt=None):
@@ -66,6 +75,22 @@ def fwi_c3(nt=None):
     wav = synth.ricker(nt, c["dt"], c["f0"])
     rec = synth.surface_line(c["nrec"], 0.0, c["dx"], 0.0)
     return vt, vs, sx, wav, rec
+
+
+def elastic3d_c5(nt=None, true_model=False):
+    """vp, vs, rho [nz][ny][nx] (starting model, or the true one), sources [nshots][3],
+    wavelet [nt], receivers [nrec][3]."""
+    c = C5
+    nt = nt or c["nt"]
+    vp, vs, rho = synth.elastic_blobs_3d(c["nx"], c["ny"], c["nz"], c["dx"], seed=7, blobs=true_model)
+    ext = (c["nx"] - 1) * c["dx"]
+    g = np.linspace(0.2, 0.8, 4) * ext
+    src = np.array([[x, y, c["sz"]] for y in g for x in g]) + np.random.default_rng(8).uniform(-40, 40, (16, 3)) * \
+        np.array([1.0, 1.0, 0.0])
+    r1 = (ext - (c["nrec_side"] - 1) * c["drec"]) / 2 + np.arange(c["nrec_side"]) * c["drec"]
+    rec = np.array([[x, y, c["rz"]] for y in r1 for x in r1])
+    wav = synth.ricker(nt, c["dt"], c["f0"])
+    return vp, vs, rho, src, wav, rec
 
 
 def digest(a: np.ndarray) -> str:
