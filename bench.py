@@ -879,6 +879,60 @@ def cpu_e3d_reference(ncheck_full, nt_sample=4, procs=None, f=E3D):
                       f"correlation steps", "max_process_s": round(max(times), 3)}
 
 
+def e3d_forward_config(nshots, f=E3D):
+    return {"workload": f"elastic3d_forward_{nshots}shots_256cubed", "nx": f["nx"], "ny": f["ny"], "nz": f["nz"],
+            "dx": f["dx"], "lpml": f["lpml"], "order": f["order"], "dt": f["dt"], "nt": f["nt"], "shots": nshots,
+            "time_steps_per_bench_step": 20, "receivers": f["nrec_side"] ** 2,
+            "l2": "working set > 126 MB L2 (no flush needed)"}
+
+
+def run_e3d_forward(args, device=0, f=E3D):
+    """Gpts/s of the elastic 3D forward modelling of the C5 shots (Vx receivers):
+    bench steps of 20 time steps of the whole batch."""
+    import ctypes as C
+    import torch
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import make_config, make_shot
+    prec = abi.F32_FAST if args.precision == "fast" else abi.F32_EXACT
+    ns = args.shots or f["nshots"]
+    m, srcs, recsets = e3d_problem(prec, f["nt"], True, ns)
+    cfg = make_config(m, f["order"], f["nt"], f["dt"], prec)
+    keep: list = []
+    shots = (abi.Shot * ns)(*[make_shot(m, s_, rs[0], keep) for s_, rs in zip(srcs, recsets)])
+    h = C.c_void_p()
+    abi.check(abi.lib.rsgpu_plan_create(C.byref(cfg), ns, shots, C.byref(h)))
+    del keep, shots
+    L = f["lpml"]
+    pts = ns * (f["nx"] + 2 * L) * (f["ny"] + 2 * L) * (f["nz"] + 2 * L)
+    st = torch.cuda.ExternalStream(abi.lib.rsgpu_plan_stream(h))
+    ch, it = 20, 0
+    for _ in range(args.warmup):
+        abi.check(abi.lib.rsgpu_plan_run(h, it, ch))
+        it += ch
+    abi.check(abi.lib.rsgpu_plan_sync(h))
+    l0 = abi.lib.rsgpu_plan_launch_count(h)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            abi.check(abi.lib.rsgpu_plan_run(h, it, ch))
+            it += ch
+        e1.record(st)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = abi.lib.rsgpu_plan_launch_count(h) - l0
+    abi.lib.rsgpu_plan_destroy(h)
+    peak, peak_kind = measured_peak()
+    achieved = 140.0 * pts * ch / (ms / 1e3) / 1e9
+    return {"metric": "Gpts/s", "value": round(pts * ch / (ms / 1e3) / 1e9, 3), "unit": "Gpts/s",
+            "ms_per_step": round(ms, 3), "gpu_launches": int(launches), "padded_points_per_step": int(pts),
+            "roofline": {"bound": "hbm", "kernel": "e3d_velocity + e3d_stress + inject_record_e3d (whole step)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_point_step": 140, "traffic": None},
+            "clocks": clk.summary(), "config": e3d_forward_config(ns)}
+
+
 def run_e3d(args, device=0, f=E3D):
     """Shots/s of the batched elastic 3D FWI gradient (FMA, BF16 checkpoints, FP64
     accumulation) on a shortened time axis, the one-shot-at-a-time gradient beside it,
@@ -1038,7 +1092,7 @@ def main():
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
     ap.add_argument("--workload", default="elastic2d",
-                    choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d", "elastic3d_fwi"],
+                    choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d", "elastic3d", "elastic3d_fwi"],
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
     ap.add_argument("--launch-mode", type=int, default=0,
@@ -1132,6 +1186,17 @@ def main():
                 "config": a3d_config(args.shots), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
                 "clocks": r["clocks"], "acoustic3d": {k: v for k, v in r.items() if k not in ("roofline", "clocks")},
                 "cpu_baseline": cpu}
+        print(json.dumps(line))
+        return
+    if args.workload == "elastic3d":
+        import torch
+        torch.cuda.set_device(local)
+        r = run_e3d_forward(args, device=local)
+        line = {"metric": "Gpts/s", "value": r["value"], "unit": "Gpts/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layers + Gaussian blobs)",
+                "config": r["config"], "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "clocks": r["clocks"], "cpu_baseline": None}
         print(json.dumps(line))
         return
     if args.workload == "elastic3d_fwi":

@@ -23,7 +23,8 @@ benchmark all see identical inputs:
                   C-PML, dt = 0.8 ms, nt = 2000; four flat layers 1800 -> 4000
                   m/s with vp/vs 1.7-2.0 per layer and Gardner density; true
                   model = layers + 12 Gaussian blobs of +-8 % vp (seed 7),
-                  starting model = the layers; explosive sources on a 4 x 4 grid
+                  starting model = the layers 4 % slower (vp and vs); explosive
+                  sources on a 4 x 4 grid
                   at z = 20 m; 20 x 20 receivers (Ux, Uy, Uz) every 120 m at
                   z = 10 m.
 """
@@ -83,6 +84,9 @@ def elastic3d_c5(nt=None, true_model=False):
     c = C5
     nt = nt or c["nt"]
     vp, vs, rho = synth.elastic_blobs_3d(c["nx"], c["ny"], c["nz"], c["dx"], seed=7, blobs=true_model)
+    if not true_model:
+        vp *= np.float32(0.96)
+        vs *= np.float32(0.96)
     ext = (c["nx"] - 1) * c["dx"]
     g = np.linspace(0.2, 0.8, 4) * ext
     src = np.array([[x, y, c["sz"]] for y in g for x in g]) + np.random.default_rng(8).uniform(-40, 40, (16, 3)) * \
