@@ -65,8 +65,8 @@ __device__ __forceinline__ T taps3_reg(const T (&q)[16], const T *cu, T d, T r)
 // backwardstepVelocity (lib/waves.cpp:3307, 3353, 3399, 3446, 3491, 3535, 3582,
 // 3628, 3672), evaluated in the reference's expression order.
 enum { OP_XX = 0, OP_YY = 1, OP_ZZ = 2, OP_XY = 3, OP_XZ = 4, OP_YZ = 5 };
-template <typename T, int MODE, bool ADJ>
-__device__ __forceinline__ T opnd(const Shot3D<T> &sh, long long o, int kind)
+template <typename T, int MODE, bool ADJ, typename I>
+__device__ __forceinline__ T opnd(const Shot3D<T> &sh, I o, int kind)
 {
     using A = Ar<T, MODE>;
     if (!ADJ) {
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_velocity(Step3DArgs<T> a, con
         vyy0 = opnd<T, MODE, ADJ>(sh, o - 8 * pitch, OP_YY); vyy1 = opnd<T, MODE, ADJ>(sh, o + TY3 * pitch, OP_YY);
         vyz0 = opnd<T, MODE, ADJ>(sh, o - 8 * pitch, OP_YZ); vyz1 = opnd<T, MODE, ADJ>(sh, o + TY3 * pitch, OP_YZ);
     }
-    const T *cux = S.cs.cx + order * CROW3, *cuy = S.cs.cy + order * CROW3, *cuz = S.cs.cz + order * CROW3;
+    const T *cux = a.cf[0], *cuy = a.cf[1], *cuz = a.cf[2];
     __syncthreads();
     for (int iz = z0; iz < ze; iz++, o += plane) {
         const int b = (iz - z0) & 1;
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress(Step3DArgs<T> a, const
         yy0 = Vy[o - 8 * pitch]; yy1 = Vy[o + TY3 * pitch];
         yz0 = Vz[o - 8 * pitch]; yz1 = Vz[o + TY3 * pitch];
     }
-    const T *cux = S.cs.cx + order * CROW3, *cuy = S.cs.cy + order * CROW3, *cuz = S.cs.cz + order * CROW3;
+    const T *cux = a.cf[0], *cuy = a.cf[1], *cuz = a.cf[2];
     __syncthreads();
     for (int iz = z0; iz < ze; iz++, o += plane) {
         const int b = (iz - z0) & 1;
@@ -468,6 +468,383 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress(Step3DArgs<T> a, const
     }
 }
 
+// ---------------------------------------------------------------- fast-mode kernels
+// RSGPU_F32_FAST versions of the two half-steps: the same stencils, C-PML and
+// update order, with derivatives that share an axis and a direction computed in
+// pairs -- one 64-bit shared load and one FADD2/FFMA2 per tap for two fields -- and
+// the full-order coefficients taken from the launch's parameter space.
+//   velocity: x backward (XY, XZ), y backward (XY, YZ), z backward (XZ, YZ);
+//             single: x forward XX, y forward YY, z forward ZZ
+//   stress:   x forward (Vz, Vy), y forward (Vz, Vx), z forward (Vx, Vy);
+//             single: x backward Vx, y backward Vy, z backward Vz
+__device__ __forceinline__ float2 taps_pair(const float2 *b, int s, const float (&c2)[NCOEF][2])
+{
+    using A2 = Ar2<float, MODE_FAST>;
+    const float2 *cc = reinterpret_cast<const float2 *>(c2);
+    float2 acc = A2::mul(A2::sub(b[8 * s], b[7 * s]), cc[0]);
+#pragma unroll
+    for (int k = 1; k < NCOEF; k++) acc = A2::acc(acc, A2::sub(b[(8 + k) * s], b[(7 - k) * s]), cc[k]);
+    return acc;
+}
+__device__ __forceinline__ float2 taps_pair_reg(const float2 (&q)[16], const float (&c2)[NCOEF][2])
+{
+    using A2 = Ar2<float, MODE_FAST>;
+    const float2 *cc = reinterpret_cast<const float2 *>(c2);
+    float2 acc = A2::mul(A2::sub(q[8], q[7]), cc[0]);
+#pragma unroll
+    for (int k = 1; k < NCOEF; k++) acc = A2::acc(acc, A2::sub(q[8 + k], q[7 - k]), cc[k]);
+    return acc;
+}
+
+struct VelSmemF {
+    float xx[2][TY3][WX];      // XX, x halo
+    float2 xq[2][TY3][WX];     // (XY, XZ), x halo
+    float2 yq[2][HY][TX3];     // (XY, YZ), y halo
+    float yy[2][HY][TX3];      // YY, y halo
+    CoefSet3<float> cs;
+};
+
+template <bool ADJ>
+__global__ void __launch_bounds__(TX3 *TY3, 2) e3d_velocity_fast(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    VelSmemF &S = *reinterpret_cast<VelSmemF *>(smraw);
+    load_coefs3e(S.cs, coefs);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    const int ix = tl.x0 + tx, iy = tl.y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const int plane = (int)sh.plane;   // a field holds fewer than 2^31 elements
+    const int col = iy * pitch + ix;
+    T *Vx = sh.f[E3_VX], *Vy = sh.f[E3_VY], *Vz = sh.f[E3_VZ];
+    const T *Rx = sh.m[ME_RX], *Ry = sh.m[ME_RY], *Rz = sh.m[ME_RZ];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kxf = kfw(ix, nxp, order), Kxb = kbw(ix, nxp, order);
+    const int Kyf = kfw(iy, nyp, order), Kyb = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    const int hx = tx < 8 ? -8 : TX3 - 8;
+    // z windows: (XZ, YZ) backward (planes z-8..z+7), ZZ forward (z-7..z+8)
+    float2 qp[16];
+    T qzz[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const int oj = (z0 - 8 + j) * plane + col;
+        qp[j] = make_float2(opnd<T, MODE, ADJ>(sh, oj, OP_XZ), opnd<T, MODE, ADJ>(sh, oj, OP_YZ));
+        qzz[j] = opnd<T, MODE, ADJ>(sh, (z0 - 7 + j) * plane + col, OP_ZZ);
+    }
+    int o = z0 * plane + col;
+    T vx = Vx[o], vy = Vy[o], vz = Vz[o], rx = __ldg(Rx + o), ry = __ldg(Ry + o), rz = __ldg(Rz + o);
+    T cxx = opnd<T, MODE, ADJ>(sh, o, OP_XX), cxy = opnd<T, MODE, ADJ>(sh, o, OP_XY), cyy = opnd<T, MODE, ADJ>(sh, o, OP_YY);
+    T hxx = 0, hxy = 0, hxz = 0;
+    if (tx < 16) {
+        hxx = opnd<T, MODE, ADJ>(sh, o + hx, OP_XX);
+        hxy = opnd<T, MODE, ADJ>(sh, o + hx, OP_XY);
+        hxz = opnd<T, MODE, ADJ>(sh, o + hx, OP_XZ);
+    }
+    T vxy0 = opnd<T, MODE, ADJ>(sh, o - 8 * pitch, OP_XY), vxy1 = opnd<T, MODE, ADJ>(sh, o + TY3 * pitch, OP_XY);
+    T vyy0 = opnd<T, MODE, ADJ>(sh, o - 8 * pitch, OP_YY), vyy1 = opnd<T, MODE, ADJ>(sh, o + TY3 * pitch, OP_YY);
+    T vyz0 = opnd<T, MODE, ADJ>(sh, o - 8 * pitch, OP_YZ), vyz1 = opnd<T, MODE, ADJ>(sh, o + TY3 * pitch, OP_YZ);
+    __syncthreads();
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int b = (iz - z0) & 1;
+        S.xx[b][ty][tx + 8] = cxx;
+        S.xq[b][ty][tx + 8] = make_float2(cxy, qp[8].x);
+        S.yq[b][ty + 8][tx] = make_float2(cxy, qp[8].y);
+        S.yy[b][ty + 8][tx] = cyy;
+        if (tx < 16) {
+            const int c = tx < 8 ? tx : tx + TX3;
+            S.xx[b][ty][c] = hxx;
+            S.xq[b][ty][c] = make_float2(hxy, hxz);
+        }
+        S.yq[b][ty][tx] = make_float2(vxy0, vyz0);
+        S.yq[b][ty + TY3 + 8][tx] = make_float2(vxy1, vyz1);
+        S.yy[b][ty][tx] = vyy0;
+        S.yy[b][ty + TY3 + 8][tx] = vyy1;
+        // next plane's inputs (the plane after the chunk lies inside the allocation; unused)
+        const int on = o + plane;
+        const T nvx = Vx[on], nvy = Vy[on], nvz = Vz[on];
+        const T nrx = __ldg(Rx + on), nry = __ldg(Ry + on), nrz = __ldg(Rz + on);
+        const T ncxx = opnd<T, MODE, ADJ>(sh, on, OP_XX), ncxy = opnd<T, MODE, ADJ>(sh, on, OP_XY),
+                ncyy = opnd<T, MODE, ADJ>(sh, on, OP_YY);
+        if (tx < 16) {
+            hxx = opnd<T, MODE, ADJ>(sh, on + hx, OP_XX);
+            hxy = opnd<T, MODE, ADJ>(sh, on + hx, OP_XY);
+            hxz = opnd<T, MODE, ADJ>(sh, on + hx, OP_XZ);
+        }
+        vxy0 = opnd<T, MODE, ADJ>(sh, on - 8 * pitch, OP_XY); vxy1 = opnd<T, MODE, ADJ>(sh, on + TY3 * pitch, OP_XY);
+        vyy0 = opnd<T, MODE, ADJ>(sh, on - 8 * pitch, OP_YY); vyy1 = opnd<T, MODE, ADJ>(sh, on + TY3 * pitch, OP_YY);
+        vyz0 = opnd<T, MODE, ADJ>(sh, on - 8 * pitch, OP_YZ); vyz1 = opnd<T, MODE, ADJ>(sh, on + TY3 * pitch, OP_YZ);
+        __syncthreads();
+        const int Kzf = kfw(iz, nzp, order), Kzb = kbw(iz, nzp, order);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        const int px = (iz * nyp + iy) * 2 * L + xc;
+        const int py = (iz * 2 * L + yc) * nxp + ix;
+        const int pz = (zc * nyp + iy) * nxp + ix;
+        // full-order derivatives, then the reduced-order ones near the array ends
+        const T *cx1 = &S.xx[b][ty][tx + 8];
+        T dxx = taps3<T, MODE>(cx1 - 7, 1, a.cf[0], a.dx, a.rdx);
+        const float2 *cxq = &S.xq[b][ty][tx + 8];
+        float2 dxq = taps_pair(cxq - 8, 1, a.cf2[0]);
+        const float2 *cyq = &S.yq[b][ty + 8][tx];
+        float2 dyq = taps_pair(cyq - 8 * TX3, TX3, a.cf2[1]);
+        const T *cy1 = &S.yy[b][ty + 8][tx];
+        T dyy = taps3<T, MODE>(cy1 - 7 * TX3, TX3, a.cf[1], a.dy, a.rdy);
+        float2 dzq = taps_pair_reg(qp, a.cf2[2]);
+        T dzz = taps3_reg<T, MODE>(qzz, a.cf[2], a.dz, a.rdz);
+        if (Kxf != order) dxx = stencil_k<T, MODE>(cx1, 1, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+        if (Kxb != order) {
+            const T *c = reinterpret_cast<const T *>(cxq);
+            dxq.x = stencil_k<T, MODE>(c, 2, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+            dxq.y = stencil_k<T, MODE>(c + 1, 2, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+        }
+        if (Kyb != order) {
+            const T *c = reinterpret_cast<const T *>(cyq);
+            dyq.x = stencil_k<T, MODE>(c, 2 * TX3, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+            dyq.y = stencil_k<T, MODE>(c + 1, 2 * TX3, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+        }
+        if (Kyf != order) dyy = stencil_k<T, MODE>(cy1, TX3, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+        if (Kzb != order) {
+            dzq.x = stencil_z_op<T, MODE, ADJ>(sh, o, plane, Kzb, S.cs.cz + Kzb * CROW3, false, OP_XZ, a.dz, a.rdz);
+            dzq.y = stencil_z_op<T, MODE, ADJ>(sh, o, plane, Kzb, S.cs.cz + Kzb * CROW3, false, OP_YZ, a.dz, a.rdz);
+        }
+        if (Kzf != order)
+            dzz = stencil_z_op<T, MODE, ADJ>(sh, o, plane, Kzf, S.cs.cz + Kzf * CROW3, true, OP_ZZ, a.dz, a.rdz);
+        // ---- Vx: Dx+ XX, Dy- XY, Dz- XZ
+        {
+            const T am = A::mul(a.dt, rx);
+            vx = A::mad(vx, am, dxx);
+            if (xi >= 0) vx = pml_correct<T, MODE>(vx, am, dxx, sh.psix[0] + px, a.pml, L, xb + 3, xi);
+            vx = A::mad(vx, am, dyq.x);
+            if (yi >= 0) vx = pml_correct<T, MODE>(vx, am, dyq.x, sh.psiy[0] + py, a.pml, L, yb, yi);
+            vx = A::mad(vx, am, dzq.x);
+            if (zi >= 0) vx = pml_correct<T, MODE>(vx, am, dzq.x, sh.psiz[0] + pz, a.pml, L, zb, zi);
+            Vx[o] = vx;
+        }
+        // ---- Vy: Dx- XY, Dy+ YY, Dz- YZ
+        {
+            const T am = A::mul(a.dt, ry);
+            vy = A::mad(vy, am, dxq.x);
+            if (xi >= 0) vy = pml_correct<T, MODE>(vy, am, dxq.x, sh.psix[1] + px, a.pml, L, xb, xi);
+            vy = A::mad(vy, am, dyy);
+            if (yi >= 0) vy = pml_correct<T, MODE>(vy, am, dyy, sh.psiy[1] + py, a.pml, L, yb + 3, yi);
+            vy = A::mad(vy, am, dzq.y);
+            if (zi >= 0) vy = pml_correct<T, MODE>(vy, am, dzq.y, sh.psiz[1] + pz, a.pml, L, zb, zi);
+            Vy[o] = vy;
+        }
+        // ---- Vz: Dx- XZ, Dy- YZ, Dz+ ZZ
+        {
+            const T am = A::mul(a.dt, rz);
+            vz = A::mad(vz, am, dxq.y);
+            if (xi >= 0) vz = pml_correct<T, MODE>(vz, am, dxq.y, sh.psix[2] + px, a.pml, L, xb, xi);
+            vz = A::mad(vz, am, dyq.y);
+            if (yi >= 0) vz = pml_correct<T, MODE>(vz, am, dyq.y, sh.psiy[2] + py, a.pml, L, yb, yi);
+            vz = A::mad(vz, am, dzz);
+            if (zi >= 0) vz = pml_correct<T, MODE>(vz, am, dzz, sh.psiz[2] + pz, a.pml, L, zb + 3, zi);
+            Vz[o] = vz;
+        }
+#pragma unroll
+        for (int j = 0; j < 15; j++) { qp[j] = qp[j + 1]; qzz[j] = qzz[j + 1]; }
+        qp[15] = make_float2(opnd<T, MODE, ADJ>(sh, o + 8 * plane, OP_XZ), opnd<T, MODE, ADJ>(sh, o + 8 * plane, OP_YZ));
+        qzz[15] = opnd<T, MODE, ADJ>(sh, o + 9 * plane, OP_ZZ);
+        vx = nvx; vy = nvy; vz = nvz; rx = nrx; ry = nry; rz = nrz;
+        cxx = ncxx; cxy = ncxy; cyy = ncyy;
+    }
+}
+
+struct StrSmemF {
+    float sx[2][TY3][WX];      // Vx, x halo
+    float2 px[2][TY3][WX];     // (Vz, Vy), x halo
+    float sy[2][HY][TX3];      // Vy, y halo
+    float2 py[2][HY][TX3];     // (Vz, Vx), y halo
+    CoefSet3<float> cs;
+};
+
+template <bool ADJ>
+__global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress_fast(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    StrSmemF &S = *reinterpret_cast<StrSmemF *>(smraw);
+    load_coefs3e(S.cs, coefs);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    const int ix = tl.x0 + tx, iy = tl.y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const int plane = (int)sh.plane;   // a field holds fewer than 2^31 elements
+    const int col = iy * pitch + ix;
+    const T *Vx = sh.f[E3_VX], *Vy = sh.f[E3_VY], *Vz = sh.f[E3_VZ];
+    T *Sxx = sh.f[E3_SXX], *Syy = sh.f[E3_SYY], *Szz = sh.f[E3_SZZ];
+    T *Syz = sh.f[E3_SYZ], *Sxz = sh.f[E3_SXZ], *Sxy = sh.f[E3_SXY];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kxf = kfw(ix, nxp, order), Kxb = kbw(ix, nxp, order);
+    const int Kyf = kfw(iy, nyp, order), Kyb = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    const int hx = tx < 8 ? -8 : TX3 - 8;
+    // z windows: Vz backward (planes z-8..z+7), (Vx, Vy) forward (z-7..z+8)
+    T qz[16];
+    float2 qv[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        qz[j] = Vz[(z0 - 8 + j) * plane + col];
+        const int oj = (z0 - 7 + j) * plane + col;
+        qv[j] = make_float2(Vx[oj], Vy[oj]);
+    }
+    int o = z0 * plane + col;
+    T sxx = Sxx[o], syy = Syy[o], szz = Szz[o], syz = Syz[o], sxz = Sxz[o], sxy = Sxy[o];
+    T l = 0, l2m = 0, myz = 0, mxz = 0, mxy = 0;
+    if (!ADJ) {
+        l = __ldg(sh.m[ME_L] + o); l2m = __ldg(sh.m[ME_L2M] + o);
+        myz = __ldg(sh.m[ME_MYZ] + o); mxz = __ldg(sh.m[ME_MXZ] + o); mxy = __ldg(sh.m[ME_MXY] + o);
+    }
+    T hvx = 0, hvy = 0, hvz = 0;
+    if (tx < 16) { hvx = Vx[o + hx]; hvy = Vy[o + hx]; hvz = Vz[o + hx]; }
+    T yx0 = Vx[o - 8 * pitch], yx1 = Vx[o + TY3 * pitch];
+    T yy0 = Vy[o - 8 * pitch], yy1 = Vy[o + TY3 * pitch];
+    T yz0 = Vz[o - 8 * pitch], yz1 = Vz[o + TY3 * pitch];
+    __syncthreads();
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int b = (iz - z0) & 1;
+        const T cvx = qv[7].x, cvy = qv[7].y, cvz = qz[8];
+        S.sx[b][ty][tx + 8] = cvx;
+        S.px[b][ty][tx + 8] = make_float2(cvz, cvy);
+        S.sy[b][ty + 8][tx] = cvy;
+        S.py[b][ty + 8][tx] = make_float2(cvz, cvx);
+        if (tx < 16) {
+            const int c = tx < 8 ? tx : tx + TX3;
+            S.sx[b][ty][c] = hvx;
+            S.px[b][ty][c] = make_float2(hvz, hvy);
+        }
+        S.sy[b][ty][tx] = yy0; S.sy[b][ty + TY3 + 8][tx] = yy1;
+        S.py[b][ty][tx] = make_float2(yz0, yx0); S.py[b][ty + TY3 + 8][tx] = make_float2(yz1, yx1);
+        const int on = o + plane;
+        const T nsxx = Sxx[on], nsyy = Syy[on], nszz = Szz[on], nsyz = Syz[on], nsxz = Sxz[on], nsxy = Sxy[on];
+        T nl = 0, nl2m = 0, nmyz = 0, nmxz = 0, nmxy = 0;
+        if (!ADJ) {
+            nl = __ldg(sh.m[ME_L] + on); nl2m = __ldg(sh.m[ME_L2M] + on);
+            nmyz = __ldg(sh.m[ME_MYZ] + on); nmxz = __ldg(sh.m[ME_MXZ] + on); nmxy = __ldg(sh.m[ME_MXY] + on);
+        }
+        if (tx < 16) { hvx = Vx[on + hx]; hvy = Vy[on + hx]; hvz = Vz[on + hx]; }
+        yx0 = Vx[on - 8 * pitch]; yx1 = Vx[on + TY3 * pitch];
+        yy0 = Vy[on - 8 * pitch]; yy1 = Vy[on + TY3 * pitch];
+        yz0 = Vz[on - 8 * pitch]; yz1 = Vz[on + TY3 * pitch];
+        __syncthreads();
+        const int Kzf = kfw(iz, nzp, order), Kzb = kbw(iz, nzp, order);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        const int px = (iz * nyp + iy) * 2 * L + xc;
+        const int py = (iz * 2 * L + yc) * nxp + ix;
+        const int pz = (zc * nyp + iy) * nxp + ix;
+        const T *csx = &S.sx[b][ty][tx + 8];
+        T dxx = taps3<T, MODE>(csx - 8, 1, a.cf[0], a.dx, a.rdx);
+        const float2 *cpx = &S.px[b][ty][tx + 8];
+        float2 dxp = taps_pair(cpx - 7, 1, a.cf2[0]);                 // (Dx+ Vz, Dx+ Vy)
+        const T *csy = &S.sy[b][ty + 8][tx];
+        T dyy = taps3<T, MODE>(csy - 8 * TX3, TX3, a.cf[1], a.dy, a.rdy);
+        const float2 *cpy = &S.py[b][ty + 8][tx];
+        float2 dyp = taps_pair(cpy - 7 * TX3, TX3, a.cf2[1]);         // (Dy+ Vz, Dy+ Vx)
+        T dzz = taps3_reg<T, MODE>(qz, a.cf[2], a.dz, a.rdz);
+        float2 dzp = taps_pair_reg(qv, a.cf2[2]);                     // (Dz+ Vx, Dz+ Vy)
+        if (Kxb != order) dxx = stencil_k<T, MODE>(csx, 1, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+        if (Kxf != order) {
+            const T *c = reinterpret_cast<const T *>(cpx);
+            dxp.x = stencil_k<T, MODE>(c, 2, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+            dxp.y = stencil_k<T, MODE>(c + 1, 2, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+        }
+        if (Kyb != order) dyy = stencil_k<T, MODE>(csy, TX3, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+        if (Kyf != order) {
+            const T *c = reinterpret_cast<const T *>(cpy);
+            dyp.x = stencil_k<T, MODE>(c, 2 * TX3, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+            dyp.y = stencil_k<T, MODE>(c + 1, 2 * TX3, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+        }
+        if (Kzb != order) dzz = stencil_k<T, MODE>(Vz + o, (int)plane, Kzb, S.cs.cz + Kzb * CROW3, false, a.dz, a.rdz);
+        if (Kzf != order) {
+            dzp.x = stencil_k<T, MODE>(Vx + o, (int)plane, Kzf, S.cs.cz + Kzf * CROW3, true, a.dz, a.rdz);
+            dzp.y = stencil_k<T, MODE>(Vy + o, (int)plane, Kzf, S.cs.cz + Kzf * CROW3, true, a.dz, a.rdz);
+        }
+        // ---- normal stresses
+        {
+            const bool fsrow = sh.fs && iz == L;
+            if (!ADJ) {
+                const T a2 = A::mul(a.dt, l2m), a1 = A::mul(a.dt, l);
+                auto upd3 = [&](T d, T cxx_, T cyy_, T czz_) {
+                    sxx = A::mad(sxx, cxx_, d); syy = A::mad(syy, cyy_, d); szz = A::mad(szz, czz_, d);
+                };
+                auto pml3 = [&](T d, T *psi, int base, int idx, T cxx_, T cyy_, T czz_) {
+                    const T tA = __ldg(a.pml + (base + PT_A) * L + idx), tB = __ldg(a.pml + (base + PT_B) * L + idx),
+                            tC = __ldg(a.pml + (base + PT_C) * L + idx);
+                    const T p = A::mad(A::mul(tB, *psi), tA, d);
+                    *psi = p;
+                    const T cq = A::mad(p, tC, d);
+                    sxx = A::msub(sxx, cxx_, cq); syy = A::msub(syy, cyy_, cq); szz = A::msub(szz, czz_, cq);
+                };
+                upd3(dxx, a2, a1, a1);
+                if (xi >= 0) pml3(dxx, sh.psix[3] + px, xb, xi, a2, a1, a1);
+                upd3(dyy, a1, a2, a1);
+                if (yi >= 0) pml3(dyy, sh.psiy[3] + py, yb, yi, a1, a2, a1);
+                upd3(dzz, a1, a1, a2);
+                if (fsrow) szz = T(0);
+                if (zi >= 0) pml3(dzz, sh.psiz[3] + pz, zb, zi, a1, a1, a2);
+            } else {
+                sxx = A::mad(sxx, a.dt, dxx);
+                if (xi >= 0) sxx = pml_correct<T, MODE>(sxx, a.dt, dxx, sh.psix[3] + px, a.pml, L, xb, xi);
+                syy = A::mad(syy, a.dt, dyy);
+                if (yi >= 0) syy = pml_correct<T, MODE>(syy, a.dt, dyy, sh.psiy[3] + py, a.pml, L, yb, yi);
+                szz = A::mad(szz, a.dt, dzz);
+                if (fsrow) szz = T(0);
+                if (zi >= 0) szz = pml_correct<T, MODE>(szz, a.dt, dzz, sh.psiz[3] + pz, a.pml, L, zb, zi);
+            }
+            Sxx[o] = sxx; Syy[o] = syy; Szz[o] = szz;
+        }
+        // ---- Sxz: Dx+ Vz, Dz+ Vx
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, mxz);
+            sxz = A::mad(sxz, am, dxp.x);
+            if (xi >= 0) sxz = pml_correct<T, MODE>(sxz, am, dxp.x, sh.psix[4] + px, a.pml, L, xb + 3, xi);
+            sxz = A::mad(sxz, am, dzp.x);
+            if (zi >= 0) sxz = pml_correct<T, MODE>(sxz, am, dzp.x, sh.psiz[4] + pz, a.pml, L, zb + 3, zi);
+            Sxz[o] = sxz;
+        }
+        // ---- Syz: Dz+ Vy, Dy+ Vz
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, myz);
+            syz = A::mad(syz, am, dzp.y);
+            if (zi >= 0) syz = pml_correct<T, MODE>(syz, am, dzp.y, sh.psiz[5] + pz, a.pml, L, zb + 3, zi);
+            syz = A::mad(syz, am, dyp.x);
+            if (yi >= 0) syz = pml_correct<T, MODE>(syz, am, dyp.x, sh.psiy[4] + py, a.pml, L, yb + 3, yi);
+            Syz[o] = syz;
+        }
+        // ---- Sxy: Dy+ Vx, Dx+ Vy
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, mxy);
+            sxy = A::mad(sxy, am, dyp.y);
+            if (yi >= 0) sxy = pml_correct<T, MODE>(sxy, am, dyp.y, sh.psiy[5] + py, a.pml, L, yb + 3, yi);
+            sxy = A::mad(sxy, am, dxp.y);
+            if (xi >= 0) sxy = pml_correct<T, MODE>(sxy, am, dxp.y, sh.psix[5] + px, a.pml, L, xb + 3, xi);
+            Sxy[o] = sxy;
+        }
+#pragma unroll
+        for (int j = 0; j < 15; j++) { qz[j] = qz[j + 1]; qv[j] = qv[j + 1]; }
+        qz[15] = Vz[o + 8 * plane];
+        qv[15] = make_float2(Vx[o + 9 * plane], Vy[o + 9 * plane]);
+        sxx = nsxx; syy = nsyy; szz = nszz; syz = nsyz; sxz = nsxz; sxy = nsxy;
+        l = nl; l2m = nl2m; myz = nmyz; mxz = nmxz; mxy = nmxy;
+    }
+}
+
 // ---------------------------------------------------------------- sources and receivers
 // One CTA per shot: injection of every source set (lib/waves.cpp:4104-4244), then,
 // after a barrier, recording of every receiver set (lib/waves.cpp:4247-4400) of
@@ -570,6 +947,27 @@ __global__ void inject_record_e3d(const Shot3D<T> *shots, const InjRec3<T> *plan
     for (int k = 0; k < nsets; k++) record_set<T, MODE>(sh, pl[k], it);
 }
 
+template <bool ADJ>
+cudaError_t step_e3_fast(int half, const void *args, const void *coefs, int grid, cudaStream_t st)
+{
+    const Step3DArgs<float> &a = *reinterpret_cast<const Step3DArgs<float> *>(args);
+    const dim3 block(TX3, TY3);
+    if (half == 0) {
+        auto k = e3d_velocity_fast<ADJ>;
+        static const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          (int)sizeof(VelSmemF));
+        if (e != cudaSuccess) return e;
+        k<<<grid, block, sizeof(VelSmemF), st>>>(a, (const CoefSet3<float> *)coefs);
+    } else {
+        auto k = e3d_stress_fast<ADJ>;
+        static const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          (int)sizeof(StrSmemF));
+        if (e != cudaSuccess) return e;
+        k<<<grid, block, sizeof(StrSmemF), st>>>(a, (const CoefSet3<float> *)coefs);
+    }
+    return cudaGetLastError();
+}
+
 template <typename T, int MODE, bool ADJ>
 cudaError_t step_e3(int half, const void *args, const void *coefs, int grid, cudaStream_t st)
 {
@@ -602,8 +1000,7 @@ cudaError_t launch_step_e3d(int prec, int half, int adj, const void *args, const
     if (prec == PREC_F32_EXACT)
         return adj ? step_e3<float, MODE_IEEE, true>(half, args, coefs, grid, st)
                    : step_e3<float, MODE_IEEE, false>(half, args, coefs, grid, st);
-    return adj ? step_e3<float, MODE_FAST, true>(half, args, coefs, grid, st)
-               : step_e3<float, MODE_FAST, false>(half, args, coefs, grid, st);
+    return adj ? step_e3_fast<true>(half, args, coefs, grid, st) : step_e3_fast<false>(half, args, coefs, grid, st);
 }
 
 cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, int nsets, double dt,

@@ -134,7 +134,11 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
         L.rows = GUARD + (int)rup3(L.nyp, TY3) + GUARD;
         L.planes = GUARD + L.nzp + GUARD + 2;
         L.plane = (long long)L.pitch * L.rows;
-        if ((long long)L.plane * 10 > 0x7fffffffLL) { set_error("shot %d: plane of %lld cells too large", i, L.plane); return RSGPU_ERR_ARG; }
+        if ((long long)L.plane * L.planes > 0x7fffffffLL) {
+            set_error("shot %d: padded 3D arrays of %lld cells exceed the kernels' 32-bit offsets", i,
+                      (long long)L.plane * L.planes);
+            return RSGPU_ERR_ARG;
+        }
         const size_t fbytes = (size_t)L.plane * L.planes * es;
         for (int k = 0; k < nf3(); k++) L.f[k] = take(fbytes);
         for (int k = 0; k < npsi3(); k++) {
@@ -360,6 +364,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     }
     std::memcpy(meta.data() + m_tiles, tiles.data(), tiles.size() * sizeof(Tile3D));
     std::memcpy(meta.data() + m_coef, coefs.data(), coefs.size());
+    h_coefs = coefs;
     CU(cudaMemcpy(d_meta, meta.data(), m_end, cudaMemcpyHostToDevice));
     d_shots = (char *)d_meta + m_shots;
     d_injrec = (char *)d_meta + m_ir;
@@ -437,6 +442,11 @@ static void make_args3(void *out, const Plan3D &p)
     a.dt = (T)p.cfg.dt; a.dx = (T)p.cfg.dx; a.dy = (T)p.cfg.dy; a.dz = (T)p.cfg.dz;
     a.rdx = (T)1 / a.dx; a.rdy = (T)1 / a.dy; a.rdz = (T)1 / a.dz;
     a.pml = (const T *)p.d_pml;
+    const CoefSet3<T> &cs = *reinterpret_cast<const CoefSet3<T> *>(p.h_coefs.data());
+    for (int k = 0; k < NCOEF; k++) {
+        const T c[3] = {cs.cx[a.order * CROW3 + k], cs.cy[a.order * CROW3 + k], cs.cz[a.order * CROW3 + k]};
+        for (int ax = 0; ax < 3; ax++) a.cf[ax][k] = a.cf2[ax][k][0] = a.cf2[ax][k][1] = c[ax];
+    }
     std::memcpy(out, &a, sizeof a);
 }
 

@@ -43,6 +43,12 @@ struct Tile3D {
 
 template <typename T>
 struct Step3DArgs {
+    // the full-order coefficient rows of x, y and z (row `order` of CoefSet3; fast
+    // mode: pre-divided by the spacing), kept in the launch's parameter space so
+    // that the taps take them as constant operands; cf2 holds each value twice
+    // (the operand of a paired f32x2 multiply-add)
+    alignas(16) T cf2[3][NCOEF][2];
+    T cf[3][NCOEF];
     const Shot3D<T> *shots;
     const Tile3D *tiles;
     int ntiles, order, zc, lpml;

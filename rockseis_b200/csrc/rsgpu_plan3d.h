@@ -59,6 +59,7 @@ public:
     void *arena = nullptr, *d_meta = nullptr;
     size_t arena_bytes = 0;
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
+    std::vector<unsigned char> h_coefs;        // host copy of the CoefSet3 at d_coefs
     cudaStream_t stream = nullptr;
     long long launches = 0;
 
