@@ -857,7 +857,7 @@ def _e3d_ref_sample(args):
     return time.perf_counter() - t0
 
 
-def cpu_e3d_reference(ncheck_full, nt_sample=4, procs=None, f=E3D):
+def cpu_e3d_reference(ncheck_full, nt_sample=3, procs=None, f=E3D):
     """The reference's CPU gradient, one full-grid shot per process, nt_sample steps,
     extrapolated to nt by the propagation work (Revolve forward steps + adjoint steps
     + correlations) at the GPU run's snapshot count."""
