@@ -246,6 +246,9 @@ typedef struct {
     const void *gshift_vy;
     const void *data_vy;
     void *datamod_vy, *datares_vy;
+    /* acoustic 2D FWI: source illumination, nz*nx (FwiAcoustic2D::setSrcilum;
+       srcilum -= vpscale*Pfw*Pfw in crossCorr, lib/fwi.cpp:565-567), NULL = off */
+    void *srcilum;
 } rsgpu_adjoint_shot;
 
 /* FwiAcoustic2D<float>::run_optimal (cfg->physics RSGPU_ACOUSTIC2D),

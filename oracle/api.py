@@ -102,6 +102,7 @@ def ref() -> C.CDLL:
         _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
         _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+        _ref.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
         _ref.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
         _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
         _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
@@ -174,7 +175,8 @@ def _keep(*arrs, dtype=None):
     return [None if a is None else np.ascontiguousarray(a, dtype if dtype is not None else a.dtype) for a in arrs]
 
 
-def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit=0):
+def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit=0, srcilum=False):
+    """FwiAcoustic2D::run_optimal; with srcilum (float only) also the source illumination image."""
     t = "f" if dtype == np.float32 else "d"
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
@@ -186,6 +188,12 @@ def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit
     dr = np.zeros((nr, pb.nt), dtype)
     mis = C.c_double()
     vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=dtype)
+    if srcilum:
+        il = np.zeros((pb.nz, pb.nx), np.float32)
+        r = ref().ref_fwi_a2d_ilum_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
+                                     misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis), _p(il))
+        assert r == 1
+        return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value, srcilum=il)
     r = getattr(ref(), f"ref_fwi_a2d_{t}")(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
                                            ncheck, misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 1

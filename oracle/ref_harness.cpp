@@ -113,7 +113,7 @@ int mod_e3d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
 template <typename T>
 int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav,
             int nr, const double *gc, const T *obs, int ncheck, int misfit_type, T *vpgrad,
-            T *rhograd, T *wavgrad, T *datamod, T *datares, double *misfit)
+            T *rhograd, T *wavgrad, T *datamod, T *datares, double *misfit, T *srcilum = nullptr)
 {
     auto model = make_a2d<T>(g, vp, rho);
     auto src = make_data2d<T>(ns, g, sc, PRESSURE, SMAP, model->getGeom(), wav);
@@ -130,12 +130,18 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     fwi.setVpgrad(ivp);
     fwi.setRhograd(irho);
     fwi.setWavgrad(wg);
+    std::shared_ptr<Image2D<T>> ilum;
+    if (srcilum) {
+        ilum = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
+        fwi.setSrcilum(ilum);
+    }
     fwi.setMisfit_type((rs_fwimisfit)misfit_type);
     fwi.setNcheck(ncheck);
     fwi.setIncore(true);
     fwi.setSnapfile(tmpname("fwia2d"));
     int r = fwi.run_optimal();
     size_t n = (size_t)g->nx * g->nz;
+    if (srcilum) std::memcpy(srcilum, ilum->getImagedata(), sizeof(T) * n);
     std::memcpy(vpgrad, ivp->getImagedata(), sizeof(T) * n);
     std::memcpy(rhograd, irho->getImagedata(), sizeof(T) * n);
     std::memcpy(wavgrad, wg->getData(), sizeof(T) * (size_t)ns * g->nt);
@@ -588,6 +594,12 @@ int ref_fwi_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, 
                   float *datares, double *misfit)
 { return fwi_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, misfit_type, vpgrad, rhograd,
                         wavgrad, datamod, datares, misfit); }
+int ref_fwi_a2d_ilum_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                       const float *wav, int nr, const double *gc, const float *obs, int ncheck,
+                       int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod,
+                       float *datares, double *misfit, float *srcilum)
+{ return fwi_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, misfit_type, vpgrad, rhograd,
+                        wavgrad, datamod, datares, misfit, srcilum); }
 int ref_fwi_a2d_d(const ref_grid *g, const double *vp, const double *rho, int ns, const double *sc,
                   const double *wav, int nr, const double *gc, const double *obs, int ncheck,
                   int misfit_type, double *vpgrad, double *rhograd, double *wavgrad, double *datamod,

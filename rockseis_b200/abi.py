@@ -63,7 +63,8 @@ class AdjointShot(C.Structure):
                 ("data_vx", C.c_void_p), ("data_vz", C.c_void_p), ("vs", C.c_void_p), ("vsgrad", C.c_void_p),
                 ("datamod_vx", C.c_void_p), ("datamod_vz", C.c_void_p), ("datares_vx", C.c_void_p),
                 ("datares_vz", C.c_void_p), ("gmap_vy", C.c_void_p), ("gshift_vy", C.c_void_p),
-                ("data_vy", C.c_void_p), ("datamod_vy", C.c_void_p), ("datares_vy", C.c_void_p)]
+                ("data_vy", C.c_void_p), ("datamod_vy", C.c_void_p), ("datares_vy", C.c_void_p),
+                ("srcilum", C.c_void_p)]
 
 
 def _load() -> C.CDLL:

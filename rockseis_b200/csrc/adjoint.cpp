@@ -71,6 +71,7 @@ public:
     size_t slot_elems = 0, ck_es = 4;
     std::vector<CkptSeg> segs;
     std::vector<size_t> o_vp, o_vs, o_rho, o_obs, o_obsx, o_obsz, o_g0, o_g1, o_g2;
+    std::vector<size_t> o_ilum;      // acoustic FWI source illumination (0 = not asked for)
     size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
     std::vector<int> nx, nz, nrec, nsrc;
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
@@ -143,6 +144,10 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
         if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
         if (kind == RSGPU_KIND_FWI && (!s[i].vp || !s[i].rho)) { set_error("shot %d: vp/rho are null", i); return RSGPU_ERR_ARG; }
+        if (s[i].srcilum && (el || kind != RSGPU_KIND_FWI)) {
+            set_error("shot %d: source illumination belongs to the acoustic 2D FWI gradient (FwiAcoustic2D::setSrcilum)", i);
+            return RSGPU_ERR_ARG;
+        }
     }
     return RSGPU_OK;
 }
@@ -240,7 +245,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off = rup(off + std::max<size_t>(bytes, 1), 256); return r; };
-    for (auto *v : {&o_vp, &o_vs, &o_rho, &o_obs, &o_obsx, &o_obsz, &o_g0, &o_g1, &o_g2}) v->assign(ns, 0);
+    for (auto *v : {&o_vp, &o_vs, &o_rho, &o_obs, &o_obsx, &o_obsz, &o_g0, &o_g1, &o_g2, &o_ilum}) v->assign(ns, 0);
     nx.resize(ns); nz.resize(ns); nrec.resize(ns); nsrc.resize(ns);
     for (int i = 0; i < ns; i++) {
         nx[i] = s[i].shot.nx; nz[i] = s[i].shot.nz; nrec[i] = s[i].shot.nrec; nsrc[i] = s[i].shot.nsrc;
@@ -253,6 +258,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
             o_obs[i] = take((size_t)nrec[i] * cfg.nt * es);
             o_g0[i] = take(n2 * gs);
             o_g1[i] = take(n2 * gs);
+            if (!elastic() && s[i].srcilum) o_ilum[i] = take(n2 * gs);
             if (elastic()) {
                 o_vs[i] = take(n2 * es);
                 o_obsx[i] = take((size_t)nrec[i] * cfg.nt * es);
@@ -350,6 +356,7 @@ void Adjoint::build_desc(std::vector<unsigned char> &corr, std::vector<unsigned 
         c.rho = kind == RSGPU_KIND_FWI ? (const T *)D(o_rho[i]) : nullptr;
         c.g0 = D(o_g0[i]);
         c.g1 = kind == RSGPU_KIND_FWI ? D(o_g1[i]) : nullptr;
+        c.ilum = o_ilum[i] ? D(o_ilum[i]) : nullptr;
         c.nx = nx[i]; c.nz = nz[i]; c.pitch = F.pitch; c.lpml = cfg.lpml;
         std::memcpy(corr.data() + i * sizeof c, &c, sizeof c);
         Resid2D<T> r{};
@@ -451,6 +458,7 @@ rsgpu_status Adjoint::run()
         CU(cudaMemsetAsync(D(o_g0[i]), 0, n2 * (kind == RSGPU_KIND_FWI ? 1 : (size_t)nhx * nhz) * gs, stream));
         if (kind == RSGPU_KIND_FWI) CU(cudaMemsetAsync(D(o_g1[i]), 0, n2 * gs, stream));
         if (elastic()) CU(cudaMemsetAsync(D(o_g2[i]), 0, n2 * gs, stream));
+        if (o_ilum[i]) CU(cudaMemsetAsync(D(o_ilum[i]), 0, n2 * gs, stream));
     }
     ST(fw->set_recording(true));
     RevolveSchedule rev(nt, ncheck);
@@ -554,6 +562,7 @@ rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
             ST(fetch(o_g1[i], n2 * gs));
             accumulate(s[i].rhograd, n2);
         }
+        if (o_ilum[i] && s[i].srcilum) { ST(fetch(o_ilum[i], n2 * gs)); accumulate(s[i].srcilum, n2); }
         void *mods[3] = {s[i].shot.rec_out, elastic() ? s[i].datamod_vx : nullptr, elastic() ? s[i].datamod_vz : nullptr};
         void *ress[3] = {s[i].datares, elastic() ? s[i].datares_vx : nullptr, elastic() ? s[i].datares_vz : nullptr};
         for (int k = 0; k < 3; k++) {

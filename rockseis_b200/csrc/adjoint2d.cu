@@ -30,6 +30,7 @@ namespace {
 // vpgrad -= (-2/vp) * Pfw * (dx- Vx_adj + dz- Vz_adj)
 // rhograd -= (-1/rho) * Pfw * (same)
 // rhograd += 1/2 [ Vx_adj Rx dx+ Pfw ] averaged over the two staggered x-faces (and z)
+// srcilum -= (-2/vp) * Pfw * Pfw   (when the shot asks for the source illumination)
 // on the interior 1..n-2 of the unpadded window.  G is the accumulator type.
 template <typename T, bool EXACT, typename G>
 __global__ void __launch_bounds__(256) corr_fwi_a2d(const Corr2D<T> *desc, T dx, T dz)
@@ -47,10 +48,11 @@ __global__ void __launch_bounds__(256) corr_fwi_a2d(const Corr2D<T> *desc, T dx,
     const T vp = c.vp[u], rho = c.rho[u];
     G *vg = (G *)c.g0 + u;
     G *rg = (G *)c.g1 + u;
-    T a, b, uder;
+    T a, b, uder, il = 0;
     if (EXACT) {
         using O = X<T>;
         const T vpscale = O::rnd(__ddiv_rn(-2.0, (double)vp));
+        if (c.ilum) il = O::mul(O::mul(vpscale, ws), ws);
         const T rhoscale1 = O::rnd(__ddiv_rn(-1.0, (double)rho));
         const T mrxx = O::div(O::sub(wx0, wx1), dx);
         const T mrzz = O::div(O::sub(wz0, wz1), dz);
@@ -70,6 +72,7 @@ __global__ void __launch_bounds__(256) corr_fwi_a2d(const Corr2D<T> *desc, T dx,
         const T s = (wx0 - wx1) * rdx + (wz0 - wz1) * rdz;
         a = (T(-2) / vp) * ws * s;
         b = (T(-1) / rho) * ws * s;
+        if (c.ilum) il = (T(-2) / vp) * ws * ws;
         uder = T(0.5) * ((wx0 * rx0 * (wsr - ws) + wx1 * rx1 * (ws - wsl)) * rdx +
                          (wz0 * rz0 * (wsd - ws) + wz1 * rz1 * (ws - wsu)) * rdz);
     }
@@ -79,9 +82,17 @@ __global__ void __launch_bounds__(256) corr_fwi_a2d(const Corr2D<T> *desc, T dx,
         *(T *)vg = EXACT ? O::sub(*(T *)vg, a) : *(T *)vg - a;
         const T r1 = EXACT ? O::sub(*(T *)rg, b) : *(T *)rg - b;
         *(T *)rg = EXACT ? O::add(r1, uder) : r1 + uder;
+        if (c.ilum) {
+            T *ig = (T *)c.ilum + u;
+            *ig = EXACT ? O::sub(*ig, il) : *ig - il;
+        }
     } else {
         *vg = __dsub_rn((double)*vg, (double)a);
         *rg = __dadd_rn(__dsub_rn((double)*rg, (double)b), (double)uder);
+        if (c.ilum) {
+            G *ig = (G *)c.ilum + u;
+            *ig = __dsub_rn((double)*ig, (double)il);
+        }
     }
 }
 

@@ -116,6 +116,10 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
         if (sh.nsrc < 1 || sh.nrec < 1) { set_error("shot %d: needs sources and receivers", i); return RSGPU_ERR_ARG; }
         if (!s[i].data) { set_error("shot %d: data is null", i); return RSGPU_ERR_ARG; }
+        if (s[i].srcilum) {
+            set_error("shot %d: the 3D gradients have no source illumination (FwiAcoustic3D/FwiElastic3D::crossCorr)", i);
+            return RSGPU_ERR_ARG;
+        }
         if (k_ == RSGPU_KIND_FWI && (!s[i].vp || !s[i].rho)) { set_error("shot %d: vp/rho are null", i); return RSGPU_ERR_ARG; }
     }
     int ndev = 0;

@@ -15,6 +15,7 @@ struct Corr2D {
     const T *rx, *rz;           // staggered inverse densities of the forward plan
     const T *vp, *rho;          // unpadded models (FWI gradient scaling)
     void *g0, *g1;              // FWI: vpgrad, rhograd; RTM: g0 = image [nhz][nhx][nz][nx]
+    void *ilum;                 // FWI: source illumination [nz][nx], or null
     int nx, nz, pitch, lpml;
 };
 

@@ -643,9 +643,10 @@ class FwiAcoustic2D(_Adjoint):
 
     def __init__(self, model=None, source=None, dataP=None, order=4, snapinc=1, precision=None):
         super().__init__(model, source, dataP, order, snapinc, precision)
-        self.vpgrad = self.rhograd = self.wavgrad = self.datamodP = self.dataresP = None
+        self.vpgrad = self.rhograd = self.wavgrad = self.datamodP = self.dataresP = self.srcilum = None
         self.misfit = 0.0
 
+    def setSrcilum(self, img): self.srcilum = img
     def setVpgrad(self, img): self.vpgrad = img
     def setRhograd(self, img): self.rhograd = img
     def setWavgrad(self, d): self.wavgrad = d
@@ -663,6 +664,7 @@ class FwiAcoustic2D(_Adjoint):
         a.wavgrad = ptr(self.wavgrad.data) if self.wavgrad is not None else None
         a.datares = ptr(self.dataresP.data) if self.dataresP is not None else None
         a.shot.rec_out = ptr(self.datamodP.data) if self.datamodP is not None else None
+        a.srcilum = ptr(self.srcilum.getImagedata()) if self.srcilum is not None else None
         self._mis = C.c_double(0.0)
         a.misfit = C.pointer(self._mis)
         return a

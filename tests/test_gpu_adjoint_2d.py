@@ -52,6 +52,42 @@ def assert_same(got, ref):
     assert got["misfit"] == ref["misfit"]
 
 
+@pytest.mark.parametrize("ncheck", [4, 300])
+def test_fwi_source_illumination_equals_reference(require_gpu, ncheck):
+    # FwiAcoustic2D::setSrcilum: srcilum -= (-2/vp) Pfw^2 inside crossCorr, checked against
+    # the reference library itself together with every other output
+    from oracle import api
+    if not api.ref_available():
+        pytest.skip("reference library oracle/_ref not built")
+    c = fwi_case()
+    ref = api.ref_fwi_a2d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords, c.obs, ncheck,
+                          srcilum=True)
+    f = make_fwi(c, ncheck=ncheck)
+    f.setSrcilum(Image2D("srcilum", c.model, 1, 1, c.precision))
+    assert f.run_optimal() == 1
+    assert_same(outputs(f), ref)
+    il = f.srcilum.getImagedata()[0, 0]
+    assert np.abs(ref["srcilum"]).max() > 0
+    assert np.array_equal(il, ref["srcilum"]), f"srcilum: max abs diff {np.abs(il - ref['srcilum']).max()}"
+
+
+def test_fwi_source_illumination_batched_fp64_accumulation(require_gpu):
+    # batched windows, only the second shot asks for the illumination; FP64 accumulation
+    # against the per-shot exact result
+    cases = [fwi_case(nx=81, nz=61, seed=1, scoord=(400.3, 23.7)), fwi_case(nx=97, nz=53, seed=2, scoord=(150.9, 31.2))]
+    exact = []
+    for c in cases:
+        f = make_fwi(c, ncheck=6)
+        f.setSrcilum(Image2D("srcilum", c.model, 1, 1, c.precision))
+        f.run_optimal()
+        exact.append(f.srcilum.getImagedata()[0, 0].copy())
+    jobs = [make_fwi(c, ncheck=6, accum=abi.ACCUM_F64) for c in cases]
+    jobs[1].setSrcilum(Image2D("srcilum", cases[1].model, 1, 1, cases[1].precision))
+    fwi_gradient_batch(jobs)
+    assert jobs[0].srcilum is None
+    assert rel_l2(jobs[1].srcilum.getImagedata()[0, 0], exact[1]) < 1e-6
+
+
 @pytest.mark.parametrize("ncheck", [2, 5, 17, 300])
 def test_fwi_gradient_exact_bitwise(require_gpu, ncheck):
     c = fwi_case()

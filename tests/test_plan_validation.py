@@ -4,6 +4,8 @@ grids narrower than the stencil, missing arrays, unknown fields and physics,
 and the gradient drivers' own option checks."""
 import ctypes as C
 
+import numpy as np
+
 import pytest
 
 from rockseis_b200 import abi
@@ -76,3 +78,20 @@ def test_gradient_driver_option_checks():
     o = abi.AdjointOpts()
     o.ncheck, o.nhx, o.nhz, o.nhy = 5, 2, 1, 1                               # RTM lags must be odd
     assert abi.lib.rsgpu_rtm_image(C.byref(cfg), C.byref(o), 1, C.byref(a)) == abi.ERR_ARG
+
+
+def test_source_illumination_only_for_acoustic_2d_fwi():
+    """FwiAcoustic2D alone has setSrcilum: elastic and 3D gradients and RTM refuse it."""
+    c = Case2D(abi.ACOUSTIC2D, nt=20)
+    keep: list = []
+    cfg = make_config(c.model, c.order, c.nt, c.dt, abi.F32_EXACT)
+    a = abi.AdjointShot()
+    a.shot = make_shot(c.model, c.src, c.rec, keep)
+    ilum = np.zeros((c.model.nz, c.model.nx), np.float32)
+    a.srcilum = ilum.ctypes.data
+    a.data = a.vp = a.rho = a.vs = ilum.ctypes.data
+    o = abi.AdjointOpts()
+    o.ncheck, o.nhx, o.nhz = 4, 1, 1
+    st = abi.lib.rsgpu_rtm_image(C.byref(cfg), C.byref(o), 1, C.byref(a))
+    assert st == abi.ERR_ARG
+    assert b"illumination" in abi.lib.rsgpu_last_error()
