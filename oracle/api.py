@@ -18,6 +18,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "librsoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "librsref.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "librsref_gpu.so")
+INTEGRATION = os.path.join(os.path.dirname(HERE), "integration")
 # Root of the reference source tree, from the environment (the build recipe sets it);
 # without it only the C restatement is built.
 REFSRC_ENV = "RSGPU_REFERENCE_SRC"
@@ -29,6 +31,9 @@ def build(ref: bool = True) -> None:
     use_ref = ref and bool(refsrc) and os.path.isdir(refsrc)
     targets = ["oracle"] + (["ref", f"REFSRC={refsrc}"] if use_ref else [])
     subprocess.run(["make", "-s", "-C", HERE, f"-j{os.cpu_count() or 4}"] + targets, check=True)
+    gpu_lib = os.path.join(os.path.dirname(HERE), "rockseis_b200", "librsgpu.so")
+    if use_ref and os.path.exists(gpu_lib):
+        subprocess.run(["make", "-s", "-C", INTEGRATION, f"-j{os.cpu_count() or 4}", f"REFSRC={refsrc}"], check=True)
 
 
 class OrcGrid(C.Structure):
@@ -84,46 +89,72 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+def _load_ref(path: str) -> C.CDLL:
+    """The harness library at path with its argument types declared."""
+    lib = C.CDLL(path)
+    V, I, D = C.c_void_p, C.c_int, C.c_double
+    G = C.POINTER(RefGrid)
+    for t in ("f", "d"):
+        getattr(lib, f"ref_der_{t}").argtypes = [I, I, I, D, D, D, I, I, V, V]
+        getattr(lib, f"ref_pml_tables_{t}").argtypes = [I, D, V]
+        getattr(lib, f"ref_mod_a2d_{t}").argtypes = [G, V, V, I, V, V, I, I, V, I, V]
+        getattr(lib, f"ref_mod_e2d_{t}").argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
+        getattr(lib, f"ref_fwi_a2d_{t}").argtypes = [G, V, V, I, V, V, I, V, V, I, I, V, V, V, V, V, V]
+    lib.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
+    lib.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
+    lib.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+    lib.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+    lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
+    lib.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+    lib.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
+    lib.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
+    lib.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
+    lib.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
+    lib.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
+    lib.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
+    lib.ref_stagger_e2d_f.argtypes = [G, V, V, V, V, V, V, V, V]
+    lib.ref_stagger_a3d_f.argtypes = [G, V, V, V, V, V, V]
+    lib.ref_stagger_e3d_f.argtypes = [G, V, V, V] + [V] * 8
+    lib.ref_makemap2d_f.argtypes = [G, I, V, I, V, V]
+    lib.ref_makemap2d_field_f.argtypes = [G, I, V, I, I, V, V]
+    lib.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
+    lib.ref_makemap3d_field_f.argtypes = [G, I, V, I, I, V, V]
+    lib.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
+    lib.ref_revolve_numforw.argtypes = [I, I]
+    lib.ref_revolve_adjust.argtypes = [I]
+    lib.ref_steps_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
+    lib.ref_steps_a2d_f.argtypes = [G, V, V, I, V, V, I, I, V]
+    lib.ref_steps_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
+    return lib
+
+
 def ref() -> C.CDLL:
+    """The unmodified reference library and its harness."""
     global _ref
     if _ref is None:
         if not os.path.exists(REF_SO):
             raise FileNotFoundError("reference oracle not built (oracle/_ref/librsref.so)")
-        _ref = C.CDLL(REF_SO)
-        V, I, D = C.c_void_p, C.c_int, C.c_double
-        G = C.POINTER(RefGrid)
-        for t in ("f", "d"):
-            getattr(_ref, f"ref_der_{t}").argtypes = [I, I, I, D, D, D, I, I, V, V]
-            getattr(_ref, f"ref_pml_tables_{t}").argtypes = [I, D, V]
-            getattr(_ref, f"ref_mod_a2d_{t}").argtypes = [G, V, V, I, V, V, I, I, V, I, V]
-            getattr(_ref, f"ref_mod_e2d_{t}").argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
-            getattr(_ref, f"ref_fwi_a2d_{t}").argtypes = [G, V, V, I, V, V, I, V, V, I, I, V, V, V, V, V, V]
-        _ref.ref_mod_a3d_f.argtypes = [G, V, V, I, V, V, I, I, V, I, V]
-        _ref.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
-        _ref.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
-        _ref.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
-        _ref.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
-        _ref.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
-        _ref.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
-        _ref.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
-        _ref.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
-        _ref.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
-        _ref.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
-        _ref.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
-        _ref.ref_stagger_e2d_f.argtypes = [G, V, V, V, V, V, V, V, V]
-        _ref.ref_stagger_a3d_f.argtypes = [G, V, V, V, V, V, V]
-        _ref.ref_stagger_e3d_f.argtypes = [G, V, V, V] + [V] * 8
-        _ref.ref_makemap2d_f.argtypes = [G, I, V, I, V, V]
-        _ref.ref_makemap2d_field_f.argtypes = [G, I, V, I, I, V, V]
-        _ref.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
-        _ref.ref_makemap3d_field_f.argtypes = [G, I, V, I, I, V, V]
-        _ref.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
-        _ref.ref_revolve_numforw.argtypes = [I, I]
-        _ref.ref_revolve_adjust.argtypes = [I]
-        _ref.ref_steps_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
-        _ref.ref_steps_a2d_f.argtypes = [G, V, V, I, V, V, I, I, V]
-        _ref.ref_steps_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
+        _ref = _load_ref(REF_SO)
     return _ref
+
+
+_ref_gpu = None
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+def ref_gpu() -> C.CDLL:
+    """The reference library built with the GPU binding (integration/rockseis_gpu.cpp):
+    its ModellingAcoustic2D/ModellingElastic2D<float>::run and
+    FwiAcoustic2D<float>::run_optimal call librsgpu; same harness entry points."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        if not os.path.exists(REF_GPU_SO):
+            raise FileNotFoundError("reference build with the GPU binding missing (oracle/_ref/librsref_gpu.so)")
+        _ref_gpu = _load_ref(REF_GPU_SO)
+    return _ref_gpu
 
 
 # ---------------------------------------------------------------- problem description
@@ -145,26 +176,26 @@ class Problem2D:
                        int(self.fs), self.dx, self.dz, self.dt, self.nt)
 
 
-def ref_modelling_a2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32):
+def ref_modelling_a2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32, lib=None):
     t = "f" if dtype == np.float32 else "d"
     out = np.zeros((len(gcoords), pb.nt), dtype)
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     vp, rho, w = (np.ascontiguousarray(a, dtype) for a in (pb.vp, pb.rho, wav))
-    r = getattr(ref(), f"ref_mod_a2d_{t}")(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), sfield, len(gc),
+    r = getattr(lib or ref(), f"ref_mod_a2d_{t}")(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), sfield, len(gc),
                                            _p(gc), rfield, _p(out))
     assert r == 1
     return out
 
 
-def ref_modelling_e2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32):
+def ref_modelling_e2d(pb, scoords, wav, sfield, gcoords, rfield, dtype=np.float32, lib=None):
     t = "f" if dtype == np.float32 else "d"
     out = np.zeros((len(gcoords), pb.nt), dtype)
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     vp, vs, rho = (np.ascontiguousarray(a, dtype) for a in (pb.vp, pb.vs, pb.rho))
     w = np.ascontiguousarray(wav, dtype)
-    r = getattr(ref(), f"ref_mod_e2d_{t}")(C.byref(g), _p(vp), _p(vs), _p(rho), len(sc), _p(sc), _p(w), sfield,
+    r = getattr(lib or ref(), f"ref_mod_e2d_{t}")(C.byref(g), _p(vp), _p(vs), _p(rho), len(sc), _p(sc), _p(w), sfield,
                                            len(gc), _p(gc), rfield, _p(out))
     assert r == 1
     return out
@@ -175,7 +206,7 @@ def _keep(*arrs, dtype=None):
     return [None if a is None else np.ascontiguousarray(a, dtype if dtype is not None else a.dtype) for a in arrs]
 
 
-def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit=0, srcilum=False):
+def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit=0, srcilum=False, lib=None):
     """FwiAcoustic2D::run_optimal; with srcilum (float only) also the source illumination image."""
     t = "f" if dtype == np.float32 else "d"
     g = pb.ref_grid()
@@ -190,11 +221,11 @@ def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit
     vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=dtype)
     if srcilum:
         il = np.zeros((pb.nz, pb.nx), np.float32)
-        r = ref().ref_fwi_a2d_ilum_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
+        r = (lib or ref()).ref_fwi_a2d_ilum_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
                                      misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis), _p(il))
         assert r == 1
         return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value, srcilum=il)
-    r = getattr(ref(), f"ref_fwi_a2d_{t}")(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
+    r = getattr(lib or ref(), f"ref_fwi_a2d_{t}")(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
                                            ncheck, misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 1
     return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
