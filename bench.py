@@ -786,7 +786,7 @@ def run_a3d(args, device=0, f=A3D):
 
 
 # ---------------------------------------------------------------- 3D elastic FWI workload
-E3D = dict(W.C5, ncheck_max=40, nt_bench=200, plain_sample=1)
+E3D = dict(W.C5, ncheck=10, nt_bench=200, plain_sample=1)
 
 
 def e3d_config(nt, ncheck, f=E3D):
@@ -857,10 +857,10 @@ def _e3d_ref_sample(args):
     return time.perf_counter() - t0
 
 
-def cpu_e3d_reference(ncheck_full, nt_sample=3, procs=None, f=E3D):
+def cpu_e3d_reference(ncheck_full, nt_target, nt_sample=3, procs=None, f=E3D):
     """The reference's CPU gradient, one full-grid shot per process, nt_sample steps,
-    extrapolated to nt by the propagation work (Revolve forward steps + adjoint steps
-    + correlations) at the GPU run's snapshot count."""
+    extrapolated to nt_target by the propagation work (Revolve forward steps + adjoint
+    steps + correlations) at the GPU run's snapshot count."""
     import multiprocessing as mp
     from oracle import api
     from rockseis_b200 import abi
@@ -872,10 +872,10 @@ def cpu_e3d_reference(ncheck_full, nt_sample=3, procs=None, f=E3D):
 
     def work(nt, nc):
         return abi.lib.rsgpu_revolve_numforw(nt, nc) + 1 + 2 * nt
-    t_shot = max(times) * work(f["nt"], ncheck_full) / work(nt_sample, 2)
+    t_shot = max(times) * work(nt_target, ncheck_full) / work(nt_sample, 2)
     return {"value": float("%.4g" % (procs / t_shot)), "unit": "shots/s", "cores": procs, "kind": "reference",
             "sample": f"{procs} processes x 1 shot, full 296^3 padded grid, nt={nt_sample} (ncheck 2), "
-                      f"extrapolated to nt={f['nt']} with ncheck {ncheck_full} by Revolve forward + adjoint + "
+                      f"extrapolated to nt={nt_target} with ncheck {ncheck_full} by Revolve forward + adjoint + "
                       f"correlation steps", "max_process_s": round(max(times), 3)}
 
 
@@ -958,14 +958,10 @@ def run_e3d(args, device=0, f=E3D):
     for rs, o in zip(recsets, obs):
         for r, d in zip(rs, o):
             r.data = d
-    # snapshots: as many as fit next to the two propagators of every shot
+    # ten Revolve snapshots: what fits next to the two propagators of 16 shots in HBM
     L = f["lpml"]
     pts = (f["nx"] + 2 * L) * (f["ny"] + 2 * L) * (f["nz"] + 2 * L)
-    psi = 18 * 2 * L * (f["nx"] + 2 * L) * (f["ny"] + 2 * L)
-    slot = ns * (9 * pts + psi) * 2
-    free, _ = torch.cuda.mem_get_info(device)
-    need = ns * (2 * 9 * pts * 1.33 + 8 * pts * 1.33 + 2 * psi + 3 * f["nx"] * f["ny"] * f["nz"] * 2) * 4
-    ncheck = int(max(2, min(f["ncheck_max"], (free * 0.92 - need) // slot)))
+    ncheck = f["ncheck"]
     jobs = e3d_jobs(m, srcs, recsets, prec, ckpt, accum, ncheck)
     batch = AdjointBatch(jobs)
     batch.run()                                   # warm-up
@@ -1123,7 +1119,7 @@ def main():
 
     if args.impl == "reference" and args.workload == "elastic3d_fwi":
         if int(os.environ.get("RANK", "0")) == 0:
-            r = cpu_e3d_reference(E3D["ncheck_max"])
+            r = cpu_e3d_reference(E3D["ncheck"], args.e3d_nt)
             if r is None:
                 print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
                 return
@@ -1131,7 +1127,7 @@ def main():
                               "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1,
                               "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                               "dtype": "f32", "data": "synthetic",
-                              "config": e3d_config(E3D["nt"], E3D["ncheck_max"]), "cpu_baseline": r,
+                              "config": e3d_config(args.e3d_nt, E3D["ncheck"]), "cpu_baseline": r,
                               "e2e": {"value": r["value"], "unit": "shots/s", "h2d_bytes_per_step": 0,
                                       "d2h_bytes_per_step": 0}}))
         return
@@ -1205,7 +1201,7 @@ def main():
         import torch
         torch.cuda.set_device(local)
         r = run_e3d(args, device=local)
-        cpu = None if args.no_cpu_baseline else cpu_e3d_reference(r["ncheck"])
+        cpu = None if args.no_cpu_baseline else cpu_e3d_reference(r["ncheck"], args.e3d_nt)
         line = {"metric": "FWI gradient shots/s", "value": r["shots_per_s_batched"], "unit": "shots/s", "n_gpus": 1,
                 "steps": args.fwi_steps, "warmup": 1, "ms_per_step": round(r["s_per_batch"] * 1e3, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -619,14 +619,18 @@ template <> struct Store<__nv_bfloat16> {
 };
 
 // Power-of-two scale that maps the block's largest magnitude below 2^15 (exact
-// scaling; FP16's largest finite value is 65504).
+// scaling; FP16's largest finite value is 65504).  The exponent is kept at or
+// above -126 so that the scale and its reciprocal are both normal floats: a block
+// whose largest magnitude is itself subnormal (the numerical tails ahead of a
+// wavefront in C-PML memory) would otherwise get a zero scale and an infinite
+// reciprocal.
 __device__ __forceinline__ float pow2_scale(unsigned maxbits)
 {
     const float m = __uint_as_float(maxbits);
     if (!(m > 0.0f) || !isfinite(m)) return 1.0f;
     int e;
     frexpf(m, &e);          // m < 2^e
-    return ldexpf(1.0f, e - 15);
+    return ldexpf(1.0f, max(e - 15, -126));
 }
 
 // Element offset of row r of a block (rows of a 3D block run plane by plane).

@@ -33,7 +33,7 @@ class Fwi3DCase:
     by the reference in a model with a slow block."""
 
     def __init__(self, nx=22, ny=18, nz=20, lpml=6, dx=10.0, dt=1e-3, nt=70, fs=0, seed=11, sfield=abi.PRESSURE,
-                 scoord=(104.3, 91.7, 62.2), nrec=8, precision=abi.F32_EXACT):
+                 scoord=(104.3, 91.7, 62.2), nrec=8, precision=abi.F32_EXACT, amp=AMP):
         rng = np.random.default_rng(seed)
         self.nt, self.dt, self.precision, self.sfield = nt, dt, precision, sfield
         t = abi.real_dtype(precision)
@@ -51,7 +51,7 @@ class Fwi3DCase:
         self.scoords = np.array([scoord])
         src = Data3D(1, nt, dt, 0.0, precision)
         src.scoords[:] = self.scoords
-        src.data[:] = AMP * synth.ricker(nt, dt, 25.0, t)[None, :]
+        src.data[:] = amp * synth.ricker(nt, dt, 25.0, t)[None, :]
         src.setField(sfield)
         src.makeMap(m, 0)
         self.src = src
@@ -66,7 +66,7 @@ class Fwi3DCase:
             self.recs.append(r)
         self.pb = api.Problem3D(nx, ny, nz, dx, dx, dx, lpml, 8, fs, dt, nt, vp, rho, vs)
         pbt = api.Problem3D(nx, ny, nz, dx, dx, dx, lpml, 8, fs, dt, nt, vt, rho, vs)
-        wav32 = (AMP * synth.ricker(nt, dt, 25.0)[None, :]).astype(np.float32)
+        wav32 = (amp * synth.ricker(nt, dt, 25.0)[None, :]).astype(np.float32)
         self.obs = [api.ref_modelling_e3d(pbt, self.scoords, wav32, sfield, self.gcoords, f).astype(t)
                     for f in (abi.VX, abi.VY, abi.VZ)]
 
@@ -170,3 +170,19 @@ def test_elastic3d_fwi_lossless_fast_within_fp32(require_gpu):
         base, err = rel_l2(exact[k], ref64[k]), rel_l2(got[k], ref64[k])
         print(f"{k}: FMA, lossless checkpoints {err:.3g}, reference float {base:.3g} (vs FP64)")
         assert err <= max(2.0 * base, 1e-5), k
+
+
+def test_elastic3d_fwi_16bit_checkpoints_of_subnormal_tails(require_gpu):
+    # unit source amplitude: C-PML memory blocks whose largest value is subnormal are
+    # checkpointed; their scale must stay finite (the gradient stays finite and close)
+    c = Fwi3DCase(amp=1.0)
+    lossless = make_job(c, precision=abi.F32_FAST, ncheck=6, accum=abi.ACCUM_F64)
+    lossless.run_optimal()
+    ref = outputs(lossless)
+    for ckpt in (abi.CKPT_F16, abi.CKPT_BF16):
+        f = make_job(Fwi3DCase(amp=1.0), precision=abi.F32_FAST, ncheck=6, ckpt=ckpt, accum=abi.ACCUM_F64)
+        f.run_optimal()
+        got = outputs(f)
+        for k in ("vpgrad", "vsgrad", "rhograd"):
+            assert np.isfinite(got[k]).all(), (ckpt, k)
+            assert rel_l2(got[k], ref[k]) < 5e-3, (ckpt, k, rel_l2(got[k], ref[k]))
