@@ -488,6 +488,8 @@ rsgpu_status Adjoint3D::run()
     }
     launches += fw->launches + bw->launches - l0;
     CU(cudaStreamSynchronize(stream));
+    ST(fw->check_device_error());
+    ST(bw->check_device_error());
     ran = true;
     return RSGPU_OK;
 }

@@ -40,6 +40,19 @@ __device__ __forceinline__ void load_coefs3e(CoefSet3<T> &s, const CoefSet3<T> *
     for (int i = tid; i < (int)(sizeof(CoefSet3<T>) / sizeof(T)); i += blockDim.x * blockDim.y) dst[i] = src[i];
 }
 
+// Copy the shot descriptor into shared memory: the field pointers are then read
+// from a space that the kernel's global stores cannot alias, so the compiler may
+// keep or re-read them freely instead of reloading them from global memory after
+// every store.  Visible after the block's next barrier.
+template <typename T>
+__device__ __forceinline__ void stage_shot(Shot3D<T> &dst, const Shot3D<T> *src)
+{
+    constexpr int n = sizeof(Shot3D<T>) / sizeof(int);
+    static_assert(sizeof(Shot3D<T>) % sizeof(int) == 0, "descriptor size");
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid < n) reinterpret_cast<int *>(&dst)[tid] = reinterpret_cast<const int *>(src)[tid];
+}
+
 // Staggered derivative with all NCOEF taps: b[0] = f[i-7] (forward) or f[i-8]
 // (backward); sum_k (b[8+k] - b[7-k]) c_k in the reference's order.
 template <typename T, int MODE>
@@ -125,10 +138,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_velocity(Step3DArgs<T> a, con
     using A = Ar<T, MODE>;
     extern __shared__ __align__(16) unsigned char smraw[];
     VelSmem<T> &S = *reinterpret_cast<VelSmem<T> *>(smraw);
-    load_coefs3e(S.cs, coefs);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ Shot3D<T> shs;
     const Tile3D tl = a.tiles[blockIdx.x];
-    const Shot3D<T> &sh = a.shots[tl.shot];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Shot3D<T> &sh = shs;
     const int ix = tl.x0 + tx, iy = tl.y0 + ty;
     const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
     const long long plane = sh.plane;
@@ -301,10 +317,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress(Step3DArgs<T> a, const
     using A = Ar<T, MODE>;
     extern __shared__ __align__(16) unsigned char smraw[];
     StrSmem<T> &S = *reinterpret_cast<StrSmem<T> *>(smraw);
-    load_coefs3e(S.cs, coefs);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ Shot3D<T> shs;
     const Tile3D tl = a.tiles[blockIdx.x];
-    const Shot3D<T> &sh = a.shots[tl.shot];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Shot3D<T> &sh = shs;
     const int ix = tl.x0 + tx, iy = tl.y0 + ty;
     const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
     const long long plane = sh.plane;
@@ -512,10 +531,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_velocity_fast(Step3DArgs<floa
     using A = Ar<T, MODE>;
     extern __shared__ __align__(16) unsigned char smraw[];
     VelSmemF &S = *reinterpret_cast<VelSmemF *>(smraw);
-    load_coefs3e(S.cs, coefs);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ Shot3D<T> shs;
     const Tile3D tl = a.tiles[blockIdx.x];
-    const Shot3D<T> &sh = a.shots[tl.shot];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Shot3D<T> &sh = shs;
     const int ix = tl.x0 + tx, iy = tl.y0 + ty;
     const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
     const int plane = (int)sh.plane;   // a field holds fewer than 2^31 elements
@@ -675,10 +697,13 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress_fast(Step3DArgs<float>
     using A = Ar<T, MODE>;
     extern __shared__ __align__(16) unsigned char smraw[];
     StrSmemF &S = *reinterpret_cast<StrSmemF *>(smraw);
-    load_coefs3e(S.cs, coefs);
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ Shot3D<T> shs;
     const Tile3D tl = a.tiles[blockIdx.x];
-    const Shot3D<T> &sh = a.shots[tl.shot];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    __syncthreads();
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const Shot3D<T> &sh = shs;
     const int ix = tl.x0 + tx, iy = tl.y0 + ty;
     const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
     const int plane = (int)sh.plane;   // a field holds fewer than 2^31 elements
@@ -845,6 +870,374 @@ __global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress_fast(Step3DArgs<float>
     }
 }
 
+// ---------------------------------------------------------------- fast mode with TMA-staged planes
+// The forward velocity step and both stress steps of RSGPU_F32_FAST with every
+// plane tile brought in by TMA (cp.async.bulk.tensor.2d, one thread issuing,
+// completion on an mbarrier per stage) NSTG3 - 1 planes ahead of the plane being
+// computed: the loads in flight no longer depend on registers or resident warps.
+// The z-derivatives still come from 16-plane register windows, refilled by plain
+// loads eight planes ahead.  Same stencils, C-PML and update order as
+// e3d_velocity_fast / e3d_stress_fast.  Every wait is bounded (2 s): on timeout the
+// CTA records RSGPU_ERR_TIMEOUT in the error word and stops.
+constexpr int NSTG3 = 3;
+
+struct VelStageT {
+    float xx[TY3][WX];         // Sxx, x halo
+    float xz[TY3][WX];         // Sxz, x halo
+    float xy[HY][WX];          // Sxy, x and y halos
+    float yy[HY][TX3];         // Syy, y halo
+    float yz[HY][TX3];         // Syz, y halo
+    float pv[6][TY3][TX3];     // Vx, Vy, Vz, Rx, Ry, Rz
+};
+struct StrStageT {
+    float v[3][HY][WX];        // Vx, Vy, Vz, x and y halos
+    float sv[6][TY3][TX3];     // Sxx, Syy, Szz, Syz, Sxz, Sxy
+    float mv[5][TY3][TX3];     // L, L2M, M_yz, M_xz, M_xy (forward only)
+};
+static_assert(sizeof(VelStageT) % 128 == 0 && sizeof(StrStageT) % 128 == 0, "TMA destinations stay 128-byte aligned");
+static_assert(sizeof(float) * TY3 * WX % 128 == 0 && sizeof(float) * HY * WX % 128 == 0 &&
+              sizeof(float) * HY * TX3 % 128 == 0 && sizeof(float) * TY3 * TX3 % 128 == 0, "tile sizes");
+constexpr uint32_t VEL_STAGE_BYTES = sizeof(VelStageT);
+constexpr uint32_t STR_STAGE_BYTES_FW = sizeof(StrStageT);
+constexpr uint32_t STR_STAGE_BYTES_ADJ = sizeof(StrStageT) - sizeof(float) * 5 * TY3 * TX3;
+
+template <typename Stage>
+struct TmaSmem {
+    Stage st[NSTG3];
+    uint64_t bar[NSTG3];
+    CoefSet3<float> cs;
+};
+template <typename Stage>
+constexpr size_t tma_smem_bytes() { return sizeof(TmaSmem<Stage>) + 128; }   // + alignment slack
+
+// (a - b) pairs of two arrays with the same tap spacing: sum_k c_k (p[(8+k)s] - p[(7-k)s])
+__device__ __forceinline__ float2 taps_pair2(const float *p, const float *q, int sp, int sq,
+                                             const float (&c2)[NCOEF][2])
+{
+    using A2 = Ar2<float, MODE_FAST>;
+    const float2 *cc = reinterpret_cast<const float2 *>(c2);
+    float2 acc = A2::mul(A2::sub(make_float2(p[8 * sp], q[8 * sq]), make_float2(p[7 * sp], q[7 * sq])), cc[0]);
+#pragma unroll
+    for (int k = 1; k < NCOEF; k++)
+        acc = A2::acc(acc, A2::sub(make_float2(p[(8 + k) * sp], q[(8 + k) * sq]),
+                                   make_float2(p[(7 - k) * sp], q[(7 - k) * sq])), cc[k]);
+    return acc;
+}
+
+// Allocation row of plane iz, padded row iy_alloc (guards included).
+__device__ __forceinline__ int alloc_row(const Shot3D<float> &sh, int iz, int iy_alloc)
+{
+    return (GUARD + iz) * sh.rows + iy_alloc;
+}
+
+__global__ void __launch_bounds__(TX3 *TY3, 2) e3d_velocity_tma(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ unsigned char smraw[];
+    TmaSmem<VelStageT> &S =
+        *reinterpret_cast<TmaSmem<VelStageT> *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    __shared__ Shot3D<T> shs;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0)
+        for (int k = 0; k < NSTG3; k++) mbar_init(&S.bar[k], 1);
+    __syncthreads();
+    const Shot3D<T> &sh = shs;
+    const CUtensorMap *M = reinterpret_cast<const CUtensorMap *>(a.maps) + (size_t)tl.shot * NMAP_E3;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = tl.x0, y0 = tl.y0;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const int plane = (int)sh.plane;
+    const int col = iy * pitch + ix;
+    T *Vx = sh.f[E3_VX], *Vy = sh.f[E3_VY], *Vz = sh.f[E3_VZ];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kxf = kfw(ix, nxp, order), Kxb = kbw(ix, nxp, order);
+    const int Kyf = kfw(iy, nyp, order), Kyb = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    // stage k <- plane iz: every box starts on a 16-byte boundary (x0 and x0 + 8 are
+    // multiples of 4 floats)
+    auto issue = [&](int iz, int k) {
+        VelStageT &g = S.st[k];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&S.bar[k], VEL_STAGE_BYTES);
+        const int rh = alloc_row(sh, iz, GUARD + y0), ry = alloc_row(sh, iz, y0);
+        tma_load_2d(g.xx, M + VM_SXX, &S.bar[k], x0, rh);
+        tma_load_2d(g.xz, M + VM_SXZ, &S.bar[k], x0, rh);
+        tma_load_2d(g.xy, M + VM_SXY, &S.bar[k], x0, ry);
+        tma_load_2d(g.yy, M + VM_SYY, &S.bar[k], x0 + GUARD, ry);
+        tma_load_2d(g.yz, M + VM_SYZ, &S.bar[k], x0 + GUARD, ry);
+#pragma unroll
+        for (int q = 0; q < 6; q++) tma_load_2d(g.pv[q], M + VM_VX + q, &S.bar[k], x0 + GUARD, rh);
+    };
+    if (tid == 0)
+        for (int j = 0; j < NSTG3 - 1 && z0 + j < ze; j++) issue(z0 + j, j);
+    // z windows: (XZ, YZ) backward (planes z-8..z+7), ZZ forward (z-7..z+8)
+    const T *Sxz = sh.f[E3_SXZ], *Syz = sh.f[E3_SYZ], *Szz = sh.f[E3_SZZ];
+    float2 qp[16];
+    T qzz[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        const int oj = (z0 - 8 + j) * plane + col;
+        qp[j] = make_float2(Sxz[oj], Syz[oj]);
+        qzz[j] = Szz[(z0 - 7 + j) * plane + col];
+    }
+    int o = z0 * plane + col;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int j = iz - z0, k = j % NSTG3;
+        if (tid == 0 && iz + NSTG3 - 1 < ze) issue(iz + NSTG3 - 1, (j + NSTG3 - 1) % NSTG3);
+        // window refills of this iteration, in flight while the stage arrives
+        const float2 nq = make_float2(Sxz[o + 8 * plane], Syz[o + 8 * plane]);
+        const T nzz = Szz[o + 9 * plane];
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], (uint32_t)(j / NSTG3) & 1u, a.err))) return;
+        const VelStageT &g = S.st[k];
+        const int Kzf = kfw(iz, nzp, order), Kzb = kbw(iz, nzp, order);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        const int px = (iz * nyp + iy) * 2 * L + xc;
+        const int py = (iz * 2 * L + yc) * nxp + ix;
+        const int pz = (zc * nyp + iy) * nxp + ix;
+        const T *cxx = &g.xx[ty][tx + 8], *cxy = &g.xy[ty + 8][tx + 8], *cxz = &g.xz[ty][tx + 8];
+        const T *cyy = &g.yy[ty + 8][tx], *cyz = &g.yz[ty + 8][tx];
+        T dxx = taps3<T, MODE>(cxx - 7, 1, a.cf[0], a.dx, a.rdx);
+        float2 dxq = taps_pair2(cxy - 8, cxz - 8, 1, 1, a.cf2[0]);                  // (Dx- XY, Dx- XZ)
+        float2 dyq = taps_pair2(cxy - 8 * WX, cyz - 8 * TX3, WX, TX3, a.cf2[1]);  // (Dy- XY, Dy- YZ)
+        T dyy = taps3<T, MODE>(cyy - 7 * TX3, TX3, a.cf[1], a.dy, a.rdy);
+        float2 dzq = taps_pair_reg(qp, a.cf2[2]);
+        T dzz = taps3_reg<T, MODE>(qzz, a.cf[2], a.dz, a.rdz);
+        if (Kxf != order) dxx = stencil_k<T, MODE>(cxx, 1, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+        if (Kxb != order) {
+            dxq.x = stencil_k<T, MODE>(cxy, 1, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+            dxq.y = stencil_k<T, MODE>(cxz, 1, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+        }
+        if (Kyb != order) {
+            dyq.x = stencil_k<T, MODE>(cxy, WX, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+            dyq.y = stencil_k<T, MODE>(cyz, TX3, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+        }
+        if (Kyf != order) dyy = stencil_k<T, MODE>(cyy, TX3, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+        if (Kzb != order) {
+            dzq.x = stencil_z_op<T, MODE, false>(sh, o, plane, Kzb, S.cs.cz + Kzb * CROW3, false, OP_XZ, a.dz, a.rdz);
+            dzq.y = stencil_z_op<T, MODE, false>(sh, o, plane, Kzb, S.cs.cz + Kzb * CROW3, false, OP_YZ, a.dz, a.rdz);
+        }
+        if (Kzf != order)
+            dzz = stencil_z_op<T, MODE, false>(sh, o, plane, Kzf, S.cs.cz + Kzf * CROW3, true, OP_ZZ, a.dz, a.rdz);
+        T vx = g.pv[0][ty][tx], vy = g.pv[1][ty][tx], vz = g.pv[2][ty][tx];
+        // ---- Vx: Dx+ XX, Dy- XY, Dz- XZ
+        {
+            const T am = A::mul(a.dt, g.pv[3][ty][tx]);
+            vx = A::mad(vx, am, dxx);
+            if (xi >= 0) vx = pml_correct<T, MODE>(vx, am, dxx, sh.psix[0] + px, a.pml, L, xb + 3, xi);
+            vx = A::mad(vx, am, dyq.x);
+            if (yi >= 0) vx = pml_correct<T, MODE>(vx, am, dyq.x, sh.psiy[0] + py, a.pml, L, yb, yi);
+            vx = A::mad(vx, am, dzq.x);
+            if (zi >= 0) vx = pml_correct<T, MODE>(vx, am, dzq.x, sh.psiz[0] + pz, a.pml, L, zb, zi);
+            Vx[o] = vx;
+        }
+        // ---- Vy: Dx- XY, Dy+ YY, Dz- YZ
+        {
+            const T am = A::mul(a.dt, g.pv[4][ty][tx]);
+            vy = A::mad(vy, am, dxq.x);
+            if (xi >= 0) vy = pml_correct<T, MODE>(vy, am, dxq.x, sh.psix[1] + px, a.pml, L, xb, xi);
+            vy = A::mad(vy, am, dyy);
+            if (yi >= 0) vy = pml_correct<T, MODE>(vy, am, dyy, sh.psiy[1] + py, a.pml, L, yb + 3, yi);
+            vy = A::mad(vy, am, dzq.y);
+            if (zi >= 0) vy = pml_correct<T, MODE>(vy, am, dzq.y, sh.psiz[1] + pz, a.pml, L, zb, zi);
+            Vy[o] = vy;
+        }
+        // ---- Vz: Dx- XZ, Dy- YZ, Dz+ ZZ
+        {
+            const T am = A::mul(a.dt, g.pv[5][ty][tx]);
+            vz = A::mad(vz, am, dxq.y);
+            if (xi >= 0) vz = pml_correct<T, MODE>(vz, am, dxq.y, sh.psix[2] + px, a.pml, L, xb, xi);
+            vz = A::mad(vz, am, dyq.y);
+            if (yi >= 0) vz = pml_correct<T, MODE>(vz, am, dyq.y, sh.psiy[2] + py, a.pml, L, yb, yi);
+            vz = A::mad(vz, am, dzz);
+            if (zi >= 0) vz = pml_correct<T, MODE>(vz, am, dzz, sh.psiz[2] + pz, a.pml, L, zb + 3, zi);
+            Vz[o] = vz;
+        }
+#pragma unroll
+        for (int q = 0; q < 15; q++) { qp[q] = qp[q + 1]; qzz[q] = qzz[q + 1]; }
+        qp[15] = nq;
+        qzz[15] = nzz;
+        __syncthreads();   // stage k is refilled next iteration
+    }
+}
+
+template <bool ADJ>
+__global__ void __launch_bounds__(TX3 *TY3, 2) e3d_stress_tma(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ unsigned char smraw[];
+    TmaSmem<StrStageT> &S =
+        *reinterpret_cast<TmaSmem<StrStageT> *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    __shared__ Shot3D<T> shs;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    stage_shot(shs, a.shots + tl.shot);
+    load_coefs3e(S.cs, coefs);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0)
+        for (int k = 0; k < NSTG3; k++) mbar_init(&S.bar[k], 1);
+    __syncthreads();
+    const Shot3D<T> &sh = shs;
+    const CUtensorMap *M = reinterpret_cast<const CUtensorMap *>(a.maps) + (size_t)tl.shot * NMAP_E3;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = tl.x0, y0 = tl.y0;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const int plane = (int)sh.plane;
+    const int col = iy * pitch + ix;
+    const T *Vx = sh.f[E3_VX], *Vy = sh.f[E3_VY], *Vz = sh.f[E3_VZ];
+    T *Sxx = sh.f[E3_SXX], *Syy = sh.f[E3_SYY], *Szz = sh.f[E3_SZZ];
+    T *Syz = sh.f[E3_SYZ], *Sxz = sh.f[E3_SXZ], *Sxy = sh.f[E3_SXY];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kxf = kfw(ix, nxp, order), Kxb = kbw(ix, nxp, order);
+    const int Kyf = kfw(iy, nyp, order), Kyb = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    auto issue = [&](int iz, int k) {
+        StrStageT &g = S.st[k];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&S.bar[k], ADJ ? STR_STAGE_BYTES_ADJ : STR_STAGE_BYTES_FW);
+        const int rh = alloc_row(sh, iz, GUARD + y0), ry = alloc_row(sh, iz, y0);
+#pragma unroll
+        for (int q = 0; q < 3; q++) tma_load_2d(g.v[q], M + SM_VX + q, &S.bar[k], x0, ry);
+#pragma unroll
+        for (int q = 0; q < 6; q++) tma_load_2d(g.sv[q], M + SM_SXX + q, &S.bar[k], x0 + GUARD, rh);
+        if (!ADJ) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) tma_load_2d(g.mv[q], M + SM_L + q, &S.bar[k], x0 + GUARD, rh);
+        }
+    };
+    if (tid == 0)
+        for (int j = 0; j < NSTG3 - 1 && z0 + j < ze; j++) issue(z0 + j, j);
+    // z windows: Vz backward (planes z-8..z+7), (Vx, Vy) forward (z-7..z+8)
+    T qz[16];
+    float2 qv[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        qz[j] = Vz[(z0 - 8 + j) * plane + col];
+        const int oj = (z0 - 7 + j) * plane + col;
+        qv[j] = make_float2(Vx[oj], Vy[oj]);
+    }
+    int o = z0 * plane + col;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int j = iz - z0, k = j % NSTG3;
+        if (tid == 0 && iz + NSTG3 - 1 < ze) issue(iz + NSTG3 - 1, (j + NSTG3 - 1) % NSTG3);
+        const T nz = Vz[o + 8 * plane];
+        const float2 nv = make_float2(Vx[o + 9 * plane], Vy[o + 9 * plane]);
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], (uint32_t)(j / NSTG3) & 1u, a.err))) return;
+        const StrStageT &g = S.st[k];
+        const int Kzf = kfw(iz, nzp, order), Kzb = kbw(iz, nzp, order);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        const int px = (iz * nyp + iy) * 2 * L + xc;
+        const int py = (iz * 2 * L + yc) * nxp + ix;
+        const int pz = (zc * nyp + iy) * nxp + ix;
+        const T *cvx = &g.v[0][ty + 8][tx + 8], *cvy = &g.v[1][ty + 8][tx + 8], *cvz = &g.v[2][ty + 8][tx + 8];
+        T dxx = taps3<T, MODE>(cvx - 8, 1, a.cf[0], a.dx, a.rdx);
+        float2 dxp = taps_pair2(cvz - 7, cvy - 7, 1, 1, a.cf2[0]);                  // (Dx+ Vz, Dx+ Vy)
+        T dyy = taps3<T, MODE>(cvy - 8 * WX, WX, a.cf[1], a.dy, a.rdy);
+        float2 dyp = taps_pair2(cvz - 7 * WX, cvx - 7 * WX, WX, WX, a.cf2[1]);     // (Dy+ Vz, Dy+ Vx)
+        T dzz = taps3_reg<T, MODE>(qz, a.cf[2], a.dz, a.rdz);
+        float2 dzp = taps_pair_reg(qv, a.cf2[2]);                                   // (Dz+ Vx, Dz+ Vy)
+        if (Kxb != order) dxx = stencil_k<T, MODE>(cvx, 1, Kxb, S.cs.cx + Kxb * CROW3, false, a.dx, a.rdx);
+        if (Kxf != order) {
+            dxp.x = stencil_k<T, MODE>(cvz, 1, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+            dxp.y = stencil_k<T, MODE>(cvy, 1, Kxf, S.cs.cx + Kxf * CROW3, true, a.dx, a.rdx);
+        }
+        if (Kyb != order) dyy = stencil_k<T, MODE>(cvy, WX, Kyb, S.cs.cy + Kyb * CROW3, false, a.dy, a.rdy);
+        if (Kyf != order) {
+            dyp.x = stencil_k<T, MODE>(cvz, WX, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+            dyp.y = stencil_k<T, MODE>(cvx, WX, Kyf, S.cs.cy + Kyf * CROW3, true, a.dy, a.rdy);
+        }
+        if (Kzb != order) dzz = stencil_k<T, MODE>(Vz + o, plane, Kzb, S.cs.cz + Kzb * CROW3, false, a.dz, a.rdz);
+        if (Kzf != order) {
+            dzp.x = stencil_k<T, MODE>(Vx + o, plane, Kzf, S.cs.cz + Kzf * CROW3, true, a.dz, a.rdz);
+            dzp.y = stencil_k<T, MODE>(Vy + o, plane, Kzf, S.cs.cz + Kzf * CROW3, true, a.dz, a.rdz);
+        }
+        T sxx = g.sv[0][ty][tx], syy = g.sv[1][ty][tx], szz = g.sv[2][ty][tx];
+        T syz = g.sv[3][ty][tx], sxz = g.sv[4][ty][tx], sxy = g.sv[5][ty][tx];
+        // ---- normal stresses
+        {
+            const bool fsrow = sh.fs && iz == L;
+            if (!ADJ) {
+                const T l = g.mv[0][ty][tx], l2m = g.mv[1][ty][tx];
+                const T a2 = A::mul(a.dt, l2m), a1 = A::mul(a.dt, l);
+                auto upd3 = [&](T d, T cxx_, T cyy_, T czz_) {
+                    sxx = A::mad(sxx, cxx_, d); syy = A::mad(syy, cyy_, d); szz = A::mad(szz, czz_, d);
+                };
+                auto pml3 = [&](T d, T *psi, int base, int idx, T cxx_, T cyy_, T czz_) {
+                    const T tA = __ldg(a.pml + (base + PT_A) * L + idx), tB = __ldg(a.pml + (base + PT_B) * L + idx),
+                            tC = __ldg(a.pml + (base + PT_C) * L + idx);
+                    const T p = A::mad(A::mul(tB, *psi), tA, d);
+                    *psi = p;
+                    const T cq = A::mad(p, tC, d);
+                    sxx = A::msub(sxx, cxx_, cq); syy = A::msub(syy, cyy_, cq); szz = A::msub(szz, czz_, cq);
+                };
+                upd3(dxx, a2, a1, a1);
+                if (xi >= 0) pml3(dxx, sh.psix[3] + px, xb, xi, a2, a1, a1);
+                upd3(dyy, a1, a2, a1);
+                if (yi >= 0) pml3(dyy, sh.psiy[3] + py, yb, yi, a1, a2, a1);
+                upd3(dzz, a1, a1, a2);
+                if (fsrow) szz = T(0);
+                if (zi >= 0) pml3(dzz, sh.psiz[3] + pz, zb, zi, a1, a1, a2);
+            } else {
+                sxx = A::mad(sxx, a.dt, dxx);
+                if (xi >= 0) sxx = pml_correct<T, MODE>(sxx, a.dt, dxx, sh.psix[3] + px, a.pml, L, xb, xi);
+                syy = A::mad(syy, a.dt, dyy);
+                if (yi >= 0) syy = pml_correct<T, MODE>(syy, a.dt, dyy, sh.psiy[3] + py, a.pml, L, yb, yi);
+                szz = A::mad(szz, a.dt, dzz);
+                if (fsrow) szz = T(0);
+                if (zi >= 0) szz = pml_correct<T, MODE>(szz, a.dt, dzz, sh.psiz[3] + pz, a.pml, L, zb, zi);
+            }
+            Sxx[o] = sxx; Syy[o] = syy; Szz[o] = szz;
+        }
+        // ---- Sxz: Dx+ Vz, Dz+ Vx
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, g.mv[3][ty][tx]);
+            sxz = A::mad(sxz, am, dxp.x);
+            if (xi >= 0) sxz = pml_correct<T, MODE>(sxz, am, dxp.x, sh.psix[4] + px, a.pml, L, xb + 3, xi);
+            sxz = A::mad(sxz, am, dzp.x);
+            if (zi >= 0) sxz = pml_correct<T, MODE>(sxz, am, dzp.x, sh.psiz[4] + pz, a.pml, L, zb + 3, zi);
+            Sxz[o] = sxz;
+        }
+        // ---- Syz: Dz+ Vy, Dy+ Vz
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, g.mv[2][ty][tx]);
+            syz = A::mad(syz, am, dzp.y);
+            if (zi >= 0) syz = pml_correct<T, MODE>(syz, am, dzp.y, sh.psiz[5] + pz, a.pml, L, zb + 3, zi);
+            syz = A::mad(syz, am, dyp.x);
+            if (yi >= 0) syz = pml_correct<T, MODE>(syz, am, dyp.x, sh.psiy[4] + py, a.pml, L, yb + 3, yi);
+            Syz[o] = syz;
+        }
+        // ---- Sxy: Dy+ Vx, Dx+ Vy
+        {
+            const T am = ADJ ? a.dt : A::mul(a.dt, g.mv[4][ty][tx]);
+            sxy = A::mad(sxy, am, dyp.y);
+            if (yi >= 0) sxy = pml_correct<T, MODE>(sxy, am, dyp.y, sh.psiy[5] + py, a.pml, L, yb + 3, yi);
+            sxy = A::mad(sxy, am, dxp.y);
+            if (xi >= 0) sxy = pml_correct<T, MODE>(sxy, am, dxp.y, sh.psix[5] + px, a.pml, L, xb + 3, xi);
+            Sxy[o] = sxy;
+        }
+#pragma unroll
+        for (int q = 0; q < 15; q++) { qz[q] = qz[q + 1]; qv[q] = qv[q + 1]; }
+        qz[15] = nz;
+        qv[15] = nv;
+        __syncthreads();   // stage k is refilled next iteration
+    }
+}
+
 // ---------------------------------------------------------------- sources and receivers
 // One CTA per shot: injection of every source set (lib/waves.cpp:4104-4244), then,
 // after a barrier, recording of every receiver set (lib/waves.cpp:4247-4400) of
@@ -952,6 +1345,24 @@ cudaError_t step_e3_fast(int half, const void *args, const void *coefs, int grid
 {
     const Step3DArgs<float> &a = *reinterpret_cast<const Step3DArgs<float> *>(args);
     const dim3 block(TX3, TY3);
+    if (a.maps && !(half == 0 && ADJ)) {
+        // TMA-staged planes (the adjoint velocity step differentiates work arrays formed
+        // from five fields and keeps the register-staged kernel)
+        if (half == 0) {
+            auto k = e3d_velocity_tma;
+            static const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)tma_smem_bytes<VelStageT>());
+            if (e != cudaSuccess) return e;
+            k<<<grid, block, tma_smem_bytes<VelStageT>(), st>>>(a, (const CoefSet3<float> *)coefs);
+        } else {
+            auto k = e3d_stress_tma<ADJ>;
+            static const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                              (int)tma_smem_bytes<StrStageT>());
+            if (e != cudaSuccess) return e;
+            k<<<grid, block, tma_smem_bytes<StrStageT>(), st>>>(a, (const CoefSet3<float> *)coefs);
+        }
+        return cudaGetLastError();
+    }
     if (half == 0) {
         auto k = e3d_velocity_fast<ADJ>;
         static const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,

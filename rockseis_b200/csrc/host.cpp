@@ -828,7 +828,7 @@ rsgpu_status rsgpu_plan_sync(rsgpu_plan *p)
     if (!p) { set_error("null plan"); return RSGPU_ERR_ARG; }
     cudaError_t e = cudaStreamSynchronize(p->p3 ? p->p3->stream : p->p->stream);
     if (e != cudaSuccess) { set_error("stream sync: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-    return p->p3 ? RSGPU_OK : p->p->check_device_error();
+    return p->p3 ? p->p3->check_device_error() : p->p->check_device_error();
 }
 void *rsgpu_plan_stream(rsgpu_plan *p) { return p ? (void *)(p->p3 ? p->p3->stream : p->p->stream) : nullptr; }
 rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *p)

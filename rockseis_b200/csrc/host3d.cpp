@@ -13,6 +13,7 @@
 #include <map>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "rsgpu.h"
@@ -345,11 +346,43 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     const size_t ir_bytes = prec == PREC_F64 ? sizeof(InjRec3<double>) : sizeof(InjRec3<float>);
     const size_t m_shots = 0, m_ir = rup3(ns * shot_bytes, 256), m_tiles = rup3(m_ir + (size_t)nps * ir_bytes, 256);
     const size_t m_coef = rup3(m_tiles + tiles.size() * sizeof(Tile3D), 256);
-    const size_t m_gate = rup3(m_coef + coefs.size(), 256), m_end = m_gate + 256;
+    // elastic fast mode: the tensor maps of the TMA-staged kernels
+    const bool tma = phys == PHYS_E3D && prec == PREC_F32_FAST;
+    const size_t m_maps = rup3(m_coef + coefs.size(), 256);
+    const size_t m_gate = rup3(m_maps + (tma ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
+    const size_t m_end = m_gate + 256;
     CU(cudaMalloc(&d_meta, m_end));
     d_gate = reinterpret_cast<int *>((char *)d_meta + m_gate);
+    d_err = d_gate + 1;
     std::vector<unsigned char> meta(m_end, 0);
     reinterpret_cast<int *>(meta.data() + m_gate)[0] = 1;   // recording on
+    if (tma) {
+        struct Spec { int slot; bool param; int boxw, boxh; };
+        // VM_* then SM_* (rsgpu_3d.h)
+        const Spec spec[NMAP_E3] = {
+            {E3_SXX, false, WX3, TY3}, {E3_SXZ, false, WX3, TY3}, {E3_SXY, false, WX3, HY3},
+            {E3_SYY, false, TX3, HY3}, {E3_SYZ, false, TX3, HY3},
+            {E3_VX, false, TX3, TY3}, {E3_VY, false, TX3, TY3}, {E3_VZ, false, TX3, TY3},
+            {ME_RX, true, TX3, TY3}, {ME_RY, true, TX3, TY3}, {ME_RZ, true, TX3, TY3},
+            {E3_VX, false, WX3, HY3}, {E3_VY, false, WX3, HY3}, {E3_VZ, false, WX3, HY3},
+            {E3_SXX, false, TX3, TY3}, {E3_SYY, false, TX3, TY3}, {E3_SZZ, false, TX3, TY3},
+            {E3_SYZ, false, TX3, TY3}, {E3_SXZ, false, TX3, TY3}, {E3_SXY, false, TX3, TY3},
+            {ME_L, true, TX3, TY3}, {ME_L2M, true, TX3, TY3}, {ME_MYZ, true, TX3, TY3},
+            {ME_MXZ, true, TX3, TY3}, {ME_MXY, true, TX3, TY3}};
+        for (int i = 0; i < ns; i++) {
+            const Layout3D &L = shots[i];
+            for (int k = 0; k < NMAP_E3; k++) {
+                const Spec &q = spec[k];
+                // 2D map over the whole allocation: pitch x (rows * planes)
+                void *base = q.param ? (void *)(param_base(i, q.slot) - origin_bytes(L)) : (void *)(A + L.f[q.slot]);
+                void *m = meta.data() + m_maps + ((size_t)i * NMAP_E3 + k) * sizeof(CUtensorMap);
+                if (!encode_field_map_host(m, base, prec, L.pitch, L.rows * L.planes, q.boxw, q.boxh)) {
+                    set_error("cuTensorMapEncodeTiled failed for map %d of shot %d", k, i);
+                    return RSGPU_ERR_CUDA;
+                }
+            }
+        }
+    }
     for (int i = 0; i < ns; i++) {
         const ShotSets &e = eff[i];
         if (prec == PREC_F64) fill_shot<double>(meta.data() + m_shots + i * shot_bytes, i);
@@ -370,6 +403,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     d_injrec = (char *)d_meta + m_ir;
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
+    d_maps = tma ? (char *)d_meta + m_maps : nullptr;
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -442,6 +476,8 @@ static void make_args3(void *out, const Plan3D &p)
     a.dt = (T)p.cfg.dt; a.dx = (T)p.cfg.dx; a.dy = (T)p.cfg.dy; a.dz = (T)p.cfg.dz;
     a.rdx = (T)1 / a.dx; a.rdy = (T)1 / a.dy; a.rdz = (T)1 / a.dz;
     a.pml = (const T *)p.d_pml;
+    a.maps = p.d_maps;
+    a.err = p.d_err;
     const CoefSet3<T> &cs = *reinterpret_cast<const CoefSet3<T> *>(p.h_coefs.data());
     for (int k = 0; k < NCOEF; k++) {
         const T c[3] = {cs.cx[a.order * CROW3 + k], cs.cy[a.order * CROW3 + k], cs.cz[a.order * CROW3 + k]};
@@ -477,6 +513,19 @@ rsgpu_status Plan3D::step(int it)
 fail:
     set_error("3D kernel launch failed: %s", cudaGetErrorString(e));
     return RSGPU_ERR_CUDA;
+}
+
+// Device-side error word (a bounded wait that gave up); read after a sync.
+rsgpu_status Plan3D::check_device_error()
+{
+    int e = 0;
+    CU(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CU(cudaStreamSynchronize(stream));
+    if (e != 0) {
+        set_error("a device-side wait exceeded its time limit (code %d)", e);
+        return (rsgpu_status)e;
+    }
+    return RSGPU_OK;
 }
 
 rsgpu_status Plan3D::set_recording(bool on)
@@ -516,6 +565,7 @@ rsgpu_status Plan3D::read_traces(int shot, void *host_out, int set)
     std::vector<unsigned char> tmp(n * es);
     CU(cudaMemcpyAsync(tmp.data(), (char *)arena + L.tracesk[set], n * es, cudaMemcpyDeviceToHost, stream));
     CU(cudaStreamSynchronize(stream));
+    if (rsgpu_status st = check_device_error()) return st;
     if (es == 8) { double *o = (double *)host_out; const double *t = (const double *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
     else { float *o = (float *)host_out; const float *t = (const float *)tmp.data(); for (size_t k = 0; k < n; k++) o[k] += t[k]; }
     return RSGPU_OK;

@@ -14,6 +14,7 @@ namespace rsgpu {
 
 constexpr int TX3 = 32;   // x columns per CTA (one warp row)
 constexpr int TY3 = 8;    // y rows per CTA
+constexpr int WX3 = TX3 + 16, HY3 = TY3 + 16;   // a tile with its 8-cell x or y halos
 
 enum { A3_P = 0, A3_VX = 1, A3_VY = 2, A3_VZ = 3 };
 enum { M3_RX = 0, M3_RY = 1, M3_RZ = 2, M3_L = 3 };
@@ -55,6 +56,19 @@ struct Step3DArgs {
     T dt, dx, dy, dz;
     T rdx, rdy, rdz;
     const T *pml;
+    const void *maps;          // elastic fast mode: NMAP_E3 CUtensorMaps per shot (null: no TMA kernels)
+    int *err;                  // device error word (a bounded wait that gave up)
+};
+
+// Tensor maps of the elastic 3D TMA kernels, per shot: 2D maps over a whole
+// pitched array (pitch x rows*planes) with the box each staged tile needs.
+//   velocity: Sxx, Sxz {48 x 8} (x halo); Sxy {48 x 24} (x and y halos);
+//             Syy, Syz {32 x 24} (y halo); Vx, Vy, Vz, Rx, Ry, Rz {32 x 8}
+//   stress:   Vx, Vy, Vz {48 x 24}; the six stresses and L, L2M, M_yz, M_xz, M_xy {32 x 8}
+enum {
+    VM_SXX = 0, VM_SXZ, VM_SXY, VM_SYY, VM_SYZ, VM_VX, VM_VY, VM_VZ, VM_RX, VM_RY, VM_RZ,
+    SM_VX, SM_VY, SM_VZ, SM_SXX, SM_SYY, SM_SZZ, SM_SYZ, SM_SXZ, SM_SXY, SM_L, SM_L2M, SM_MYZ, SM_MXZ, SM_MXY,
+    NMAP_E3
 };
 
 constexpr int CROW3 = 9;

@@ -60,6 +60,9 @@ public:
     size_t arena_bytes = 0;
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
     std::vector<unsigned char> h_coefs;        // host copy of the CoefSet3 at d_coefs
+    void *d_maps = nullptr;                    // elastic fast mode: NMAP_E3 tensor maps per shot
+    int *d_err = nullptr;                      // device error word (bounded waits)
+    rsgpu_status check_device_error();
     cudaStream_t stream = nullptr;
     long long launches = 0;
 
