@@ -897,6 +897,7 @@ def run_e3d_forward(args, device=0, f=E3D):
     ns = args.shots or f["nshots"]
     m, srcs, recsets = e3d_problem(prec, f["nt"], True, ns)
     cfg = make_config(m, f["order"], f["nt"], f["dt"], prec)
+    cfg.zchunk = int(args.zchunk)
     keep: list = []
     shots = (abi.Shot * ns)(*[make_shot(m, s_, rs[0], keep) for s_, rs in zip(srcs, recsets)])
     h = C.c_void_p()
@@ -1096,7 +1097,7 @@ def main():
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
     ap.add_argument("--zchunk", type=int, default=0,
-                    help="acoustic3d: planes per z-march; 2D fused step: rows per work item (0 = library default)")
+                    help="3D: planes per z-march; 2D fused step: rows per work item (0 = library default)")
     ap.add_argument("--shots", type=int, default=None,
                     help="acoustic3d / elastic3d_fwi: only the first N shots (profiling runs)")
     ap.add_argument("--e3d-nt", type=int, default=E3D["nt_bench"],
