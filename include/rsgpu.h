@@ -301,6 +301,13 @@ rsgpu_status rsgpu_interp_traces(int precision, int mode, int ntr, int n1, doubl
  * usable for further calls.  Any other status means the failure path is broken. */
 rsgpu_status rsgpu_selftest_bounded_wait(void);
 
+/* Plans and gradient drivers take their device memory from a library-owned
+ * stream-ordered pool per device that keeps up to 8 GiB of freed blocks mapped
+ * between calls (so a call that creates and destroys a plan does not map and
+ * unmap its arena every time).  This returns every cached block of the current
+ * device to the driver; it synchronises the device.  No reference counterpart. */
+rsgpu_status rsgpu_release_cached_memory(void);
+
 /* 2D kernel tile shapes, the search space of the tile autotuner (no counterpart in
  * the reference, whose loops have no tiles).  rsgpu_tile_count returns how many
  * shapes the library holds for `precision`; rsgpu_tile_shape gives shape `idx`:

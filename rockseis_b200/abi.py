@@ -88,6 +88,7 @@ def _load() -> C.CDLL:
         "rsgpu_plan_enable_timing": (I, [V]),
         "rsgpu_plan_kernel_times": (I, [V, P(C.c_float), P(C.c_float)]),
         "rsgpu_plan_info": (I, [V, P(I), P(I), P(I)]),
+        "rsgpu_release_cached_memory": (I, []),
         "rsgpu_plan_destroy": (None, [V]),
         "rsgpu_modelling_a2d_noalloc": (I, [P(Config), P(Shot), V]),
         "rsgpu_selftest_bounded_wait": (I, []),

@@ -93,8 +93,8 @@ Adjoint::~Adjoint()
 {
     fw.reset();
     bw.reset();
-    if (dbuf) cudaFree(dbuf);
-    if (ckpt) cudaFree(ckpt);
+    dev_free(dbuf, stream);
+    dev_free(ckpt, stream);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -299,14 +299,14 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     o_segs = take(sizeof(CkptSeg) * segs.size());
     o_scales = take(sizeof(float) * segs.size() * ncheck);
     o_maxbits = take(sizeof(unsigned) * segs.size());
-    if (cudaMalloc(&dbuf, off) != cudaSuccess) {
+    if (dev_alloc(&dbuf, off, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %zu bytes failed", off);
         return RSGPU_ERR_NOMEM;
     }
     nslots = ncheck;
     const size_t ck_bytes = slot_elems * ck_es * (size_t)nslots;
-    if (cudaMalloc(&ckpt, ck_bytes) != cudaSuccess) {
+    if (dev_alloc(&ckpt, ck_bytes, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("checkpoint allocation of %zu bytes (%d slots) failed", ck_bytes, nslots);
         return RSGPU_ERR_NOMEM;

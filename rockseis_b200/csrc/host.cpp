@@ -10,6 +10,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -122,6 +123,60 @@ static bool encode_field_map(CUtensorMap *m, void *base, int prec, int pitch, in
     return r == CUDA_SUCCESS;
 }
 
+// ---------------------------------------------------------------- device memory pool
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64] = {};
+
+static cudaMemPool_t library_pool(cudaError_t *err)
+{
+    int dev = 0;
+    if ((*err = cudaGetDevice(&dev)) != cudaSuccess) return nullptr;
+    if (dev < 0 || dev >= 64) { *err = cudaErrorInvalidDevice; return nullptr; }
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if ((*err = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return nullptr;
+        cuuint64_t keep = 8ull << 30;
+        if ((*err = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return nullptr;
+        }
+        g_pool[dev] = pool;
+    }
+    *err = cudaSuccess;
+    return g_pool[dev];
+}
+
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t st)
+{
+    cudaError_t e;
+    cudaMemPool_t pool = library_pool(&e);
+    if (!pool) return e;
+    if ((e = cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), pool, st)) != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    return cudaStreamSynchronize(st);
+}
+
+void dev_free(void *p, cudaStream_t st)
+{
+    if (p) cudaFreeAsync(p, st);
+}
+
+cudaError_t dev_trim()
+{
+    cudaError_t e;
+    cudaMemPool_t pool = library_pool(&e);
+    if (!pool) return e;
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e;
+    return cudaMemPoolTrimTo(pool, 0);
+}
+
 // Shared with other host translation units (no-allocation entry point).
 void coef_table_host(int prec, double dx, double dz, std::vector<unsigned char> &out)
 {
@@ -138,12 +193,12 @@ Plan::~Plan()
 {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (zm_graph) cudaGraphExecDestroy(zm_graph);
-    if (d_zm) cudaFree(d_zm);
+    dev_free(d_zm, stream);
     for (auto &row : tev)
         for (auto &e : row)
             if (e) cudaEventDestroy(e);
-    if (arena) cudaFree(arena);
-    if (d_meta) cudaFree(d_meta);
+    dev_free(arena, stream);
+    dev_free(d_meta, stream);
     if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
@@ -381,7 +436,7 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     rec_pt_offsets.assign((size_t)ns * MAXSETS, 0);
     for (size_t j = 0; j < ro.size(); j++) rec_pt_offsets[j] = ro[j].pt;
     arena_bytes = off;
-    if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
+    if (dev_alloc(&arena, arena_bytes, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %zu bytes failed", arena_bytes);
         return RSGPU_ERR_NOMEM;
@@ -467,7 +522,7 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     const size_t m_maps = rup(m_coef + coefs.size(), 256);
     const size_t m_it = rup(m_maps + (size_t)ns * NMAP2D * sizeof(CUtensorMap), 256);
     const size_t m_end = m_it + 256;
-    CU(cudaMalloc(&d_meta, m_end));
+    CU(dev_alloc(&d_meta, m_end, stream));
     d_it = (int *)((char *)d_meta + m_it);
     d_err = d_it + 1;
     d_gate = d_it + 2;
@@ -869,6 +924,19 @@ rsgpu_status rsgpu_modelling(const rsgpu_config *cfg, int nshots, const rsgpu_sh
         }
     rsgpu_plan_destroy(p);
     return st;
+}
+
+rsgpu_status rsgpu_release_cached_memory(void)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        cudaGetLastError();
+        set_error("no CUDA device");
+        return RSGPU_ERR_NODEVICE;
+    }
+    cudaError_t e = dev_trim();
+    if (e != cudaSuccess) { set_error("releasing the memory pool: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    return RSGPU_OK;
 }
 
 rsgpu_status rsgpu_selftest_bounded_wait(void)

@@ -36,8 +36,8 @@ static inline size_t rup3(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
 Plan3D::~Plan3D()
 {
-    if (arena) cudaFree(arena);
-    if (d_meta) cudaFree(d_meta);
+    dev_free(arena, stream);
+    dev_free(d_meta, stream);
     if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
@@ -260,7 +260,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     rec_pt_offsets.assign(nps, 0);
     for (int j = 0; j < nps; j++) rec_pt_offsets[j] = tabs[j].rp;
     arena_bytes = off;
-    if (cudaMalloc(&arena, arena_bytes) != cudaSuccess) {
+    if (dev_alloc(&arena, arena_bytes, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %zu bytes failed", arena_bytes);
         return RSGPU_ERR_NOMEM;
@@ -351,7 +351,7 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     const size_t m_maps = rup3(m_coef + coefs.size(), 256);
     const size_t m_gate = rup3(m_maps + (tma ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
     const size_t m_end = m_gate + 256;
-    CU(cudaMalloc(&d_meta, m_end));
+    CU(dev_alloc(&d_meta, m_end, stream));
     d_gate = reinterpret_cast<int *>((char *)d_meta + m_gate);
     d_err = d_gate + 1;
     std::vector<unsigned char> meta(m_end, 0);

@@ -164,7 +164,7 @@ rsgpu_status Plan::setup_fused(const std::vector<std::vector<int>> &inj_pts)
                 }
             }
     }
-    CU(cudaMalloc(&d_zm, bytes));
+    CU(dev_alloc(&d_zm, bytes, stream));
     CU(cudaMemcpy(d_zm, h.data(), bytes, cudaMemcpyHostToDevice));
     char *Z = (char *)d_zm;
     if (prec == PREC_F64)

@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <string>
 #include <vector>
+#include <cuda_runtime.h>
 #include "rsgpu_kernels.h"
 
 namespace rsgpu {
@@ -18,6 +19,16 @@ template <typename T>
 int stagger_e3d_host(int nx, int ny, int nz, int l, int fs, const T *vp, const T *vs, const T *rho, T *const *out);
 void coef_table_host(int prec, double dx, double dz, std::vector<unsigned char> &out);
 bool encode_field_map_host(void *map, void *base, int prec, int pitch, int rows, int boxw, int boxh);
+
+// Device memory of plans and drivers: a library-owned stream-ordered pool per
+// device that keeps up to 8 GiB of freed blocks mapped, so that creating and
+// destroying a plan per call (rsgpu_modelling, rsgpu_fwi_gradient) does not map and
+// unmap its arena every time.  dev_alloc returns memory usable at once by any
+// stream and by synchronous copies; dev_free releases it in `st`'s order.
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t st);
+void dev_free(void *p, cudaStream_t st);
+// Return the cached blocks of the current device's pool to the driver.
+cudaError_t dev_trim();
 void make_map_host(int dim, int prec, int ntr, const double *coords, const int *n, const double *o, const double *d,
                    const double *gshift, int *map, void *shift);
 
