@@ -584,7 +584,7 @@ def run_fwi(args, device=0, f=FWI):
     """Shots/s of the checkpointed FWI gradient: all shots batched vs one shot at a time."""
     from rockseis_b200 import abi
     from rockseis_b200.rockseis import AdjointBatch, fwi_gradient_batch, modelling_batch
-    ns = f["nshots"]
+    ns = min(args.shots or f["nshots"], f["nshots"])
     prec, ckpt, accum = abi.F32_FAST, abi.CKPT_F16, abi.ACCUM_F64
     # observed data: modelled in the true model on the GPU
     mt, srcs, obs = fwi_problem(prec, ns, start=False)
@@ -636,6 +636,17 @@ def run_fwi(args, device=0, f=FWI):
         d2h = ns * (2 * m.Vp.nbytes + srcs[0].data.nbytes)
         e2e = {"value": round(ns / t_e2e, 3), "unit": "shots/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "path": "rsgpu_fwi_gradient (C ABI) from host buffers"}
+    # whole-gradient roofline with the byte budget of the workload: forward steps 36 B per
+    # point (P, Vx, Vz read and written, Rx, Rz, L read), adjoint step with correlation
+    # 80 B (the same 36 + forward P 4 + vp, rho 8 + two FP64 gradients read and written
+    # 32), plus the checkpoint bytes written and read by the schedule
+    peak, peak_kind = measured_peak()
+    grad_bytes = ns * pts * (36.0 * stats["fw_steps"] + 80.0 * stats["bw_steps"]) + stats["ckpt_bytes"]
+    roof = {"bound": "hbm", "kernel": "whole gradient (forward, adjoint, correlation, checkpoints)",
+            "achieved": round(grad_bytes / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(grad_bytes / t_batch / 1e9 / peak, 4), "peak_source": peak_kind,
+            "algorithmic_bytes": "36 B per forward point-step, 80 B per adjoint+correlation point-step, "
+                                 "checkpoint bytes from the schedule", "traffic": None}
     return {"metric": "FWI gradient shots/s", "shots_per_s_batched": round(ns / t_batch, 3),
             "shots_per_s_plain": round(plain, 3), "batched_over_plain": round((ns / t_batch) / plain, 2),
             "s_per_batch": round(t_batch, 4), "plain_sample_shots": len(t_plain),
@@ -643,7 +654,7 @@ def run_fwi(args, device=0, f=FWI):
             "FP64 accumulation", "forward_steps": stats["fw_steps"], "adjoint_steps": stats["bw_steps"],
             "checkpoint_bytes": stats["ckpt_bytes"], "gpu_launches": stats["launches"],
             "gpts_per_s_propagation": round(ns * pts * (stats["fw_steps"] + stats["bw_steps"]) / t_batch / 1e9, 3),
-            "config": fwi_config(), "e2e": e2e, "clocks": clk.summary()}
+            "roofline": roof, "config": fwi_config(), "e2e": e2e, "clocks": clk.summary()}
 
 
 # ---------------------------------------------------------------- 3D acoustic workload
@@ -1030,6 +1041,16 @@ def run_e3d(args, device=0, f=E3D):
                "d2h_bytes_per_step": int(d2h), "path": "rsgpu_fwi_gradient (C ABI) from host buffers"}
     work_full = abi.lib.rsgpu_revolve_numforw(f["nt"], ncheck) + 1 + 2 * f["nt"]
     work = stats["fw_steps"] + stats["bw_steps"] + 1
+    # whole gradient against the workload's byte budget: 104 B per forward point-step
+    # (nine fields read and written, eight parameters read), 188 B per adjoint step with
+    # its correlation (104 + nine forward fields 36 + three FP64 gradients read and
+    # written 48), plus the checkpoint bytes of the schedule
+    grad_bytes = ns * pts * (104.0 * stats["fw_steps"] + 188.0 * stats["bw_steps"]) + stats["ckpt_bytes"]
+    roof_grad = {"bound": "hbm", "kernel": "whole gradient (forward, adjoint, correlation, checkpoints)",
+                 "achieved": round(grad_bytes / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
+                 "frac": round(grad_bytes / t_batch / 1e9 / peak, 4), "peak_source": peak_kind,
+                 "algorithmic_bytes": "104 B per forward point-step, 188 B per adjoint+correlation point-step, "
+                                      "checkpoint bytes from the schedule"}
     return {"shots_per_s_batched": float("%.4g" % (ns / t_batch)), "shots_per_s_plain": float("%.4g" % plain),
             "batched_over_plain": round((ns / t_batch) / plain, 2), "s_per_batch": round(t_batch, 3),
             "shots_per_s_at_full_nt_extrapolated": float("%.4g" % (ns / t_batch * work / work_full)),
@@ -1038,11 +1059,114 @@ def run_e3d(args, device=0, f=E3D):
             "checkpoint_bytes": stats["ckpt_bytes"], "gpu_launches": stats["launches"],
             "gpts_per_s_propagation": round(ns * pts * (stats["fw_steps"] + stats["bw_steps"]) / t_batch / 1e9, 3),
             "forward_step_ms": round(fw_ms, 3), "forward_gpts_per_s": round(ns * pts / fw_ms / 1e6, 3),
+            "roofline_gradient": roof_grad,
             "roofline": {"bound": "hbm", "kernel": "e3d_velocity + e3d_stress + inject_record_e3d (forward step)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                          "algorithmic_bytes_per_point_step": 140, "traffic": None},
             "config": e3d_config(nt, ncheck), "e2e": e2e, "clocks": clk.summary()}
+
+
+# ---------------------------------------------------------------- 3D acoustic RTM workload
+RTM3 = dict(nt_bench=250, ncheck=10)
+
+
+def rtm3d_config(nt, nshots=None, f=A3D):
+    c = a3d_config(nshots, f)
+    c.update(workload=f"acoustic3d_rtm_{c['shots']}shots_400x400x300_windows_nt{nt}", nt=nt, nt_full=f["nt"],
+             ncheck=RTM3["ncheck"], checkpoints="FP16, power-of-two scale per array", accumulation="FP64",
+             image="zero lag")
+    c.pop("time_steps_per_bench_step", None)
+    return c
+
+
+def _rtm3d_ref_sample(args):
+    """One process: the reference's RtmAcoustic3D::run_optimal on one mean-size window, nt steps."""
+    nxw, nyw, nt = args
+    sys.path.insert(0, ROOT)
+    from oracle import api
+    from rockseis_b200 import synth
+    f = A3D
+    vp = synth.dipping_vp_3d(nxw, nyw, f["nz"], f["dx"], seed=5, vclip=4550.0)
+    pb = api.Problem3D(nxw, nyw, f["nz"], f["dx"], f["dx"], f["dx"], f["lpml"], f["order"], 0, f["dt"], nt, vp,
+                       synth.gardner(vp))
+    wav = synth.ricker(nt, f["dt"], f["f0"])[None, :]
+    c = nxw * f["dx"] / 2
+    gc = np.stack([np.linspace(0.0, (nxw - 1) * f["dx"], f["nrec"]), np.full(f["nrec"], c), np.zeros(f["nrec"])], 1)
+    data = np.zeros((f["nrec"], nt), np.float32)
+    t0 = time.perf_counter()
+    api.ref_rtm_a3d(pb, np.array([[c, c, f["sz"]]]), wav, gc, data, 2)
+    return time.perf_counter() - t0
+
+
+def cpu_rtm3d_reference(models, nt_target, ncheck, nt_sample=3, procs=None):
+    """The reference's CPU RTM image on the batch's mean window, one per process, nt_sample
+    steps, extrapolated to nt_target by Revolve forward steps + adjoint steps + correlations."""
+    import multiprocessing as mp
+    from oracle import api
+    from rockseis_b200 import abi
+    if not api.ref_available():
+        return None
+    procs = procs or min(8, os.cpu_count() or 1)
+    nxw = int(round(np.mean([m.nx for m in models])))
+    nyw = int(round(np.mean([m.ny for m in models])))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        times = pool.map(_rtm3d_ref_sample, [(nxw, nyw, nt_sample)] * procs)
+
+    def work(nt, nc):
+        return abi.lib.rsgpu_revolve_numforw(nt, nc) + 1 + 2 * nt
+    t_img = max(times) * work(nt_target, ncheck) / work(nt_sample, 2)
+    return {"value": float("%.4g" % (procs / t_img)), "unit": "images/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} processes x one {nxw}x{nyw}x{A3D['nz']} window (the batch's mean), nt={nt_sample} "
+                      f"(ncheck 2), extrapolated to nt={nt_target} with ncheck {ncheck} by Revolve forward + "
+                      f"adjoint + correlation steps", "max_process_s": round(max(times), 3)}
+
+
+def run_rtm3d(args, device=0, f=A3D):
+    """Shot images/s of the batched 3D RTM (zero lag) over the windowed C4 shots, on a
+    shortened time axis: data modelled on the GPU in the same model, then one
+    rsgpu_adjoint batch (FMA arithmetic, FP16 checkpoints, FP64 image accumulation)."""
+    from rockseis_b200 import abi
+    from rockseis_b200.rockseis import AdjointBatch, Image3D, RtmAcoustic3D, modelling_batch
+    nt = int(args.rtm_nt)
+    ff = dict(f, nt=nt)
+    prec = abi.F32_FAST
+    models, srcs, recs = a3d_batch(prec, f=ff, nshots=args.shots)
+    ns = len(models)
+    modelling_batch(models, srcs, recs, ff["order"], prec)
+    jobs = []
+    for m, s_, r in zip(models, srcs, recs):
+        j = RtmAcoustic3D(m, Image3D("pimage", m, 1, 1, 1, prec), s_, r, ff["order"], 1, precision=prec)
+        j.setNcheck(RTM3["ncheck"])
+        j.setCheckpointPrecision(abi.CKPT_F16)
+        j.setAccumulation(abi.ACCUM_F64)
+        jobs.append(j)
+    batch = AdjointBatch(jobs, kind=abi.KIND_RTM)
+    batch.run()                                   # warm-up
+    with ClockSampler(device) as clk:
+        t_batch = _timed_runs(batch, max(1, args.fwi_steps))
+    stats = batch.stats()
+    batch.close()
+    L = f["lpml"]
+    pts = sum((m.nx + 2 * L) * (m.ny + 2 * L) * (m.nz + 2 * L) for m in models)
+    peak, peak_kind = measured_peak()
+    # 48 B per forward point-step (four fields read and written, four parameters read),
+    # 60 B per adjoint step with the image correlation (48 + forward P 4 + FP32 image
+    # read and written 8; FP64 accumulation moves 8 more), checkpoint bytes of the schedule
+    img_bytes = pts * (48.0 * stats["fw_steps"] + 60.0 * stats["bw_steps"]) + stats["ckpt_bytes"]
+    roof = {"bound": "hbm", "kernel": "whole image (forward, adjoint, correlation, checkpoints)",
+            "achieved": round(img_bytes / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(img_bytes / t_batch / 1e9 / peak, 4), "peak_source": peak_kind,
+            "algorithmic_bytes": "48 B per forward point-step, 60 B per adjoint+correlation point-step, "
+                                 "checkpoint bytes from the schedule", "traffic": None}
+    work_full = abi.lib.rsgpu_revolve_numforw(f["nt"], RTM3["ncheck"]) + 1 + 2 * f["nt"]
+    work = stats["fw_steps"] + stats["bw_steps"] + 1
+    return {"images_per_s": float("%.4g" % (ns / t_batch)), "s_per_batch": round(t_batch, 3), "shots": ns,
+            "images_per_s_at_full_nt_extrapolated": float("%.4g" % (ns / t_batch * work / work_full)),
+            "forward_steps": stats["fw_steps"], "adjoint_steps": stats["bw_steps"],
+            "checkpoint_bytes": stats["ckpt_bytes"], "gpu_launches": stats["launches"],
+            "gpts_per_s_propagation": round(pts * (stats["fw_steps"] + stats["bw_steps"]) / t_batch / 1e9, 3),
+            "roofline": roof, "clocks": clk.summary(), "models": models}
 
 
 # ---------------------------------------------------------------- distributed plumbing
@@ -1086,10 +1210,14 @@ def main():
     ap.add_argument("--tile", type=int, default=-2,
                     help="2D tile shape index; -2 = autotuned (cached in JSON), -1 = library default")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=None,
+                    help="elastic2d: time steps of the reference CPU sample (default 100 for the reference arm, "
+                         "400 for our line's cpu_baseline; 4000 = the whole modelling)")
     ap.add_argument("--nt", type=int, default=NT, help="time steps per modelling (profiling runs shorten it)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C ABI measurement")
     ap.add_argument("--workload", default="elastic2d",
-                    choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d", "elastic3d", "elastic3d_fwi"],
+                    choices=["elastic2d", "acoustic2d", "fwi", "acoustic3d", "acoustic3d_rtm", "elastic3d",
+                             "elastic3d_fwi"],
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
     ap.add_argument("--launch-mode", type=int, default=0,
@@ -1100,6 +1228,8 @@ def main():
                     help="3D: planes per z-march; 2D fused step: rows per work item (0 = library default)")
     ap.add_argument("--shots", type=int, default=None,
                     help="acoustic3d / elastic3d_fwi: only the first N shots (profiling runs)")
+    ap.add_argument("--rtm-nt", type=int, default=RTM3["nt_bench"],
+                    help="acoustic3d_rtm: time steps of the timed images (the full workload has 2500)")
     ap.add_argument("--e3d-nt", type=int, default=E3D["nt_bench"],
                     help="elastic3d_fwi: time steps of the timed gradients (the full workload has 2000)")
     args = ap.parse_args()
@@ -1133,6 +1263,22 @@ def main():
                                       "d2h_bytes_per_step": 0}}))
         return
 
+    if args.impl == "reference" and args.workload == "acoustic3d_rtm":
+        if int(os.environ.get("RANK", "0")) == 0:
+            from rockseis_b200 import abi
+            models, _, _ = a3d_batch(abi.F32_EXACT, f=dict(A3D, nt=args.rtm_nt), nshots=args.shots)
+            r = cpu_rtm3d_reference(models, args.rtm_nt, RTM3["ncheck"])
+            if r is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
+                return
+            print(json.dumps({"metric": "RTM images/s", "value": r["value"], "unit": "images/s",
+                              "impl": "reference", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": 1,
+                              "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f32", "data": "synthetic", "config": rtm3d_config(args.rtm_nt, args.shots),
+                              "cpu_baseline": r, "e2e": {"value": r["value"], "unit": "images/s",
+                                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
     if args.impl == "reference" and args.workload == "acoustic3d":
         if int(os.environ.get("RANK", "0")) == 0:
             from rockseis_b200 import abi
@@ -1155,7 +1301,7 @@ def main():
         if rank == 0:
             per = []
             for _ in range(args.steps):
-                r = cpu_reference()
+                r = cpu_reference(args.cpu_steps or CPU_SAMPLE_STEPS)
                 if r is None:
                     print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref not built"}))
                     return
@@ -1183,6 +1329,23 @@ def main():
                 "config": a3d_config(args.shots), "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
                 "clocks": r["clocks"], "acoustic3d": {k: v for k, v in r.items() if k not in ("roofline", "clocks")},
                 "cpu_baseline": cpu}
+        print(json.dumps(line))
+        return
+    if args.workload == "acoustic3d_rtm":
+        if world > 1:
+            raise SystemExit("the 3D RTM line is a one-GPU measurement")
+        import torch
+        torch.cuda.set_device(local)
+        r = run_rtm3d(args, device=local)
+        models = r.pop("models")
+        cpu = None if args.no_cpu_baseline else cpu_rtm3d_reference(models, args.rtm_nt, RTM3["ncheck"])
+        line = {"metric": "RTM images/s", "value": r["images_per_s"], "unit": "images/s", "n_gpus": 1,
+                "steps": args.fwi_steps, "warmup": 1, "ms_per_step": round(r["s_per_batch"] * 1e3, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded dipping layers, windowed shots; data modelled in the same model)",
+                "config": rtm3d_config(args.rtm_nt, args.shots), "gpu_launches": r["gpu_launches"],
+                "roofline": r["roofline"], "clocks": r["clocks"],
+                "rtm_image": {k: v for k, v in r.items() if k not in ("roofline", "clocks")}, "cpu_baseline": cpu}
         print(json.dumps(line))
         return
     if args.workload == "elastic3d":
@@ -1223,8 +1386,8 @@ def main():
                 "steps": args.fwi_steps, "warmup": 1, "ms_per_step": round(r["s_per_batch"] * 1e3, 3),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded smooth background + Gaussian anomalies; start model smoothed)",
-                "config": r["config"], "gpu_launches": r["gpu_launches"], "fwi_gradient": r, "e2e": r.get("e2e"),
-                "clocks": r["clocks"], "cpu_baseline": cpu}
+                "config": r["config"], "gpu_launches": r["gpu_launches"], "roofline": r["roofline"],
+                "fwi_gradient": r, "e2e": r.get("e2e"), "clocks": r["clocks"], "cpu_baseline": cpu}
         print(json.dumps(line))
         return
     if args.workload == "acoustic2d":
@@ -1243,7 +1406,7 @@ def main():
         return
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference(CPU_BASELINE_STEPS)   # before the first CUDA call of this process (spawned workers)
+        cpu = cpu_reference(args.cpu_steps or CPU_BASELINE_STEPS)   # before the first CUDA call (spawned workers)
     r = run_gpu(args, rank, world, local)
     fwi = None
     if rank == 0 and world == 1 and not args.no_fwi:
