@@ -105,6 +105,8 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
+    lib.ref_localsize2d_f.argtypes = [G, I, V, V, D, I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.ref_localsize3d_f.argtypes = [G, I, V, V, D, D, I, V]
     lib.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
     lib.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
@@ -392,6 +394,23 @@ def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
     assert r == 1
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out
+
+
+def ref_localsize2d(grid, scoords, gcoords, aperture, map_):
+    """Model::getLocalsize2d: (start, size) of the x window of traces (sx, sz) / (gx, gz)."""
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    st, sz = C.c_longlong(), C.c_longlong()
+    ref().ref_localsize2d_f(C.byref(grid), len(sc), _p(sc), _p(gc), float(aperture), int(map_), C.byref(st),
+                            C.byref(sz))
+    return st.value, sz.value
+
+
+def ref_localsize3d(grid, scoords, gcoords, apx, apy, map_):
+    """Model::getLocalsize3d: ((start_x, size_x), (start_y, size_y))."""
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    out = np.zeros(4, np.int64)
+    ref().ref_localsize3d_f(C.byref(grid), len(sc), _p(sc), _p(gc), float(apx), float(apy), int(map_), _p(out))
+    return (int(out[0]), int(out[1])), (int(out[2]), int(out[3]))
 
 
 def ref_fwi_e3d(pb, scoords, wav, sfield, gcoords, obs3, ncheck):

@@ -564,6 +564,45 @@ int ref_fwi_a3d_corr_f(const ref_grid *g, const float *vp, const float *rho, int
     return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
                           misfit, 1);
 }
+/* Model::getLocalsize2d / getLocalsize3d (lib/model.cpp:272-470): the aperture window of
+ * ntr traces whose source and receiver coordinates are both given (x,z or x,y,z per
+ * trace); map = 0 (SMAP) or 1 (GMAP). */
+void ref_localsize2d_f(const ref_grid *g, int ntr, const double *sc, const double *gc, double aperture, int map,
+                       long long *start, long long *size)
+{
+    ModelAcoustic2D<float> m(g->nx, g->nz, g->lpml, (float)g->dx, (float)g->dz, (float)g->ox, (float)g->oz,
+                             g->fs != 0);
+    auto d = std::make_shared<Data2D<float>>(ntr, 1, 1.0f, 0.0f);
+    auto geo = d->getGeom();
+    for (int i = 0; i < ntr; i++) {
+        geo->getScoords()[i].x = (float)sc[2 * i];
+        geo->getScoords()[i].y = (float)sc[2 * i + 1];
+        geo->getGcoords()[i].x = (float)gc[2 * i];
+        geo->getGcoords()[i].y = (float)gc[2 * i + 1];
+    }
+    off_t st = 0;
+    size_t sz = 0;
+    m.getLocalsize2d(d, (float)aperture, map != 0, &st, &sz);
+    *start = (long long)st;
+    *size = (long long)sz;
+}
+void ref_localsize3d_f(const ref_grid *g, int ntr, const double *sc, const double *gc, double apx, double apy,
+                       int map, long long *out)
+{
+    ModelAcoustic3D<float> m(g->nx, g->ny, g->nz, g->lpml, (float)g->dx, (float)g->dy, (float)g->dz, (float)g->ox,
+                             (float)g->oy, (float)g->oz, g->fs != 0);
+    auto d = std::make_shared<Data3D<float>>(ntr, 1, 1.0f, 0.0f);
+    auto geo = d->getGeom();
+    for (int i = 0; i < ntr; i++) {
+        Point3D<float> *s = geo->getScoords(), *r = geo->getGcoords();
+        s[i].x = (float)sc[3 * i]; s[i].y = (float)sc[3 * i + 1]; s[i].z = (float)sc[3 * i + 2];
+        r[i].x = (float)gc[3 * i]; r[i].y = (float)gc[3 * i + 1]; r[i].z = (float)gc[3 * i + 2];
+    }
+    off_t sx = 0, sy = 0;
+    size_t nx = 0, ny = 0;
+    m.getLocalsize3d(d, (float)apx, (float)apy, map != 0, &sx, &nx, &sy, &ny);
+    out[0] = (long long)sx; out[1] = (long long)nx; out[2] = (long long)sy; out[3] = (long long)ny;
+}
 int ref_fwi_e3d_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns, const double *sc,
                   const float *wav, int sfield, int nr, const double *gc, const float *obsx, const float *obsy,
                   const float *obsz, int ncheck, float *vpgrad, float *vsgrad, float *rhograd, float *wavgrad,

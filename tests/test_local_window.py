@@ -1,11 +1,64 @@
 """Aperture windows of the batched drivers: Model::getLocalsize2d/3d and the
 edge-clamped copy of Model*::getLocal (lib/model.cpp:272-470, 1443-1509,
-2369-2450), restated in rockseis_b200.rockseis.  The reference reads its models
-from .rss files inside getLocal, so these cases are checked against the formulas
-worked by hand rather than against the reference library."""
+2369-2450), restated in rockseis_b200.rockseis.  The window sizes are pinned to the
+reference's own getLocalsize2d/3d: against golden cases it computed
+(tests/golden/localsize.json, tests/golden/make_golden_localsize.py) and, where
+oracle/_ref is built, against the live library on further seeded cases.  The
+reference reads its models from .rss files inside getLocal, so the copy itself is
+checked against cases worked by hand."""
+import json
+import os
+
 import numpy as np
+import pytest
 
 from rockseis_b200.rockseis import SMAP, GMAP, Data2D, Data3D, ModelAcoustic2D, ModelAcoustic3D
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "localsize.json")
+
+
+def _ours(c):
+    s, g = np.array(c["s"]), np.array(c["g"])
+    if c["dim"] == 2:
+        m = ModelAcoustic2D(400, 100, 10, c["dx"], c["dx"], c["ox"], 0.0, 0)
+        d = Data2D(len(s), 1, 1e-3, 0.0)
+        d.scoords[:] = s[:, [0, 2]]
+        d.gcoords[:] = g[:, [0, 2]]
+        return list(m.getLocalsize2d(d, c["ap"], c["map"]))
+    m = ModelAcoustic3D(400, 300, 100, 10, c["dx"], c["dy"], c["dx"], c["ox"], c["oy"], 0.0, 0)
+    d = Data3D(len(s), 1, 1e-3, 0.0)
+    d.scoords[:] = s
+    d.gcoords[:] = g
+    (sx, nx), (sy, ny) = m.getLocalsize3d(d, c["ap"], c["apy"], c["map"])
+    return [sx, nx, sy, ny]
+
+
+def test_windows_equal_the_reference_golden_cases():
+    with open(GOLDEN) as f:
+        cases = json.load(f)
+    assert len(cases) >= 60
+    for c in cases:
+        assert _ours(c) == c["want"], c
+
+
+def test_windows_equal_the_live_reference():
+    from oracle import api
+    if not api.ref_available():
+        pytest.skip("reference library oracle/_ref not built")
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mk", os.path.join(os.path.dirname(GOLDEN), "make_golden_localsize.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    for c in mk.cases(seed=99, n=200):
+        s, g = np.array(c["s"]), np.array(c["g"])
+        if c["dim"] == 2:
+            grid = api.RefGrid(400, 1, 100, 10, 8, 0, c["dx"], 1.0, c["dx"], c["ox"], 0.0, 0.0, 1e-3, 10)
+            want = list(api.ref_localsize2d(grid, s[:, [0, 2]], g[:, [0, 2]], c["ap"], c["map"]))
+        else:
+            grid = api.RefGrid(400, 300, 100, 10, 8, 0, c["dx"], c["dy"], c["dx"], c["ox"], c["oy"], 0.0, 1e-3, 10)
+            (sx, nx), (sy, ny) = api.ref_localsize3d(grid, s, g, c["ap"], c["apy"], c["map"])
+            want = [sx, nx, sy, ny]
+        assert _ours(c) == want, c
 
 
 def model2d(nx=100, nz=20):
