@@ -207,8 +207,15 @@ typedef struct {
                             elastic 2D :2939-3001, 3309-3426 with the x/z and P clips) */
     int nhx, nhz;        /* RTM extended-image lags (Rtm::setNhx/setNhz; odd, 1 = zero lag) */
     int nhy;             /* 3D RTM y lags (Rtm::setNhy; odd, 0 or 1 = zero lag) */
-    int reserved[9];
+    int snapmethod;      /* RSGPU_SNAP_OPTIMAL: Revolve checkpointing (run_optimal);
+                            RSGPU_SNAP_FULL: the forward pressure saved every snapinc steps and
+                            correlated at those steps only (FwiAcoustic2D::run, lib/fwi.cpp:1030-1156;
+                            RtmAcoustic2D::run, lib/rtm.cpp:222-326); acoustic 2D */
+    int snapinc;         /* FULL: snapshot increment (Fwi/Rtm snapinc; < 1 means 1) */
+    int noreverse;       /* FULL FWI: forward run and misfit only (Fwi::setNoreverse) */
+    int reserved[6];
 } rsgpu_adjoint_opts;
+enum { RSGPU_SNAP_OPTIMAL = 0, RSGPU_SNAP_FULL = 1 };
 
 /* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332),
  * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545), FwiElastic2D::run_optimal

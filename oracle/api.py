@@ -105,6 +105,8 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
+    lib.ref_fwi_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I] + [V] * 5 + [V]
+    lib.ref_rtm_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
     lib.ref_localsize2d_f.argtypes = [G, I, V, V, D, I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     lib.ref_localsize3d_f.argtypes = [G, I, V, V, D, D, I, V]
     lib.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
@@ -231,6 +233,36 @@ def ref_fwi_a2d(pb, scoords, wav, gcoords, obs, ncheck, dtype=np.float32, misfit
                                            ncheck, misfit, _p(vpg), _p(rhog), _p(wg), _p(dm), _p(dr), C.byref(mis))
     assert r == 1
     return dict(vpgrad=vpg, rhograd=rhog, wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
+
+
+def ref_fwi_a2d_full(pb, scoords, wav, gcoords, obs, snapinc, noreverse=0, misfit=0, lib=None):
+    """FwiAcoustic2D::run, the full-snapshot gradient (snapshots every snapinc steps)."""
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    ns, nr = len(sc), len(gc)
+    out = dict(vpgrad=np.zeros((pb.nz, pb.nx), np.float32), rhograd=np.zeros((pb.nz, pb.nx), np.float32),
+               wavgrad=np.zeros((ns, pb.nt), np.float32), datamod=np.zeros((nr, pb.nt), np.float32),
+               datares=np.zeros((nr, pb.nt), np.float32))
+    mis = C.c_double()
+    vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=np.float32)
+    r = (lib or ref()).ref_fwi_a2d_full_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob),
+                                          snapinc, noreverse, misfit, _p(out["vpgrad"]), _p(out["rhograd"]),
+                                          _p(out["wavgrad"]), _p(out["datamod"]), _p(out["datares"]), C.byref(mis))
+    assert r == 1
+    out["misfit"] = mis.value
+    return out
+
+
+def ref_rtm_a2d_full(pb, scoords, wav, gcoords, data, snapinc, nhx=1, nhz=1):
+    """RtmAcoustic2D::run, the full-snapshot image."""
+    g = pb.ref_grid()
+    sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
+    img = np.zeros((nhz, nhx, pb.nz, pb.nx), np.float32)
+    vp, rho, w, d = _keep(pb.vp, pb.rho, wav, data, dtype=np.float32)
+    r = ref().ref_rtm_a2d_full_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d),
+                                 snapinc, nhx, nhz, _p(img))
+    assert r == 1
+    return img
 
 
 def ref_rtm_a2d(pb, scoords, wav, gcoords, data, ncheck, nhx=1, nhz=1):

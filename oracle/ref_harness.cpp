@@ -113,7 +113,8 @@ int mod_e3d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
 template <typename T>
 int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *sc, const T *wav,
             int nr, const double *gc, const T *obs, int ncheck, int misfit_type, T *vpgrad,
-            T *rhograd, T *wavgrad, T *datamod, T *datares, double *misfit, T *srcilum = nullptr)
+            T *rhograd, T *wavgrad, T *datamod, T *datares, double *misfit, T *srcilum = nullptr,
+            int full_snapinc = 0, int noreverse = 0)
 {
     auto model = make_a2d<T>(g, vp, rho);
     auto src = make_data2d<T>(ns, g, sc, PRESSURE, SMAP, model->getGeom(), wav);
@@ -124,12 +125,13 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     auto ivp = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
     auto irho = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
     irho->allocateImage();
-    FwiAcoustic2D<T> fwi(model, src, dobs, g->order, 1);
+    FwiAcoustic2D<T> fwi(model, src, dobs, g->order, full_snapinc > 0 ? full_snapinc : 1);
     fwi.setDatamodP(dmod);
     fwi.setDataresP(dres);
     fwi.setVpgrad(ivp);
     fwi.setRhograd(irho);
     fwi.setWavgrad(wg);
+    fwi.setNoreverse(noreverse != 0);
     std::shared_ptr<Image2D<T>> ilum;
     if (srcilum) {
         ilum = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
@@ -139,7 +141,7 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     fwi.setNcheck(ncheck);
     fwi.setIncore(true);
     fwi.setSnapfile(tmpname("fwia2d"));
-    int r = fwi.run_optimal();
+    int r = full_snapinc > 0 ? fwi.run() : fwi.run_optimal();
     size_t n = (size_t)g->nx * g->nz;
     if (srcilum) std::memcpy(srcilum, ilum->getImagedata(), sizeof(T) * n);
     std::memcpy(vpgrad, ivp->getImagedata(), sizeof(T) * n);
@@ -633,6 +635,13 @@ int ref_fwi_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, 
                   float *datares, double *misfit)
 { return fwi_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, misfit_type, vpgrad, rhograd,
                         wavgrad, datamod, datares, misfit); }
+/* FwiAcoustic2D::run (lib/fwi.cpp:1030-1156): full snapshots every snapinc steps. */
+int ref_fwi_a2d_full_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                       const float *wav, int nr, const double *gc, const float *obs, int snapinc, int noreverse,
+                       int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod,
+                       float *datares, double *misfit)
+{ return fwi_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, 0, misfit_type, vpgrad, rhograd, wavgrad, datamod,
+                        datares, misfit, nullptr, snapinc, noreverse); }
 int ref_fwi_a2d_ilum_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                        const float *wav, int nr, const double *gc, const float *obs, int ncheck,
                        int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod,

@@ -60,4 +60,21 @@ int ref_rtm_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, 
                   int nhz, float *image)
 { return rtm_a2d<float>(g, vp, rho, ns, sc, wav, nr, gc, data, ncheck, nhx, nhz, image); }
 
+/* RtmAcoustic2D::run (lib/rtm.cpp:222-326): full snapshots every snapinc steps. */
+int ref_rtm_a2d_full_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                       const float *wav, int nr, const double *gc, const float *data, int snapinc, int nhx,
+                       int nhz, float *image)
+{
+    auto model = make_a2d<float>(g, vp, rho);
+    auto src = make_data2d<float>(ns, g, sc, PRESSURE, SMAP, model->getGeom(), wav);
+    auto drec = make_data2d<float>(nr, g, gc, PRESSURE, GMAP, model->getGeom(), data);
+    auto img = std::make_shared<Image2D<float>>(g->nx, g->nz, nhx, nhz, (float)g->dx, (float)g->dz, (float)g->ox,
+                                                (float)g->oz);
+    RtmAcoustic2D<float> rtm(model, img, src, drec, g->order, snapinc);
+    rtm.setSnapfile(tmpname("rtma2dfull"));
+    int r = rtm.run();
+    std::memcpy(image, img->getImagedata(), sizeof(float) * (size_t)g->nx * g->nz * nhx * nhz);
+    return r;
+}
+
 } // extern "C"

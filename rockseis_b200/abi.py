@@ -50,9 +50,13 @@ class Shot(C.Structure):
                 ("rec_field", C.c_int), ("rec_factor", C.c_void_p), ("rec_out", C.c_void_p)]
 
 
+SNAP_OPTIMAL, SNAP_FULL = 0, 1
+
+
 class AdjointOpts(C.Structure):
     _fields_ = [("ncheck", C.c_int), ("ckpt_precision", C.c_int), ("accum", C.c_int), ("misfit", C.c_int),
-                ("nhx", C.c_int), ("nhz", C.c_int), ("nhy", C.c_int), ("reserved", C.c_int * 9)]
+                ("nhx", C.c_int), ("nhz", C.c_int), ("nhy", C.c_int), ("snapmethod", C.c_int), ("snapinc", C.c_int),
+                ("noreverse", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class AdjointShot(C.Structure):

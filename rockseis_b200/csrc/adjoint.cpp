@@ -21,6 +21,7 @@
 //             after step capo-1 (the reference's pairing)
 // Every correlation launch covers all shots.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -63,6 +64,11 @@ public:
     int kind = RSGPU_KIND_FWI, phys = PHYS_A2D, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE;
     int nhx = 1, nhz = 1;
     int ncheck = 0, nslots = 0, nxmax = 0, nzmax = 0;
+    // FULL snapshots (FwiAcoustic2D::run, RtmAcoustic2D::run): the forward P interior
+    // every snapinc steps, snapnt of them, correlated at adjoint times t with
+    // (t - enddiff) % snapinc == 0
+    int snapmethod = RSGPU_SNAP_OPTIMAL, snapinc = 1, snapnt = 0, enddiff = 0;
+    bool noreverse = false;
     int misfit_type = RSGPU_MISFIT_DIFFERENCE, nrec_max = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan> fw, bw;
@@ -78,6 +84,9 @@ public:
     bool ran = false;
 
 private:
+    rsgpu_status run_full();
+    rsgpu_status reset_outputs();
+    rsgpu_status residuals();
     rsgpu_status correlate();
     rsgpu_status save(int slot);
     rsgpu_status load(int slot);
@@ -96,6 +105,19 @@ Adjoint::~Adjoint()
     dev_free(dbuf, stream);
     dev_free(ckpt, stream);
     if (stream) cudaStreamDestroy(stream);
+}
+
+// Snapshot2D's enddiff (lib/snap.cpp:334-337), evaluated in the element type:
+// the adjoint time of the last snapshot minus that of the last forward step.
+static int snap_enddiff(int nt, double dt_cfg, int snapinc, int prec)
+{
+    const int snapnt = (nt - 1) / snapinc + 1;
+    if (prec == PREC_F64) {
+        const double dt = dt_cfg, snapdt = dt * snapinc;
+        return (int)rintf((float)(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt));
+    }
+    const float dt = (float)dt_cfg, snapdt = dt * snapinc;
+    return (int)rintf(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt);
 }
 
 static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
@@ -125,6 +147,14 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_ARG;
     }
     if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && o->snapmethod != RSGPU_SNAP_FULL) {
+        set_error("bad snapmethod %d", o->snapmethod);
+        return RSGPU_ERR_ARG;
+    }
+    if (o->snapmethod == RSGPU_SNAP_FULL && el) {
+        set_error("FULL snapshots are built for the acoustic 2D gradient and image (FwiAcoustic2D::run, RtmAcoustic2D::run)");
+        return RSGPU_ERR_UNSUPPORTED;
+    }
     if (kind == RSGPU_KIND_RTM && (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || o->nhz % 2 == 0)) {
         set_error("nhx and nhz must be odd and positive");
         return RSGPU_ERR_ARG;
@@ -174,7 +204,13 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     ck_es = ck == CK_NATIVE ? (size_t)es : 2;
     nhx = kind == RSGPU_KIND_RTM ? o->nhx : 1;
     nhz = kind == RSGPU_KIND_RTM ? o->nhz : 1;
-    {
+    snapmethod = o->snapmethod;
+    if (snapmethod == RSGPU_SNAP_FULL) {
+        snapinc = std::max(o->snapinc, 1);
+        snapnt = (c->nt - 1) / snapinc + 1;
+        enddiff = snap_enddiff(c->nt, c->dt, snapinc, prec);
+        noreverse = kind == RSGPU_KIND_FWI && o->noreverse != 0;
+    } else {
         RevolveSchedule probe(c->nt, o->ncheck);
         ncheck = probe.snaps();
     }
@@ -280,6 +316,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     // and the C-PML memory strips
     segs.clear();
     slot_elems = 0;
+    nslots = snapmethod == RSGPU_SNAP_FULL ? snapnt : ncheck;
     for (int i = 0; i < ns; i++) {
         const ShotLayout &L = fw->shots[i];
         const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
@@ -292,19 +329,23 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
             slot_elems = rup(slot_elems, 64);   // keep every block 128-byte aligned in 16-bit slots
             segs.push_back(g);
         };
+        if (snapmethod == RSGPU_SNAP_FULL) {
+            // Snapshot2D::writeSnap: the nx*nz interior of P (lib/snap.cpp:638-667)
+            add(L.f[A2_P] + org + ((size_t)cfg.lpml * L.pitch + cfg.lpml) * es, nz[i], nx[i], L.pitch);
+            continue;
+        }
         for (int f = 0; f < nfields(phys); f++) add(L.f[f] + org, L.nzp, L.nxp, L.pitch);
         for (int p = 0; p < npsi(phys); p++) add(L.psix[p], L.nzp, 2 * cfg.lpml, 2 * cfg.lpml);
         for (int p = 0; p < npsi(phys); p++) add(L.psiz[p], 2 * cfg.lpml, L.nxp, L.nxp);
     }
     o_segs = take(sizeof(CkptSeg) * segs.size());
-    o_scales = take(sizeof(float) * segs.size() * ncheck);
+    o_scales = take(sizeof(float) * segs.size() * nslots);
     o_maxbits = take(sizeof(unsigned) * segs.size());
     if (dev_alloc(&dbuf, off, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %zu bytes failed", off);
         return RSGPU_ERR_NOMEM;
     }
-    nslots = ncheck;
     const size_t ck_bytes = slot_elems * ck_es * (size_t)nslots;
     if (dev_alloc(&ckpt, ck_bytes, stream) != cudaSuccess) {
         cudaGetLastError();
@@ -444,12 +485,11 @@ rsgpu_status Adjoint::correlate()
     return RSGPU_OK;
 }
 
-rsgpu_status Adjoint::run()
+rsgpu_status Adjoint::reset_outputs()
 {
-    const int nt = cfg.nt;
-    const long long l0 = fw->launches + bw->launches;
     launches = 0;
     fw_steps = bw_steps = ckpt_bytes = 0;
+    ran = false;
     ST(fw->reset());
     ST(bw->reset());
     for (int i = 0; i < nshots; i++) {
@@ -460,6 +500,78 @@ rsgpu_status Adjoint::run()
         if (elastic()) CU(cudaMemsetAsync(D(o_g2[i]), 0, n2 * gs, stream));
         if (o_ilum[i]) CU(cudaMemsetAsync(D(o_ilum[i]), 0, n2 * gs, stream));
     }
+    return RSGPU_OK;
+}
+
+// computeMisfit + computeResiduals of every shot: the misfit and the residual
+// traces that the adjoint plan injects
+rsgpu_status Adjoint::residuals()
+{
+    const bool corr = misfit_type == RSGPU_MISFIT_CORRELATION;
+    cudaError_t e = elastic()
+                    ? (corr ? launch_residual_corr_e2d(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream)
+                            : launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream))
+                    : corr ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream, true)
+                           : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+    if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+    launches += 1;
+    return RSGPU_OK;
+}
+
+// FwiAcoustic2D::run (lib/fwi.cpp:1030-1156) and RtmAcoustic2D::run
+// (lib/rtm.cpp:222-326): the forward loop records every step and saves the P
+// interior after steps 0, snapinc, 2*snapinc, ...; the adjoint loop steps the
+// adjoint wavefield from a zero state and, at the adjoint times t with
+// (t - enddiff) % snapinc == 0, correlates it with snapshot (t - enddiff)/snapinc
+// (Snapshot2D::readSnap counts the snapshots down from the last one written).
+// Steps between two saves or two correlations go to the plans as one range.
+rsgpu_status Adjoint::run_full()
+{
+    const int nt = cfg.nt;
+    const long long l0 = fw->launches + bw->launches;
+    ST(reset_outputs());
+    ST(fw->set_recording(true));
+    ST(fw->run(0, 1));
+    ST(save(0));
+    for (int k = 1; k < snapnt; k++) {
+        ST(fw->run((k - 1) * snapinc + 1, snapinc));
+        ST(save(k));
+    }
+    const int done = (snapnt - 1) * snapinc + 1;
+    if (done < nt) ST(fw->run(done, nt - done));
+    fw_steps = nt;
+    ST(fw->set_recording(false));
+    if (kind == RSGPU_KIND_FWI) ST(residuals());
+    if (!noreverse) {
+        // adjoint step index k runs data time t = nt-1-k
+        auto aligned = [&](int k) { return ((nt - 1 - k) - enddiff) % snapinc == 0; };
+        for (int k = 0; k < nt;) {
+            int e = k;
+            while (e < nt && !aligned(e)) e++;
+            const int n = (e < nt ? e + 1 : nt) - k;
+            ST(bw->run(k, n));
+            bw_steps += n;
+            k += n;
+            if (e < nt) {
+                ST(load(((nt - 1 - e) - enddiff) / snapinc));
+                ST(correlate());
+            }
+        }
+    }
+    launches += fw->launches + bw->launches - l0;
+    CU(cudaStreamSynchronize(stream));
+    ST(fw->check_device_error());
+    ST(bw->check_device_error());
+    ran = true;
+    return RSGPU_OK;
+}
+
+rsgpu_status Adjoint::run()
+{
+    if (snapmethod == RSGPU_SNAP_FULL) return run_full();
+    const int nt = cfg.nt;
+    const long long l0 = fw->launches + bw->launches;
+    ST(reset_outputs());
     ST(fw->set_recording(true));
     RevolveSchedule rev(nt, ncheck);
     for (;;) {
@@ -478,18 +590,7 @@ rsgpu_status Adjoint::run()
             ST(fw->run(capo, 1));
             fw_steps += 1;
             ST(fw->set_recording(false));
-            if (kind == RSGPU_KIND_FWI) {
-                const bool corr = misfit_type == RSGPU_MISFIT_CORRELATION;
-                cudaError_t e = elastic()
-                                ? (corr ? launch_residual_corr_e2d(prec, acc, D(o_res), nshots, nrec_max,
-                                                                   (double *)D(o_misfit), stream)
-                                        : launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream))
-                                : corr
-                                    ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream, true)
-                                    : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
-                if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-                launches += 1;
-            }
+            if (kind == RSGPU_KIND_FWI) ST(residuals());
             ST(bw->inject_record_only(nt - 1 - capo));
             ST(correlate());
         } else if (a == RSGPU_YOUTURN) {
@@ -567,7 +668,7 @@ rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
         void *ress[3] = {s[i].datares, elastic() ? s[i].datares_vx : nullptr, elastic() ? s[i].datares_vz : nullptr};
         for (int k = 0; k < 3; k++) {
             if (mods[k]) ST(fw->read_traces(i, mods[k], k));
-            if (!ress[k]) continue;
+            if (!ress[k] || noreverse) continue;   // FwiAcoustic2D::run leaves dataresP unset
             const size_t n = (size_t)nrec[i] * cfg.nt;
             tmp.resize(n * es);
             CU(cudaMemcpyAsync(tmp.data(), (char *)bw->arena + bw->shots[i].wavk[k], n * es, cudaMemcpyDeviceToHost,
@@ -576,7 +677,7 @@ rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
             if (es == 8) add_into<double, double>(ress[k], tmp, n);
             else add_into<float, float>(ress[k], tmp, n);
         }
-        if (s[i].wavgrad) ST(bw->read_traces(i, s[i].wavgrad));
+        if (s[i].wavgrad && !noreverse) ST(bw->read_traces(i, s[i].wavgrad));
         if (s[i].misfit) {
             // the reference keeps the misfit in T
             if (acc == ACC_REF && es == 4) *s[i].misfit = (double)(float)((float)*s[i].misfit + (float)mis[i]);

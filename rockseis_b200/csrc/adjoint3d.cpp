@@ -94,6 +94,10 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         return RSGPU_ERR_ARG;
     }
     if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL) {
+        set_error("snapmethod %d: the 3D drivers are built with Revolve checkpointing (run_optimal)", o->snapmethod);
+        return o->snapmethod == RSGPU_SNAP_FULL ? RSGPU_ERR_UNSUPPORTED : RSGPU_ERR_ARG;
+    }
     const int hy = o->nhy > 0 ? o->nhy : 1;
     if (k_ == RSGPU_KIND_RTM && (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || hy % 2 == 0 || o->nhz % 2 == 0)) {
         set_error("nhx, nhy and nhz must be odd and positive");

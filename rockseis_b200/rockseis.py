@@ -606,10 +606,13 @@ class _Adjoint:
         self.accum = abi.ACCUM_REFERENCE
         self.misfit_type = abi.MISFIT_DIFFERENCE
         self.tile = -1
+        self.noreverse = False
 
     def setModel(self, m): self.model = m
     def setSource(self, s): self.source = s
     def setDataP(self, d): self.dataP = d
+    def setSnapinc(self, n): self.snapinc = int(n) if int(n) > 0 else 1
+    def getSnapinc(self): return self.snapinc
     def setNcheck(self, n): self.ncheck = int(n)
     def setMisfit_type(self, t): self.misfit_type = int(t)
     def setCheckpointPrecision(self, p): self.ckpt_precision = int(p)   # no reference counterpart
@@ -619,11 +622,13 @@ class _Adjoint:
         check_stability(self.model, self.source.dt, self.cls)
         return True
 
-    def _opts(self, nhx=1, nhz=1, nhy=1) -> abi.AdjointOpts:
+    def _opts(self, nhx=1, nhz=1, nhy=1, full=False) -> abi.AdjointOpts:
         o = abi.AdjointOpts()
         o.ncheck, o.ckpt_precision, o.accum, o.misfit, o.nhx, o.nhz = (self.ncheck, self.ckpt_precision, self.accum,
                                                                         self.misfit_type, nhx, nhz)
         o.nhy = nhy
+        o.snapmethod = abi.SNAP_FULL if full else abi.SNAP_OPTIMAL
+        o.snapinc, o.noreverse = self.snapinc, int(bool(self.noreverse))
         return o
 
     def _adjoint_shot(self, keep: list) -> abi.AdjointShot:
@@ -647,6 +652,8 @@ class FwiAcoustic2D(_Adjoint):
         self.misfit = 0.0
 
     def setSrcilum(self, img): self.srcilum = img
+    def setNoreverse(self, v): self.noreverse = bool(v)
+    def getNoreverse(self): return self.noreverse
     def setVpgrad(self, img): self.vpgrad = img
     def setRhograd(self, img): self.rhograd = img
     def setWavgrad(self, d): self.wavgrad = d
@@ -668,6 +675,11 @@ class FwiAcoustic2D(_Adjoint):
         self._mis = C.c_double(0.0)
         a.misfit = C.pointer(self._mis)
         return a
+
+    def run(self):
+        """FwiAcoustic2D::run (lib/fwi.cpp:1030-1156): FULL snapshots every snapinc
+        steps; with setNoreverse(True) the forward run, datamodP and the misfit only."""
+        return fwi_gradient_batch([self], full=True)
 
     def run_optimal(self):
         return fwi_gradient_batch([self])
@@ -808,6 +820,10 @@ class RtmAcoustic2D(_Adjoint):
         a.image = ptr(self.pimage.getImagedata())
         return a
 
+    def run(self):
+        """RtmAcoustic2D::run (lib/rtm.cpp:222-326): FULL snapshots every snapinc steps."""
+        return rtm_image_batch([self], full=True)
+
     def run_optimal(self):
         return rtm_image_batch([self])
 
@@ -845,11 +861,11 @@ def _adjoint_tile(jobs) -> int:
                  j0.precision)
 
 
-def _adjoint_batch(jobs, fn):
+def _adjoint_batch(jobs, fn, full):
     j0 = jobs[0]
     j0.checkStability()
     cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
-    opts = j0._opts(*_lags(j0))
+    opts = j0._opts(*_lags(j0), full=full)
     keep: list = []
     shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
     check(fn(C.byref(cfg), C.byref(opts), len(jobs), shots))
@@ -859,25 +875,26 @@ def _adjoint_batch(jobs, fn):
     return FWI_OK
 
 
-def fwi_gradient_batch(jobs):
+def fwi_gradient_batch(jobs, full=False):
     """Many FwiAcoustic2D shots (each with its own model window) in one batched
-    gradient computation; per-shot outputs accumulate like run_optimal's."""
-    return _adjoint_batch(jobs, abi.lib.rsgpu_fwi_gradient)
+    gradient computation; per-shot outputs accumulate like run_optimal's (run's
+    with full=True: FULL snapshots every snapinc steps of the first job)."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_fwi_gradient, full)
 
 
-def rtm_image_batch(jobs):
-    """Many RtmAcoustic2D shots imaged in one batched run."""
-    return _adjoint_batch(jobs, abi.lib.rsgpu_rtm_image)
+def rtm_image_batch(jobs, full=False):
+    """Many RtmAcoustic2D shots imaged in one batched run (full: as RtmAcoustic2D::run)."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_rtm_image, full)
 
 
 class AdjointBatch:
     """Device-resident gradient/image batch (rsgpu_adjoint_*): create once, run many times."""
 
-    def __init__(self, jobs, kind=abi.KIND_FWI):
+    def __init__(self, jobs, kind=abi.KIND_FWI, full=False):
         j0 = jobs[0]
         self.jobs = jobs
         self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
-        self.opts = j0._opts(*_lags(j0))
+        self.opts = j0._opts(*_lags(j0), full=full)
         self._keep: list = []
         self.shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(self._keep) for j in jobs])
         self.h = C.c_void_p()

@@ -259,3 +259,109 @@ def test_fwi_correlation_fp64_accumulation_close(require_gpu):
     assert abs(got["misfit"] - ref["misfit"]) <= 1e-5 * abs(ref["misfit"])
     for k in GRAD:
         assert rel_l2(got[k], ref[k]) <= 1e-5, k
+
+
+# ---------------------------------------------------------------- FULL snapshots (FwiAcoustic2D::run, RtmAcoustic2D::run)
+def _snapfull():
+    import os
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "snapfull.npz"))
+
+
+def full_reference(c, snapinc, noreverse=0):
+    """FwiAcoustic2D::run of the reference: the library itself where oracle/_ref is
+    built, else the committed outputs (tests/golden/make_golden_snapfull.py)."""
+    from oracle import api
+    if api.ref_available():
+        return api.ref_fwi_a2d_full(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords,
+                                    c.obs.astype(np.float32), snapinc, noreverse=noreverse)
+    g = _snapfull()
+    if f"fwi_s{snapinc}_vpgrad" not in g.files and not noreverse:
+        pytest.skip(f"no committed outputs for snapinc {snapinc} and the reference library is not built")
+    assert np.array_equal(c.obs.astype(np.float32), g["obs"]) and np.array_equal(c.pb.vp, g["vp"])
+    out = {k: g[f"fwi_{k}"] for k in ("datamod", "datares")}
+    out["misfit"] = float(g["fwi_misfit"])
+    for k in ("vpgrad", "rhograd", "wavgrad"):
+        out[k] = np.zeros_like(g["fwi_s3_vpgrad"] if k != "wavgrad" else g["fwi_s3_wavgrad"]) if noreverse \
+            else g[f"fwi_s{snapinc}_{k}"]
+    if noreverse:
+        out["datares"] = np.zeros_like(out["datares"])
+    return out
+
+
+@pytest.mark.parametrize("snapinc", [1, 3, 7])
+def test_fwi_full_snapshots_bitwise(require_gpu, snapinc):
+    # snapinc 3 and 7 leave enddiff = 2 and 5: the adjoint times that correlate are not
+    # the forward times that were saved, as in Snapshot2D
+    c = fwi_case()
+    ref = full_reference(c, snapinc)
+    f = make_fwi(c)
+    f.setSnapinc(snapinc)
+    assert f.run() == 1
+    assert_same(outputs(f), ref)
+
+
+def test_fwi_full_snapshots_noreverse(require_gpu):
+    # forward pass, datamodP and the misfit only; gradients, wavelet gradient and
+    # residuals stay as the caller left them
+    c = fwi_case()
+    ref = full_reference(c, 3, noreverse=1)
+    f = make_fwi(c)
+    f.setSnapinc(3)
+    f.setNoreverse(True)
+    assert f.run() == 1
+    got = outputs(f)
+    assert np.abs(ref["datamod"]).max() > 0
+    assert np.array_equal(got["datamod"], ref["datamod"])
+    assert got["misfit"] == ref["misfit"]
+    for k in ("vpgrad", "rhograd", "wavgrad", "datares"):
+        assert not np.any(got[k]), k
+
+
+@pytest.mark.parametrize("snapinc,nhx,nhz", [(4, 3, 1), (1, 1, 1), (5, 1, 3)])
+def test_rtm_full_snapshots_bitwise(require_gpu, snapinc, nhx, nhz):
+    from oracle import api
+    c = fwi_case()
+    if api.ref_available():
+        ref = api.ref_rtm_a2d_full(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords,
+                                   c.obs.astype(np.float32), snapinc, nhx=nhx, nhz=nhz)
+    elif (snapinc, nhx, nhz) == (4, 3, 1):
+        ref = _snapfull()["rtm_s4_h3"]
+    else:
+        pytest.skip("reference library not built")
+    c.rec.data = np.ascontiguousarray(c.obs)
+    img = Image2D("pimage", c.model, nhx, nhz)
+    r = RtmAcoustic2D(c.model, img, c.src, c.rec, c.order, snapinc)
+    assert r.run() == 1
+    got = img.getImagedata()
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(got, ref), f"max abs diff {np.abs(got - ref).max()}"
+
+
+def test_fwi_full_snapshots_batched_windows_bitwise(require_gpu):
+    from oracle import api
+    if not api.ref_available():
+        pytest.skip("reference library not built")
+    cases = [fwi_case(nx=81, nz=61, seed=1, scoord=(400.3, 23.7)), fwi_case(nx=97, nz=53, seed=2, scoord=(150.9, 31.2))]
+    refs = [full_reference(c, 5) for c in cases]
+    jobs = [make_fwi(c) for c in cases]
+    for j in jobs:
+        j.setSnapinc(5)
+    assert fwi_gradient_batch(jobs, full=True) == 1
+    for j, ref in zip(jobs, refs):
+        assert_same(outputs(j), ref)
+
+
+@pytest.mark.parametrize("ckpt", [abi.CKPT_F16, abi.CKPT_BF16])
+def test_fwi_full_16bit_snapshots_close(require_gpu, ckpt):
+    # 16-bit snapshots with a power-of-two scale per shot: the same bars as the
+    # 16-bit Revolve checkpoints hold against the lossless result
+    c = fwi_case()
+    ref = full_reference(c, 3)
+    f = make_fwi(c, ckpt=ckpt)
+    f.setSnapinc(3)
+    assert f.run() == 1
+    got = outputs(f)
+    tol = CKPT16_TOL if ckpt == abi.CKPT_F16 else 3e-3
+    for k in GRAD:
+        assert rel_l2(got[k], ref[k]) < tol, (k, rel_l2(got[k], ref[k]))
+    assert np.array_equal(got["datamod"], ref["datamod"])

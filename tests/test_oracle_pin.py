@@ -347,3 +347,37 @@ def test_stagger_elastic3d_matches_reference(fs):
                                 *[a.ctypes.data for a in ref])
     for name, got, r in zip(m.names, m.padded(), ref):
         assert np.array_equal(got, r), name
+
+
+# ---------------------------------------------------------------- FULL snapshots (Fwi/RtmAcoustic2D::run)
+def _snapfull():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "snapfull.npz"))
+
+
+@needs_ref
+def test_snapfull_fixture_matches_reference_live():
+    from tests.cases import fwi_case
+    g = _snapfull()
+    c = fwi_case()
+    assert np.array_equal(c.obs.astype(np.float32), g["obs"]) and np.array_equal(c.pb.vp, g["vp"])
+    r = api.ref_fwi_a2d_full(c.pb, g["scoords"], g["wav"], g["gcoords"], g["obs"], 7)
+    for k in ("vpgrad", "rhograd", "wavgrad"):
+        assert np.array_equal(r[k], g[f"fwi_s7_{k}"]), k
+    for k in ("datamod", "datares", "misfit"):
+        assert np.array_equal(r[k], g[f"fwi_{k}"]), k
+    img = api.ref_rtm_a2d_full(c.pb, g["scoords"], g["wav"], g["gcoords"], g["obs"], 4, nhx=3)
+    assert np.array_equal(img, g["rtm_s4_h3"])
+
+
+def test_snapshot_enddiff_and_count():
+    """Snapshot2D (lib/snap.cpp:334-337): snapnt = (nt-1)/snapinc + 1 snapshots and
+    enddiff = (nt-1) mod snapinc for the time steps in use; the last adjoint time
+    that correlates is nt-1, the snapshot it reads is the one saved at nt-1-enddiff."""
+    for nt in (2, 3, 300, 1001, 2000):
+        for si in (1, 2, 3, 7, 64, nt - 1):
+            if si < 1:
+                continue
+            snapnt = (nt - 1) // si + 1
+            dt = np.float32(6e-4)
+            enddiff = int(np.rint(np.float32((nt - 1) * dt - (snapnt - 1) * (dt * np.float32(si))) / dt))
+            assert enddiff == (nt - 1) % si, (nt, si)
