@@ -55,7 +55,13 @@ enum { RSGPU_F32_EXACT = 0, RSGPU_F32_FAST = 1, RSGPU_F64 = 2 };
 /* field codes: identical to the reference's rs_field (include/utils.h:22) */
 enum { RSGPU_PRESSURE = 0, RSGPU_VX = 1, RSGPU_VY = 2, RSGPU_VZ = 3 };
 /* misfit codes: identical to rs_fwimisfit (include/utils.h:26) */
-enum { RSGPU_MISFIT_DIFFERENCE = 0, RSGPU_MISFIT_CORRELATION = 1 };
+enum {
+    RSGPU_MISFIT_DIFFERENCE = 0,
+    RSGPU_MISFIT_CORRELATION = 1,
+    RSGPU_MISFIT_ADAPTIVE_GAUSS = 2,   /* acoustic FWI: Wiener shaping filter, Gaussian weight */
+    RSGPU_MISFIT_ADAPTIVE_LINEAR = 3,  /* acoustic FWI: Wiener shaping filter, ramp weight */
+    RSGPU_MISFIT_ADAPTIVE_SINGLE = 4   /* elastic only in the reference; not built */
+};
 enum { RSGPU_INTERP_LINEAR = 0, RSGPU_INTERP_BSPLINE = 1, RSGPU_INTERP_SINC = 2 };   /* rs_interpmode */
 /* checkpoint storage precision of the FWI/RTM gradient drivers */
 enum { RSGPU_CKPT_NATIVE = 0, RSGPU_CKPT_F16 = 1, RSGPU_CKPT_BF16 = 2 };

@@ -112,6 +112,7 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
     lib.ref_fwi_a3d_corr_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V]
+    lib.ref_fwi_a3d_misfit_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V, I]
     lib.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
     lib.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
     lib.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
@@ -521,9 +522,8 @@ def ref_fwi_a3d(pb, scoords, wav, gcoords, obs, ncheck, misfit=0):
     dr = np.zeros((nr, pb.nt), np.float32)
     mis = C.c_double()
     vp, rho, w, ob = _keep(pb.vp, pb.rho, wav, obs, dtype=np.float32)
-    fn = ref().ref_fwi_a3d_corr_f if misfit == 1 else ref().ref_fwi_a3d_f
-    r = fn(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
-           _p(o["vpgrad"]), _p(o["rhograd"]), _p(wg), _p(dm), _p(dr), C.byref(mis))
+    r = ref().ref_fwi_a3d_misfit_f(C.byref(g), _p(vp), _p(rho), ns, _p(sc), _p(w), nr, _p(gc), _p(ob), ncheck,
+                                   _p(o["vpgrad"]), _p(o["rhograd"]), _p(wg), _p(dm), _p(dr), C.byref(mis), misfit)
     assert r == 1
     o.update(wavgrad=wg, datamod=dm, datares=dr, misfit=mis.value)
     return o

@@ -566,6 +566,15 @@ int ref_fwi_a3d_corr_f(const ref_grid *g, const float *vp, const float *rho, int
     return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
                           misfit, 1);
 }
+/* FwiAcoustic3D::run_optimal with any rs_fwimisfit value (ADAPTIVE_GAUSS = 2, ADAPTIVE_LINEAR = 3). */
+int ref_fwi_a3d_misfit_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
+                         const float *wav, int nr, const double *gc, const float *obs, int ncheck, float *vpgrad,
+                         float *rhograd, float *wavgrad, float *datamod, float *datares, double *misfit,
+                         int misfit_type)
+{
+    return fwi_a3d<float>(g, vp, rho, ns, sc, wav, nr, gc, obs, ncheck, vpgrad, rhograd, wavgrad, datamod, datares,
+                          misfit, misfit_type);
+}
 /* Model::getLocalsize2d / getLocalsize3d (lib/model.cpp:272-470): the aperture window of
  * ntr traces whose source and receiver coordinates are both given (x,z or x,y,z per
  * trace); map = 0 (SMAP) or 1 (GMAP). */

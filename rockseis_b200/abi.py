@@ -25,7 +25,7 @@ PRESSURE, VX, VY, VZ, SXX, SYY, SZZ, SYZ, SXZ, SXY = range(10)
 CKPT_NATIVE, CKPT_F16, CKPT_BF16 = 0, 1, 2
 ADVANCE, TAKESHOT, RESTORE, FIRSTURN, YOUTURN, TERMINATE, ERROR = range(7)
 ACCUM_REFERENCE, ACCUM_F64 = 0, 1
-MISFIT_DIFFERENCE, MISFIT_CORRELATION = 0, 1
+MISFIT_DIFFERENCE, MISFIT_CORRELATION, MISFIT_ADAPTIVE_GAUSS, MISFIT_ADAPTIVE_LINEAR, MISFIT_ADAPTIVE_SINGLE = 0, 1, 2, 3, 4
 INTERP_LINEAR, INTERP_BSPLINE, INTERP_SINC = 0, 1, 2
 KIND_FWI, KIND_RTM = 0, 1
 

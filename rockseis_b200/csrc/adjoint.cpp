@@ -79,6 +79,8 @@ public:
     std::vector<size_t> o_vp, o_vs, o_rho, o_obs, o_obsx, o_obsz, o_g0, o_g1, o_g2;
     std::vector<size_t> o_ilum;      // acoustic FWI source illumination (0 = not asked for)
     size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    std::vector<size_t> o_work, o_tnorm;   // ADAPTIVE misfits: per-trace scratch and filter norms
+    size_t o_atab = 0;                      // ADAPTIVE misfits: weights and summation-order tables
     std::vector<int> nx, nz, nrec, nsrc;
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
     bool ran = false;
@@ -130,8 +132,10 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_UNSUPPORTED;
     }
     const bool el = c->physics == RSGPU_ELASTIC2D;
-    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION) {
-        set_error("misfit %d: DIFFERENCE and CORRELATION are built", o->misfit);
+    const bool adaptive = o->misfit == RSGPU_MISFIT_ADAPTIVE_GAUSS || o->misfit == RSGPU_MISFIT_ADAPTIVE_LINEAR;
+    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION && !(adaptive && !el)) {
+        set_error("misfit %d: DIFFERENCE and CORRELATION are built%s", o->misfit,
+                  el ? "" : ", and ADAPTIVE_GAUSS / ADAPTIVE_LINEAR for the acoustic gradient");
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (o->misfit == RSGPU_MISFIT_CORRELATION && kind == RSGPU_KIND_FWI) {
@@ -306,6 +310,17 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         }
     }
     o_misfit = take(sizeof(double) * ns);
+    const bool adaptive = kind == RSGPU_KIND_FWI && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
+                                                     misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR);
+    o_work.assign(ns, 0);
+    o_tnorm.assign(ns, 0);
+    if (adaptive) {
+        for (int i = 0; i < ns; i++) {
+            o_work[i] = take((size_t)5 * nrec[i] * cfg.nt * es);
+            o_tnorm[i] = take((size_t)nrec[i] * es);
+        }
+        o_atab = take(adaptive_table_bytes(prec, cfg.nt));
+    }
     const size_t corr_bytes = elastic() ? (prec == PREC_F64 ? sizeof(Corr2DE<double>) : sizeof(Corr2DE<float>))
                                         : (prec == PREC_F64 ? sizeof(Corr2D<double>) : sizeof(Corr2D<float>));
     const size_t res_bytes = elastic() ? (prec == PREC_F64 ? sizeof(Resid2DE<double>) : sizeof(Resid2DE<float>))
@@ -365,6 +380,12 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         }
     }
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
+    std::vector<unsigned char> atab;
+    if (adaptive) {
+        atab.resize(adaptive_table_bytes(prec, cfg.nt));
+        adaptive_fill_tables(prec, misfit_type, cfg.nt, atab.data());
+        CU(cudaMemcpyAsync(D(o_atab), atab.data(), atab.size(), cudaMemcpyHostToDevice, stream));
+    }
     std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
     if (elastic()) {
         if (prec == PREC_F64) build_desc_e2d<double>(corr, res);
@@ -407,6 +428,10 @@ void Adjoint::build_desc(std::vector<unsigned char> &corr, std::vector<unsigned 
             r.res = (T *)(ba + B.wav);
             // the forward plan's receiver plan marks off-grid receivers with -1
             r.rec_pt = (const int *)(fa + fw->rec_pt_offsets[(size_t)i * MAXSETS]);
+            if (o_work[i]) {
+                r.work = (T *)D(o_work[i]);
+                r.tnorm = (T *)D(o_tnorm[i]);
+            }
         }
         r.nrec = nrec[i];
         r.nt = cfg.nt;
@@ -508,6 +533,13 @@ rsgpu_status Adjoint::reset_outputs()
 rsgpu_status Adjoint::residuals()
 {
     const bool corr = misfit_type == RSGPU_MISFIT_CORRELATION;
+    if (o_atab) {
+        cudaError_t e = launch_residual_adaptive(prec, acc, misfit_type, D(o_res), nshots, nrec_max, cfg.nt, D(o_atab),
+                                                 (double *)D(o_misfit), stream, true);
+        if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
+        launches += 2;
+        return RSGPU_OK;
+    }
     cudaError_t e = elastic()
                     ? (corr ? launch_residual_corr_e2d(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream)
                             : launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream))

@@ -215,67 +215,6 @@ __global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, d
 // comes from a radix select on the magnitude bit patterns, which order like the
 // non-negative values.  One CTA per shot; dynamic shared memory holds n1*n2 of
 // every trace.
-template <typename T> struct Bits;
-template <> struct Bits<float> { using U = unsigned int; static constexpr int NB = 32; };
-template <> struct Bits<double> { using U = unsigned long long; static constexpr int NB = 64; };
-
-template <typename T> __device__ __forceinline__ T sqrt_rn(T x);
-template <> __device__ __forceinline__ float sqrt_rn<float>(float x) { return __fsqrt_rn(x); }
-template <> __device__ __forceinline__ double sqrt_rn<double>(double x) { return __dsqrt_rn(x); }
-
-template <typename T>
-__device__ __forceinline__ typename Bits<T>::U mag_bits(T x)
-{
-    using U = typename Bits<T>::U;
-    U u;
-    memcpy(&u, &x, sizeof u);
-    return u & ~((U)1 << (Bits<T>::NB - 1));
-}
-
-// Magnitude bit pattern of the k-th smallest |r[i]|, i < n (k < n), found by the
-// whole CTA with four (float) or eight (double) 8-bit histogram passes.
-template <typename T>
-__device__ typename Bits<T>::U kth_mag_bits(const T *r, long n, long k)
-{
-    using U = typename Bits<T>::U;
-    __shared__ unsigned int hist[256];
-    __shared__ U prefix_s;
-    __shared__ long rank_s;
-    __syncthreads();
-    if (threadIdx.x == 0) { prefix_s = 0; rank_s = k; }
-    U mask = 0;
-    for (int shift = Bits<T>::NB - 8; shift >= 0; shift -= 8) {
-        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
-        __syncthreads();
-        const U prefix = prefix_s;
-        for (long i = threadIdx.x; i < n; i += blockDim.x) {
-            const U u = mag_bits(r[i]);
-            if ((u & mask) == prefix) atomicAdd(&hist[(unsigned)(u >> shift) & 255u], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            long rr = rank_s;
-            int b = 0;
-            while (b < 255 && rr >= (long)hist[b]) { rr -= hist[b]; b++; }
-            rank_s = rr;
-            prefix_s = prefix | ((U)b << shift);
-        }
-        mask |= (U)255 << shift;
-        __syncthreads();
-    }
-    const U out = prefix_s;
-    __syncthreads();
-    return out;
-}
-
-template <typename T>
-__device__ __forceinline__ T from_bits(typename Bits<T>::U u)
-{
-    T x;
-    memcpy(&x, &u, sizeof x);
-    return x;
-}
-
 __device__ __forceinline__ bool finite_f(float v) { return isfinite(v); }
 __device__ __forceinline__ bool finite_f(double v) { return isfinite(v); }
 

@@ -75,8 +75,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         set_error("elastic 3D: misfit %d: DIFFERENCE is built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
-    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION) {
-        set_error("misfit %d: DIFFERENCE and CORRELATION are built", o->misfit);
+    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION &&
+        o->misfit != RSGPU_MISFIT_ADAPTIVE_GAUSS && o->misfit != RSGPU_MISFIT_ADAPTIVE_LINEAR) {
+        set_error("misfit %d: DIFFERENCE, CORRELATION, ADAPTIVE_GAUSS and ADAPTIVE_LINEAR are built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (k_ == RSGPU_KIND_FWI && o->misfit == RSGPU_MISFIT_CORRELATION) {
@@ -244,6 +245,17 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     o_corr = take(corr_bytes * ns);
     o_res = take(res_bytes * ns);
     o_misfit = take(sizeof(double) * ns);
+    const bool adaptive = fwi() && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
+                                    misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR);
+    o_work.assign(ns, 0);
+    o_tnorm.assign(ns, 0);
+    if (adaptive) {
+        for (int i = 0; i < ns; i++) {
+            o_work[i] = take((size_t)5 * nrec[i] * cfg.nt * es);
+            o_tnorm[i] = take((size_t)nrec[i] * es);
+        }
+        o_atab = take(adaptive_table_bytes(prec, cfg.nt));
+    }
     segs.clear();
     slot_elems = 0;
     for (int i = 0; i < ns; i++) {
@@ -281,6 +293,12 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     }
     CU(cudaMemsetAsync(dbuf, 0, off, stream));
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
+    std::vector<unsigned char> atab;
+    if (adaptive) {
+        atab.resize(adaptive_table_bytes(prec, cfg.nt));
+        adaptive_fill_tables(prec, misfit_type, cfg.nt, atab.data());
+        CU(cudaMemcpyAsync(D(o_atab), atab.data(), atab.size(), cudaMemcpyHostToDevice, stream));
+    }
     std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
     std::vector<std::vector<int>> valids(ns);   // host copies stay alive until the stream sync below
     for (int i = 0; i < ns && fwi(); i++) {
@@ -367,6 +385,10 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
             r->obs = (const T *)D(o_obs[i]);
             r->res = (T *)(ba + B.wav);
             r->rec_pt = (const int *)D(o_valid[i]);
+            if (o_work[i]) {
+                r->work = (decltype(r->work))D(o_work[i]);
+                r->tnorm = (decltype(r->tnorm))D(o_tnorm[i]);
+            }
             r->nrec = nrec[i];
             r->nt = cfg.nt;
         };
@@ -465,6 +487,9 @@ rsgpu_status Adjoint3D::run()
             if (fwi()) {
                 ST(fw->set_recording(false));
                 cudaError_t e = elastic() ? launch_residual_e3d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream)
+                                : o_atab ? launch_residual_adaptive(prec, acc, misfit_type, D(o_res), nshots, nrec_max,
+                                                                    cfg.nt, D(o_atab), (double *)D(o_misfit), stream,
+                                                                    false)
                                 : misfit_type == RSGPU_MISFIT_CORRELATION
                                     ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit),
                                                            stream, false)

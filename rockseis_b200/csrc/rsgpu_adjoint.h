@@ -90,6 +90,8 @@ struct Resid2D {
     T *res;                     // residual [nrec][nt] (adjoint plan source traces)
     const int *rec_pt;          // -1 for receivers off the grid (excluded from the misfit)
     int nrec, nt;
+    T *work;                    // ADAPTIVE misfits: 5*nt scratch values per trace
+    T *tnorm;                   // ADAPTIVE misfits: the shaping filter's squared norm per trace
 };
 
 // One contiguous 2D block of state copied into / out of a checkpoint slot.
@@ -118,6 +120,15 @@ cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, dou
 // bounds the shared memory.
 cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
                                  cudaStream_t st, bool clip);
+// ADAPTIVE_GAUSS / ADAPTIVE_LINEAR misfits (Wiener shaping filter per trace) and
+// their residuals, with the 97th-percentile clip of the 2D drivers when `clip`.
+// `tables` holds adaptive_table_bytes(prec, nt) bytes filled by
+// adaptive_fill_tables; every Resid2D carries its work and tnorm arrays.
+enum { ADAPT_GAUSS = 2, ADAPT_LINEAR = 3 };
+size_t adaptive_table_bytes(int prec, int nt);
+void adaptive_fill_tables(int prec, int mode, int nt, void *host_tables);
+cudaError_t launch_residual_adaptive(int prec, int acc, int mode, const void *desc, int nshots, int nrec_max, int nt,
+                                     const void *tables, double *misfit, cudaStream_t st, bool clip);
 // The elastic CORRELATION misfit and residuals (P, Ux, Uz) with the reference's clips.
 cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
                                      cudaStream_t st);

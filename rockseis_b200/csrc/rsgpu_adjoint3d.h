@@ -31,6 +31,8 @@ public:
     std::vector<size_t> o_img, o_vp, o_rho, o_obs, o_g1, o_valid;
     std::vector<size_t> o_vs, o_obsy, o_obsz, o_g2;    // elastic: vs, Uy/Uz data, density gradient
     size_t o_corr = 0, o_res = 0, o_misfit = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    std::vector<size_t> o_work, o_tnorm;   // ADAPTIVE misfits: per-trace scratch and filter norms
+    size_t o_atab = 0;                      // ADAPTIVE misfits: weights and summation-order tables
     std::vector<int> nx, ny, nz, nrec;
     bool fwi() const { return kind == RSGPU_KIND_FWI; }
     bool elastic() const { return phys == PHYS_E3D; }

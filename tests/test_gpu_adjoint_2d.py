@@ -365,3 +365,61 @@ def test_fwi_full_16bit_snapshots_close(require_gpu, ckpt):
     for k in GRAD:
         assert rel_l2(got[k], ref[k]) < tol, (k, rel_l2(got[k], ref[k]))
     assert np.array_equal(got["datamod"], ref["datamod"])
+
+
+# ---------------------------------------------------------------- ADAPTIVE misfits (Wiener shaping filters)
+def adaptive_reference(c, misfit, ncheck=7, dims="a2d"):
+    """FwiAcoustic2D::run_optimal with an ADAPTIVE misfit: the reference library where
+    oracle/_ref is built, else the committed outputs (tests/golden/make_golden_adaptive.py)."""
+    import os
+    from oracle import api
+    if api.ref_available():
+        return api.ref_fwi_a2d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords,
+                               c.obs.astype(np.float32), ncheck, misfit=misfit)
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "adaptive.npz"))
+    assert ncheck == 7 and np.array_equal(c.obs.astype(np.float32), g[f"{dims}_obs"])
+    name = {abi.MISFIT_ADAPTIVE_GAUSS: "gauss", abi.MISFIT_ADAPTIVE_LINEAR: "linear"}[misfit]
+    out = {k: g[f"{dims}_{name}_{k}"] for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares")}
+    out["misfit"] = float(g[f"{dims}_{name}_misfit"])
+    return out
+
+
+@pytest.mark.parametrize("misfit", [abi.MISFIT_ADAPTIVE_GAUSS, abi.MISFIT_ADAPTIVE_LINEAR])
+def test_fwi_adaptive_misfit_bitwise(require_gpu, misfit):
+    # shaping filters by Levinson recursion, SU-ordered correlations and convolution,
+    # the 97th-percentile residual clip: every output equal to the reference's
+    c = fwi_case()
+    ref = adaptive_reference(c, misfit)
+    f = make_fwi(c, ncheck=7)
+    f.setMisfit_type(misfit)
+    assert f.run_optimal() == 1
+    got = outputs(f)
+    assert_same(got, ref)
+    assert (got["misfit"] < 0) == (misfit == abi.MISFIT_ADAPTIVE_GAUSS)
+    assert (got["datares"] == 0).mean() >= 0.03
+
+
+def test_fwi_adaptive_misfit_batched_windows_bitwise(require_gpu):
+    from oracle import api
+    if not api.ref_available():
+        pytest.skip("reference library not built")
+    cases = [fwi_case(nx=81, nz=61, seed=1, scoord=(400.3, 23.7)), fwi_case(nx=97, nz=53, seed=2, scoord=(150.9, 31.2))]
+    refs = [adaptive_reference(c, abi.MISFIT_ADAPTIVE_LINEAR, ncheck=6) for c in cases]
+    jobs = [make_fwi(c, ncheck=6) for c in cases]
+    for j in jobs:
+        j.setMisfit_type(abi.MISFIT_ADAPTIVE_LINEAR)
+    assert fwi_gradient_batch(jobs) == 1
+    for j, ref in zip(jobs, refs):
+        assert_same(outputs(j), ref)
+
+
+def test_fwi_adaptive_misfit_fp64_accumulation_close(require_gpu):
+    c = fwi_case()
+    ref = adaptive_reference(c, abi.MISFIT_ADAPTIVE_GAUSS)
+    f = make_fwi(c, ncheck=7, accum=abi.ACCUM_F64)
+    f.setMisfit_type(abi.MISFIT_ADAPTIVE_GAUSS)
+    assert f.run_optimal() == 1
+    got = outputs(f)
+    for k in GRAD:
+        assert rel_l2(got[k], ref[k]) < 1e-5, (k, rel_l2(got[k], ref[k]))
+    assert abs(got["misfit"] - ref["misfit"]) <= 1e-5 * abs(ref["misfit"])

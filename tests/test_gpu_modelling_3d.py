@@ -229,3 +229,23 @@ def test_fwi3d_correlation_misfit_exact_bitwise(require_gpu):
         assert np.abs(ref[k]).max() > 0, k
         assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
     assert got["misfit"] == ref["misfit"] and got["misfit"] < 0
+
+
+@pytest.mark.parametrize("misfit", [2, 3])
+def test_fwi3d_adaptive_misfit_bitwise(require_gpu, misfit):
+    # FwiAcoustic3D with ADAPTIVE_GAUSS / ADAPTIVE_LINEAR: no residual clip in 3D
+    import os
+    c = fwi3d_case()
+    if api.ref_available():
+        ref = api.ref_fwi_a3d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords,
+                              c.obs.astype(np.float32), 5, misfit=misfit)
+    else:
+        g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "adaptive.npz"))
+        assert np.array_equal(c.obs.astype(np.float32), g["a3d_obs"])
+        name = {2: "gauss", 3: "linear"}[misfit]
+        ref = {k: g[f"a3d_{name}_{k}"] for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares", "misfit")}
+    got = gpu_fwi3d(c, ncheck=5, misfit=misfit)
+    for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        assert np.abs(ref[k]).max() > 0, k
+        assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
+    assert got["misfit"] == float(ref["misfit"])
