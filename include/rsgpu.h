@@ -58,9 +58,11 @@ enum { RSGPU_PRESSURE = 0, RSGPU_VX = 1, RSGPU_VY = 2, RSGPU_VZ = 3 };
 enum {
     RSGPU_MISFIT_DIFFERENCE = 0,
     RSGPU_MISFIT_CORRELATION = 1,
-    RSGPU_MISFIT_ADAPTIVE_GAUSS = 2,   /* acoustic FWI: Wiener shaping filter, Gaussian weight */
-    RSGPU_MISFIT_ADAPTIVE_LINEAR = 3,  /* acoustic FWI: Wiener shaping filter, ramp weight */
-    RSGPU_MISFIT_ADAPTIVE_SINGLE = 4   /* elastic only in the reference; not built */
+    RSGPU_MISFIT_ADAPTIVE_GAUSS = 2,   /* Wiener shaping filter per trace, Gaussian weight */
+    RSGPU_MISFIT_ADAPTIVE_LINEAR = 3,  /* Wiener shaping filter per trace, ramp weight */
+    RSGPU_MISFIT_ADAPTIVE_SINGLE = 4   /* elastic 2D: one filter for the joined Ux/Uz traces;
+                                          the acoustic drivers treat it as DIFFERENCE, as the
+                                          reference's switch defaults do */
 };
 enum { RSGPU_INTERP_LINEAR = 0, RSGPU_INTERP_BSPLINE = 1, RSGPU_INTERP_SINC = 2 };   /* rs_interpmode */
 /* checkpoint storage precision of the FWI/RTM gradient drivers */
@@ -207,10 +209,13 @@ typedef struct {
                             checkpoint slots hold the state as 16-bit values with a power-of-two
                             scale per array */
     int accum;           /* RSGPU_ACCUM_* */
-    int misfit;          /* RSGPU_MISFIT_DIFFERENCE; RSGPU_MISFIT_CORRELATION for the FWI drivers
-                            (acoustic 2D lib/fwi.cpp:617-645, 808-849 with the 97th-percentile
-                            residual clip; acoustic 3D :1511-1540, 1696-1722 without it;
-                            elastic 2D :2939-3001, 3309-3426 with the x/z and P clips) */
+    int misfit;          /* RSGPU_MISFIT_*: DIFFERENCE; CORRELATION (acoustic 2D lib/fwi.cpp:617-645,
+                            808-849 with the 97th-percentile residual clip; acoustic 3D
+                            :1511-1540, 1696-1722 without it; elastic 2D :2939-3001, 3309-3426
+                            with the x/z and P clips); ADAPTIVE_GAUSS / ADAPTIVE_LINEAR (acoustic
+                            2D :646-735, 851-1014, acoustic 3D :1541-1630, 1725-1840, elastic 2D
+                            :3002-3148, 3428-3674); ADAPTIVE_SINGLE (elastic 2D :3149-3196,
+                            3675-3753).  The elastic 3D gradient takes DIFFERENCE only */
     int nhx, nhz;        /* RTM extended-image lags (Rtm::setNhx/setNhz; odd, 1 = zero lag) */
     int nhy;             /* 3D RTM y lags (Rtm::setNhy; odd, 0 or 1 = zero lag) */
     int snapmethod;      /* RSGPU_SNAP_OPTIMAL: Revolve checkpointing (run_optimal);

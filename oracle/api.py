@@ -104,6 +104,7 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_mod_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, I, V]
     lib.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
+    lib.ref_fwi_e2d_misfit_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V, I]
     lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
     lib.ref_fwi_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I] + [V] * 5 + [V]
     lib.ref_rtm_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
@@ -420,10 +421,9 @@ def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
     ress = np.zeros((3, nr, pb.nt), np.float32)
     mis = C.c_double()
     vp, vs, rho, w, op, ox, oz = _keep(pb.vp, pb.vs, pb.rho, wav, obs3[0], obs3[1], obs3[2], dtype=np.float32)
-    fn = ref().ref_fwi_e2d_corr_f if misfit == 1 else ref().ref_fwi_e2d_f
-    r = fn(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
-           _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]), _p(wg),
-           _p(mods), _p(ress), C.byref(mis))
+    r = ref().ref_fwi_e2d_misfit_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
+                                   _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]),
+                                   _p(wg), _p(mods), _p(ress), C.byref(mis), misfit)
     assert r == 1
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out

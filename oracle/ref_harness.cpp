@@ -638,6 +638,16 @@ int ref_fwi_e2d_corr_f(const ref_grid *g, const float *vp, const float *vs, cons
     return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
                           rhograd, wavgrad, mods, ress, misfit, 1);
 }
+/* FwiElastic2D::run_optimal with any rs_fwimisfit value (ADAPTIVE_GAUSS = 2, ADAPTIVE_LINEAR = 3,
+ * ADAPTIVE_SINGLE = 4). */
+int ref_fwi_e2d_misfit_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns,
+                         const double *sc, const float *wav, int sfield, int nr, const double *gc, const float *obsp,
+                         const float *obsx, const float *obsz, int ncheck, float *vpgrad, float *vsgrad,
+                         float *rhograd, float *wavgrad, float *mods, float *ress, double *misfit, int misfit_type)
+{
+    return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
+                          rhograd, wavgrad, mods, ress, misfit, misfit_type);
+}
 int ref_fwi_a2d_f(const ref_grid *g, const float *vp, const float *rho, int ns, const double *sc,
                   const float *wav, int nr, const double *gc, const float *obs, int ncheck,
                   int misfit_type, float *vpgrad, float *rhograd, float *wavgrad, float *datamod,

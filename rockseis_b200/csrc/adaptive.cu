@@ -1,6 +1,6 @@
-// ADAPTIVE_GAUSS / ADAPTIVE_LINEAR misfits and residuals of the acoustic FWI
+// ADAPTIVE_GAUSS / ADAPTIVE_LINEAR / ADAPTIVE_SINGLE misfits and residuals of the FWI
 // drivers (FwiAcoustic2D::computeMisfit / computeResiduals, lib/fwi.cpp:646-751,
-// 851-1026; FwiAcoustic3D, lib/fwi.cpp:1541-1631, 1725-1842).
+// 851-1026; FwiAcoustic3D, lib/fwi.cpp:1541-1631, 1725-1842; FwiElastic2D below).
 //
 // Per trace the reference designs a Wiener shaping filter w that turns the
 // observed trace d into the modelled trace u: with R the (whitened) Toeplitz
@@ -29,6 +29,15 @@
 //     the updates of the prediction filter and of the solution are independent per
 //     index and spread over the warp.
 // One warp per trace; the per-trace arrays live in a work buffer of 5*nt values.
+//
+// The elastic gradient (FwiElastic2D, lib/fwi.cpp:3002-3196, 3428-3753) shapes the
+// Ux and Uz traces the same way, each with its own filter, clips the two together
+// (both lose the samples where |Ux residual| reaches the larger of the two
+// 97th-percentile magnitudes) and counts 0.5 (|Hw_x|^2/|w_x|^2 + |Hw_z|^2/|w_z|^2);
+// ADAPTIVE_SINGLE joins the Ux and Uz traces end to end (2 nt samples), designs one
+// nt-sample filter from the joined traces' correlations, convolves it with the joined
+// observed trace and splits the 2 nt outputs into the Ux and Uz residuals (9*nt work
+// values per trace: the joined traces are copied in).  The P residual is zero.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -45,7 +54,7 @@ enum : unsigned char { FL_DESC = 1, FL_LEAD = 2, FL_ZERO = 4 };
 
 constexpr double STDEV_FRAC = 0.01;      // Gaussian width as a fraction of nt (fwi.h STDEV)
 constexpr double RAMP_MAX = 500;         // ramp clip of ADAPTIVE_LINEAR (fwi.h HMAX)
-constexpr double WHITEN = 0.01;          // prewhitening of the autocorrelation (fwi.h PNOISE_ACOUSTIC)
+constexpr double WHITEN = 0.01;          // prewhitening of the autocorrelation (fwi.h PNOISE_ACOUSTIC and PNOISE_ELASTIC)
 
 // Labels the outputs z[ifz .. ifz+lz-1] of z = x (*) y, x on [ifx, ifx+lx-1] and y on
 // [ify, ify+ly-1] (lx <= ly), by the region of the Seismic Unix convolution loop that
@@ -232,6 +241,115 @@ __global__ void __launch_bounds__(256) adaptive_finish(const Resid2D<T> *desc, c
     misfit[blockIdx.x] = ACC == ACC_REF ? (double)mis : mis64;
 }
 
+// ADAPTIVE_SINGLE, one warp per trace: the Ux and Uz traces joined end to end.
+template <typename T>
+__global__ void __launch_bounds__(128) adaptive_shape_single(const Resid2DE<T> *desc, const unsigned char *tab, int nt)
+{
+    const int lane = threadIdx.x & 31;
+    const Resid2DE<T> d = desc[blockIdx.y];
+    const int tr = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (tr >= d.nrec) return;
+    const T *H = weights<T>(tab);
+    const unsigned char *fx = tab + (size_t)nt * sizeof(T), *fc = fx + nt;
+    const int n2 = 2 * nt;
+    T *r = d.work[0] + (long)tr * 9 * nt, *g = r + nt, *f = g + nt, *a = f + nt, *s1 = a + nt;
+    T *jo = s1 + nt, *jm = jo + n2;            // joined observed and modelled traces
+    const long t0 = (long)tr * nt;
+    for (int i = lane; i < nt; i += 32) {
+        jo[i] = d.obs[1][t0 + i];
+        jo[nt + i] = d.obs[2][t0 + i];
+        jm[i] = d.mod[1][t0 + i];
+        jm[nt + i] = d.mod[2][t0 + i];
+    }
+    __syncwarp();
+    for (int i = lane; i < nt; i += 32) {
+        r[i] = conv_out<T, true>(jo, n2, 1 - n2, jo, n2, 0, i, fx[i]);
+        g[i] = conv_out<T, true>(jo, n2, 1 - n2, jm, n2, 0, i, fx[i]);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        T r0 = r[0];
+        if (r0 == T(0)) r0 = T(1);
+        r[0] = X<T>::rnd(__dmul_rn((double)r0, 1.0 + WHITEN));
+    }
+    __syncwarp();
+    toeplitz_solve(nt, r, g, f, a, lane);
+    T norm = T(0), mis = T(0);
+    if (lane == 0) {
+        for (int it = 0; it < nt; it++) norm = X<T>::add(norm, X<T>::mul(f[it], f[it]));
+        if (norm == T(0)) norm = T(1);
+        for (int it = 0; it < nt; it++) {
+            const double hs = (double)X<T>::mul(H[it], f[it]);
+            mis = X<T>::rnd(__dadd_rn((double)mis, __ddiv_rn(__dmul_rn(__dmul_rn(0.5, hs), hs), (double)norm)));
+        }
+        d.tnorm[0][tr] = norm;
+    }
+    norm = __shfl_sync(0xffffffffu, norm, 0);
+    mis = __shfl_sync(0xffffffffu, mis, 0);
+    for (int i = lane; i < nt; i += 32) {
+        s1[i] = f[i];
+        const double t = __dsub_rn((double)X<T>::mul(H[i], H[i]), __dmul_rn(2.0, (double)mis));
+        g[i] = X<T>::rnd(__ddiv_rn(__dmul_rn(t, (double)f[i]), (double)norm));
+    }
+    __syncwarp();
+    toeplitz_solve(nt, r, g, f, a, lane);
+    for (int i = lane; i < n2; i += 32) {
+        const T v = conv_out<T, false>(f, nt, 0, jo, n2, 0, i, fc[i]);
+        if (i < nt) d.res[1][t0 + i] = v;
+        else d.res[2][t0 + i - nt] = v;
+    }
+}
+
+// One CTA per shot of the elastic gradient: zero P residual, the joint Ux/Uz clip
+// (not for ADAPTIVE_SINGLE), the misfit over the traces whose Ux map is on the grid.
+template <typename T, int ACC, int MODE>
+__global__ void __launch_bounds__(256) adaptive_finish_e2d(const Resid2DE<T> *desc, const unsigned char *tab,
+                                                           double *misfit)
+{
+    const Resid2DE<T> d = desc[blockIdx.x];
+    const int nt = d.nt;
+    const long n = (long)d.nrec * nt;
+    for (long k = threadIdx.x; k < n; k += blockDim.x) d.res[0][k] = T(0);
+    if (MODE != ADAPT_SINGLE) {
+        const long pos = (long)((97ull * (unsigned long long)nt * (unsigned long long)d.nrec) / 100ull);
+        T cx = from_bits<T>(kth_mag_bits(d.res[1], n, pos));
+        const T cz = from_bits<T>(kth_mag_bits(d.res[2], n, pos));
+        if (cz > cx) cx = cz;
+        for (long k = threadIdx.x; k < n; k += blockDim.x)
+            if (fabs(d.res[1][k]) >= cx) {
+                d.res[1][k] = T(0);
+                d.res[2][k] = T(0);
+            }
+    }
+    if (threadIdx.x != 0) return;
+    const T *H = weights<T>(tab);
+    const int stride = (int)(MODE == ADAPT_SINGLE ? 9 : 5);
+    T mis = T(0);
+    double mis64 = 0.0;
+    for (int tr = 0; tr < d.nrec; tr++) {
+        if (d.rec_pt_vx[tr] < 0) continue;
+        const T *wx = d.work[0] + (long)tr * stride * nt + 4L * nt;
+        const T nx = d.tnorm[0][tr];
+        const T *wz = MODE == ADAPT_SINGLE ? wx : d.work[1] + (long)tr * 5 * nt + 4L * nt;
+        const T nz = MODE == ADAPT_SINGLE ? nx : d.tnorm[1][tr];
+        for (int it = 0; it < nt; it++) {
+            // 0.5*(rx*rx/nx + rz*rz/nz) with the sum in the element type (0.5*(rx*rx/nx) for SINGLE)
+            const T rx = X<T>::mul(H[it], wx[it]);
+            T sum = X<T>::div(X<T>::mul(rx, rx), nx);
+            if (MODE != ADAPT_SINGLE) {
+                const T rz = X<T>::mul(H[it], wz[it]);
+                sum = X<T>::add(sum, X<T>::div(X<T>::mul(rz, rz), nz));
+            }
+            const double term = __dmul_rn(0.5, (double)sum);
+            if (ACC == ACC_REF)
+                mis = X<T>::rnd(MODE == ADAPT_GAUSS ? __dsub_rn((double)mis, term) : __dadd_rn((double)mis, term));
+            else
+                mis64 = MODE == ADAPT_GAUSS ? mis64 - term : mis64 + term;
+        }
+    }
+    misfit[blockIdx.x] = ACC == ACC_REF ? (double)mis : mis64;
+}
+
 template <typename T>
 void fill_tables_t(int mode, int nt, unsigned char *tab)
 {
@@ -242,13 +360,18 @@ void fill_tables_t(int mode, int nt, unsigned char *tab)
         for (int it = 0; it < nt; it++)
             H[it] = stdev == T(0) ? T(0) : (T)std::exp(-1.0 * (it * it) / (2.0 * (stdev * stdev)));
     } else {
-        // Fwi::linear(it, stdev) with stdev = HMAX (lib/fwi.cpp:408-417)
+        // Fwi::linear(it, stdev) with stdev = HMAX (lib/fwi.cpp:408-417); also ADAPTIVE_SINGLE
         const T stdev = (T)RAMP_MAX;
         for (int it = 0; it < nt; it++) H[it] = stdev == T(0) ? T(0) : (it < stdev ? (T)it : stdev);
     }
     unsigned char *fx = tab + (size_t)nt * sizeof(T), *fc = fx + nt;
-    conv_flags(nt, 1 - nt, nt, 0, nt, 0, fx);   // xcor(nt, 0, d, nt, 0, y, nt, 0, z): x reversed
-    conv_flags(nt, 0, nt, 0, nt, 0, fc);        // convolve(nt, 0, w, nt, 0, d, nt, 0, z)
+    if (mode == ADAPT_SINGLE) {
+        conv_flags(2 * nt, 1 - 2 * nt, 2 * nt, 0, nt, 0, fx);   // xcor(2nt, 0, d, 2nt, 0, y, nt, 0, z)
+        conv_flags(nt, 0, 2 * nt, 0, 2 * nt, 0, fc);            // convolve(nt, 0, w, 2nt, 0, d, 2nt, 0, z)
+    } else {
+        conv_flags(nt, 1 - nt, nt, 0, nt, 0, fx);   // xcor(nt, 0, d, nt, 0, y, nt, 0, z): x reversed
+        conv_flags(nt, 0, nt, 0, nt, 0, fc);        // convolve(nt, 0, w, nt, 0, d, nt, 0, z)
+    }
 }
 
 template <typename T, int ACC, int MODE>
@@ -273,11 +396,54 @@ void launch_acc(int mode, const void *desc, int nshots, int nrec_max, int nt, co
     else launch_t<T, ACC, ADAPT_LINEAR>(desc, nshots, nrec_max, nt, tables, misfit, st, clip);
 }
 
+template <typename T, int ACC, int MODE>
+void launch_e2d_t(const void *desc, const void *comp, int nshots, int nrec_max, int nt, const void *tables,
+                  double *misfit, cudaStream_t st)
+{
+    const unsigned char *tab = (const unsigned char *)tables;
+    if (MODE == ADAPT_SINGLE) {
+        const dim3 grid((unsigned)((nrec_max + 3) / 4), (unsigned)nshots);
+        adaptive_shape_single<T><<<grid, 128, 0, st>>>((const Resid2DE<T> *)desc, tab, nt);
+    } else {
+        const dim3 grid((unsigned)((nrec_max + 3) / 4), (unsigned)(2 * nshots));
+        adaptive_shape<T, MODE><<<grid, 128, 0, st>>>((const Resid2D<T> *)comp, tab, nt);
+    }
+    adaptive_finish_e2d<T, ACC, MODE><<<nshots, 256, 0, st>>>((const Resid2DE<T> *)desc, tab, misfit);
+}
+
+template <typename T, int ACC>
+void launch_e2d_acc(int mode, const void *desc, const void *comp, int nshots, int nrec_max, int nt, const void *tables,
+                    double *misfit, cudaStream_t st)
+{
+    if (mode == ADAPT_GAUSS) launch_e2d_t<T, ACC, ADAPT_GAUSS>(desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+    else if (mode == ADAPT_LINEAR) launch_e2d_t<T, ACC, ADAPT_LINEAR>(desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+    else launch_e2d_t<T, ACC, ADAPT_SINGLE>(desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+}
+
 }  // namespace
 
-size_t adaptive_table_bytes(int prec, int nt)
+size_t adaptive_table_bytes(int prec, int mode, int nt)
 {
-    return (size_t)nt * (prec == PREC_F64 ? 8 : 4) + 2 * (size_t)nt;
+    return (size_t)nt * (prec == PREC_F64 ? 8 : 4) + (size_t)nt + (size_t)(mode == ADAPT_SINGLE ? 2 : 1) * nt;
+}
+
+size_t adaptive_work_values(int mode, int nt)
+{
+    return (size_t)(mode == ADAPT_SINGLE ? 9 : 5) * nt;
+}
+
+cudaError_t launch_residual_adaptive_e2d(int prec, int acc, int mode, const void *desc, const void *comp, int nshots,
+                                         int nrec_max, int nt, const void *tables, double *misfit, cudaStream_t st)
+{
+    if (mode != ADAPT_GAUSS && mode != ADAPT_LINEAR && mode != ADAPT_SINGLE) return cudaErrorInvalidValue;
+    if (prec == PREC_F64) {
+        if (acc == ACC_F64) launch_e2d_acc<double, ACC_F64>(mode, desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+        else launch_e2d_acc<double, ACC_REF>(mode, desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+    } else {
+        if (acc == ACC_F64) launch_e2d_acc<float, ACC_F64>(mode, desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+        else launch_e2d_acc<float, ACC_REF>(mode, desc, comp, nshots, nrec_max, nt, tables, misfit, st);
+    }
+    return cudaGetLastError();
 }
 
 void adaptive_fill_tables(int prec, int mode, int nt, void *host_tables)

@@ -80,6 +80,9 @@ public:
     std::vector<size_t> o_ilum;      // acoustic FWI source illumination (0 = not asked for)
     size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
     std::vector<size_t> o_work, o_tnorm;   // ADAPTIVE misfits: per-trace scratch and filter norms
+    std::vector<size_t> o_work2, o_tnorm2; // elastic ADAPTIVE_GAUSS / _LINEAR: the Uz filters
+    size_t o_comp = 0;                      // elastic ADAPTIVE_GAUSS / _LINEAR: Ux and Uz views per shot
+    std::vector<unsigned char> comp;        // host copy of those views until the upload completes
     size_t o_atab = 0;                      // ADAPTIVE misfits: weights and summation-order tables
     std::vector<int> nx, nz, nrec, nsrc;
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
@@ -132,10 +135,9 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_UNSUPPORTED;
     }
     const bool el = c->physics == RSGPU_ELASTIC2D;
-    const bool adaptive = o->misfit == RSGPU_MISFIT_ADAPTIVE_GAUSS || o->misfit == RSGPU_MISFIT_ADAPTIVE_LINEAR;
-    if (o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION && !(adaptive && !el)) {
-        set_error("misfit %d: DIFFERENCE and CORRELATION are built%s", o->misfit,
-                  el ? "" : ", and ADAPTIVE_GAUSS / ADAPTIVE_LINEAR for the acoustic gradient");
+    if (o->misfit < RSGPU_MISFIT_DIFFERENCE || o->misfit > RSGPU_MISFIT_ADAPTIVE_SINGLE) {
+        set_error("misfit %d: DIFFERENCE, CORRELATION, ADAPTIVE_GAUSS, ADAPTIVE_LINEAR and ADAPTIVE_SINGLE are built",
+                  o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (o->misfit == RSGPU_MISFIT_CORRELATION && kind == RSGPU_KIND_FWI) {
@@ -202,7 +204,10 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     prec = c->precision;
     es = esize(prec);
     acc = o->accum == RSGPU_ACCUM_F64 ? ACC_F64 : ACC_REF;
-    misfit_type = o->misfit;
+    // FwiAcoustic2D has no ADAPTIVE_SINGLE case: its misfit and residual switches fall
+    // through to the DIFFERENCE code (lib/fwi.cpp:737-749, 1015-1026)
+    misfit_type = c->physics != RSGPU_ELASTIC2D && o->misfit == RSGPU_MISFIT_ADAPTIVE_SINGLE ? RSGPU_MISFIT_DIFFERENCE
+                                                                                              : o->misfit;
     for (int i = 0; i < ns; i++) nrec_max = std::max(nrec_max, s[i].shot.nrec);
     ck = o->ckpt_precision;
     ck_es = ck == CK_NATIVE ? (size_t)es : 2;
@@ -311,15 +316,21 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     }
     o_misfit = take(sizeof(double) * ns);
     const bool adaptive = kind == RSGPU_KIND_FWI && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
-                                                     misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR);
-    o_work.assign(ns, 0);
-    o_tnorm.assign(ns, 0);
+                                                     misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR ||
+                                                     misfit_type == RSGPU_MISFIT_ADAPTIVE_SINGLE);
+    const bool two_filters = adaptive && elastic() && misfit_type != RSGPU_MISFIT_ADAPTIVE_SINGLE;
+    for (auto *v : {&o_work, &o_tnorm, &o_work2, &o_tnorm2}) v->assign(ns, 0);
     if (adaptive) {
         for (int i = 0; i < ns; i++) {
-            o_work[i] = take((size_t)5 * nrec[i] * cfg.nt * es);
+            o_work[i] = take(adaptive_work_values(misfit_type, cfg.nt) * nrec[i] * es);
             o_tnorm[i] = take((size_t)nrec[i] * es);
+            if (two_filters) {
+                o_work2[i] = take(adaptive_work_values(misfit_type, cfg.nt) * nrec[i] * es);
+                o_tnorm2[i] = take((size_t)nrec[i] * es);
+            }
         }
-        o_atab = take(adaptive_table_bytes(prec, cfg.nt));
+        o_atab = take(adaptive_table_bytes(prec, misfit_type, cfg.nt));
+        if (two_filters) o_comp = take(2 * ns * (prec == PREC_F64 ? sizeof(Resid2D<double>) : sizeof(Resid2D<float>)));
     }
     const size_t corr_bytes = elastic() ? (prec == PREC_F64 ? sizeof(Corr2DE<double>) : sizeof(Corr2DE<float>))
                                         : (prec == PREC_F64 ? sizeof(Corr2D<double>) : sizeof(Corr2D<float>));
@@ -382,11 +393,12 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
     std::vector<unsigned char> atab;
     if (adaptive) {
-        atab.resize(adaptive_table_bytes(prec, cfg.nt));
+        atab.resize(adaptive_table_bytes(prec, misfit_type, cfg.nt));
         adaptive_fill_tables(prec, misfit_type, cfg.nt, atab.data());
         CU(cudaMemcpyAsync(D(o_atab), atab.data(), atab.size(), cudaMemcpyHostToDevice, stream));
     }
     std::vector<unsigned char> corr(corr_bytes * ns), res(res_bytes * ns);
+    comp.clear();
     if (elastic()) {
         if (prec == PREC_F64) build_desc_e2d<double>(corr, res);
         else build_desc_e2d<float>(corr, res);
@@ -396,6 +408,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     }
     CU(cudaMemcpyAsync(D(o_corr), corr.data(), corr.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(D(o_res), res.data(), res.size(), cudaMemcpyHostToDevice, stream));
+    if (o_comp) CU(cudaMemcpyAsync(D(o_comp), comp.data(), comp.size(), cudaMemcpyHostToDevice, stream));
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -471,7 +484,29 @@ void Adjoint::build_desc_e2d(std::vector<unsigned char> &corr, std::vector<unsig
         r.rec_pt_vx = (const int *)(fa + fw->rec_pt_offsets[(size_t)i * MAXSETS + 1]);
         r.nrec = nrec[i];
         r.nt = cfg.nt;
+        if (o_work[i]) {
+            r.work[0] = (T *)D(o_work[i]);
+            r.tnorm[0] = (T *)D(o_tnorm[i]);
+            r.work[1] = o_work2[i] ? (T *)D(o_work2[i]) : nullptr;
+            r.tnorm[1] = o_tnorm2[i] ? (T *)D(o_tnorm2[i]) : nullptr;
+        }
         std::memcpy(res.data() + i * sizeof r, &r, sizeof r);
+        if (o_comp) {
+            // the Ux and Uz traces as two single-component views, shaped like acoustic traces
+            comp.resize(2 * nshots * sizeof(Resid2D<T>));
+            for (int k = 0; k < 2; k++) {
+                Resid2D<T> v{};
+                v.mod = r.mod[1 + k];
+                v.obs = r.obs[1 + k];
+                v.res = r.res[1 + k];
+                v.rec_pt = r.rec_pt_vx;
+                v.nrec = nrec[i];
+                v.nt = cfg.nt;
+                v.work = r.work[k];
+                v.tnorm = r.tnorm[k];
+                std::memcpy(comp.data() + (2 * i + k) * sizeof v, &v, sizeof v);
+            }
+        }
     }
 }
 
@@ -534,8 +569,11 @@ rsgpu_status Adjoint::residuals()
 {
     const bool corr = misfit_type == RSGPU_MISFIT_CORRELATION;
     if (o_atab) {
-        cudaError_t e = launch_residual_adaptive(prec, acc, misfit_type, D(o_res), nshots, nrec_max, cfg.nt, D(o_atab),
-                                                 (double *)D(o_misfit), stream, true);
+        cudaError_t e = elastic() ? launch_residual_adaptive_e2d(prec, acc, misfit_type, D(o_res),
+                                                                 o_comp ? D(o_comp) : nullptr, nshots, nrec_max, cfg.nt,
+                                                                 D(o_atab), (double *)D(o_misfit), stream)
+                                  : launch_residual_adaptive(prec, acc, misfit_type, D(o_res), nshots, nrec_max, cfg.nt,
+                                                             D(o_atab), (double *)D(o_misfit), stream, true);
         if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
         launches += 2;
         return RSGPU_OK;

@@ -75,9 +75,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         set_error("elastic 3D: misfit %d: DIFFERENCE is built", o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
-    if (k_ == RSGPU_KIND_FWI && o->misfit != RSGPU_MISFIT_DIFFERENCE && o->misfit != RSGPU_MISFIT_CORRELATION &&
-        o->misfit != RSGPU_MISFIT_ADAPTIVE_GAUSS && o->misfit != RSGPU_MISFIT_ADAPTIVE_LINEAR) {
-        set_error("misfit %d: DIFFERENCE, CORRELATION, ADAPTIVE_GAUSS and ADAPTIVE_LINEAR are built", o->misfit);
+    if (k_ == RSGPU_KIND_FWI && (o->misfit < RSGPU_MISFIT_DIFFERENCE || o->misfit > RSGPU_MISFIT_ADAPTIVE_SINGLE)) {
+        set_error("misfit %d: DIFFERENCE, CORRELATION, ADAPTIVE_GAUSS, ADAPTIVE_LINEAR and ADAPTIVE_SINGLE are built",
+                  o->misfit);
         return RSGPU_ERR_UNSUPPORTED;
     }
     if (k_ == RSGPU_KIND_FWI && o->misfit == RSGPU_MISFIT_CORRELATION) {
@@ -88,7 +88,9 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
                 return RSGPU_ERR_UNSUPPORTED;
             }
     }
-    misfit_type = o->misfit;
+    // FwiAcoustic3D has no ADAPTIVE_SINGLE case: its switches fall through to the
+    // DIFFERENCE code (lib/fwi.cpp:1631-1644, 1841-1852)
+    misfit_type = o->misfit == RSGPU_MISFIT_ADAPTIVE_SINGLE ? RSGPU_MISFIT_DIFFERENCE : o->misfit;
     for (int i = 0; i < ns; i++) nrec_max = std::max(nrec_max, s[i].shot.nrec);
     if (o->ckpt_precision < RSGPU_CKPT_NATIVE || o->ckpt_precision > RSGPU_CKPT_BF16) {
         set_error("bad checkpoint precision %d", o->ckpt_precision);
@@ -251,10 +253,10 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     o_tnorm.assign(ns, 0);
     if (adaptive) {
         for (int i = 0; i < ns; i++) {
-            o_work[i] = take((size_t)5 * nrec[i] * cfg.nt * es);
+            o_work[i] = take(adaptive_work_values(misfit_type, cfg.nt) * nrec[i] * es);
             o_tnorm[i] = take((size_t)nrec[i] * es);
         }
-        o_atab = take(adaptive_table_bytes(prec, cfg.nt));
+        o_atab = take(adaptive_table_bytes(prec, misfit_type, cfg.nt));
     }
     segs.clear();
     slot_elems = 0;
@@ -295,7 +297,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     CU(cudaMemcpyAsync(D(o_segs), segs.data(), sizeof(CkptSeg) * segs.size(), cudaMemcpyHostToDevice, stream));
     std::vector<unsigned char> atab;
     if (adaptive) {
-        atab.resize(adaptive_table_bytes(prec, cfg.nt));
+        atab.resize(adaptive_table_bytes(prec, misfit_type, cfg.nt));
         adaptive_fill_tables(prec, misfit_type, cfg.nt, atab.data());
         CU(cudaMemcpyAsync(D(o_atab), atab.data(), atab.size(), cudaMemcpyHostToDevice, stream));
     }

@@ -38,6 +38,8 @@ struct Resid2DE {
     T *res[3];
     const int *rec_pt_vx;       // validity of a trace for the misfit: the Ux set's map
     int nrec, nt;
+    T *work[2];                 // ADAPTIVE misfits: per-trace scratch of the Ux and Uz filters
+    T *tnorm[2];                // ADAPTIVE misfits: the filters' squared norms per trace
 };
 
 // 3D image correlation inputs of one shot (RtmAcoustic3D::crossCorr).
@@ -124,11 +126,20 @@ cudaError_t launch_residual_corr(int prec, int acc, const void *desc, int nshots
 // their residuals, with the 97th-percentile clip of the 2D drivers when `clip`.
 // `tables` holds adaptive_table_bytes(prec, nt) bytes filled by
 // adaptive_fill_tables; every Resid2D carries its work and tnorm arrays.
-enum { ADAPT_GAUSS = 2, ADAPT_LINEAR = 3 };
-size_t adaptive_table_bytes(int prec, int nt);
+enum { ADAPT_GAUSS = 2, ADAPT_LINEAR = 3, ADAPT_SINGLE = 4 };
+size_t adaptive_table_bytes(int prec, int mode, int nt);
 void adaptive_fill_tables(int prec, int mode, int nt, void *host_tables);
+// Per-trace scratch values of one filter (work) for a mode.
+size_t adaptive_work_values(int mode, int nt);
 cudaError_t launch_residual_adaptive(int prec, int acc, int mode, const void *desc, int nshots, int nrec_max, int nt,
                                      const void *tables, double *misfit, cudaStream_t st, bool clip);
+// FwiElastic2D (lib/fwi.cpp:3002-3196, 3428-3753): ADAPTIVE_GAUSS / ADAPTIVE_LINEAR
+// shape the Ux and Uz traces separately (`comp`: two Resid2D per shot, Ux then Uz,
+// pointing into the Resid2DE arrays) and clip them together; ADAPTIVE_SINGLE shapes
+// the Ux and Uz traces joined end to end with one filter, without a clip.  The P
+// residual is zero.
+cudaError_t launch_residual_adaptive_e2d(int prec, int acc, int mode, const void *desc, const void *comp, int nshots,
+                                         int nrec_max, int nt, const void *tables, double *misfit, cudaStream_t st);
 // The elastic CORRELATION misfit and residuals (P, Ux, Uz) with the reference's clips.
 cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int nshots, int nrec_max, double *misfit,
                                      cudaStream_t st);

@@ -379,7 +379,8 @@ def adaptive_reference(c, misfit, ncheck=7, dims="a2d"):
     g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "adaptive.npz"))
     assert ncheck == 7 and np.array_equal(c.obs.astype(np.float32), g[f"{dims}_obs"])
     name = {abi.MISFIT_ADAPTIVE_GAUSS: "gauss", abi.MISFIT_ADAPTIVE_LINEAR: "linear"}[misfit]
-    out = {k: g[f"{dims}_{name}_{k}"] for k in ("vpgrad", "rhograd", "wavgrad", "datamod", "datares")}
+    out = {k: g[f"{dims}_{name}_{k}"] for k in ("vpgrad", "rhograd", "wavgrad", "datares")}
+    out["datamod"] = g[f"{dims}_datamod"]
     out["misfit"] = float(g[f"{dims}_{name}_misfit"])
     return out
 

@@ -104,3 +104,40 @@ def test_elastic_fwi_correlation_misfit_exact_bitwise(require_gpu, ncheck):
     assert_same(got, ref)
     assert got["misfit"] < 0
     assert (ref["datares"][0] == 0).mean() >= 0.03 and (ref["datares"][1] == 0).any()
+
+
+# ---------------------------------------------------------------- ADAPTIVE misfits (FwiElastic2D)
+def adaptive_reference(c, misfit, ncheck=7):
+    """FwiElastic2D::run_optimal with an ADAPTIVE misfit: the reference library where
+    oracle/_ref is built, else the committed outputs (tests/golden/make_golden_adaptive.py)."""
+    import os
+    from oracle import api
+    obs3 = [o.astype(np.float32) for o in c.obs]
+    if api.ref_available():
+        return api.ref_fwi_e2d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.sfield, c.recs[0].gcoords, obs3,
+                               ncheck, misfit=misfit)
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "adaptive.npz"))
+    assert ncheck == 7 and np.array_equal(np.stack(obs3), g["e2d_obs"])
+    name = {2: "gauss", 3: "linear", 4: "single"}[misfit]
+    out = {k: g[f"e2d_{name}_{k}"] for k in ("vpgrad", "vsgrad", "rhograd", "wavgrad", "datares")}
+    out["datamod"] = g["e2d_datamod"]
+    out["misfit"] = float(g[f"e2d_{name}_misfit"])
+    return out
+
+
+@pytest.mark.parametrize("misfit", [abi.MISFIT_ADAPTIVE_GAUSS, abi.MISFIT_ADAPTIVE_LINEAR,
+                                    abi.MISFIT_ADAPTIVE_SINGLE])
+def test_elastic_fwi_adaptive_misfit_bitwise(require_gpu, misfit):
+    # Ux and Uz shaped separately and clipped together (GAUSS, LINEAR) or joined end to
+    # end under one filter (SINGLE); the P residual is zero
+    c = ElasticFwiCase()
+    ref = adaptive_reference(c, misfit)
+    f = make_job(c, ncheck=7)
+    f.setMisfit_type(misfit)
+    assert f.run_optimal() == 1
+    got = outputs(f)
+    for k in ("vpgrad", "vsgrad", "rhograd", "wavgrad", "datamod", "datares"):
+        assert np.abs(ref[k]).max() > 0, k
+        assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
+    assert got["misfit"] == ref["misfit"]
+    assert not np.any(got["datares"][0])
