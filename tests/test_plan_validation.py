@@ -68,7 +68,7 @@ def test_gradient_driver_option_checks():
     cfg = make_config(c.model, c.order, c.nt, c.dt, abi.F32_EXACT)
     a = abi.AdjointShot()
     a.shot = make_shot(c.model, c.src, c.rec, keep)
-    for field, value, status in (("misfit", 4, abi.ERR_UNSUPPORTED), ("ckpt_precision", 9, abi.ERR_ARG),
+    for field, value, status in (("misfit", 7, abi.ERR_UNSUPPORTED), ("ckpt_precision", 9, abi.ERR_ARG),
                                  ("accum", 5, abi.ERR_ARG), ("snapmethod", 7, abi.ERR_ARG)):
         o = abi.AdjointOpts()
         o.ncheck, o.nhx, o.nhz, o.nhy = 5, 1, 1, 1
