@@ -221,12 +221,15 @@ typedef struct {
     int snapmethod;      /* RSGPU_SNAP_OPTIMAL: Revolve checkpointing (run_optimal);
                             RSGPU_SNAP_FULL: the forward pressure saved every snapinc steps and
                             correlated at those steps only (FwiAcoustic2D::run, lib/fwi.cpp:1030-1156;
-                            RtmAcoustic2D::run, lib/rtm.cpp:222-326); acoustic 2D */
+                            RtmAcoustic2D::run, lib/rtm.cpp:222-326); acoustic 2D;
+                            RSGPU_SNAP_EDGES: RtmAcoustic2D::run_edge (lib/rtm.cpp:328-421), the
+                            RTM image from the wavefield's four edge lines saved every snapinc
+                            steps, the source wavefield re-propagated from them */
     int snapinc;         /* FULL: snapshot increment (Fwi/Rtm snapinc; < 1 means 1) */
     int noreverse;       /* FULL FWI: forward run and misfit only (Fwi::setNoreverse) */
     int reserved[6];
 } rsgpu_adjoint_opts;
-enum { RSGPU_SNAP_OPTIMAL = 0, RSGPU_SNAP_FULL = 1 };
+enum { RSGPU_SNAP_OPTIMAL = 0, RSGPU_SNAP_FULL = 1, RSGPU_SNAP_EDGES = 2 };
 
 /* One shot of FwiAcoustic2D::run_optimal (lib/fwi.cpp:1159-1332),
  * RtmAcoustic2D::run_optimal (lib/rtm.cpp:423-545), FwiElastic2D::run_optimal

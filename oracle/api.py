@@ -108,6 +108,7 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
     lib.ref_fwi_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I] + [V] * 5 + [V]
     lib.ref_rtm_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
+    lib.ref_rtm_a2d_edge_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
     lib.ref_localsize2d_f.argtypes = [G, I, V, V, D, I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     lib.ref_localsize3d_f.argtypes = [G, I, V, V, D, D, I, V]
     lib.ref_fwi_e3d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
@@ -116,6 +117,7 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_a3d_misfit_f.argtypes = [G, V, V, I, V, V, I, V, V, I] + [V] * 5 + [V, I]
     lib.ref_interp_f.argtypes = [I, I, I, C.c_float, C.c_float, V, I, C.c_float, C.c_float, V]
     lib.ref_rtm_a3d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
+    lib.ref_rtm_a3d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, I, V]
     lib.ref_rtm_a2d_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
     lib.ref_stagger_a2d_f.argtypes = [G, V, V, V, V, V]
     lib.ref_stagger_e2d_f.argtypes = [G, V, V, V, V, V, V, V, V]
@@ -255,14 +257,14 @@ def ref_fwi_a2d_full(pb, scoords, wav, gcoords, obs, snapinc, noreverse=0, misfi
     return out
 
 
-def ref_rtm_a2d_full(pb, scoords, wav, gcoords, data, snapinc, nhx=1, nhz=1):
-    """RtmAcoustic2D::run, the full-snapshot image."""
+def ref_rtm_a2d_full(pb, scoords, wav, gcoords, data, snapinc, nhx=1, nhz=1, edges=False):
+    """RtmAcoustic2D::run, the full-snapshot image (edges: RtmAcoustic2D::run_edge)."""
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     img = np.zeros((nhz, nhx, pb.nz, pb.nx), np.float32)
     vp, rho, w, d = _keep(pb.vp, pb.rho, wav, data, dtype=np.float32)
-    r = ref().ref_rtm_a2d_full_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d),
-                                 snapinc, nhx, nhz, _p(img))
+    fn = ref().ref_rtm_a2d_edge_f if edges else ref().ref_rtm_a2d_full_f
+    r = fn(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d), snapinc, nhx, nhz, _p(img))
     assert r == 1
     return img
 
@@ -490,13 +492,14 @@ def orc_fwi_e2d(pb, padded, tab, smap, sshift, wav, sfield, gmaps, gshifts, obs3
     return out
 
 
-def ref_rtm_a3d(pb, scoords, wav, gcoords, data, ncheck, nhx=1, nhy=1, nhz=1):
+def ref_rtm_a3d(pb, scoords, wav, gcoords, data, ncheck, nhx=1, nhy=1, nhz=1, full_snapinc=0):
+    """RtmAcoustic3D::run_optimal, or RtmAcoustic3D::run with snapshots every full_snapinc steps."""
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     img = np.zeros((nhz, nhy, nhx, pb.nz, pb.ny, pb.nx), np.float32)
     vp, rho, w, d = _keep(pb.vp, pb.rho, wav, data, dtype=np.float32)
-    r = ref().ref_rtm_a3d_f(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d), ncheck,
-                            nhx, nhy, nhz, _p(img))
+    fn, n = (ref().ref_rtm_a3d_full_f, full_snapinc) if full_snapinc > 0 else (ref().ref_rtm_a3d_f, ncheck)
+    r = fn(C.byref(g), _p(vp), _p(rho), len(sc), _p(sc), _p(w), len(gc), _p(gc), _p(d), n, nhx, nhy, nhz, _p(img))
     assert r == 1
     return img
 

@@ -50,7 +50,7 @@ class Shot(C.Structure):
                 ("rec_field", C.c_int), ("rec_factor", C.c_void_p), ("rec_out", C.c_void_p)]
 
 
-SNAP_OPTIMAL, SNAP_FULL = 0, 1
+SNAP_OPTIMAL, SNAP_FULL, SNAP_EDGES = 0, 1, 2
 
 
 class AdjointOpts(C.Structure):

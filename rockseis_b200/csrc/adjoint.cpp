@@ -83,6 +83,7 @@ public:
     std::vector<size_t> o_work2, o_tnorm2; // elastic ADAPTIVE_GAUSS / _LINEAR: the Uz filters
     size_t o_comp = 0;                      // elastic ADAPTIVE_GAUSS / _LINEAR: Ux and Uz views per shot
     std::vector<unsigned char> comp;        // host copy of those views until the upload completes
+    std::vector<size_t> o_wav0;             // EDGES: the forward plan's source traces, kept aside
     size_t o_atab = 0;                      // ADAPTIVE misfits: weights and summation-order tables
     std::vector<int> nx, nz, nrec, nsrc;
     long long fw_steps = 0, bw_steps = 0, ckpt_bytes = 0, launches = 0;
@@ -110,19 +111,6 @@ Adjoint::~Adjoint()
     dev_free(dbuf, stream);
     dev_free(ckpt, stream);
     if (stream) cudaStreamDestroy(stream);
-}
-
-// Snapshot2D's enddiff (lib/snap.cpp:334-337), evaluated in the element type:
-// the adjoint time of the last snapshot minus that of the last forward step.
-static int snap_enddiff(int nt, double dt_cfg, int snapinc, int prec)
-{
-    const int snapnt = (nt - 1) / snapinc + 1;
-    if (prec == PREC_F64) {
-        const double dt = dt_cfg, snapdt = dt * snapinc;
-        return (int)rintf((float)(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt));
-    }
-    const float dt = (float)dt_cfg, snapdt = dt * snapinc;
-    return (int)rintf(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt);
 }
 
 static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opts *o, int kind, int ns,
@@ -153,11 +141,15 @@ static rsgpu_status check_adjoint(const rsgpu_config *c, const rsgpu_adjoint_opt
         return RSGPU_ERR_ARG;
     }
     if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
-    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && o->snapmethod != RSGPU_SNAP_FULL) {
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && o->snapmethod != RSGPU_SNAP_FULL && o->snapmethod != RSGPU_SNAP_EDGES) {
         set_error("bad snapmethod %d", o->snapmethod);
         return RSGPU_ERR_ARG;
     }
-    if (o->snapmethod == RSGPU_SNAP_FULL && el) {
+    if (o->snapmethod == RSGPU_SNAP_EDGES && kind != RSGPU_KIND_RTM) {
+        set_error("EDGES snapshots belong to the acoustic 2D RTM image (RtmAcoustic2D::run_edge)");
+        return RSGPU_ERR_UNSUPPORTED;
+    }
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && el) {
         set_error("FULL snapshots are built for the acoustic 2D gradient and image (FwiAcoustic2D::run, RtmAcoustic2D::run)");
         return RSGPU_ERR_UNSUPPORTED;
     }
@@ -214,7 +206,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     nhx = kind == RSGPU_KIND_RTM ? o->nhx : 1;
     nhz = kind == RSGPU_KIND_RTM ? o->nhz : 1;
     snapmethod = o->snapmethod;
-    if (snapmethod == RSGPU_SNAP_FULL) {
+    if (snapmethod != RSGPU_SNAP_OPTIMAL) {
         snapinc = std::max(o->snapinc, 1);
         snapnt = (c->nt - 1) / snapinc + 1;
         enddiff = snap_enddiff(c->nt, c->dt, snapinc, prec);
@@ -318,6 +310,9 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     const bool adaptive = kind == RSGPU_KIND_FWI && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
                                                      misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR ||
                                                      misfit_type == RSGPU_MISFIT_ADAPTIVE_SINGLE);
+    o_wav0.assign(ns, 0);
+    for (int i = 0; i < ns && snapmethod == RSGPU_SNAP_EDGES; i++)
+        o_wav0[i] = take((size_t)fw->shots[i].nsrcs[0] * cfg.nt * es);
     const bool two_filters = adaptive && elastic() && misfit_type != RSGPU_MISFIT_ADAPTIVE_SINGLE;
     for (auto *v : {&o_work, &o_tnorm, &o_work2, &o_tnorm2}) v->assign(ns, 0);
     if (adaptive) {
@@ -342,7 +337,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
     // and the C-PML memory strips
     segs.clear();
     slot_elems = 0;
-    nslots = snapmethod == RSGPU_SNAP_FULL ? snapnt : ncheck;
+    nslots = snapmethod != RSGPU_SNAP_OPTIMAL ? snapnt : ncheck;
     for (int i = 0; i < ns; i++) {
         const ShotLayout &L = fw->shots[i];
         const size_t org = ((size_t)GUARD * L.pitch + GUARD) * es;
@@ -358,6 +353,17 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         if (snapmethod == RSGPU_SNAP_FULL) {
             // Snapshot2D::writeSnap: the nx*nz interior of P (lib/snap.cpp:638-667)
             add(L.f[A2_P] + org + ((size_t)cfg.lpml * L.pitch + cfg.lpml) * es, nz[i], nx[i], L.pitch);
+            continue;
+        }
+        if (snapmethod == RSGPU_SNAP_EDGES) {
+            // Snapshot2D::writeEdge (lib/snap.cpp:690-733): P on the columns x = lpml and
+            // x = nx+lpml (the first C-PML column) over the interior rows, and on the rows
+            // z = lpml and z = nz+lpml over the interior columns
+            const size_t p0 = L.f[A2_P] + org, l = (size_t)cfg.lpml;
+            add(p0 + (l * L.pitch + l) * es, nz[i], 1, L.pitch);
+            add(p0 + (l * L.pitch + nx[i] + l) * es, nz[i], 1, L.pitch);
+            add(p0 + (l * L.pitch + l) * es, 1, nx[i], L.pitch);
+            add(p0 + ((nz[i] + l) * L.pitch + l) * es, 1, nx[i], L.pitch);
             continue;
         }
         for (int f = 0; f < nfields(phys); f++) add(L.f[f] + org, L.nzp, L.nxp, L.pitch);
@@ -379,6 +385,10 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         return RSGPU_ERR_NOMEM;
     }
     CU(cudaMemsetAsync(dbuf, 0, off, stream));
+    for (int i = 0; i < ns; i++)
+        if (o_wav0[i])
+            CU(cudaMemcpyAsync(D(o_wav0[i]), (char *)fw->arena + fw->shots[i].wavk[0],
+                               (size_t)fw->shots[i].nsrcs[0] * cfg.nt * es, cudaMemcpyDeviceToDevice, stream));
     for (int i = 0; i < ns && kind == RSGPU_KIND_FWI; i++) {
         const size_t n2 = (size_t)nx[i] * nz[i];
         CU(cudaMemcpyAsync(D(o_vp[i]), s[i].vp, n2 * es, cudaMemcpyHostToDevice, stream));
@@ -594,12 +604,21 @@ rsgpu_status Adjoint::residuals()
 // adjoint wavefield from a zero state and, at the adjoint times t with
 // (t - enddiff) % snapinc == 0, correlates it with snapshot (t - enddiff)/snapinc
 // (Snapshot2D::readSnap counts the snapshots down from the last one written).
+// RtmAcoustic2D::run_edge (lib/rtm.cpp:328-421) saves only P's four edge lines;
+// its adjoint loop also steps the forward wavefield again from a zero state,
+// without the source (the plan's source traces are zeroed for that pass: adding
+// zero leaves every value as it is), and writes the saved edge lines into it at
+// those adjoint times before correlating.
 // Steps between two saves or two correlations go to the plans as one range.
 rsgpu_status Adjoint::run_full()
 {
     const int nt = cfg.nt;
+    const bool edges = snapmethod == RSGPU_SNAP_EDGES;
     const long long l0 = fw->launches + bw->launches;
     ST(reset_outputs());
+    for (int i = 0; i < nshots && edges; i++)
+        CU(cudaMemcpyAsync((char *)fw->arena + fw->shots[i].wavk[0], D(o_wav0[i]),
+                           (size_t)fw->shots[i].nsrcs[0] * cfg.nt * es, cudaMemcpyDeviceToDevice, stream));
     ST(fw->set_recording(true));
     ST(fw->run(0, 1));
     ST(save(0));
@@ -612,6 +631,12 @@ rsgpu_status Adjoint::run_full()
     fw_steps = nt;
     ST(fw->set_recording(false));
     if (kind == RSGPU_KIND_FWI) ST(residuals());
+    if (edges) {
+        ST(fw->reset());
+        for (int i = 0; i < nshots; i++)
+            CU(cudaMemsetAsync((char *)fw->arena + fw->shots[i].wavk[0], 0,
+                               (size_t)fw->shots[i].nsrcs[0] * cfg.nt * es, stream));
+    }
     if (!noreverse) {
         // adjoint step index k runs data time t = nt-1-k
         auto aligned = [&](int k) { return ((nt - 1 - k) - enddiff) % snapinc == 0; };
@@ -619,6 +644,10 @@ rsgpu_status Adjoint::run_full()
             int e = k;
             while (e < nt && !aligned(e)) e++;
             const int n = (e < nt ? e + 1 : nt) - k;
+            if (edges) {
+                ST(fw->run(k, n));
+                fw_steps += n;
+            }
             ST(bw->run(k, n));
             bw_steps += n;
             k += n;
@@ -638,7 +667,7 @@ rsgpu_status Adjoint::run_full()
 
 rsgpu_status Adjoint::run()
 {
-    if (snapmethod == RSGPU_SNAP_FULL) return run_full();
+    if (snapmethod != RSGPU_SNAP_OPTIMAL) return run_full();
     const int nt = cfg.nt;
     const long long l0 = fw->launches + bw->launches;
     ST(reset_outputs());

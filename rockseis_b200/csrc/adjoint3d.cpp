@@ -97,9 +97,18 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         return RSGPU_ERR_ARG;
     }
     if (o->accum != RSGPU_ACCUM_REFERENCE && o->accum != RSGPU_ACCUM_F64) { set_error("bad accumulation %d", o->accum); return RSGPU_ERR_ARG; }
-    if (o->snapmethod != RSGPU_SNAP_OPTIMAL) {
-        set_error("snapmethod %d: the 3D drivers are built with Revolve checkpointing (run_optimal)", o->snapmethod);
-        return o->snapmethod == RSGPU_SNAP_FULL ? RSGPU_ERR_UNSUPPORTED : RSGPU_ERR_ARG;
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && o->snapmethod != RSGPU_SNAP_FULL && o->snapmethod != RSGPU_SNAP_EDGES) {
+        set_error("bad snapmethod %d", o->snapmethod);
+        return RSGPU_ERR_ARG;
+    }
+    // FULL snapshots: RtmAcoustic3D::run.  FwiAcoustic3D::run correlates against its
+    // unpadded snapshot with crossCorr's index range 1..n-1, which at the last interior
+    // corner reads one element past the snapshot array (lib/fwi.cpp:1441-1459 with
+    // Snapshot3D, lib/snap.cpp:1138-1195): not reproducible, so not offered.
+    if (o->snapmethod != RSGPU_SNAP_OPTIMAL && (el || k_ != RSGPU_KIND_RTM || o->snapmethod == RSGPU_SNAP_EDGES)) {
+        set_error("snapmethod %d: the 3D drivers offer FULL snapshots for the acoustic RTM image (RtmAcoustic3D::run) "
+                  "and Revolve checkpointing otherwise", o->snapmethod);
+        return RSGPU_ERR_UNSUPPORTED;
     }
     const int hy = o->nhy > 0 ? o->nhy : 1;
     if (k_ == RSGPU_KIND_RTM && (o->nhx < 1 || o->nhz < 1 || o->nhx % 2 == 0 || hy % 2 == 0 || o->nhz % 2 == 0)) {
@@ -147,9 +156,16 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     nhx = fwi() ? 1 : o->nhx;
     nhy = fwi() ? 1 : hy;
     nhz = fwi() ? 1 : o->nhz;
-    {
+    snapmethod = o->snapmethod;
+    if (snapmethod == RSGPU_SNAP_FULL) {
+        snapinc = std::max(o->snapinc, 1);
+        snapnt = (c->nt - 1) / snapinc + 1;
+        enddiff = snap_enddiff(c->nt, c->dt, snapinc, prec);
+        nslots = snapnt;
+    } else {
         RevolveSchedule probe(c->nt, o->ncheck);
         ncheck = probe.snaps();
+        nslots = ncheck;
     }
     CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
@@ -271,6 +287,13 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
             segs.push_back(g);
         };
         const int l2 = 2 * cfg.lpml;
+        if (snapmethod == RSGPU_SNAP_FULL) {
+            // Snapshot3D::writeSnap: the nx*ny*nz interior of P (lib/snap.cpp:1138-1172)
+            const size_t l = (size_t)cfg.lpml;
+            add(L.f[A3_P] + fw->origin_bytes(L) + (l * L.plane + l * L.pitch + l) * es, ny[i] * nz[i], nx[i], L.pitch,
+                ny[i], L.plane);
+            continue;
+        }
         for (int f = 0; f < fw->nf3(); f++)
             add(L.f[f] + fw->origin_bytes(L), L.nyp * L.nzp, L.nxp, L.pitch, L.nyp, L.plane);
         for (int k = 0; k < fw->npsi3(); k++) {
@@ -280,17 +303,17 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
     }
     o_segs = take(sizeof(CkptSeg) * segs.size());
-    o_scales = take(sizeof(float) * segs.size() * ncheck);
+    o_scales = take(sizeof(float) * segs.size() * nslots);
     o_maxbits = take(sizeof(unsigned) * segs.size());
     if (dev_alloc(&dbuf, off, stream) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of %zu bytes failed", off);
         return RSGPU_ERR_NOMEM;
     }
-    const size_t ck_bytes = slot_elems * ck_es * (size_t)ncheck;
+    const size_t ck_bytes = slot_elems * ck_es * (size_t)nslots;
     if (dev_alloc(&ckpt, ck_bytes, stream) != cudaSuccess) {
         cudaGetLastError();
-        set_error("checkpoint allocation of %zu bytes (%d slots) failed", ck_bytes, ncheck);
+        set_error("checkpoint allocation of %zu bytes (%d slots) failed", ck_bytes, nslots);
         return RSGPU_ERR_NOMEM;
     }
     CU(cudaMemsetAsync(dbuf, 0, off, stream));
@@ -434,7 +457,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
 
 rsgpu_status Adjoint3D::slot_io(bool save, int slot)
 {
-    if (slot < 0 || slot >= ncheck) { set_error("checkpoint slot %d outside [0,%d)", slot, ncheck); return RSGPU_ERR_REVOLVE; }
+    if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
     char *sl = (char *)ckpt + (size_t)slot * slot_elems * ck_es;
     float *sc = (float *)D(o_scales) + (size_t)slot * segs.size();
     cudaError_t e = save ? launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), sl, sc,
@@ -456,8 +479,54 @@ rsgpu_status Adjoint3D::correlate()
     return RSGPU_OK;
 }
 
+// RtmAcoustic3D::run (lib/rtm.cpp:640-733): as the 2D FULL driver, the P interior
+// saved after steps 0, snapinc, ... and correlated at the adjoint times t with
+// (t - enddiff) % snapinc == 0 against snapshot (t - enddiff)/snapinc.
+rsgpu_status Adjoint3D::run_full()
+{
+    const int nt = cfg.nt;
+    const long long l0 = fw->launches + bw->launches;
+    launches = 0;
+    fw_steps = bw_steps = ckpt_bytes = 0;
+    ran = false;
+    ST(fw->reset());
+    ST(bw->reset());
+    const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
+    for (int i = 0; i < nshots; i++)
+        CU(cudaMemsetAsync(D(o_img[i]), 0, (size_t)nx[i] * ny[i] * nz[i] * nhx * nhy * nhz * gs, stream));
+    ST(fw->run(0, 1));
+    ST(slot_io(true, 0));
+    for (int k = 1; k < snapnt; k++) {
+        ST(fw->run((k - 1) * snapinc + 1, snapinc));
+        ST(slot_io(true, k));
+    }
+    const int done = (snapnt - 1) * snapinc + 1;
+    if (done < nt) ST(fw->run(done, nt - done));
+    fw_steps = nt;
+    auto aligned = [&](int k) { return ((nt - 1 - k) - enddiff) % snapinc == 0; };
+    for (int k = 0; k < nt;) {
+        int e = k;
+        while (e < nt && !aligned(e)) e++;
+        const int n = (e < nt ? e + 1 : nt) - k;
+        ST(bw->run(k, n));
+        bw_steps += n;
+        k += n;
+        if (e < nt) {
+            ST(slot_io(false, ((nt - 1 - e) - enddiff) / snapinc));
+            ST(correlate());
+        }
+    }
+    launches += fw->launches + bw->launches - l0;
+    CU(cudaStreamSynchronize(stream));
+    ST(fw->check_device_error());
+    ST(bw->check_device_error());
+    ran = true;
+    return RSGPU_OK;
+}
+
 rsgpu_status Adjoint3D::run()
 {
+    if (snapmethod == RSGPU_SNAP_FULL) return run_full();
     const int nt = cfg.nt;
     const long long l0 = fw->launches + bw->launches;
     launches = 0;

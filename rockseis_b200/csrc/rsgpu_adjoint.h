@@ -1,7 +1,9 @@
 // Kernels of the FWI-gradient and RTM-image drivers (host runtime internals, not ABI).
 #pragma once
+#include <cmath>
 #include <cstddef>
 #include <cuda_runtime.h>
+#include "rsgpu_kernels.h"
 
 namespace rsgpu {
 
@@ -106,6 +108,19 @@ struct CkptSeg {
 };
 
 enum { ACC_REF = 0, ACC_F64 = 1 };
+
+// Snapshot2D/3D's enddiff (lib/snap.cpp:334-337), evaluated in the element type:
+// the adjoint time of the last snapshot minus that of the last forward step.
+inline int snap_enddiff(int nt, double dt_cfg, int snapinc, int prec)
+{
+    const int snapnt = (nt - 1) / snapinc + 1;
+    if (prec == PREC_F64) {
+        const double dt = dt_cfg, snapdt = dt * snapinc;
+        return (int)rintf((float)(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt));
+    }
+    const float dt = (float)dt_cfg, snapdt = dt * snapinc;
+    return (int)rintf(((nt - 1) * dt - (snapnt - 1) * snapdt) / dt);
+}
 enum { CK_NATIVE = 0, CK_F16 = 1, CK_BF16 = 2 };
 
 // Gradient/image correlation of one adjoint time step over all shots.

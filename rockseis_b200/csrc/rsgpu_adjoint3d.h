@@ -20,7 +20,9 @@ public:
 
     int kind = RSGPU_KIND_RTM, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE, nhx = 1, nhy = 1, nhz = 1;
     int phys = PHYS_A3D;
-    int ncheck = 0, nxmax = 0, nymax = 0;
+    int ncheck = 0, nslots = 0, nxmax = 0, nymax = 0;
+    // FULL snapshots (RtmAcoustic3D::run): the P interior every snapinc steps
+    int snapmethod = RSGPU_SNAP_OPTIMAL, snapinc = 1, snapnt = 0, enddiff = 0;
     int misfit_type = 0, nrec_max = 0;
     rsgpu_config cfg{};
     std::unique_ptr<Plan3D> fw, bw;
@@ -40,6 +42,7 @@ public:
     bool ran = false;
 
 private:
+    rsgpu_status run_full();
     rsgpu_status slot_io(bool save, int slot);
     rsgpu_status correlate();
     char *D(size_t o) const { return (char *)dbuf + o; }

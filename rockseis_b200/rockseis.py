@@ -622,12 +622,12 @@ class _Adjoint:
         check_stability(self.model, self.source.dt, self.cls)
         return True
 
-    def _opts(self, nhx=1, nhz=1, nhy=1, full=False) -> abi.AdjointOpts:
+    def _opts(self, nhx=1, nhz=1, nhy=1, snapmethod=abi.SNAP_OPTIMAL) -> abi.AdjointOpts:
         o = abi.AdjointOpts()
         o.ncheck, o.ckpt_precision, o.accum, o.misfit, o.nhx, o.nhz = (self.ncheck, self.ckpt_precision, self.accum,
                                                                         self.misfit_type, nhx, nhz)
         o.nhy = nhy
-        o.snapmethod = abi.SNAP_FULL if full else abi.SNAP_OPTIMAL
+        o.snapmethod = snapmethod
         o.snapinc, o.noreverse = self.snapinc, int(bool(self.noreverse))
         return o
 
@@ -679,7 +679,7 @@ class FwiAcoustic2D(_Adjoint):
     def run(self):
         """FwiAcoustic2D::run (lib/fwi.cpp:1030-1156): FULL snapshots every snapinc
         steps; with setNoreverse(True) the forward run, datamodP and the misfit only."""
-        return fwi_gradient_batch([self], full=True)
+        return fwi_gradient_batch([self], snapmethod=abi.SNAP_FULL)
 
     def run_optimal(self):
         return fwi_gradient_batch([self])
@@ -822,7 +822,13 @@ class RtmAcoustic2D(_Adjoint):
 
     def run(self):
         """RtmAcoustic2D::run (lib/rtm.cpp:222-326): FULL snapshots every snapinc steps."""
-        return rtm_image_batch([self], full=True)
+        return rtm_image_batch([self], snapmethod=abi.SNAP_FULL)
+
+    def run_edge(self):
+        """RtmAcoustic2D::run_edge (lib/rtm.cpp:328-421): only the wavefield's four edge
+        lines are kept every snapinc steps; the source wavefield is re-propagated from
+        them during the adjoint pass."""
+        return rtm_image_batch([self], snapmethod=abi.SNAP_EDGES)
 
     def run_optimal(self):
         return rtm_image_batch([self])
@@ -843,6 +849,10 @@ class RtmAcoustic3D(_Adjoint):
         a.image = ptr(self.pimage.getImagedata())
         return a
 
+    def run(self):
+        """RtmAcoustic3D::run (lib/rtm.cpp:640-733): FULL snapshots every snapinc steps."""
+        return rtm_image_batch([self], snapmethod=abi.SNAP_FULL)
+
     def run_optimal(self):
         return rtm_image_batch([self])
 
@@ -861,11 +871,11 @@ def _adjoint_tile(jobs) -> int:
                  j0.precision)
 
 
-def _adjoint_batch(jobs, fn, full):
+def _adjoint_batch(jobs, fn, snapmethod):
     j0 = jobs[0]
     j0.checkStability()
     cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
-    opts = j0._opts(*_lags(j0), full=full)
+    opts = j0._opts(*_lags(j0), snapmethod=snapmethod)
     keep: list = []
     shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(keep) for j in jobs])
     check(fn(C.byref(cfg), C.byref(opts), len(jobs), shots))
@@ -875,26 +885,27 @@ def _adjoint_batch(jobs, fn, full):
     return FWI_OK
 
 
-def fwi_gradient_batch(jobs, full=False):
+def fwi_gradient_batch(jobs, snapmethod=abi.SNAP_OPTIMAL):
     """Many FwiAcoustic2D shots (each with its own model window) in one batched
     gradient computation; per-shot outputs accumulate like run_optimal's (run's
-    with full=True: FULL snapshots every snapinc steps of the first job)."""
-    return _adjoint_batch(jobs, abi.lib.rsgpu_fwi_gradient, full)
+    with SNAP_FULL: snapshots every snapinc steps of the first job)."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_fwi_gradient, snapmethod)
 
 
-def rtm_image_batch(jobs, full=False):
-    """Many RtmAcoustic2D shots imaged in one batched run (full: as RtmAcoustic2D::run)."""
-    return _adjoint_batch(jobs, abi.lib.rsgpu_rtm_image, full)
+def rtm_image_batch(jobs, snapmethod=abi.SNAP_OPTIMAL):
+    """Many RtmAcoustic2D shots imaged in one batched run (SNAP_FULL: as
+    RtmAcoustic2D::run, SNAP_EDGES: as RtmAcoustic2D::run_edge)."""
+    return _adjoint_batch(jobs, abi.lib.rsgpu_rtm_image, snapmethod)
 
 
 class AdjointBatch:
     """Device-resident gradient/image batch (rsgpu_adjoint_*): create once, run many times."""
 
-    def __init__(self, jobs, kind=abi.KIND_FWI, full=False):
+    def __init__(self, jobs, kind=abi.KIND_FWI, snapmethod=abi.SNAP_OPTIMAL):
         j0 = jobs[0]
         self.jobs = jobs
         self.cfg = make_config(j0.model, j0.order, j0.source.nt, j0.source.dt, j0.precision, _adjoint_tile(jobs))
-        self.opts = j0._opts(*_lags(j0), full=full)
+        self.opts = j0._opts(*_lags(j0), snapmethod=snapmethod)
         self._keep: list = []
         self.shots = (abi.AdjointShot * len(jobs))(*[j._adjoint_shot(self._keep) for j in jobs])
         self.h = C.c_void_p()

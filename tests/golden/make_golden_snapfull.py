@@ -13,7 +13,12 @@ Writes tests/golden/snapfull.npz for the acoustic FWI case of tests/cases.py
     residuals at zero: the script asserts both);
   * the gradients for snapinc 3 and 7 (enddiff 2 and 5: the correlated times
     are shifted against the saved ones);
-  * the RTM image for snapinc 4 with three x lags.
+  * the RTM image for snapinc 4 with three x lags, from full snapshots
+    (RtmAcoustic2D::run) and from edge lines (RtmAcoustic2D::run_edge,
+    lib/rtm.cpp:328-421);
+  * the 3D RTM image (RtmAcoustic3D::run, lib/rtm.cpp:640-733) of the small 3D
+    case of tests/test_gpu_modelling_3d.py (29 x 27 x 25, nt = 120) for snapinc 4,
+    with the data it migrates.
 """
 import os
 import sys
@@ -54,6 +59,14 @@ def main():
         assert not np.any(runs["noreverse"][k]), k
     out[f"rtm_s{RTM_SNAPINC}_h{RTM_NHX}"] = api.ref_rtm_a2d_full(c.pb, c.src.scoords, wav, c.rec.gcoords, obs,
                                                                  RTM_SNAPINC, nhx=RTM_NHX)
+    out[f"rtm_edge_s{RTM_SNAPINC}_h{RTM_NHX}"] = api.ref_rtm_a2d_full(c.pb, c.src.scoords, wav, c.rec.gcoords, obs,
+                                                                      RTM_SNAPINC, nhx=RTM_NHX, edges=True)
+    from tests.test_gpu_modelling_3d import Case3D, rtm_inputs
+    c3 = Case3D(nx=29, ny=27, nz=25)
+    data3 = rtm_inputs(c3)
+    out["rtm3d_data"] = data3
+    out["rtm3d_s4"] = api.ref_rtm_a3d(c3.pb, c3.src.scoords, c3.src.data.astype(np.float32), c3.rec.gcoords, data3,
+                                      0, full_snapinc=4)
     path = os.path.join(ROOT, "tests", "golden", "snapfull.npz")
     np.savez_compressed(path, **out)
     print(path, os.path.getsize(path), "bytes")

@@ -346,7 +346,7 @@ def test_fwi_full_snapshots_batched_windows_bitwise(require_gpu):
     jobs = [make_fwi(c) for c in cases]
     for j in jobs:
         j.setSnapinc(5)
-    assert fwi_gradient_batch(jobs, full=True) == 1
+    assert fwi_gradient_batch(jobs, snapmethod=abi.SNAP_FULL) == 1
     for j, ref in zip(jobs, refs):
         assert_same(outputs(j), ref)
 
@@ -424,3 +424,25 @@ def test_fwi_adaptive_misfit_fp64_accumulation_close(require_gpu):
     for k in GRAD:
         assert rel_l2(got[k], ref[k]) < 1e-5, (k, rel_l2(got[k], ref[k]))
     assert abs(got["misfit"] - ref["misfit"]) <= 1e-5 * abs(ref["misfit"])
+
+
+@pytest.mark.parametrize("snapinc,nhx", [(1, 1), (3, 1), (4, 3)])
+def test_rtm_edge_snapshots_bitwise(require_gpu, snapinc, nhx):
+    # RtmAcoustic2D::run_edge: the four edge lines of P saved every snapinc steps; the
+    # source wavefield is stepped again from zero with the saved lines written back in
+    from oracle import api
+    c = fwi_case()
+    if api.ref_available():
+        ref = api.ref_rtm_a2d_full(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords,
+                                   c.obs.astype(np.float32), snapinc, nhx=nhx, edges=True)
+    elif (snapinc, nhx) == (4, 3):
+        ref = _snapfull()["rtm_edge_s4_h3"]
+    else:
+        pytest.skip("reference library not built")
+    c.rec.data = np.ascontiguousarray(c.obs)
+    img = Image2D("pimage", c.model, nhx, 1)
+    r = RtmAcoustic2D(c.model, img, c.src, c.rec, c.order, snapinc)
+    assert r.run_edge() == 1
+    got = img.getImagedata()
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(got, ref), f"max abs diff {np.abs(got - ref).max()}"

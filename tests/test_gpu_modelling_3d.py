@@ -250,3 +250,29 @@ def test_fwi3d_adaptive_misfit_bitwise(require_gpu, misfit):
         assert np.abs(ref[k]).max() > 0, k
         assert np.array_equal(got[k], ref[k]), f"{k}: max abs diff {np.abs(got[k] - ref[k]).max()}"
     assert got["misfit"] == float(ref["misfit"])
+
+
+@pytest.mark.parametrize("snapinc,lags", [(4, (1, 1, 1)), (3, (3, 1, 3)), (1, (1, 3, 1))])
+def test_rtm3d_full_snapshots_bitwise(require_gpu, snapinc, lags):
+    # RtmAcoustic3D::run: the P interior every snapinc steps, correlated at the adjoint
+    # times shifted by enddiff (nt = 120: enddiff 3, 2, 0)
+    import os
+    from rockseis_b200.rockseis import Image3D, RtmAcoustic3D
+    c = Case3D(nx=29, ny=27, nz=25)
+    data = rtm_inputs(c)
+    if api.ref_available():
+        ref = api.ref_rtm_a3d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.rec.gcoords, data, 0, *lags,
+                              full_snapinc=snapinc)
+    elif (snapinc, lags) == (4, (1, 1, 1)):
+        g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "snapfull.npz"))
+        assert np.array_equal(data, g["rtm3d_data"])
+        ref = g["rtm3d_s4"]
+    else:
+        pytest.skip("reference library not built")
+    c.rec.data = np.ascontiguousarray(data)
+    img = Image3D("pimage", c.model, *lags)
+    r = RtmAcoustic3D(c.model, img, c.src, c.rec, c.order, snapinc)
+    assert r.run() == 1
+    got = img.getImagedata()
+    assert np.abs(ref).max() > 0
+    assert np.array_equal(got, ref), f"max abs diff {np.abs(got - ref).max()}"
