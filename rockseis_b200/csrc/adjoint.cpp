@@ -75,10 +75,12 @@ public:
     cudaStream_t stream = nullptr;
     void *dbuf = nullptr, *ckpt = nullptr;
     size_t slot_elems = 0, ck_es = 4;
+    int seg_rows = 1;                       // rows of the tallest checkpoint block
     std::vector<CkptSeg> segs;
     std::vector<size_t> o_vp, o_vs, o_rho, o_obs, o_obsx, o_obsz, o_g0, o_g1, o_g2;
     std::vector<size_t> o_ilum;      // acoustic FWI source illumination (0 = not asked for)
     size_t o_misfit = 0, o_corr = 0, o_res = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    size_t o_rpart = 0;                     // residual pass: per-CTA partial misfits
     std::vector<size_t> o_work, o_tnorm;   // ADAPTIVE misfits: per-trace scratch and filter norms
     std::vector<size_t> o_work2, o_tnorm2; // elastic ADAPTIVE_GAUSS / _LINEAR: the Uz filters
     size_t o_comp = 0;                      // elastic ADAPTIVE_GAUSS / _LINEAR: Ux and Uz views per shot
@@ -307,6 +309,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         }
     }
     o_misfit = take(sizeof(double) * ns);
+    o_rpart = take(sizeof(double) * residual_partials(ns));
     const bool adaptive = kind == RSGPU_KIND_FWI && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
                                                      misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR ||
                                                      misfit_type == RSGPU_MISFIT_ADAPTIVE_SINGLE);
@@ -371,6 +374,7 @@ rsgpu_status Adjoint::create(const rsgpu_config *c, const rsgpu_adjoint_opts *o,
         for (int p = 0; p < npsi(phys); p++) add(L.psiz[p], 2 * cfg.lpml, L.nxp, L.nxp);
     }
     o_segs = take(sizeof(CkptSeg) * segs.size());
+    seg_rows = ckpt_max_rows(segs.data(), segs.size());
     o_scales = take(sizeof(float) * segs.size() * nslots);
     o_maxbits = take(sizeof(unsigned) * segs.size());
     if (dev_alloc(&dbuf, off, stream) != cudaSuccess) {
@@ -523,7 +527,7 @@ void Adjoint::build_desc_e2d(std::vector<unsigned char> &corr, std::vector<unsig
 rsgpu_status Adjoint::save(int slot)
 {
     if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
-    cudaError_t e = launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(),
+    cudaError_t e = launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), seg_rows,
                                      (char *)ckpt + (size_t)slot * slot_elems * ck_es,
                                      (float *)D(o_scales) + (size_t)slot * segs.size(), (unsigned *)D(o_maxbits), stream);
     if (e != cudaSuccess) { set_error("checkpoint save: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
@@ -535,7 +539,7 @@ rsgpu_status Adjoint::save(int slot)
 rsgpu_status Adjoint::load(int slot)
 {
     if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
-    cudaError_t e = launch_ckpt_load(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(),
+    cudaError_t e = launch_ckpt_load(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), seg_rows,
                                      (const char *)ckpt + (size_t)slot * slot_elems * ck_es,
                                      (const float *)D(o_scales) + (size_t)slot * segs.size(), stream);
     if (e != cudaSuccess) { set_error("checkpoint restore: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
@@ -592,9 +596,10 @@ rsgpu_status Adjoint::residuals()
                     ? (corr ? launch_residual_corr_e2d(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream)
                             : launch_residual_e2d(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream))
                     : corr ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit), stream, true)
-                           : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                           : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), (double *)D(o_rpart),
+                                             stream);
     if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-    launches += 1;
+    launches += elastic() || corr ? 1 : 2;
     return RSGPU_OK;
 }
 

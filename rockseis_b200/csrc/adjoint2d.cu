@@ -165,42 +165,58 @@ __global__ void __launch_bounds__(256) corr_rtm_a3d(const Corr3D<T> *desc, int n
 }
 
 // ---------------------------------------------------------------- residuals and misfit
+// Residual pass: RES_BLOCKS CTAs per shot, each over a contiguous share of the
+// shot's samples; with FP64 accumulation each CTA also leaves its partial sum of
+// r*r/2 over on-grid traces (fixed-order tree, so the result is reproducible).
+constexpr int RES_BLOCKS = 64;
+
 template <typename T, int ACC>
-__global__ void __launch_bounds__(256) residual_misfit(const Resid2D<T> *desc, double *misfit)
+__global__ void __launch_bounds__(256) residual_diff(const Resid2D<T> *desc, double *partials)
 {
-    const Resid2D<T> d = desc[blockIdx.x];
+    const Resid2D<T> d = desc[blockIdx.y];
     const long n = (long)d.nrec * d.nt;
-    for (long k = threadIdx.x; k < n; k += blockDim.x) d.res[k] = X<T>::sub(d.mod[k], d.obs[k]);
-    if (ACC == ACC_REF) {
-        __syncthreads();
-        if (threadIdx.x != 0) return;
-        // mis += 0.5*r*r with a T-typed accumulator, traces then samples
-        T mis = 0;
-        for (int tr = 0; tr < d.nrec; tr++) {
-            if (d.rec_pt[tr] < 0) continue;
-            const T *r = d.res + (long)tr * d.nt;
-            for (int it = 0; it < d.nt; it++) {
-                const double rr = (double)r[it];
-                mis = X<T>::rnd(__dadd_rn((double)mis, __dmul_rn(__dmul_rn(0.5, rr), rr)));
-            }
-        }
-        misfit[blockIdx.x] = (double)mis;
-    } else {
-        double acc = 0.0;
-        for (long k = threadIdx.x; k < n; k += blockDim.x) {
-            if (d.rec_pt[k / d.nt] < 0) continue;
-            const double r = (double)X<T>::sub(d.mod[k], d.obs[k]);
-            acc = fma(0.5 * r, r, acc);
-        }
-        __shared__ double red[256];
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-            if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) misfit[blockIdx.x] = red[0];
+    const long chunk = (n + gridDim.x - 1) / gridDim.x;
+    const long k0 = (long)blockIdx.x * chunk, k1 = min(n, k0 + chunk);
+    double acc = 0.0;
+    for (long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        const T r = X<T>::sub(d.mod[k], d.obs[k]);
+        d.res[k] = r;
+        if (ACC == ACC_F64 && d.rec_pt[k / d.nt] >= 0) acc = fma(0.5 * (double)r, (double)r, acc);
     }
+    if (ACC != ACC_F64) return;
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+}
+
+// Misfit per shot: ACC_REF sums 0.5*r*r into a T-typed accumulator, traces then
+// samples, as the reference does (one thread); ACC_F64 adds the CTA partials in order.
+template <typename T, int ACC>
+__global__ void __launch_bounds__(32) residual_sum(const Resid2D<T> *desc, const double *partials, double *misfit)
+{
+    if (threadIdx.x != 0) return;
+    const Resid2D<T> d = desc[blockIdx.x];
+    if (ACC == ACC_F64) {
+        double m = 0.0;
+        for (int b = 0; b < RES_BLOCKS; b++) m += partials[(long)blockIdx.x * RES_BLOCKS + b];
+        misfit[blockIdx.x] = m;
+        return;
+    }
+    T mis = 0;
+    for (int tr = 0; tr < d.nrec; tr++) {
+        if (d.rec_pt[tr] < 0) continue;
+        const T *r = d.res + (long)tr * d.nt;
+        for (int it = 0; it < d.nt; it++) {
+            const double rr = (double)r[it];
+            mis = X<T>::rnd(__dadd_rn((double)mis, __dmul_rn(__dmul_rn(0.5, rr), rr)));
+        }
+    }
+    misfit[blockIdx.x] = (double)mis;
 }
 
 // ---------------------------------------------------------------- CORRELATION misfit
@@ -580,71 +596,130 @@ __device__ __forceinline__ long long seg_row(const CkptSeg &s, int r)
     return pl * s.pstride + (long long)(r - pl * s.prow) * s.pitch;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) ckpt_copy_out(const CkptSeg *segs, T *slot)
+// Checkpoint kernels: one warp per row of a block (rows of a 3D block run plane by
+// plane), grid.y = block; lanes walk the row with four independent loads in flight
+// before their stores, so the copy is not serialised on load latency.
+constexpr int CK_WARPS = 8;       // warps (rows in flight) per CTA
+
+// Applies op(src_index, slot_index) to every element of row r of block s, in
+// groups of four per lane.
+template <typename F>
+__device__ __forceinline__ void ck_row(const CkptSeg &s, int r, int lane, F op)
 {
-    const CkptSeg s = segs[blockIdx.y];
-    const T *src = (const T *)s.src;
-    T *dst = slot + s.dst;
-    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[(long)r * s.cols + c] = src[seg_row(s, r) + c];
+    const long long so = seg_row(s, r), dof = s.dst + (long long)r * s.cols;
+    int c = lane;
+    for (; c + 96 < s.cols; c += 128) op(so + c, dof + c, 4);
+    for (; c < s.cols; c += 32) op(so + c, dof + c, 1);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) ckpt_copy_in(const CkptSeg *segs, const T *slot)
+__global__ void __launch_bounds__(256) ckpt_copy_out(const CkptSeg *segs, T *__restrict__ slot)
 {
     const CkptSeg s = segs[blockIdx.y];
-    T *dst = (T *)s.src;
-    const T *src = slot + s.dst;
-    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) dst[seg_row(s, r) + c] = src[(long)r * s.cols + c];
+    const T *__restrict__ src = (const T *)s.src;
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * CK_WARPS + (threadIdx.x >> 5); r < s.rows; r += gridDim.x * CK_WARPS)
+        ck_row(s, r, lane, [&](long long i, long long o, int n) {
+            if (n == 4) {
+                const T a = src[i], b = src[i + 32], c = src[i + 64], d = src[i + 96];
+                slot[o] = a; slot[o + 32] = b; slot[o + 64] = c; slot[o + 96] = d;
+            } else {
+                slot[o] = src[i];
+            }
+        });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ckpt_copy_in(const CkptSeg *segs, const T *__restrict__ slot)
+{
+    const CkptSeg s = segs[blockIdx.y];
+    T *__restrict__ dst = (T *)s.src;
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * CK_WARPS + (threadIdx.x >> 5); r < s.rows; r += gridDim.x * CK_WARPS)
+        ck_row(s, r, lane, [&](long long i, long long o, int n) {
+            if (n == 4) {
+                const T a = slot[o], b = slot[o + 32], c = slot[o + 64], d = slot[o + 96];
+                dst[i] = a; dst[i + 32] = b; dst[i + 64] = c; dst[i + 96] = d;
+            } else {
+                dst[i] = slot[o];
+            }
+        });
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) ckpt_maxabs(const CkptSeg *segs, unsigned *maxbits)
 {
     const CkptSeg s = segs[blockIdx.y];
-    const T *src = (const T *)s.src;
+    const T *__restrict__ src = (const T *)s.src;
+    const int lane = threadIdx.x & 31;
     float m = 0.0f;
-    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x) m = fmaxf(m, fabsf((float)src[seg_row(s, r) + c]));
+    for (int r = blockIdx.x * CK_WARPS + (threadIdx.x >> 5); r < s.rows; r += gridDim.x * CK_WARPS)
+        ck_row(s, r, lane, [&](long long i, long long, int n) {
+            if (n == 4) {
+                const float a = fabsf((float)src[i]), b = fabsf((float)src[i + 32]);
+                const float c = fabsf((float)src[i + 64]), d = fabsf((float)src[i + 96]);
+                m = fmaxf(m, fmaxf(fmaxf(a, b), fmaxf(c, d)));
+            } else {
+                m = fmaxf(m, fabsf((float)src[i]));
+            }
+        });
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(&maxbits[blockIdx.y], __float_as_uint(m));
+    if (lane == 0 && m > 0.0f) atomicMax(&maxbits[blockIdx.y], __float_as_uint(m));
 }
 
 template <typename T, typename S>
-__global__ void __launch_bounds__(256) ckpt_pack(const CkptSeg *segs, S *slot, const unsigned *maxbits, float *scales)
+__global__ void __launch_bounds__(256) ckpt_pack(const CkptSeg *segs, S *__restrict__ slot, const unsigned *maxbits,
+                                                 float *scales)
 {
     const CkptSeg s = segs[blockIdx.y];
     const float scale = pow2_scale(maxbits[blockIdx.y]);
     const float inv = 1.0f / scale;            // exact: a power of two
     if (blockIdx.x == 0 && threadIdx.x == 0) scales[blockIdx.y] = scale;
-    const T *src = (const T *)s.src;
-    S *dst = slot + s.dst;
-    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
-            dst[(long)r * s.cols + c] = Store<S>::to((float)src[seg_row(s, r) + c] * inv);
+    const T *__restrict__ src = (const T *)s.src;
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * CK_WARPS + (threadIdx.x >> 5); r < s.rows; r += gridDim.x * CK_WARPS)
+        ck_row(s, r, lane, [&](long long i, long long o, int n) {
+            if (n == 4) {
+                const float a = (float)src[i], b = (float)src[i + 32], c = (float)src[i + 64], d = (float)src[i + 96];
+                slot[o] = Store<S>::to(a * inv); slot[o + 32] = Store<S>::to(b * inv);
+                slot[o + 64] = Store<S>::to(c * inv); slot[o + 96] = Store<S>::to(d * inv);
+            } else {
+                slot[o] = Store<S>::to((float)src[i] * inv);
+            }
+        });
 }
 
 template <typename T, typename S>
-__global__ void __launch_bounds__(256) ckpt_unpack(const CkptSeg *segs, const S *slot, const float *scales)
+__global__ void __launch_bounds__(256) ckpt_unpack(const CkptSeg *segs, const S *__restrict__ slot, const float *scales)
 {
     const CkptSeg s = segs[blockIdx.y];
     const float scale = scales[blockIdx.y];
-    T *dst = (T *)s.src;
-    const S *src = slot + s.dst;
-    for (int r = blockIdx.x; r < s.rows; r += gridDim.x)
-        for (int c = threadIdx.x; c < s.cols; c += blockDim.x)
-            dst[seg_row(s, r) + c] = (T)(Store<S>::from(src[(long)r * s.cols + c]) * scale);
+    T *__restrict__ dst = (T *)s.src;
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * CK_WARPS + (threadIdx.x >> 5); r < s.rows; r += gridDim.x * CK_WARPS)
+        ck_row(s, r, lane, [&](long long i, long long o, int n) {
+            if (n == 4) {
+                const S a = slot[o], b = slot[o + 32], c = slot[o + 64], d = slot[o + 96];
+                dst[i] = (T)(Store<S>::from(a) * scale); dst[i + 32] = (T)(Store<S>::from(b) * scale);
+                dst[i + 64] = (T)(Store<S>::from(c) * scale); dst[i + 96] = (T)(Store<S>::from(d) * scale);
+            } else {
+                dst[i] = (T)(Store<S>::from(slot[o]) * scale);
+            }
+        });
 }
 
-constexpr int CK_BLOCKS = 64;   // row-blocks per segment (grid.x)
+// CTAs per block: enough warps for the tallest block's rows, at most 128 CTAs.
+inline dim3 ck_grid(int nseg, int max_rows)
+{
+    const int bx = std::min(128, std::max(1, (max_rows + CK_WARPS - 1) / CK_WARPS));
+    return dim3((unsigned)bx, (unsigned)nseg);
+}
 
 template <typename T>
-cudaError_t ckpt_save_t(int ck, const CkptSeg *segs, int nseg, void *slot, float *scales, unsigned *maxbits,
-                        cudaStream_t st)
+cudaError_t ckpt_save_t(int ck, const CkptSeg *segs, int nseg, int max_rows, void *slot, float *scales,
+                        unsigned *maxbits, cudaStream_t st)
 {
-    const dim3 grid(CK_BLOCKS, nseg);
+    const dim3 grid = ck_grid(nseg, max_rows);
     if (ck == CK_NATIVE) {
         ckpt_copy_out<T><<<grid, 256, 0, st>>>(segs, (T *)slot);
         return cudaGetLastError();
@@ -658,9 +733,10 @@ cudaError_t ckpt_save_t(int ck, const CkptSeg *segs, int nseg, void *slot, float
 }
 
 template <typename T>
-cudaError_t ckpt_load_t(int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales, cudaStream_t st)
+cudaError_t ckpt_load_t(int ck, const CkptSeg *segs, int nseg, int max_rows, const void *slot, const float *scales,
+                        cudaStream_t st)
 {
-    const dim3 grid(CK_BLOCKS, nseg);
+    const dim3 grid = ck_grid(nseg, max_rows);
     if (ck == CK_NATIVE) ckpt_copy_in<T><<<grid, 256, 0, st>>>(segs, (const T *)slot);
     else if (ck == CK_F16) ckpt_unpack<T, __half><<<grid, 256, 0, st>>>(segs, (const __half *)slot, scales);
     else ckpt_unpack<T, __nv_bfloat16><<<grid, 256, 0, st>>>(segs, (const __nv_bfloat16 *)slot, scales);
@@ -772,14 +848,24 @@ cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int ns
     return cudaGetLastError();
 }
 
-cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st)
+template <typename T, int ACC>
+void residual_t(const void *desc, int nshots, double *misfit, double *partials, cudaStream_t st)
+{
+    residual_diff<T, ACC><<<dim3(RES_BLOCKS, nshots), 256, 0, st>>>((const Resid2D<T> *)desc, partials);
+    residual_sum<T, ACC><<<nshots, 32, 0, st>>>((const Resid2D<T> *)desc, partials, misfit);
+}
+
+size_t residual_partials(int nshots) { return (size_t)nshots * RES_BLOCKS; }
+
+cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, double *partials,
+                            cudaStream_t st)
 {
     if (prec == PREC_F64) {
-        if (acc == ACC_F64) residual_misfit<double, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2D<double> *)desc, misfit);
-        else residual_misfit<double, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2D<double> *)desc, misfit);
+        if (acc == ACC_F64) residual_t<double, ACC_F64>(desc, nshots, misfit, partials, st);
+        else residual_t<double, ACC_REF>(desc, nshots, misfit, partials, st);
     } else {
-        if (acc == ACC_F64) residual_misfit<float, ACC_F64><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
-        else residual_misfit<float, ACC_REF><<<nshots, 256, 0, st>>>((const Resid2D<float> *)desc, misfit);
+        if (acc == ACC_F64) residual_t<float, ACC_F64>(desc, nshots, misfit, partials, st);
+        else residual_t<float, ACC_REF>(desc, nshots, misfit, partials, st);
     }
     return cudaGetLastError();
 }
@@ -822,18 +908,18 @@ cudaError_t launch_residual_e2d(int prec, int acc, const void *desc, int nshots,
     return cudaGetLastError();
 }
 
-cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,
+cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, int max_rows, void *slot, float *scales,
                              unsigned *maxbits, cudaStream_t st)
 {
-    return prec == PREC_F64 ? ckpt_save_t<double>(ck, segs, nseg, slot, scales, maxbits, st)
-                            : ckpt_save_t<float>(ck, segs, nseg, slot, scales, maxbits, st);
+    return prec == PREC_F64 ? ckpt_save_t<double>(ck, segs, nseg, max_rows, slot, scales, maxbits, st)
+                            : ckpt_save_t<float>(ck, segs, nseg, max_rows, slot, scales, maxbits, st);
 }
 
-cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales,
-                             cudaStream_t st)
+cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, int max_rows, const void *slot,
+                             const float *scales, cudaStream_t st)
 {
-    return prec == PREC_F64 ? ckpt_load_t<double>(ck, segs, nseg, slot, scales, st)
-                            : ckpt_load_t<float>(ck, segs, nseg, slot, scales, st);
+    return prec == PREC_F64 ? ckpt_load_t<double>(ck, segs, nseg, max_rows, slot, scales, st)
+                            : ckpt_load_t<float>(ck, segs, nseg, max_rows, slot, scales, st);
 }
 
 }  // namespace rsgpu

@@ -263,6 +263,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
     o_corr = take(corr_bytes * ns);
     o_res = take(res_bytes * ns);
     o_misfit = take(sizeof(double) * ns);
+    o_rpart = take(sizeof(double) * residual_partials(ns));
     const bool adaptive = fwi() && (misfit_type == RSGPU_MISFIT_ADAPTIVE_GAUSS ||
                                     misfit_type == RSGPU_MISFIT_ADAPTIVE_LINEAR);
     o_work.assign(ns, 0);
@@ -303,6 +304,7 @@ rsgpu_status Adjoint3D::create(const rsgpu_config *c, const rsgpu_adjoint_opts *
         }
     }
     o_segs = take(sizeof(CkptSeg) * segs.size());
+    seg_rows = ckpt_max_rows(segs.data(), segs.size());
     o_scales = take(sizeof(float) * segs.size() * nslots);
     o_maxbits = take(sizeof(unsigned) * segs.size());
     if (dev_alloc(&dbuf, off, stream) != cudaSuccess) {
@@ -460,9 +462,9 @@ rsgpu_status Adjoint3D::slot_io(bool save, int slot)
     if (slot < 0 || slot >= nslots) { set_error("checkpoint slot %d outside [0,%d)", slot, nslots); return RSGPU_ERR_REVOLVE; }
     char *sl = (char *)ckpt + (size_t)slot * slot_elems * ck_es;
     float *sc = (float *)D(o_scales) + (size_t)slot * segs.size();
-    cudaError_t e = save ? launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), sl, sc,
+    cudaError_t e = save ? launch_ckpt_save(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), seg_rows, sl, sc,
                                             (unsigned *)D(o_maxbits), stream)
-                         : launch_ckpt_load(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), sl, sc, stream);
+                         : launch_ckpt_load(prec, ck, (const CkptSeg *)D(o_segs), (int)segs.size(), seg_rows, sl, sc, stream);
     if (e != cudaSuccess) { set_error("checkpoint %s: %s", save ? "save" : "restore", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
     launches += (save && ck != CK_NATIVE) ? 2 : 1;
     ckpt_bytes += (long long)(slot_elems * ck_es);
@@ -564,9 +566,10 @@ rsgpu_status Adjoint3D::run()
                                 : misfit_type == RSGPU_MISFIT_CORRELATION
                                     ? launch_residual_corr(prec, acc, D(o_res), nshots, nrec_max, (double *)D(o_misfit),
                                                            stream, false)
-                                    : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit), stream);
+                                    : launch_residual(prec, acc, D(o_res), nshots, (double *)D(o_misfit),
+                                                      (double *)D(o_rpart), stream);
                 if (e != cudaSuccess) { set_error("residual launch: %s", cudaGetErrorString(e)); return RSGPU_ERR_CUDA; }
-                launches += 1;
+                launches += elastic() || misfit_type == RSGPU_MISFIT_CORRELATION ? 1 : 2;
             }
             ST(bw->inject_record_only(nt - 1 - capo));
             ST(correlate());

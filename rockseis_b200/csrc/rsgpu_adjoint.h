@@ -130,8 +130,11 @@ cudaError_t launch_corr_rtm_a2d(int prec, int acc, const void *desc, int nshots,
                                 int nhz, cudaStream_t st);
 // Residuals (mod - obs) and per-shot misfit (sum of r^2/2 over on-grid traces):
 // ACC_REF in the element type, sequentially in the reference's order; ACC_F64 in
-// double by a fixed-order tree reduction.
-cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
+// double by fixed-order tree reductions (64 CTAs per shot, then their partials).
+// partials: residual_partials(nshots) doubles of scratch.
+cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, double *partials,
+                            cudaStream_t st);
+size_t residual_partials(int nshots);
 // CORRELATION misfit (normalised zero-lag correlation per trace) and its residuals,
 // with the 97th-percentile magnitude clip of the 2D driver when `clip`; nrec_max
 // bounds the shared memory.
@@ -175,10 +178,18 @@ cudaError_t launch_scale_grad_e3d(int prec, int acc, const void *desc, int nshot
                                   cudaStream_t st);
 cudaError_t launch_residual_e3d(int prec, int acc, const void *desc, int nshots, double *misfit, cudaStream_t st);
 // Checkpoint slot I/O.  scales[nseg] holds the power-of-two scale of each block
-// for the 16-bit formats (written by save, read by load).
-cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, void *slot, float *scales,
+// for the 16-bit formats (written by save, read by load); max_rows is the largest
+// `rows` of the blocks (it sizes the grid).
+cudaError_t launch_ckpt_save(int prec, int ck, const CkptSeg *segs, int nseg, int max_rows, void *slot, float *scales,
                              unsigned *maxbits, cudaStream_t st);
-cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, const void *slot, const float *scales,
-                             cudaStream_t st);
+cudaError_t launch_ckpt_load(int prec, int ck, const CkptSeg *segs, int nseg, int max_rows, const void *slot,
+                             const float *scales, cudaStream_t st);
+// The largest row count of a list of blocks.
+inline int ckpt_max_rows(const CkptSeg *segs, size_t n)
+{
+    int m = 1;
+    for (size_t i = 0; i < n; i++) m = segs[i].rows > m ? segs[i].rows : m;
+    return m;
+}
 
 }  // namespace rsgpu

@@ -29,10 +29,12 @@ public:
     cudaStream_t stream = nullptr;
     void *dbuf = nullptr, *ckpt = nullptr;
     size_t slot_elems = 0, ck_es = 4;
+    int seg_rows = 1;                       // rows of the tallest checkpoint block
     std::vector<CkptSeg> segs;
     std::vector<size_t> o_img, o_vp, o_rho, o_obs, o_g1, o_valid;
     std::vector<size_t> o_vs, o_obsy, o_obsz, o_g2;    // elastic: vs, Uy/Uz data, density gradient
     size_t o_corr = 0, o_res = 0, o_misfit = 0, o_segs = 0, o_scales = 0, o_maxbits = 0;
+    size_t o_rpart = 0;                     // residual pass: per-CTA partial misfits
     std::vector<size_t> o_work, o_tnorm;   // ADAPTIVE misfits: per-trace scratch and filter norms
     size_t o_atab = 0;                      // ADAPTIVE misfits: weights and summation-order tables
     std::vector<int> nx, ny, nz, nrec;
