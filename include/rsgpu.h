@@ -329,6 +329,63 @@ rsgpu_status rsgpu_selftest_bounded_wait(void);
  * device to the driver; it synchronises the device.  No reference counterpart. */
 rsgpu_status rsgpu_release_cached_memory(void);
 
+/* ------------------------------------------------------------------ shot-gather files
+ * The reference's .rss container (File::writeHeader / readHeader, lib/file.cpp:184-250):
+ * magic "R0CKS", data_format, header_format, type, Nheader, Ndims, N[9], D[9], O[9],
+ * then per trace Nheader header values and N1 samples.  Trace files
+ * (Data2D::write / read, lib/data.cpp:463-635; Data3D::write :1265-1320) carry the
+ * source and receiver coordinates as trace headers: (sx, sz, gx, gz) in 2D,
+ * (sx, sy, sz, gx, gy, gz) in 3D, in the sample type.  precision: RSGPU_F32_EXACT or
+ * RSGPU_F32_FAST (float files) or RSGPU_F64 (double files). */
+enum { RSGPU_RSS_GENERIC = 0, RSGPU_RSS_REGULAR = 1, RSGPU_RSS_DATA2D = 2, RSGPU_RSS_DATA3D = 3 };
+typedef struct {
+    int data_format, header_format, type;
+    long long nheader, ndims;
+    long long n[9];
+    double d[9], o[9];
+} rsgpu_rss_header;
+rsgpu_status rsgpu_rss_read_header(const char *path, rsgpu_rss_header *h);
+/* Data2D::write (dim 2) / Data3D::write (dim 3): ntrace traces of nt samples;
+ * scoords/gcoords hold dim values per trace ([x, z] or [x, y, z]). */
+rsgpu_status rsgpu_rss_write_traces(const char *path, int precision, int dim, long long nt, double dt, double ot,
+                                    long long ntrace, const void *scoords, const void *gcoords, const void *data);
+/* Traces [first, first+count) of a Data2D/Data3D file; any output may be NULL. */
+rsgpu_status rsgpu_rss_read_traces(const char *path, int precision, long long first, long long count, void *scoords,
+                                   void *gcoords, void *data);
+/* ModelAcoustic2D::writeVp and the other model writers (lib/model.cpp:1283-1313):
+ * a REGULAR file, N1 = nx, N2 = ny (pass 0 in 2D: the file records 1), N3 = nz;
+ * values [nz][ny][nx]. */
+rsgpu_status rsgpu_rss_write_model(const char *path, int precision, int nx, int ny, int nz, double dx, double dy,
+                                   double dz, double ox, double oy, double oz, const void *values);
+rsgpu_status rsgpu_rss_read_model(const char *path, int precision, long long count, void *values);
+
+/* Sort (lib/sort.cpp:132-1055): gathers of a trace file by source, receiver or CMP
+ * position (CMP snapped to dx, dy bins), ordered by x, y, z (order 0), y, x, z (1)
+ * or z, x, y (2), each gather's traces in file order; and the gather queue of the
+ * MPI drivers: rsgpu_sort_next gives the first gather that is NOT_STARTED or
+ * FAILED (Sort::get2DGather()), reading a gather marks it RUNNING, the caller
+ * marks it FINISHED or FAILED (a failed gather is handed out again). */
+enum { RSGPU_SORT_SOURCE = 0, RSGPU_SORT_RECEIVER = 1, RSGPU_SORT_CMP = 2 };
+enum { RSGPU_GATHER_FINISHED = 0, RSGPU_GATHER_RUNNING = 1, RSGPU_GATHER_NOT_STARTED = 2, RSGPU_GATHER_FAILED = 3 };
+typedef struct rsgpu_sort rsgpu_sort;
+rsgpu_status rsgpu_sort_create(const char *path, int key, double dx, double dy, int order, rsgpu_sort **out);
+void rsgpu_sort_destroy(rsgpu_sort *s);
+rsgpu_status rsgpu_sort_info(const rsgpu_sort *s, long long *ngathers, long long *ntraces, long long *nt);
+long long rsgpu_sort_gather_size(const rsgpu_sort *s, long long number);
+long long rsgpu_sort_next(const rsgpu_sort *s);
+int rsgpu_sort_status(const rsgpu_sort *s, long long number);
+rsgpu_status rsgpu_sort_set_status(rsgpu_sort *s, long long number, int status);
+/* Sort::get2DGather(number) / get3DGather(number): coordinates and samples of the
+ * gather's traces (reciprocity swaps sources and receivers). */
+rsgpu_status rsgpu_sort_read_gather(rsgpu_sort *s, long long number, int reciprocity, void *scoords, void *gcoords,
+                                    void *data);
+/* Sort::createEmptydataset: an output trace file with the survey's headers and n1
+ * zero samples per trace; Sort::put2DGather / put3DGather: a gather written to its
+ * traces' places in such a file. */
+rsgpu_status rsgpu_sort_create_output(const rsgpu_sort *s, const char *path, long long n1, double d1, double o1);
+rsgpu_status rsgpu_sort_write_gather(const rsgpu_sort *s, const char *path, long long number, int reciprocity,
+                                     long long n1, const void *scoords, const void *gcoords, const void *data);
+
 /* 2D kernel tile shapes, the search space of the tile autotuner (no counterpart in
  * the reference, whose loops have no tiles).  rsgpu_tile_count returns how many
  * shapes the library holds for `precision`; rsgpu_tile_shape gives shape `idx`:

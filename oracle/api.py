@@ -128,6 +128,15 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_makemap3d_f.argtypes = [G, I, V, I, V, V]
     lib.ref_makemap3d_field_f.argtypes = [G, I, V, I, I, V, V]
     lib.ref_revolve_trace.argtypes = [I, I, V, V, V, I]
+    if hasattr(lib, "ref_data_write_f"):          # file / sort harness (oracle/ref_harness_io.cpp)
+        S, LL = C.c_char_p, C.POINTER(C.c_longlong)
+        lib.ref_data_write_f.argtypes = [S, I, I, D, D, I, V, V, V]
+        lib.ref_data_write_d.argtypes = [S, I, I, D, D, I, V, V, V]
+        lib.ref_data_read2d_f.argtypes = [S, I, I, V, V, V]
+        lib.ref_model_write_f.argtypes = [S, I, I, D, D, D, D, V]
+        lib.ref_sort_gather_f.argtypes = [S, I, I, D, D, I, I, I, LL, V, V, V, I]
+        lib.ref_sort_gather_d.argtypes = [S, I, I, D, D, I, I, I, LL, V, V, V, I]
+        lib.ref_sort_put2d_f.argtypes = [S, S, I, I, D, D, V]
     lib.ref_revolve_numforw.argtypes = [I, I]
     lib.ref_revolve_adjust.argtypes = [I]
     lib.ref_steps_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, I, V]
@@ -591,3 +600,43 @@ def ref_steps_e3d(pb, scoords, wav, sfield, nsteps, state=None):
                               0 if state is None else 1, _p(st))
     assert r == 1
     return st
+
+
+# ---------------------------------------------------------------- shot-gather files and sorting
+def ref_data_write(path, dim, nt, dt, ot, scoords, gcoords, data, dtype=np.float32):
+    """Data2D::write (dim 2) / Data3D::write (dim 3) of the reference."""
+    sc, gc, d = _keep(scoords, gcoords, data, dtype=dtype)
+    fn = ref().ref_data_write_f if dtype == np.float32 else ref().ref_data_write_d
+    assert fn(str(path).encode(), dim, nt, dt, ot, len(d), _p(sc), _p(gc), _p(d)) == 1
+
+
+def ref_data_read2d(path, nt, ntrace):
+    sc = np.zeros((ntrace, 2), np.float32)
+    gc = np.zeros((ntrace, 2), np.float32)
+    d = np.zeros((ntrace, nt), np.float32)
+    assert ref().ref_data_read2d_f(str(path).encode(), nt, ntrace, _p(sc), _p(gc), _p(d)) == 1
+    return sc, gc, d
+
+
+def ref_model_write(path, vp, dx, dz, ox, oz):
+    v = np.ascontiguousarray(vp, np.float32)
+    nz, nx = v.shape
+    assert ref().ref_model_write_f(str(path).encode(), nx, nz, dx, dz, ox, oz, _p(v)) == 1
+
+
+def ref_sort_gather(path, dim, key, number, nt, dx=0.0, dy=0.0, order=0, reciprocity=0, dtype=np.float32, maxtr=4096):
+    """Sort::create*map then get2DGather/get3DGather(number): (ngathers, scoords, gcoords, data)."""
+    sc = np.zeros((maxtr, dim), dtype)
+    gc = np.zeros((maxtr, dim), dtype)
+    d = np.zeros((maxtr, nt), dtype)
+    ng = C.c_longlong()
+    fn = ref().ref_sort_gather_f if dtype == np.float32 else ref().ref_sort_gather_d
+    n = fn(str(path).encode(), dim, key, dx, dy, order, number, reciprocity, C.byref(ng), _p(sc), _p(gc), _p(d),
+           maxtr)
+    assert n >= 0, n
+    return ng.value, sc[:n], gc[:n], d[:n]
+
+
+def ref_sort_put2d(survey, out, number, n1, d1, o1, data):
+    d = np.ascontiguousarray(data, np.float32)
+    return ref().ref_sort_put2d_f(str(survey).encode(), str(out).encode(), number, n1, d1, o1, _p(d))

@@ -71,6 +71,17 @@ class AdjointShot(C.Structure):
                 ("srcilum", C.c_void_p)]
 
 
+class RssHeader(C.Structure):
+    _fields_ = [("data_format", C.c_int), ("header_format", C.c_int), ("type", C.c_int),
+                ("nheader", C.c_longlong), ("ndims", C.c_longlong), ("n", C.c_longlong * 9),
+                ("d", C.c_double * 9), ("o", C.c_double * 9)]
+
+
+RSS_GENERIC, RSS_REGULAR, RSS_DATA2D, RSS_DATA3D = 0, 1, 2, 3
+SORT_SOURCE, SORT_RECEIVER, SORT_CMP = 0, 1, 2
+GATHER_FINISHED, GATHER_RUNNING, GATHER_NOT_STARTED, GATHER_FAILED = 0, 1, 2, 3
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `python -m rockseis_b200.build`")
@@ -112,6 +123,21 @@ def _load() -> C.CDLL:
         "rsgpu_adjoint_stats": (I, [V] + [P(C.c_longlong)] * 4),
         "rsgpu_adjoint_stream": (V, [V]),
         "rsgpu_adjoint_destroy": (None, [V]),
+        "rsgpu_rss_read_header": (I, [C.c_char_p, P(RssHeader)]),
+        "rsgpu_rss_write_traces": (I, [C.c_char_p, I, I, C.c_longlong, D, D, C.c_longlong, V, V, V]),
+        "rsgpu_rss_read_traces": (I, [C.c_char_p, I, C.c_longlong, C.c_longlong, V, V, V]),
+        "rsgpu_rss_write_model": (I, [C.c_char_p, I, I, I, I, D, D, D, D, D, D, V]),
+        "rsgpu_rss_read_model": (I, [C.c_char_p, I, C.c_longlong, V]),
+        "rsgpu_sort_create": (I, [C.c_char_p, I, D, D, I, P(V)]),
+        "rsgpu_sort_destroy": (None, [V]),
+        "rsgpu_sort_info": (I, [V, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]),
+        "rsgpu_sort_gather_size": (C.c_longlong, [V, C.c_longlong]),
+        "rsgpu_sort_next": (C.c_longlong, [V]),
+        "rsgpu_sort_status": (I, [V, C.c_longlong]),
+        "rsgpu_sort_set_status": (I, [V, C.c_longlong, I]),
+        "rsgpu_sort_read_gather": (I, [V, C.c_longlong, I, V, V, V]),
+        "rsgpu_sort_create_output": (I, [V, C.c_char_p, C.c_longlong, D, D]),
+        "rsgpu_sort_write_gather": (I, [V, C.c_char_p, C.c_longlong, I, C.c_longlong, V, V, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

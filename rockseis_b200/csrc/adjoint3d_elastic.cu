@@ -8,11 +8,13 @@
 // Memory-bound passes; one launch covers every shot (blockIdx.z selects it).  The
 // correlation marches z with one thread per (x, y) column of the unpadded window.
 //
-// The per-point arithmetic is the reference's, operation for operation (see
-// adjoint_ops.cuh): in ACCUM_REFERENCE mode the three gradients are float arrays
-// updated exactly as the reference updates them, including the mu correlation's
-// thirteen separate double-rounded subtractions; in ACCUM_F64 mode the same
-// per-step terms are subtracted from double accumulators.
+// The exact (and FP64) kernel evaluates each point's arithmetic as the reference
+// does, operation for operation (see adjoint_ops.cuh): with ACCUM_REFERENCE the three
+// gradients are float arrays updated exactly as the reference updates them,
+// including the mu correlation's thirteen separate double-rounded subtractions;
+// with ACCUM_F64 the same per-step terms are subtracted from double accumulators.
+// The FAST kernel sums each gradient's terms in float with multiply-adds and
+// subtracts one term per gradient and step.
 #include <cuda_runtime.h>
 
 #include "adjoint_ops.cuh"
@@ -133,6 +135,81 @@ __global__ void __launch_bounds__(256) corr_fwi_e3d(const Corr3DE<T> *desc, T dx
     }
 }
 
+// FAST arithmetic (float, reciprocal spacings, contracted multiply-adds) of the same
+// correlation: the three gradients take one summed term per step each.  The z-march
+// keeps in registers the values that the next plane reuses (z-1 / z / z+1 of the
+// columns whose z-derivatives appear, and the rz of the plane below), so a point
+// loads 49 values instead of about 100; x and y neighbours come from L1.
+template <typename G>
+__global__ void __launch_bounds__(256) corr_fwi_e3d_fast(const Corr3DE<float> *desc, float idx, float idy, float idz)
+{
+    const Corr3DE<float> c = desc[blockIdx.z];
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix < 1 || iy < 1 || ix >= c.nx - 1 || iy >= c.ny - 1 || c.nz < 3) return;
+    const long long P = c.pitch, PL = c.plane;
+    const int L = c.lpml;
+    const float *__restrict__ wsx = c.ws[0], *__restrict__ wsy = c.ws[1], *__restrict__ wsz = c.ws[2];
+    const float *__restrict__ fsxx = c.ws[3], *__restrict__ fsyy = c.ws[4], *__restrict__ fszz = c.ws[5];
+    const float *__restrict__ fsyz = c.ws[6], *__restrict__ fsxz = c.ws[7], *__restrict__ fsxy = c.ws[8];
+    const float *__restrict__ wrx = c.wr[0], *__restrict__ wry = c.wr[1], *__restrict__ wrz = c.wr[2];
+    const float *__restrict__ rsxx = c.wr[3], *__restrict__ rsyy = c.wr[4], *__restrict__ rszz = c.wr[5];
+    const float *__restrict__ rsyz = c.wr[6], *__restrict__ rsxz = c.wr[7], *__restrict__ rsxy = c.wr[8];
+    const float *__restrict__ rx = c.rx, *__restrict__ ry = c.ry, *__restrict__ rz = c.rz;
+    long long q = (long long)(1 + L) * PL + (long long)(iy + L) * P + (ix + L);
+    long long u = ((long long)c.ny + iy) * c.nx + ix;
+    const long long un = (long long)c.ny * c.nx;
+    // values carried from plane to plane: (array, column) at z-1 ("m") and z
+    float sx0m = wsx[q - PL], sx0 = wsx[q], sx1m = wsx[q - 1 - PL], sx1 = wsx[q - 1];
+    float sy0m = wsy[q - PL], sy0 = wsy[q], sy1m = wsy[q - P - PL], sy1 = wsy[q - P];
+    float sz0m = wsz[q - PL], szymm = wsz[q - P - PL], szypm = wsz[q + P - PL];
+    float szxmm = wsz[q - 1 - PL], szxpm = wsz[q + 1 - PL];
+    float xz0m = fsxz[q - PL], xz1m = fsxz[q - 1 - PL], yz0m = fsyz[q - PL], yz1m = fsyz[q - P - PL];
+    float zzm = fszz[q - PL], zz0 = fszz[q], rzm = rz[q - PL];
+    for (int iz = 1; iz < c.nz - 1; iz++, q += PL, u += un) {
+        const float sx0p = wsx[q + PL], sx1p = wsx[q - 1 + PL], sy0p = wsy[q + PL], sy1p = wsy[q - P + PL];
+        const float zzp = fszz[q + PL];
+        const float sz0 = wsz[q], szym = wsz[q - P], szyp = wsz[q + P], szxm = wsz[q - 1], szxp = wsz[q + 1];
+        const float sxym = wsx[q - P], sxyp = wsx[q + P], sxxmym = wsx[q - 1 - P], sxxmyp = wsx[q - 1 + P];
+        const float syxm = wsy[q - 1], syxp = wsy[q + 1], syymxm = wsy[q - P - 1], syymxp = wsy[q - P + 1];
+        const float xx0 = fsxx[q], xxp = fsxx[q + 1], xxm = fsxx[q - 1];
+        const float xy0 = fsxy[q], xyym = fsxy[q - P], xyxm = fsxy[q - 1], xyxmym = fsxy[q - 1 - P];
+        const float xz0 = fsxz[q], xz1 = fsxz[q - 1], yz0 = fsyz[q], yz1 = fsyz[q - P];
+        const float yy0 = fsyy[q], yyp = fsyy[q + P], yym = fsyy[q - P];
+        const float wq = wrx[q] * rx[q], wm = wrx[q - 1] * rx[q - 1];
+        const float vq = wry[q] * ry[q], vm = wry[q - P] * ry[q - P];
+        const float rz0 = rz[q];
+        const float zq = wrz[q] * rz0, zmm = wrz[q - P] * rzm;
+        const float rxx = rsxx[q], ryy = rsyy[q], rzz = rszz[q], ryz = rsyz[q], rxz = rsxz[q], rxy = rsxy[q];
+
+        const float msxx = (sx0 - sx1) * idx, msyy = (sy0 - sy1) * idy, mszz = (sz0 - sz0m) * idz;
+        const float a = (msxx + msyy + mszz) * (rxx + ryy + rzz);
+        const float myz = ((sy1 - sy1m) * idz + (sz0m - szymm) * idy) + ((sy0 - sy0m) * idz + (szypm - sz0m) * idy) +
+                          ((sy1p - sy1) * idz + (sz0 - szym) * idy) + ((sy0p - sy0) * idz + (szyp - sz0) * idy);
+        const float mxz = ((sx1 - sx1m) * idz + (sz0m - szxmm) * idx) + ((sx0 - sx0m) * idz + (szxpm - sz0m) * idx) +
+                          ((sx1p - sx1) * idz + (sz0 - szxm) * idx) + ((sx0p - sx0) * idz + (szxp - sz0) * idx);
+        const float mxy = ((sy1 - syymxm) * idx + (sx1 - sxxmym) * idy) + ((syymxp - sy1) * idx + (sx0 - sxym) * idy) +
+                          ((sy0 - syxm) * idx + (sxxmyp - sx1) * idy) + ((syxp - sy0) * idx + (sxyp - sx0) * idy);
+        const float mu = 2.0f * (msxx * rxx + msyy * ryy + mszz * rzz) + 0.25f * (myz * ryz + mxz * rxz + mxy * rxy);
+        const float ux = wq * ((xxp - xx0) * idx + (xy0 - xyym) * idy + (xz0 - xz0m) * idz) +
+                         wm * ((xx0 - xxm) * idx + (xyxm - xyxmym) * idy + (xz1 - xz1m) * idz);
+        const float uy = vq * ((xy0 - xyxm) * idx + (yyp - yy0) * idy + (yz0 - yz0m) * idz) +
+                         vm * ((xyym - xyxmym) * idx + (yy0 - yym) * idy + (yz1 - yz1m) * idz);
+        const float uz = zq * ((xz0 - xz1) * idx + (yz0 - yz1) * idy + (zzp - zz0) * idz) +
+                         zmm * ((xz0m - xz1m) * idx + (yz0m - yz1m) * idy + (zz0 - zzm) * idz);
+        const float rh = 0.5f * (ux + uy + uz);
+        G *g0 = (G *)c.g[0] + u, *g1 = (G *)c.g[1] + u, *g2 = (G *)c.g[2] + u;
+        *g0 -= (G)a;
+        *g1 -= (G)mu;
+        *g2 -= (G)rh;
+        sx0m = sx0; sx0 = sx0p; sx1m = sx1; sx1 = sx1p;
+        sy0m = sy0; sy0 = sy0p; sy1m = sy1; sy1 = sy1p;
+        sz0m = sz0; szymm = szym; szypm = szyp; szxmm = szxm; szxpm = szxp;
+        xz0m = xz0; xz1m = xz1; yz0m = yz0; yz1m = yz1;
+        zzm = zz0; zz0 = zzp; rzm = rz0;
+    }
+}
+
 // FwiElastic3D::scaleGrad over the whole window:
 //   vp  <- 2 rho vp lambda
 //   vs  <- 2 rho vs mu - 2 (2 rho vs) lambda
@@ -213,7 +290,11 @@ cudaError_t launch_corr_fwi_e3d(int prec, int acc, const void *desc, int nshots,
                                 double dy, double dz, cudaStream_t st)
 {
     const dim3 block(32, 8), grid((nxmax + 31) / 32, (nymax + 7) / 8, nshots);
-    if (prec == PREC_F64)
+    if (prec == PREC_F32_FAST) {
+        const float ix = (float)(1.0 / dx), iy = (float)(1.0 / dy), iz = (float)(1.0 / dz);
+        if (acc == ACC_F64) corr_fwi_e3d_fast<double><<<grid, block, 0, st>>>((const Corr3DE<float> *)desc, ix, iy, iz);
+        else corr_fwi_e3d_fast<float><<<grid, block, 0, st>>>((const Corr3DE<float> *)desc, ix, iy, iz);
+    } else if (prec == PREC_F64)
         corr_fwi_e3d<double, double><<<grid, block, 0, st>>>((const Corr3DE<double> *)desc, dx, dy, dz);
     else if (acc == ACC_F64)
         corr_fwi_e3d<float, double><<<grid, block, 0, st>>>((const Corr3DE<float> *)desc, (float)dx, (float)dy,

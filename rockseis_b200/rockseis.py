@@ -292,6 +292,38 @@ class Data2D:
     def getField(self): return self.field
     def setField(self, f): self.field = int(f)
     def setReciprocity(self, v): self.reciprocity = bool(v)
+    def setFile(self, path): self.file = str(path)
+    def getFile(self): return getattr(self, "file", "")
+
+    def write(self):
+        """Data2D::write / Data3D::write (lib/data.cpp:580-635, 1265-1320): the traces
+        and their source/receiver coordinates to the .rss file set with setFile."""
+        check(abi.lib.rsgpu_rss_write_traces(self.getFile().encode(), self.precision, self.dim, self.nt,
+                                             float(self.dt), float(self.ot), self.ntrace,
+                                             ptr(np.ascontiguousarray(self.scoords)),
+                                             ptr(np.ascontiguousarray(self.gcoords)),
+                                             ptr(np.ascontiguousarray(self.data))))
+        return 1
+
+    def read(self):
+        """Data2D::read (lib/data.cpp:463-506): traces and coordinates from the file;
+        the file's sample count must equal nt."""
+        h = rss_header(self.getFile())
+        if h.n[0] != self.nt:
+            raise abi.RsgpuError(abi.ERR_ARG, f"Data2D::read: Nt in {self.getFile()} is different from nt")
+        n = min(self.ntrace, int(h.n[1]))
+        check(abi.lib.rsgpu_rss_read_traces(self.getFile().encode(), self.precision, 0, n, ptr(self.scoords),
+                                            ptr(self.gcoords), ptr(self.data)))
+        return 1
+
+    @classmethod
+    def fromFile(cls, path, precision=abi.F32_EXACT):
+        """A container sized and filled from an .rss trace file."""
+        h = rss_header(path)
+        d = cls(int(h.n[1]), int(h.n[0]), h.d[0], h.o[0], precision)
+        d.setFile(path)
+        d.read()
+        return d
 
     def makeMap(self, model: _Model, which=None):
         """Geometry2D::makeMap: coordinates -> (cell, fractional shift); -1 if off the grid."""
@@ -322,6 +354,91 @@ class Data2D:
 class Data3D(Data2D):
     """Trace container (Data3D<T>): coordinates and maps (x, y, z)."""
     dim = 3
+
+
+def rss_header(path) -> abi.RssHeader:
+    """File::readHeader (lib/file.cpp:221-250)."""
+    h = abi.RssHeader()
+    check(abi.lib.rsgpu_rss_read_header(str(path).encode(), C.byref(h)))
+    return h
+
+
+class Sort:
+    """Sort<T> (include/sort.h, lib/sort.cpp): gathers of an .rss trace file by source,
+    receiver or CMP position, and the gather queue (NOT_STARTED / RUNNING / FINISHED /
+    FAILED) the MPI drivers hand out."""
+
+    def __init__(self, precision=abi.F32_EXACT):
+        self.precision = precision
+        self.dtype = abi.real_dtype(precision)
+        self.reciprocity = False
+        self.h = C.c_void_p()
+        self.dim = 2
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            abi.lib.rsgpu_sort_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def setReciprocity(self, v): self.reciprocity = bool(v)
+    def getReciprocity(self): return self.reciprocity
+
+    def _create(self, path, key, dx=0.0, dy=0.0, order=0):
+        if self.h:
+            abi.lib.rsgpu_sort_destroy(self.h)
+            self.h = C.c_void_p()
+        check(abi.lib.rsgpu_sort_create(str(path).encode(), key, float(dx), float(dy), int(order), C.byref(self.h)))
+        self.file = str(path)
+        self.dim = 3 if rss_header(path).type == abi.RSS_DATA3D else 2
+        return True
+
+    def createShotmap(self, path, order=0): return self._create(path, abi.SORT_SOURCE, 0.0, 0.0, order)
+    def createReceivermap(self, path, order=0): return self._create(path, abi.SORT_RECEIVER, 0.0, 0.0, order)
+    def createCMPmap(self, path, dx, dy, order=0): return self._create(path, abi.SORT_CMP, dx, dy, order)
+
+    def _info(self):
+        ng, ntr, nt = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        check(abi.lib.rsgpu_sort_info(self.h, C.byref(ng), C.byref(ntr), C.byref(nt)))
+        return ng.value, ntr.value, nt.value
+
+    def getNensemb(self): return self._info()[0]
+    def getNtraces(self): return self._info()[1]
+    def getStatus(self, number): return abi.lib.rsgpu_sort_status(self.h, int(number))
+    def setStatus(self, number, status): check(abi.lib.rsgpu_sort_set_status(self.h, int(number), int(status)))
+
+    def get2DGather(self, number=None):
+        """Sort::get2DGather(number), or without a number the next gather not started or
+        failed (None when every gather is running or finished); marks it RUNNING."""
+        if number is None:
+            number = abi.lib.rsgpu_sort_next(self.h)
+            if number < 0:
+                return None
+        n = abi.lib.rsgpu_sort_gather_size(self.h, int(number))
+        if n < 0:
+            raise abi.RsgpuError(abi.ERR_ARG, f"Sort::get2DGather: no gather {number}")
+        _, _, nt = self._info()
+        h = rss_header(self.file)
+        g = (Data3D if self.dim == 3 else Data2D)(n, nt, h.d[0], h.o[0], self.precision)
+        check(abi.lib.rsgpu_sort_read_gather(self.h, int(number), int(self.reciprocity), ptr(g.scoords),
+                                             ptr(g.gcoords), ptr(g.data)))
+        g.setReciprocity(self.reciprocity)
+        g.number = int(number)
+        return g
+
+    get3DGather = get2DGather
+
+    def createEmptydataset(self, path, n1, d1, o1):
+        """Sort::createEmptydataset (lib/sort.cpp:999-1055)."""
+        check(abi.lib.rsgpu_sort_create_output(self.h, str(path).encode(), int(n1), float(d1), float(o1)))
+
+    def put2DGather(self, data, number):
+        """Sort::put2DGather (lib/sort.cpp:535-579): the gather into the file data.getFile()."""
+        check(abi.lib.rsgpu_sort_write_gather(self.h, data.getFile().encode(), int(number), int(self.reciprocity),
+                                              data.nt, ptr(np.ascontiguousarray(data.scoords)),
+                                              ptr(np.ascontiguousarray(data.gcoords)),
+                                              ptr(np.ascontiguousarray(data.data))))
+
+    put3DGather = put2DGather
 
 
 def check_stability(model: _Model, dt: float, cls: str) -> None:
