@@ -295,6 +295,17 @@ rsgpu_status rsgpu_adjoint_create(const rsgpu_config *cfg, const rsgpu_adjoint_o
                                   const rsgpu_adjoint_shot *shots, rsgpu_adjoint **adj);
 rsgpu_status rsgpu_adjoint_run(rsgpu_adjoint *adj);
 rsgpu_status rsgpu_adjoint_read(rsgpu_adjoint *adj, int nshots, const rsgpu_adjoint_shot *shots);
+/* Image2D::stackImage (lib/image.cpp:348-438) of the last run's per-shot results
+ * into global images, done on the device (the reference stacks per-shot files on
+ * the master, Inversion*::runGrad lib/inversion.cpp:309-321): shot i's window is
+ * added at global column ix_start[i] and row iz_start[i] (the reference's
+ * (int)(ox_local/dx - ox_global/dx) in the element type; parts outside the global
+ * grid are dropped), shots in batch order, onto the running global images held in
+ * the host arrays out* (uploaded, stacked, written back: batch after batch this is
+ * the reference's shot-by-shot stack): FWI acoustic (vpgrad, rhograd), elastic
+ * (vpgrad, vsgrad, rhograd), RTM (image with its lags, out0).  2D drivers. */
+rsgpu_status rsgpu_adjoint_stack(rsgpu_adjoint *adj, int nxg, int nzg, const int *ix_start, const int *iz_start,
+                                 void *out0, void *out1, void *out2);
 /* forward steps, adjoint steps, checkpoint bytes written + read, kernel launches */
 rsgpu_status rsgpu_adjoint_stats(rsgpu_adjoint *adj, long long *fw_steps, long long *bw_steps,
                                  long long *ckpt_bytes, long long *launches);

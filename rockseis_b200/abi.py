@@ -123,6 +123,7 @@ def _load() -> C.CDLL:
         "rsgpu_adjoint_stats": (I, [V] + [P(C.c_longlong)] * 4),
         "rsgpu_adjoint_stream": (V, [V]),
         "rsgpu_adjoint_destroy": (None, [V]),
+        "rsgpu_adjoint_stack": (I, [V, I, I, P(I), P(I), V, V, V]),
         "rsgpu_rss_read_header": (I, [C.c_char_p, P(RssHeader)]),
         "rsgpu_rss_write_traces": (I, [C.c_char_p, I, I, C.c_longlong, D, D, C.c_longlong, V, V, V]),
         "rsgpu_rss_read_traces": (I, [C.c_char_p, I, C.c_longlong, C.c_longlong, V, V, V]),

@@ -60,6 +60,7 @@ public:
                         const rsgpu_adjoint_shot *s);
     rsgpu_status run();
     rsgpu_status read(int ns, const rsgpu_adjoint_shot *s);
+    rsgpu_status stack(int nxg, int nzg, const int *x0, const int *z0, void *const *out);
 
     int kind = RSGPU_KIND_FWI, phys = PHYS_A2D, nshots = 0, prec = 0, es = 4, acc = ACC_REF, ck = CK_NATIVE;
     int nhx = 1, nhz = 1;
@@ -730,6 +731,71 @@ static void add_into(void *host, const std::vector<unsigned char> &dev, size_t n
     for (size_t k = 0; k < n; k++) o[k] = (T)((G)o[k] + d[k]);
 }
 
+// Image2D::stackImage of every shot's window into global arrays, on the device: the
+// host arrays out[] (element type) are the running global images; they are uploaded,
+// every shot's window is added in shot order and the result is written back, so a
+// sequence of batches stacks exactly as the reference's shot-by-shot stackImage
+// does.  Components: FWI acoustic vpgrad, rhograd; elastic vpgrad, vsgrad, rhograd;
+// RTM the image with its lags.
+rsgpu_status Adjoint::stack(int nxg, int nzg, const int *x0, const int *z0, void *const *out)
+{
+    if (!ran) { set_error("no run to stack"); return RSGPU_ERR_STATE; }
+    if (nxg < 1 || nzg < 1 || !x0 || !z0 || !out) { set_error("stack: bad arguments"); return RSGPU_ERR_ARG; }
+    const int ncomp = kind == RSGPU_KIND_RTM ? 1 : elastic() ? 3 : 2;
+    const int nh = kind == RSGPU_KIND_RTM ? nhx * nhz : 1;
+    const size_t gs = acc == ACC_F64 ? 8 : (size_t)es;
+    std::vector<StackWin> w(nshots);
+    for (int i = 0; i < nshots; i++) {
+        w[i].g[0] = D(o_g0[i]);
+        w[i].g[1] = kind == RSGPU_KIND_FWI ? D(o_g1[i]) : nullptr;
+        w[i].g[2] = elastic() ? D(o_g2[i]) : nullptr;
+        w[i].nx = nx[i];
+        w[i].nz = nz[i];
+        w[i].x0 = x0[i];
+        w[i].z0 = z0[i];
+    }
+    const size_t n = (size_t)nxg * nzg * nh;
+    void *buf = nullptr;
+    const size_t bytes = gs * n * ncomp + sizeof(StackWin) * nshots;
+    if (dev_alloc(&buf, bytes, stream) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("stack: device allocation of %zu bytes failed", bytes);
+        return RSGPU_ERR_NOMEM;
+    }
+    char *b = (char *)buf;
+    StackWin *dw = (StackWin *)(b + gs * n * ncomp);
+    rsgpu_status st = RSGPU_OK;
+    // the running global images in the accumulator type (a missing output stacks from zero)
+    std::vector<unsigned char> tmp(gs * n * ncomp, 0);
+    for (int c = 0; c < ncomp; c++) {
+        if (!out[c]) continue;
+        unsigned char *t = tmp.data() + c * gs * n;
+        if (gs == (size_t)es) std::memcpy(t, out[c], gs * n);
+        else for (size_t k = 0; k < n; k++) ((double *)t)[k] = (double)((const float *)out[c])[k];
+    }
+    cudaError_t e = cudaMemcpyAsync(b, tmp.data(), gs * n * ncomp, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dw, w.data(), sizeof(StackWin) * nshots, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = launch_stack_windows((int)gs, dw, nshots, ncomp, nxg, nzg, nh, b, ncomp > 1 ? b + gs * n : nullptr,
+                                 ncomp > 2 ? b + 2 * gs * n : nullptr, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp.data(), b, gs * n * ncomp, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    for (int c = 0; c < ncomp && e == cudaSuccess; c++) {
+        if (!out[c]) continue;
+        const unsigned char *t = tmp.data() + c * gs * n;
+        if (gs == (size_t)es) std::memcpy(out[c], t, gs * n);
+        else for (size_t k = 0; k < n; k++) ((float *)out[c])[k] = (float)((const double *)t)[k];
+    }
+    if (e != cudaSuccess) {
+        set_error("stack: %s", cudaGetErrorString(e));
+        st = RSGPU_ERR_CUDA;
+    }
+    cudaStreamSynchronize(stream);
+    dev_free(buf, stream);
+    return st;
+}
+
+
 rsgpu_status Adjoint::read(int ns, const rsgpu_adjoint_shot *s)
 {
     if (!ran) { set_error("no run to read"); return RSGPU_ERR_STATE; }
@@ -831,6 +897,15 @@ rsgpu_status rsgpu_adjoint_read(rsgpu_adjoint *adj, int nshots, const rsgpu_adjo
 {
     if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
     return adj->a3 ? adj->a3->read(nshots, shots) : adj->a->read(nshots, shots);
+}
+
+rsgpu_status rsgpu_adjoint_stack(rsgpu_adjoint *adj, int nxg, int nzg, const int *ix_start, const int *iz_start,
+                                 void *out0, void *out1, void *out2)
+{
+    if (!adj) { set_error("null handle"); return RSGPU_ERR_ARG; }
+    if (adj->a3) { set_error("stacking is built for the 2D drivers"); return RSGPU_ERR_UNSUPPORTED; }
+    void *out[3] = {out0, out1, out2};
+    return adj->a->stack(nxg, nzg, ix_start, iz_start, out);
 }
 
 rsgpu_status rsgpu_adjoint_stats(rsgpu_adjoint *adj, long long *fw_steps, long long *bw_steps, long long *ckpt_bytes,

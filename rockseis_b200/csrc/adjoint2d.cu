@@ -848,6 +848,33 @@ cudaError_t launch_residual_corr_e2d(int prec, int acc, const void *desc, int ns
     return cudaGetLastError();
 }
 
+// Image2D::stackImage (lib/image.cpp:348-438) of every shot's window into one global
+// image per component: one thread per global point (and lag), the shots added in
+// their order, each where its window covers the point.
+template <typename G>
+__global__ void __launch_bounds__(256) stack_windows(const StackWin *w, int nshots, int ncomp, int nxg, int nzg, int nh,
+                                                     G *out0, G *out1, G *out2)
+{
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ng = (long long)nxg * nzg;
+    if (k >= ng * nh) return;
+    const int ih = (int)(k / ng);
+    const int iz = (int)((k % ng) / nxg), ix = (int)(k % nxg);
+    G *out[3] = {out0, out1, out2};
+    for (int c = 0; c < ncomp; c++) {
+        G acc = out[c][k];
+        for (int i = 0; i < nshots; i++) {
+            const StackWin &s = w[i];
+            const int lx = ix - s.x0, lz = iz - s.z0;
+            if (lx < 0 || lx >= s.nx || lz < 0 || lz >= s.nz) continue;
+            const G v = ((const G *)s.g[c])[((long long)ih * s.nz + lz) * s.nx + lx];
+            if (sizeof(G) == 4) acc = (G)__fadd_rn((float)acc, (float)v);
+            else acc = (G)__dadd_rn((double)acc, (double)v);
+        }
+        out[c][k] = acc;
+    }
+}
+
 template <typename T, int ACC>
 void residual_t(const void *desc, int nshots, double *misfit, double *partials, cudaStream_t st)
 {
@@ -856,6 +883,20 @@ void residual_t(const void *desc, int nshots, double *misfit, double *partials, 
 }
 
 size_t residual_partials(int nshots) { return (size_t)nshots * RES_BLOCKS; }
+
+cudaError_t launch_stack_windows(int gbytes, const StackWin *w, int nshots, int ncomp, int nxg, int nzg, int nh,
+                                 void *out0, void *out1, void *out2, cudaStream_t st)
+{
+    const long long n = (long long)nxg * nzg * nh;
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (gbytes == 8)
+        stack_windows<double><<<grid, 256, 0, st>>>(w, nshots, ncomp, nxg, nzg, nh, (double *)out0, (double *)out1,
+                                                     (double *)out2);
+    else
+        stack_windows<float><<<grid, 256, 0, st>>>(w, nshots, ncomp, nxg, nzg, nh, (float *)out0, (float *)out1,
+                                                   (float *)out2);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_residual(int prec, int acc, const void *desc, int nshots, double *misfit, double *partials,
                             cudaStream_t st)

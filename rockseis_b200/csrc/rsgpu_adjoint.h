@@ -98,6 +98,17 @@ struct Resid2D {
     T *tnorm;                   // ADAPTIVE misfits: the shaping filter's squared norm per trace
 };
 
+// One shot's window of gradients / image for the global stack: component arrays of
+// the accumulator type, [nh][nz][nx], placed at (x0, z0) of the global grid.
+struct StackWin {
+    const void *g[3];
+    int nx, nz, x0, z0;
+};
+// Adds every shot's window into the global arrays out0..out2 (nxg*nzg*nh values of
+// gbytes-byte type, components beyond ncomp unused), shots in order.
+cudaError_t launch_stack_windows(int gbytes, const StackWin *w, int nshots, int ncomp, int nxg, int nzg, int nh,
+                                 void *out0, void *out1, void *out2, cudaStream_t st);
+
 // One contiguous 2D block of state copied into / out of a checkpoint slot.
 struct CkptSeg {
     void *src;                  // first element

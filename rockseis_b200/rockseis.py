@@ -1038,6 +1038,16 @@ class AdjointBatch:
                 j.misfit += j._mis.value
                 j._mis.value = 0.0
 
+    def stack(self, nxg, nzg, ix_start, iz_start, out0, out1=None, out2=None):
+        """Image2D::stackImage of every shot's result into global images, on the device
+        (rsgpu_adjoint_stack); out* are the running global images (host arrays of the
+        element type), updated in place."""
+        x0 = np.ascontiguousarray(ix_start, np.int32)
+        z0 = np.ascontiguousarray(iz_start, np.int32)
+        check(abi.lib.rsgpu_adjoint_stack(self.h, int(nxg), int(nzg), x0.ctypes.data_as(C.POINTER(C.c_int)),
+                                          z0.ctypes.data_as(C.POINTER(C.c_int)),
+                                          *[ptr(o) if o is not None else None for o in (out0, out1, out2)]))
+
     def stats(self):
         v = [C.c_longlong() for _ in range(4)]
         check(abi.lib.rsgpu_adjoint_stats(self.h, *[C.byref(x) for x in v]))
