@@ -1414,6 +1414,49 @@ cudaError_t launch_step_e3d(int prec, int half, int adj, const void *args, const
     return adj ? step_e3_fast<true>(half, args, coefs, grid, st) : step_e3_fast<false>(half, args, coefs, grid, st);
 }
 
+// Work arrays of the adjoint velocity step (FAST arithmetic), the operands that
+// opnd<.., ADJ=true> forms per tap, computed once per point over a shot's whole field
+// allocation: W_xx = L2M Sxx + L Syy + L Szz, W_yy, W_zz likewise, W_yz = M_yz Syz,
+// W_xz = M_xz Sxz, W_xy = M_xy Sxy.  The forward TMA velocity kernel then
+// differentiates them as it differentiates stresses.  Four values per thread.
+__global__ void __launch_bounds__(256) e3d_work_arrays(const WorkE3 *desc)
+{
+    using A = Ar<float, MODE_FAST>;
+    const WorkE3 &e = desc[blockIdx.y];
+    const long long n4 = e.n / 4;
+    auto ld = [](const float *p, long long k) { return __ldg(reinterpret_cast<const float4 *>(p) + k); };
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += (long long)gridDim.x * blockDim.x) {
+        const float4 sxx = ld(e.s[0], k), syy = ld(e.s[1], k), szz = ld(e.s[2], k);
+        const float4 l = ld(e.l, k), l2m = ld(e.l2m, k);
+        float4 wxx, wyy, wzz;
+        const float *pxx = &sxx.x, *pyy = &syy.x, *pzz = &szz.x, *pl = &l.x, *pl2m = &l2m.x;
+        float *oxx = &wxx.x, *oyy = &wyy.x, *ozz = &wzz.x;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            oxx[c] = A::add(A::add(A::mul(pl2m[c], pxx[c]), A::mul(pl[c], pyy[c])), A::mul(pl[c], pzz[c]));
+            oyy[c] = A::add(A::add(A::mul(pl[c], pxx[c]), A::mul(pl2m[c], pyy[c])), A::mul(pl[c], pzz[c]));
+            ozz[c] = A::add(A::add(A::mul(pl[c], pxx[c]), A::mul(pl[c], pyy[c])), A::mul(pl2m[c], pzz[c]));
+        }
+        reinterpret_cast<float4 *>(e.w[0])[k] = wxx;
+        reinterpret_cast<float4 *>(e.w[1])[k] = wyy;
+        reinterpret_cast<float4 *>(e.w[2])[k] = wzz;
+        const float4 syz = ld(e.s[3], k), sxz = ld(e.s[4], k), sxy = ld(e.s[5], k);
+        const float4 myz = ld(e.myz, k), mxz = ld(e.mxz, k), mxy = ld(e.mxy, k);
+        reinterpret_cast<float4 *>(e.w[3])[k] = make_float4(A::mul(myz.x, syz.x), A::mul(myz.y, syz.y),
+                                                            A::mul(myz.z, syz.z), A::mul(myz.w, syz.w));
+        reinterpret_cast<float4 *>(e.w[4])[k] = make_float4(A::mul(mxz.x, sxz.x), A::mul(mxz.y, sxz.y),
+                                                            A::mul(mxz.z, sxz.z), A::mul(mxz.w, sxz.w));
+        reinterpret_cast<float4 *>(e.w[5])[k] = make_float4(A::mul(mxy.x, sxy.x), A::mul(mxy.y, sxy.y),
+                                                            A::mul(mxy.z, sxy.z), A::mul(mxy.w, sxy.w));
+    }
+}
+
+cudaError_t launch_work_e3d(const void *desc, int nshots, cudaStream_t st)
+{
+    e3d_work_arrays<<<dim3(4 * 148, (unsigned)nshots), 256, 0, st>>>((const WorkE3 *)desc);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_injrec_e3d(int prec, const void *shots, const void *plans, int nshots, int nsets, double dt,
                               int it, cudaStream_t st)
 {

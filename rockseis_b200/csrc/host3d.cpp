@@ -34,10 +34,27 @@ namespace rsgpu {
 
 static inline size_t rup3(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
+// Index of the work array that stands in for field slot k in the adjoint velocity
+// step (WorkE3 order: Sxx, Syy, Szz, Syz, Sxz, Sxy), -1 for the other slots.
+static int work_slot(int k)
+{
+    switch (k) {
+    case E3_SXX: return 0;
+    case E3_SYY: return 1;
+    case E3_SZZ: return 2;
+    case E3_SYZ: return 3;
+    case E3_SXZ: return 4;
+    case E3_SXY: return 5;
+    default: return -1;
+    }
+}
+
+
 Plan3D::~Plan3D()
 {
     dev_free(arena, stream);
     dev_free(d_meta, stream);
+    dev_free(d_work, stream);
     if (stream && stream != shared_stream) cudaStreamDestroy(stream);
 }
 
@@ -349,8 +366,23 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     // elastic fast mode: the tensor maps of the TMA-staged kernels
     const bool tma = phys == PHYS_E3D && prec == PREC_F32_FAST;
     const size_t m_maps = rup3(m_coef + coefs.size(), 256);
-    const size_t m_gate = rup3(m_maps + (tma ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
+    // adjoint velocity through work arrays: a second set of shot descriptors and maps
+    const bool wpass = tma && adjoint_steps;
+    const size_t m_maps_w = rup3(m_maps + (tma ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
+    const size_t m_shots_w = rup3(m_maps_w + (wpass ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
+    const size_t m_wdesc = rup3(m_shots_w + (wpass ? ns * shot_bytes : 0), 256);
+    const size_t m_gate = rup3(m_wdesc + (wpass ? ns * sizeof(WorkE3) : 0), 256);
     const size_t m_end = m_gate + 256;
+    std::vector<size_t> woff(ns, 0);
+    if (wpass) {
+        size_t wb = 0;
+        for (int i = 0; i < ns; i++) {
+            woff[i] = wb;
+            wb = rup3(wb + 6 * (size_t)shots[i].plane * shots[i].planes * es, 256);
+        }
+        CU(dev_alloc(&d_work, wb, stream));
+        CU(cudaMemsetAsync(d_work, 0, wb, stream));
+    }
     CU(dev_alloc(&d_meta, m_end, stream));
     d_gate = reinterpret_cast<int *>((char *)d_meta + m_gate);
     d_err = d_gate + 1;
@@ -380,8 +412,37 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
                     set_error("cuTensorMapEncodeTiled failed for map %d of shot %d", k, i);
                     return RSGPU_ERR_CUDA;
                 }
+                if (!wpass) continue;
+                // the same map on the work array that stands in for a stress slot
+                void *mw = meta.data() + m_maps_w + ((size_t)i * NMAP_E3 + k) * sizeof(CUtensorMap);
+                const int ws = work_slot(q.param ? -1 : q.slot);
+                void *wbase = ws < 0 ? base : (void *)((char *)d_work + woff[i] + (size_t)ws * L.plane * L.planes * es);
+                if (!encode_field_map_host(mw, wbase, prec, L.pitch, L.rows * L.planes, q.boxw, q.boxh)) {
+                    set_error("cuTensorMapEncodeTiled failed for work map %d of shot %d", k, i);
+                    return RSGPU_ERR_CUDA;
+                }
             }
         }
+    }
+    for (int i = 0; i < ns && wpass; i++) {
+        const Layout3D &L = shots[i];
+        const size_t fb = (size_t)L.plane * L.planes * es, org = origin_bytes(L);
+        char *W = (char *)d_work + woff[i];
+        // descriptors: the stress slots point at the work arrays
+        Shot3D<float> d{};
+        fill_shot<float>(reinterpret_cast<unsigned char *>(&d), i);
+        for (int k = E3_SXX; k <= E3_SXY; k++) d.f[k] = (float *)(W + (size_t)work_slot(k) * fb + org);
+        std::memcpy(meta.data() + m_shots_w + i * shot_bytes, &d, sizeof d);
+        WorkE3 w{};
+        const int sl[6] = {E3_SXX, E3_SYY, E3_SZZ, E3_SYZ, E3_SXZ, E3_SXY};
+        for (int k = 0; k < 6; k++) {
+            w.s[k] = (const float *)((char *)arena + L.f[sl[k]]);
+            w.w[k] = (float *)(W + (size_t)k * fb);
+        }
+        auto pb = [&](int k) { return (const float *)(param_base(i, k) - org); };
+        w.l = pb(ME_L); w.l2m = pb(ME_L2M); w.myz = pb(ME_MYZ); w.mxz = pb(ME_MXZ); w.mxy = pb(ME_MXY);
+        w.n = (long long)L.plane * L.planes;
+        std::memcpy(meta.data() + m_wdesc + i * sizeof(WorkE3), &w, sizeof w);
     }
     for (int i = 0; i < ns; i++) {
         const ShotSets &e = eff[i];
@@ -404,6 +465,9 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
     d_maps = tma ? (char *)d_meta + m_maps : nullptr;
+    d_maps_w = wpass ? (char *)d_meta + m_maps_w : nullptr;
+    d_shots_w = wpass ? (char *)d_meta + m_shots_w : nullptr;
+    d_wdesc = wpass ? (char *)d_meta + m_wdesc : nullptr;
     CU(cudaStreamSynchronize(stream));
     return RSGPU_OK;
 }
@@ -498,6 +562,20 @@ rsgpu_status Plan3D::step(int it)
     if (prec == PREC_F64) make_args3<double>(args, *this);
     else make_args3<float>(args, *this);
     cudaError_t e;
+    if (phys == PHYS_E3D && d_wdesc) {
+        // adjoint velocity: work arrays, then the forward TMA velocity kernel on them
+        alignas(16) unsigned char wargs[sizeof(Step3DArgs<double>)];
+        std::memcpy(wargs, args, sizeof wargs);
+        Step3DArgs<float> &wa = *reinterpret_cast<Step3DArgs<float> *>(wargs);
+        wa.shots = (const Shot3D<float> *)d_shots_w;
+        wa.maps = d_maps_w;
+        if ((e = launch_work_e3d(d_wdesc, nshots, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_step_e3d(prec, 0, 0, wargs, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_step_e3d(prec, 1, 1, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
+        if ((e = launch_injrec_e3d(prec, d_shots, d_injrec, nshots, nsets, cfg.dt, it, stream)) != cudaSuccess) goto fail;
+        launches += 4;
+        return RSGPU_OK;
+    }
     if (phys == PHYS_E3D) {
         if ((e = launch_step_e3d(prec, 0, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;
         if ((e = launch_step_e3d(prec, 1, adjoint_steps, args, d_coefs, ntiles, stream)) != cudaSuccess) goto fail;

@@ -37,6 +37,18 @@ struct Shot3D {
     T *psix[6], *psiy[6], *psiz[6];
 };
 
+// Work arrays of the elastic adjoint velocity step (FAST): per shot the allocation
+// bases of the six stresses (Sxx, Syy, Szz, Syz, Sxz, Sxy), of L, L2M, M_yz, M_xz,
+// M_xy, of the six work arrays in the same order, and the elements of one field
+// allocation (a multiple of 4; every base 16-byte aligned).
+struct WorkE3 {
+    const float *s[6];
+    const float *l, *l2m, *myz, *mxz, *mxy;
+    float *w[6];
+    long long n;
+};
+cudaError_t launch_work_e3d(const void *desc, int nshots, cudaStream_t st);
+
 // One CTA: a TX3 x TY3 column block of one shot, marching planes [z0, z0 + zc).
 struct Tile3D {
     int shot, x0, y0, z0;

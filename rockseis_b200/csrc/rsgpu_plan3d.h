@@ -61,6 +61,9 @@ public:
     void *d_shots = nullptr, *d_injrec = nullptr, *d_tiles = nullptr, *d_coefs = nullptr, *d_pml = nullptr;
     std::vector<unsigned char> h_coefs;        // host copy of the CoefSet3 at d_coefs
     void *d_maps = nullptr;                    // elastic fast mode: NMAP_E3 tensor maps per shot
+    // elastic fast adjoint plans: the velocity step runs the forward TMA kernel on work
+    // arrays (launch_work_e3d); shot descriptors and maps whose stress slots are those
+    void *d_work = nullptr, *d_shots_w = nullptr, *d_maps_w = nullptr, *d_wdesc = nullptr;
     int *d_err = nullptr;                      // device error word (bounded waits)
     rsgpu_status check_device_error();
     cudaStream_t stream = nullptr;
