@@ -14,6 +14,8 @@
 // rounded ops and IEEE division; MODE_FAST: FMA, coefficients pre-divided).  Near
 // the array ends the reference's reduced-order stencils are evaluated by
 // stencil_k (the same rules as in 2D).  One launch covers all tiles of all shots.
+#include <type_traits>
+
 #include "fd2d_kernels.cuh"
 #include "rsgpu_3d.h"
 
@@ -278,11 +280,237 @@ __global__ void inject_record_3d(const Shot3D<T> *shots, const InjRec3<T> *plans
     }
 }
 
+// ---------------------------------------------------------------- fast mode with TMA-staged planes
+// The two half-steps of RSGPU_F32_FAST with every plane tile brought in by TMA
+// (cp.async.bulk.tensor.2d issued by one thread, completion on an mbarrier per
+// stage) two planes ahead of the plane being computed, so the loads in flight do
+// not depend on registers or resident warps.  The z-derivative still comes from the
+// 16-plane register window, refilled by a plain load eight planes ahead.  Same
+// stencils, C-PML and update order as a3d_velocity / a3d_stress.  Every wait is
+// bounded (2 s): on timeout the CTA records RSGPU_ERR_TIMEOUT and stops.
+constexpr int NSTG_A3 = 3;
+
+struct A3VelStage {
+    float p[HY3][WX3];         // P with its x and y halos
+    float pv[6][TY3][TX3];     // Vx, Vy, Vz, Rx, Ry, Rz
+};
+struct A3StrStage {
+    float vx[TY3][WX3];        // Vx, x halo
+    float vy[HY3][TX3];        // Vy, y halo
+    float pl[2][TY3][TX3];     // P, L
+};
+static_assert(sizeof(A3VelStage) % 128 == 0 && sizeof(A3StrStage) % 128 == 0, "TMA destinations stay 128-byte aligned");
+static_assert(sizeof(float) * HY3 * WX3 % 128 == 0 && sizeof(float) * TY3 * WX3 % 128 == 0 &&
+              sizeof(float) * HY3 * TX3 % 128 == 0 && sizeof(float) * TY3 * TX3 % 128 == 0, "tile sizes");
+
+template <typename Stage>
+struct A3Smem {
+    Stage st[NSTG_A3];
+    uint64_t bar[NSTG_A3];
+    CoefSet3<float> cs;
+};
+template <typename Stage>
+constexpr size_t a3_smem_bytes() { return sizeof(A3Smem<Stage>) + 128; }   // + alignment slack
+
+// Allocation row of plane iz, padded row iy_alloc (guards included).
+__device__ __forceinline__ int a3_row(const Shot3D<float> &sh, int iz, int iy_alloc)
+{
+    return (GUARD + iz) * sh.rows + iy_alloc;
+}
+
+__global__ void __launch_bounds__(TX3 *TY3, 3) a3d_velocity_tma(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ unsigned char smraw[];
+    A3Smem<A3VelStage> &S =
+        *reinterpret_cast<A3Smem<A3VelStage> *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX3 + tx;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    load_coefs3(S.cs, coefs);
+    if (tid == 0)
+        for (int k = 0; k < NSTG_A3; k++) mbar_init(&S.bar[k], 1);
+    __syncthreads();
+    const CUtensorMap *M = reinterpret_cast<const CUtensorMap *>(a.maps) + (size_t)tl.shot * NMAP_A3;
+    const int x0 = tl.x0, y0 = tl.y0, ix = x0 + tx, iy = y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const long long plane = sh.plane;
+    const int col = iy * pitch + ix;
+    const T *P = sh.f[A3_P];
+    T *Vx = sh.f[A3_VX], *Vy = sh.f[A3_VY], *Vz = sh.f[A3_VZ];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kx = kfw(ix, nxp, order), Ky = kfw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    // stage k <- plane iz; the boxes start on 16-byte boundaries (x0, x0 + 8 multiples of 4)
+    auto issue = [&](int iz, int k) {
+        A3VelStage &g = S.st[k];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&S.bar[k], (uint32_t)sizeof(A3VelStage));
+        tma_load_2d(g.p, M + AM_PH, &S.bar[k], x0, a3_row(sh, iz, y0));
+        for (int q = 0; q < 6; q++) tma_load_2d(g.pv[q], M + AM_VX + q, &S.bar[k], x0 + GUARD, a3_row(sh, iz, GUARD + y0));
+    };
+    if (tid == 0)
+        for (int j = 0; j < NSTG_A3 - 1 && z0 + j < ze; j++) issue(z0 + j, j);
+    T q[16];                                     // P, planes z-7..z+8 (forward z-derivative)
+#pragma unroll
+    for (int j = 0; j < 16; j++) q[j] = P[(z0 - 7 + j) * plane + col];
+    const T *cux = S.cs.cx + order * CROW3, *cuy = S.cs.cy + order * CROW3, *cuz = S.cs.cz + order * CROW3;
+    long long o = (long long)z0 * plane + col;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int j = iz - z0, k = j % NSTG_A3;
+        if (tid == 0 && iz + NSTG_A3 - 1 < ze) issue(iz + NSTG_A3 - 1, (j + NSTG_A3 - 1) % NSTG_A3);
+        const T nq = P[o + 9 * plane];          // window refill, in flight while the stage arrives
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], (uint32_t)(j / NSTG_A3) & 1u, a.err))) return;
+        const A3VelStage &g = S.st[k];
+        const T *cx = &g.p[ty + 8][tx + 8];
+        const T dfx = (Kx == order) ? taps<T, MODE>(cx - 7, 1, cux, a.dx, a.rdx)
+                                    : stencil_k<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, true, a.dx, a.rdx);
+        const T dfy = (Ky == order) ? taps<T, MODE>(cx - 7 * WX3, WX3, cuy, a.dy, a.rdy)
+                                    : stencil_k<T, MODE>(cx, WX3, Ky, S.cs.cy + Ky * CROW3, true, a.dy, a.rdy);
+        const int Kz = kfw(iz, nzp, order);
+        const T dfz = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
+                                    : stencil_k<T, MODE>(P + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, true, a.dz, a.rdz);
+        T vx = g.pv[0][ty][tx], vy = g.pv[1][ty][tx], vz = g.pv[2][ty][tx];
+        T am = A::mul(a.dt, g.pv[3][ty][tx]);
+        vx = A::mad(vx, am, dfx);
+        if (xi >= 0)
+            vx = pml_correct<T, MODE>(vx, am, dfx, sh.psix[0] + ((long long)iz * nyp + iy) * 2 * L + xc, a.pml, L,
+                                      xb + 3, xi);
+        Vx[o] = vx;
+        am = A::mul(a.dt, g.pv[4][ty][tx]);
+        vy = A::mad(vy, am, dfy);
+        if (yi >= 0)
+            vy = pml_correct<T, MODE>(vy, am, dfy, sh.psiy[0] + ((long long)iz * 2 * L + yc) * nxp + ix, a.pml, L,
+                                      yb + 3, yi);
+        Vy[o] = vy;
+        am = A::mul(a.dt, g.pv[5][ty][tx]);
+        vz = A::mad(vz, am, dfz);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        if (zi >= 0)
+            vz = pml_correct<T, MODE>(vz, am, dfz, sh.psiz[0] + ((long long)zc * nyp + iy) * nxp + ix, a.pml, L,
+                                      zb + 3, zi);
+        Vz[o] = vz;
+#pragma unroll
+        for (int jj = 0; jj < 15; jj++) q[jj] = q[jj + 1];
+        q[15] = nq;
+        __syncthreads();   // stage k is refilled next iteration
+    }
+}
+
+__global__ void __launch_bounds__(TX3 *TY3, 3) a3d_stress_tma(Step3DArgs<float> a, const CoefSet3<float> *coefs)
+{
+    using T = float;
+    constexpr int MODE = MODE_FAST;
+    using A = Ar<T, MODE>;
+    extern __shared__ unsigned char smraw[];
+    A3Smem<A3StrStage> &S =
+        *reinterpret_cast<A3Smem<A3StrStage> *>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~uintptr_t(127));
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX3 + tx;
+    const Tile3D tl = a.tiles[blockIdx.x];
+    const Shot3D<T> &sh = a.shots[tl.shot];
+    load_coefs3(S.cs, coefs);
+    if (tid == 0)
+        for (int k = 0; k < NSTG_A3; k++) mbar_init(&S.bar[k], 1);
+    __syncthreads();
+    const CUtensorMap *M = reinterpret_cast<const CUtensorMap *>(a.maps) + (size_t)tl.shot * NMAP_A3;
+    const int x0 = tl.x0, y0 = tl.y0, ix = x0 + tx, iy = y0 + ty;
+    const int nxp = sh.nxp, nyp = sh.nyp, nzp = sh.nzp, pitch = sh.pitch, L = a.lpml, order = a.order;
+    const long long plane = sh.plane;
+    const int col = iy * pitch + ix;
+    T *P = sh.f[A3_P];
+    const T *Vz = sh.f[A3_VZ];
+    const bool in_grid = ix < nxp && iy < nyp;
+    const int Kx = kbw(ix, nxp, order), Ky = kbw(iy, nyp, order);
+    int xb = 0, xc = 0, yb = 0, yc = 0;
+    const int xi = in_grid ? xstrip(ix, nxp, L, xb, xc) : -1;
+    const int yi = in_grid ? xstrip(iy, nyp, L, yb, yc) : -1;
+    const int z0 = tl.z0, ze = min(z0 + a.zc, nzp);
+    auto issue = [&](int iz, int k) {
+        A3StrStage &g = S.st[k];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&S.bar[k], (uint32_t)sizeof(A3StrStage));
+        const int rh = a3_row(sh, iz, GUARD + y0);
+        tma_load_2d(g.vx, M + AM_VXH, &S.bar[k], x0, rh);
+        tma_load_2d(g.vy, M + AM_VYH, &S.bar[k], x0 + GUARD, a3_row(sh, iz, y0));
+        tma_load_2d(g.pl[0], M + AM_P, &S.bar[k], x0 + GUARD, rh);
+        tma_load_2d(g.pl[1], M + AM_L, &S.bar[k], x0 + GUARD, rh);
+    };
+    if (tid == 0)
+        for (int j = 0; j < NSTG_A3 - 1 && z0 + j < ze; j++) issue(z0 + j, j);
+    T q[16];                                     // Vz, planes z-8..z+7 (backward z-derivative)
+#pragma unroll
+    for (int j = 0; j < 16; j++) q[j] = Vz[(z0 - 8 + j) * plane + col];
+    const T *cux = S.cs.cx + order * CROW3, *cuy = S.cs.cy + order * CROW3, *cuz = S.cs.cz + order * CROW3;
+    long long o = (long long)z0 * plane + col;
+    for (int iz = z0; iz < ze; iz++, o += plane) {
+        const int j = iz - z0, k = j % NSTG_A3;
+        if (tid == 0 && iz + NSTG_A3 - 1 < ze) issue(iz + NSTG_A3 - 1, (j + NSTG_A3 - 1) % NSTG_A3);
+        const T nq = Vz[o + 8 * plane];
+        if (!__syncthreads_and(mbar_wait_bounded(&S.bar[k], (uint32_t)(j / NSTG_A3) & 1u, a.err))) return;
+        const A3StrStage &g = S.st[k];
+        const T *cx = &g.vx[ty][tx + 8];
+        const T *cy = &g.vy[ty + 8][tx];
+        const T d1 = (Kx == order) ? taps<T, MODE>(cx - 8, 1, cux, a.dx, a.rdx)
+                                   : stencil_k<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, false, a.dx, a.rdx);
+        const T d2 = (Ky == order) ? taps<T, MODE>(cy - 8 * TX3, TX3, cuy, a.dy, a.rdy)
+                                   : stencil_k<T, MODE>(cy, TX3, Ky, S.cs.cy + Ky * CROW3, false, a.dy, a.rdy);
+        const int Kz = kbw(iz, nzp, order);
+        const T d3 = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
+                                   : stencil_k<T, MODE>(Vz + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, false, a.dz, a.rdz);
+        T p = g.pl[0][ty][tx];
+        const T am = A::mul(a.dt, g.pl[1][ty][tx]);
+        p = A::mad(p, am, d1);
+        if (xi >= 0)
+            p = pml_correct<T, MODE>(p, am, d1, sh.psix[1] + ((long long)iz * nyp + iy) * 2 * L + xc, a.pml, L, xb,
+                                     xi);
+        p = A::mad(p, am, d2);
+        if (yi >= 0)
+            p = pml_correct<T, MODE>(p, am, d2, sh.psiy[1] + ((long long)iz * 2 * L + yc) * nxp + ix, a.pml, L, yb,
+                                     yi);
+        p = A::mad(p, am, d3);
+        int zb = 0, zc = 0;
+        const int zi = in_grid ? xstrip(iz, nzp, L, zb, zc) : -1;
+        if (zi >= 0)
+            p = pml_correct<T, MODE>(p, am, d3, sh.psiz[1] + ((long long)zc * nyp + iy) * nxp + ix, a.pml, L, zb,
+                                     zi);
+        P[o] = p;
+#pragma unroll
+        for (int jj = 0; jj < 15; jj++) q[jj] = q[jj + 1];
+        q[15] = nq;
+        __syncthreads();
+    }
+}
+
 template <typename T, int MODE>
 cudaError_t step3(int half, const void *args, const void *coefs, int grid, cudaStream_t st)
 {
     const Step3DArgs<T> &a = *reinterpret_cast<const Step3DArgs<T> *>(args);
     const dim3 block(TX3, TY3);
+    if constexpr (MODE == MODE_FAST && std::is_same<T, float>::value) {
+        if (a.maps) {
+            // TMA-staged planes (the plan builds the maps in fast mode)
+            if (half == 0) {
+                auto k = a3d_velocity_tma;
+                const size_t sm = a3_smem_bytes<A3VelStage>();
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return e;
+                k<<<grid, block, sm, st>>>(a, (const CoefSet3<float> *)coefs);
+            } else {
+                auto k = a3d_stress_tma;
+                const size_t sm = a3_smem_bytes<A3StrStage>();
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+                if (e != cudaSuccess) return e;
+                k<<<grid, block, sm, st>>>(a, (const CoefSet3<float> *)coefs);
+            }
+            return cudaGetLastError();
+        }
+    }
     if (half == 0) a3d_velocity<T, MODE><<<grid, block, 0, st>>>(a, (const CoefSet3<T> *)coefs);
     else a3d_stress<T, MODE><<<grid, block, 0, st>>>(a, (const CoefSet3<T> *)coefs);
     return cudaGetLastError();

@@ -363,12 +363,13 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     const size_t ir_bytes = prec == PREC_F64 ? sizeof(InjRec3<double>) : sizeof(InjRec3<float>);
     const size_t m_shots = 0, m_ir = rup3(ns * shot_bytes, 256), m_tiles = rup3(m_ir + (size_t)nps * ir_bytes, 256);
     const size_t m_coef = rup3(m_tiles + tiles.size() * sizeof(Tile3D), 256);
-    // elastic fast mode: the tensor maps of the TMA-staged kernels
-    const bool tma = phys == PHYS_E3D && prec == PREC_F32_FAST;
+    // fast mode: the tensor maps of the TMA-staged kernels
+    const bool tma = prec == PREC_F32_FAST;
+    const int nmap = phys == PHYS_E3D ? NMAP_E3 : NMAP_A3;
     const size_t m_maps = rup3(m_coef + coefs.size(), 256);
     // adjoint velocity through work arrays: a second set of shot descriptors and maps
-    const bool wpass = tma && adjoint_steps;
-    const size_t m_maps_w = rup3(m_maps + (tma ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
+    const bool wpass = tma && adjoint_steps && phys == PHYS_E3D;
+    const size_t m_maps_w = rup3(m_maps + (tma ? (size_t)ns * nmap * sizeof(CUtensorMap) : 0), 256);
     const size_t m_shots_w = rup3(m_maps_w + (wpass ? (size_t)ns * NMAP_E3 * sizeof(CUtensorMap) : 0), 256);
     const size_t m_wdesc = rup3(m_shots_w + (wpass ? ns * shot_bytes : 0), 256);
     const size_t m_gate = rup3(m_wdesc + (wpass ? ns * sizeof(WorkE3) : 0), 256);
@@ -391,7 +392,12 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
     if (tma) {
         struct Spec { int slot; bool param; int boxw, boxh; };
         // VM_* then SM_* (rsgpu_3d.h)
-        const Spec spec[NMAP_E3] = {
+        // acoustic: AM_* (rsgpu_3d.h)
+        const Spec spec_a[NMAP_A3] = {
+            {A3_P, false, WX3, HY3}, {A3_VX, false, TX3, TY3}, {A3_VY, false, TX3, TY3}, {A3_VZ, false, TX3, TY3},
+            {M3_RX, true, TX3, TY3}, {M3_RY, true, TX3, TY3}, {M3_RZ, true, TX3, TY3},
+            {A3_VX, false, WX3, TY3}, {A3_VY, false, TX3, HY3}, {A3_P, false, TX3, TY3}, {M3_L, true, TX3, TY3}};
+        const Spec spec_e[NMAP_E3] = {
             {E3_SXX, false, WX3, TY3}, {E3_SXZ, false, WX3, TY3}, {E3_SXY, false, WX3, HY3},
             {E3_SYY, false, TX3, HY3}, {E3_SYZ, false, TX3, HY3},
             {E3_VX, false, TX3, TY3}, {E3_VY, false, TX3, TY3}, {E3_VZ, false, TX3, TY3},
@@ -401,13 +407,14 @@ rsgpu_status Plan3D::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, 
             {E3_SYZ, false, TX3, TY3}, {E3_SXZ, false, TX3, TY3}, {E3_SXY, false, TX3, TY3},
             {ME_L, true, TX3, TY3}, {ME_L2M, true, TX3, TY3}, {ME_MYZ, true, TX3, TY3},
             {ME_MXZ, true, TX3, TY3}, {ME_MXY, true, TX3, TY3}};
+        const Spec *spec = phys == PHYS_E3D ? spec_e : spec_a;
         for (int i = 0; i < ns; i++) {
             const Layout3D &L = shots[i];
-            for (int k = 0; k < NMAP_E3; k++) {
+            for (int k = 0; k < nmap; k++) {
                 const Spec &q = spec[k];
                 // 2D map over the whole allocation: pitch x (rows * planes)
                 void *base = q.param ? (void *)(param_base(i, q.slot) - origin_bytes(L)) : (void *)(A + L.f[q.slot]);
-                void *m = meta.data() + m_maps + ((size_t)i * NMAP_E3 + k) * sizeof(CUtensorMap);
+                void *m = meta.data() + m_maps + ((size_t)i * nmap + k) * sizeof(CUtensorMap);
                 if (!encode_field_map_host(m, base, prec, L.pitch, L.rows * L.planes, q.boxw, q.boxh)) {
                     set_error("cuTensorMapEncodeTiled failed for map %d of shot %d", k, i);
                     return RSGPU_ERR_CUDA;

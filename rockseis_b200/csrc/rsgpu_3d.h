@@ -37,6 +37,15 @@ struct Shot3D {
     T *psix[6], *psiy[6], *psiz[6];
 };
 
+// Tensor maps of the acoustic 3D TMA kernels (FAST), per shot, over whole pitched
+// arrays like the elastic ones:
+//   velocity: P {48 x 24} (x and y halos); Vx, Vy, Vz, Rx, Ry, Rz {32 x 8}
+//   stress:   Vx {48 x 8} (x halo); Vy {32 x 24} (y halo); P, L {32 x 8}
+enum {
+    AM_PH = 0, AM_VX, AM_VY, AM_VZ, AM_RX, AM_RY, AM_RZ, AM_VXH, AM_VYH, AM_P, AM_L,
+    NMAP_A3
+};
+
 // Work arrays of the elastic adjoint velocity step (FAST): per shot the allocation
 // bases of the six stresses (Sxx, Syy, Szz, Syz, Sxz, Sxy), of L, L2M, M_yz, M_xz,
 // M_xy, of the six work arrays in the same order, and the elements of one field
