@@ -348,7 +348,7 @@ def run_gpu(args, rank, world, device, physics="elastic2d"):
     plan = Plan(models, srcs, recs, ORDER, precision, args.tile if args.tile >= -1 else -1,
                 launch_mode=args.launch_mode, zchunk=args.zchunk)
     mode, items, band = plan.info()
-    if mode != 3:
+    if mode not in (3, 4):
         # per-tile kernels: the tile shape is the autotuner's pick (cached in JSON), measured before timing
         plan.close()
         from rockseis_b200.autotune import tune_tile
@@ -395,6 +395,10 @@ def run_gpu(args, rank, world, device, physics="elastic2d"):
         dom, ms_dom, b_dom = "zm_step_2d", ms_a, b_fused
         extra = {"launch": "fused z-marching step (velocity + stress + injection + recording of the previous "
                            "step)", "work_items": items, "rows_per_item": band}
+    elif mode == 4:
+        dom, ms_dom, b_dom = ("e2d_march_stress", ms_b, b_str) if ms_b >= ms_a else ("e2d_march_velocity", ms_a, b_vel)
+        extra = {"launch": "column-marching velocity and stress kernels", "ms_velocity": round(ms_a, 5),
+                 "ms_stress": round(ms_b, 5), "work_items": items, "rows_per_item": band}
     else:
         dom, ms_dom, b_dom = (("e2d_stress" if physics == "elastic2d" else "a2d_stress"), ms_b, b_str) \
             if ms_b >= ms_a else (("e2d_velocity" if physics == "elastic2d" else "a2d_velocity"), ms_a, b_vel)
@@ -1221,7 +1225,8 @@ def main():
                     help="elastic2d: the forward modelling line (with the FWI gradient figures attached); "
                          "acoustic2d: the one-shot acoustic forward; fwi: the FWI gradient line alone")
     ap.add_argument("--launch-mode", type=int, default=0,
-                    help="2D: rsgpu_config.launch_mode (0 = library choice: per-tile kernels, 3 = fused step)")
+                    help="2D: rsgpu_config.launch_mode (0 = library choice: per-tile kernels, 3 = fused step, "
+                         "4 = column-marching elastic half-steps)")
     ap.add_argument("--no-fwi", action="store_true", help="leave the FWI gradient figures out of the elastic2d line")
     ap.add_argument("--fwi-steps", type=int, default=2, help="timed gradient batches")
     ap.add_argument("--zchunk", type=int, default=0,

@@ -194,6 +194,7 @@ Plan::~Plan()
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (zm_graph) cudaGraphExecDestroy(zm_graph);
     dev_free(d_zm, stream);
+    dev_free(d_march, stream);
     for (auto &row : tev)
         for (auto &e : row)
             if (e) cudaEventDestroy(e);
@@ -307,6 +308,9 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     // slower on B200 (it issues as many instructions per point with a third of the
     // resident warps), so the library's choice (mode 0) is the per-tile kernels.
     fused = c->launch_mode == 3 && !adjoint_steps;
+    // Launch mode 4: the column-marching half-steps (fd2d_march.cu) for FAST elastic
+    // forward propagation; other plans keep the per-tile kernels.
+    march = c->launch_mode == 4 && phys == PHYS_E2D && prec == PREC_F32_FAST && !adjoint_steps;
     const int ztx = zm_strip_width();
 
     // ---- per-shot layout (byte offsets into the arena)
@@ -557,6 +561,7 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     d_tiles = (char *)d_meta + m_tiles;
     d_coefs = (char *)d_meta + m_coef;
     d_maps = (char *)d_meta + m_maps;
+    if (march && (st = setup_march(coefs)) != RSGPU_OK) return st;
     if (fused) {
         std::vector<std::vector<int>> inj_pts(inj.size());
         for (size_t j = 0; j < inj.size(); j++) inj_pts[j] = inj[j].pt;
@@ -663,12 +668,17 @@ rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj, cudaEve
     else make_args<float>(args, *this);
     const int grid = ntiles;
     const int flags = (adj ? LAUNCH_ADJ : 0) | (cfg.launch_mode == 1 ? LAUNCH_PERSISTENT : 0);
+    const bool mh = march && !adj;
     cudaError_t e;
     // external records so the events become timestamp nodes of a captured graph
     if (ev && (e = cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 0, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = mh ? launch_march_2d(0, march_args, march_nitems, stream)
+                : launch_step_2d(prec, tilecfg, phys, 0, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess)
+        goto fail;
     if (ev && (e = cudaEventRecordWithFlags(ev[1], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
-    if ((e = launch_step_2d(prec, tilecfg, phys, 1, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess) goto fail;
+    if ((e = mh ? launch_march_2d(1, march_args, march_nitems, stream)
+                : launch_step_2d(prec, tilecfg, phys, 1, flags, args, d_coefs, d_maps, d_err, grid, stream)) != cudaSuccess)
+        goto fail;
     if (ev && (e = cudaEventRecordWithFlags(ev[2], stream, cudaEventRecordExternal)) != cudaSuccess) goto fail;
     if ((e = launch_injrec_2d(prec, d_shots, d_injrec, nshots, cfg.dt, it_base, it_dev, stream)) != cudaSuccess) goto fail;
     launches += 3;
@@ -903,9 +913,9 @@ rsgpu_status rsgpu_plan_info(rsgpu_plan *p, int *launch_mode, int *work_items, i
     if (!p || !launch_mode || !work_items || !band_rows) { set_error("null argument"); return RSGPU_ERR_ARG; }
     if (p->p3) { set_error("3D plans have no 2D launch mode"); return RSGPU_ERR_UNSUPPORTED; }
     const Plan &q = *p->p;
-    *launch_mode = q.fused ? 3 : (q.cfg.launch_mode == 1 ? 1 : 2);
-    *work_items = q.fused ? q.zm_nitems : 0;
-    *band_rows = q.fused ? q.zm_band : 0;
+    *launch_mode = q.fused ? 3 : q.march ? 4 : (q.cfg.launch_mode == 1 ? 1 : 2);
+    *work_items = q.fused ? q.zm_nitems : q.march ? q.march_nitems : 0;
+    *band_rows = q.fused ? q.zm_band : q.march ? q.march_band : 0;
     return RSGPU_OK;
 }
 long long rsgpu_plan_launch_count(rsgpu_plan *p) { return p ? (p->p3 ? p->p3->launches : p->p->launches) : 0; }

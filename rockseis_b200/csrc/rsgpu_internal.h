@@ -160,4 +160,22 @@ struct Zm2DArgs {
     int lpml;
 };
 
+// ---- column-marching elastic 2D half-steps (fd2d_march.cu, launch mode 4)
+// One work item: rows [z0, z1) of the strip [x0, x0 + MSTRIP2D) of a shot.
+constexpr int MSTRIP2D = 128;
+struct MarchItem {
+    int shot, x0, z0, z1;
+};
+struct March2DArgs {
+    const Shot2D<float> *shots;
+    const MarchItem *items;
+    const void *maps;             // CUtensorMap [shot][NMAP2D] with box (MSTRIP2D + 16) x 8 rows
+    const float *pml;             // 12*lpml C-PML tables
+    const float *coefs;           // CoefSet<float> (per-K rows, divided by the spacing)
+    int *err;                     // device error word (bounded waits)
+    int order, lpml;
+    float dt;
+    float cx[NCOEF], cz[NCOEF];   // the full-order rows of coefs
+};
+
 }  // namespace rsgpu

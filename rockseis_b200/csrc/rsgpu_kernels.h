@@ -49,5 +49,11 @@ cudaError_t launch_zm_set_run(int *ctl, int it0, cudaStream_t st);
 int zm_resident_ctas(int prec, int physics);
 size_t coefset_bytes(int prec);
 int coef_row_stride();
+// Column-marching elastic 2D half-steps (fd2d_march.cu): FAST arithmetic, forward
+// propagation; half 0 = velocity, 1 = stress; args: March2DArgs.
+struct March2DArgs;
+cudaError_t launch_march_2d(int half, const March2DArgs &args, int nitems, cudaStream_t st);
+int march_resident_ctas();   // CTAs of the slower half-step resident per SM (0 = query failed)
+int march_smem_bytes();
 
 }  // namespace rsgpu

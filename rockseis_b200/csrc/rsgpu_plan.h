@@ -111,8 +111,17 @@ public:
     void *d_zm = nullptr;                 // items, injection entries, receiver list, tensor maps
     cudaGraphExec_t zm_graph = nullptr;
 
+    // column-marching elastic half-steps (fd2d_march.cu, launch mode 4): chosen at
+    // create() for FAST elastic forward propagation when launch_mode asks for it
+    bool march = false;
+    int march_nitems = 0, march_band = 0;
+    March2DArgs march_args{};
+    void *d_march = nullptr;              // work items and tensor maps
+
 private:
     rsgpu_status run_fused(int it0, int nsteps);
+    // builds the marching kernels' work items and tensor maps; coefs = the host CoefSet bytes
+    rsgpu_status setup_march(const std::vector<unsigned char> &coefs);
     // builds the fused step's tables; inj_pts[shot*MAXSETS + set] = the set's CSR target offsets
     rsgpu_status setup_fused(const std::vector<std::vector<int>> &inj_pts);
     rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s, bool sets_given);
