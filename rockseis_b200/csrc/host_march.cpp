@@ -51,8 +51,12 @@ rsgpu_status Plan::setup_march(const std::vector<unsigned char> &coefs)
     std::vector<MarchItem> items;
     for (int i = 0; i < nshots; i++) {
         const ShotLayout &L = shots[i];
-        for (int x0 = 0; x0 < L.nxp; x0 += MSTRIP2D)
-            for (int z0 = 0; z0 < L.nzp; z0 += band) items.push_back({i, x0, z0, std::min(z0 + band, L.nzp)});
+        // strips that hold C-PML columns or columns with reduced-order stencils
+        const int xlo = std::max(cfg.lpml, cfg.order), xhi = L.nxp - std::max(cfg.lpml, cfg.order + 1);
+        for (int x0 = 0; x0 < L.nxp; x0 += MSTRIP2D) {
+            const int flags = (x0 < xlo || x0 + MSTRIP2D > xhi) ? MARCH_XGEN : 0;
+            for (int z0 = 0; z0 < L.nzp; z0 += band) items.push_back({i, x0, z0, std::min(z0 + band, L.nzp), flags});
+        }
     }
     march_nitems = (int)items.size();
     march_band = band;

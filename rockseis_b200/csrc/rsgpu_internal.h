@@ -164,8 +164,9 @@ struct Zm2DArgs {
 // One work item: rows [z0, z1) of the strip [x0, x0 + MSTRIP2D) of a shot.
 constexpr int MSTRIP2D = 128;
 struct MarchItem {
-    int shot, x0, z0, z1;
+    int shot, x0, z0, z1, flags;
 };
+enum { MARCH_XGEN = 1 };   // the strip holds C-PML or reduced-order columns
 struct March2DArgs {
     const Shot2D<float> *shots;
     const MarchItem *items;
