@@ -92,7 +92,9 @@ typedef struct {
                            faster on B200), 1 = persistent per-tile kernels (elastic forward),
                            2 = per-tile velocity and stress kernels, 3 = fused z-marching step:
                            velocity, stress and injection of a time step plus recording of
-                           the previous one in one launch (forward propagation) */
+                           the previous one in one launch (forward propagation), 4 = column-
+                           marching velocity and stress kernels (elastic, FAST arithmetic,
+                           forward propagation; other plans use mode 2) */
     int reserved[5];
 } rsgpu_config;
 
@@ -162,9 +164,9 @@ rsgpu_status rsgpu_plan_enable_timing(rsgpu_plan *plan);
 rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *plan, float *ms_velocity, float *ms_stress);
 /* How a 2D plan propagates (no counterpart in the reference): the launch mode in
  * use (3 = fused z-marching step, whose one launch per step rsgpu_plan_kernel_times
- * reports as ms_velocity with ms_stress 0; 2 = per-tile velocity and stress
- * kernels; 1 = persistent per-tile kernels), the fused step's work items and
- * their height in rows (0 when not fused). */
+ * reports as ms_velocity with ms_stress 0; 4 = column-marching half-steps; 2 =
+ * per-tile velocity and stress kernels; 1 = persistent per-tile kernels), and the
+ * work items of modes 3 and 4 with their height in rows (0 otherwise). */
 rsgpu_status rsgpu_plan_info(rsgpu_plan *plan, int *launch_mode, int *work_items, int *band_rows);
 /* Copy one wavefield (reference field code, SXX=4.. for elastic) of one shot to the host
  * in the reference's padded layout (for step-level parity tests). */
