@@ -89,7 +89,8 @@ typedef struct {
     int zchunk;         /* 3D: planes marched by one CTA (0 = 64); 2D fused step: rows per
                            work item (rounded up to 8; 0 = chosen from the batch size) */
     int launch_mode;    /* 2D propagation: 0 = library choice (the per-tile kernels, the
-                           faster on B200), 1 = persistent per-tile kernels (elastic forward),
+                           faster on B200), 1 = the same as 2 (a persistent variant of the
+                           per-tile kernels measured slower and was removed),
                            2 = per-tile velocity and stress kernels, 3 = fused z-marching step:
                            velocity, stress and injection of a time step plus recording of
                            the previous one in one launch (forward propagation), 4 = column-
@@ -165,7 +166,7 @@ rsgpu_status rsgpu_plan_kernel_times(rsgpu_plan *plan, float *ms_velocity, float
 /* How a 2D plan propagates (no counterpart in the reference): the launch mode in
  * use (3 = fused z-marching step, whose one launch per step rsgpu_plan_kernel_times
  * reports as ms_velocity with ms_stress 0; 4 = column-marching half-steps; 2 =
- * per-tile velocity and stress kernels; 1 = persistent per-tile kernels), and the
+ * per-tile velocity and stress kernels), and the
  * work items of modes 3 and 4 with their height in rows (0 otherwise). */
 rsgpu_status rsgpu_plan_info(rsgpu_plan *plan, int *launch_mode, int *work_items, int *band_rows);
 /* Copy one wavefield (reference field code, SXX=4.. for elastic) of one shot to the host

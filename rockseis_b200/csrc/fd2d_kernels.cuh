@@ -838,101 +838,6 @@ e2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, in
     e2d_stress_tile<T, MODE, TX, TZ, RZ, ADJ>(a, sh, tl, sVx, sVz, cs, bar, err);
 }
 
-// ---------------------------------------------------------------- persistent elastic forward kernels
-// Launched with one or a few CTAs per SM; each CTA walks the tile table with a
-// stride of gridDim.x and keeps two shared-memory stages: while tile k is
-// computed from stage k&1, the TMA loads of tile k+1 fill the other stage, so the
-// copy latency overlaps the arithmetic inside the CTA instead of relying on other
-// CTAs.  Each stage has its own mbarrier, initialised once; its n-th use waits on
-// parity n&1.  The arithmetic is the per-tile code of the kernels above.
-// Measured on the 16-shot 801x401 elastic workload it is slower than one CTA per
-// tile (23.5 vs 31.2 Gpts/s): two stages of three halo'd tiles limit residency to
-// four CTAs per SM, and the point-wise loads are not prefetched across tiles.
-template <typename T, int TX, int TZ, int RZ, int NF>
-struct Pers2D {
-    using G = Geo2D<T, TX, TZ, RZ>;
-    static constexpr size_t STAGE = (size_t)NF * G::TILE_STRIDE;
-    __host__ __device__ static constexpr size_t coef_off() { return 2 * STAGE; }
-    __host__ __device__ static constexpr size_t bar_off() { return (2 * STAGE + sizeof(CoefSet<T>) + 15) / 16 * 16; }
-    __host__ __device__ static constexpr size_t bytes() { return bar_off() + 2 * sizeof(uint64_t); }
-};
-
-// Thread 0: expect the stage's bytes and issue the tile's loads on the stage barrier.
-template <typename T, int TX, int TZ, int RZ, int NF>
-__device__ __forceinline__ void pers_issue(unsigned char *sm, uint64_t *bar, const CUtensorMap *maps,
-                                           const Step2DArgs<T> &a, int tile, int stage, const int (&fields)[NF])
-{
-    using P = Pers2D<T, TX, TZ, RZ, NF>;
-    using G = Geo2D<T, TX, TZ, RZ>;
-    if (threadIdx.x != 0) return;
-    const Tile2D tl = a.tiles[tile];
-    // the stage was last read through the generic proxy; order those reads before the async writes
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&bar[stage], (uint32_t)(NF * G::TILE_BYTES));
-    for (int m = 0; m < NF; m++)
-        tma_load_2d(sm + stage * P::STAGE + m * G::TILE_STRIDE, maps + tl.shot * NMAP + fields[m], &bar[stage], tl.x0,
-                    tl.z0);
-}
-
-template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, int HALF>
-__global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
-e2d_forward_persistent(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
-{
-    constexpr int NF = HALF == 0 ? 3 : 2;
-    using P = Pers2D<T, TX, TZ, RZ, NF>;
-    using G = Geo2D<T, TX, TZ, RZ>;
-    extern __shared__ __align__(128) unsigned char sm[];
-    CoefSet<T> &cs = *reinterpret_cast<CoefSet<T> *>(sm + P::coef_off());
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + P::bar_off());
-    int fields[NF];
-    if (HALF == 0) { fields[0] = E2_SXX; fields[1] = E2_SZZ; fields[NF - 1] = E2_SXZ; }
-    else { fields[0] = E2_VX; fields[NF - 1] = E2_VZ; }
-    int t = blockIdx.x;
-    if (t >= a.ntiles) return;
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-    }
-    pers_issue<T, TX, TZ, RZ, NF>(sm, bar, maps, a, t, 0, fields);
-    load_coefs(cs, coefs);
-    __syncthreads();
-    for (int k = 0;; k++) {
-        const int s = k & 1;
-        const int tn = t + gridDim.x;
-        if (tn < a.ntiles) pers_issue<T, TX, TZ, RZ, NF>(sm, bar, maps, a, tn, s ^ 1, fields);
-        const Tile2D tl = a.tiles[t];
-        const Shot2D<T> &sh = a.shots[tl.shot];
-        T *st = reinterpret_cast<T *>(sm + s * P::STAGE);
-        constexpr int TS = G::TILE_STRIDE / (int)sizeof(T);
-        const uint32_t phase = (uint32_t)(k >> 1) & 1u;
-        if (HALF == 0)
-            e2d_velocity_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, st, st + TS, st + 2 * TS, cs, &bar[s], err, phase);
-        else
-            e2d_stress_tile<T, MODE, TX, TZ, RZ, false>(a, sh, tl, st, st + TS, cs, &bar[s], err, phase);
-        // a wait that gave up stops the CTA, after its copy in flight has landed (bounded)
-        if (__syncthreads_or(*(volatile int *)err != 0)) {
-            if (tn < a.ntiles && threadIdx.x == 0) mbar_wait_bounded(&bar[s ^ 1], (uint32_t)((k + 1) >> 1) & 1u, nullptr);
-            return;
-        }
-        if (tn >= a.ntiles) break;
-        t = tn;
-    }
-}
-
-// Resident CTAs of a persistent kernel on the whole device (occupancy x SMs).
-template <typename K>
-static int persistent_ctas(K kernel, int threads, size_t smem)
-{
-    int dev = 0, b = 0, nsm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem) != cudaSuccess) {
-        cudaGetLastError();
-        b = 1;
-    }
-    return (b > 0 ? b : 1) * (nsm > 0 ? nsm : 1);
-}
-
 // ---------------------------------------------------------------- sources and receivers
 // One CTA per shot.  Injection first (lib/waves.cpp:407-497, 2085-2174), then,
 // after a CTA barrier, recording (lib/waves.cpp:500-595, 2178-2288) of the same step.
@@ -1055,24 +960,6 @@ cudaError_t launch_2d_cfg(int physics, int half, int flags, const Step2DArgs<T> 
     using G = Geo2D<T, TX, TZ, RZ>;
     using S = Smem2D<T, TX, TZ, RZ>;
     const bool adj = (flags & LAUNCH_ADJ) != 0;
-    if (physics == PHYS_E2D && !adj && (flags & LAUNCH_PERSISTENT)) {
-        if (half == 0) {
-            auto k = e2d_forward_persistent<T, MODE, TX, TZ, RZ, MINB, 0>;
-            const size_t b = Pers2D<T, TX, TZ, RZ, 3>::bytes();
-            static const cudaError_t e = set_smem(k, b);
-            if (e != cudaSuccess) return e;
-            static const int ctas = persistent_ctas(k, G::NT, b);
-            k<<<ctas < a.ntiles ? ctas : a.ntiles, G::NT, b, st>>>(a, coefs, maps, err);
-        } else {
-            auto k = e2d_forward_persistent<T, MODE, TX, TZ, RZ, MINB, 1>;
-            const size_t b = Pers2D<T, TX, TZ, RZ, 2>::bytes();
-            static const cudaError_t e = set_smem(k, b);
-            if (e != cudaSuccess) return e;
-            static const int ctas = persistent_ctas(k, G::NT, b);
-            k<<<ctas < a.ntiles ? ctas : a.ntiles, G::NT, b, st>>>(a, coefs, maps, err);
-        }
-        return cudaGetLastError();
-    }
     if (physics == PHYS_A2D) {
         if (half == 0) {
             static const cudaError_t e = set_smem(a2d_velocity<T, MODE, TX, TZ, RZ, MINB>, S::bytes(1));

@@ -667,7 +667,7 @@ rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj, cudaEve
     if (prec == PREC_F64) make_args<double>(args, *this);
     else make_args<float>(args, *this);
     const int grid = ntiles;
-    const int flags = (adj ? LAUNCH_ADJ : 0) | (cfg.launch_mode == 1 ? LAUNCH_PERSISTENT : 0);
+    const int flags = adj ? LAUNCH_ADJ : 0;
     const bool mh = march && !adj;
     cudaError_t e;
     // external records so the events become timestamp nodes of a captured graph
@@ -913,7 +913,7 @@ rsgpu_status rsgpu_plan_info(rsgpu_plan *p, int *launch_mode, int *work_items, i
     if (!p || !launch_mode || !work_items || !band_rows) { set_error("null argument"); return RSGPU_ERR_ARG; }
     if (p->p3) { set_error("3D plans have no 2D launch mode"); return RSGPU_ERR_UNSUPPORTED; }
     const Plan &q = *p->p;
-    *launch_mode = q.fused ? 3 : q.march ? 4 : (q.cfg.launch_mode == 1 ? 1 : 2);
+    *launch_mode = q.fused ? 3 : q.march ? 4 : 2;
     *work_items = q.fused ? q.zm_nitems : q.march ? q.march_nitems : 0;
     *band_rows = q.fused ? q.zm_band : q.march ? q.march_band : 0;
     return RSGPU_OK;

@@ -17,9 +17,8 @@ enum { TILECFG_64x32 = 0, TILECFG_32x16 = 3, TILECFG_DEFAULT = 6 };
 
 // One half-step (half = 0 velocity, 1 stress) of every tile in args.
 // maps: per shot NMAP2D CUtensorMaps of the halo-loaded fields; err: device error word.
-// flags: LAUNCH_ADJ (adjoint kernels), LAUNCH_PERSISTENT (elastic forward only:
-// one persistent CTA set walking all tiles with double-buffered TMA stages)
-enum { LAUNCH_ADJ = 1, LAUNCH_PERSISTENT = 2 };
+// flags: LAUNCH_ADJ (adjoint kernels)
+enum { LAUNCH_ADJ = 1 };
 cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, int flags, const void *args, const void *coefs,
                            const void *maps, int *err, int grid, cudaStream_t st);
 constexpr int NMAP2D = 5;

@@ -117,14 +117,3 @@ def test_graph_replay_matches_direct_launches(require_gpu):
     p.close()
 
 
-@pytest.mark.parametrize("fs", [0, 1])
-def test_elastic2d_persistent_launch_bitwise(require_gpu, fs):
-    """The optional persistent elastic forward kernels (launch_mode 1) compute the same tiles."""
-    c = Case2D(abi.ELASTIC2D, fs=fs, sfield=abi.PRESSURE, rfield=abi.VX, nt=250)
-    c.rec.data[:] = 0
-    mod = ModellingElastic2D(c.model, c.src, c.order, 1)
-    mod.launch_mode = 1
-    mod.setRecVx(c.rec)
-    assert mod.run() == 1
-    ref = c.oracle_traces()
-    assert np.array_equal(c.rec.data, ref), f"max abs diff {np.abs(c.rec.data - ref).max()}"
