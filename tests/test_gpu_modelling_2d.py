@@ -115,5 +115,3 @@ def test_graph_replay_matches_direct_launches(require_gpu):
     assert np.array_equal(a, b)
     assert np.array_equal(a, c.oracle_traces())
     p.close()
-
-
