@@ -745,6 +745,18 @@ def cpu_a3d_reference(models, nsteps=6, procs=None, f=A3D):
                       f"steps", "max_process_s": round(max(times), 3)}
 
 
+def a3d_strip_points(models, L):
+    """Point-axis pairs in the C-PML strips of the 3D windows: sum over windows of the
+    points in the x, the y and the z strips (a corner point counts once per axis).
+    Each velocity and each stress half-step reads and writes one 4-byte memory
+    variable per pair: 16 B per pair and time step."""
+    n = 0
+    for m in models:
+        nx, ny, nz = m.nx + 2 * L, m.ny + 2 * L, m.nz + 2 * L
+        n += 2 * L * ny * nz + nx * 2 * L * nz + nx * ny * 2 * L
+    return n
+
+
 def run_a3d(args, device=0, f=A3D):
     """Gpts/s of the windowed 3D batch: chunks of time steps of all 32 shots."""
     import ctypes as C
@@ -787,16 +799,18 @@ def run_a3d(args, device=0, f=A3D):
     abi.lib.rsgpu_plan_destroy(h)
     value = pts * ch / (ms / 1e3) / 1e9
     # algorithmic bytes per time step: velocity reads P,Vx,Vy,Vz,Rx,Ry,Rz, writes Vx,Vy,Vz (40 B);
-    # stress reads Vx,Vy,Vz,P,L, writes P (24 B)
+    # stress reads Vx,Vy,Vz,P,L, writes P (24 B); 16 B per C-PML strip point-axis pair
     peak, peak_kind = measured_peak()
-    achieved = 64.0 * pts * ch / (ms / 1e3) / 1e9
+    strip = a3d_strip_points(models, L)
+    achieved = (64.0 * pts + 16.0 * strip) * ch / (ms / 1e3) / 1e9
     return {"metric": "Gpts/s", "value": round(value, 3), "unit": "Gpts/s", "ms_per_step": round(ms, 3),
             "gpu_launches": int(launches), "padded_points_per_step": int(pts),
             "window_sizes": {"min": min(win), "max": max(win)},
             "roofline": {"bound": "hbm", "kernel": "a3d_velocity + a3d_stress (whole step)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                         "algorithmic_bytes_per_point_step": 64},
+                         "algorithmic_bytes_per_point_step": 64, "cpml_bytes_per_strip_point_step": 16,
+                         "strip_points": int(strip)},
             "clocks": clk.summary(), "models": models}
 
 
@@ -1157,12 +1171,14 @@ def run_rtm3d(args, device=0, f=A3D):
     # 48 B per forward point-step (four fields read and written, four parameters read),
     # 60 B per adjoint step with the image correlation (48 + forward P 4 + FP32 image
     # read and written 8; FP64 accumulation moves 8 more), checkpoint bytes of the schedule
-    img_bytes = pts * (48.0 * stats["fw_steps"] + 60.0 * stats["bw_steps"]) + stats["ckpt_bytes"]
+    img_bytes = pts * (48.0 * stats["fw_steps"] + 60.0 * stats["bw_steps"]) + stats["ckpt_bytes"] + \
+        16.0 * a3d_strip_points(models, L) * (stats["fw_steps"] + stats["bw_steps"])
     roof = {"bound": "hbm", "kernel": "whole image (forward, adjoint, correlation, checkpoints)",
             "achieved": round(img_bytes / t_batch / 1e9, 1), "peak": peak, "unit": "GB/s",
             "frac": round(img_bytes / t_batch / 1e9 / peak, 4), "peak_source": peak_kind,
             "algorithmic_bytes": "48 B per forward point-step, 60 B per adjoint+correlation point-step, "
-                                 "checkpoint bytes from the schedule", "traffic": None}
+                                 "16 B per C-PML strip point-axis pair and step, checkpoint bytes from the "
+                                 "schedule", "traffic": None}
     work_full = abi.lib.rsgpu_revolve_numforw(f["nt"], RTM3["ncheck"]) + 1 + 2 * f["nt"]
     work = stats["fw_steps"] + stats["bw_steps"] + 1
     return {"images_per_s": float("%.4g" % (ns / t_batch)), "s_per_batch": round(t_batch, 3), "shots": ns,
