@@ -119,12 +119,12 @@ __global__ void __launch_bounds__(TX3 *TY3, 3) a3d_velocity(Step3DArgs<T> a, con
         __syncthreads();
         const T *cx = &sP[ty + 8][tx + 8];
         const T dfx = (Kx == order) ? taps<T, MODE>(cx - 7, 1, cux, a.dx, a.rdx)
-                                    : stencil_k<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, true, a.dx, a.rdx);
+                                    : stencil_ki<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, true, a.dx, a.rdx);
         const T dfy = (Ky == order) ? taps<T, MODE>(cx - 7 * (TX3 + 16), TX3 + 16, cuy, a.dy, a.rdy)
-                                    : stencil_k<T, MODE>(cx, TX3 + 16, Ky, cs.cy + Ky * CROW3, true, a.dy, a.rdy);
+                                    : stencil_ki<T, MODE>(cx, TX3 + 16, Ky, cs.cy + Ky * CROW3, true, a.dy, a.rdy);
         const int Kz = kfw(iz, nzp, order);
         const T dfz = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
-                                    : stencil_k<T, MODE>(P + o, (int)plane, Kz, cs.cz + Kz * CROW3, true, a.dz, a.rdz);
+                                    : stencil_ki<T, MODE>(P + o, (int)plane, Kz, cs.cz + Kz * CROW3, true, a.dz, a.rdz);
         T am = A::mul(a.dt, rx);
         vx = A::mad(vx, am, dfx);
         if (xi >= 0)
@@ -209,12 +209,12 @@ __global__ void __launch_bounds__(TX3 *TY3, 3) a3d_stress(Step3DArgs<T> a, const
         const T *cx = &sVx[ty][tx + 8];
         const T *cy = &sVy[ty + 8][tx];
         const T d1 = (Kx == order) ? taps<T, MODE>(cx - 8, 1, cux, a.dx, a.rdx)
-                                   : stencil_k<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, false, a.dx, a.rdx);
+                                   : stencil_ki<T, MODE>(cx, 1, Kx, cs.cx + Kx * CROW3, false, a.dx, a.rdx);
         const T d2 = (Ky == order) ? taps<T, MODE>(cy - 8 * TX3, TX3, cuy, a.dy, a.rdy)
-                                   : stencil_k<T, MODE>(cy, TX3, Ky, cs.cy + Ky * CROW3, false, a.dy, a.rdy);
+                                   : stencil_ki<T, MODE>(cy, TX3, Ky, cs.cy + Ky * CROW3, false, a.dy, a.rdy);
         const int Kz = kbw(iz, nzp, order);
         const T d3 = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
-                                   : stencil_k<T, MODE>(Vz + o, (int)plane, Kz, cs.cz + Kz * CROW3, false, a.dz, a.rdz);
+                                   : stencil_ki<T, MODE>(Vz + o, (int)plane, Kz, cs.cz + Kz * CROW3, false, a.dz, a.rdz);
         const T am = A::mul(a.dt, lm);
         p = A::mad(p, am, d1);
         if (xi >= 0)
@@ -369,12 +369,12 @@ __global__ void __launch_bounds__(TX3 *TY3, 3) a3d_velocity_tma(Step3DArgs<float
         const A3VelStage &g = S.st[k];
         const T *cx = &g.p[ty + 8][tx + 8];
         const T dfx = (Kx == order) ? taps<T, MODE>(cx - 7, 1, cux, a.dx, a.rdx)
-                                    : stencil_k<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, true, a.dx, a.rdx);
+                                    : stencil_ki<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, true, a.dx, a.rdx);
         const T dfy = (Ky == order) ? taps<T, MODE>(cx - 7 * WX3, WX3, cuy, a.dy, a.rdy)
-                                    : stencil_k<T, MODE>(cx, WX3, Ky, S.cs.cy + Ky * CROW3, true, a.dy, a.rdy);
+                                    : stencil_ki<T, MODE>(cx, WX3, Ky, S.cs.cy + Ky * CROW3, true, a.dy, a.rdy);
         const int Kz = kfw(iz, nzp, order);
         const T dfz = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
-                                    : stencil_k<T, MODE>(P + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, true, a.dz, a.rdz);
+                                    : stencil_ki<T, MODE>(P + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, true, a.dz, a.rdz);
         T vx = g.pv[0][ty][tx], vy = g.pv[1][ty][tx], vz = g.pv[2][ty][tx];
         T am = A::mul(a.dt, g.pv[3][ty][tx]);
         vx = A::mad(vx, am, dfx);
@@ -457,12 +457,12 @@ __global__ void __launch_bounds__(TX3 *TY3, 3) a3d_stress_tma(Step3DArgs<float> 
         const T *cx = &g.vx[ty][tx + 8];
         const T *cy = &g.vy[ty + 8][tx];
         const T d1 = (Kx == order) ? taps<T, MODE>(cx - 8, 1, cux, a.dx, a.rdx)
-                                   : stencil_k<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, false, a.dx, a.rdx);
+                                   : stencil_ki<T, MODE>(cx, 1, Kx, S.cs.cx + Kx * CROW3, false, a.dx, a.rdx);
         const T d2 = (Ky == order) ? taps<T, MODE>(cy - 8 * TX3, TX3, cuy, a.dy, a.rdy)
-                                   : stencil_k<T, MODE>(cy, TX3, Ky, S.cs.cy + Ky * CROW3, false, a.dy, a.rdy);
+                                   : stencil_ki<T, MODE>(cy, TX3, Ky, S.cs.cy + Ky * CROW3, false, a.dy, a.rdy);
         const int Kz = kbw(iz, nzp, order);
         const T d3 = (Kz == order) ? taps_reg<T, MODE>(q, cuz, a.dz, a.rdz)
-                                   : stencil_k<T, MODE>(Vz + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, false, a.dz, a.rdz);
+                                   : stencil_ki<T, MODE>(Vz + o, (int)plane, Kz, S.cs.cz + Kz * CROW3, false, a.dz, a.rdz);
         T p = g.pl[0][ty][tx];
         const T am = A::mul(a.dt, g.pl[1][ty][tx]);
         p = A::mad(p, am, d1);
