@@ -575,7 +575,7 @@ __device__ __forceinline__ void update_field_any(bool pml, T (&F)[RZ][4], const 
 
 // Velocity half-step: Vx += dt*Rx*Dx+P (+ x C-PML), Vz += dt*Rz*Dz+P (+ z C-PML)
 // (lib/waves.cpp:217-310).
-template <typename T, int MODE, int TX, int TZ, int RZ>
+template <typename T, int MODE, int TX, int TZ, int RZ, bool INL>
 __device__ __forceinline__ void a2d_velocity_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
                                                   const T *sP, const CoefSet<T> &cs, int *err, uint64_t *bar)
 {
@@ -587,21 +587,21 @@ __device__ __forceinline__ void a2d_velocity_tile(const Step2DArgs<T> &a, const 
     load_block<T, RZ>(sh.m[M_RZ], o0, pitch, M2);
     if (!mbar_wait_bounded(bar, 0, err)) return;
 #pragma unroll
-    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sP, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d[q]);
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, INL>(sP, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d[q]);
     update_field_any<T, MODE, RZ>(pml, F, M, d, d, true, false, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
     store_block<T, RZ>(sh.f[A2_VX], o0, pitch, F);
 #pragma unroll
     for (int q = 0; q < RZ; q++)
 #pragma unroll
         for (int j = 0; j < 4; j++) { F[q][j] = F2[q][j]; M[q][j] = M2[q][j]; }
-    block_dz<T, MODE, TX, TZ, RZ, true>(sP, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d);
+    block_dz<T, MODE, TX, TZ, RZ, true, INL>(sP, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d);
     update_field_any<T, MODE, RZ>(pml, F, M, d, d, false, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
     store_block<T, RZ>(sh.f[A2_VZ], o0, pitch, F);
 }
 
 // Stress half-step: P += dt*L*Dx-Vx (+x C-PML), then P += dt*L*Dz-Vz (+z C-PML)
 // (lib/waves.cpp:313-404).
-template <typename T, int MODE, int TX, int TZ, int RZ>
+template <typename T, int MODE, int TX, int TZ, int RZ, bool INL>
 __device__ __forceinline__ void a2d_stress_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
                                                 const T *sVx, const T *sVz, const CoefSet<T> &cs, int *err,
                                                 uint64_t *bar)
@@ -612,8 +612,8 @@ __device__ __forceinline__ void a2d_stress_tile(const Step2DArgs<T> &a, const Sh
     load_block<T, RZ>(sh.m[M_L], o0, pitch, M);
     if (!mbar_wait_bounded(bar, 0, err)) return;
 #pragma unroll
-    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ>(sVx, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
-    block_dz<T, MODE, TX, TZ, RZ, false>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
+    for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, INL>(sVx, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
+    block_dz<T, MODE, TX, TZ, RZ, false, INL>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
     update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 0, false);
     store_block<T, RZ>(sh.f[A2_P], o0, pitch, F);
 }
@@ -763,7 +763,7 @@ __device__ __forceinline__ void e2d_stress_tile(const Step2DArgs<T> &a, const Sh
 
 // ------------------------------------------------------------------ kernels
 
-template <typename T, int MODE, int TX, int TZ, int RZ, int MINB>
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, bool INL>
 __global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
 a2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
 {
@@ -778,10 +778,10 @@ a2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, 
     load_coefs(cs, coefs);
     __syncthreads();
     const T *sP = reinterpret_cast<const T *>(sm);
-    a2d_velocity_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, sP, cs, err, bar);
+    a2d_velocity_tile<T, MODE, TX, TZ, RZ, INL>(a, sh, tl, sP, cs, err, bar);
 }
 
-template <typename T, int MODE, int TX, int TZ, int RZ, int MINB>
+template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, bool INL>
 __global__ void __launch_bounds__(Geo2D<T, TX, TZ, RZ>::NT, MINB)
 a2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, int *err)
 {
@@ -797,7 +797,7 @@ a2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, in
     load_coefs(cs, coefs);
     __syncthreads();
     const T *sVx = reinterpret_cast<const T *>(sm), *sVz = reinterpret_cast<const T *>(sm + G::TILE_STRIDE);
-    a2d_stress_tile<T, MODE, TX, TZ, RZ>(a, sh, tl, sVx, sVz, cs, err, bar);
+    a2d_stress_tile<T, MODE, TX, TZ, RZ, INL>(a, sh, tl, sVx, sVz, cs, err, bar);
 }
 
 // Adjoint work arrays in place: wrk1 = L2M*Sxx + L*Szz, wrk3 = L*Sxx + L2M*Szz,
@@ -987,16 +987,22 @@ cudaError_t launch_2d_cfg(int physics, int half, int flags, const Step2DArgs<T> 
 {
     using G = Geo2D<T, TX, TZ, RZ>;
     using S = Smem2D<T, TX, TZ, RZ>;
-    const bool adj = (flags & LAUNCH_ADJ) != 0;
+    const bool adj = (flags & LAUNCH_ADJ) != 0, inl = (flags & LAUNCH_INL) != 0;
     if (physics == PHYS_A2D) {
         if (half == 0) {
-            static const cudaError_t e = set_smem(a2d_velocity<T, MODE, TX, TZ, RZ, MINB>, S::bytes(1));
-            if (e != cudaSuccess) return e;
-            a2d_velocity<T, MODE, TX, TZ, RZ, MINB><<<grid, G::NT, S::bytes(1), st>>>(a, coefs, maps, err);
+            static const cudaError_t e0 = set_smem(a2d_velocity<T, MODE, TX, TZ, RZ, MINB, false>, S::bytes(1));
+            static const cudaError_t e1 = set_smem(a2d_velocity<T, MODE, TX, TZ, RZ, MINB, true>, S::bytes(1));
+            if (e0 != cudaSuccess) return e0;
+            if (e1 != cudaSuccess) return e1;
+            if (inl) a2d_velocity<T, MODE, TX, TZ, RZ, MINB, true><<<grid, G::NT, S::bytes(1), st>>>(a, coefs, maps, err);
+            else a2d_velocity<T, MODE, TX, TZ, RZ, MINB, false><<<grid, G::NT, S::bytes(1), st>>>(a, coefs, maps, err);
         } else {
-            static const cudaError_t e = set_smem(a2d_stress<T, MODE, TX, TZ, RZ, MINB>, S::bytes(2));
-            if (e != cudaSuccess) return e;
-            a2d_stress<T, MODE, TX, TZ, RZ, MINB><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
+            static const cudaError_t e0 = set_smem(a2d_stress<T, MODE, TX, TZ, RZ, MINB, false>, S::bytes(2));
+            static const cudaError_t e1 = set_smem(a2d_stress<T, MODE, TX, TZ, RZ, MINB, true>, S::bytes(2));
+            if (e0 != cudaSuccess) return e0;
+            if (e1 != cudaSuccess) return e1;
+            if (inl) a2d_stress<T, MODE, TX, TZ, RZ, MINB, true><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
+            else a2d_stress<T, MODE, TX, TZ, RZ, MINB, false><<<grid, G::NT, S::bytes(2), st>>>(a, coefs, maps, err);
         }
     } else {
         if (half == 0) {

@@ -49,6 +49,12 @@ void set_error(const char *fmt, ...)
 
 static inline size_t rup(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
+// Acoustic batches of at most this many tiles (about one wave of resident CTAs on
+// B200: 148 SMs x 6) launch the tile kernels with inlined edge stencils.  Measured:
+// one 541x341 shot (187 tiles) 6.2 -> 8.4 Gpts/s; 64 shots of 641x241 (10,752
+// tiles) 25.1 -> 23.3 FWI gradients/s, so large batches keep the stencil calls.
+static constexpr int INLINE_EDGE_TILES = 888;
+
 // Coefficient rows for each stencil half-length K (lib/der.cpp:3-53).  The values
 // are the reference's optimised staggered-grid coefficients; row K holds the K
 // pairs used where the reference reduces the order near an array end.  The K=1
@@ -668,7 +674,10 @@ rsgpu_status Plan::launch_step(int it_base, const int *it_dev, bool adj, cudaEve
     if (prec == PREC_F64) make_args<double>(args, *this);
     else make_args<float>(args, *this);
     const int grid = ntiles;
-    const int flags = adj ? LAUNCH_ADJ : 0;
+    // acoustic plans of at most about one wave of tiles: inlined edge stencils (the
+    // edge tiles, up to 4.4x slower than interior ones with the stencil calls,
+    // otherwise set the time of a launch that has no second wave to hide them)
+    const int flags = (adj ? LAUNCH_ADJ : 0) | (phys == PHYS_A2D && ntiles <= INLINE_EDGE_TILES ? LAUNCH_INL : 0);
     const bool mh = march && !adj;
     cudaError_t e;
     // external records so the events become timestamp nodes of a captured graph

@@ -17,8 +17,10 @@ enum { TILECFG_64x32 = 0, TILECFG_32x16 = 3, TILECFG_DEFAULT = 6, TILECFG_E2D_FA
 
 // One half-step (half = 0 velocity, 1 stress) of every tile in args.
 // maps: per shot NMAP2D CUtensorMaps of the halo-loaded fields; err: device error word.
-// flags: LAUNCH_ADJ (adjoint kernels)
-enum { LAUNCH_ADJ = 1 };
+// flags: LAUNCH_ADJ (adjoint kernels), LAUNCH_INL (acoustic: the kernels whose
+// reduced-order edge stencils are inlined; faster when the batch's tiles fit about
+// one wave, slower for large batches; the elastic kernels always inline them)
+enum { LAUNCH_ADJ = 1, LAUNCH_INL = 2 };
 cudaError_t launch_step_2d(int prec, int cfg, int physics, int half, int flags, const void *args, const void *coefs,
                            const void *maps, int *err, int grid, cudaStream_t st);
 constexpr int NMAP2D = 5;
