@@ -725,9 +725,9 @@ __device__ __forceinline__ void e2d_stress_tile(const Step2DArgs<T> &a, const Sh
                                                 int *err, uint32_t phase = 0)
 {
     RS_TILE_SETUP();
-    T d1[RZ][4], d2[RZ][4];
+    T d1[RZ][4], d2[RZ][4], sxx[RZ][4], szz[RZ][4];
     {
-        T sxx[RZ][4], szz[RZ][4], l[RZ][4], l2m[RZ][4];
+        T l[RZ][4], l2m[RZ][4];
         load_block_rw<T, RZ>(sh.f[E2_SXX], o0, pitch, sxx);
         load_block_rw<T, RZ>(sh.f[E2_SZZ], o0, pitch, szz);
         if (!ADJ) {
@@ -746,13 +746,16 @@ __device__ __forceinline__ void e2d_stress_tile(const Step2DArgs<T> &a, const Sh
         block_dz<T, MODE, TX, TZ, RZ, false, true>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
         if (pml) update_normal<T, MODE, RZ, true, ADJ>(sxx, szz, l, l2m, d1, d2, sh, a, gx, gz);
         else update_normal<T, MODE, RZ, false, ADJ>(sxx, szz, l, l2m, d1, d2, sh, a, gx, gz);
-        store_block<T, RZ>(sh.f[E2_SXX], o0, pitch, sxx);
-        store_block<T, RZ>(sh.f[E2_SZZ], o0, pitch, szz);
     }
     {
+        // the shear inputs are requested before the normal stresses are stored: a
+        // load that follows a store to memory the compiler cannot tell apart waits
+        // behind it
         T F[RZ][4], M[RZ][4];
         load_block_rw<T, RZ>(sh.f[E2_SXZ], o0, pitch, F);
         if (!ADJ) load_block<T, RZ>(sh.m[M_M], o0, pitch, M);
+        store_block<T, RZ>(sh.f[E2_SXX], o0, pitch, sxx);
+        store_block<T, RZ>(sh.f[E2_SZZ], o0, pitch, szz);
 #pragma unroll
         for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, true>(sVz, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
         block_dz<T, MODE, TX, TZ, RZ, true, true>(sVx, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
