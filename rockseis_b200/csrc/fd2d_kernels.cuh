@@ -512,6 +512,90 @@ __device__ __forceinline__ void store_block(T *base, int o0, int pitch, const T 
         *reinterpret_cast<typename Vec4<T>::type *>(base + o0 + q * pitch) = {v[q][0], v[q][1], v[q][2], v[q][3]};
 }
 
+// C-PML memory variables of a thread's RZ x 4 block in the x strip and the z strip,
+// all loaded before any is stored back, so that the loads are in flight together
+// (a load that follows a store to memory the compiler cannot tell apart waits
+// behind it: one L2 round trip per point otherwise).  Costs 2 x RZ x 4 registers,
+// so only the kernels with room for them (the elastic ones) use it.
+template <typename T, int RZ>
+struct PmlBlock {
+    int xi[4], xb[4], xc[4];     // per column: x strip index (-1: none), table base, psix column
+    int zi[RZ], zb[RZ], zr[RZ];  // per row: z strip index (-1: none), table base, psiz row
+    bool rowin[RZ], colin[4];
+    T px[RZ][4], pz[RZ][4];
+    __device__ __forceinline__ bool ux(int q, int j) const { return xi[j] >= 0 && rowin[q]; }
+    __device__ __forceinline__ bool uz(int q, int j) const { return zi[q] >= 0 && colin[j]; }
+    __device__ __forceinline__ void load(const Shot2D<T> &sh, int lpml, int gx, int gz, const T *psix, const T *psiz,
+                                         bool has1, bool has2)
+    {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            xi[j] = has1 ? xstrip(gx + j, sh.nxp, lpml, xb[j], xc[j]) : -1;
+            colin[j] = gx + j < sh.nxp;
+        }
+#pragma unroll
+        for (int q = 0; q < RZ; q++) {
+            zi[q] = has2 ? zstrip(gz + q, sh.nzp, lpml, zb[q], zr[q]) : -1;
+            rowin[q] = gz + q < sh.nzp;
+        }
+#pragma unroll
+        for (int q = 0; q < RZ; q++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                px[q][j] = ux(q, j) ? psix[(gz + q) * 2 * lpml + xc[j]] : T(0);
+                pz[q][j] = uz(q, j) ? psiz[zr[q] * sh.nxp + gx + j] : T(0);
+            }
+    }
+    __device__ __forceinline__ void store(const Shot2D<T> &sh, int lpml, int gx, int gz, T *psix, T *psiz) const
+    {
+#pragma unroll
+        for (int q = 0; q < RZ; q++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (ux(q, j)) psix[(gz + q) * 2 * lpml + xc[j]] = px[q][j];
+                if (uz(q, j)) psiz[zr[q] * sh.nxp + gx + j] = pz[q][j];
+            }
+    }
+};
+
+// One C-PML memory update with the memory value in a register (pml_correct's
+// arithmetic): psi = B*psi + A*df; F -= a*(psi + C*df).
+template <typename T, int MODE>
+__device__ __forceinline__ T pml_step(T F, T a, T df, T &psi, const T *tab, int lp, int base, int idx)
+{
+    using A = Ar<T, MODE>;
+    const T tA = __ldg(tab + (base + PT_A) * lp + idx);
+    const T tB = __ldg(tab + (base + PT_B) * lp + idx);
+    const T tC = __ldg(tab + (base + PT_C) * lp + idx);
+    psi = A::mad(A::mul(tB, psi), tA, df);
+    return A::msub(F, a, A::mad(psi, tC, df));
+}
+
+// update_field with the block's C-PML memory gathered first (PmlBlock).
+template <typename T, int MODE, int RZ>
+__device__ __forceinline__ void update_field_g(T (&F)[RZ][4], const T (&Mo)[RZ][4], const T (&d1)[RZ][4],
+                                               const T (&d2)[RZ][4], const Shot2D<T> &sh, const Step2DArgs<T> &a,
+                                               int gx, int gz, T *psix, int xb_add, T *psiz, int zb_add, bool const_mod)
+{
+    using A = Ar<T, MODE>;
+    PmlBlock<T, RZ> pm;
+    pm.load(sh, a.lpml, gx, gz, psix, psiz, true, true);
+#pragma unroll
+    for (int q = 0; q < RZ; q++) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const T am = const_mod ? a.dt : A::mul(a.dt, Mo[q][j]);
+            F[q][j] = A::mad(F[q][j], am, d1[q][j]);
+            if (pm.ux(q, j))
+                F[q][j] = pml_step<T, MODE>(F[q][j], am, d1[q][j], pm.px[q][j], a.pml, a.lpml, pm.xb[j] + xb_add, pm.xi[j]);
+            F[q][j] = A::mad(F[q][j], am, d2[q][j]);
+            if (pm.uz(q, j))
+                F[q][j] = pml_step<T, MODE>(F[q][j], am, d2[q][j], pm.pz[q][j], a.pml, a.lpml, pm.zb[q] + zb_add, pm.zi[q]);
+        }
+    }
+    pm.store(sh, a.lpml, gx, gz, psix, psiz);
+}
+
 // x-part then z-part of one field, a = dt*modulus (lib/waves.cpp:245-307):
 //   F += a*d1 ; [x strip] psi = B*psi + A*d1, F -= a*(psi + C*d1) ;
 //   F += a*d2 ; [z strip] the same with the z memory variable.
@@ -640,7 +724,8 @@ __device__ __forceinline__ void e2d_velocity_tile(const Step2DArgs<T> &a, const 
 #pragma unroll
     for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, true>(sXX, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
     block_dz<T, MODE, TX, TZ, RZ, false, true>(sXZ, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
-    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 0, false);
+    if (pml) update_field_g<T, MODE, RZ>(F, M, d1, d2, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 0, false);
+    else update_field<T, MODE, RZ, false>(F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 0, false);
     store_block<T, RZ>(sh.f[E2_VX], o0, pitch, F);
 #pragma unroll
     for (int q = 0; q < RZ; q++)
@@ -649,7 +734,8 @@ __device__ __forceinline__ void e2d_velocity_tile(const Step2DArgs<T> &a, const 
 #pragma unroll
     for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, true>(sXZ, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
     block_dz<T, MODE, TX, TZ, RZ, true, true>(sZZ, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
-    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 3, false);
+    if (pml) update_field_g<T, MODE, RZ>(F, M, d1, d2, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 3, false);
+    else update_field<T, MODE, RZ, false>(F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 3, false);
     store_block<T, RZ>(sh.f[E2_VZ], o0, pitch, F);
 }
 
@@ -664,56 +750,53 @@ __device__ __forceinline__ void update_normal(T (&sxx)[RZ][4], T (&szz)[RZ][4], 
                                               const Shot2D<T> &sh, const Step2DArgs<T> &a, int gx, int gz)
 {
     using A = Ar<T, MODE>;
+    PmlBlock<T, RZ> pm;
+    if (PML) pm.load(sh, a.lpml, gx, gz, sh.psix[2], sh.psiz[2], true, true);
 #pragma unroll
     for (int q = 0; q < RZ; q++) {
-        const int iz = gz + q;
-        int zb = 0, zrow = 0, zi = -1;
-        if (PML) zi = zstrip(iz, sh.nzp, a.lpml, zb, zrow);
-        const bool fsrow = sh.fs && iz == a.lpml;
+        const bool fsrow = sh.fs && gz + q == a.lpml;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const int ix = gx + j;
-            int xb = 0, xcol = 0, xi = -1;
-            if (PML && iz < sh.nzp) xi = xstrip(ix, sh.nxp, a.lpml, xb, xcol);
             if (!ADJ) {
                 const T a2 = A::mul(a.dt, l2m[q][j]), a1 = A::mul(a.dt, l[q][j]);
                 sxx[q][j] = A::mad(sxx[q][j], a2, d1[q][j]);
                 szz[q][j] = A::mad(szz[q][j], a1, d1[q][j]);
-                if (PML && xi >= 0) {
-                    T *ps = sh.psix[2] + iz * 2 * a.lpml + xcol;
+                if (PML && pm.ux(q, j)) {
+                    const int xb = pm.xb[j], xi = pm.xi[j];
                     const T tA = __ldg(a.pml + (xb + PT_A) * a.lpml + xi), tB = __ldg(a.pml + (xb + PT_B) * a.lpml + xi),
                             tC = __ldg(a.pml + (xb + PT_C) * a.lpml + xi);
-                    const T p = A::mad(A::mul(tB, *ps), tA, d1[q][j]);
-                    *ps = p;
+                    const T p = A::mad(A::mul(tB, pm.px[q][j]), tA, d1[q][j]);
+                    pm.px[q][j] = p;
                     const T cq = A::mad(p, tC, d1[q][j]);
                     sxx[q][j] = A::msub(sxx[q][j], a2, cq);
                     szz[q][j] = A::msub(szz[q][j], a1, cq);
                 }
                 sxx[q][j] = A::mad(sxx[q][j], a1, d2[q][j]);
                 szz[q][j] = A::mad(szz[q][j], a2, d2[q][j]);
-                if (PML && zi >= 0 && ix < sh.nxp) {
-                    T *ps = sh.psiz[2] + zrow * sh.nxp + ix;
+                if (PML && pm.uz(q, j)) {
+                    const int zb = pm.zb[q], zi = pm.zi[q];
                     const T tA = __ldg(a.pml + (zb + PT_A) * a.lpml + zi), tB = __ldg(a.pml + (zb + PT_B) * a.lpml + zi),
                             tC = __ldg(a.pml + (zb + PT_C) * a.lpml + zi);
-                    const T p = A::mad(A::mul(tB, *ps), tA, d2[q][j]);
-                    *ps = p;
+                    const T p = A::mad(A::mul(tB, pm.pz[q][j]), tA, d2[q][j]);
+                    pm.pz[q][j] = p;
                     const T cq = A::mad(p, tC, d2[q][j]);
                     sxx[q][j] = A::msub(sxx[q][j], a1, cq);
                     szz[q][j] = A::msub(szz[q][j], a2, cq);
                 }
             } else {
                 sxx[q][j] = A::mad(sxx[q][j], a.dt, d1[q][j]);
-                if (PML && xi >= 0)
-                    sxx[q][j] = pml_correct<T, MODE>(sxx[q][j], a.dt, d1[q][j], sh.psix[2] + iz * 2 * a.lpml + xcol,
-                                                     a.pml, a.lpml, xb, xi);
+                if (PML && pm.ux(q, j))
+                    sxx[q][j] = pml_step<T, MODE>(sxx[q][j], a.dt, d1[q][j], pm.px[q][j], a.pml, a.lpml, pm.xb[j],
+                                                  pm.xi[j]);
                 szz[q][j] = A::mad(szz[q][j], a.dt, d2[q][j]);
-                if (PML && zi >= 0 && ix < sh.nxp)
-                    szz[q][j] = pml_correct<T, MODE>(szz[q][j], a.dt, d2[q][j], sh.psiz[2] + zrow * sh.nxp + ix, a.pml,
-                                                     a.lpml, zb, zi);
+                if (PML && pm.uz(q, j))
+                    szz[q][j] = pml_step<T, MODE>(szz[q][j], a.dt, d2[q][j], pm.pz[q][j], a.pml, a.lpml, pm.zb[q],
+                                                  pm.zi[q]);
             }
             if (fsrow) szz[q][j] = T(0);
         }
     }
+    if (PML) pm.store(sh, a.lpml, gx, gz, sh.psix[2], sh.psiz[2]);
 }
 
 // Stress half-step.  Forward (lib/waves.cpp:1571-1735): normal stresses as
@@ -759,7 +842,8 @@ __device__ __forceinline__ void e2d_stress_tile(const Step2DArgs<T> &a, const Sh
 #pragma unroll
         for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, true>(sVz, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
         block_dz<T, MODE, TX, TZ, RZ, true, true>(sVx, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
-        update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[3], 3, sh.psiz[3], 3, ADJ);
+        if (pml) update_field_g<T, MODE, RZ>(F, M, d1, d2, sh, a, gx, gz, sh.psix[3], 3, sh.psiz[3], 3, ADJ);
+        else update_field<T, MODE, RZ, false>(F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[3], 3, sh.psiz[3], 3, ADJ);
         store_block<T, RZ>(sh.f[E2_SXZ], o0, pitch, F);
     }
 }
