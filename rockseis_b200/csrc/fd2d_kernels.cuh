@@ -575,22 +575,29 @@ __device__ __forceinline__ T pml_step(T F, T a, T df, T &psi, const T *tab, int 
 template <typename T, int MODE, int RZ>
 __device__ __forceinline__ void update_field_g(T (&F)[RZ][4], const T (&Mo)[RZ][4], const T (&d1)[RZ][4],
                                                const T (&d2)[RZ][4], const Shot2D<T> &sh, const Step2DArgs<T> &a,
-                                               int gx, int gz, T *psix, int xb_add, T *psiz, int zb_add, bool const_mod)
+                                               int gx, int gz, T *psix, int xb_add, T *psiz, int zb_add, bool const_mod,
+                                               bool has1 = true, bool has2 = true)
 {
     using A = Ar<T, MODE>;
     PmlBlock<T, RZ> pm;
-    pm.load(sh, a.lpml, gx, gz, psix, psiz, true, true);
+    pm.load(sh, a.lpml, gx, gz, psix, psiz, has1, has2);
 #pragma unroll
     for (int q = 0; q < RZ; q++) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const T am = const_mod ? a.dt : A::mul(a.dt, Mo[q][j]);
-            F[q][j] = A::mad(F[q][j], am, d1[q][j]);
-            if (pm.ux(q, j))
-                F[q][j] = pml_step<T, MODE>(F[q][j], am, d1[q][j], pm.px[q][j], a.pml, a.lpml, pm.xb[j] + xb_add, pm.xi[j]);
-            F[q][j] = A::mad(F[q][j], am, d2[q][j]);
-            if (pm.uz(q, j))
-                F[q][j] = pml_step<T, MODE>(F[q][j], am, d2[q][j], pm.pz[q][j], a.pml, a.lpml, pm.zb[q] + zb_add, pm.zi[q]);
+            if (has1) {
+                F[q][j] = A::mad(F[q][j], am, d1[q][j]);
+                if (pm.ux(q, j))
+                    F[q][j] = pml_step<T, MODE>(F[q][j], am, d1[q][j], pm.px[q][j], a.pml, a.lpml, pm.xb[j] + xb_add,
+                                                pm.xi[j]);
+            }
+            if (has2) {
+                F[q][j] = A::mad(F[q][j], am, d2[q][j]);
+                if (pm.uz(q, j))
+                    F[q][j] = pml_step<T, MODE>(F[q][j], am, d2[q][j], pm.pz[q][j], a.pml, a.lpml, pm.zb[q] + zb_add,
+                                                pm.zi[q]);
+            }
         }
     }
     pm.store(sh, a.lpml, gx, gz, psix, psiz);
@@ -645,6 +652,18 @@ __device__ __forceinline__ void update_field_any(bool pml, T (&F)[RZ][4], const 
     else update_field<T, MODE, RZ, false>(F, Mo, d1, d2, has1, has2, sh, a, gx, gz, psix, xb_add, psiz, zb_add, const_mod);
 }
 
+// C-PML update of a tile: gathered memory loads (GAT, for tile shapes with the
+// registers for them) or the point-by-point form.
+template <typename T, int MODE, int RZ, bool GAT>
+__device__ __forceinline__ void update_field_sel(bool pml, T (&F)[RZ][4], const T (&Mo)[RZ][4], const T (&d1)[RZ][4],
+                                                 const T (&d2)[RZ][4], bool has1, bool has2, const Shot2D<T> &sh,
+                                                 const Step2DArgs<T> &a, int gx, int gz, T *psix, int xb_add, T *psiz,
+                                                 int zb_add, bool const_mod)
+{
+    if (GAT && pml) update_field_g<T, MODE, RZ>(F, Mo, d1, d2, sh, a, gx, gz, psix, xb_add, psiz, zb_add, const_mod, has1, has2);
+    else update_field_any<T, MODE, RZ>(pml, F, Mo, d1, d2, has1, has2, sh, a, gx, gz, psix, xb_add, psiz, zb_add, const_mod);
+}
+
 #define RS_TILE_SETUP()                                                                        \
     using G = Geo2D<T, TX, TZ, RZ>;                                                            \
     const int tx = threadIdx.x % G::NTX, tz = threadIdx.x / G::NTX;                            \
@@ -659,7 +678,7 @@ __device__ __forceinline__ void update_field_any(bool pml, T (&F)[RZ][4], const 
 
 // Velocity half-step: Vx += dt*Rx*Dx+P (+ x C-PML), Vz += dt*Rz*Dz+P (+ z C-PML)
 // (lib/waves.cpp:217-310).
-template <typename T, int MODE, int TX, int TZ, int RZ, bool INL>
+template <typename T, int MODE, int TX, int TZ, int RZ, bool INL, bool GAT>
 __device__ __forceinline__ void a2d_velocity_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
                                                   const T *sP, const CoefSet<T> &cs, int *err, uint64_t *bar)
 {
@@ -672,20 +691,20 @@ __device__ __forceinline__ void a2d_velocity_tile(const Step2DArgs<T> &a, const 
     if (!mbar_wait_bounded(bar, 0, err)) return;
 #pragma unroll
     for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, INL>(sP, zr + q + GUARD, xq, cs, cux, true, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d[q]);
-    update_field_any<T, MODE, RZ>(pml, F, M, d, d, true, false, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
+    update_field_sel<T, MODE, RZ, GAT>(pml, F, M, d, d, true, false, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
     store_block<T, RZ>(sh.f[A2_VX], o0, pitch, F);
 #pragma unroll
     for (int q = 0; q < RZ; q++)
 #pragma unroll
         for (int j = 0; j < 4; j++) { F[q][j] = F2[q][j]; M[q][j] = M2[q][j]; }
     block_dz<T, MODE, TX, TZ, RZ, true, INL>(sP, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d);
-    update_field_any<T, MODE, RZ>(pml, F, M, d, d, false, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
+    update_field_sel<T, MODE, RZ, GAT>(pml, F, M, d, d, false, true, sh, a, gx, gz, sh.psix[0], 3, sh.psiz[0], 3, false);
     store_block<T, RZ>(sh.f[A2_VZ], o0, pitch, F);
 }
 
 // Stress half-step: P += dt*L*Dx-Vx (+x C-PML), then P += dt*L*Dz-Vz (+z C-PML)
 // (lib/waves.cpp:313-404).
-template <typename T, int MODE, int TX, int TZ, int RZ, bool INL>
+template <typename T, int MODE, int TX, int TZ, int RZ, bool INL, bool GAT>
 __device__ __forceinline__ void a2d_stress_tile(const Step2DArgs<T> &a, const Shot2D<T> &sh, const Tile2D &tl,
                                                 const T *sVx, const T *sVz, const CoefSet<T> &cs, int *err,
                                                 uint64_t *bar)
@@ -698,7 +717,7 @@ __device__ __forceinline__ void a2d_stress_tile(const Step2DArgs<T> &a, const Sh
 #pragma unroll
     for (int q = 0; q < RZ; q++) row_dx<T, MODE, TX, TZ, RZ, INL>(sVx, zr + q + GUARD, xq, cs, cux, false, xe, gx, sh.nxp, a.order, a.dx, a.rdx, d1[q]);
     block_dz<T, MODE, TX, TZ, RZ, false, INL>(sVz, zr, xq, cs, cuz, ze, gz, sh.nzp, a.order, a.dz, a.rdz, d2);
-    update_field_any<T, MODE, RZ>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 0, false);
+    update_field_sel<T, MODE, RZ, GAT>(pml, F, M, d1, d2, true, true, sh, a, gx, gz, sh.psix[1], 0, sh.psiz[1], 0, false);
     store_block<T, RZ>(sh.f[A2_P], o0, pitch, F);
 }
 
@@ -865,7 +884,7 @@ a2d_velocity(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, 
     load_coefs(cs, coefs);
     __syncthreads();
     const T *sP = reinterpret_cast<const T *>(sm);
-    a2d_velocity_tile<T, MODE, TX, TZ, RZ, INL>(a, sh, tl, sP, cs, err, bar);
+    a2d_velocity_tile<T, MODE, TX, TZ, RZ, INL, (65536 / (Geo2D<T, TX, TZ, RZ>::NT * MINB) >= 128)>(a, sh, tl, sP, cs, err, bar);
 }
 
 template <typename T, int MODE, int TX, int TZ, int RZ, int MINB, bool INL>
@@ -884,7 +903,7 @@ a2d_stress(Step2DArgs<T> a, const CoefSet<T> *coefs, const CUtensorMap *maps, in
     load_coefs(cs, coefs);
     __syncthreads();
     const T *sVx = reinterpret_cast<const T *>(sm), *sVz = reinterpret_cast<const T *>(sm + G::TILE_STRIDE);
-    a2d_stress_tile<T, MODE, TX, TZ, RZ, INL>(a, sh, tl, sVx, sVz, cs, err, bar);
+    a2d_stress_tile<T, MODE, TX, TZ, RZ, INL, (65536 / (Geo2D<T, TX, TZ, RZ>::NT * MINB) >= 128)>(a, sh, tl, sVx, sVz, cs, err, bar);
 }
 
 // Adjoint work arrays in place: wrk1 = L2M*Sxx + L*Szz, wrk3 = L*Sxx + L2M*Szz,

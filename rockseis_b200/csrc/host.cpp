@@ -303,7 +303,10 @@ rsgpu_status Plan::create(const rsgpu_config *c, int ns, const rsgpu_shot *s, co
     if (shared_stream) stream = shared_stream;
     else CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 
-    tilecfg = (c->tile >= 0 && c->tile < tile_count_2d()) ? c->tile : default_tile();
+    long tiles32 = 0;   // 32x32 tiles of the batch (the default shape's count)
+    for (int i = 0; i < ns; i++)
+        tiles32 += (long)((s[i].nx + 2 * c->lpml + 31) / 32) * ((s[i].nz + 2 * c->lpml + 31) / 32);
+    tilecfg = (c->tile >= 0 && c->tile < tile_count_2d()) ? c->tile : default_tile(tiles32);
     // the FP64 oracle propagator is built for two tile shapes only
     if (prec == PREC_F64 && tilecfg != TILECFG_64x32 && tilecfg != TILECFG_32x16) tilecfg = TILECFG_64x32;
     const TileShape ts = tile_shape_2d(tilecfg);
@@ -635,13 +638,17 @@ void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L,
     std::memcpy(irp, &r, sizeof r);
 }
 
-int Plan::default_tile() const
+int Plan::default_tile(long tiles32) const
 {
     // Elastic FAST forward propagation: 32x16 tiles at eight CTAs per SM measured
     // fastest on B200 (16-shot 801x401 batch: 34.5 Gpts/s against 27.3 for 32x32
     // tiles at six, whose kernels carry the inlined reduced-order stencils in more
-    // registers); the other kernels keep 32x32 tiles at six CTAs per SM.
+    // registers).  Acoustic FAST batches of about one wave of tiles (one 541x341
+    // shot): the same shape, whose register budget also holds the gathered C-PML
+    // memory (9.8 Gpts/s against 8.6); large acoustic batches (the 64-shot FWI:
+    // 25.0 against 22.5 gradients/s) and all other plans keep 32x32 tiles at six.
     if (phys == PHYS_E2D && prec == PREC_F32_FAST && !adjoint_steps) return TILECFG_E2D_FAST;
+    if (phys == PHYS_A2D && prec == PREC_F32_FAST && tiles32 <= INLINE_EDGE_TILES / 2) return TILECFG_E2D_FAST;
     return TILECFG_DEFAULT;
 }
 

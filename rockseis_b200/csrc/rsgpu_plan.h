@@ -125,7 +125,7 @@ private:
     // builds the fused step's tables; inj_pts[shot*MAXSETS + set] = the set's CSR target offsets
     rsgpu_status setup_fused(const std::vector<std::vector<int>> &inj_pts);
     rsgpu_status check_config(const rsgpu_config *c, int ns, const rsgpu_shot *s, bool sets_given);
-    int default_tile() const;
+    int default_tile(long tiles32) const;   // tiles32: the batch's count of 32x32 tiles
     template <typename T>
     void fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L, size_t org, const SetOffsets *so,
                    const ShotSets &t);
