@@ -640,15 +640,15 @@ void Plan::fill_desc(unsigned char *sd, unsigned char *irp, const ShotLayout &L,
 
 int Plan::default_tile(long tiles32) const
 {
-    // Elastic FAST forward propagation: 32x16 tiles at eight CTAs per SM measured
-    // fastest on B200 (16-shot 801x401 batch: 34.5 Gpts/s against 27.3 for 32x32
-    // tiles at six, whose kernels carry the inlined reduced-order stencils in more
-    // registers).  Acoustic FAST batches of about one wave of tiles (one 541x341
-    // shot): the same shape, whose register budget also holds the gathered C-PML
-    // memory (9.8 Gpts/s against 8.6); large acoustic batches (the 64-shot FWI:
-    // 25.0 against 22.5 gradients/s) and all other plans keep 32x32 tiles at six.
-    if (phys == PHYS_E2D && prec == PREC_F32_FAST && !adjoint_steps) return TILECFG_E2D_FAST;
-    if (phys == PHYS_A2D && prec == PREC_F32_FAST && tiles32 <= INLINE_EDGE_TILES / 2) return TILECFG_E2D_FAST;
+    // Elastic float plans: 32x16 tiles at eight CTAs per SM, whose 128-register
+    // budget holds the inlined reduced-order stencils and the gathered C-PML memory
+    // without spills (16-shot 801x401 batch on B200: FAST 34.5 Gpts/s against 27.3
+    // for 32x32 tiles at six before the gather, EXACT 16.7 against 15.8).  Acoustic
+    // FAST batches of about one wave of tiles (one 541x341 shot): the same shape
+    // (9.8 Gpts/s against 8.6); large acoustic batches (the 64-shot FWI: 25.0
+    // against 22.5 gradients/s) and all other plans keep 32x32 tiles at six.
+    if (phys == PHYS_E2D && prec != PREC_F64) return TILECFG_E2D;
+    if (phys == PHYS_A2D && prec == PREC_F32_FAST && tiles32 <= INLINE_EDGE_TILES / 2) return TILECFG_E2D;
     return TILECFG_DEFAULT;
 }
 

@@ -13,7 +13,7 @@ enum { PREC_F32_EXACT = 0, PREC_F32_FAST = 1, PREC_F64 = 2 };
 struct TileShape { int tx, tz, rz, minb; };
 TileShape tile_shape_2d(int cfg);
 int tile_count_2d();
-enum { TILECFG_64x32 = 0, TILECFG_32x16 = 3, TILECFG_DEFAULT = 6, TILECFG_E2D_FAST = 9 };
+enum { TILECFG_64x32 = 0, TILECFG_32x16 = 3, TILECFG_DEFAULT = 6, TILECFG_E2D = 9 };
 
 // One half-step (half = 0 velocity, 1 stress) of every tile in args.
 // maps: per shot NMAP2D CUtensorMaps of the halo-loaded fields; err: device error word.
