@@ -507,14 +507,14 @@ int march_resident_ctas()
 
 cudaError_t launch_march_2d(int half, const March2DArgs &a, int nitems, cudaStream_t st)
 {
-    static bool attr = false;
-    if (!attr) {
+    // set once per process (thread-safe static initialisation)
+    static const cudaError_t attr = [] {
         cudaError_t e = cudaFuncSetAttribute(e2d_march_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)march_smem(3));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(e2d_march_stress, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)march_smem(2));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+        return e;
+    }();
+    if (attr != cudaSuccess) return attr;
     if (half == 0) e2d_march_velocity<<<nitems, MNT, march_smem(3), st>>>(a);
     else e2d_march_stress<<<nitems, MNT, march_smem(2), st>>>(a);
     return cudaGetLastError();
