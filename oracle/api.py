@@ -105,6 +105,8 @@ def _load_ref(path: str) -> C.CDLL:
     lib.ref_fwi_e2d_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_e2d_corr_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_e2d_misfit_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V, I]
+    if hasattr(lib, "ref_fwi_e2d_full_f"):
+        lib.ref_fwi_e2d_full_f.argtypes = [G, V, V, V, I, V, V, I, I, V, V, V, V, I] + [V] * 6 + [V]
     lib.ref_fwi_a2d_ilum_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I] + [V] * 5 + [V, V]
     lib.ref_fwi_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I] + [V] * 5 + [V]
     lib.ref_rtm_a2d_full_f.argtypes = [G, V, V, I, V, V, I, V, V, I, I, I, V]
@@ -421,8 +423,10 @@ def orc_modelling_a3d(pb, padded, tab, smap, sshift, wav, sfield, gmap, gshift, 
 
 
 # ---------------------------------------------------------------- elastic FWI
-def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
-    """FwiElastic2D::run_optimal; obs3 = [P, Ux, Uz] observed data, each [nr][nt]."""
+def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0, full_snapinc=0):
+    """FwiElastic2D::run_optimal; obs3 = [P, Ux, Uz] observed data, each [nr][nt].  With
+    full_snapinc > 0: FwiElastic2D::run (full Vx/Vz snapshots every full_snapinc steps,
+    DIFFERENCE misfit)."""
     g = pb.ref_grid()
     sc, gc = np.ascontiguousarray(scoords, np.float64), np.ascontiguousarray(gcoords, np.float64)
     ns, nr = len(sc), len(gc)
@@ -432,9 +436,14 @@ def ref_fwi_e2d(pb, scoords, wav, sfield, gcoords, obs3, ncheck, misfit=0):
     ress = np.zeros((3, nr, pb.nt), np.float32)
     mis = C.c_double()
     vp, vs, rho, w, op, ox, oz = _keep(pb.vp, pb.vs, pb.rho, wav, obs3[0], obs3[1], obs3[2], dtype=np.float32)
-    r = ref().ref_fwi_e2d_misfit_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc), _p(op),
-                                   _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]), _p(out["rhograd"]),
-                                   _p(wg), _p(mods), _p(ress), C.byref(mis), misfit)
+    if full_snapinc > 0:
+        r = ref().ref_fwi_e2d_full_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc),
+                                     _p(op), _p(ox), _p(oz), full_snapinc, _p(out["vpgrad"]), _p(out["vsgrad"]),
+                                     _p(out["rhograd"]), _p(wg), _p(mods), _p(ress), C.byref(mis))
+    else:
+        r = ref().ref_fwi_e2d_misfit_f(C.byref(g), _p(vp), _p(vs), _p(rho), ns, _p(sc), _p(w), sfield, nr, _p(gc),
+                                       _p(op), _p(ox), _p(oz), ncheck, _p(out["vpgrad"]), _p(out["vsgrad"]),
+                                       _p(out["rhograd"]), _p(wg), _p(mods), _p(ress), C.byref(mis), misfit)
     assert r == 1
     out.update(wavgrad=wg, datamod=mods, datares=ress, misfit=mis.value)
     return out

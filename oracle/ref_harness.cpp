@@ -153,11 +153,13 @@ int fwi_a2d(const ref_grid *g, const T *vp, const T *rho, int ns, const double *
     return r;
 }
 
-/* FwiElastic2D::run_optimal (lib/fwi.cpp:3937-4143) with P, Ux (VX) and Uz (VZ) data. */
+/* FwiElastic2D::run_optimal (lib/fwi.cpp:3937-4143) with P, Ux (VX) and Uz (VZ) data, or, with
+ * full_snapinc > 0, FwiElastic2D::run (lib/fwi.cpp:3774-3934): Vx/Vz snapshots every snapinc steps. */
 template <typename T>
 int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, const double *sc, const T *wav,
             int sfield, int nr, const double *gc, const T *obsp, const T *obsx, const T *obsz, int ncheck, T *vpgrad,
-            T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit, int misfit_type = 0)
+            T *vsgrad, T *rhograd, T *wavgrad, T *mods, T *ress, double *misfit, int misfit_type = 0,
+            int full_snapinc = 0)
 {
     auto model = make_e2d<T>(g, vp, vs, rho);
     auto geom = model->getGeom();
@@ -177,7 +179,7 @@ int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
         img[k] = std::make_shared<Image2D<T>>(g->nx, g->nz, 1, 1, (T)g->dx, (T)g->dz, (T)g->ox, (T)g->oz);
         img[k]->allocateImage();
     }
-    FwiElastic2D<T> fwi(model, src, dp, dx, dz, g->order, 1);
+    FwiElastic2D<T> fwi(model, src, dp, dx, dz, g->order, full_snapinc > 0 ? full_snapinc : 1);
     fwi.setDatamodP(dm[0]); fwi.setDatamodUx(dm[1]); fwi.setDatamodUz(dm[2]);
     fwi.setDataresP(dr[0]); fwi.setDataresUx(dr[1]); fwi.setDataresUz(dr[2]);
     fwi.setVpgrad(img[0]); fwi.setVsgrad(img[1]); fwi.setRhograd(img[2]);
@@ -186,7 +188,7 @@ int fwi_e2d(const ref_grid *g, const T *vp, const T *vs, const T *rho, int ns, c
     fwi.setNcheck(ncheck);
     fwi.setIncore(true);
     fwi.setSnapfile(tmpname("fwie2d"));
-    int r = fwi.run_optimal();
+    int r = full_snapinc > 0 ? fwi.run() : fwi.run_optimal();
     size_t n = (size_t)g->nx * g->nz, nd = (size_t)nr * g->nt;
     std::memcpy(vpgrad, img[0]->getImagedata(), sizeof(T) * n);
     std::memcpy(vsgrad, img[1]->getImagedata(), sizeof(T) * n);
@@ -637,6 +639,15 @@ int ref_fwi_e2d_corr_f(const ref_grid *g, const float *vp, const float *vs, cons
 {
     return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, ncheck, vpgrad, vsgrad,
                           rhograd, wavgrad, mods, ress, misfit, 1);
+}
+/* FwiElastic2D::run (lib/fwi.cpp:3774-3934): full Vx/Vz snapshots every snapinc steps. */
+int ref_fwi_e2d_full_f(const ref_grid *g, const float *vp, const float *vs, const float *rho, int ns,
+                       const double *sc, const float *wav, int sfield, int nr, const double *gc, const float *obsp,
+                       const float *obsx, const float *obsz, int snapinc, float *vpgrad, float *vsgrad,
+                       float *rhograd, float *wavgrad, float *mods, float *ress, double *misfit)
+{
+    return fwi_e2d<float>(g, vp, vs, rho, ns, sc, wav, sfield, nr, gc, obsp, obsx, obsz, 0, vpgrad, vsgrad,
+                          rhograd, wavgrad, mods, ress, misfit, 0, snapinc);
 }
 /* FwiElastic2D::run_optimal with any rs_fwimisfit value (ADAPTIVE_GAUSS = 2, ADAPTIVE_LINEAR = 3,
  * ADAPTIVE_SINGLE = 4). */

@@ -381,3 +381,35 @@ def test_snapshot_enddiff_and_count():
             dt = np.float32(6e-4)
             enddiff = int(np.rint(np.float32((nt - 1) * dt - (snapnt - 1) * (dt * np.float32(si))) / dt))
             assert enddiff == (nt - 1) % si, (nt, si)
+
+
+# ---------------------------------------------------------------- FULL snapshots, elastic 2D (FwiElastic2D::run)
+def _e2d_full():
+    return np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "e2d_full.npz"))
+
+
+@needs_ref
+def test_e2d_full_fixture_matches_reference_live():
+    """tests/golden/e2d_full.npz (make_golden_e2d_full.py) is what the reference's
+    FwiElastic2D::run returns on the elastic FWI case: the checker for a GPU FULL
+    elastic gradient."""
+    from tests.cases import ElasticFwiCase
+    g = _e2d_full()
+    c = ElasticFwiCase()
+    obs3 = [o.astype(np.float32) for o in c.obs]
+    assert np.array_equal(np.stack(obs3), g["obs"])
+    r = api.ref_fwi_e2d(c.pb, c.src.scoords, c.src.data.astype(np.float32), c.sfield, c.recs[0].gcoords, obs3, 0,
+                        full_snapinc=3)
+    for k in ("vpgrad", "vsgrad", "rhograd", "wavgrad"):
+        assert np.array_equal(r[k], g[f"s3_{k}"]), k
+    for k in ("datamod", "datares", "misfit"):
+        assert np.array_equal(r[k], g[k]), k
+
+
+def test_e2d_full_fixture_is_complete():
+    g = _e2d_full()
+    for si in (1, 3, 5):
+        for k in ("vpgrad", "vsgrad", "rhograd", "wavgrad"):
+            assert np.all(np.isfinite(g[f"s{si}_{k}"])), (si, k)
+    # coarser snapshots change the gradient: the adjoint correlates with older states
+    assert not np.array_equal(g["s1_vpgrad"], g["s3_vpgrad"])
